@@ -1,0 +1,200 @@
+/*
+ * mcmax_gpu.h -- C-ABI of the B200 (sm_100a) MCMax hot-path library
+ * (libmcmax_gpu.so).
+ *
+ * Two reference entry points are replaced:
+ *
+ *   ComputePart  (ComputePart.f:1)   subroutine ComputePart(p,ii,input,amin,
+ *                amax,apow,fmax,blend,porosity,inp_abun,iopac,normalize_abun,
+ *                standard,nsubgrains) -- DHS/Mie opacities of one grain bin.
+ *                Replaced by mcg_compute_part / mcg_compute_part_batch.  The
+ *                caller passes the refractive indices already read from the
+ *                .lnk files and regridded (readrefindCP, ComputePart.f:1102)
+ *                and receives what ComputePart writes into p%Kabs/Ksca/Kext
+ *                (iopac,:), p%F(iopac,:), p%rho(iopac), p%mscale/rscale.
+ *
+ *   MCRadiation  (MCRadiation.f:6)   subroutine MCRadiation(NphotTot,niter,
+ *                dofastvisc) -- the photon-packet loop.  MCRadiation reads
+ *                module globals (grid, densities, grain opacities, BB table);
+ *                the library receives them once through mcg_set_model
+ *                (mirroring what Init.f builds) and mcg_mcradiation runs the
+ *                packet loop, returning C(i,j)%EJv/EJv2/Eabs/Ni/T and the
+ *                MC spectra (MCRadiation.f:581-646).  NphotTot is in/out as
+ *                in the reference.
+ *
+ *   mcg_finalize_t replaces the temperature step that follows the call
+ *   (Main.f:498-549: EJv/V, EJv2/V^2, determineT, dEJv, dT).
+ *
+ * Layout conventions (all arrays are plain host pointers, row-major):
+ *   cells      (i,j), i = 0..nr-1 (i = 0 is the star-to-Rin cell),
+ *              j = 1..nt-1, flattened as c = i*(nt-1) + (j-1)
+ *   components q = one (grain ii, opacity set iopac) pair of the reference;
+ *              comp_w[c*ncomp + q] = C(i,j)%w(ii) * C(i,j)%wopac(ii,iopac)
+ *   Mueller    F[((q*nlam + l)*6 + e)*180 + k], e = F11,F12,F22,F33,F34,F44
+ *   BB         BB[l*(TMAX+1) + iT], TMAX = 10000 (Modules.f:5)
+ *   spectra    spec[l*31 + iangle], iangle = 1..30 (MCRadiation.f:20)
+ *
+ * Errors: every call returns mcg_status; the library never aborts the
+ * process (the reference stops on e.g. MCRadiation.f:1231).  mcg_last_error
+ * gives the message of the last failing call on a context.  A context is
+ * used from one host thread at a time.
+ */
+#ifndef MCMAX_GPU_H
+#define MCMAX_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MCG_TMAX 10000
+#define MCG_NANG 180
+#define MCG_NANGLE_SED 30
+#define MCG_NCOUNTERS 16
+
+typedef enum {
+  MCG_OK = 0,
+  MCG_ERR_ARG = 1,     /* invalid argument (sizes, null pointers, ranges) */
+  MCG_ERR_CUDA = 2,    /* a CUDA call failed */
+  MCG_ERR_STATE = 3,   /* call out of order (e.g. mcradiation before set_model) */
+  MCG_ERR_NOMEM = 4,   /* device allocation failed */
+  MCG_ERR_LIMIT = 5,   /* a size is beyond a documented maximum */
+  MCG_ERR_RUN = 6      /* the run finished with packets in an error state */
+} mcg_status;
+
+typedef struct mcg_ctx mcg_ctx;
+
+/* Create a context on CUDA device `device`. */
+mcg_status mcg_create(mcg_ctx **out, int device);
+/* Release all device memory of the context. */
+void mcg_destroy(mcg_ctx *ctx);
+/* Message of the last failing call (empty string when none). */
+const char *mcg_last_error(const mcg_ctx *ctx);
+/* Library version (major*10000 + minor*100 + patch). */
+int mcg_version(void);
+
+/* ----------------------------------------------------------------------
+ * ComputePart (ComputePart.f:1-552), standard = 'FILE' form.
+ * -------------------------------------------------------------------- */
+typedef struct {
+  int nlam;
+  const double *lam;   /* nlam, micron */
+  int nm;              /* materials in the particle file */
+  const double *e1;    /* nm*nlam: real refractive index n on the grid */
+  const double *e2;    /* nm*nlam: imaginary index k (>= 0) on the grid */
+  const double *frac;  /* nm: abundances as read (inp_abun already applied) */
+  const double *rho;   /* nm: material densities g/cm^3 */
+  double amin, amax;   /* micron */
+  double apow;         /* size distribution n(a) ~ a^-apow */
+  double fmax;         /* DHS maximum vacuum-core volume fraction */
+  double porosity;     /* vacuum volume fraction mixed in when blend != 0 */
+  double normalize_abun; /* <= 0: none (ComputePart.f:139-156) */
+  int blend;           /* Bruggeman-blend materials and vacuum */
+  int ns;              /* sizes per bin (nsubgrains / particle-file ns) */
+  int nf;              /* DHS filling-fraction nodes */
+} mcg_part_in;
+
+typedef struct {
+  double *kabs, *ksca, *kext; /* nlam, cm^2/g */
+  double *F;                  /* nlam*6*180 */
+  double rho_av, mscale, rscale;
+  int64_t n_dhs;              /* coated-sphere evaluations */
+  int64_t n_mie;              /* homogeneous-sphere evaluations */
+  int64_t n_dhs_fail;         /* DHS evaluations that fell back to Mie (Err=1) */
+} mcg_part_out;
+
+/* One grain bin, as one ComputePart call. */
+mcg_status mcg_compute_part(mcg_ctx *ctx, const mcg_part_in *in, mcg_part_out *out);
+/* Several grain bins in one launch sequence (the per-bin loop of
+ * Init.f:3365-3400 folded into one device pass). */
+mcg_status mcg_compute_part_batch(mcg_ctx *ctx, int nparts, const mcg_part_in *in,
+                                  mcg_part_out *out);
+
+/* ----------------------------------------------------------------------
+ * Model: what Init.f builds and MCRadiation reads.
+ * -------------------------------------------------------------------- */
+typedef struct {
+  int nr;                 /* D%nR: radial cells incl. the star cell */
+  int nt;                 /* D%nTheta: theta edges; cells j = 1..nt-1 */
+  const double *R;        /* nr+1 radial edges in AU, R[0] = Rstar/AU */
+  const double *Theta;    /* nt: cos(theta) edges, Theta[0] = 1 ... Theta[nt-1] = 0 */
+  const double *SinTheta; /* nt */
+  const double *dens;     /* ncell: dust density g/cm^3 */
+  const double *V;        /* ncell: cell volume cm^3 */
+  int ncomp;
+  const double *comp_w;   /* ncell*ncomp */
+} mcg_grid;
+
+typedef struct {
+  int nlam;
+  const double *lam;      /* nlam, micron */
+  const double *nu;       /* nlam, Hz */
+  int ncomp;
+  const double *Kabs;     /* ncomp*nlam, cm^2/g */
+  const double *Ksca;     /* ncomp*nlam */
+  const double *F;        /* ncomp*nlam*6*180 normalised Mueller elements */
+  const double *BB;       /* nlam*(TMAX+1) Planck table (Init.f:2616-2622) */
+  const double *Fstar;    /* nlam stellar spectrum */
+  double Lstar;           /* integrate(Fstar) */
+  double Tstar;           /* K, for the star-cell temperature (Main.f:545) */
+  double Rstar_cm;        /* cm */
+  int scat_how;           /* 0 none, 1 isotropic, 2 full Mueller (Init.f:596-611) */
+} mcg_opacity;
+
+/* Planck table BB[l*(TMAX+1)+iT] = B_nu(iT K, lam[l]) with the reference's
+ * quad-precision exponential (Init.f:2616-2622, Subroutines.f:4-21); host
+ * side, needs no context. */
+mcg_status mcg_bb_table(int nlam, const double *lam, double *BB);
+/* one Planck value, B_nu(T, lam) in erg/s/cm^2/Hz/sr, lam in micron */
+double mcg_planck(double T, double lam);
+
+/* Upload grid and opacities and build the device tables (per-cell
+ * KabsTot/KscaTot, Planck means, Mueller normalisations IF11/IF12, g,
+ * random-walk diffusion tables).  Replaces the previous model. */
+mcg_status mcg_set_model(mcg_ctx *ctx, const mcg_grid *grid, const mcg_opacity *opac);
+
+typedef enum { MCG_PREC_FP64 = 0, MCG_PREC_MIXED = 1 } mcg_precision;
+
+typedef struct {
+  uint64_t seed;          /* Philox key: packet p draws stream (seed, p) */
+  int randomwalk;         /* RNDW keyword 'randomwalk' */
+  double factRW;          /* keyword 'factrw' (Init.f:205, default 10) */
+  int64_t maxinteract;    /* > 0: overflow roulette (MCRadiation.f:568-571) */
+  int nruns;              /* keyword 'nruns' (MCRadiation.f:269), >= 1 */
+  int precision;          /* mcg_precision */
+  int threads;            /* 0: persistent grid; n > 0: exactly n threads
+                             (1 reproduces the serial packet order) */
+  int block;              /* threads per block, 0: default */
+} mcg_run;
+
+typedef struct {
+  /* per-cell outputs, ncell each; NULL leaves the result on the device */
+  double *EJv, *EJv2, *Eabs, *T;
+  int32_t *Ni;
+  /* MC spectra, nlam*31; NULL skips the copy */
+  double *spec, *scatspec;
+  int32_t *ispec;
+  /* 0 emissions (nemit), 1 interactions, 2 absorptions, 3 scatterings,
+   * 4 random-walk steps, 5 star hits, 6 abandoned traces, 7 overflow
+   * kills, 8 cell crossings, 9 escapes, 10 averaged-matrix scatterings,
+   * 11 geometry failures */
+  int64_t counters[MCG_NCOUNTERS];
+  double tautot;
+  float device_ms;        /* transport kernel time of the call */
+} mcg_result;
+
+/* The packet loop (MCRadiation.f:6-887).  *nphot_inout = NphotTot. */
+mcg_status mcg_mcradiation(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot_inout,
+                           mcg_result *res);
+
+/* Temperatures from the last run (Main.f:498-549): T, dT, dEJv per cell
+ * (any may be NULL).  Uses EJv/V and EJv2/V^2 of the last mcg_mcradiation. */
+mcg_status mcg_finalize_t(mcg_ctx *ctx, double *T, double *dT, double *dEJv);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MCMAX_GPU_H */

@@ -1,0 +1,120 @@
+"""ctypes view of include/mcmax_gpu.h (the C-ABI of libmcmax_gpu.so).
+
+The shared library is built in-tree by mcmax_b200.build; loading fails loudly
+when it is missing: there is no CPU fallback for any entry point.
+"""
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmcmax_gpu.so")
+
+TMAX = 10000
+TT = TMAX + 1
+NANG = 180
+NANGLE_SED = 30
+NCOUNTERS = 16
+
+MCG_OK, MCG_ERR_ARG, MCG_ERR_CUDA, MCG_ERR_STATE, MCG_ERR_NOMEM, MCG_ERR_LIMIT, MCG_ERR_RUN = range(7)
+STATUS_NAMES = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_STATE", 4: "ERR_NOMEM", 5: "ERR_LIMIT", 6: "ERR_RUN"}
+PREC_FP64, PREC_MIXED = 0, 1
+
+dp = C.POINTER(C.c_double)
+ip = C.POINTER(C.c_int32)
+
+
+class PartIn(C.Structure):
+    _fields_ = [
+        ("nlam", C.c_int), ("lam", dp), ("nm", C.c_int), ("e1", dp), ("e2", dp),
+        ("frac", dp), ("rho", dp), ("amin", C.c_double), ("amax", C.c_double),
+        ("apow", C.c_double), ("fmax", C.c_double), ("porosity", C.c_double),
+        ("normalize_abun", C.c_double), ("blend", C.c_int), ("ns", C.c_int), ("nf", C.c_int),
+    ]
+
+
+class PartOut(C.Structure):
+    _fields_ = [
+        ("kabs", dp), ("ksca", dp), ("kext", dp), ("F", dp),
+        ("rho_av", C.c_double), ("mscale", C.c_double), ("rscale", C.c_double),
+        ("n_dhs", C.c_int64), ("n_mie", C.c_int64), ("n_dhs_fail", C.c_int64),
+    ]
+
+
+class Grid(C.Structure):
+    _fields_ = [
+        ("nr", C.c_int), ("nt", C.c_int), ("R", dp), ("Theta", dp), ("SinTheta", dp),
+        ("dens", dp), ("V", dp), ("ncomp", C.c_int), ("comp_w", dp),
+    ]
+
+
+class Opacity(C.Structure):
+    _fields_ = [
+        ("nlam", C.c_int), ("lam", dp), ("nu", dp), ("ncomp", C.c_int),
+        ("Kabs", dp), ("Ksca", dp), ("F", dp), ("BB", dp), ("Fstar", dp),
+        ("Lstar", C.c_double), ("Tstar", C.c_double), ("Rstar_cm", C.c_double),
+        ("scat_how", C.c_int),
+    ]
+
+
+class Run(C.Structure):
+    _fields_ = [
+        ("seed", C.c_uint64), ("randomwalk", C.c_int), ("factRW", C.c_double),
+        ("maxinteract", C.c_int64), ("nruns", C.c_int), ("precision", C.c_int),
+        ("threads", C.c_int), ("block", C.c_int),
+    ]
+
+
+class Result(C.Structure):
+    _fields_ = [
+        ("EJv", dp), ("EJv2", dp), ("Eabs", dp), ("T", dp), ("Ni", ip),
+        ("spec", dp), ("scatspec", dp), ("ispec", ip),
+        ("counters", C.c_int64 * NCOUNTERS), ("tautot", C.c_double), ("device_ms", C.c_float),
+    ]
+
+
+# name -> (restype, argtypes): every symbol the header declares
+SIGNATURES = {
+    "mcg_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int]),
+    "mcg_destroy": (None, [C.c_void_p]),
+    "mcg_last_error": (C.c_char_p, [C.c_void_p]),
+    "mcg_version": (C.c_int, []),
+    "mcg_compute_part": (C.c_int, [C.c_void_p, C.POINTER(PartIn), C.POINTER(PartOut)]),
+    "mcg_compute_part_batch": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(PartIn), C.POINTER(PartOut)]),
+    "mcg_bb_table": (C.c_int, [C.c_int, dp, dp]),
+    "mcg_planck": (C.c_double, [C.c_double, C.c_double]),
+    "mcg_set_model": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Opacity)]),
+    "mcg_mcradiation": (C.c_int, [C.c_void_p, C.POINTER(Run), C.POINTER(C.c_int64), C.POINTER(Result)]),
+    "mcg_finalize_t": (C.c_int, [C.c_void_p, dp, dp, dp]),
+}
+
+_lib = None
+
+
+def load(path=LIB_PATH):
+    """Load libmcmax_gpu.so (raises when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(
+            "libmcmax_gpu.so is not built (%s); run `python -m mcmax_b200.build` "
+            "or __graft_entry__.build()" % path)
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def ptr(a):
+    """double* / int32* of a contiguous numpy array (None stays NULL)."""
+    if a is None:
+        return None
+    import numpy as np
+    if a.dtype == np.float64:
+        return a.ctypes.data_as(dp)
+    if a.dtype == np.int32:
+        return a.ctypes.data_as(ip)
+    raise TypeError("unsupported dtype %s" % a.dtype)

@@ -1,0 +1,227 @@
+"""Python host mirror of the two MCMax entry points the library replaces.
+
+    ComputePart(p, ii, input, amin, amax, apow, fmax, blend, porosity,
+                inp_abun, iopac, normalize_abun, standard, nsubgrains)
+        ComputePart.f:1 -- fills p.Kabs/Ksca/Kext[iopac], p.F[iopac],
+        p.rho[iopac], p.mscale/rscale[iopac] from a particle file.
+
+    MCRadiation(model, NphotTot, niter, dofastvisc)
+        MCRadiation.f:6 -- runs the photon-packet loop on the model's grid and
+        opacities and stores EJv/EJv2/Eabs/Ni/T and the MC spectra in the
+        model; returns NphotTot (in/out in the reference).
+
+Both go through libmcmax_gpu.so (include/mcmax_gpu.h); errors raise McgError
+with the library's message, the counterpart of the reference's `stop`.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import _ffi
+from ._ffi import TT, NANG
+
+
+class McgError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("%s: %s" % (_ffi.STATUS_NAMES.get(status, status), msg))
+        self.status = status
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Context:
+    """One library context on one CUDA device."""
+
+    def __init__(self, device=0):
+        self.lib = _ffi.load()
+        h = C.c_void_p()
+        st = self.lib.mcg_create(C.byref(h), int(device))
+        if st != 0:
+            raise McgError(st, "mcg_create(device=%d) failed" % device)
+        self.h = h
+        self._keep = []
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mcg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st):
+        if st != 0:
+            raise McgError(st, self.lib.mcg_last_error(self.h).decode())
+
+    # ------------------------------------------------------------ opacities
+    def compute_part_batch(self, parts):
+        """parts: list of dicts with lam, e1, e2 (nm x nlam), frac, rho, amin,
+        amax, apow, fmax, porosity, blend, ns, nf, normalize_abun.  Returns a
+        list of dicts with kabs, ksca, kext, F (nlam,6,180), rho_av, mscale,
+        rscale and the evaluation counters."""
+        n = len(parts)
+        ins = (_ffi.PartIn * n)()
+        outs = (_ffi.PartOut * n)()
+        keep, res = [], []
+        for k, p in enumerate(parts):
+            lam = _f64(p["lam"])
+            e1 = _f64(np.atleast_2d(p["e1"]))
+            e2 = _f64(np.atleast_2d(p["e2"]))
+            frac = _f64(np.atleast_1d(p["frac"]))
+            rho = _f64(np.atleast_1d(p["rho"]))
+            nlam = lam.size
+            o = dict(kabs=np.zeros(nlam), ksca=np.zeros(nlam), kext=np.zeros(nlam),
+                     F=np.zeros((nlam, 6, NANG)))
+            keep += [lam, e1, e2, frac, rho]
+            ins[k] = _ffi.PartIn(nlam, _ffi.ptr(lam), e1.shape[0], _ffi.ptr(e1), _ffi.ptr(e2),
+                                 _ffi.ptr(frac), _ffi.ptr(rho), float(p["amin"]), float(p["amax"]),
+                                 float(p["apow"]), float(p["fmax"]), float(p.get("porosity", 0.0)),
+                                 float(p.get("normalize_abun", -1.0)), int(bool(p.get("blend", False))),
+                                 int(p["ns"]), int(p["nf"]))
+            outs[k].kabs = _ffi.ptr(o["kabs"])
+            outs[k].ksca = _ffi.ptr(o["ksca"])
+            outs[k].kext = _ffi.ptr(o["kext"])
+            outs[k].F = _ffi.ptr(o["F"])
+            res.append(o)
+        self._check(self.lib.mcg_compute_part_batch(self.h, n, ins, outs))
+        for k, o in enumerate(res):
+            o.update(rho_av=outs[k].rho_av, mscale=outs[k].mscale, rscale=outs[k].rscale,
+                     n_dhs=outs[k].n_dhs, n_mie=outs[k].n_mie, n_dhs_fail=outs[k].n_dhs_fail)
+        return res
+
+    # ------------------------------------------------------------ transport
+    def set_model(self, model):
+        """Upload a model (see mcmax_b200.model.Model) and build the device
+        tables."""
+        m = model
+        arrs = dict(R=_f64(m.R), Theta=_f64(m.Theta), SinTheta=_f64(m.SinTheta), dens=_f64(m.dens),
+                    V=_f64(m.V), comp_w=_f64(m.comp_w), lam=_f64(m.lam), nu=_f64(m.nu),
+                    Kabs=_f64(m.Kabs), Ksca=_f64(m.Ksca), F=_f64(m.F) if m.F is not None else None,
+                    BB=_f64(m.BB), Fstar=_f64(m.Fstar))
+        self._model_arrays = arrs
+        g = _ffi.Grid(m.nr, m.nt, _ffi.ptr(arrs["R"]), _ffi.ptr(arrs["Theta"]), _ffi.ptr(arrs["SinTheta"]),
+                      _ffi.ptr(arrs["dens"]), _ffi.ptr(arrs["V"]), m.ncomp, _ffi.ptr(arrs["comp_w"]))
+        o = _ffi.Opacity(m.nlam, _ffi.ptr(arrs["lam"]), _ffi.ptr(arrs["nu"]), m.ncomp, _ffi.ptr(arrs["Kabs"]),
+                         _ffi.ptr(arrs["Ksca"]), _ffi.ptr(arrs["F"]), _ffi.ptr(arrs["BB"]),
+                         _ffi.ptr(arrs["Fstar"]), float(m.Lstar), float(m.Tstar), float(m.Rstar_cm),
+                         int(m.scat_how))
+        self._check(self.lib.mcg_set_model(self.h, C.byref(g), C.byref(o)))
+        self.model = m
+
+    def mcradiation(self, nphot, seed=1, randomwalk=False, factRW=10.0, maxinteract=0, nruns=1,
+                    precision="fp64", threads=0, block=0, fetch=True):
+        """Run the packet loop; returns (nphot_out, result dict)."""
+        m = self.model
+        prec = {"fp64": _ffi.PREC_FP64, "mixed": _ffi.PREC_MIXED}[precision]
+        run = _ffi.Run(int(seed), int(bool(randomwalk)), float(factRW), int(maxinteract), int(nruns), prec,
+                       int(threads), int(block))
+        out = {}
+        res = _ffi.Result()
+        if fetch:
+            nc = m.ncell
+            ns = m.nlam * (_ffi.NANGLE_SED + 1)
+            out = dict(EJv=np.zeros(nc), EJv2=np.zeros(nc), Eabs=np.zeros(nc), T=np.zeros(nc),
+                       Ni=np.zeros(nc, np.int32), spec=np.zeros(ns), scatspec=np.zeros(ns),
+                       ispec=np.zeros(ns, np.int32))
+            for k, v in out.items():
+                setattr(res, k, _ffi.ptr(v))
+        n = C.c_int64(int(nphot))
+        self._check(self.lib.mcg_mcradiation(self.h, C.byref(run), C.byref(n), C.byref(res)))
+        out["counters"] = np.array(res.counters[:], dtype=np.int64)
+        out["tautot"] = res.tautot
+        out["device_ms"] = res.device_ms
+        if fetch:
+            for k in ("spec", "scatspec", "ispec"):
+                out[k] = out[k].reshape(m.nlam, _ffi.NANGLE_SED + 1)
+        return n.value, out
+
+    def finalize_t(self):
+        nc = self.model.ncell
+        T, dT, dE = np.zeros(nc), np.zeros(nc), np.zeros(nc)
+        self._check(self.lib.mcg_finalize_t(self.h, _ffi.ptr(T), _ffi.ptr(dT), _ffi.ptr(dE)))
+        return T, dT, dE
+
+
+def bb_table(lam):
+    """Planck table BB[l, iT] (Init.f:2616-2622) built by the library."""
+    lib = _ffi.load()
+    lam = _f64(lam)
+    BB = np.zeros((lam.size, TT))
+    st = lib.mcg_bb_table(lam.size, _ffi.ptr(lam), _ffi.ptr(BB))
+    if st != 0:
+        raise McgError(st, "mcg_bb_table: invalid wavelengths")
+    return BB
+
+
+def planck(T, lam):
+    return _ffi.load().mcg_planck(float(T), float(lam))
+
+
+# ---------------------------------------------------------------- mirrors
+
+class Particle:
+    """The fields of `type(Particle)` (Modules.f:59-83) that ComputePart
+    writes, one entry per opacity set iopac."""
+
+    def __init__(self, nlam, nopac=1):
+        self.nopac = nopac
+        self.Kabs = np.zeros((nopac, nlam))
+        self.Ksca = np.zeros((nopac, nlam))
+        self.Kext = np.zeros((nopac, nlam))
+        self.F = np.zeros((nopac, nlam, 6, NANG))
+        self.rho = np.zeros(nopac)
+        self.mscale = np.ones(nopac)
+        self.rscale = np.ones(nopac)
+        self.counters = [None] * nopac
+
+
+def ComputePart(ctx, p, ii, input, amin, amax, apow, fmax, blend, porosity, inp_abun, iopac,
+                normalize_abun, standard, nsubgrains, lam):
+    """ComputePart.f:1 for standard='FILE': `input` is a particle file (ns,
+    nf, then per material an .lnk path and 'frac rho').  iopac is 1-based as
+    in the reference.  `lam` is the wavelength grid (module global there)."""
+    from .model import read_particle_file, readrefind
+    if standard != "FILE":
+        raise McgError(_ffi.MCG_ERR_ARG, "standard=%r: only 'FILE' particle files are supported" % standard)
+    ns, nf, mats = read_particle_file(input)
+    e1, e2, frac, rho = [], [], [], []
+    for k, (lnk, fr, rh) in enumerate(mats):
+        if inp_abun is not None and k < len(inp_abun) and inp_abun[k] >= 0.0:
+            fr = inp_abun[k]
+        n_, k_ = readrefind(lnk, lam)
+        e1.append(n_)
+        e2.append(k_)
+        frac.append(fr)
+        rho.append(rh)
+    res = ctx.compute_part_batch([dict(lam=lam, e1=np.array(e1), e2=np.array(e2), frac=frac, rho=rho,
+                                       amin=amin, amax=amax, apow=apow, fmax=fmax, porosity=porosity,
+                                       blend=blend, ns=ns, nf=nf, normalize_abun=normalize_abun)])[0]
+    io = iopac - 1
+    p.Kabs[io] = res["kabs"]
+    p.Ksca[io] = res["ksca"]
+    p.Kext[io] = res["kext"]
+    p.F[io] = res["F"]
+    p.rho[io] = res["rho_av"]
+    p.mscale[io] = res["mscale"]
+    p.rscale[io] = res["rscale"]
+    p.counters[io] = (res["n_dhs"], res["n_mie"], res["n_dhs_fail"])
+    return p
+
+
+def MCRadiation(ctx, model, NphotTot, niter=1, dofastvisc=False, **run):
+    """MCRadiation.f:6: the packet loop on `model` (uploaded on first use).
+    Results are stored on the model (EJv, EJv2, Eabs, Ni, T, spec, ...).
+    Viscous heating is not part of the built path (dofastvisc is accepted
+    for signature parity and ignored)."""
+    if getattr(ctx, "model", None) is not model:
+        ctx.set_model(model)
+    n, out = ctx.mcradiation(NphotTot, **run)
+    for k, v in out.items():
+        setattr(model, k, v)
+    return n

@@ -1,0 +1,114 @@
+/*
+ * mcg_internal.h -- shared host-side definitions of libmcmax_gpu.
+ */
+#ifndef MCG_INTERNAL_H
+#define MCG_INTERNAL_H
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/mcmax_gpu.h"
+
+#define MCG_TT (MCG_TMAX + 1)
+
+/* device buffer owned by a context */
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+};
+
+/* Tables of the current model on the device (built by mcg_set_model). */
+struct DevModel {
+  bool valid = false;
+  int nr = 0, nt = 0, nc = 0, ncell = 0, nlam = 0, ncomp = 0, scat_how = 0;
+  int scattering = 0;       /* scat_how != 0 and some Ksca > 0 */
+  int uniform_mix = 0;      /* all cells have the same comp_w row */
+  double Lstar = 0.0, Tstar = 0.0, Rstar_cm = 0.0;
+  /* geometry */
+  double *R = nullptr, *Theta = nullptr, *SinTheta = nullptr;
+  double *dens = nullptr;   /* floored at 1e-50 */
+  double *mass = nullptr;   /* dens*V before the floor */
+  double *V = nullptr;
+  double *comp_w = nullptr; /* ncell*ncomp */
+  /* spectra */
+  double *nu = nullptr, *dnu_half = nullptr; /* |nu_i - nu_i+1| * 0.5 */
+  double *BB = nullptr;     /* nlam*TT */
+  double *star_cdf = nullptr; /* nlam-1 cumulative trapezoid of Fstar */
+  double *wlam = nullptr;   /* nlam SED weights */
+  /* per component */
+  double *Kabs_c = nullptr, *Ksca_c = nullptr, *g_c = nullptr; /* ncomp*nlam */
+  double *F_c = nullptr;    /* ncomp*nlam*1080 */
+  double *IF_c = nullptr;   /* ncomp*nlam*2 */
+  double *Kp_c = nullptr;   /* ncomp*TT */
+  /* per cell */
+  double *KabsTot = nullptr, *KscaTot = nullptr; /* ncell*nlam */
+  float *KabsTotF = nullptr, *KextTotF = nullptr; /* ncell*nlam, mixed path */
+  double *KpCell = nullptr; /* ncell*TT (uniform mix: 1*TT) */
+  /* re-emission CDF for iT0 == iT1 in a uniform mixture: TT*(nlam-1) */
+  double *emit_cdf = nullptr;
+  /* random walk */
+  double *KDext = nullptr, *KDabs = nullptr; /* nthick_alloc*TT */
+  int *kd_index = nullptr;  /* ncell -> row of KDext/KDabs or -1 */
+  unsigned char *thick = nullptr;
+  double *rw_y = nullptr, *rw_phi = nullptr; /* 1000 each */
+  int kd_rows = 0;
+  double kd_factRW = -1.0;  /* factRW the thick flags were built for */
+  /* constant tables */
+  double *sinthet = nullptr; /* 180 */
+  double *cos2phi = nullptr, *sin2phi = nullptr; /* 361 */
+  float *sinthetF = nullptr, *cos2phiF = nullptr, *sin2phiF = nullptr;
+  std::vector<void *> owned;
+};
+
+/* Accumulators of a run on the device. */
+struct DevRun {
+  int ncell = 0, nlam = 0;
+  double *EJv = nullptr, *EJv2 = nullptr, *Eabs = nullptr, *T = nullptr;
+  int *Ni = nullptr, *lastphot = nullptr;
+  double *spec = nullptr, *scatspec = nullptr;
+  int *ispec = nullptr;
+  unsigned long long *counters = nullptr; /* MCG_NCOUNTERS */
+  double *tautot = nullptr;
+  unsigned long long *next_packet = nullptr;
+  /* nruns accumulation */
+  double *EJvTot = nullptr, *EJv2Tot = nullptr;
+  std::vector<void *> owned;
+};
+
+struct mcg_ctx {
+  int device = 0;
+  int sm_count = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::string err;
+  DevModel model;
+  DevRun run;
+  bool have_run = false;
+  /* reusable scratch for ComputePart */
+  DevBuf part_scratch;
+};
+
+/* error helpers */
+mcg_status mcg_fail(mcg_ctx *ctx, mcg_status st, const char *fmt, ...);
+#define MCG_CUDA(ctx, call)                                                                     \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess)                                                                      \
+      return mcg_fail((ctx), MCG_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                      __FILE__, __LINE__);                                                      \
+  } while (0)
+
+/* entry points implemented in the kernel translation units */
+mcg_status mcg_part_batch_impl(mcg_ctx *ctx, int nparts, const mcg_part_in *in, mcg_part_out *out);
+mcg_status mcg_set_model_impl(mcg_ctx *ctx, const mcg_grid *grid, const mcg_opacity *opac);
+mcg_status mcg_mcradiation_impl(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot, mcg_result *res);
+mcg_status mcg_finalize_impl(mcg_ctx *ctx, double *T, double *dT, double *dEJv);
+void mcg_free_model(DevModel &m);
+void mcg_free_run(DevRun &r);
+
+#endif /* MCG_INTERNAL_H */

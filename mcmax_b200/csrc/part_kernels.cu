@@ -1,0 +1,694 @@
+/*
+ * part_kernels.cu -- the DHS/Mie opacity stage (ComputePart.f:1-552) on
+ * sm_100a.
+ *
+ * Decomposition of one batch of grain bins ("parts"):
+ *   host   : the per-part set-up of ComputePart.f:1-297 (abundance
+ *            normalisation, Bruggeman blend with vacuum, Gauss-Legendre
+ *            filling fractions, size grid and number weights), producing one
+ *            sample per (part, wavelength, material, size, filling fraction).
+ *   K1a    : dhs_kernel   -- one warp per coated-sphere sample (dhs_core.cuh);
+ *            writes the 4 x 180 Mueller elements and the cross sections of
+ *            the sample, or flags Err = 1.
+ *   K1b    : mie_kernel   -- one warp per (part, wavelength, material, size)
+ *            that needs the homogeneous-sphere fallback (f = 0, x > 1e4, or a
+ *            DHS failure, ComputePart.f:332-383).
+ *   K1c    : accum_kernel -- one warp per (part, wavelength): replays the
+ *            (material, size, f) loop of the reference in its order
+ *            (sticky Err, Mie reuse, forward-peak renormalisation
+ *            ComputePart.f:407-415, weighted sums :417-429) and writes
+ *            Kabs/Ksca/Kext and the six normalised Mueller elements.
+ * All FP64, compiled with --fmad=false: the result is bit-identical to the
+ * CPU checker.  Scratch (down-recurrence arrays) lives in one device buffer
+ * sliced per resident warp.
+ */
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "dhs_core.cuh"
+#include "mcg_internal.h"
+
+namespace {
+
+constexpr int NA = 180;
+constexpr int WARP = 32;
+constexpr int APL_DHS = 3;  /* ceil(90/32) angles per lane */
+constexpr int APL_MIE = 3;
+
+/* status of a sample */
+enum : int8_t { S_DHS = 0, S_DHS_ERR = 1, S_MIE = 2 };
+
+struct SampleDev {
+  const double *rcore, *rshell, *wvno, *mre, *mim;
+  int8_t *status;
+  double *F;      /* nsamp*4*180 */
+  double *cs;     /* nsamp*2 (cemie, csmie) */
+  int *mie_need;  /* per (part, lam, l, k) */
+  int nsamp;
+};
+
+__global__ void __launch_bounds__(128) dhs_kernel(SampleDev s, const double *mu, cx *scratch,
+                                                  int cap, unsigned long long *next) {
+  const int lane = threadIdx.x & 31;
+  const int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  cx *my = scratch + (size_t)warp_global * 4 * cap;
+  for (;;) {
+    unsigned long long idx = 0;
+    if (lane == 0) idx = atomicAdd(next, 1ULL);
+    idx = __shfl_sync(0xffffffffu, idx, 0);
+    if (idx >= (unsigned long long)s.nsamp) break;
+    const int i = (int)idx;
+    if (s.status[i] != S_DHS) continue;
+    double *F = s.F + (size_t)i * 4 * NA;
+    double ce = 0.0, cs = 0.0;
+    int e = dhs_sample<WARP, APL_DHS>(s.rcore[i], s.rshell[i], s.wvno[i], s.mre[i], -s.mim[i], mu,
+                                      my, cap, lane, F, F + NA, F + 2 * NA, F + 3 * NA, &ce, &cs);
+    if (lane == 0) {
+      if (e) {
+        s.status[i] = S_DHS_ERR;
+      } else {
+        s.cs[2 * i] = ce;
+        s.cs[2 * i + 1] = cs;
+      }
+    }
+    __syncwarp();
+  }
+}
+
+struct MieDev {
+  const double *rad, *lam, *e1, *e2; /* per mie slot */
+  const int *need;
+  double *F;   /* nslot*4*180 */
+  double *cs;  /* nslot*2 (cemie, csmie) */
+  int8_t *ok;
+  int nslot;
+};
+
+__global__ void __launch_bounds__(128) mie_kernel(MieDev m, double *scratch, int cap,
+                                                  unsigned long long *next) {
+  const int lane = threadIdx.x & 31;
+  const int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  double *my = scratch + (size_t)warp_global * 8 * cap;
+  for (;;) {
+    unsigned long long idx = 0;
+    if (lane == 0) idx = atomicAdd(next, 1ULL);
+    idx = __shfl_sync(0xffffffffu, idx, 0);
+    if (idx >= (unsigned long long)m.nslot) break;
+    const int i = (int)idx;
+    if (!m.need[i]) continue;
+    double *F = m.F + (size_t)i * 4 * NA;
+    double cs = 0.0, ce = 0.0;
+    int e = mie_sample<WARP, APL_MIE>(m.rad[i], m.lam[i], m.e1[i], m.e2[i], my, cap, lane, F,
+                                      F + NA, F + 2 * NA, F + 3 * NA, &cs, &ce);
+    if (lane == 0) {
+      m.ok[i] = e ? 0 : 1;
+      m.cs[2 * i] = ce;
+      m.cs[2 * i + 1] = cs;
+    }
+    __syncwarp();
+  }
+}
+
+/* per-part description for the accumulation kernel */
+struct PartDev {
+  int nlam, nmc, ns, nf;
+  int samp0;   /* first sample index of the part */
+  int mie0;    /* first Mie slot of the part */
+  int out0;    /* first output wavelength row of the part */
+  double mscale;
+  const double *frac;  /* nmc */
+  const double *rho;   /* nmc */
+  const double *r1;    /* ns */
+  const double *nr;    /* nmc*ns */
+  const double *wf;    /* nf */
+};
+
+struct AccDev {
+  const PartDev *parts;
+  int nparts;
+  const int *row_part;  /* for each output row: part index */
+  const int8_t *status;
+  const double *sF, *scs;
+  const double *mF, *mcs;
+  const double *sinw;   /* 180 */
+  double tot2;          /* sum of sinw in order */
+  double *kabs, *ksca, *kext, *Fout; /* rows x ..., Fout rows*6*180 */
+  double *rho_av;       /* per part */
+  int nrows;
+};
+
+/* ComputePart.f:318-447 for one (part, wavelength), in the reference's loop
+ * order.  Lane L owns bins L, L+32, ... of the 180. */
+__global__ void __launch_bounds__(128) accum_kernel(AccDev a) {
+  const int lane = threadIdx.x & 31;
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (row >= a.nrows) return;
+  const int p = a.row_part[row];
+  const PartDev P = a.parts[p];
+  const int ilam = row - P.out0;
+  constexpr int BPL = (NA + WARP - 1) / WARP; /* 6 */
+  double acc[6][BPL];
+#pragma unroll
+  for (int e = 0; e < 6; ++e)
+#pragma unroll
+    for (int b = 0; b < BPL; ++b) acc[e][b] = 0.0;
+  double csca = 0.0, cabs = 0.0, cext = 0.0, mass = 0.0, vol = 0.0;
+  /* Mie working state that survives across f (the reference's Mief arrays) */
+  double f11_0 = 0.0;     /* current Mief11(1) */
+  for (int l = 0; l < P.nmc; ++l) {
+    if (P.frac[l] == 0.0) continue;
+    for (int k = 0; k < P.ns; ++k) {
+      const double r1 = P.r1[k];
+      const int mslot = P.mie0 + (ilam * P.nmc + l) * P.ns + k;
+      int err = 0;
+      for (int i = 0; i < P.nf; ++i) {
+        const int s = P.samp0 + ((ilam * P.nmc + l) * P.ns + k) * P.nf + i;
+        const int8_t st = a.status[s];
+        if (st == S_DHS_ERR) err = 1;
+        const double *src;
+        double ce, cs, f22_0;
+        if (err || st == S_MIE) {
+          src = a.mF + (size_t)mslot * 4 * NA;
+          ce = a.mcs[2 * mslot];
+          cs = a.mcs[2 * mslot + 1];
+          if (err || i == 0) {
+            f11_0 = src[0];
+          }
+          f22_0 = f11_0;  /* Mief22 = Mief11 (current contents) */
+        } else {
+          src = a.sF + (size_t)s * 4 * NA;
+          ce = a.scs[2 * s];
+          cs = a.scs[2 * s + 1];
+          f11_0 = src[0];
+          f22_0 = f11_0;
+        }
+        /* forward-peak renormalisation, sequential over the 180 bins */
+        double t1 = f11_0 * a.sinw[0];
+        for (int j = 1; j < NA; ++j) t1 = t1 + src[j] * a.sinw[j];
+        f11_0 = f11_0 + (a.tot2 - t1) / a.sinw[0];
+        if (f11_0 < 0.0) f11_0 = 0.0;
+        const double wn = P.wf[i] * P.nr[l * P.ns + k];
+#pragma unroll
+        for (int b = 0; b < BPL; ++b) {
+          const int j = lane + b * WARP;
+          if (j < NA) {
+            const double v11 = j == 0 ? f11_0 : src[j];
+            const double v22 = j == 0 ? f22_0 : src[j];
+            const double v12 = src[NA + j];
+            const double v33 = src[2 * NA + j];
+            const double v34 = src[3 * NA + j];
+            acc[0][b] += (wn * v11) * cs;
+            acc[1][b] += (wn * v12) * cs;
+            acc[2][b] += (wn * v22) * cs;
+            acc[3][b] += (wn * v33) * cs;
+            acc[4][b] += (wn * v34) * cs;
+            acc[5][b] += (wn * v33) * cs;
+          }
+        }
+        cext = cext + wn * ce;
+        csca = csca + wn * cs;
+        cabs = cabs + wn * (ce - cs);
+        const double r13 = (r1 * r1) * r1;
+        mass = mass + (((wn * P.rho[l]) * 4.0) * DHS_PI) * r13 / 3.0;
+        vol = vol + ((wn * 4.0) * DHS_PI) * r13 / 3.0;
+      }
+    }
+  }
+  if (lane == 0) {
+    a.kabs[row] = 1.0e4 * cabs / (mass / P.mscale);
+    a.ksca[row] = 1.0e4 * csca / (mass / P.mscale);
+    a.kext[row] = 1.0e4 * cext / (mass / P.mscale);
+    if (ilam == P.nlam - 1) a.rho_av[p] = mass / vol;
+  }
+#pragma unroll
+  for (int e = 0; e < 6; ++e)
+#pragma unroll
+    for (int b = 0; b < BPL; ++b) {
+      const int j = lane + b * WARP;
+      if (j < NA) a.Fout[((size_t)row * 6 + e) * NA + j] = acc[e][b] / csca;
+    }
+}
+
+/* ---------------- host side ---------------- */
+
+/* Bruggeman mixing, ComputePart.f:1177-1212 (same operation order as the
+ * checker) */
+void blender(const double *e1, const double *e2, const double *abun, int nm, double *e1out,
+             double *e2out) {
+  cx mm = cx_make(1.0, 0.0), me = mm;
+  for (int iter = 0; iter < 100; ++iter) {
+    cx sum = cx_make(0.0, 0.0);
+    cx mm2 = cx_mul(mm, mm);
+    for (int j = 0; j < nm; ++j) {
+      cx mj = cx_make(e1[j], e2[j]);
+      cx mj2 = cx_mul(mj, mj);
+      cx q = cx_div(cx_sub(mj2, mm2), cx_add(mj2, cx_scale(2.0, mm2)));
+      sum = cx_add(sum, cx_scale(abun[j], q));
+    }
+    cx num = cx_make(2.0 * sum.re + 1.0, 2.0 * sum.im);
+    cx den = cx_make(1.0 - sum.re, -sum.im);
+    me = cx_div(num, den);
+    me = cx_mul(mm, cx_sqrt(me));
+    mm = me;
+  }
+  *e1out = me.re;
+  *e2out = me.im;
+}
+
+/* Gauss-Legendre nodes on [x1,x2], ComputePart.f:1219-1249 */
+void gauleg2(double x1, double x2, double *x, double *w, int n) {
+  int m = (n + 1) / 2;
+  double xm = 0.5 * (x2 + x1);
+  double xl = 0.5 * (x2 - x1);
+  for (int i = 1; i <= m; ++i) {
+    double z = cos(3.141592654 * ((double)i - 0.25) / ((double)n + 0.5));
+    double z1, pp = 1.0;
+    for (int it = 0; it < 100; ++it) {
+      double p1 = 1.0, p2 = 0.0, p3;
+      for (int j = 1; j <= n; ++j) {
+        p3 = p2;
+        p2 = p1;
+        p1 = ((2.0 * j - 1.0) * z * p2 - (j - 1.0) * p3) / j;
+      }
+      pp = n * (z * p1 - p2) / (z * z - 1.0);
+      z1 = z;
+      z = z1 - p1 / pp;
+      if (!(std::fabs(z - z1) > 3.0e-14)) break;
+    }
+    x[i - 1] = xm - xl * z;
+    x[n - i] = xm + xl * z;
+    w[i - 1] = 2.0 * xl / ((1.0 - z * z) * pp * pp);
+    w[n - i] = w[i - 1];
+  }
+}
+
+/* per-part host set-up (ComputePart.f:1-297) */
+struct PartHost {
+  int nlam = 0, nmc = 0, ns = 0, nf = 0;
+  double mscale = 1.0, rscale = 1.0;
+  std::vector<double> e1, e2;  /* nmc*nlam */
+  std::vector<double> frac, rho, f, wf, r, r1, nr;
+  std::vector<double> rad, rcore; /* ns*nf */
+};
+
+bool part_setup(const mcg_part_in &in, PartHost &h, std::string &why) {
+  if (in.nlam < 2 || !in.lam || in.nm < 1 || !in.e1 || !in.e2 || !in.frac || !in.rho) {
+    why = "part: nlam >= 2, nm >= 1 and non-null lam/e1/e2/frac/rho are required";
+    return false;
+  }
+  if (!(in.amin > 0.0) || !(in.amax > 0.0) || in.ns < 1 || in.nf < 1) {
+    why = "part: amin, amax > 0 and ns, nf >= 1 are required";
+    return false;
+  }
+  if (in.nm + 1 > 64) {
+    why = "part: at most 63 materials";
+    return false;
+  }
+  for (int l = 0; l < in.nm; ++l)
+    if (!(in.rho[l] > 0.0)) {
+      why = "part: material densities must be > 0";
+      return false;
+    }
+  const int nlam = in.nlam, nm = in.nm;
+  h.nlam = nlam;
+  int nmat = nm + (in.blend ? 1 : 0);
+  h.e1.assign(in.e1, in.e1 + (size_t)nm * nlam);
+  h.e2.assign(in.e2, in.e2 + (size_t)nm * nlam);
+  h.e1.resize((size_t)nmat * nlam);
+  h.e2.resize((size_t)nmat * nlam);
+  h.frac.resize(nmat);
+  h.rho.resize(nmat);
+  for (int l = 0; l < nm; ++l) {
+    h.rho[l] = in.rho[l];
+    h.frac[l] = in.frac[l] / in.rho[l];
+  }
+  double minlog = log10(in.amin), maxlog = log10(in.amax);
+  double pw = -in.apow;
+  double maxf = in.fmax;
+  int nf = in.nf;
+  if (maxf == 0.0) nf = 1;
+  double tot = 0.0;
+  for (int i = 0; i < nm; ++i) tot += h.frac[i];
+  if (in.normalize_abun <= 0.0) {
+    for (int i = 0; i < nm; ++i) h.frac[i] /= tot;
+    h.mscale = 1.0;
+    h.rscale = 1.0;
+  } else {
+    h.mscale = 0.0;
+    for (int i = 0; i < nm; ++i) h.mscale += h.frac[i] * h.rho[i] / in.normalize_abun;
+    h.rscale = pow(h.mscale, 1.0 / 3.0);
+    for (int i = 0; i < nm; ++i) h.frac[i] /= tot;
+  }
+  int nmc = nm;
+  if (in.blend) {
+    nmc = nm + 1;
+    for (int i = 0; i < nlam; ++i) {
+      h.e1[(size_t)nm * nlam + i] = 1.0;
+      h.e2[(size_t)nm * nlam + i] = 0.0;
+    }
+    h.rho[nm] = 0.0;
+    h.frac[nm] = in.porosity;
+    for (int l = 0; l < nm; ++l) h.frac[l] *= (1.0 - in.porosity);
+    double ee1[64], ee2[64];
+    for (int i = 0; i < nlam; ++i) {
+      for (int l = 0; l < nmc; ++l) {
+        ee1[l] = h.e1[(size_t)l * nlam + i];
+        ee2[l] = h.e2[(size_t)l * nlam + i];
+      }
+      double b1, b2;
+      blender(ee1, ee2, h.frac.data(), nmc, &b1, &b2);
+      h.e1[i] = b1;
+      h.e2[i] = b2;
+    }
+    double rav = 0.0;
+    for (int l = 0; l < nmc; ++l) rav += h.frac[l] * h.rho[l];
+    h.rho[0] = rav;
+    h.frac[0] = 1.0;
+    nmc = 1;
+  }
+  h.nmc = nmc;
+  h.f.assign(nf, 0.0);
+  h.wf.assign(nf, 0.0);
+  if (nf > 1 && maxf > 0.01) {
+    gauleg2(0.01, maxf, h.f.data(), h.wf.data(), nf);
+  } else if (maxf == 0.0) {
+    for (int i = 0; i < nf; ++i) {
+      h.f[i] = 0.0;
+      h.wf[i] = 1.0 / (double)nf;
+    }
+  } else {
+    nf = 1;
+    h.f.assign(1, maxf);
+    h.wf.assign(1, 1.0);
+  }
+  h.nf = nf;
+  const int ns = in.ns;
+  h.ns = ns;
+  h.r.assign(ns, 0.0);
+  h.nr.assign((size_t)nmc * ns, 0.0);
+  for (int l = 0; l < nmc; ++l) {
+    if (ns == 1) {
+      h.r[0] = pow(10.0, (minlog + maxlog) / 2.0);
+      h.nr[(size_t)l * ns] = h.frac[l];
+    } else {
+      double t2 = 0.0;
+      for (int k = 0; k < ns; ++k) {
+        h.r[k] = pow(10.0, minlog + (maxlog - minlog) * (double)k / (double)(ns - 1));
+        h.nr[(size_t)l * ns + k] = pow(h.r[k], pw + 1.0);
+        t2 += h.nr[(size_t)l * ns + k] * (h.r[k] * h.r[k] * h.r[k]);
+      }
+      for (int k = 0; k < ns; ++k) h.nr[(size_t)l * ns + k] = h.frac[l] * h.nr[(size_t)l * ns + k] / t2;
+    }
+  }
+  h.r1.resize(ns);
+  h.rad.resize((size_t)ns * nf);
+  h.rcore.resize((size_t)ns * nf);
+  for (int k = 0; k < ns; ++k) {
+    h.r1[k] = h.r[k] * h.rscale;
+    for (int i = 0; i < nf; ++i) {
+      h.rad[(size_t)k * nf + i] = h.r1[k] / pow(1.0 - h.f[i], 1.0 / 3.0);
+      h.rcore[(size_t)k * nf + i] = h.f[i] > 0.0 ? h.rad[(size_t)k * nf + i] * pow(h.f[i], 1.0 / 3.0) : 0.0;
+    }
+  }
+  return true;
+}
+
+template <typename T>
+T *dev_alloc(std::vector<void *> &own, size_t n, cudaError_t &err) {
+  void *p = nullptr;
+  if (n == 0) n = 1;
+  err = cudaMalloc(&p, n * sizeof(T));
+  if (err == cudaSuccess) own.push_back(p);
+  return (T *)p;
+}
+
+}  // namespace
+
+mcg_status mcg_part_batch_impl(mcg_ctx *ctx, int nparts, const mcg_part_in *in, mcg_part_out *out) {
+  if (nparts < 1 || !in || !out) return mcg_fail(ctx, MCG_ERR_ARG, "compute_part: nparts >= 1 and non-null in/out required");
+  std::vector<PartHost> H(nparts);
+  for (int p = 0; p < nparts; ++p) {
+    std::string why;
+    if (!part_setup(in[p], H[p], why)) return mcg_fail(ctx, MCG_ERR_ARG, "%s (part %d)", why.c_str(), p);
+    if (!out[p].kabs || !out[p].ksca || !out[p].kext || !out[p].F)
+      return mcg_fail(ctx, MCG_ERR_ARG, "compute_part: null output array (part %d)", p);
+  }
+  /* constant tables, ComputePart.f:294-297 and :407-415 */
+  double mu[90], sinw[NA], tot2 = 0.0;
+  for (int i = 1; i <= 90; ++i) mu[i - 1] = cos(((double)i - 0.5) / (double)(NA / 2) * DHS_PI / 2.0);
+  for (int j = 1; j <= NA; ++j) sinw[j - 1] = sin(DHS_PI * ((double)j - 0.5) / (double)NA);
+  for (int j = 0; j < NA; ++j) tot2 = tot2 + sinw[j];
+
+  /* enumerate samples and Mie slots */
+  std::vector<double> srcore, srshell, swvno, smre, smim;
+  std::vector<int8_t> sstat;
+  std::vector<double> mrad, mlam, me1, me2;
+  std::vector<int> mneed;
+  std::vector<PartDev> pd(nparts);
+  std::vector<int> row_part;
+  int maxnmx1 = 150, maxmie = 0;
+  for (int p = 0; p < nparts; ++p) {
+    PartHost &h = H[p];
+    PartDev &d = pd[p];
+    d.nlam = h.nlam;
+    d.nmc = h.nmc;
+    d.ns = h.ns;
+    d.nf = h.nf;
+    d.samp0 = (int)sstat.size();
+    d.mie0 = (int)mneed.size();
+    d.out0 = (int)row_part.size();
+    d.mscale = h.mscale;
+    for (int ilam = 0; ilam < h.nlam; ++ilam) {
+      row_part.push_back(p);
+      double wvno = 2.0 * DHS_PI / in[p].lam[ilam];
+      for (int l = 0; l < h.nmc; ++l) {
+        double e1 = h.e1[(size_t)l * h.nlam + ilam], e2 = h.e2[(size_t)l * h.nlam + ilam];
+        for (int k = 0; k < h.ns; ++k) {
+          double r1 = h.r1[k];
+          int need = 0;
+          for (int i = 0; i < h.nf; ++i) {
+            double rad = h.rad[(size_t)k * h.nf + i];
+            int8_t st = S_DHS;
+            if (h.f[i] == 0.0 || r1 * wvno > 10000.0) st = S_MIE;
+            if (h.frac[l] == 0.0) {
+              st = S_MIE; /* skipped by the accumulation, never evaluated */
+            } else if (st == S_MIE) {
+              need = 1;
+            }
+            srcore.push_back(h.rcore[(size_t)k * h.nf + i]);
+            srshell.push_back(rad);
+            swvno.push_back(wvno);
+            smre.push_back(e1);
+            smim.push_back(e2);
+            sstat.push_back(st);
+            if (st == S_DHS) maxnmx1 = std::max(maxnmx1, dhs_nmx1(rad, wvno, e1, -e2));
+          }
+          double lm = in[p].lam[ilam];
+          if (r1 / lm >= 5000.0) lm = r1 / 5000.0;
+          mrad.push_back(r1);
+          mlam.push_back(lm);
+          me1.push_back(e1);
+          me2.push_back(e2);
+          mneed.push_back(need);
+        }
+      }
+    }
+  }
+  const int nsamp = (int)sstat.size();
+  const int nslot = (int)mneed.size();
+  const int nrows = (int)row_part.size();
+  if (maxnmx1 + 1 > DHS_LL) maxnmx1 = DHS_LL; /* larger samples return Err inside */
+  /* Mie term counts of every slot (any slot can be needed after a DHS
+   * failure) */
+  for (int q = 0; q < nslot; ++q) {
+    int nmax, nfi, nD;
+    mie_counts(mrad[q], mlam[q], me1[q], me2[q], &nmax, &nfi, &nD);
+    maxmie = std::max(maxmie, std::max(nfi, nD));
+  }
+  const int dcap = maxnmx1 + 2;
+  const int mcap = maxmie + 2;
+  if ((long long)mcap > 50000000LL)
+    return mcg_fail(ctx, MCG_ERR_LIMIT, "compute_part: Mie term count %d beyond the 5e7 limit", maxmie);
+
+  std::vector<void *> own;
+  cudaError_t ce = cudaSuccess;
+  auto fail_free = [&](const char *what) {
+    for (void *q : own) cudaFree(q);
+    return mcg_fail(ctx, MCG_ERR_NOMEM, "compute_part: cudaMalloc of %s failed: %s", what, cudaGetErrorString(ce));
+  };
+#define ALLOC(T, n, name)                          \
+  dev_alloc<T>(own, (size_t)(n), ce);              \
+  if (ce != cudaSuccess) return fail_free(name)
+  double *d_rcore = ALLOC(double, nsamp, "rcore");
+  double *d_rshell = ALLOC(double, nsamp, "rshell");
+  double *d_wvno = ALLOC(double, nsamp, "wvno");
+  double *d_mre = ALLOC(double, nsamp, "mre");
+  double *d_mim = ALLOC(double, nsamp, "mim");
+  int8_t *d_stat = ALLOC(int8_t, nsamp, "status");
+  double *d_sF = ALLOC(double, (size_t)nsamp * 4 * NA, "sample F");
+  double *d_scs = ALLOC(double, (size_t)nsamp * 2, "sample cs");
+  double *d_mrad = ALLOC(double, nslot, "mie rad");
+  double *d_mlam = ALLOC(double, nslot, "mie lam");
+  double *d_me1 = ALLOC(double, nslot, "mie e1");
+  double *d_me2 = ALLOC(double, nslot, "mie e2");
+  int *d_mneed = ALLOC(int, nslot, "mie need");
+  double *d_mF = ALLOC(double, (size_t)nslot * 4 * NA, "mie F");
+  double *d_mcs = ALLOC(double, (size_t)nslot * 2, "mie cs");
+  int8_t *d_mok = ALLOC(int8_t, nslot, "mie ok");
+  double *d_mu = ALLOC(double, 90, "mu");
+  double *d_sinw = ALLOC(double, NA, "sinw");
+  unsigned long long *d_next = ALLOC(unsigned long long, 2, "counters");
+  PartDev *d_parts = ALLOC(PartDev, nparts, "parts");
+  int *d_rowpart = ALLOC(int, nrows, "row map");
+  double *d_kabs = ALLOC(double, nrows, "kabs");
+  double *d_ksca = ALLOC(double, nrows, "ksca");
+  double *d_kext = ALLOC(double, nrows, "kext");
+  double *d_Fout = ALLOC(double, (size_t)nrows * 6 * NA, "F out");
+  double *d_rhoav = ALLOC(double, nparts, "rho_av");
+  /* per-part small arrays */
+  std::vector<double> pflat;
+  std::vector<size_t> off_frac(nparts), off_rho(nparts), off_r1(nparts), off_nr(nparts), off_wf(nparts);
+  for (int p = 0; p < nparts; ++p) {
+    off_frac[p] = pflat.size(); pflat.insert(pflat.end(), H[p].frac.begin(), H[p].frac.begin() + H[p].nmc);
+    off_rho[p] = pflat.size(); pflat.insert(pflat.end(), H[p].rho.begin(), H[p].rho.begin() + H[p].nmc);
+    off_r1[p] = pflat.size(); pflat.insert(pflat.end(), H[p].r1.begin(), H[p].r1.end());
+    off_nr[p] = pflat.size(); pflat.insert(pflat.end(), H[p].nr.begin(), H[p].nr.end());
+    off_wf[p] = pflat.size(); pflat.insert(pflat.end(), H[p].wf.begin(), H[p].wf.begin() + H[p].nf);
+  }
+  double *d_pflat = ALLOC(double, pflat.size(), "part tables");
+#undef ALLOC
+  for (int p = 0; p < nparts; ++p) {
+    pd[p].frac = d_pflat + off_frac[p];
+    pd[p].rho = d_pflat + off_rho[p];
+    pd[p].r1 = d_pflat + off_r1[p];
+    pd[p].nr = d_pflat + off_nr[p];
+    pd[p].wf = d_pflat + off_wf[p];
+  }
+  cudaStream_t st = ctx->stream;
+#define H2D(dst, src, n) cudaMemcpyAsync(dst, src, (size_t)(n) * sizeof(*(src)), cudaMemcpyHostToDevice, st)
+  H2D(d_rcore, srcore.data(), nsamp);
+  H2D(d_rshell, srshell.data(), nsamp);
+  H2D(d_wvno, swvno.data(), nsamp);
+  H2D(d_mre, smre.data(), nsamp);
+  H2D(d_mim, smim.data(), nsamp);
+  H2D(d_stat, sstat.data(), nsamp);
+  H2D(d_mrad, mrad.data(), nslot);
+  H2D(d_mlam, mlam.data(), nslot);
+  H2D(d_me1, me1.data(), nslot);
+  H2D(d_me2, me2.data(), nslot);
+  H2D(d_mneed, mneed.data(), nslot);
+  H2D(d_mu, mu, 90);
+  H2D(d_sinw, sinw, NA);
+  H2D(d_parts, pd.data(), nparts);
+  H2D(d_rowpart, row_part.data(), nrows);
+  H2D(d_pflat, pflat.data(), pflat.size());
+#undef H2D
+  cudaMemsetAsync(d_next, 0, 2 * sizeof(unsigned long long), st);
+  cudaMemsetAsync(d_mok, 0, nslot, st);
+
+  /* launch shapes: 4 warps per block, a multiple of the SM count; the number
+   * of warps is bounded by the scratch budget */
+  const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;
+  const size_t budget = (size_t)1 << 31; /* 2 GiB of down-recurrence scratch */
+  auto warps_for = [&](size_t per_warp, int work) {
+    long long w = std::min<long long>((long long)sms * 32, (long long)work);
+    long long wb = (long long)(budget / std::max<size_t>(per_warp, 1));
+    w = std::max<long long>(1, std::min(w, wb));
+    return (int)w;
+  };
+  /* whole blocks of 4 warps: scratch is sliced per launched warp */
+  int nw_dhs = (warps_for((size_t)4 * dcap * sizeof(cx), nsamp) + 3) / 4 * 4;
+  int nw_mie = (warps_for((size_t)8 * mcap * sizeof(double), nslot) + 3) / 4 * 4;
+  size_t scratch_bytes = std::max((size_t)nw_dhs * 4 * dcap * sizeof(cx), (size_t)nw_mie * 8 * mcap * sizeof(double));
+  if (ctx->part_scratch.bytes < scratch_bytes) {
+    if (ctx->part_scratch.p) cudaFree(ctx->part_scratch.p);
+    ctx->part_scratch.p = nullptr;
+    ctx->part_scratch.bytes = 0;
+    ce = cudaMalloc(&ctx->part_scratch.p, scratch_bytes);
+    if (ce != cudaSuccess) return fail_free("recurrence scratch");
+    ctx->part_scratch.bytes = scratch_bytes;
+  }
+  SampleDev sd{d_rcore, d_rshell, d_wvno, d_mre, d_mim, d_stat, d_sF, d_scs, d_mneed, nsamp};
+  int blocks = (nw_dhs + 3) / 4;
+  dhs_kernel<<<blocks, 128, 0, st>>>(sd, d_mu, (cx *)ctx->part_scratch.p, dcap, d_next);
+  /* a failed DHS sample marks its (part, lam, l, k) slot for the Mie pass */
+  {
+    /* status is tiny: bring it back and mark on the host */
+    std::vector<int8_t> stat(nsamp);
+    cudaMemcpyAsync(stat.data(), d_stat, nsamp, cudaMemcpyDeviceToHost, st);
+    ce = cudaStreamSynchronize(st);
+    if (ce != cudaSuccess) {
+      for (void *q : own) cudaFree(q);
+      return mcg_fail(ctx, MCG_ERR_CUDA, "compute_part: DHS kernel failed: %s", cudaGetErrorString(ce));
+    }
+    bool changed = false;
+    for (int p = 0; p < nparts; ++p) {
+      const PartHost &h = H[p];
+      for (int ilam = 0; ilam < h.nlam; ++ilam)
+        for (int l = 0; l < h.nmc; ++l)
+          for (int k = 0; k < h.ns; ++k) {
+            int slot = pd[p].mie0 + (ilam * h.nmc + l) * h.ns + k;
+            for (int i = 0; i < h.nf; ++i) {
+              int s = pd[p].samp0 + ((ilam * h.nmc + l) * h.ns + k) * h.nf + i;
+              if (stat[s] == S_DHS_ERR && !mneed[slot]) {
+                mneed[slot] = 1;
+                changed = true;
+              }
+            }
+          }
+    }
+    int64_t nd = 0, nfail = 0, nm = 0;
+    for (int p = 0; p < nparts; ++p) {
+      const PartHost &h = H[p];
+      int64_t pdhs = 0, pfail = 0, pmie = 0;
+      for (int s = pd[p].samp0; s < pd[p].samp0 + h.nlam * h.nmc * h.ns * h.nf; ++s) {
+        if (stat[s] == S_DHS) pdhs++;
+        if (stat[s] == S_DHS_ERR) { pdhs++; pfail++; }
+      }
+      for (int q = pd[p].mie0; q < pd[p].mie0 + h.nlam * h.nmc * h.ns; ++q) pmie += mneed[q];
+      out[p].n_dhs = pdhs;
+      out[p].n_dhs_fail = pfail;
+      out[p].n_mie = pmie;
+      nd += pdhs; nfail += pfail; nm += pmie;
+    }
+    if (changed) cudaMemcpyAsync(d_mneed, mneed.data(), (size_t)nslot * sizeof(int), cudaMemcpyHostToDevice, st);
+  }
+  MieDev md{d_mrad, d_mlam, d_me1, d_me2, d_mneed, d_mF, d_mcs, d_mok, nslot};
+  blocks = (nw_mie + 3) / 4;
+  mie_kernel<<<blocks, 128, 0, st>>>(md, (double *)ctx->part_scratch.p, mcap, d_next + 1);
+  AccDev ad{d_parts, nparts, d_rowpart, d_stat, d_sF, d_scs, d_mF, d_mcs, d_sinw, tot2,
+            d_kabs, d_ksca, d_kext, d_Fout, d_rhoav, nrows};
+  accum_kernel<<<(nrows + 3) / 4, 128, 0, st>>>(ad);
+  ce = cudaGetLastError();
+  std::vector<double> kabs(nrows), ksca(nrows), kext(nrows), Fo((size_t)nrows * 6 * NA), rhoav(nparts);
+  std::vector<int8_t> mok(nslot);
+  cudaMemcpyAsync(kabs.data(), d_kabs, nrows * sizeof(double), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(ksca.data(), d_ksca, nrows * sizeof(double), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(kext.data(), d_kext, nrows * sizeof(double), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(Fo.data(), d_Fout, Fo.size() * sizeof(double), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(rhoav.data(), d_rhoav, nparts * sizeof(double), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(mok.data(), d_mok, nslot, cudaMemcpyDeviceToHost, st);
+  cudaError_t se = cudaStreamSynchronize(st);
+  for (void *q : own) cudaFree(q);
+  if (ce != cudaSuccess || se != cudaSuccess)
+    return mcg_fail(ctx, MCG_ERR_CUDA, "compute_part: kernels failed: %s",
+                    cudaGetErrorString(ce != cudaSuccess ? ce : se));
+  for (int q = 0; q < nslot; ++q)
+    if (mneed[q] && !mok[q])
+      return mcg_fail(ctx, MCG_ERR_LIMIT, "compute_part: homogeneous-sphere fallback did not fit (slot %d)", q);
+  for (int p = 0; p < nparts; ++p) {
+    const int r0 = pd[p].out0, n = H[p].nlam;
+    memcpy(out[p].kabs, kabs.data() + r0, n * sizeof(double));
+    memcpy(out[p].ksca, ksca.data() + r0, n * sizeof(double));
+    memcpy(out[p].kext, kext.data() + r0, n * sizeof(double));
+    memcpy(out[p].F, Fo.data() + (size_t)r0 * 6 * NA, (size_t)n * 6 * NA * sizeof(double));
+    out[p].rho_av = rhoav[p];
+    out[p].mscale = H[p].mscale;
+    out[p].rscale = H[p].rscale;
+  }
+  return MCG_OK;
+}

@@ -1,0 +1,356 @@
+"""Host-side model set-up: the parts of Init.f that build what the packet loop
+reads, plus the keyword-deck surface.
+
+    parse_deck            key=value decks, lower-cased keys, '*' comments,
+                          quotes stripped, -s overrides (Init.f:462-498)
+    readrefind            .lnk refractive-index regridding (readrefindCP,
+                          ComputePart.f:1102-1172, log-log interpolation and
+                          the dielectric long-wavelength extrapolation)
+    wavelength_grid       Init.f:2580-2614 (log grid, nu, dnu)
+    spatial_grid          Init.f:2779-2930 (radial log grid with the star cell
+                          i = 0, cos-theta edges from the midpoint rule)
+    zones_density         Init.f:3054-3139 ('ZONES' density, one or more zones)
+    mrn_abundances        MRN.f:21-201 (gsd_MRN mass fractions of size bins)
+    grain_bins            Init.f:1323-1420 (computepartNN:ngrains -> log bins)
+
+The radial/theta regridding MCMax applies during its first iterations
+(RegridR, RegridTheta) is outside the packet loop and not restated: models
+here use the plain log radial grid.
+"""
+import math
+import os
+import shlex
+
+import numpy as np
+
+from . import api
+from ._ffi import TT, NANG
+
+AU = 1.49598e13
+RSUN = 6.9599e10
+MSUN = 1.98892e33
+LSUN = 3.846e33
+CLIGHT_MICRON = 2.9979e14
+
+
+# ---------------------------------------------------------------- keyword deck
+def parse_deck(text, overrides=()):
+    """Parse an MCMax input deck.  Returns {key: value-string}; `overrides`
+    are 'key=value' strings applied after the file (the -s switches)."""
+    out = {}
+
+    def take(line):
+        line = line.split("*", 1)[0] if line.lstrip().startswith("*") else line
+        if "=" not in line:
+            return
+        key, val = line.split("=", 1)
+        key = key.strip().lower()
+        val = val.strip()
+        if val[:1] in ("'", '"'):
+            q = val[0]
+            val = val[1:].split(q, 1)[0]
+        else:
+            val = val.split()[0] if val.split() else ""
+        if key:
+            out[key] = val
+
+    for line in text.splitlines():
+        if line.strip().startswith("*") or not line.strip():
+            continue
+        take(line)
+    for ov in overrides:
+        take(ov)
+    return out
+
+
+def deck_value(d, key, default, cast=float):
+    if key not in d:
+        return default
+    v = d[key]
+    if cast is bool:
+        return v.strip(".").lower() in ("true", "t", "1", "yes")
+    if cast is float:
+        return float(v.lower().replace("d", "e"))
+    return cast(v)
+
+
+# ---------------------------------------------------------------- refractive index
+def read_lnk(path):
+    rows = []
+    with open(path) as f:
+        for line in f:
+            s = line.strip()
+            if not s or s[0] in "#*!":
+                continue
+            parts = s.replace("D", "E").replace("d", "e").split()
+            try:
+                rows.append([float(x) for x in parts[:3]])
+            except ValueError:
+                continue
+    return np.array(rows)
+
+
+def readrefind(path_or_table, grid, loglog=False):
+    """Regrid (lam, n, k) onto `grid` (ComputePart.f:1102-1172)."""
+    tab = read_lnk(path_or_table) if isinstance(path_or_table, str) else np.asarray(path_or_table, float)
+    grid = np.asarray(grid, float)
+    n = grid.size
+    e1 = np.zeros(n)
+    e2 = np.zeros(n)
+    i = 0
+    x0, y01, y02 = tab[0]
+    y02 = max(y02, 1e-8)
+    while i < n and x0 >= grid[i]:
+        e1[i], e2[i] = y01, y02
+        i += 1
+    for x1, y11, y12 in tab[1:]:
+        if i >= n:
+            break
+        y12 = max(y12, 1e-8)
+        while i < n and grid[i] <= x1 and grid[i] > x0:
+            e1[i] = 10 ** (math.log10(y11) + math.log10(grid[i] / x1) * math.log10(y01 / y11) / math.log10(x0 / x1))
+            e2[i] = 10 ** (math.log10(y12) + math.log10(grid[i] / x1) * math.log10(y02 / y12) / math.log10(x0 / x1))
+            i += 1
+        x0, y01, y02 = x1, y11, y12
+    if i < n:
+        if loglog and i >= 2:
+            for j in range(i, n):
+                r = math.log10(grid[i - 2] / grid[j]) / math.log10(grid[i - 2] / grid[i - 1])
+                e1[j] = 10 ** (math.log10(e1[i - 2]) + math.log10(e1[i - 1] / e1[i - 2]) * r)
+                e2[j] = 10 ** (math.log10(e2[i - 2]) + math.log10(e2[i - 1] / e2[i - 2]) * r)
+        else:
+            for j in range(i, n):
+                e1[j] = e1[i - 1]
+                e2[j] = e2[i - 1] * grid[i - 1] / grid[j]
+    return e1, e2
+
+
+def read_particle_file(path):
+    """Particle file of ComputePart's 'FILE' standard (ComputePart.f:65-92):
+    ns, nf, then per material a .lnk path line and a 'frac rho' line."""
+    lines = []
+    with open(path) as f:
+        for line in f:
+            s = line.strip()
+            if s and not s.startswith("*"):
+                lines.append(s)
+    ns = int(lines[0].split()[0])
+    nf = int(lines[1].split()[0])
+    mats = []
+    k = 2
+    base = os.path.dirname(os.path.abspath(path))
+    while k + 1 < len(lines):
+        name = shlex.split(lines[k])[0]
+        if not os.path.isabs(name):
+            name = os.path.join(base, name)
+        fr, rh = [float(x.replace("d", "e").replace("D", "E")) for x in lines[k + 1].split()[:2]]
+        mats.append((name, fr, rh))
+        k += 2
+    return ns, nf, mats
+
+
+# ---------------------------------------------------------------- grids
+def wavelength_grid(lam1, lam2, nlam):
+    i = np.arange(nlam)
+    lam = 10.0 ** (math.log10(lam1) + (math.log10(lam2) - math.log10(lam1)) * i / (nlam - 1))
+    nu = CLIGHT_MICRON / lam
+    return lam, nu
+
+
+def spatial_grid(rstar_cm, rin, rout, nrad, ntheta):
+    """Edges R[0..nR] (AU, R[0] = Rstar) and cos-theta edges Theta[0..nTheta-1]
+    following Init.f:2779-2890 without refinement (ntspan = ntlev = 0)."""
+    nR = nrad + 1
+    nT = ntheta + 1
+    th = []
+    k = nT // 2
+    for j in range(1, k + 1):
+        th.append((j - 1) / (k - 1))
+        th.append(math.cos(0.5 * math.pi * j / (k + 1)))
+    i = len(th)
+    if i < nT:
+        for j in range(i + 1, nT + 1):
+            th.append((j - i + 1) / (nT - i + 1))
+    th = sorted(th)[:nT]
+    theta_av = [math.acos((th[nT - i] + th[nT - i - 1]) / 2.0) for i in range(1, nT)]
+    R = np.zeros(nR + 1)
+    R[0] = rstar_cm / AU
+    ii = np.arange(nR)
+    R[1:] = 10.0 ** (math.log10(rin) + (math.log10(rout) - math.log10(rin)) * ii / (nR - 1))
+    Theta = np.zeros(nT)
+    thet = np.zeros(nT)
+    Theta[0] = 1.0
+    thet[0] = 0.0
+    for i in range(2, nT):
+        thet[i - 1] = (theta_av[i - 2] + theta_av[i - 1]) / 2.0
+        Theta[i - 1] = math.cos(thet[i - 1])
+    Theta[nT - 1] = 0.0
+    thet[nT - 1] = math.pi / 2.0
+    SinTheta = np.sin(thet)
+    return R, Theta, thet, SinTheta
+
+
+def cell_volumes(R, Theta):
+    nR = R.size - 1
+    nc = Theta.size - 1
+    V = np.zeros((nR, nc))
+    for i in range(nR):
+        for j in range(nc):
+            V[i, j] = (4.0 * math.pi / 3.0) * (R[i + 1] ** 3 - R[i] ** 3) * (Theta[j] - Theta[j + 1]) * AU ** 3
+    return V
+
+
+def zones_density(R, Theta, thet, zones):
+    """'ZONES' dust density (Init.f:3054-3139).  zones: list of dicts with
+    rin, rout, mdust (Msun), denspow, sh, rsh, shpow.  Cell i = 0 gets 1e-60
+    (Init.f:2932-2938)."""
+    nR = R.size - 1
+    nc = Theta.size - 1
+    V = cell_volumes(R, Theta)
+    R_av = AU * 10.0 ** ((np.log10(R[:-1]) + np.log10(R[1:])) / 2.0)
+    dens = np.full((nR, nc), 1e-60)
+    total = np.zeros((nR, nc))
+    for z in zones:
+        zd = np.zeros((nR, nc))
+        tot = 0.0
+        for i in range(1, nR):
+            if not (R_av[i] >= z["rin"] * AU and R_av[i] <= z["rout"] * AU):
+                continue
+            for j in range(nc):
+                acc = 0.0
+                for jj in range(1, 11):
+                    theta = thet[j] + (thet[j + 1] - thet[j]) * jj / 11.0
+                    r = R_av[i] * math.sin(theta) / AU
+                    zz = R_av[i] * math.cos(theta) / AU
+                    hr = z["sh"] * (r / z["rsh"]) ** z["shpow"]
+                    f1 = r ** (-z["denspow"])
+                    f2 = math.exp(-(zz / hr) ** 2)
+                    acc += f1 * f2 / hr / 10.0
+                zd[i, j] = acc
+                tot += acc * V[i, j]
+        zd *= z["mdust"] * MSUN / tot
+        total += zd
+    dens[1:] = 1e-60 + total[1:]
+    return dens, V
+
+
+def mrn_abundances(rgrain, rmin, rmax, index):
+    """Mass fraction of each size bin for n(a) ~ a^-index (MRN.f gsd_MRN)."""
+    rg = np.asarray(rgrain, float)
+    n = rg.size
+    lr = np.zeros(n + 1)
+    for i in range(1, n):
+        lr[i] = (math.log(rg[i - 1]) + math.log(rg[i])) / 2.0
+    lr[0] = 2 * math.log(rg[0]) - lr[1] if n > 1 else math.log(rmin)
+    lr[n] = 2 * math.log(rg[n - 1]) - lr[n - 1] if n > 1 else math.log(rmax)
+    rint = np.exp(lr)
+    ri = 4.0 - index
+    fac = 3.0 / ri
+
+    def piece(a, b):
+        if abs(index - 4.0) <= 1e-6:
+            return math.log(b) - math.log(a)
+        return fac * (b ** ri - a ** ri)
+
+    ab = np.zeros(n)
+    for i in range(n):
+        a, b = rint[i], rint[i + 1]
+        if a >= rmax or b <= rmin:
+            continue
+        ab[i] = piece(max(a, rmin), min(b, rmax))
+    norm = piece(max(rint[0], rmin), min(rint[n], rmax))
+    ab /= norm
+    ab[ab <= 1e-100] = 0.0
+    return ab
+
+
+def grain_bins(amin, amax, ngrains):
+    """computepartNN:ngrains=N -> N log-spaced [amin_i, amax_i] bins
+    (Init.f:1388-1447)."""
+    edges = [10 ** (math.log10(amin) + math.log10(amax / amin) * i / ngrains) for i in range(ngrains + 1)]
+    return [(edges[i], edges[i + 1]) for i in range(ngrains)]
+
+
+# ---------------------------------------------------------------- model
+def integrate(nu, spec):
+    """Trapezoid over frequency in the reference's order (Radiation.f:1-18)."""
+    L = 0.0
+    for i in range(len(nu) - 1):
+        L = L + (abs(nu[i] - nu[i + 1]) * 0.5) * (spec[i] + spec[i + 1])
+    return L
+
+
+class Model:
+    """Everything mcg_set_model uploads (module globals of the reference)."""
+
+    def __init__(self, **kw):
+        self.__dict__.update(kw)
+
+    @property
+    def ncell(self):
+        return self.nr * (self.nt - 1)
+
+
+def synthetic_lnk(lam, kpref=0.03):
+    """n(lam) = clip(1.7 + 0.1 log10 lam, 1.5, 3.5), k(lam) = clip(kpref lam^0.5,
+    1e-3, 2) on the grid (the synthetic dust of the benchmark decks)."""
+    lam = np.asarray(lam, float)
+    n = np.clip(1.7 + 0.1 * np.log10(lam), 1.5, 3.5)
+    k = np.clip(kpref * lam ** 0.5, 1e-3, 2.0)
+    return n, k
+
+
+def disk_model(ctx, *, tstar=10000.0, rstar=2.5, rin=0.5, rout=100.0, mdust=1e-5, sh=0.05 * math.sqrt(2.0),
+               rsh=1.0, shpow=1.125, denspow=1.0, nrad=100, ntheta=60, lam1=0.1, lam2=3000.0, nlam=100,
+               amin=0.1, amax=1.0, apow=3.5, ngrains=20, ns=5, nf=20, fmax=0.8, blend=True, porosity=0.25,
+               rho=3.0, kpref=0.03, scat_how=2, compositions=None, opacities=None):
+    """Build a passive-disk model: star, ZONES density, grain bins with DHS
+    opacities from the library (ComputePart per bin), Planck table.
+    `opacities` may pass precomputed (Kabs, Ksca, F) per bin."""
+    rstar_cm = rstar * RSUN
+    lam, nu = wavelength_grid(lam1, lam2, nlam)
+    R, Theta, thet, SinTheta = spatial_grid(rstar_cm, rin, rout, nrad, ntheta)
+    dens, V = zones_density(R, Theta, thet, [dict(rin=rin, rout=rout, mdust=mdust, denspow=denspow, sh=sh,
+                                                  rsh=rsh, shpow=shpow)])
+    BB = api.bb_table(lam)
+    Fstar = math.pi * rstar_cm ** 2 * BB[:, 0].copy()
+    for i in range(nlam):
+        Fstar[i] = math.pi * rstar_cm ** 2 * api.planck(tstar, lam[i])
+    Lstar = integrate(nu, Fstar)
+    bins = grain_bins(amin, amax, ngrains)
+    rg = [math.sqrt(a * b) * 1e-4 for a, b in bins]
+    w = mrn_abundances(rg, amin * 1e-4, amax * 1e-4, apow)
+    if opacities is None:
+        comps = compositions or [synthetic_lnk(lam, kpref)]
+        parts = []
+        for a, b in bins:
+            parts.append(dict(lam=lam, e1=np.array([c[0] for c in comps]), e2=np.array([c[1] for c in comps]),
+                              frac=np.ones(len(comps)), rho=np.full(len(comps), rho), amin=a, amax=b, apow=apow,
+                              fmax=fmax, porosity=porosity, blend=blend, ns=ns, nf=nf))
+        res = ctx.compute_part_batch(parts)
+        Kabs = np.array([r["kabs"] for r in res])
+        Ksca = np.array([r["ksca"] for r in res])
+        F = np.array([r["F"] for r in res])
+    else:
+        Kabs, Ksca, F = opacities
+    if scat_how == 0:
+        Kabs = Kabs.copy()
+        Ksca = np.zeros_like(Ksca)
+    if scat_how == 1:
+        F = np.ones_like(F)
+    nr = R.size - 1
+    nt = Theta.size
+    ncomp = len(bins)
+    comp_w = np.tile(w, (nr * (nt - 1), 1))
+    return Model(nr=nr, nt=nt, R=R, Theta=Theta, SinTheta=SinTheta, thet=thet, dens=dens.reshape(-1),
+                 V=V.reshape(-1), ncomp=ncomp, comp_w=comp_w, nlam=nlam, lam=lam, nu=nu, Kabs=Kabs, Ksca=Ksca,
+                 F=F, BB=BB, Fstar=Fstar, Lstar=Lstar, Tstar=tstar, Rstar_cm=rstar_cm, scat_how=scat_how,
+                 bins=bins, w=w)
+
+
+CONFIGS = {
+    # the reference's CPU-runnable case
+    "cfg0_small": dict(mdust=1e-5, nrad=100, ntheta=60, nlam=100),
+    # thick disk exercising the random walk
+    "cfg1_thick": dict(mdust=1e-3, nrad=200, ntheta=120, nlam=200),
+}

@@ -1,0 +1,816 @@
+/*
+ * oracle_mc.c -- serial CPU restatement of MCMax's photon-packet loop.
+ * Test infrastructure only (checker for the GPU transport kernels and the
+ * timed CPU baseline).
+ *
+ * Follows:
+ *   MCRadiation  MCRadiation.f:6-887   (star emission :355-382, packet loop
+ *                                       :320-648, SED binning :576-646)
+ *   trace2d      MCRadiation.f:901-1141
+ *   Trace2edge   MCRadiation.f:1150-1272, hitR :1274, hitT :1306, hitTsame :1340
+ *   interact     Radiation.f:41-355 (thermal-contact branch)
+ *   scatangle    Radiation.f:381-495, RotateStokes :506-534
+ *   emit         Radiation.f:940-1001, randomdirection :1007-1024
+ *   rotate       Subroutines.f:1648-1675, hunt :2086-2132
+ *   MinDist, RandomWalk  RandomWalk.f:15-147
+ *
+ * Differences from the reference, all deliberate and shared with the GPU
+ * kernels:
+ *   - opacities at the packet wavelength come from the per-cell totals
+ *     KabsTot/KscaTot (the reference builds them in MCRadiation.f:199-236 and
+ *     uses them in interact; trace2d re-sums the grains, which only differs by
+ *     floating-point reassociation);
+ *   - the Planck-mean table of a cell is the pre-summed KpCell[iT] and the
+ *     re-emission normalisation kp is formed from it (linear in the grains);
+ *   - random numbers: Philox4x32-10 per packet (rng = 0) or the reference's
+ *     ran1 (rng = 1);
+ *   - sin/cos/log come from detmath.h so the FP64 GPU path can replay a run
+ *     bit for bit;
+ *   - a packet whose cell search at emission finds no cell (|z|/R* exactly on
+ *     a cone) takes the cell below; a zero-width emission interval takes its
+ *     lower edge; an escape with |vz| = 1 goes to the last angle bin (the
+ *     reference would index bin 31).
+ * Options not built (not used by the hot-path configurations): per-grain
+ * temperatures (tcontact = .false.), QHP grains, viscous / inner-gas / ISRF
+ * emission, forced first interaction, multi-wavelength spectra, local
+ * radiation field, radiation pressure, etrace.
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "oracle.h"
+#include "../mcmax_b200/csrc/detmath.h"
+#include "../mcmax_b200/csrc/philox.h"
+
+#define AU_CM 1.49598e13
+#define PI_D 3.14159265358979323846
+#define NY_RW 1000
+
+typedef struct {
+  double x, y, z, vx, vy, vz, E, Q, U, V, Sx, Sy, Sz;
+  double wl1, wl2;
+  int ilam1, ilam2, edgeNr, i, j;
+  int onEdge, scatt, pol;
+} orc_phot;
+
+typedef struct {
+  int rng;
+  px_stream px;
+  int32_t idum, iv[32], iy;
+} rng_t;
+
+static double rnd(rng_t *r) {
+  if (r->rng == 0) return px_next(&r->px);
+  return orc_ran1(&r->idum, r->iv, &r->iy);
+}
+
+typedef struct {
+  const orc_model *m;
+  orc_result *out;
+  int nc;         /* theta cells per radius = nt-1 */
+  int scattering; /* any Ksca > 0 and scat_how != 0 */
+  int scat_how;
+  int rw;
+  double factRW;
+  double *mass;
+  double *Tcell;
+  int *lastphot;
+  int *iTD;
+  double nEJv;
+} mc_t;
+
+static inline int cidx(const mc_t *s, int i, int j) { return i * s->nc + (j - 1); }
+
+static void randomdirection(rng_t *r, double *x, double *y, double *z) {
+  double rr;
+  for (;;) {
+    *x = 2.0 * rnd(r) - 1.0;
+    *y = 2.0 * rnd(r) - 1.0;
+    *z = 2.0 * rnd(r) - 1.0;
+    rr = ((*x) * (*x) + (*y) * (*y)) + (*z) * (*z);
+    if (!(rr > 1.0)) break;
+  }
+  rr = sqrt(rr);
+  *x = *x / rr;
+  *y = *y / rr;
+  *z = *z / rr;
+}
+
+static void set_s_from_v(orc_phot *p) {
+  double x = -p->vy, y = p->vx, z = 0.0;
+  double r = sqrt((x * x + y * y) + z * z);
+  p->Sx = x / r;
+  p->Sy = y / r;
+  p->Sz = z / r;
+}
+
+/* emit from a spectrum given as a callback-free array (Radiation.f:940-1001) */
+static void emit_scan(mc_t *s, rng_t *r, orc_phot *p, const double *spec, double Lttot) {
+  const orc_model *m = s->m;
+  s->out->counters[0]++;
+  randomdirection(r, &p->vx, &p->vy, &p->vz);
+  p->scatt = 0;
+  p->pol = 0;
+  set_s_from_v(p);
+  double Lr = rnd(r) * Lttot;
+  double Ltold = 0.0, Lt = 0.0;
+  for (int i = 0; i < m->nlam - 1; ++i) {
+    Lt = Lt + (fabs(m->nu[i] - m->nu[i + 1]) * 0.5) * (spec[i] + spec[i + 1]);
+    if (Lt >= Lr) {
+      double d = Lt - Ltold;
+      p->wl1 = d != 0.0 ? (Lr - Ltold) / d : 1.0;
+      p->wl2 = 1.0 - p->wl1;
+      p->ilam1 = i;
+      p->ilam2 = i + 1;
+      return;
+    }
+    Ltold = Lt;
+  }
+  p->wl1 = 0.0;
+  p->wl2 = 1.0;
+  p->ilam1 = m->nlam - 2;
+  p->ilam2 = m->nlam - 1;
+}
+
+static int hitR(double Rad, double r, double b, double *v) {
+  int hit = 0;
+  *v = 1e200;
+  double cc = r - Rad;
+  double discr = b * b - 4.0 * cc;
+  if (discr >= 0.0) {
+    discr = sqrt(discr);
+    double q = (b > 0.0) ? -0.5 * (b + discr) : -0.5 * (b - discr);
+    double vr1 = q, vr2 = cc / q;
+    if (vr1 > 0.0) {
+      *v = vr1;
+      hit = 1;
+    }
+    if (vr2 > 0.0 && vr2 < *v) {
+      *v = vr2;
+      hit = 1;
+    }
+  }
+  return hit;
+}
+
+static int hitT(const orc_phot *p, double Thet, double r, double b, double *v) {
+  int hit = 0;
+  *v = 1e200;
+  double at = Thet - p->vz * p->vz;
+  double bt = Thet * b - (2.0 * p->z) * p->vz;
+  double ct = Thet * r - p->z * p->z;
+  double discr = bt * bt - (4.0 * at) * ct;
+  if (discr >= 0.0) {
+    discr = sqrt(discr);
+    double q = (bt > 0.0) ? -0.5 * (bt + discr) : -0.5 * (bt - discr);
+    double vt1 = q / at, vt2 = ct / q;
+    if (vt1 > 0.0) {
+      *v = vt1;
+      hit = 1;
+    }
+    if (vt2 > 0.0 && vt2 < *v) {
+      *v = vt2;
+      hit = 1;
+    }
+  }
+  return hit;
+}
+
+static int hitTsame(const orc_phot *p, double Thet, double b, double *v) {
+  double bt = Thet * b - (2.0 * p->z) * p->vz;
+  double at = Thet - p->vz * p->vz;
+  *v = (-bt) / at;
+  return *v > 0.0;
+}
+
+/* returns 0 on success, 1 when nothing can be hit (reference: stop) */
+static int trace2edge(mc_t *s, orc_phot *p, double *v, int *inext, int *jnext) {
+  const orc_model *m = s->m;
+  int nt = m->nt;
+  double r = (p->x * p->x + p->y * p->y) + p->z * p->z;
+  double R1 = m->R[p->i] * m->R[p->i];
+  double R2 = m->R[p->i + 1] * m->R[p->i + 1];
+  double T1 = m->Theta[p->j - 1] * m->Theta[p->j - 1];
+  double T2 = m->Theta[p->j] * m->Theta[p->j];
+  double b = 2.0 * ((p->x * p->vx + p->y * p->vy) + p->z * p->vz);
+  int hR1, hR2, hT1, hT2;
+  double vR1, vR2, vT1, vT2;
+  if (!p->onEdge) {
+    hR1 = hitR(R1, r, b, &vR1);
+    hR2 = hitR(R2, r, b, &vR2);
+    hT1 = hitT(p, T1, r, b, &vT1);
+    hT2 = hitT(p, T2, r, b, &vT2);
+  } else if (p->edgeNr == 1) {
+    hR1 = 0;
+    vR1 = 1e200;
+    hR2 = hitR(R2, r, b, &vR2);
+    hT1 = hitT(p, T1, r, b, &vT1);
+    hT2 = hitT(p, T2, r, b, &vT2);
+  } else if (p->edgeNr == 2) {
+    hR1 = hitR(R1, r, b, &vR1);
+    hR2 = 1;
+    vR2 = -b;
+    hT1 = hitT(p, T1, r, b, &vT1);
+    hT2 = hitT(p, T2, r, b, &vT2);
+  } else if (p->edgeNr == 3) {
+    hR1 = hitR(R1, r, b, &vR1);
+    hR2 = hitR(R2, r, b, &vR2);
+    hT1 = 0;
+    vT1 = 1e200;
+    if (p->j != nt - 1) {
+      hT2 = hitT(p, T2, r, b, &vT2);
+    } else {
+      vT2 = -p->z / p->vz;
+      hT2 = vT2 > 0.0;
+    }
+  } else {
+    hR1 = hitR(R1, r, b, &vR1);
+    hR2 = hitR(R2, r, b, &vR2);
+    if (p->j != 1) {
+      hT1 = hitT(p, T1, r, b, &vT1);
+    } else {
+      hT1 = 0;
+      vT1 = 1e200;
+    }
+    if (p->j != nt - 1) {
+      hT2 = hitTsame(p, T2, b, &vT2);
+    } else {
+      hT2 = 0;
+      vT2 = 1e200;
+    }
+  }
+  if (!hR1 && !hR2 && !hT1 && !hT2) {
+    hR1 = hitR(R1, r, b, &vR1);
+    hR2 = hitR(R2, r, b, &vR2);
+    hT1 = hitT(p, T1, r, b, &vT1);
+    hT2 = hitT(p, T2, r, b, &vT2);
+    if (!hR1 && !hR2 && !hT1 && !hT2) return 1;
+  }
+  *v = 1e200;
+  *inext = p->i;
+  *jnext = p->j;
+  if (hR1 && vR1 < *v) {
+    *v = vR1;
+    *inext = p->i - 1;
+    *jnext = p->j;
+    p->edgeNr = 2;
+  }
+  if (hR2 && vR2 < *v) {
+    *v = vR2;
+    *inext = p->i + 1;
+    *jnext = p->j;
+    p->edgeNr = 1;
+  }
+  if (hT1 && vT1 < *v) {
+    *v = vT1;
+    *inext = p->i;
+    *jnext = p->j - 1;
+    p->edgeNr = 4;
+  }
+  if (hT2 && vT2 < *v) {
+    *v = vT2;
+    *inext = p->i;
+    *jnext = p->j + 1;
+    p->edgeNr = 3;
+  }
+  if (*jnext == nt) {
+    *jnext = nt - 1;
+    p->edgeNr = 4;
+  }
+  if (*jnext == 0) {
+    *jnext = 1;
+    p->edgeNr = 3;
+  }
+  return 0;
+}
+
+static void rotate(double *x, double *y, double *z, double u, double v, double w, double theta) {
+  double cost = dm_cos(theta), sint = dm_sin(theta);
+  double u2 = u * u, v2 = v * v, w2 = w * w;
+  double inp = (*x * u + *y * v) + *z * w;
+  double y1 = (u * inp + (*x * (v2 + w2) - u * (v * *y + w * *z)) * cost) + (v * *z - w * *y) * sint;
+  double y2 = (v * inp + (*y * (u2 + w2) - v * (u * *x + w * *z)) * cost) + (w * *x - u * *z) * sint;
+  double y3 = (w * inp + (*z * (u2 + v2) - w * (u * *x + v * *y)) * cost) + (u * *y - v * *x) * sint;
+  *x = y1;
+  *y = y2;
+  *z = y3;
+}
+
+static void rotate_stokes(orc_phot *p, double x, double y, double z) {
+  double P = (p->U / p->E) * (p->U / p->E) + (p->Q / p->E) * (p->Q / p->E);
+  if (P == 0.0) return;
+  double cost = (p->Sx * x + p->Sy * y) + p->Sz * z;
+  double sint = (x - (p->Sx * (p->vy * p->vy + p->vz * p->vz) - p->vx * (p->vy * p->Sy + p->vz * p->Sz)) * cost) /
+                (p->vy * p->Sz - p->vz * p->Sy);
+  double cos2t = cost * cost - sint * sint;
+  double sin2t = (2.0 * sint) * cost;
+  double Q = p->Q * cos2t + p->U * sin2t;
+  double U = (-p->Q) * sin2t + p->U * cos2t;
+  double P2 = (U / p->E) * (U / p->E) + (Q / p->E) * (Q / p->E);
+  double sPP2 = sqrt(P / P2);
+  p->U = sPP2 * U;
+  p->Q = sPP2 * Q;
+}
+
+/* Radiation.f:381-495 for the component matrix F[6*180] and IF[2] */
+static void scatangle(mc_t *s, rng_t *r, orc_phot *p, const double *F, const double *IF) {
+  const orc_model *m = s->m;
+  const double *F11 = F, *F12 = F + 180, *F22 = F + 360, *F33 = F + 540, *F34 = F + 720, *F44 = F + 900;
+  double IF11 = IF[0] * 180.0, IF12 = IF[1] * 180.0;
+  double phi;
+  if (p->pol) {
+    double Itot = 0.0;
+    for (int i = 1; i <= 180; ++i)
+      Itot = (Itot + IF11 * p->E) + IF12 * (p->Q * m->cos2phi[i] + p->U * m->sin2phi[i]);
+    Itot = rnd(r) * Itot;
+    double I1 = 0.0, I0 = 0.0;
+    phi = PI_D;
+    for (int i = 1; i <= 180; ++i) {
+      I0 = (I0 + IF11 * p->E) + IF12 * (p->Q * m->cos2phi[i] + p->U * m->sin2phi[i]);
+      if (I0 > Itot) {
+        double wp1 = (I0 - Itot) / (I0 - I1);
+        phi = (PI_D * ((double)i - wp1)) / 180.0;
+        break;
+      }
+      I1 = I0;
+    }
+  } else {
+    phi = rnd(r) * PI_D;
+  }
+  double x = p->Sx, y = p->Sy, z = p->Sz;
+  rotate(&x, &y, &z, p->vx, p->vy, p->vz, phi);
+  if (p->pol) rotate_stokes(p, x, y, z);
+  p->Sx = x;
+  p->Sy = y;
+  p->Sz = z;
+  double Fr = 180.0 * (p->E * IF[0] + p->Q * IF[1]);
+  Fr = rnd(r) * Fr;
+  double Fi = 0.0, FiOld = 0.0, theta = PI_D;
+  int ib = 180;
+  for (int i = 1; i <= 180; ++i) {
+    Fi = Fi + (PI_D * m->sinthet[i - 1]) * (F11[i - 1] * p->E + F12[i - 1] * p->Q);
+    if (Fi > Fr) {
+      theta = (double)i - (Fi - Fr) / (Fi - FiOld);
+      theta = (theta * PI_D) / 180.0;
+      ib = i;
+      break;
+    }
+    FiOld = Fi;
+  }
+  if (rnd(r) < 0.5) theta = -theta;
+  int k = ib - 1;
+  double E = (0.0 + F11[k] * p->E) + F12[k] * p->Q;
+  double Q = (0.0 + F12[k] * p->E) + F22[k] * p->Q;
+  double U = 0.0 + F33[k] * p->U;
+  double Fs = (theta >= 0.0 && !signbit(theta)) ? fabs(F34[k]) : -fabs(F34[k]);
+  U = U + Fs * p->V;
+  double V = (0.0 - Fs * p->U) + F44[k] * p->V;
+  if (E != 0.0) {
+    p->Q = (p->E * Q) / E;
+    p->U = (p->E * U) / E;
+    p->V = (p->E * V) / E;
+  }
+  rotate(&p->vx, &p->vy, &p->vz, p->Sx, p->Sy, p->Sz, theta);
+  double rr = sqrt((p->vx * p->vx + p->vy * p->vy) + p->vz * p->vz);
+  p->vx /= rr;
+  p->vy /= rr;
+  p->vz /= rr;
+  rr = sqrt((p->Sx * p->Sx + p->Sy * p->Sy) + p->Sz * p->Sz);
+  p->Sx /= rr;
+  p->Sy /= rr;
+  p->Sz /= rr;
+  if (ib != 1 && ib != 180) p->pol = 1;
+}
+
+/* interact, thermal-contact branch (Radiation.f:41-76, :160-258, :262-315) */
+static void interact(mc_t *s, rng_t *r, orc_phot *p) {
+  const orc_model *m = s->m;
+  int c = cidx(s, p->i, p->j);
+  int nlam = m->nlam;
+  const double *KabsT = m->KabsTot + (size_t)c * nlam;
+  const double *KscaT = m->KscaTot + (size_t)c * nlam;
+  double Ksca = KscaT[p->ilam1] * p->wl1 + KscaT[p->ilam2] * p->wl2;
+  double Kext = Ksca + (KabsT[p->ilam1] * p->wl1 + KabsT[p->ilam2] * p->wl2);
+  double KabsTot = Kext - Ksca;
+  double Albedo = Ksca / Kext;
+  s->out->counters[1]++;
+  if (!s->scattering || rnd(r) > Albedo) {
+    s->out->counters[2]++;
+    p->scatt = 0;
+    p->pol = 0;
+    p->Q = 0.0;
+    p->U = 0.0;
+    p->V = 0.0;
+    const double *kp = m->KpCell + (size_t)c * (ORC_TMAX + 1);
+    s->out->Eabs[c] = s->out->Eabs[c] + (p->E * (KabsTot - 0.0)) / KabsTot;
+    double T0 = s->Tcell[c];
+    double T1 = orc_increase_t(kp, s->out->Eabs[c] / s->mass[c], T0);
+    int iT0 = (int)(T0 / 1.0), iT1 = (int)(T1 / 1.0);
+    double epsT0 = T0 - (double)iT0 * 1.0, epsT1 = T1 - (double)iT1 * 1.0;
+    if (iT0 >= ORC_TMAX - 1) iT0 = ORC_TMAX - 2;
+    if (iT1 >= ORC_TMAX - 1) iT1 = ORC_TMAX - 1;
+    if (iT0 < 1) iT0 = 1;
+    if (iT1 < 2) iT1 = 2;
+    double *spec = (double *)malloc(sizeof(double) * (size_t)nlam);
+    const int TT = ORC_TMAX + 1;
+    double kpe;
+    if (iT0 == iT1) {
+      for (int l = 0; l < nlam; ++l)
+        spec[l] = (m->BB[(size_t)l * TT + iT0 + 1] - m->BB[(size_t)l * TT + iT0]) * KabsT[l];
+      kpe = kp[iT0 + 1] - kp[iT0];
+    } else {
+      for (int l = 0; l < nlam; ++l) {
+        const double *B = m->BB + (size_t)l * TT;
+        spec[l] = (((epsT1 * B[iT1 + 1] + (1.0 - epsT1) * B[iT1]) - epsT0 * B[iT0 + 1]) - (1.0 - epsT0) * B[iT0]) * KabsT[l];
+      }
+      kpe = ((epsT1 * kp[iT1 + 1] + (1.0 - epsT1) * kp[iT1]) - epsT0 * kp[iT0 + 1]) - (1.0 - epsT0) * kp[iT0];
+    }
+    if (kpe == 0.0) {
+      for (int l = 0; l < nlam; ++l) spec[l] = 0.0;
+      kpe = 0.0 / KabsTot;
+    }
+    emit_scan(s, r, p, spec, kpe);
+    free(spec);
+    s->Tcell[c] = T1;
+  } else {
+    s->out->counters[3]++;
+    p->scatt = 1;
+    if (s->scat_how == 1) {
+      randomdirection(r, &p->vx, &p->vy, &p->vz);
+    } else {
+      double KscaR = Ksca * rnd(r);
+      const double *F = NULL, *IF = NULL;
+      for (int q = 0; q < m->ncomp && F == NULL; ++q) {
+        double w1 = m->comp_w[(size_t)c * m->ncomp + q];
+        double w2 = (w1 * p->wl2) * m->Ksca_comp[(size_t)q * nlam + p->ilam2];
+        KscaR = KscaR - w2;
+        if (KscaR < 0.0) {
+          F = m->F_comp + ((size_t)q * nlam + p->ilam2) * 1080;
+          IF = m->IF_comp + ((size_t)q * nlam + p->ilam2) * 2;
+          break;
+        }
+        w1 = (w1 * p->wl1) * m->Ksca_comp[(size_t)q * nlam + p->ilam1];
+        KscaR = KscaR - w1;
+        if (KscaR < 0.0) {
+          F = m->F_comp + ((size_t)q * nlam + p->ilam1) * 1080;
+          IF = m->IF_comp + ((size_t)q * nlam + p->ilam1) * 2;
+          break;
+        }
+      }
+      double Mavg[1080], IFavg[2];
+      if (F == NULL) {
+        /* averaged matrix fallback, Radiation.f:293-315 */
+        memset(Mavg, 0, sizeof Mavg);
+        IFavg[0] = IFavg[1] = 0.0;
+        for (int q = 0; q < m->ncomp; ++q) {
+          double w1 = m->comp_w[(size_t)c * m->ncomp + q];
+          double w2 = ((w1 * p->wl2) * m->Ksca_comp[(size_t)q * nlam + p->ilam2]) / Ksca;
+          w1 = ((w1 * p->wl1) * m->Ksca_comp[(size_t)q * nlam + p->ilam1]) / Ksca;
+          const double *Fa = m->F_comp + ((size_t)q * nlam + p->ilam1) * 1080;
+          const double *Fb = m->F_comp + ((size_t)q * nlam + p->ilam2) * 1080;
+          const double *Ia = m->IF_comp + ((size_t)q * nlam + p->ilam1) * 2;
+          const double *Ib = m->IF_comp + ((size_t)q * nlam + p->ilam2) * 2;
+          IFavg[0] = (IFavg[0] + w1 * Ia[0]) + w2 * Ib[0];
+          IFavg[1] = (IFavg[1] + w1 * Ia[1]) + w2 * Ib[1];
+          for (int e = 0; e < 1080; ++e) Mavg[e] = (Mavg[e] + w1 * Fa[e]) + w2 * Fb[e];
+        }
+        F = Mavg;
+        IF = IFavg;
+        s->out->counters[10]++;
+      }
+      scatangle(s, r, p, F, IF);
+    }
+  }
+}
+
+static double mindist(mc_t *s, const orc_phot *p) {
+  const orc_model *m = s->m;
+  double rho = p->x * p->x + p->y * p->y;
+  double r = sqrt(rho + p->z * p->z);
+  rho = sqrt(rho);
+  double z = fabs(p->z);
+  double R1 = m->R[p->i], R2 = m->R[p->i + 1];
+  double T1 = m->Theta[p->j - 1], T2 = m->Theta[p->j];
+  double ST1 = m->SinTheta[p->j - 1], ST2 = m->SinTheta[p->j];
+  double vR1 = fabs(r - R1), vR2 = fabs(R2 - r);
+  double vT1 = fabs(T1 * rho - ST1 * z), vT2 = fabs(T2 * rho - ST2 * z);
+  double d = vR1;
+  if (vR2 < d) d = vR2;
+  if (vT1 < d) d = vT1;
+  if (vT2 < d) d = vT2;
+  return d;
+}
+
+/* Numerical Recipes hunt on a table of n entries, 1-based jlo in/out */
+static void hunt(const double *xx, int n, double x, int *jlo) {
+  int jhi, jm, inc;
+  int ascnd = xx[n - 1] >= xx[0];
+  if (*jlo <= 0 || *jlo > n) {
+    *jlo = 0;
+    jhi = n + 1;
+  } else {
+    inc = 1;
+    if ((x >= xx[*jlo - 1]) == ascnd) {
+      for (;;) {
+        jhi = *jlo + inc;
+        if (jhi > n) {
+          jhi = n + 1;
+          break;
+        } else if ((x >= xx[jhi - 1]) == ascnd) {
+          *jlo = jhi;
+          inc += inc;
+        } else {
+          break;
+        }
+      }
+    } else {
+      jhi = *jlo;
+      for (;;) {
+        *jlo = jhi - inc;
+        if (*jlo < 1) {
+          *jlo = 0;
+          break;
+        } else if ((x < xx[*jlo - 1]) == ascnd) {
+          jhi = *jlo;
+          inc += inc;
+        } else {
+          break;
+        }
+      }
+    }
+  }
+  while (jhi - *jlo != 1) {
+    jm = (jhi + *jlo) / 2;
+    if ((x >= xx[jm - 1]) == ascnd)
+      *jlo = jm;
+    else
+      jhi = jm;
+  }
+  if (x == xx[n - 1]) *jlo = n - 1;
+  if (x == xx[0]) *jlo = 1;
+}
+
+/* RandomWalk.f:47-147 (thermal contact); returns 1 when a step was taken */
+static int random_walk(mc_t *s, rng_t *r, orc_phot *p, double dmin) {
+  const orc_model *m = s->m;
+  int c = cidx(s, p->i, p->j);
+  int iT = (int)(s->Tcell[c] / 1.0);
+  if (iT == 0) iT = 1;
+  if (iT > ORC_TMAX) iT = ORC_TMAX;
+  if (iT > ORC_TMAX - 1) iT = ORC_TMAX - 1; /* DiffCoeffCell clamp */
+  double Kext = m->KDext[(size_t)c * (ORC_TMAX + 1) + iT];
+  double lr = 1.0 / ((AU_CM * Kext) * m->dens[c]);
+  if (dmin <= s->factRW * lr) return 0;
+  double x = rnd(r);
+  int iy = 1;
+  hunt(m->rw_phi, NY_RW, x, &iy);
+  double v = (((-3.0 * dm_log(m->rw_y[iy - 1])) * (dmin * dmin)) / (lr * (PI_D * PI_D)));
+  double Kabs = m->KDabs[(size_t)c * (ORC_TMAX + 1) + iT];
+  randomdirection(r, &p->vx, &p->vy, &p->vz);
+  p->x = p->x + dmin * p->vx;
+  p->y = p->y + dmin * p->vy;
+  p->z = p->z + dmin * p->vz;
+  double EJv = (p->E * v) * AU_CM;
+  s->out->Eabs[c] = s->out->Eabs[c] + (EJv * Kabs) * m->dens[c];
+  s->out->EJv[c] = s->out->EJv[c] + EJv * Kabs;
+  s->nEJv = s->nEJv + EJv * Kabs;
+  const double *kp = m->KpCell + (size_t)c * (ORC_TMAX + 1);
+  s->Tcell[c] = orc_increase_t(kp, s->out->Eabs[c] / s->mass[c], s->Tcell[c]);
+  s->out->tautot += v / dmin;
+  s->out->counters[4]++;
+  return 1;
+}
+
+/* trace2d, MCRadiation.f:901-1141.  Returns 0 interaction, 1 escape, 2 star
+ * hit / abandoned, -1 geometry failure. */
+static int trace2d(mc_t *s, rng_t *r, orc_phot *p, double tau0, int64_t pid) {
+  const orc_model *m = s->m;
+  int nlam = m->nlam;
+  double tau = 0.0;
+  int ntrace = 0;
+  if (s->rw && m->thick && m->thick[cidx(s, p->i, p->j)] && !p->onEdge) {
+    for (;;) {
+      double dmin = mindist(s, p);
+      if (!random_walk(s, r, p, dmin)) break;
+      double vx, vy, vz, inp;
+      do {
+        randomdirection(r, &vx, &vy, &vz);
+        inp = (p->vx * vx + p->vy * vy) + p->vz * vz;
+      } while (inp < 0.0);
+      p->vx = vx;
+      p->vy = vy;
+      p->vz = vz;
+    }
+  }
+  for (;;) {
+    int c = cidx(s, p->i, p->j);
+    if (s->lastphot[c] != (int)(pid + 1)) {
+      s->out->Ni[c] += 1;
+      s->lastphot[c] = (int)(pid + 1);
+    }
+    const double *KabsT = m->KabsTot + (size_t)c * nlam;
+    const double *KscaT = m->KscaTot + (size_t)c * nlam;
+    double Kabs = KabsT[p->ilam1] * p->wl1 + KabsT[p->ilam2] * p->wl2;
+    double Kext = Kabs;
+    if (s->scattering) Kext = (KscaT[p->ilam1] * p->wl1 + KscaT[p->ilam2] * p->wl2) + Kabs;
+    double KabsBB = Kabs;
+    double v;
+    int inext, jnext;
+    if (trace2edge(s, p, &v, &inext, &jnext)) return -1;
+    s->out->counters[8]++;
+    double tau1 = ((Kext * v) * m->dens[c]) * AU_CM;
+    if (tau + tau1 > tau0) {
+      v = (v * (tau0 - tau)) / tau1;
+      tau1 = tau0 - tau;
+      s->out->tautot += tau1;
+      p->x = p->x + p->vx * v;
+      p->y = p->y + p->vy * v;
+      p->z = p->z + p->vz * v;
+      p->onEdge = 0;
+      double EJv = (p->E * v) * AU_CM;
+      s->out->EJv[c] = s->out->EJv[c] + EJv * KabsBB;
+      s->nEJv = s->nEJv + EJv * KabsBB;
+      return 0;
+    }
+    p->x = p->x + p->vx * v;
+    p->y = p->y + p->vy * v;
+    p->z = p->z + p->vz * v;
+    double EJv = (p->E * v) * AU_CM;
+    s->nEJv = s->nEJv + EJv * KabsBB;
+    s->out->EJv2[c] = s->out->EJv2[c] + s->nEJv * s->nEJv;
+    s->nEJv = 0.0;
+    s->out->EJv[c] = s->out->EJv[c] + EJv * KabsBB;
+    p->onEdge = 1;
+    tau = tau + tau1;
+    s->out->tautot += tau1;
+    if (inext >= m->nr) return 1;
+    if (inext < 0) return 2;
+    p->i = inext;
+    p->j = jnext;
+    ntrace++;
+    if (tau < 0.0) return 2;
+    if (ntrace > m->nr * m->nt * 2) {
+      s->out->counters[6]++;
+      return 2;
+    }
+  }
+}
+
+int orc_mcradiation(const orc_model *m, const orc_run *run, orc_result *out) {
+  const int nr = m->nr, nt = m->nt, nlam = m->nlam;
+  const int nc = nt - 1;
+  const int ncell = nr * nc;
+  mc_t S;
+  memset(&S, 0, sizeof S);
+  S.m = m;
+  S.out = out;
+  S.nc = nc;
+  S.scat_how = run->scat_how;
+  S.scattering = 0;
+  if (run->scat_how != 0)
+    for (size_t k = 0; k < (size_t)ncell * nlam; ++k)
+      if (m->KscaTot[k] != 0.0) {
+        S.scattering = 1;
+        break;
+      }
+  S.rw = run->randomwalk;
+  S.factRW = run->factRW;
+  S.mass = (double *)malloc(sizeof(double) * ncell);
+  S.Tcell = (double *)calloc(ncell, sizeof(double));
+  S.lastphot = (int *)calloc(ncell, sizeof(int));
+  for (int c = 0; c < ncell; ++c) S.mass[c] = m->dens[c] * m->V[c];
+  /* the transport floors the dust density at 1e-50 (CheckMinimumDensity,
+   * DiskStructure.f:2966-2979) after the mass was formed */
+  double *dens = (double *)malloc(sizeof(double) * ncell);
+  for (int c = 0; c < ncell; ++c) dens[c] = m->dens[c] <= 1e-50 ? 1e-50 : m->dens[c];
+  orc_model mm = *m;
+  mm.dens = dens;
+  S.m = &mm;
+
+  memset(out->EJv, 0, sizeof(double) * ncell);
+  memset(out->EJv2, 0, sizeof(double) * ncell);
+  memset(out->Eabs, 0, sizeof(double) * ncell);
+  memset(out->Ni, 0, sizeof(int32_t) * ncell);
+  memset(out->spec, 0, sizeof(double) * nlam * (ORC_NANGLE_SED + 1));
+  memset(out->scatspec, 0, sizeof(double) * nlam * (ORC_NANGLE_SED + 1));
+  memset(out->ispec, 0, sizeof(int32_t) * nlam * (ORC_NANGLE_SED + 1));
+  memset(out->counters, 0, sizeof out->counters);
+  out->tautot = 0.0;
+
+  /* SED weights, MCRadiation.f:52-80 */
+  double *wlam = (double *)malloc(sizeof(double) * nlam);
+  for (int i = 0; i < nlam; ++i) {
+    if (i == 0)
+      wlam[i] = -1e23 / (m->nu[1] / 2.0);
+    else if (i == nlam - 1)
+      wlam[i] = -1e23 / ((m->nu[nlam - 1] - m->nu[nlam - 2]) / 2.0);
+    else
+      wlam[i] = -1e23 / ((m->nu[i + 1] - m->nu[i - 1]) / 2.0);
+  }
+  double wangle[ORC_NANGLE_SED + 1];
+  for (int i = 1; i <= ORC_NANGLE_SED; ++i)
+    wangle[i] = 1.0 / ((double)i / (double)ORC_NANGLE_SED - (double)(i - 1) / (double)ORC_NANGLE_SED);
+
+  rng_t R;
+  memset(&R, 0, sizeof R);
+  R.rng = run->rng;
+  R.idum = run->idum;
+  const int64_t Nphot = run->nphot;
+  const double Epkt = m->Lstar / ((double)Nphot * 1.0);
+  int status = 0;
+
+  for (int64_t ip = 0; ip < Nphot; ++ip) {
+    if (R.rng == 0) px_init(&R.px, run->seed, (uint64_t)ip);
+    orc_phot p;
+    memset(&p, 0, sizeof p);
+    int done = 0;
+    while (!done) {
+      /* (re-)emission from the star, MCRadiation.f:350-382 */
+      S.nEJv = 0.0;
+      int64_t ninteract = 0;
+      (void)rnd(&R); /* where_emit */
+      double x, y, z;
+      randomdirection(&R, &x, &y, &z);
+      p.x = m->R[0] * x;
+      p.y = m->R[0] * y;
+      p.z = m->R[0] * z;
+      emit_scan(&S, &R, &p, m->Fstar, m->Lstar);
+      p.E = Epkt;
+      randomdirection(&R, &p.vx, &p.vy, &p.vz);
+      if ((p.x * p.vx + p.y * p.vy) + p.z * p.vz < 0.0) {
+        p.vx = -p.vx;
+        p.vy = -p.vy;
+        p.vz = -p.vz;
+      }
+      p.edgeNr = 1;
+      p.onEdge = 1;
+      double ct = fabs(p.z) / m->R[0];
+      p.i = 0;
+      p.j = -1;
+      for (int j = 1; j <= nt - 1; ++j)
+        if (ct < m->Theta[j - 1] && ct > m->Theta[j]) p.j = j;
+      if (p.j < 0) {
+        for (int j = 1; j <= nt - 1; ++j)
+          if (ct >= m->Theta[j]) {
+            p.j = j;
+            break;
+          }
+        if (p.j < 0) p.j = nt - 1;
+      }
+      if (S.scattering) {
+        p.pol = 0;
+        p.scatt = 0;
+        p.Q = p.U = p.V = 0.0;
+        set_s_from_v(&p);
+      }
+      double tau = -dm_log(rnd(&R));
+      for (;;) {
+        int st = trace2d(&S, &R, &p, tau, ip);
+        if (st < 0) {
+          status = 1;
+          out->counters[11]++;
+          done = 1;
+          break;
+        }
+        if (st == 2) {
+          out->counters[5]++;
+          break; /* re-launch this packet from the star */
+        }
+        if (st == 1) {
+          /* escape: SED bin, MCRadiation.f:576-646 (non-multiwav branch) */
+          out->counters[9]++;
+          double av = p.vz > 0.0 ? p.vz : -p.vz;
+          int ia = (int)(av * (double)ORC_NANGLE_SED + 1.0);
+          if (ia > ORC_NANGLE_SED) ia = ORC_NANGLE_SED;
+          int il = (p.wl1 > p.wl2) ? p.ilam1 : p.ilam2;
+          size_t k = (size_t)il * (ORC_NANGLE_SED + 1) + ia;
+          double add = ((wangle[ia] * p.E) * wlam[il]) / 1.0;
+          out->spec[k] += add;
+          out->ispec[k] += 1;
+          if (p.scatt) out->scatspec[k] += add;
+          done = 1;
+          break;
+        }
+        ninteract++;
+        interact(&S, &R, &p);
+        if (run->maxinteract > 0) {
+          if (rnd(&R) < 1.0 / (double)run->maxinteract) {
+            out->counters[7]++;
+            done = 1;
+            break;
+          }
+          p.E = (p.E * (double)run->maxinteract) / (double)(run->maxinteract - 1);
+        }
+        tau = -dm_log(rnd(&R));
+      }
+    }
+  }
+  for (int c = 0; c < ncell; ++c) out->T[c] = S.Tcell[c];
+  free(wlam);
+  free(dens);
+  free(S.mass);
+  free(S.Tcell);
+  free(S.lastphot);
+  return status;
+}

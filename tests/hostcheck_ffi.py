@@ -1,0 +1,91 @@
+"""ctypes bindings of tests/native/libhostcheck.so: the device cores built
+for the host (test infrastructure only)."""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from oracle_ffi import P, dp
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SRC = os.path.join(HERE, "native", "hostcheck.cpp")
+LIB = os.path.join(HERE, "native", "libhostcheck.so")
+DEPS = [SRC] + [os.path.join(HERE, "..", "mcmax_b200", "csrc", f) for f in
+                ("dhs_core.cuh", "transport_core.cuh", "detmath.h", "cplx.h", "philox.h")]
+
+
+class HcModel(C.Structure):
+    _fields_ = [("nr", C.c_int), ("nt", C.c_int), ("nlam", C.c_int), ("ncomp", C.c_int), ("scat_how", C.c_int),
+                ("uniform_mix", C.c_int), ("rw", C.c_int), ("factRW", C.c_double), ("Lstar", C.c_double),
+                ("nphot", C.c_int64), ("maxinteract", C.c_int64), ("seed", C.c_uint64)] + \
+               [(n, dp) for n in ("R", "Theta", "SinTheta", "dens", "V", "nu", "BB", "Fstar", "KabsTot", "KscaTot",
+                                  "KpCell", "comp_w", "Ksca_c", "F_c", "IF_c", "sinthet", "cos2phi", "sin2phi",
+                                  "KDext", "KDabs", "rw_y", "rw_phi")] + [("thick", C.POINTER(C.c_uint8))]
+
+
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(d) for d in DEPS):
+            subprocess.run(["g++", "-O2", "-fPIC", "-shared", "-std=c++17", "-ffp-contract=off", "-fno-fast-math",
+                            "-o", LIB, SRC], check=True)
+        _lib = C.CDLL(LIB)
+    return _lib
+
+
+def dhs_sample(rcore, rshell, wvno, mre, mim, mu):
+    L = load()
+    F = np.zeros(720)
+    ce, cs = C.c_double(), C.c_double()
+    mu = np.ascontiguousarray(mu, float)
+    e = L.hc_dhs_sample(C.c_double(rcore), C.c_double(rshell), C.c_double(wvno), C.c_double(mre), C.c_double(mim),
+                        P(mu), P(F), C.byref(ce), C.byref(cs))
+    return e, ce.value, cs.value, F.reshape(4, 180)
+
+
+def mie_sample(rad, lam, e1, e2):
+    L = load()
+    F = np.zeros(720)
+    cs, ce = C.c_double(), C.c_double()
+    e = L.hc_mie_sample(C.c_double(rad), C.c_double(lam), C.c_double(e1), C.c_double(e2), P(F), C.byref(cs),
+                        C.byref(ce))
+    return e, cs.value, ce.value, F.reshape(4, 180)
+
+
+def mcradiation(model, tables, nphot, seed=1, randomwalk=False, factRW=10.0, maxinteract=0):
+    L = load()
+    m, t = model, tables
+    keep = {}
+
+    def A(name, a, dt=np.float64):
+        if a is None:
+            return None
+        keep[name] = np.ascontiguousarray(a, dt)
+        return P(keep[name])
+
+    uniform = int(all(np.array_equal(m.comp_w[0], m.comp_w[c]) for c in range(m.ncell)))
+    h = HcModel(m.nr, m.nt, m.nlam, m.ncomp, int(m.scat_how), uniform, int(bool(randomwalk)), float(factRW),
+                float(m.Lstar), int(nphot), int(maxinteract), int(seed),
+                A("R", m.R), A("Theta", m.Theta), A("SinTheta", m.SinTheta), A("dens", m.dens), A("V", m.V),
+                A("nu", m.nu), A("BB", m.BB), A("Fstar", m.Fstar), A("KabsTot", t["KabsTot"]),
+                A("KscaTot", t["KscaTot"]), A("KpCell", t["KpCell"]), A("comp_w", m.comp_w), A("Ksca", m.Ksca),
+                A("F", m.F), A("IF", t["IF"]), A("sinthet", t["sinthet"]), A("cos2phi", t["cos2phi"]),
+                A("sin2phi", t["sin2phi"]), A("KDext", t["KDext"]), A("KDabs", t["KDabs"]), A("rw_y", t["rw_y"]),
+                A("rw_phi", t["rw_phi"]), A("thick", t["thick"], np.uint8))
+    nc = m.ncell
+    ns = m.nlam * 31
+    out = dict(EJv=np.zeros(nc), EJv2=np.zeros(nc), Eabs=np.zeros(nc), T=np.zeros(nc), Ni=np.zeros(nc, np.int32),
+               spec=np.zeros(ns), scatspec=np.zeros(ns), ispec=np.zeros(ns, np.int32))
+    cnt = (C.c_ulonglong * 16)()
+    tau = C.c_double(0.0)
+    L.hc_mcradiation(C.byref(h), *[P(out[k]) for k in ("EJv", "EJv2", "Eabs", "T", "Ni", "spec", "scatspec", "ispec")],
+                     cnt, C.byref(tau))
+    out["counters"] = np.array(cnt[:], np.int64)
+    out["tautot"] = tau.value
+    for k in ("spec", "scatspec", "ispec"):
+        out[k] = out[k].reshape(m.nlam, 31)
+    return out

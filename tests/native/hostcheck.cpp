@@ -1,0 +1,130 @@
+// Host build of the device cores (dhs_core.cuh, transport_core.cuh) for the
+// CPU tests: the same source the GPU kernels run, executed by one host
+// thread, so it can be compared bit for bit with the checker without a GPU.
+// Test infrastructure only.
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "../../mcmax_b200/csrc/dhs_core.cuh"
+#include "../../mcmax_b200/csrc/transport_core.cuh"
+
+extern "C" {
+
+int hc_dhs_sample(double rcore, double rshell, double wvno, double mre, double mim, const double *mu, double *F,
+                  double *ce, double *cs) {
+  int n1 = dhs_nmx1(rshell, wvno, mre, -mim);
+  if (n1 > 300000) n1 = 300000;
+  std::vector<cx> scratch(4 * (size_t)(n1 + 2));
+  return dhs_sample<1, 90>(rcore, rshell, wvno, mre, -mim, mu, scratch.data(), n1 + 2, 0, F, F + 180, F + 360,
+                           F + 540, ce, cs);
+}
+
+int hc_mie_sample(double rad, double lam, double e1, double e2, double *F, double *cs, double *ce) {
+  int nmax, nfi, nD;
+  mie_counts(rad, lam, e1, e2, &nmax, &nfi, &nD);
+  int cap = (nfi > nD ? nfi : nD) + 2;
+  std::vector<double> scratch(8 * (size_t)cap);
+  return mie_sample<1, 90>(rad, lam, e1, e2, scratch.data(), cap, 0, F, F + 180, F + 360, F + 540, cs, ce);
+}
+
+struct HcModel {
+  int nr, nt, nlam, ncomp, scat_how, uniform_mix, rw;
+  double factRW, Lstar;
+  int64_t nphot, maxinteract;
+  uint64_t seed;
+  const double *R, *Theta, *SinTheta, *dens, *V, *nu, *BB, *Fstar;
+  const double *KabsTot, *KscaTot, *KpCell, *comp_w, *Ksca_c, *F_c, *IF_c;
+  const double *sinthet, *cos2phi, *sin2phi, *KDext, *KDabs, *rw_y, *rw_phi;
+  const unsigned char *thick;
+};
+
+// serial run of the device packet loop on the host; outputs as the oracle's
+int hc_mcradiation(const HcModel *h, double *EJv, double *EJv2, double *Eabs, double *T, int *Ni, double *spec,
+                   double *scatspec, int *ispec, unsigned long long *counters, double *tautot) {
+  const int nc = h->nt - 1, ncell = h->nr * nc, nlam = h->nlam;
+  std::vector<double> dens(ncell), mass(ncell), dnu_half(nlam - 1), star_cdf(nlam - 1), wlam(nlam);
+  for (int c = 0; c < ncell; ++c) {
+    mass[c] = h->dens[c] * h->V[c];
+    dens[c] = h->dens[c] <= 1e-50 ? 1e-50 : h->dens[c];
+  }
+  for (int i = 0; i < nlam - 1; ++i) dnu_half[i] = std::fabs(h->nu[i] - h->nu[i + 1]) * 0.5;
+  double Lt = 0.0;
+  for (int i = 0; i < nlam - 1; ++i) {
+    Lt = Lt + dnu_half[i] * (h->Fstar[i] + h->Fstar[i + 1]);
+    star_cdf[i] = Lt;
+  }
+  for (int i = 0; i < nlam; ++i) {
+    if (i == 0)
+      wlam[i] = -1e23 / (h->nu[1] / 2.0);
+    else if (i == nlam - 1)
+      wlam[i] = -1e23 / ((h->nu[nlam - 1] - h->nu[nlam - 2]) / 2.0);
+    else
+      wlam[i] = -1e23 / ((h->nu[i + 1] - h->nu[i - 1]) / 2.0);
+  }
+  std::vector<double> emit_cdf;
+  if (h->uniform_mix) {
+    emit_cdf.resize((size_t)TP_TMAX * (nlam - 1));
+    for (int iT = 0; iT < TP_TMAX; ++iT) {
+      double L = 0.0, s0 = (h->BB[iT + 1] - h->BB[iT]) * h->KabsTot[0];
+      for (int i = 0; i < nlam - 1; ++i) {
+        const double *B = h->BB + (size_t)(i + 1) * TP_TT;
+        double s1 = (B[iT + 1] - B[iT]) * h->KabsTot[i + 1];
+        L = L + dnu_half[i] * (s0 + s1);
+        emit_cdf[(size_t)iT * (nlam - 1) + i] = L;
+        s0 = s1;
+      }
+    }
+  }
+  std::vector<int> kd_index(ncell, -1);
+  for (int c = 0; c < ncell; ++c)
+    if (h->thick && h->thick[c]) kd_index[c] = c;
+  TModel m;
+  memset(&m, 0, sizeof m);
+  m.nr = h->nr; m.nt = h->nt; m.nc = nc; m.ncell = ncell; m.nlam = nlam; m.ncomp = h->ncomp;
+  m.scat_how = h->scat_how;
+  m.scattering = 0;
+  if (h->scat_how != 0)
+    for (size_t k = 0; k < (size_t)ncell * nlam; ++k)
+      if (h->KscaTot[k] != 0.0) { m.scattering = 1; break; }
+  m.uniform_mix = h->uniform_mix;
+  m.rw = h->rw;
+  m.factRW = h->factRW;
+  m.R0 = h->R[0];
+  m.Lstar = h->Lstar;
+  m.Epkt = h->Lstar / ((double)h->nphot * 1.0);
+  m.nphot = h->nphot;
+  m.maxinteract = h->maxinteract;
+  m.pid0 = 0;
+  m.nruns_d = 1.0;
+  m.seed = h->seed;
+  m.R = h->R; m.Theta = h->Theta; m.SinTheta = h->SinTheta; m.dens = dens.data(); m.mass = mass.data();
+  m.nu = h->nu; m.dnu_half = dnu_half.data(); m.BB = h->BB; m.star_cdf = star_cdf.data(); m.wlam = wlam.data();
+  m.KabsTot = h->KabsTot; m.KscaTot = h->KscaTot; m.KpCell = h->KpCell;
+  m.emit_cdf = h->uniform_mix ? emit_cdf.data() : nullptr;
+  m.comp_w = h->comp_w; m.Ksca_c = h->Ksca_c; m.F_c = h->F_c; m.IF_c = h->IF_c;
+  m.sinthet = h->sinthet; m.cos2phi = h->cos2phi; m.sin2phi = h->sin2phi;
+  m.KDext = h->KDext; m.KDabs = h->KDabs; m.rw_y = h->rw_y; m.rw_phi = h->rw_phi;
+  m.kd_index = kd_index.data();
+  m.thick = h->thick;
+  std::vector<unsigned char> nothick;
+  if (!m.thick) {
+    nothick.assign(ncell, 0);
+    m.thick = nothick.data();
+  }
+  std::vector<int> lastphot(ncell, 0);
+  unsigned long long next = 0;
+  TAcc A;
+  A.EJv = EJv; A.EJv2 = EJv2; A.Eabs = Eabs; A.T = T; A.Ni = Ni; A.lastphot = lastphot.data();
+  A.spec = spec; A.scatspec = scatspec; A.ispec = ispec; A.counters = counters; A.tautot = tautot; A.next = &next;
+  TLocal L;
+  memset(&L, 0, sizeof L);
+  // with uniform_mix the KpCell table has a single row
+  if (h->uniform_mix) m.KpCell = h->KpCell;
+  for (int64_t pid = 0; pid < h->nphot; ++pid) tp_run_packet(m, A, pid, L);
+  for (int k = 0; k < TC_N; ++k) counters[k] += L.cnt[k];
+  *tautot += L.tautot;
+  return 0;
+}
+}
