@@ -1,0 +1,326 @@
+"""Packets/s of the MCMax photon-packet loop on B200 (configs[1] workload).
+
+Workload (configs[1], "precision" deck): star Teff = 10000 K, R* = 2.5 Rsun;
+ZONES disk Rin = 0.5 AU, Rout = 100 AU, Sigma ~ r^-1, Mdust = 1e-3 Msun,
+H/R = 0.05 at 1 AU (MCMax scale height sh = 0.05*sqrt(2)), flaring 1.125;
+grid nr = 200 x ntheta = 120 (+ the star cell), nlam = 200 from 0.1 to 3000
+micron; one synthetic .lnk composition, MRN 0.1-1 micron in 20 bins (5 sizes,
+20 DHS filling fractions each, fmax = 0.8, blend with porosity 0.25), full
+Mueller scattering, Bjorkman-Wood re-emission, modified random walk
+(factRW = 10).  Opacities come from the library's own DHS kernels.
+
+One step = one MCRadiation call over `--nphot` packets (default 1e7; the deck's
+1e8 packets are ten steps).  `value` is device time of the transport kernel
+with all tables resident in HBM; `e2e` times the reference-facing C-ABI
+(mcg_set_model from host buffers + mcg_mcradiation + result copies to host).
+
+--impl reference runs the CPU restatement of the reference's loop (the
+checker; the Fortran reference cannot be compiled here) on all host cores.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NPHOT_DEFAULT = 10_000_000
+WORKLOAD = dict(mdust=1e-3, nrad=200, ntheta=120, nlam=200, lam1=0.1, lam2=3000.0, ngrains=20, ns=5, nf=20,
+                fmax=0.8, blend=True, porosity=0.25, scat_how=2)
+RUN = dict(randomwalk=True, factRW=10.0)
+METRIC = "packets/s (MCRadiation packet loop, 1 B200)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nphot", type=int, default=NPHOT_DEFAULT)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        load = [s for s in sm if smax and s > 0.5 * smax] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def algorithmic_bytes(counters, nlam):
+    """Per-event byte model of the packet loop (the reads and read-modify-
+    writes an event needs at minimum): crossing 72 B + 16 B EJv2 on exit,
+    absorption 64 B + nlam*24 B re-emission row, scattering 2*180*8 + 48 B,
+    random-walk step 56 B, escape 16 B."""
+    cross, absorb, scat, rw, esc = (int(counters[k]) for k in (8, 2, 3, 4, 9))
+    return cross * (72 + 16) + absorb * (64 + 24 * nlam) + scat * (2 * 180 * 8 + 48) + rw * 56 + esc * 16
+
+
+def cpu_baseline_sample(model, seconds, cores):
+    """Time the CPU restatement (oracle) on a bounded sample of the same
+    workload: serial, packets until ~`seconds` of work."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_ffi as O
+    tab = O.transport_tables(model, randomwalk=RUN["randomwalk"], factRW=RUN["factRW"], lazy_kd=True)
+    n = 20
+    total_n, total_t = 0, 0.0
+    while total_t < seconds and total_n < 200000:
+        t0 = time.perf_counter()
+        O.mcradiation(model, n, seed=1000 + total_n, randomwalk=RUN["randomwalk"], factRW=RUN["factRW"], tables=tab)
+        dt = time.perf_counter() - t0
+        total_n += n
+        total_t += dt
+        n = min(4 * n, max(20, int(n * (seconds - total_t) / max(dt, 1e-3))))
+        if n <= 0:
+            break
+    return total_n / total_t, total_n, total_t
+
+
+def build_model(ctx):
+    from mcmax_b200 import model as M
+    return M.disk_model(ctx, **WORKLOAD)
+
+
+def run_reference(args, rank, world):
+    """CPU restatement on all host cores: independent packet batches per
+    process (multiprocessing, spawn), reported like our arm."""
+    import multiprocessing as mp
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    model = _cpu_model()
+    per = max(1, int(os.environ.get("MCMAX_REF_PACKETS", "200")))
+    ctxmp = mp.get_context("spawn")
+    step_times = []
+    with ctxmp.Pool(cores, initializer=_ref_init) as pool:
+        for it in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            pool.map(_ref_work, [(s + 1000 * it, per) for s in range(cores)])
+            dt = time.perf_counter() - t0
+            if it >= args.warmup:
+                step_times.append(dt)
+    total = per * cores
+    value = total / statistics.mean(step_times)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "packets/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(step_times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "configs[1]-deck precision disk (CPU restatement, packets per step %d)" % total,
+                       "nr": 200, "ntheta": 120, "nlam": 200, "packets_per_step": total},
+            "cpu_baseline": {"value": value, "unit": "packets/s", "cores": cores, "kind": "port",
+                             "sample": "%d packets per step on %d processes" % (total, cores)},
+            "e2e": {"value": value, "unit": "packets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+_REF = {}
+
+
+def _cpu_model():
+    """configs[1] model with opacities from the CPU checker."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import models
+    return models.small_disk(nrad=WORKLOAD["nrad"], ntheta=WORKLOAD["ntheta"], nlam=WORKLOAD["nlam"],
+                             ngrains=WORKLOAD["ngrains"], ns=WORKLOAD["ns"], nf=WORKLOAD["nf"],
+                             mdust=WORKLOAD["mdust"], scat_how=2)
+
+
+def _ref_init():
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_ffi as O
+    m = _cpu_model()
+    _REF["m"] = m
+    _REF["tab"] = O.transport_tables(m, randomwalk=True, factRW=RUN["factRW"], lazy_kd=True)
+
+
+def _ref_work(a):
+    import oracle_ffi as O
+    seed, n = a
+    O.mcradiation(_REF["m"], n, seed=seed, randomwalk=True, factRW=RUN["factRW"], tables=_REF["tab"])
+    return n
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    import numpy as np
+    from mcmax_b200 import api
+
+    ctx = api.Context(local)
+    model = build_model(ctx)
+    ctx.set_model(model)
+    # warm-up steps (also builds the random-walk tables once)
+    for w in range(args.warmup):
+        ctx.mcradiation(args.nphot, seed=10_000 * (rank + 1) + w, precision=args.precision, fetch=False, **RUN)
+    sync = _barrier(dist)
+    clocks = ClockSampler(local)
+    clocks.start()
+    dev_ms = []
+    counters = np.zeros(16, np.int64)
+    t0 = time.perf_counter()
+    for s in range(args.steps):
+        _, out = ctx.mcradiation(args.nphot, seed=rank * 1_000_003 + s + 1, precision=args.precision, fetch=False,
+                                 **RUN)
+        dev_ms.append(out["device_ms"])
+        counters += out["counters"]
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    t_dev = sum(dev_ms) / 1e3
+    t_max = _max_over_ranks(dist, t_dev)
+    packets = args.nphot * args.steps * world
+    value = packets / t_max
+    # end to end through the C-ABI with host buffers
+    import ctypes
+    h2d = sum(np.asarray(getattr(model, k)).nbytes for k in ("R", "Theta", "SinTheta", "dens", "V", "comp_w", "lam",
+                                                               "nu", "Kabs", "Ksca", "F", "BB", "Fstar"))
+    nc = model.ncell
+    d2h = nc * (8 * 4 + 4) + model.nlam * 31 * (8 * 2 + 4)
+    e2e_steps = max(1, min(args.steps, 2))
+    _barrier(dist)
+    t1 = time.perf_counter()
+    for s in range(e2e_steps):
+        ctx.set_model(model)
+        ctx.mcradiation(args.nphot, seed=rank * 7_000_001 + s + 1, precision=args.precision, fetch=True, **RUN)
+    e2e_t = _max_over_ranks(dist, time.perf_counter() - t1)
+    e2e_value = args.nphot * e2e_steps * world / e2e_t
+    # roofline of the transport kernel against the measured HBM copy bandwidth
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    algo = algorithmic_bytes(counters, model.nlam) / args.steps
+    per_launch_s = t_dev / args.steps
+    achieved = algo / per_launch_s / 1e9
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cm = _cpu_model()
+            v, n, t = cpu_baseline_sample(cm, args.cpu_sample_seconds, 1)
+            cpu = {"value": v, "unit": "packets/s", "cores": 1, "kind": "port",
+                   "sample": "%d packets of the same deck, serial CPU restatement, %.1f s" % (n, t)}
+        except Exception as e:  # the baseline must not sink the GPU line
+            cpu = {"value": None, "unit": "packets/s", "cores": 1, "kind": "port", "sample": "failed: %s" % e}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "packets/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "data": "synthetic",
+            "config": {"workload": "configs[1] precision disk: Mdust 1e-3 Msun, nr 200 x ntheta 120, nlam 200, "
+                                   "random walk, full Mueller scattering, %s transport" % args.precision,
+                       "packets_per_step": args.nphot, "precision": args.precision,
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "model tables exceed L2 (126 MB): per-cell opacity rows, emission CDF, "
+                             "random-walk tables"},
+            "e2e": {"value": e2e_value, "unit": "packets/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(args.steps),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "note": "algorithmic bytes from the event counters (crossings, absorptions, scatterings, "
+                                 "random-walk steps) per launch / transport-kernel time; peak = measured HBM copy"},
+            "events_per_step": {"crossings": int(counters[8] // args.steps), "absorptions": int(counters[2] // args.steps),
+                                "scatterings": int(counters[3] // args.steps), "rw_steps": int(counters[4] // args.steps)},
+            "wall_s": wall, "clocks": clk, "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def _barrier(dist):
+    if dist:
+        import torch
+        torch.cuda.synchronize()
+        dist.barrier()
+    return True
+
+
+def _max_over_ranks(dist, v):
+    if not dist:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+if __name__ == "__main__":
+    main()

@@ -155,14 +155,24 @@ double mcg_planck(double T, double lam);
  * random-walk diffusion tables).  Replaces the previous model. */
 mcg_status mcg_set_model(mcg_ctx *ctx, const mcg_grid *grid, const mcg_opacity *opac);
 
-typedef enum { MCG_PREC_FP64 = 0, MCG_PREC_MIXED = 1 } mcg_precision;
+/* Transport forms.  EXACT keeps the reference's evaluation order (linear
+ * scans, detmath.h transcendentals): with threads = 1 it reproduces the
+ * serial reference loop bit for bit.  FP64 and MIXED are the GPU-ordered
+ * kernels (cumulative tables + binary search, shared-memory tables); MIXED
+ * runs direction, Stokes, opacity and scattering-table arithmetic in FP32
+ * and keeps positions, intersection quadratics, energies, accumulators and
+ * the temperature inversion in FP64. */
+typedef enum { MCG_PREC_FP64 = 0, MCG_PREC_MIXED = 1, MCG_PREC_EXACT = 2 } mcg_precision;
 
 typedef struct {
   uint64_t seed;          /* Philox key: packet p draws stream (seed, p) */
   int randomwalk;         /* RNDW keyword 'randomwalk' */
   double factRW;          /* keyword 'factrw' (Init.f:205, default 10) */
   int64_t maxinteract;    /* > 0: overflow roulette (MCRadiation.f:568-571) */
-  int nruns;              /* keyword 'nruns' (MCRadiation.f:269), >= 1 */
+  int nruns;              /* keyword 'nruns' (MCRadiation.f:269), >= 1: the
+                             independent sub-runs execute concurrently in one
+                             launch, each with its own accumulators, and are
+                             averaged as the reference does */
   int precision;          /* mcg_precision */
   int threads;            /* 0: persistent grid; n > 0: exactly n threads
                              (1 reproduces the serial packet order) */
@@ -183,6 +193,9 @@ typedef struct {
   int64_t counters[MCG_NCOUNTERS];
   double tautot;
   float device_ms;        /* transport kernel time of the call */
+  float progress_ms[5];   /* time at which 50, 90, 99, 99.9, 100 % of the
+                             packets had finished (the rest is the tail of
+                             the heaviest packets) */
 } mcg_result;
 
 /* The packet loop (MCRadiation.f:6-887).  *nphot_inout = NphotTot. */

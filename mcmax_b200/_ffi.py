@@ -17,7 +17,7 @@ NCOUNTERS = 16
 
 MCG_OK, MCG_ERR_ARG, MCG_ERR_CUDA, MCG_ERR_STATE, MCG_ERR_NOMEM, MCG_ERR_LIMIT, MCG_ERR_RUN = range(7)
 STATUS_NAMES = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_STATE", 4: "ERR_NOMEM", 5: "ERR_LIMIT", 6: "ERR_RUN"}
-PREC_FP64, PREC_MIXED = 0, 1
+PREC_FP64, PREC_MIXED, PREC_EXACT = 0, 1, 2
 
 dp = C.POINTER(C.c_double)
 ip = C.POINTER(C.c_int32)
@@ -69,6 +69,7 @@ class Result(C.Structure):
         ("EJv", dp), ("EJv2", dp), ("Eabs", dp), ("T", dp), ("Ni", ip),
         ("spec", dp), ("scatspec", dp), ("ispec", ip),
         ("counters", C.c_int64 * NCOUNTERS), ("tautot", C.c_double), ("device_ms", C.c_float),
+        ("progress_ms", C.c_float * 5),
     ]
 
 

@@ -115,10 +115,10 @@ class Context:
         self.model = m
 
     def mcradiation(self, nphot, seed=1, randomwalk=False, factRW=10.0, maxinteract=0, nruns=1,
-                    precision="fp64", threads=0, block=0, fetch=True):
+                    precision="exact", threads=0, block=0, fetch=True):
         """Run the packet loop; returns (nphot_out, result dict)."""
         m = self.model
-        prec = {"fp64": _ffi.PREC_FP64, "mixed": _ffi.PREC_MIXED}[precision]
+        prec = {"fp64": _ffi.PREC_FP64, "mixed": _ffi.PREC_MIXED, "exact": _ffi.PREC_EXACT}[precision]
         run = _ffi.Run(int(seed), int(bool(randomwalk)), float(factRW), int(maxinteract), int(nruns), prec,
                        int(threads), int(block))
         out = {}
@@ -136,6 +136,7 @@ class Context:
         out["counters"] = np.array(res.counters[:], dtype=np.int64)
         out["tautot"] = res.tautot
         out["device_ms"] = res.device_ms
+        out["progress_ms"] = list(res.progress_ms)
         if fetch:
             for k in ("spec", "scatspec", "ispec"):
                 out[k] = out[k].reshape(m.nlam, _ffi.NANGLE_SED + 1)

@@ -22,8 +22,10 @@ UNITS = {
     "part_kernels.cu": ["--fmad=false"],
     "transport.cu": ["--fmad=false"],
     "host_tables.cu": ["--fmad=false"],
+    "transport_fast.cu": [],
 }
-HEADERS = ["detmath.h", "cplx.h", "philox.h", "dhs_core.cuh", "transport_core.cuh", "mcg_internal.h"]
+HEADERS = ["detmath.h", "cplx.h", "philox.h", "dhs_core.cuh", "transport_core.cuh", "transport_fast.cuh",
+           "mcg_internal.h"]
 
 
 def _nvcc():

@@ -62,12 +62,31 @@ struct DevModel {
   double *sinthet = nullptr; /* 180 */
   double *cos2phi = nullptr, *sin2phi = nullptr; /* 361 */
   float *sinthetF = nullptr, *cos2phiF = nullptr, *sin2phiF = nullptr;
+  /* tables of the GPU-ordered kernels (built on first use), per precision
+   * index 0 = fp64, 1 = mixed */
+  struct Fast {
+    bool built = false;
+    void *KabsRow = nullptr, *KextRow = nullptr, *Ksca_c = nullptr; /* R */
+    void *KabsTotR = nullptr, *KextTotR = nullptr;                 /* R, non-uniform */
+    void *scatA = nullptr, *scatB = nullptr, *F6 = nullptr;       /* R */
+    unsigned char *scatG = nullptr;
+  } fast[2];
+  double *Ccum = nullptr;   /* uniform: TT*(nlam-1) cumulative of BB(iT)*K */
+  unsigned short *emitG = nullptr; /* uniform: TMAX*32 guide table of emit_cdf rows */
+  double *c2cum = nullptr, *s2cum = nullptr, *rw_logy = nullptr;
+  double *KextTot = nullptr;  /* ncell*nlam, fp64 fast path, non-uniform */
   std::vector<void *> owned;
 };
 
 /* Accumulators of a run on the device. */
 struct DevRun {
-  int ncell = 0, nlam = 0;
+  int ncell = 0, nlam = 0, nruns = 0;
+  /* per-run blocks (nruns*ncell) below; the combined results of the last
+   * call are EJvTot/EJv2Tot (run averages), NiTot (sum), and the last run's
+   * Eabs/T block */
+  int *NiTot = nullptr;
+  unsigned long long *done = nullptr, *tmark = nullptr;
+  float progress_ms[5] = {0, 0, 0, 0, 0};
   double *EJv = nullptr, *EJv2 = nullptr, *Eabs = nullptr, *T = nullptr;
   int *Ni = nullptr, *lastphot = nullptr;
   double *spec = nullptr, *scatspec = nullptr;
@@ -77,6 +96,7 @@ struct DevRun {
   unsigned long long *next_packet = nullptr;
   /* nruns accumulation */
   double *EJvTot = nullptr, *EJv2Tot = nullptr;
+  int *kp_hint = nullptr;
   std::vector<void *> owned;
 };
 
@@ -108,6 +128,8 @@ mcg_status mcg_part_batch_impl(mcg_ctx *ctx, int nparts, const mcg_part_in *in, 
 mcg_status mcg_set_model_impl(mcg_ctx *ctx, const mcg_grid *grid, const mcg_opacity *opac);
 mcg_status mcg_mcradiation_impl(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot, mcg_result *res);
 mcg_status mcg_finalize_impl(mcg_ctx *ctx, double *T, double *dT, double *dEJv);
+mcg_status mcg_fast_run(mcg_ctx *ctx, int precision, const void *tmodel, const void *tacc, int threads,
+                        int block, float *ms);
 void mcg_free_model(DevModel &m);
 void mcg_free_run(DevRun &r);
 

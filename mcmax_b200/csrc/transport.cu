@@ -163,17 +163,22 @@ __global__ void kd_kernel(int nrows, const int *cells, int nlam, const double *d
   KDabs[(size_t)r * stride + (stride == TP_TT ? iT : k)] = int3 / int2;
 }
 
-__global__ void __launch_bounds__(128) transport_fp64_kernel(TModel m, TAcc A) {
+__global__ void __launch_bounds__(128) transport_fp64_kernel(const __grid_constant__ TModel m,
+                                                             const __grid_constant__ TAcc A) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) A.tmark[5] = tp_globaltimer();
   TLocal L;
-  for (int k = 0; k < TC_N; ++k) L.cnt[k] = 0ULL;
+#pragma unroll
+  for (int k = 0; k < TC_N; ++k) L.cnt[k] = 0u;
   L.tautot = 0.0;
   for (;;) {
     unsigned long long pid = atomicAdd(A.next, 1ULL);
     if (pid >= (unsigned long long)m.nphot) break;
     tp_run_packet(m, A, (int64_t)pid + m.pid0, L);
+    tp_packet_done(A);
   }
+#pragma unroll
   for (int k = 0; k < TC_N; ++k)
-    if (L.cnt[k]) atomicAdd(&A.counters[k], L.cnt[k]);
+    if (L.cnt[k]) atomicAdd(&A.counters[k], (unsigned long long)L.cnt[k]);
   if (L.tautot != 0.0) atomicAdd(A.tautot, L.tautot);
 }
 
@@ -503,14 +508,15 @@ static mcg_status build_rw_tables(mcg_ctx *ctx, double factRW) {
   return MCG_OK;
 }
 
-static mcg_status ensure_run_buffers(mcg_ctx *ctx) {
+static mcg_status ensure_run_buffers(mcg_ctx *ctx, int nruns) {
   DevModel &m = ctx->model;
   DevRun &r = ctx->run;
-  if (r.ncell == m.ncell && r.nlam == m.nlam && r.EJv) return MCG_OK;
+  if (r.ncell == m.ncell && r.nlam == m.nlam && r.nruns == nruns && r.EJv) return MCG_OK;
   mcg_free_run(r);
   r.ncell = m.ncell;
   r.nlam = m.nlam;
-  const size_t nc = m.ncell, ns = (size_t)m.nlam * (TP_NANG + 1);
+  r.nruns = nruns;
+  const size_t nc = m.ncell, nb = (size_t)m.ncell * nruns, ns = (size_t)m.nlam * (TP_NANG + 1);
   cudaError_t e = cudaSuccess;
   auto A = [&](size_t bytes) {
     void *p = nullptr;
@@ -518,20 +524,24 @@ static mcg_status ensure_run_buffers(mcg_ctx *ctx) {
     if (e == cudaSuccess) r.owned.push_back(p);
     return p;
   };
-  r.EJv = (double *)A(nc * 8);
-  r.EJv2 = (double *)A(nc * 8);
-  r.Eabs = (double *)A(nc * 8);
-  r.T = (double *)A(nc * 8);
-  r.Ni = (int *)A(nc * 4);
-  r.lastphot = (int *)A(nc * 4);
+  r.EJv = (double *)A(nb * 8);
+  r.EJv2 = (double *)A(nb * 8);
+  r.Eabs = (double *)A(nb * 8);
+  r.T = (double *)A(nb * 8);
+  r.Ni = (int *)A(nb * 4);
+  r.lastphot = (int *)A(nb * 4);
+  r.kp_hint = (int *)A(nb * 4);
   r.EJvTot = (double *)A(nc * 8);
   r.EJv2Tot = (double *)A(nc * 8);
+  r.NiTot = (int *)A(nc * 4);
   r.spec = (double *)A(ns * 8);
   r.scatspec = (double *)A(ns * 8);
   r.ispec = (int *)A(ns * 4);
   r.counters = (unsigned long long *)A(MCG_NCOUNTERS * 8);
   r.tautot = (double *)A(8);
   r.next_packet = (unsigned long long *)A(8);
+  r.done = (unsigned long long *)A(8);
+  r.tmark = (unsigned long long *)A(8 * 8);
   if (e != cudaSuccess) {
     mcg_free_run(r);
     return mcg_fail(ctx, MCG_ERR_NOMEM, "run buffers: %s", cudaGetErrorString(e));
@@ -539,11 +549,21 @@ static mcg_status ensure_run_buffers(mcg_ctx *ctx) {
   return MCG_OK;
 }
 
-__global__ static void add_scaled_kernel(int n, const double *a, const double *b, double s, double *ta, double *tb) {
+/* run averages in the reference's order: Tot = sum_r (EJv_r / nruns) */
+__global__ static void combine_runs_kernel(int nc, int nruns, const double *EJv, const double *EJv2, const int *Ni,
+                                           double *EJvTot, double *EJv2Tot, int *NiTot) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= n) return;
-  ta[c] = ta[c] + a[c] / s;
-  tb[c] = tb[c] + b[c] / s;
+  if (c >= nc) return;
+  double a = 0.0, b = 0.0;
+  int n = 0;
+  for (int r = 0; r < nruns; ++r) {
+    a = a + EJv[(size_t)r * nc + c] / (double)nruns;
+    b = b + EJv2[(size_t)r * nc + c] / (double)nruns;
+    n += Ni[(size_t)r * nc + c];
+  }
+  EJvTot[c] = a;
+  EJv2Tot[c] = b;
+  NiTot[c] = n;
 }
 
 mcg_status mcg_mcradiation_impl(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot, mcg_result *res) {
@@ -554,24 +574,34 @@ mcg_status mcg_mcradiation_impl(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot
   const int nruns = run->nruns < 1 ? 1 : run->nruns;
   if (run->randomwalk && !(run->factRW > 0.0)) return mcg_fail(ctx, MCG_ERR_ARG, "mcradiation: factRW must be > 0");
   if (run->maxinteract == 1) return mcg_fail(ctx, MCG_ERR_ARG, "mcradiation: maxinteract must be 0 or > 1");
-  if (run->precision != MCG_PREC_FP64 && run->precision != MCG_PREC_MIXED)
+  if (run->precision != MCG_PREC_FP64 && run->precision != MCG_PREC_MIXED && run->precision != MCG_PREC_EXACT)
     return mcg_fail(ctx, MCG_ERR_ARG, "mcradiation: unknown precision %d", run->precision);
   if (run->threads < 0 || run->block < 0) return mcg_fail(ctx, MCG_ERR_ARG, "mcradiation: threads/block must be >= 0");
   mcg_status s;
-  if ((s = ensure_run_buffers(ctx)) != MCG_OK) return s;
+  if ((s = ensure_run_buffers(ctx, nruns)) != MCG_OK) return s;
   if (run->randomwalk && (s = build_rw_tables(ctx, run->factRW)) != MCG_OK) return s;
   DevRun &R = ctx->run;
   cudaStream_t st = ctx->stream;
   const int64_t Nphot = *nphot / nruns;
   if (Nphot < 1) return mcg_fail(ctx, MCG_ERR_ARG, "mcradiation: NphotTot/nruns must be >= 1");
-  const size_t nc = m.ncell, ns = (size_t)m.nlam * (TP_NANG + 1);
+  if (Nphot * nruns > (int64_t)2000000000)
+    return mcg_fail(ctx, MCG_ERR_LIMIT, "mcradiation: at most 2e9 packets per call (packet numbers are int32)");
+  const size_t nc = m.ncell, nb = (size_t)m.ncell * nruns, ns = (size_t)m.nlam * (TP_NANG + 1);
+  MCG_CUDA(ctx, cudaMemsetAsync(R.EJv, 0, nb * 8, st));
+  MCG_CUDA(ctx, cudaMemsetAsync(R.EJv2, 0, nb * 8, st));
+  MCG_CUDA(ctx, cudaMemsetAsync(R.Eabs, 0, nb * 8, st));
+  MCG_CUDA(ctx, cudaMemsetAsync(R.T, 0, nb * 8, st));
+  MCG_CUDA(ctx, cudaMemsetAsync(R.Ni, 0, nb * 4, st));
+  MCG_CUDA(ctx, cudaMemsetAsync(R.lastphot, 0, nb * 4, st));
+  MCG_CUDA(ctx, cudaMemsetAsync(R.kp_hint, 0, nb * 4, st));
   MCG_CUDA(ctx, cudaMemsetAsync(R.spec, 0, ns * 8, st));
   MCG_CUDA(ctx, cudaMemsetAsync(R.scatspec, 0, ns * 8, st));
   MCG_CUDA(ctx, cudaMemsetAsync(R.ispec, 0, ns * 4, st));
   MCG_CUDA(ctx, cudaMemsetAsync(R.counters, 0, MCG_NCOUNTERS * 8, st));
   MCG_CUDA(ctx, cudaMemsetAsync(R.tautot, 0, 8, st));
-  MCG_CUDA(ctx, cudaMemsetAsync(R.EJvTot, 0, nc * 8, st));
-  MCG_CUDA(ctx, cudaMemsetAsync(R.EJv2Tot, 0, nc * 8, st));
+  MCG_CUDA(ctx, cudaMemsetAsync(R.next_packet, 0, 8, st));
+  MCG_CUDA(ctx, cudaMemsetAsync(R.done, 0, 8, st));
+  MCG_CUDA(ctx, cudaMemsetAsync(R.tmark, 0, 8 * 8, st));
 
   TModel tm;
   memset(&tm, 0, sizeof tm);
@@ -581,8 +611,9 @@ mcg_status mcg_mcradiation_impl(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot
   tm.factRW = run->factRW;
   tm.Lstar = m.Lstar;
   tm.Epkt = m.Lstar / ((double)Nphot * 1.0);
-  tm.nphot = Nphot;
+  tm.nphot = Nphot * nruns;
   tm.maxinteract = run->maxinteract;
+  tm.pid0 = 0;
   tm.nruns_d = (double)nruns;
   tm.seed = run->seed;
   tm.R = m.R; tm.Theta = m.Theta; tm.SinTheta = m.SinTheta; tm.dens = m.dens; tm.mass = m.mass;
@@ -598,68 +629,76 @@ mcg_status mcg_mcradiation_impl(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot
     tm.R0 = R0;
   }
   TAcc ta;
+  memset(&ta, 0, sizeof ta);
   ta.EJv = R.EJv; ta.EJv2 = R.EJv2; ta.Eabs = R.Eabs; ta.T = R.T; ta.Ni = R.Ni; ta.lastphot = R.lastphot;
+  ta.kp_hint = R.kp_hint;
   ta.spec = R.spec; ta.scatspec = R.scatspec; ta.ispec = R.ispec; ta.counters = R.counters;
   ta.tautot = R.tautot; ta.next = R.next_packet;
+  ta.run_packets = Nphot;
+  ta.ncell = m.ncell;
+  ta.done = R.done;
+  ta.tmark = R.tmark;
+  {
+    const unsigned long long tot = (unsigned long long)(Nphot * nruns);
+    const double f[5] = {0.5, 0.9, 0.99, 0.999, 1.0};
+    for (int k = 0; k < 5; ++k) {
+      unsigned long long t = (unsigned long long)std::ceil(f[k] * (double)tot);
+      ta.thresh[k] = t < 1ULL ? 1ULL : (t > tot ? tot : t);
+    }
+  }
 
   const int block = run->block > 0 ? run->block : 128;
-  int grid;
-  if (run->threads > 0) {
-    grid = (run->threads + block - 1) / block;
-  } else {
-    int per_sm = 0;
-    MCG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, transport_fp64_kernel, block, 0));
-    if (per_sm < 1) per_sm = 1;
-    grid = ctx->sm_count * per_sm;
-  }
-  if (run->precision == MCG_PREC_MIXED)
-    return mcg_fail(ctx, MCG_ERR_ARG, "mcradiation: the mixed-precision path is not built in this library");
-  float total_ms = 0.0f;
-  for (int irun = 0; irun < nruns; ++irun) {
-    MCG_CUDA(ctx, cudaMemsetAsync(R.EJv, 0, nc * 8, st));
-    MCG_CUDA(ctx, cudaMemsetAsync(R.EJv2, 0, nc * 8, st));
-    MCG_CUDA(ctx, cudaMemsetAsync(R.Eabs, 0, nc * 8, st));
-    MCG_CUDA(ctx, cudaMemsetAsync(R.T, 0, nc * 8, st));
-    MCG_CUDA(ctx, cudaMemsetAsync(R.Ni, 0, nc * 4, st));
-    MCG_CUDA(ctx, cudaMemsetAsync(R.lastphot, 0, nc * 4, st));
-    MCG_CUDA(ctx, cudaMemsetAsync(R.next_packet, 0, 8, st));
-    tm.pid0 = (int64_t)irun * Nphot;
-    MCG_CUDA(ctx, cudaEventRecord(ctx->ev0, st));
-    if (run->threads == 1) {
-      transport_fp64_kernel<<<1, 1, 0, st>>>(tm, ta);
+  float ms = 0.0f;
+  unsigned long long t_host_start = 0;
+  if (run->precision == MCG_PREC_EXACT) {
+    int grid;
+    if (run->threads > 0) {
+      grid = (run->threads + block - 1) / block;
     } else {
-      transport_fp64_kernel<<<grid, block, 0, st>>>(tm, ta);
+      int per_sm = 0;
+      MCG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, transport_fp64_kernel, block, 0));
+      grid = ctx->sm_count * std::max(per_sm, 1);
     }
+    MCG_CUDA(ctx, cudaEventRecord(ctx->ev0, st));
+    if (run->threads == 1)
+      transport_fp64_kernel<<<1, 1, 0, st>>>(tm, ta);
+    else
+      transport_fp64_kernel<<<grid, block, 0, st>>>(tm, ta);
     MCG_CUDA(ctx, cudaGetLastError());
     MCG_CUDA(ctx, cudaEventRecord(ctx->ev1, st));
     MCG_CUDA(ctx, cudaEventSynchronize(ctx->ev1));
-    float ms = 0.0f;
     MCG_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-    total_ms += ms;
-    add_scaled_kernel<<<nblk((long long)nc, 256), 256, 0, st>>>((int)nc, R.EJv, R.EJv2, (double)nruns, R.EJvTot,
-                                                               R.EJv2Tot);
+  } else {
+    mcg_status fs = mcg_fast_run(ctx, run->precision == MCG_PREC_MIXED ? 1 : 0, &tm, &ta, run->threads,
+                                 run->block, &ms);
+    if (fs != MCG_OK) return fs;
   }
-  if (nruns > 1) {
-    MCG_CUDA(ctx, cudaMemcpyAsync(R.EJv, R.EJvTot, nc * 8, cudaMemcpyDeviceToDevice, st));
-    MCG_CUDA(ctx, cudaMemcpyAsync(R.EJv2, R.EJv2Tot, nc * 8, cudaMemcpyDeviceToDevice, st));
-  }
-  res->device_ms = total_ms;
-  unsigned long long cnt[MCG_NCOUNTERS];
+  (void)t_host_start;
+  combine_runs_kernel<<<(int)((nc + 255) / 256), 256, 0, st>>>((int)nc, nruns, R.EJv, R.EJv2, R.Ni, R.EJvTot,
+                                                             R.EJv2Tot, R.NiTot);
+  MCG_CUDA(ctx, cudaGetLastError());
+  res->device_ms = ms;
+  unsigned long long cnt[MCG_NCOUNTERS], tmk[8];
   MCG_CUDA(ctx, cudaMemcpyAsync(cnt, R.counters, sizeof cnt, cudaMemcpyDeviceToHost, st));
+  MCG_CUDA(ctx, cudaMemcpyAsync(tmk, R.tmark, sizeof tmk, cudaMemcpyDeviceToHost, st));
   MCG_CUDA(ctx, cudaMemcpyAsync(&res->tautot, R.tautot, 8, cudaMemcpyDeviceToHost, st));
+  const size_t last = (size_t)(nruns - 1) * nc;
 #define DN(dst, src, n) \
   if (dst) MCG_CUDA(ctx, cudaMemcpyAsync(dst, src, (size_t)(n) * sizeof(*(dst)), cudaMemcpyDeviceToHost, st))
-  DN(res->EJv, R.EJv, nc);
-  DN(res->EJv2, R.EJv2, nc);
-  DN(res->Eabs, R.Eabs, nc);
-  DN(res->T, R.T, nc);
-  DN(res->Ni, R.Ni, nc);
+  DN(res->EJv, R.EJvTot, nc);
+  DN(res->EJv2, R.EJv2Tot, nc);
+  DN(res->Eabs, R.Eabs + last, nc);
+  DN(res->T, R.T + last, nc);
+  DN(res->Ni, R.NiTot, nc);
   DN(res->spec, R.spec, ns);
   DN(res->scatspec, R.scatspec, ns);
   DN(res->ispec, R.ispec, ns);
 #undef DN
   MCG_CUDA(ctx, cudaStreamSynchronize(st));
   for (int k = 0; k < MCG_NCOUNTERS; ++k) res->counters[k] = (int64_t)cnt[k];
+  /* progress marks relative to the kernel start (tmark[5]) */
+  for (int k = 0; k < 5; ++k)
+    res->progress_ms[k] = (tmk[k] && tmk[5] && tmk[k] >= tmk[5]) ? (float)((double)(tmk[k] - tmk[5]) * 1e-6) : -1.0f;
   ctx->have_run = true;
   if (cnt[TC_GEOFAIL] > 0)
     return mcg_fail(ctx, MCG_ERR_RUN, "mcradiation: %llu packets found no cell boundary to hit", cnt[TC_GEOFAIL]);
@@ -678,7 +717,8 @@ mcg_status mcg_finalize_impl(mcg_ctx *ctx, double *T, double *dT, double *dEJv) 
   double x = m.Rstar_cm / (R1 * TP_AU);
   double Tsc = m.Tstar * 0.5 * (1.0 - sqrt(1.0 - x * x));
   if (Tsc < 1.0) Tsc = 1.0;
-  finalize_kernel<<<nblk(nc, 256), 256, 0, ctx->stream>>>(m.nr, m.nc, m.V, R.EJv, R.EJv2, R.Ni, R.T, m.KpCell,
+  finalize_kernel<<<nblk(nc, 256), 256, 0, ctx->stream>>>(m.nr, m.nc, m.V, R.EJvTot, R.EJv2Tot, R.NiTot,
+                                                          R.T + (size_t)(R.nruns - 1) * nc, m.KpCell,
                                                           m.uniform_mix, Tsc, d, d + nc, d + 2 * nc);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess && T) e = cudaMemcpyAsync(T, d, sizeof(double) * nc, cudaMemcpyDeviceToHost, ctx->stream);

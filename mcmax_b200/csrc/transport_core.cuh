@@ -37,9 +37,11 @@
 #include "philox.h"
 
 #if defined(__CUDACC__)
+#define TP_SFN static __host__ __device__ __forceinline__
 #define TP_FN __host__ __device__ __forceinline__
-#define TP_NOINLINE __host__ __device__ __noinline__
+#define TP_NOINLINE static __host__ __device__ __noinline__
 #else
+#define TP_SFN static inline
 #define TP_FN static inline
 #define TP_NOINLINE static
 #endif
@@ -78,14 +80,59 @@ struct TModel {
 
 /* accumulators */
 struct TAcc {
+  /* per-cell arrays hold nruns blocks of ncell entries: the independent
+   * sub-runs of the reference's nruns loop (MCRadiation.f:269-316) run
+   * concurrently, packet p belonging to run p / run_packets */
   double *EJv, *EJv2, *Eabs, *T;
-  int *Ni, *lastphot;
+  int *Ni, *lastphot, *kp_hint;
   double *spec, *scatspec;
   int *ispec;
   unsigned long long *counters;
   double *tautot;
   unsigned long long *next;
+  int64_t run_packets;
+  int ncell;
+  /* progress marks: globaltimer when 50/90/99/99.9/100 % of the packets are
+   * done, [5] = kernel start */
+  unsigned long long *done, *tmark;
+  unsigned long long thresh[5];
 };
+
+/* accumulators of the run that packet pid belongs to */
+TP_FN TAcc tp_run_acc(const TAcc &A, int64_t pid) {
+  TAcc R = A;
+  const size_t off = (size_t)(pid / A.run_packets) * (size_t)A.ncell;
+  R.EJv += off;
+  R.EJv2 += off;
+  R.Eabs += off;
+  R.T += off;
+  R.Ni += off;
+  R.lastphot += off;
+  R.kp_hint += off;
+  return R;
+}
+
+TP_FN unsigned long long tp_globaltimer() {
+#if defined(__CUDA_ARCH__)
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+#else
+  return 0ULL;
+#endif
+}
+
+/* count a finished packet; record the progress marks */
+TP_FN void tp_packet_done(const TAcc &A) {
+#if defined(__CUDA_ARCH__)
+  const unsigned long long d = atomicAdd(A.done, 1ULL) + 1ULL;
+#pragma unroll
+  for (int k = 0; k < 5; ++k)
+    if (d == A.thresh[k]) A.tmark[k] = tp_globaltimer();
+#else
+  (void)A;
+#endif
+}
 
 /* ------------------------------------------------------------- atomics */
 TP_FN double tp_add(double *p, double v) {
@@ -126,7 +173,7 @@ struct TPkt {
 };
 
 struct TLocal {
-  unsigned long long cnt[TC_N];
+  unsigned int cnt[TC_N]; /* per-thread event counts, flushed at exit */
   double tautot;
 };
 
@@ -434,8 +481,10 @@ TP_NOINLINE double tp_determine_t(const double *kp, double E1, double Tcur) {
 TP_FN double tp_tinv(const double *kp, double E1, int lo, int *ibr) {
   *ibr = 0;
   if (!(E1 >= kp[1]) || !(E1 <= kp[TP_TMAX])) return tp_determine_t(kp, E1, 0.0);
-  /* galloping search from lo for the first p in [2, TMAX] with kp[p] >= E1 */
-  int a = lo < 1 ? 1 : lo; /* kp[a] <= E1 not required; only a <= answer-1 */
+  /* galloping search from lo for the first p in [2, TMAX] with kp[p] >= E1;
+   * a hint is used only when kp[lo] < E1 (then lo is below the answer) */
+  if (lo < 1 || lo >= TP_TMAX || !(kp[lo] < E1)) lo = 1;
+  int a = lo;
   int step = 1, b = a + 1;
   while (b < TP_TMAX && kp[b] < E1) {
     a = b;
@@ -459,7 +508,7 @@ TP_FN double tp_tinv(const double *kp, double E1, int lo, int *ibr) {
 }
 
 /* ------------------------------------------------------------- scattering */
-TP_NOINLINE void tp_scatangle(const TModel &m, px_stream *r, TPkt &p, const double *F,
+TP_FN void tp_scatangle(const TModel &m, px_stream *r, TPkt &p, const double *F,
                               const double *IF) {
   const double *F11 = F, *F12 = F + 180, *F22 = F + 360, *F33 = F + 540, *F34 = F + 720,
                *F44 = F + 900;
@@ -530,7 +579,7 @@ TP_NOINLINE void tp_scatangle(const TModel &m, px_stream *r, TPkt &p, const doub
 }
 
 /* ------------------------------------------------------------- interaction */
-TP_NOINLINE void tp_interact(const TModel &m, const TAcc &A, px_stream *r, TPkt &p, TLocal &L) {
+TP_FN void tp_interact(const TModel &m, const TAcc &A, px_stream *r, TPkt &p, TLocal &L) {
   const int c = p.i * m.nc + (p.j - 1);
   const int nlam = m.nlam;
   const double *KabsT = m.KabsTot + (size_t)c * nlam;
@@ -738,7 +787,7 @@ TP_FN void tp_hunt(const double *xx, int n, double x, int *jlo) {
   if (x == xx[0]) *jlo = 1;
 }
 
-TP_NOINLINE int tp_random_walk(const TModel &m, const TAcc &A, px_stream *r, TPkt &p, double dmin,
+TP_FN int tp_random_walk(const TModel &m, const TAcc &A, px_stream *r, TPkt &p, double dmin,
                                TLocal &L) {
   const int c = p.i * m.nc + (p.j - 1);
   int iT = (int)(A.T[c] / 1.0);
@@ -775,7 +824,7 @@ TP_NOINLINE int tp_random_walk(const TModel &m, const TAcc &A, px_stream *r, TPk
 /* ------------------------------------------------------------- trace2d */
 /* returns 0 interaction, 1 escape, 2 star hit / abandoned, -1 geometry
  * failure */
-TP_NOINLINE int tp_trace2d(const TModel &m, const TAcc &A, px_stream *r, TPkt &p, double tau0,
+TP_FN int tp_trace2d(const TModel &m, const TAcc &A, px_stream *r, TPkt &p, double tau0,
                            TLocal &L) {
   const int nlam = m.nlam;
   double tau = 0.0;
@@ -847,7 +896,8 @@ TP_NOINLINE int tp_trace2d(const TModel &m, const TAcc &A, px_stream *r, TPkt &p
 }
 
 /* ------------------------------------------------------------- one packet */
-TP_NOINLINE void tp_run_packet(const TModel &m, const TAcc &A, int64_t pid, TLocal &L) {
+TP_FN void tp_run_packet(const TModel &m, const TAcc &A0, int64_t pid, TLocal &L) {
+  const TAcc A = tp_run_acc(A0, pid);
   px_stream rs;
   px_init(&rs, m.seed, (uint64_t)pid);
   px_stream *r = &rs;

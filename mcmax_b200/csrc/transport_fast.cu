@@ -1,0 +1,303 @@
+/*
+ * transport_fast.cu -- table builders and launches of the GPU-ordered packet
+ * loop (transport_fast.cuh) in its two precision forms:
+ *   fp64  : R = double
+ *   mixed : R = float for direction, Stokes fractions, opacities and the
+ *           scattering tables; FP64 for positions, intersection quadratics,
+ *           energies, accumulators and the temperature inversion.
+ * Per-block shared memory holds the grid edges, the star CDF, the cumulative
+ * cos/sin(2 phi) sums, the opacity rows of a uniform mixture and (when they
+ * fit) the component scattering opacities.
+ */
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "mcg_internal.h"
+#include "transport_fast.cuh"
+
+namespace {
+
+inline int nblk(long long n, int b) { return (int)((n + b - 1) / b); }
+
+/* cumulative of BB(iT)*K over the trapezoid intervals, iT = 0..TMAX */
+__global__ void ccum_kernel(int nlam, const double *dnu_half, const double *BB, const double *K, double *C) {
+  const int iT = blockIdx.x * blockDim.x + threadIdx.x;
+  if (iT > TP_TMAX) return;
+  double L = 0.0, s0 = BB[iT] * K[0];
+  double *row = C + (size_t)iT * (nlam - 1);
+  for (int i = 0; i < nlam - 1; ++i) {
+    double s1 = BB[(size_t)(i + 1) * TP_TT + iT] * K[i + 1];
+    L = L + dnu_half[i] * (s0 + s1);
+    row[i] = L;
+    s0 = s1;
+  }
+}
+
+template <class R>
+__global__ void scat_tables_kernel(int nmat, const double *F, const double *sinthet, R *A, R *B, R *F6) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nmat) return;
+  const double *F11 = F + (size_t)k * 1080, *F12 = F11 + 180;
+  double a = 0.0, b = 0.0;
+  for (int j = 0; j < 180; ++j) {
+    a += (TP_PI * sinthet[j]) * F11[j];
+    b += (TP_PI * sinthet[j]) * F12[j];
+    A[(size_t)k * 180 + j] = (R)a;
+    B[(size_t)k * 180 + j] = (R)b;
+  }
+  for (int e = 0; e < 1080; ++e) F6[(size_t)k * 1080 + e] = (R)F[(size_t)k * 1080 + e];
+}
+
+template <class R>
+__global__ void scat_guide_kernel(int nmat, const R *A, unsigned char *G) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nmat) return;
+  const R *a = A + (size_t)k * 180;
+  const R tot = a[179];
+  int i = 0;
+  for (int g = 0; g < F_NGUIDE; ++g) {
+    const R v = tot * (R)g / (R)F_NGUIDE;
+    while (i < 179 && !(a[i] > v)) ++i;
+    G[(size_t)k * F_NGUIDE + g] = (unsigned char)i;
+  }
+}
+
+__global__ void emit_guide_kernel(int n, const double *D, unsigned short *G) {
+  const int iT = blockIdx.x * blockDim.x + threadIdx.x;
+  if (iT >= TP_TMAX) return;
+  const double *row = D + (size_t)iT * n;
+  const double tot = row[n - 1];
+  int i = 0;
+  for (int g = 0; g < F_NGUIDE; ++g) {
+    const double v = tot * (double)g / (double)F_NGUIDE;
+    while (i < n - 1 && !(row[i] >= v)) ++i;
+    G[(size_t)iT * F_NGUIDE + g] = (unsigned short)i;
+  }
+}
+
+template <class R>
+__global__ void cast_kernel(long long n, const double *a, R *b) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) b[t] = (R)a[t];
+}
+
+template <class R>
+__global__ void sum_cast_kernel(long long n, const double *a, const double *b, R *c) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) c[t] = (R)(a[t] + b[t]);
+}
+
+__global__ void sum_kernel(long long n, const double *a, const double *b, double *c) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) c[t] = a[t] + b[t];
+}
+
+/* shared-memory layout of one block */
+struct SmemPlan {
+  size_t off_R, off_Th, off_ST, off_cdf, off_c2, off_s2, off_ka, off_ke, off_ks, bytes;
+  bool ksca_in_smem;
+};
+
+template <class R>
+SmemPlan plan_smem(int nr, int nt, int nlam, int ncomp, bool uniform) {
+  SmemPlan p;
+  size_t o = 0;
+  p.off_R = o; o += (size_t)(nr + 1) * 8;
+  p.off_Th = o; o += (size_t)nt * 8;
+  p.off_ST = o; o += (size_t)nt * 8;
+  p.off_cdf = o; o += (size_t)(nlam - 1) * 8;
+  p.off_c2 = o; o += 181 * 8;
+  p.off_s2 = o; o += 181 * 8;
+  p.off_ka = o; if (uniform) o += (size_t)nlam * sizeof(R);
+  o = (o + 15) & ~(size_t)15;
+  p.off_ke = o; if (uniform) o += (size_t)nlam * sizeof(R);
+  o = (o + 15) & ~(size_t)15;
+  p.off_ks = o;
+  size_t ks = (size_t)ncomp * nlam * sizeof(R);
+  p.ksca_in_smem = (o + ks) <= 96 * 1024;
+  if (p.ksca_in_smem) o += ks;
+  p.bytes = (o + 15) & ~(size_t)15;
+  return p;
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) transport_fast_kernel(const __grid_constant__ FModel<R> g,
+                                                             const __grid_constant__ TAcc A, SmemPlan sp) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  if (blockIdx.x == 0 && threadIdx.x == 0) A.tmark[5] = tp_globaltimer();
+  double *sR = (double *)(smem + sp.off_R), *sTh = (double *)(smem + sp.off_Th), *sST = (double *)(smem + sp.off_ST);
+  double *scdf = (double *)(smem + sp.off_cdf), *sc2 = (double *)(smem + sp.off_c2), *ss2 = (double *)(smem + sp.off_s2);
+  R *ska = (R *)(smem + sp.off_ka), *ske = (R *)(smem + sp.off_ke), *sks = (R *)(smem + sp.off_ks);
+  for (int i = threadIdx.x; i <= g.nr; i += blockDim.x) sR[i] = g.Rr[i];
+  for (int i = threadIdx.x; i < g.nt; i += blockDim.x) {
+    sTh[i] = g.Theta[i];
+    sST[i] = g.SinTheta[i];
+  }
+  for (int i = threadIdx.x; i < g.nlam - 1; i += blockDim.x) scdf[i] = g.star_cdf[i];
+  for (int i = threadIdx.x; i < 181; i += blockDim.x) {
+    sc2[i] = g.c2cum[i];
+    ss2[i] = g.s2cum[i];
+  }
+  if (g.uniform_mix)
+    for (int i = threadIdx.x; i < g.nlam; i += blockDim.x) {
+      ska[i] = g.KabsRow[i];
+      ske[i] = g.KextRow[i];
+    }
+  if (sp.ksca_in_smem)
+    for (int i = threadIdx.x; i < g.ncomp * g.nlam; i += blockDim.x) sks[i] = g.Ksca_c[i];
+  __syncthreads();
+  FModel<R> m = g;
+  m.Rr = sR;
+  m.Theta = sTh;
+  m.SinTheta = sST;
+  m.star_cdf = scdf;
+  m.c2cum = sc2;
+  m.s2cum = ss2;
+  if (g.uniform_mix) {
+    m.KabsRow = ska;
+    m.KextRow = ske;
+  }
+  if (sp.ksca_in_smem) m.Ksca_c = sks;
+  TLocal L;
+#pragma unroll
+  for (int k = 0; k < TC_N; ++k) L.cnt[k] = 0u;
+  L.tautot = 0.0;
+  for (;;) {
+    unsigned long long pid = atomicAdd(A.next, 1ULL);
+    if (pid >= (unsigned long long)m.nphot) break;
+    f_run_packet<R>(m, A, (int64_t)pid + m.pid0, L);
+    tp_packet_done(A);
+  }
+#pragma unroll
+  for (int k = 0; k < TC_N; ++k)
+    if (L.cnt[k]) atomicAdd(&A.counters[k], (unsigned long long)L.cnt[k]);
+  if (L.tautot != 0.0) atomicAdd(A.tautot, L.tautot);
+}
+
+template <class R>
+mcg_status build_fast_tables(mcg_ctx *ctx, int pi) {
+  DevModel &m = ctx->model;
+  DevModel::Fast &f = m.fast[pi];
+  if (f.built) return MCG_OK;
+  cudaStream_t st = ctx->stream;
+  const int nlam = m.nlam, ncomp = m.ncomp, ncell = m.ncell, nmat = ncomp * nlam;
+  auto alloc = [&](size_t bytes, void **p) {
+    cudaError_t e = cudaMalloc(p, std::max<size_t>(bytes, 16));
+    if (e == cudaSuccess) m.owned.push_back(*p);
+    return e;
+  };
+  cudaError_t e = cudaSuccess;
+  if (!m.c2cum) {
+    std::vector<double> c2(181), s2(181), ly(TP_NY), y(TP_NY), cp(361), sp(361);
+    MCG_CUDA(ctx, cudaMemcpy(cp.data(), m.cos2phi, 361 * 8, cudaMemcpyDeviceToHost));
+    MCG_CUDA(ctx, cudaMemcpy(sp.data(), m.sin2phi, 361 * 8, cudaMemcpyDeviceToHost));
+    MCG_CUDA(ctx, cudaMemcpy(y.data(), m.rw_y, TP_NY * 8, cudaMemcpyDeviceToHost));
+    c2[0] = s2[0] = 0.0;
+    for (int k = 1; k <= 180; ++k) {
+      c2[k] = c2[k - 1] + cp[k];
+      s2[k] = s2[k - 1] + sp[k];
+    }
+    for (int i = 0; i < TP_NY; ++i) ly[i] = std::log(y[i]);
+    if ((e = alloc(181 * 8, (void **)&m.c2cum)) != cudaSuccess || (e = alloc(181 * 8, (void **)&m.s2cum)) != cudaSuccess ||
+        (e = alloc(TP_NY * 8, (void **)&m.rw_logy)) != cudaSuccess)
+      return mcg_fail(ctx, MCG_ERR_NOMEM, "fast tables: %s", cudaGetErrorString(e));
+    MCG_CUDA(ctx, cudaMemcpyAsync(m.c2cum, c2.data(), 181 * 8, cudaMemcpyHostToDevice, st));
+    MCG_CUDA(ctx, cudaMemcpyAsync(m.s2cum, s2.data(), 181 * 8, cudaMemcpyHostToDevice, st));
+    MCG_CUDA(ctx, cudaMemcpyAsync(m.rw_logy, ly.data(), TP_NY * 8, cudaMemcpyHostToDevice, st));
+    if (m.uniform_mix) {
+      if ((e = alloc((size_t)TP_TT * (nlam - 1) * 8, (void **)&m.Ccum)) != cudaSuccess)
+        return mcg_fail(ctx, MCG_ERR_NOMEM, "fast tables: %s", cudaGetErrorString(e));
+      ccum_kernel<<<nblk(TP_TT, 256), 256, 0, st>>>(nlam, m.dnu_half, m.BB, m.KabsTot, m.Ccum);
+      if ((e = alloc((size_t)TP_TMAX * F_NGUIDE * 2, (void **)&m.emitG)) != cudaSuccess)
+        return mcg_fail(ctx, MCG_ERR_NOMEM, "fast tables: %s", cudaGetErrorString(e));
+      emit_guide_kernel<<<nblk(TP_TMAX, 256), 256, 0, st>>>(nlam - 1, m.emit_cdf, m.emitG);
+    }
+  }
+  const size_t rs = sizeof(R);
+  if ((e = alloc((size_t)nlam * rs, &f.KabsRow)) != cudaSuccess || (e = alloc((size_t)nlam * rs, &f.KextRow)) != cudaSuccess ||
+      (e = alloc((size_t)nmat * rs, &f.Ksca_c)) != cudaSuccess ||
+      (e = alloc((size_t)nmat * 180 * rs, &f.scatA)) != cudaSuccess ||
+      (e = alloc((size_t)nmat * 180 * rs, &f.scatB)) != cudaSuccess ||
+      (e = alloc((size_t)nmat * 1080 * rs, &f.F6)) != cudaSuccess ||
+      (e = alloc((size_t)nmat * F_NGUIDE, (void **)&f.scatG)) != cudaSuccess)
+    return mcg_fail(ctx, MCG_ERR_NOMEM, "fast tables: %s", cudaGetErrorString(e));
+  cast_kernel<R><<<nblk(nlam, 256), 256, 0, st>>>(nlam, m.KabsTot, (R *)f.KabsRow);
+  sum_cast_kernel<R><<<nblk(nlam, 256), 256, 0, st>>>(nlam, m.KabsTot, m.KscaTot, (R *)f.KextRow);
+  cast_kernel<R><<<nblk(nmat, 256), 256, 0, st>>>(nmat, m.Ksca_c, (R *)f.Ksca_c);
+  if (m.scat_how == 2)
+  {
+    scat_tables_kernel<R><<<nblk(nmat, 128), 128, 0, st>>>(nmat, m.F_c, m.sinthet, (R *)f.scatA, (R *)f.scatB, (R *)f.F6);
+    scat_guide_kernel<R><<<nblk(nmat, 128), 128, 0, st>>>(nmat, (const R *)f.scatA, f.scatG);
+  }
+  if (!m.uniform_mix) {
+    const long long n = (long long)ncell * nlam;
+    if ((e = alloc((size_t)n * rs, &f.KabsTotR)) != cudaSuccess || (e = alloc((size_t)n * rs, &f.KextTotR)) != cudaSuccess)
+      return mcg_fail(ctx, MCG_ERR_NOMEM, "fast tables: %s", cudaGetErrorString(e));
+    cast_kernel<R><<<nblk(n, 256), 256, 0, st>>>(n, m.KabsTot, (R *)f.KabsTotR);
+    sum_cast_kernel<R><<<nblk(n, 256), 256, 0, st>>>(n, m.KabsTot, m.KscaTot, (R *)f.KextTotR);
+  }
+  MCG_CUDA(ctx, cudaGetLastError());
+  MCG_CUDA(ctx, cudaStreamSynchronize(st));
+  f.built = true;
+  return MCG_OK;
+}
+
+template <class R>
+mcg_status launch_fast(mcg_ctx *ctx, int pi, const TModel &tm, const TAcc &ta, int threads, int block, float *ms) {
+  mcg_status s = build_fast_tables<R>(ctx, pi);
+  if (s != MCG_OK) return s;
+  DevModel &m = ctx->model;
+  DevModel::Fast &f = m.fast[pi];
+  FModel<R> g;
+  memset(&g, 0, sizeof g);
+  g.nr = tm.nr; g.nt = tm.nt; g.nc = tm.nc; g.ncell = tm.ncell; g.nlam = tm.nlam; g.ncomp = tm.ncomp;
+  g.scattering = tm.scattering; g.scat_how = tm.scat_how; g.uniform_mix = tm.uniform_mix; g.rw = tm.rw;
+  g.factRW = tm.factRW; g.R0 = tm.R0; g.Lstar = tm.Lstar; g.Epkt = tm.Epkt; g.nruns_d = tm.nruns_d;
+  g.nphot = tm.nphot; g.maxinteract = tm.maxinteract; g.pid0 = tm.pid0; g.seed = tm.seed;
+  g.Rr = tm.R; g.Theta = tm.Theta; g.SinTheta = tm.SinTheta; g.star_cdf = tm.star_cdf;
+  g.KabsRow = (const R *)f.KabsRow; g.KextRow = (const R *)f.KextRow; g.Ksca_c = (const R *)f.Ksca_c;
+  g.c2cum = m.c2cum; g.s2cum = m.s2cum;
+  g.dens = tm.dens; g.mass = tm.mass; g.wlam = tm.wlam;
+  g.KabsTotR = (const R *)f.KabsTotR; g.KextTotR = (const R *)f.KextTotR; g.KabsTot = m.KabsTot;
+  g.BB = m.BB; g.dnu_half = m.dnu_half; g.KpCell = m.KpCell;
+  g.Ccum = m.Ccum; g.Dcum = m.emit_cdf; g.comp_w = m.comp_w;
+  g.scatA = (const R *)f.scatA; g.scatB = (const R *)f.scatB; g.F6 = (const R *)f.F6; g.IF_c = m.IF_c;
+  g.scatG = f.scatG; g.emitG = m.emitG;
+  g.KDext = m.KDext; g.KDabs = m.KDabs; g.rw_logy = m.rw_logy; g.rw_phi = m.rw_phi;
+  g.kd_index = m.kd_index; g.thick = m.thick;
+  SmemPlan sp = plan_smem<R>(m.nr, m.nt, m.nlam, m.ncomp, m.uniform_mix);
+  MCG_CUDA(ctx, cudaFuncSetAttribute(transport_fast_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.bytes));
+  const int b = block > 0 ? block : 256;
+  int grid;
+  if (threads > 0) {
+    grid = (threads + b - 1) / b;
+  } else {
+    int per_sm = 0;
+    MCG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, transport_fast_kernel<R>, b, sp.bytes));
+    grid = ctx->sm_count * std::max(per_sm, 1);
+  }
+  MCG_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+  if (threads == 1)
+    transport_fast_kernel<R><<<1, 1, sp.bytes, ctx->stream>>>(g, ta, sp);
+  else
+    transport_fast_kernel<R><<<grid, b, sp.bytes, ctx->stream>>>(g, ta, sp);
+  MCG_CUDA(ctx, cudaGetLastError());
+  MCG_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+  MCG_CUDA(ctx, cudaEventSynchronize(ctx->ev1));
+  MCG_CUDA(ctx, cudaEventElapsedTime(ms, ctx->ev0, ctx->ev1));
+  return MCG_OK;
+}
+
+}  // namespace
+
+mcg_status mcg_fast_run(mcg_ctx *ctx, int precision, const void *tmodel, const void *tacc, int threads, int block,
+                        float *ms) {
+  const TModel &tm = *(const TModel *)tmodel;
+  const TAcc &ta = *(const TAcc *)tacc;
+  if (precision == 1) return launch_fast<float>(ctx, 1, tm, ta, threads, block, ms);
+  return launch_fast<double>(ctx, 0, tm, ta, threads, block, ms);
+}

@@ -1,0 +1,702 @@
+/*
+ * transport_fast.cuh -- the MCMax packet loop restructured for the GPU,
+ * templated on the precision of the direction / Stokes / optical-depth /
+ * opacity arithmetic (R = double: "fp64", R = float: "mixed").  Positions,
+ * the sphere/cone intersection quadratics, packet energies, the per-cell
+ * energy accumulators and the Bjorkman-Wood temperature inversion are FP64 in
+ * both forms.
+ *
+ * Same physics and the same random-number consumption as the reference-order
+ * kernel (transport_core.cuh), with the per-event latency cut:
+ *   - geometry edges, the star spectrum CDF, the opacity rows of a uniform
+ *     mixture, component scattering opacities and the cumulative phi tables
+ *     live in shared memory;
+ *   - the opacity at the packet's wavelength is formed once per emission or
+ *     scattering-wavelength change (uniform mixture), not once per crossing;
+ *   - wavelength re-emission (Radiation.f:187-213, :966-988) samples from
+ *     cumulative tables by binary search: C(iT)[i] = cumulative of BB(iT) K
+ *     and D(iT)[i] = cumulative of (BB(iT+1) - BB(iT)) K, so the spectrum of
+ *     a (T0 -> T1) jump has the cumulative [C(iT1) + e1 D(iT1)] -
+ *     [C(iT0) + e0 D(iT0)] (exactly the reference's interpolated Delta-B);
+ *   - the scattering angle (Radiation.f:434-452) samples from the
+ *     cumulative A_k = sum pi sin(th_i) F11_i, B_k = sum pi sin(th_i) F12_i
+ *     with F_k = E A_k + Q B_k, and the polarised azimuth (:393-420) from
+ *     cumulative sums of cos 2phi / sin 2phi, both by binary search;
+ *   - the temperature inversion gallops from a per-cell bracket hint (the
+ *     absorbed energy of a cell only grows, so any stored bracket is a valid
+ *     lower bound).
+ * Stokes parameters are carried as fractions of E (q = Q/E ...), which is
+ * what the reference's renormalisation (Radiation.f:480-483) keeps invariant.
+ * Results agree with the reference-order kernel up to floating-point
+ * reassociation; the checks are statistical against the CPU checker and
+ * paired (identical Philox streams) against the reference-order kernel.
+ */
+#ifndef MCMAX_TRANSPORT_FAST_CUH
+#define MCMAX_TRANSPORT_FAST_CUH
+
+#include "transport_core.cuh"
+
+template <class R>
+struct FModel {
+  int nr, nt, nc, ncell, nlam, ncomp;
+  int scattering, scat_how, uniform_mix, rw, pol_tables;
+  double factRW, R0, Lstar, Epkt, nruns_d;
+  int64_t nphot, maxinteract, pid0;
+  uint64_t seed;
+  /* shared-memory copies (or global when not uniform) */
+  const double *Rr, *Theta, *SinTheta, *star_cdf;
+  const R *KabsRow, *KextRow;  /* uniform mixture: one row each */
+  const R *Ksca_c;             /* ncomp*nlam */
+  const double *c2cum, *s2cum; /* 181: cumulative cos/sin(2 phi_i), i = 1..k */
+  /* global */
+  const double *dens, *mass, *wlam;
+  const R *KabsTotR, *KextTotR; /* ncell*nlam (non-uniform mixtures) */
+  const double *KabsTot;        /* ncell*nlam, for the per-cell scan */
+  const double *BB, *dnu_half;
+  const double *KpCell;         /* uniform: 1 row, else ncell rows */
+  const double *Ccum, *Dcum;    /* uniform mixture: TT*(nlam-1) */
+  const double *comp_w;
+  const R *scatA, *scatB;       /* ncomp*nlam*180 */
+  const unsigned char *scatG;   /* ncomp*nlam*NGUIDE: first bin with A > k/NGUIDE of the total */
+  const unsigned short *emitG;  /* TMAX*NGUIDE: same for the rows of Dcum */
+  const R *F6;                  /* ncomp*nlam*1080 */
+  const double *IF_c;
+  const double *KDext, *KDabs, *rw_logy, *rw_phi;
+  const int *kd_index;
+  const unsigned char *thick;
+};
+
+#define F_NGUIDE 32
+
+/* first index i in [0,n) with f(i) > v (or >= when ge), starting from a
+ * guess and walking; f is non-decreasing */
+template <class F>
+TP_FN int f_walk(F f, int n, int i, double v, bool ge) {
+  if (i < 0) i = 0;
+  if (i > n) i = n;
+  auto above = [&](int k) { return ge ? f(k) >= v : f(k) > v; };
+  if (i < n && above(i)) {
+    while (i > 0 && above(i - 1)) --i;
+  } else {
+    while (i < n && !above(i)) ++i;
+  }
+  return i;
+}
+
+template <class R>
+struct FPkt {
+  double x, y, z, E, nEJv;
+  /* transport direction: FP64 and re-normalised after every FP32 rotation,
+   * so the FP64 intersection quadratics (which assume |v| = 1) put the packet
+   * on the cell faces */
+  double vx, vy, vz;
+  R q, u, v;    /* Stokes / E */
+  R Sx, Sy, Sz;
+  R wl1, wl2;
+  R kabs, kext; /* at the packet wavelength, uniform mixture */
+  int ilam1, i, j, edgeNr, onEdge, scatt, pol, pid1;
+  int cprev1, cprev2; /* last two cells this packet entered */
+};
+
+template <class R>
+struct FOps;
+template <>
+struct FOps<double> {
+  TP_SFN double sqrt_(double x) { return sqrt(x); }
+  TP_SFN double log_(double x) { return log(x); }
+  TP_SFN void sincos_(double x, double *s, double *c) { sincos(x, s, c); }
+  TP_SFN double u(double x) { return x; }
+};
+template <>
+struct FOps<float> {
+  TP_SFN float sqrt_(float x) { return sqrtf(x); }
+  TP_SFN float log_(float x) { return logf(x); }
+  TP_SFN void sincos_(float x, float *s, float *c) { sincosf(x, s, c); }
+  /* a draw in (0,1) as float, kept < 1 */
+  TP_SFN float u(double x) {
+    float f = (float)x;
+    return f < 1.0f ? f : 0.99999994f;
+  }
+};
+
+template <class R>
+TP_FN void f_randomdirection(px_stream *r, R *x, R *y, R *z) {
+  typedef FOps<R> O;
+  R rr;
+  for (;;) {
+    *x = (R)2 * O::u(px_next(r)) - (R)1;
+    *y = (R)2 * O::u(px_next(r)) - (R)1;
+    *z = (R)2 * O::u(px_next(r)) - (R)1;
+    rr = (*x) * (*x) + (*y) * (*y) + (*z) * (*z);
+    if (!(rr > (R)1)) break;
+  }
+  rr = (R)1 / O::sqrt_(rr);
+  *x *= rr;
+  *y *= rr;
+  *z *= rr;
+}
+
+template <class R>
+TP_FN void f_set_dir(FPkt<R> &p, R x, R y, R z) {
+  const double dx = (double)x, dy = (double)y, dz = (double)z;
+  const double inv = 1.0 / sqrt(dx * dx + dy * dy + dz * dz);
+  p.vx = dx * inv;
+  p.vy = dy * inv;
+  p.vz = dz * inv;
+}
+
+template <class R>
+TP_FN void f_set_s(FPkt<R> &p) {
+  typedef FOps<R> O;
+  R x = (R)-p.vy, y = (R)p.vx;
+  R r = (R)1 / O::sqrt_(x * x + y * y);
+  p.Sx = x * r;
+  p.Sy = y * r;
+  p.Sz = (R)0;
+}
+
+/* first index in [0,n) with cdf[i] >= v (n when none) */
+TP_FN int f_lower_bound(const double *cdf, int n, double v) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (cdf[mid] >= v)
+      hi = mid;
+    else
+      lo = mid + 1;
+  }
+  return lo;
+}
+
+template <class R>
+TP_FN void f_set_lambda(const FModel<R> &m, FPkt<R> &p) {
+  if (m.uniform_mix) {
+    const int l = p.ilam1;
+    p.kabs = m.KabsRow[l] * p.wl1 + m.KabsRow[l + 1] * p.wl2;
+    p.kext = m.KextRow[l] * p.wl1 + m.KextRow[l + 1] * p.wl2;
+  }
+}
+
+/* interval pick on a cumulative table (shared by star and re-emission) */
+template <class R>
+TP_FN void f_pick(const FModel<R> &m, FPkt<R> &p, int i, double Lt, double Ltold, double Lr) {
+  const int n = m.nlam - 1;
+  if (i < n) {
+    double d = Lt - Ltold;
+    double w = d != 0.0 ? (Lr - Ltold) / d : 1.0;
+    p.wl1 = (R)w;
+    p.wl2 = (R)(1.0 - w);
+    p.ilam1 = i;
+  } else {
+    p.wl1 = (R)0;
+    p.wl2 = (R)1;
+    p.ilam1 = m.nlam - 2;
+  }
+}
+
+/* ------------------------------------------------------------- geometry */
+template <class R>
+TP_FN int f_trace2edge(const FModel<R> &m, FPkt<R> &p, double *v, int *inext, int *jnext) {
+  TPkt t; /* geometry in FP64 */
+  t.x = p.x; t.y = p.y; t.z = p.z;
+  t.vx = p.vx; t.vy = p.vy; t.vz = p.vz;
+  t.i = p.i; t.j = p.j; t.edgeNr = p.edgeNr; t.onEdge = p.onEdge;
+  TModel tm;
+  tm.nt = m.nt;
+  tm.R = m.Rr;
+  tm.Theta = m.Theta;
+  int r = tp_trace2edge(tm, t, v, inext, jnext);
+  p.edgeNr = t.edgeNr;
+  return r;
+}
+
+/* ------------------------------------------------------------- rotations */
+template <class R>
+TP_FN void f_rotate(R *x, R *y, R *z, R u, R v, R w, R theta) {
+  R sint, cost;
+  FOps<R>::sincos_(theta, &sint, &cost);
+  R u2 = u * u, v2 = v * v, w2 = w * w;
+  R inp = *x * u + *y * v + *z * w;
+  R y1 = u * inp + (*x * (v2 + w2) - u * (v * *y + w * *z)) * cost + (v * *z - w * *y) * sint;
+  R y2 = v * inp + (*y * (u2 + w2) - v * (u * *x + w * *z)) * cost + (w * *x - u * *z) * sint;
+  R y3 = w * inp + (*z * (u2 + v2) - w * (u * *x + v * *y)) * cost + (u * *y - v * *x) * sint;
+  *x = y1;
+  *y = y2;
+  *z = y3;
+}
+
+template <class R>
+TP_FN void f_rotate_stokes(FPkt<R> &p, R x, R y, R z) {
+  typedef FOps<R> O;
+  R P = p.u * p.u + p.q * p.q;
+  if (P == (R)0) return;
+  const R vx = (R)p.vx, vy = (R)p.vy, vz = (R)p.vz;
+  R cost = p.Sx * x + p.Sy * y + p.Sz * z;
+  R sint = (x - (p.Sx * (vy * vy + vz * vz) - vx * (vy * p.Sy + vz * p.Sz)) * cost) / (vy * p.Sz - vz * p.Sy);
+  R cos2t = cost * cost - sint * sint;
+  R sin2t = (R)2 * sint * cost;
+  R Q = p.q * cos2t + p.u * sin2t;
+  R U = -p.q * sin2t + p.u * cos2t;
+  R P2 = U * U + Q * Q;
+  R s = O::sqrt_(P / P2);
+  p.u = s * U;
+  p.q = s * Q;
+}
+
+/* ------------------------------------------------------------- scattering */
+template <class R>
+TP_FN void f_scatangle(const FModel<R> &m, px_stream *r, FPkt<R> &p, int mat) {
+  typedef FOps<R> O;
+  const R *A = m.scatA + (size_t)mat * 180;
+  const R *B = m.scatB + (size_t)mat * 180;
+  const R *F = m.F6 + (size_t)mat * 1080;
+  R phi;
+  if (p.pol) {
+    /* I0(k) = k IF11 + IF12 (q C_k + u S_k), IF scaled by 180 as the
+     * reference does; monotone in k because |F12| <= F11 */
+    const double if11 = m.IF_c[2 * mat] * 180.0, if12 = m.IF_c[2 * mat + 1] * 180.0;
+    const double qd = (double)p.q, ud = (double)p.u;
+    const double Itot = 180.0 * if11 + if12 * (qd * m.c2cum[180] + ud * m.s2cum[180]);
+    const double It = px_next(r) * Itot;
+    int lo = 1, hi = 181; /* first k in [1,180] with I0(k) > It; 181 = none */
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      double I0 = (double)mid * if11 + if12 * (qd * m.c2cum[mid] + ud * m.s2cum[mid]);
+      if (I0 > It)
+        hi = mid;
+      else
+        lo = mid + 1;
+    }
+    if (lo <= 180) {
+      double I0 = (double)lo * if11 + if12 * (qd * m.c2cum[lo] + ud * m.s2cum[lo]);
+      double I1 = (double)(lo - 1) * if11 + if12 * (qd * m.c2cum[lo - 1] + ud * m.s2cum[lo - 1]);
+      double wp1 = (I0 - It) / (I0 - I1);
+      phi = (R)(TP_PI * ((double)lo - wp1) / 180.0);
+    } else {
+      phi = (R)TP_PI;
+    }
+  } else {
+    phi = O::u(px_next(r)) * (R)TP_PI;
+  }
+  R x = p.Sx, y = p.Sy, z = p.Sz;
+  f_rotate<R>(&x, &y, &z, (R)p.vx, (R)p.vy, (R)p.vz, phi);
+  if (p.pol) f_rotate_stokes<R>(p, x, y, z);
+  p.Sx = x;
+  p.Sy = y;
+  p.Sz = z;
+  /* scattering angle: F(k) = A_k + q B_k (per unit E); the guide table of
+   * A (q = 0) gives the starting bin, a short walk corrects for q */
+  const R q = p.q;
+  const R Ftot = A[179] + q * B[179];
+  const R xr = O::u(px_next(r));
+  const R Fr = xr * Ftot;
+  int gk = (int)(xr * (R)F_NGUIDE);
+  if (gk > F_NGUIDE - 1) gk = F_NGUIDE - 1;
+  const int lo = f_walk([&](int k) { return (double)(A[k] + q * B[k]); }, 180,
+                        (int)m.scatG[(size_t)mat * F_NGUIDE + gk], (double)Fr, false);
+  R theta;
+  int ib;
+  if (lo < 180) {
+    R Fi = A[lo] + q * B[lo];
+    R Fo = lo > 0 ? A[lo - 1] + q * B[lo - 1] : (R)0;
+    theta = ((R)(lo + 1) - (Fi - Fr) / (Fi - Fo)) * (R)(TP_PI / 180.0);
+    ib = lo + 1;
+  } else {
+    theta = (R)TP_PI;
+    ib = 180;
+  }
+  if (px_next(r) < 0.5) theta = -theta;
+  const int k = ib - 1;
+  const R F11 = F[k], F12 = F[180 + k], F22 = F[360 + k], F33 = F[540 + k], F34 = F[720 + k], F44 = F[900 + k];
+  const R E = F11 + F12 * p.q;
+  const R Q = F12 + F22 * p.q;
+  R U = F33 * p.u;
+  const R Fs = theta >= (R)0 ? (F34 >= (R)0 ? F34 : -F34) : (F34 >= (R)0 ? -F34 : F34);
+  U = U + Fs * p.v;
+  const R V = -Fs * p.u + F44 * p.v;
+  if (E != (R)0) {
+    const R ie = (R)1 / E;
+    p.q = Q * ie;
+    p.u = U * ie;
+    p.v = V * ie;
+  }
+  R vx = (R)p.vx, vy = (R)p.vy, vz = (R)p.vz;
+  f_rotate<R>(&vx, &vy, &vz, p.Sx, p.Sy, p.Sz, theta);
+  f_set_dir<R>(p, vx, vy, vz);
+  R rr = (R)1 / O::sqrt_(p.Sx * p.Sx + p.Sy * p.Sy + p.Sz * p.Sz);
+  p.Sx *= rr;
+  p.Sy *= rr;
+  p.Sz *= rr;
+  if (ib != 1 && ib != 180) p.pol = 1;
+}
+
+/* ------------------------------------------------------------- temperature */
+/* gallop from `lo` (a valid lower bound of the bracket) */
+TP_FN double f_tinv(const double *kp, double E1, int lo, int *ibr) {
+  return tp_tinv(kp, E1, lo, ibr);
+}
+
+/* ------------------------------------------------------------- interaction */
+template <class R>
+TP_FN void f_interact(const FModel<R> &m, const TAcc &A, px_stream *r, FPkt<R> &p, TLocal &L) {
+  typedef FOps<R> O;
+  const int c = p.i * m.nc + (p.j - 1);
+  const int nlam = m.nlam;
+  const int l1 = p.ilam1;
+  R kabs, ksca;
+  if (m.uniform_mix) {
+    kabs = p.kabs;
+    ksca = p.kext - p.kabs;
+  } else {
+    const R *Ka = m.KabsTotR + (size_t)c * nlam, *Ke = m.KextTotR + (size_t)c * nlam;
+    kabs = Ka[l1] * p.wl1 + Ka[l1 + 1] * p.wl2;
+    ksca = (Ke[l1] * p.wl1 + Ke[l1 + 1] * p.wl2) - kabs;
+  }
+  L.cnt[TC_INTERACT]++;
+  const R albedo = ksca / (ksca + kabs);
+  if (!m.scattering || O::u(px_next(r)) > albedo) {
+    L.cnt[TC_ABSORB]++;
+    p.scatt = 0;
+    p.pol = 0;
+    p.q = p.u = p.v = (R)0;
+    const double *kp = m.KpCell + (m.uniform_mix ? (size_t)0 : (size_t)c * TP_TT);
+    const double dE = p.E;
+    const double Eold = tp_add(&A.Eabs[c], dE);
+    const double mass = m.mass[c];
+    int hint = A.kp_hint[c];
+    int ib0, ib1;
+    const double T0 = f_tinv(kp, Eold / mass, hint, &ib0);
+    const double T1 = f_tinv(kp, (Eold + dE) / mass, ib0, &ib1);
+    if (ib1 > hint) A.kp_hint[c] = ib1;
+    int iT0 = (int)T0, iT1 = (int)T1;
+    double e0 = T0 - (double)iT0, e1 = T1 - (double)iT1;
+    if (iT0 >= TP_TMAX - 1) iT0 = TP_TMAX - 2;
+    if (iT1 >= TP_TMAX - 1) iT1 = TP_TMAX - 1;
+    if (iT0 < 1) iT0 = 1;
+    if (iT1 < 2) iT1 = 2;
+    /* new direction first (emit), then the wavelength draw */
+    L.cnt[TC_EMIT]++;
+    {
+      R ux, uy, uz;
+      f_randomdirection<R>(r, &ux, &uy, &uz);
+      f_set_dir<R>(p, ux, uy, uz);
+    }
+    p.scatt = 0;
+    p.pol = 0;
+    f_set_s<R>(p);
+    const double xi = px_next(r);
+    const int n = nlam - 1;
+    if (m.uniform_mix) {
+      const double *D0 = m.Dcum + (size_t)iT0 * n;
+      if (iT0 == iT1) {
+        const double tot = D0[n - 1];
+        const double Lr = xi * tot;
+        int gk = (int)(xi * (double)F_NGUIDE);
+        if (gk > F_NGUIDE - 1) gk = F_NGUIDE - 1;
+        const int i = f_walk([&](int k) { return D0[k]; }, n, (int)m.emitG[(size_t)iT0 * F_NGUIDE + gk], Lr, true);
+        f_pick<R>(m, p, i, i < n ? D0[i] : 0.0, i > 0 ? D0[i - 1] : 0.0, Lr);
+      } else {
+        const double *C0 = m.Ccum + (size_t)iT0 * n, *C1 = m.Ccum + (size_t)iT1 * n;
+        const double *D1 = m.Dcum + (size_t)iT1 * n;
+        auto cum = [&](int i) { return (C1[i] + e1 * D1[i]) - (C0[i] + e0 * D0[i]); };
+        const double tot = cum(n - 1);
+        const double Lr = xi * tot;
+        int lo = 0, hi = n;
+        while (lo < hi) {
+          int mid = (lo + hi) >> 1;
+          if (cum(mid) >= Lr)
+            hi = mid;
+          else
+            lo = mid + 1;
+        }
+        f_pick<R>(m, p, lo, lo < n ? cum(lo) : 0.0, lo > 0 ? cum(lo - 1) : 0.0, Lr);
+      }
+    } else {
+      /* per-cell spectrum: sequential scan (Radiation.f:187-213) */
+      const double *Ka = m.KabsTot + (size_t)c * nlam;
+      auto spec = [&](int l) {
+        const double *Bl = m.BB + (size_t)l * TP_TT;
+        if (iT0 == iT1) return (Bl[iT0 + 1] - Bl[iT0]) * Ka[l];
+        return (((e1 * Bl[iT1 + 1] + (1.0 - e1) * Bl[iT1]) - e0 * Bl[iT0 + 1]) - (1.0 - e0) * Bl[iT0]) * Ka[l];
+      };
+      double kpe = iT0 == iT1 ? kp[iT0 + 1] - kp[iT0]
+                              : ((e1 * kp[iT1 + 1] + (1.0 - e1) * kp[iT1]) - e0 * kp[iT0 + 1]) - (1.0 - e0) * kp[iT0];
+      const double Lr = xi * kpe;
+      double Lt = 0.0, Ltold = 0.0, s0 = spec(0);
+      int i = 0;
+      for (; i < n; ++i) {
+        double s1 = spec(i + 1);
+        Lt = Lt + m.dnu_half[i] * (s0 + s1);
+        if (Lt >= Lr) break;
+        Ltold = Lt;
+        s0 = s1;
+      }
+      f_pick<R>(m, p, i, Lt, Ltold, Lr);
+    }
+    f_set_lambda<R>(m, p);
+    A.T[c] = T1;
+  } else {
+    L.cnt[TC_SCATTER]++;
+    p.scatt = 1;
+    if (m.scat_how == 1) {
+      R ux, uy, uz;
+      f_randomdirection<R>(r, &ux, &uy, &uz);
+      f_set_dir<R>(p, ux, uy, uz);
+    } else {
+      R KscaR = O::u(px_next(r)) * ksca;
+      const double *w = m.comp_w + (size_t)c * m.ncomp;
+      int mat = -1, qlast = 0, llast = l1;
+      for (int q = 0; q < m.ncomp; ++q) {
+        const R wq = (R)w[q];
+        const R w2 = wq * p.wl2 * m.Ksca_c[q * nlam + l1 + 1];
+        KscaR -= w2;
+        if (KscaR < (R)0) {
+          mat = q * nlam + l1 + 1;
+          break;
+        }
+        const R w1 = wq * p.wl1 * m.Ksca_c[q * nlam + l1];
+        KscaR -= w1;
+        if (KscaR < (R)0) {
+          mat = q * nlam + l1;
+          break;
+        }
+        if (w2 > (R)0) { qlast = q; llast = l1 + 1; }
+        if (w1 > (R)0) { qlast = q; llast = l1; }
+      }
+      if (mat < 0) {
+        L.cnt[TC_AVGMAT]++;
+        mat = qlast * nlam + llast;
+      }
+      f_scatangle<R>(m, r, p, mat);
+    }
+  }
+}
+
+/* ------------------------------------------------------------- random walk */
+template <class R>
+TP_FN int f_random_walk(const FModel<R> &m, const TAcc &A, px_stream *r, FPkt<R> &p, TLocal &L) {
+  const int c = p.i * m.nc + (p.j - 1);
+  const int row = m.kd_index[c];
+  if (row < 0) return 0;
+  /* distance to the nearest face (MinDist, RandomWalk.f:15-43) */
+  double rho = p.x * p.x + p.y * p.y;
+  const double rr = sqrt(rho + p.z * p.z);
+  rho = sqrt(rho);
+  const double z = fabs(p.z);
+  double dmin = fabs(rr - m.Rr[p.i]);
+  double t = fabs(m.Rr[p.i + 1] - rr);
+  if (t < dmin) dmin = t;
+  t = fabs(m.Theta[p.j - 1] * rho - m.SinTheta[p.j - 1] * z);
+  if (t < dmin) dmin = t;
+  t = fabs(m.Theta[p.j] * rho - m.SinTheta[p.j] * z);
+  if (t < dmin) dmin = t;
+  int iT = (int)A.T[c];
+  if (iT < 1) iT = 1;
+  if (iT > TP_TMAX - 1) iT = TP_TMAX - 1;
+  const double Kext = m.KDext[(size_t)row * TP_TT + iT];
+  const double lr = 1.0 / ((TP_AU * Kext) * m.dens[c]);
+  if (dmin <= m.factRW * lr) return 0;
+  int iy = 1;
+  tp_hunt(m.rw_phi, TP_NY, px_next(r), &iy);
+  const double v = ((-3.0 * m.rw_logy[iy - 1]) * (dmin * dmin)) / (lr * (TP_PI * TP_PI));
+  const double Kabs = m.KDabs[(size_t)row * TP_TT + iT];
+  R ux, uy, uz;
+  f_randomdirection<R>(r, &ux, &uy, &uz);
+  f_set_dir<R>(p, ux, uy, uz);
+  p.x += dmin * p.vx;
+  p.y += dmin * p.vy;
+  p.z += dmin * p.vz;
+  const double EJv = (p.E * v) * TP_AU;
+  const double dEa = (EJv * Kabs) * m.dens[c];
+  const double Eold = tp_add(&A.Eabs[c], dEa);
+  tp_add(&A.EJv[c], EJv * Kabs);
+  p.nEJv += EJv * Kabs;
+  const double *kp = m.KpCell + (m.uniform_mix ? (size_t)0 : (size_t)c * TP_TT);
+  int ib;
+  A.T[c] = f_tinv(kp, (Eold + dEa) / m.mass[c], A.kp_hint[c], &ib);
+  if (ib > A.kp_hint[c]) A.kp_hint[c] = ib;
+  L.tautot += v / dmin;
+  L.cnt[TC_RWSTEP]++;
+  return 1;
+}
+
+/* ------------------------------------------------------------- trace */
+template <class R>
+TP_FN int f_trace(const FModel<R> &m, const TAcc &A, px_stream *r, FPkt<R> &p, double tau0, TLocal &L) {
+  const int nlam = m.nlam;
+  double tau = 0.0;
+  int ntrace = 0;
+  if (m.rw && !p.onEdge && m.thick[p.i * m.nc + (p.j - 1)]) {
+    while (f_random_walk<R>(m, A, r, p, L)) {
+      R vx, vy, vz;
+      do {
+        f_randomdirection<R>(r, &vx, &vy, &vz);
+      } while ((R)p.vx * vx + (R)p.vy * vy + (R)p.vz * vz < (R)0);
+      f_set_dir<R>(p, vx, vy, vz);
+    }
+  }
+  for (;;) {
+    const int c = p.i * m.nc + (p.j - 1);
+    /* Ni counts distinct packets per cell (lastphotnr, MCRadiation.f:943-946);
+     * re-entering one of its last two cells, the packet's own number is
+     * already there */
+    const bool recent = (c == p.cprev1) || (c == p.cprev2);
+    const int prev = recent ? p.pid1 : tp_exch(&A.lastphot[c], p.pid1);
+    if (!recent) {
+      p.cprev2 = p.cprev1;
+      p.cprev1 = c;
+    }
+    R kabs, kext;
+    if (m.uniform_mix) {
+      kabs = p.kabs;
+      kext = m.scattering ? p.kext : p.kabs;
+    } else {
+      const R *Ka = m.KabsTotR + (size_t)c * nlam, *Ke = m.KextTotR + (size_t)c * nlam;
+      kabs = Ka[p.ilam1] * p.wl1 + Ka[p.ilam1 + 1] * p.wl2;
+      kext = m.scattering ? Ke[p.ilam1] * p.wl1 + Ke[p.ilam1 + 1] * p.wl2 : kabs;
+    }
+    double v;
+    int inext, jnext;
+    const int geo = f_trace2edge<R>(m, p, &v, &inext, &jnext);
+    if (prev != p.pid1) tp_addi(&A.Ni[c], 1);
+    if (geo) return -1;
+    L.cnt[TC_CROSS]++;
+    const double dAU = m.dens[c] * TP_AU;
+    const double tau1 = ((double)kext * v) * dAU;
+    if (tau + tau1 > tau0) {
+      v = (v * (tau0 - tau)) / tau1;
+      L.tautot += tau0 - tau;
+      p.x += p.vx * v;
+      p.y += p.vy * v;
+      p.z += p.vz * v;
+      p.onEdge = 0;
+      const double dj = (p.E * v) * TP_AU * (double)kabs;
+      tp_add(&A.EJv[c], dj);
+      p.nEJv += dj;
+      return 0;
+    }
+    p.x += p.vx * v;
+    p.y += p.vy * v;
+    p.z += p.vz * v;
+    const double dj = (p.E * v) * TP_AU * (double)kabs;
+    p.nEJv += dj;
+    tp_add(&A.EJv2[c], p.nEJv * p.nEJv);
+    p.nEJv = 0.0;
+    tp_add(&A.EJv[c], dj);
+    p.onEdge = 1;
+    tau += tau1;
+    L.tautot += tau1;
+    if (inext >= m.nr) return 1;
+    if (inext < 0) return 2;
+    p.i = inext;
+    p.j = jnext;
+    if (++ntrace > m.nr * m.nt * 2) {
+      L.cnt[TC_ABANDON]++;
+      return 2;
+    }
+  }
+}
+
+/* ------------------------------------------------------------- one packet */
+template <class R>
+TP_FN void f_run_packet(const FModel<R> &m, const TAcc &A0, int64_t pid, TLocal &L) {
+  const TAcc A = tp_run_acc(A0, pid);
+  px_stream rs;
+  px_init(&rs, m.seed, (uint64_t)pid);
+  px_stream *r = &rs;
+  FPkt<R> p;
+  p.pid1 = (int)(pid + 1);
+  p.q = p.u = p.v = (R)0;
+  p.pol = 0;
+  p.scatt = 0;
+  p.cprev1 = p.cprev2 = -1;
+  for (;;) {
+    p.nEJv = 0.0;
+    (void)px_next(r); /* where_emit */
+    R x, y, z;
+    f_randomdirection<R>(r, &x, &y, &z);
+    p.x = m.R0 * (double)x;
+    p.y = m.R0 * (double)y;
+    p.z = m.R0 * (double)z;
+    L.cnt[TC_EMIT]++;
+    {
+      R ux, uy, uz;
+      f_randomdirection<R>(r, &ux, &uy, &uz);
+      f_set_dir<R>(p, ux, uy, uz);
+    }
+    p.scatt = 0;
+    p.pol = 0;
+    f_set_s<R>(p);
+    {
+      const double Lr = px_next(r) * m.Lstar;
+      const int n = m.nlam - 1;
+      int i = f_lower_bound(m.star_cdf, n, Lr);
+      f_pick<R>(m, p, i, i < n ? m.star_cdf[i] : 0.0, i > 0 ? m.star_cdf[i - 1] : 0.0, Lr);
+    }
+    f_set_lambda<R>(m, p);
+    p.E = m.Epkt;
+    {
+      R ux, uy, uz;
+      f_randomdirection<R>(r, &ux, &uy, &uz);
+      f_set_dir<R>(p, ux, uy, uz);
+    }
+    if (p.x * p.vx + p.y * p.vy + p.z * p.vz < 0.0) {
+      p.vx = -p.vx;
+      p.vy = -p.vy;
+      p.vz = -p.vz;
+    }
+    p.edgeNr = 1;
+    p.onEdge = 1;
+    const double ct = fabs(p.z) / m.R0;
+    p.i = 0;
+    p.j = m.nt - 1;
+    for (int j = 1; j <= m.nt - 1; ++j)
+      if (ct >= m.Theta[j]) {
+        p.j = j;
+        break;
+      }
+    if (m.scattering) {
+      p.pol = 0;
+      p.scatt = 0;
+      p.q = p.u = p.v = (R)0;
+      f_set_s<R>(p);
+    }
+    double tau = -log(px_next(r));
+    for (;;) {
+      const int st = f_trace<R>(m, A, r, p, tau, L);
+      if (st < 0) {
+        L.cnt[TC_GEOFAIL]++;
+        return;
+      }
+      if (st == 2) {
+        L.cnt[TC_HITSTAR]++;
+        break;
+      }
+      if (st == 1) {
+        L.cnt[TC_ESCAPE]++;
+        const double av = fabs(p.vz);
+        int ia = (int)(av * (double)TP_NANG + 1.0);
+        if (ia > TP_NANG) ia = TP_NANG;
+        const int il = (p.wl1 > p.wl2) ? p.ilam1 : p.ilam1 + 1;
+        const size_t k = (size_t)il * (TP_NANG + 1) + ia;
+        const double wangle = 1.0 / ((double)ia / (double)TP_NANG - (double)(ia - 1) / (double)TP_NANG);
+        const double add = ((wangle * p.E) * m.wlam[il]) / m.nruns_d;
+        tp_add(&A.spec[k], add);
+        tp_addi(&A.ispec[k], 1);
+        if (p.scatt) tp_add(&A.scatspec[k], add);
+        return;
+      }
+      f_interact<R>(m, A, r, p, L);
+      if (m.maxinteract > 0) {
+        if (px_next(r) < 1.0 / (double)m.maxinteract) {
+          L.cnt[TC_OVERFLOW]++;
+          return;
+        }
+        p.E = (p.E * (double)m.maxinteract) / (double)(m.maxinteract - 1);
+      }
+      tau = -log(px_next(r));
+    }
+  }
+}
+
+#endif /* MCMAX_TRANSPORT_FAST_CUH */

@@ -98,6 +98,7 @@ typedef struct {
   const double *KabsTot;  /* ncell*nlam */
   const double *KscaTot;  /* ncell*nlam */
   const double *KpCell;   /* ncell*(TMAX+1): sum_grains Kp w wopac */
+  int kp_uniform;         /* 1: KpCell has one row shared by all cells */
   const double *BB;       /* nlam*(TMAX+1) */
   const double *Fstar;    /* nlam */
   double Lstar;
@@ -112,9 +113,11 @@ typedef struct {
   const double *sinthet;   /* 180: sin(pi*(i-0.5)/180) */
   const double *cos2phi;   /* 361 */
   const double *sin2phi;   /* 361 */
-  /* random walk */
-  const double *KDext;     /* ncell*(TMAX+1), may be NULL when rw == 0 */
-  const double *KDabs;     /* ncell*(TMAX+1) */
+  /* random walk: per-cell diffusion tables, or NULL to evaluate
+   * DiffCoeffCell lazily per cell as the reference does (g_comp needed) */
+  const double *KDext;     /* ncell*(TMAX+1) or NULL */
+  const double *KDabs;     /* ncell*(TMAX+1) or NULL */
+  const double *g_comp;    /* ncomp*nlam asymmetry parameters, for lazy tables */
   const double *rw_y;      /* 1000 */
   const double *rw_phi;    /* 1000 */
 } orc_model;

@@ -77,6 +77,7 @@ typedef struct {
   double *Tcell;
   int *lastphot;
   int *iTD;
+  double *kdext, *kdabs;
   double nEJv;
 } mc_t;
 
@@ -402,7 +403,7 @@ static void interact(mc_t *s, rng_t *r, orc_phot *p) {
     p->Q = 0.0;
     p->U = 0.0;
     p->V = 0.0;
-    const double *kp = m->KpCell + (size_t)c * (ORC_TMAX + 1);
+    const double *kp = m->KpCell + (m->kp_uniform ? (size_t)0 : (size_t)c * (ORC_TMAX + 1));
     s->out->Eabs[c] = s->out->Eabs[c] + (p->E * (KabsTot - 0.0)) / KabsTot;
     double T0 = s->Tcell[c];
     double T1 = orc_increase_t(kp, s->out->Eabs[c] / s->mass[c], T0);
@@ -551,6 +552,34 @@ static void hunt(const double *xx, int n, double x, int *jlo) {
   if (x == xx[0]) *jlo = 1;
 }
 
+/* DiffCoeffCell (Dtable.f:97-182) for one cell and one iT */
+static void orc_diffcoeff_one(const orc_model *m, int c, int iT, int scattering, double *kdext, double *kdabs) {
+  const int nlam = m->nlam, TT = ORC_TMAX + 1;
+  const double *Ka = m->KabsTot + (size_t)c * nlam, *Ks = m->KscaTot + (size_t)c * nlam;
+  const double *w = m->comp_w + (size_t)c * m->ncomp;
+  double int1 = 0.0, int2 = 0.0, int3 = 0.0, b0 = 0.0, e0 = 0.0, a0 = 0.0;
+  for (int l = 0; l < nlam; ++l) {
+    double g = 0.0;
+    for (int q = 0; q < m->ncomp; ++q) g = g + (m->g_comp[(size_t)q * nlam + l] * m->Ksca_comp[(size_t)q * nlam + l]) * w[q];
+    g = g / Ks[l];
+    if (!scattering) g = 0.0;
+    double Kext = Ka[l] + Ks[l];
+    double b1 = m->BB[(size_t)l * TT + iT + 1] - m->BB[(size_t)l * TT + iT];
+    double e1 = b1 / (Kext - (g * g) * Ks[l]), a1 = b1 * (Ka[l] - 0.0);
+    if (l > 0) {
+      double dh = fabs(m->nu[l - 1] - m->nu[l]) * 0.5;
+      int1 = int1 + dh * (e0 + e1);
+      int2 = int2 + dh * (b0 + b1);
+      int3 = int3 + dh * (a0 + a1);
+    }
+    b0 = b1;
+    e0 = e1;
+    a0 = a1;
+  }
+  *kdext = int2 / int1;
+  *kdabs = int3 / int2;
+}
+
 /* RandomWalk.f:47-147 (thermal contact); returns 1 when a step was taken */
 static int random_walk(mc_t *s, rng_t *r, orc_phot *p, double dmin) {
   const orc_model *m = s->m;
@@ -559,14 +588,27 @@ static int random_walk(mc_t *s, rng_t *r, orc_phot *p, double dmin) {
   if (iT == 0) iT = 1;
   if (iT > ORC_TMAX) iT = ORC_TMAX;
   if (iT > ORC_TMAX - 1) iT = ORC_TMAX - 1; /* DiffCoeffCell clamp */
-  double Kext = m->KDext[(size_t)c * (ORC_TMAX + 1) + iT];
+  double Kext, KabsD;
+  if (m->KDext) {
+    Kext = m->KDext[(size_t)c * (ORC_TMAX + 1) + iT];
+    KabsD = m->KDabs[(size_t)c * (ORC_TMAX + 1) + iT];
+  } else {
+    /* DiffCoeffCell only when the cell's temperature step changed
+     * (RandomWalk.f:61, Dtable.f:97-182) */
+    if (s->iTD[c] != iT) {
+      orc_diffcoeff_one(m, c, iT, s->scattering, &s->kdext[c], &s->kdabs[c]);
+      s->iTD[c] = iT;
+    }
+    Kext = s->kdext[c];
+    KabsD = s->kdabs[c];
+  }
   double lr = 1.0 / ((AU_CM * Kext) * m->dens[c]);
   if (dmin <= s->factRW * lr) return 0;
   double x = rnd(r);
   int iy = 1;
   hunt(m->rw_phi, NY_RW, x, &iy);
   double v = (((-3.0 * dm_log(m->rw_y[iy - 1])) * (dmin * dmin)) / (lr * (PI_D * PI_D)));
-  double Kabs = m->KDabs[(size_t)c * (ORC_TMAX + 1) + iT];
+  double Kabs = KabsD;
   randomdirection(r, &p->vx, &p->vy, &p->vz);
   p->x = p->x + dmin * p->vx;
   p->y = p->y + dmin * p->vy;
@@ -575,7 +617,7 @@ static int random_walk(mc_t *s, rng_t *r, orc_phot *p, double dmin) {
   s->out->Eabs[c] = s->out->Eabs[c] + (EJv * Kabs) * m->dens[c];
   s->out->EJv[c] = s->out->EJv[c] + EJv * Kabs;
   s->nEJv = s->nEJv + EJv * Kabs;
-  const double *kp = m->KpCell + (size_t)c * (ORC_TMAX + 1);
+  const double *kp = m->KpCell + (m->kp_uniform ? (size_t)0 : (size_t)c * (ORC_TMAX + 1));
   s->Tcell[c] = orc_increase_t(kp, s->out->Eabs[c] / s->mass[c], s->Tcell[c]);
   s->out->tautot += v / dmin;
   s->out->counters[4]++;
@@ -679,6 +721,9 @@ int orc_mcradiation(const orc_model *m, const orc_run *run, orc_result *out) {
   S.mass = (double *)malloc(sizeof(double) * ncell);
   S.Tcell = (double *)calloc(ncell, sizeof(double));
   S.lastphot = (int *)calloc(ncell, sizeof(int));
+  S.iTD = (int *)calloc(ncell, sizeof(int));
+  S.kdext = (double *)calloc(ncell, sizeof(double));
+  S.kdabs = (double *)calloc(ncell, sizeof(double));
   for (int c = 0; c < ncell; ++c) S.mass[c] = m->dens[c] * m->V[c];
   /* the transport floors the dust density at 1e-50 (CheckMinimumDensity,
    * DiskStructure.f:2966-2979) after the mass was formed */
@@ -812,5 +857,33 @@ int orc_mcradiation(const orc_model *m, const orc_run *run, orc_result *out) {
   free(S.mass);
   free(S.Tcell);
   free(S.lastphot);
+  free(S.iTD);
+  free(S.kdext);
+  free(S.kdabs);
   return status;
+}
+
+/* InitRandomWalk thick flags (RandomWalk.f:172-190): a cell i >= 1 is thick
+ * when its radial width exceeds factRW mean free paths 1/(AU KDext dens) at
+ * any of iT = 100, 600, 1100, 1600. */
+void orc_init_random_walk(const orc_model *m, int scat_how, double factRW, uint8_t *thick) {
+  const int nc = m->nt - 1, ncell = m->nr * nc;
+  int scattering = 0;
+  if (scat_how != 0)
+    for (size_t k = 0; k < (size_t)ncell * m->nlam; ++k)
+      if (m->KscaTot[k] != 0.0) {
+        scattering = 1;
+        break;
+      }
+  for (int c = 0; c < ncell; ++c) {
+    int i = c / nc;
+    thick[c] = 0;
+    if (i < 1) continue;
+    for (int iT = 100; iT <= 1600; iT += 500) {
+      double kdext, kdabs;
+      orc_diffcoeff_one(m, c, iT, scattering, &kdext, &kdabs);
+      double lr = 1.0 / ((AU_CM * kdext) * m->dens[c]);
+      if ((m->R[i + 1] - m->R[i]) > factRW * lr) thick[c] = 1;
+    }
+  }
 }

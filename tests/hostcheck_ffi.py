@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "native", "hostcheck.cpp")
 LIB = os.path.join(HERE, "native", "libhostcheck.so")
 DEPS = [SRC] + [os.path.join(HERE, "..", "mcmax_b200", "csrc", f) for f in
-                ("dhs_core.cuh", "transport_core.cuh", "detmath.h", "cplx.h", "philox.h")]
+                ("dhs_core.cuh", "transport_core.cuh", "transport_fast.cuh", "detmath.h", "cplx.h", "philox.h")]
 
 
 class HcModel(C.Structure):
@@ -56,7 +56,11 @@ def mie_sample(rad, lam, e1, e2):
     return e, cs.value, ce.value, F.reshape(4, 180)
 
 
-def mcradiation(model, tables, nphot, seed=1, randomwalk=False, factRW=10.0, maxinteract=0):
+def mcradiation(model, tables, nphot, seed=1, randomwalk=False, factRW=10.0, maxinteract=0, fast=None, first=0,
+                count=None):
+    """Serial host replay of the device packet loop.  fast=None: the
+    reference-order kernel; fast='fp64' / 'mixed': the GPU-ordered kernel
+    (uniform mixtures), packets [first, first+count)."""
     L = load()
     m, t = model, tables
     keep = {}
@@ -82,8 +86,12 @@ def mcradiation(model, tables, nphot, seed=1, randomwalk=False, factRW=10.0, max
                spec=np.zeros(ns), scatspec=np.zeros(ns), ispec=np.zeros(ns, np.int32))
     cnt = (C.c_ulonglong * 16)()
     tau = C.c_double(0.0)
-    L.hc_mcradiation(C.byref(h), *[P(out[k]) for k in ("EJv", "EJv2", "Eabs", "T", "Ni", "spec", "scatspec", "ispec")],
-                     cnt, C.byref(tau))
+    if fast is None:
+        L.hc_mcradiation(C.byref(h), *[P(out[k]) for k in ("EJv", "EJv2", "Eabs", "T", "Ni", "spec", "scatspec",
+                                                           "ispec")], cnt, C.byref(tau))
+    else:
+        L.hc_fast(C.byref(h), int(fast == "mixed"), *[P(out[k]) for k in ("EJv", "EJv2", "Eabs", "T", "Ni", "spec")],
+                  cnt, C.byref(tau), C.c_int64(first), C.c_int64(nphot if count is None else count))
     out["counters"] = np.array(cnt[:], np.int64)
     out["tautot"] = tau.value
     for k in ("spec", "scatspec", "ispec"):

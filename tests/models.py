@@ -15,6 +15,22 @@ def small_disk(nrad=20, ntheta=12, nlam=30, ngrains=3, ns=2, nf=4, mdust=1e-5, s
            blend, porosity, fmax)
     if key in cache:
         return cache[key]
+    import hashlib
+    import os
+    import tempfile
+    fn = os.path.join(tempfile.gettempdir(), "mcmax_test_models",
+                      hashlib.sha1(repr(key).encode()).hexdigest()[:16] + ".npz")
+    if os.path.exists(fn):
+        z = np.load(fn, allow_pickle=False)
+        d = {k: z[k] for k in z.files}
+        for k in ("nr", "nt", "ncomp", "nlam", "scat_how"):
+            d[k] = int(d[k])
+        for k in ("Lstar", "Tstar", "Rstar_cm"):
+            d[k] = float(d[k])
+        d["bins"] = [tuple(b) for b in d["bins"]]
+        mdl = M.Model(**d)
+        cache[key] = mdl
+        return mdl
     lam, nu = M.wavelength_grid(0.1, lam2, nlam)
     n, k = M.synthetic_lnk(lam, kpref)
     bins = M.grain_bins(amin, amax, ngrains)
@@ -44,4 +60,10 @@ def small_disk(nrad=20, ntheta=12, nlam=30, ngrains=3, ns=2, nf=4, mdust=1e-5, s
                   nu=nu, Kabs=np.array(Kabs), Ksca=Ksca, F=np.array(F), BB=BB, Fstar=Fstar, Lstar=Lstar,
                   Tstar=tstar, Rstar_cm=rstar_cm, scat_how=scat_how, bins=bins, w=w)
     cache[key] = mdl
+    try:
+        os.makedirs(os.path.dirname(fn), exist_ok=True)
+        np.savez(fn + ".tmp.npz", **{k: np.asarray(v) for k, v in mdl.__dict__.items()})
+        os.replace(fn + ".tmp.npz", fn)
+    except OSError:
+        pass
     return mdl

@@ -113,9 +113,15 @@ int hc_mcradiation(const HcModel *h, double *EJv, double *EJv2, double *Eabs, do
     nothick.assign(ncell, 0);
     m.thick = nothick.data();
   }
-  std::vector<int> lastphot(ncell, 0);
-  unsigned long long next = 0;
+  std::vector<int> lastphot(ncell, 0), kp_hint(ncell, 0);
+  unsigned long long next = 0, done = 0, tmark[8] = {0};
   TAcc A;
+  memset(&A, 0, sizeof A);
+  A.kp_hint = kp_hint.data();
+  A.run_packets = h->nphot;
+  A.ncell = ncell;
+  A.done = &done;
+  A.tmark = tmark;
   A.EJv = EJv; A.EJv2 = EJv2; A.Eabs = Eabs; A.T = T; A.Ni = Ni; A.lastphot = lastphot.data();
   A.spec = spec; A.scatspec = scatspec; A.ispec = ispec; A.counters = counters; A.tautot = tautot; A.next = &next;
   TLocal L;
@@ -123,8 +129,170 @@ int hc_mcradiation(const HcModel *h, double *EJv, double *EJv2, double *Eabs, do
   // with uniform_mix the KpCell table has a single row
   if (h->uniform_mix) m.KpCell = h->KpCell;
   for (int64_t pid = 0; pid < h->nphot; ++pid) tp_run_packet(m, A, pid, L);
-  for (int k = 0; k < TC_N; ++k) counters[k] += L.cnt[k];
+  for (int k = 0; k < TC_N; ++k) counters[k] += (unsigned long long)L.cnt[k];
   *tautot += L.tautot;
   return 0;
 }
+}
+
+extern "C" {
+void hc_detmath(int which, int n, const double *x, double *y) {
+  for (int i = 0; i < n; ++i) {
+    switch (which) {
+      case 0: y[i] = dm_exp(x[i]); break;
+      case 1: y[i] = dm_log(x[i]); break;
+      case 2: y[i] = dm_sin(x[i]); break;
+      default: y[i] = dm_cos(x[i]); break;
+    }
+  }
+}
+
+void hc_philox(const uint32_t *ctr, const uint32_t *key, uint32_t *out) { px_philox4x32_10(ctr, key, out); }
+
+double hc_tinv(const double *kp, double E1, int lo) {
+  int ib;
+  return tp_tinv(kp, E1, lo, &ib);
+}
+}
+
+// ---------------------------------------------------------------------------
+// host build of the GPU-ordered kernel (transport_fast.cuh) with host-built
+// tables identical to the device table builders
+#include "../../mcmax_b200/csrc/transport_fast.cuh"
+
+template <class R>
+static int hc_fast_impl(const HcModel *h, int nruns_unused, double *EJv, double *EJv2, double *Eabs, double *T, int *Ni,
+                        double *spec, unsigned long long *counters, double *tautot, int64_t first, int64_t count) {
+  (void)nruns_unused;
+  const int nc = h->nt - 1, ncell = h->nr * nc, nlam = h->nlam, n = nlam - 1, ncomp = h->ncomp;
+  std::vector<double> dens(ncell), mass(ncell), dnu(n), star_cdf(n), wlam(nlam);
+  for (int c = 0; c < ncell; ++c) {
+    mass[c] = h->dens[c] * h->V[c];
+    dens[c] = h->dens[c] <= 1e-50 ? 1e-50 : h->dens[c];
+  }
+  for (int i = 0; i < n; ++i) dnu[i] = std::fabs(h->nu[i] - h->nu[i + 1]) * 0.5;
+  double Lt = 0.0;
+  for (int i = 0; i < n; ++i) {
+    Lt = Lt + dnu[i] * (h->Fstar[i] + h->Fstar[i + 1]);
+    star_cdf[i] = Lt;
+  }
+  for (int i = 0; i < nlam; ++i)
+    wlam[i] = i == 0 ? -1e23 / (h->nu[1] / 2.0)
+                     : (i == nlam - 1 ? -1e23 / ((h->nu[nlam - 1] - h->nu[nlam - 2]) / 2.0)
+                                      : -1e23 / ((h->nu[i + 1] - h->nu[i - 1]) / 2.0));
+  const double *K = h->KabsTot;
+  std::vector<double> C((size_t)TP_TT * n), D((size_t)TP_TMAX * n);
+  for (int iT = 0; iT <= TP_TMAX; ++iT) {
+    double L = 0.0, s0 = h->BB[iT] * K[0];
+    for (int i = 0; i < n; ++i) {
+      double s1 = h->BB[(size_t)(i + 1) * TP_TT + iT] * K[i + 1];
+      L = L + dnu[i] * (s0 + s1);
+      C[(size_t)iT * n + i] = L;
+      s0 = s1;
+    }
+  }
+  for (int iT = 0; iT < TP_TMAX; ++iT) {
+    double L = 0.0, s0 = (h->BB[iT + 1] - h->BB[iT]) * K[0];
+    for (int i = 0; i < n; ++i) {
+      const double *B = h->BB + (size_t)(i + 1) * TP_TT;
+      double s1 = (B[iT + 1] - B[iT]) * K[i + 1];
+      L = L + dnu[i] * (s0 + s1);
+      D[(size_t)iT * n + i] = L;
+      s0 = s1;
+    }
+  }
+  std::vector<unsigned short> eG((size_t)TP_TMAX * F_NGUIDE);
+  for (int iT = 0; iT < TP_TMAX; ++iT) {
+    const double *row = &D[(size_t)iT * n];
+    int i = 0;
+    for (int g = 0; g < F_NGUIDE; ++g) {
+      const double v = row[n - 1] * (double)g / (double)F_NGUIDE;
+      while (i < n - 1 && !(row[i] >= v)) ++i;
+      eG[(size_t)iT * F_NGUIDE + g] = (unsigned short)i;
+    }
+  }
+  const int nmat = ncomp * nlam;
+  std::vector<R> A((size_t)nmat * 180), B((size_t)nmat * 180), F6((size_t)nmat * 1080);
+  std::vector<unsigned char> sG((size_t)nmat * F_NGUIDE);
+  for (int k = 0; k < nmat; ++k) {
+    const double *F11 = h->F_c + (size_t)k * 1080, *F12 = F11 + 180;
+    double a = 0.0, b = 0.0;
+    for (int j = 0; j < 180; ++j) {
+      a += (TP_PI * h->sinthet[j]) * F11[j];
+      b += (TP_PI * h->sinthet[j]) * F12[j];
+      A[(size_t)k * 180 + j] = (R)a;
+      B[(size_t)k * 180 + j] = (R)b;
+    }
+    for (int e = 0; e < 1080; ++e) F6[(size_t)k * 1080 + e] = (R)h->F_c[(size_t)k * 1080 + e];
+    int i = 0;
+    for (int g = 0; g < F_NGUIDE; ++g) {
+      const R v = A[(size_t)k * 180 + 179] * (R)g / (R)F_NGUIDE;
+      while (i < 179 && !(A[(size_t)k * 180 + i] > v)) ++i;
+      sG[(size_t)k * F_NGUIDE + g] = (unsigned char)i;
+    }
+  }
+  std::vector<double> c2(181), s2(181), ly(TP_NY);
+  c2[0] = s2[0] = 0.0;
+  for (int k = 1; k <= 180; ++k) {
+    c2[k] = c2[k - 1] + h->cos2phi[k];
+    s2[k] = s2[k - 1] + h->sin2phi[k];
+  }
+  for (int i = 0; i < TP_NY; ++i) ly[i] = std::log(h->rw_y[i]);
+  std::vector<R> KaR(nlam), KeR(nlam), KsR((size_t)nmat);
+  for (int l = 0; l < nlam; ++l) {
+    KaR[l] = (R)h->KabsTot[l];
+    KeR[l] = (R)(h->KabsTot[l] + h->KscaTot[l]);
+  }
+  for (int k = 0; k < nmat; ++k) KsR[k] = (R)h->Ksca_c[k];
+  std::vector<int> kd_index(ncell, -1);
+  for (int c = 0; c < ncell; ++c)
+    if (h->thick && h->thick[c]) kd_index[c] = c;
+  std::vector<unsigned char> nothick(ncell, 0);
+  FModel<R> m;
+  memset(&m, 0, sizeof m);
+  m.nr = h->nr; m.nt = h->nt; m.nc = nc; m.ncell = ncell; m.nlam = nlam; m.ncomp = ncomp;
+  m.scat_how = h->scat_how;
+  for (size_t k = 0; k < (size_t)nlam && h->scat_how; ++k)
+    if (h->KscaTot[k] != 0.0) m.scattering = 1;
+  m.uniform_mix = 1;
+  m.rw = h->rw;
+  m.factRW = h->factRW;
+  m.R0 = h->R[0];
+  m.Lstar = h->Lstar;
+  m.Epkt = h->Lstar / ((double)h->nphot * 1.0);
+  m.nruns_d = 1.0;
+  m.nphot = h->nphot;
+  m.maxinteract = h->maxinteract;
+  m.seed = h->seed;
+  m.Rr = h->R; m.Theta = h->Theta; m.SinTheta = h->SinTheta; m.star_cdf = star_cdf.data();
+  m.KabsRow = KaR.data(); m.KextRow = KeR.data(); m.Ksca_c = KsR.data();
+  m.c2cum = c2.data(); m.s2cum = s2.data();
+  m.dens = dens.data(); m.mass = mass.data(); m.wlam = wlam.data();
+  m.KabsTot = h->KabsTot; m.BB = h->BB; m.dnu_half = dnu.data(); m.KpCell = h->KpCell;
+  m.Ccum = C.data(); m.Dcum = D.data(); m.comp_w = h->comp_w;
+  m.scatA = A.data(); m.scatB = B.data(); m.F6 = F6.data(); m.IF_c = h->IF_c;
+  m.scatG = sG.data(); m.emitG = eG.data();
+  m.KDext = h->KDext; m.KDabs = h->KDabs; m.rw_logy = ly.data(); m.rw_phi = h->rw_phi;
+  m.kd_index = kd_index.data(); m.thick = h->thick ? h->thick : nothick.data();
+  std::vector<int> lastphot(ncell, 0), kp_hint(ncell, 0), ispec((size_t)nlam * 31, 0);
+  std::vector<double> scatspec((size_t)nlam * 31, 0.0);
+  unsigned long long next = 0, done = 0, tmark[8] = {0};
+  TAcc Ac;
+  memset(&Ac, 0, sizeof Ac);
+  Ac.EJv = EJv; Ac.EJv2 = EJv2; Ac.Eabs = Eabs; Ac.T = T; Ac.Ni = Ni; Ac.lastphot = lastphot.data();
+  Ac.kp_hint = kp_hint.data(); Ac.spec = spec; Ac.scatspec = scatspec.data(); Ac.ispec = ispec.data();
+  Ac.counters = counters; Ac.tautot = tautot; Ac.next = &next; Ac.run_packets = h->nphot; Ac.ncell = ncell;
+  Ac.done = &done; Ac.tmark = tmark;
+  TLocal L;
+  memset(&L, 0, sizeof L);
+  for (int64_t pid = first; pid < first + count; ++pid) f_run_packet<R>(m, Ac, pid, L);
+  for (int k = 0; k < TC_N; ++k) counters[k] += (unsigned long long)L.cnt[k];
+  *tautot += L.tautot;
+  return 0;
+}
+
+extern "C" int hc_fast(const HcModel *h, int mixed, double *EJv, double *EJv2, double *Eabs, double *T, int *Ni,
+                       double *spec, unsigned long long *counters, double *tautot, int64_t first, int64_t count) {
+  if (mixed) return hc_fast_impl<float>(h, 1, EJv, EJv2, Eabs, T, Ni, spec, counters, tautot, first, count);
+  return hc_fast_impl<double>(h, 1, EJv, EJv2, Eabs, T, Ni, spec, counters, tautot, first, count);
 }

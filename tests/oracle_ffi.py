@@ -31,10 +31,10 @@ def P(a):
 class OrcModel(C.Structure):
     _fields_ = [("nr", C.c_int), ("nt", C.c_int), ("R", dp), ("Theta", dp), ("SinTheta", dp),
                 ("dens", dp), ("V", dp), ("thick", u8p), ("nlam", C.c_int), ("lam", dp), ("nu", dp),
-                ("KabsTot", dp), ("KscaTot", dp), ("KpCell", dp), ("BB", dp), ("Fstar", dp),
+                ("KabsTot", dp), ("KscaTot", dp), ("KpCell", dp), ("kp_uniform", C.c_int), ("BB", dp), ("Fstar", dp),
                 ("Lstar", C.c_double), ("ncomp", C.c_int), ("comp_w", dp), ("Ksca_comp", dp),
                 ("F_comp", dp), ("IF_comp", dp), ("sinthet", dp), ("cos2phi", dp), ("sin2phi", dp),
-                ("KDext", dp), ("KDabs", dp), ("rw_y", dp), ("rw_phi", dp)]
+                ("KDext", dp), ("KDabs", dp), ("g_comp", dp), ("rw_y", dp), ("rw_phi", dp)]
 
 
 class OrcRun(C.Structure):
@@ -133,7 +133,7 @@ def bb_table(lam):
     return BB
 
 
-def transport_tables(model, randomwalk=False, factRW=10.0):
+def transport_tables(model, randomwalk=False, factRW=10.0, lazy_kd=False):
     """Every table the oracle transport reads, built by the oracle's own
     table builders (Init.f / MCRadiation.f / Dtable.f restatements)."""
     L = load()
@@ -149,8 +149,17 @@ def transport_tables(model, randomwalk=False, factRW=10.0):
     L.orc_kp_table(nlam, P(nu), P(BB), ncomp, P(Kabs), P(Kp))
     KabsTot = np.zeros((ncell, nlam))
     KscaTot = np.zeros((ncell, nlam))
+    uniform = bool(np.all(comp_w == comp_w[0]))
     KpCell = np.zeros((ncell, TT))
-    L.orc_cell_tables(ncell, ncomp, nlam, P(comp_w), P(Kabs), P(Ksca), P(Kp), P(KabsTot), P(KscaTot), P(KpCell))
+    if uniform:
+        # one Planck-mean row serves every cell (identical mixtures)
+        KpCell = np.zeros((1, TT))
+        kt_a, kt_s = np.zeros((1, nlam)), np.zeros((1, nlam))
+        L.orc_cell_tables(1, ncomp, nlam, P(comp_w), P(Kabs), P(Ksca), P(Kp), P(kt_a), P(kt_s), P(KpCell))
+        KabsTot = np.ascontiguousarray(np.broadcast_to(kt_a, (ncell, nlam)))
+        KscaTot = np.ascontiguousarray(np.broadcast_to(kt_s, (ncell, nlam)))
+    else:
+        L.orc_cell_tables(ncell, ncomp, nlam, P(comp_w), P(Kabs), P(Ksca), P(Kp), P(KabsTot), P(KscaTot), P(KpCell))
     sinthet = np.array([np.nan] * 180)
     cos2phi = np.zeros(361)
     sin2phi = np.zeros(361)
@@ -162,9 +171,20 @@ def transport_tables(model, randomwalk=False, factRW=10.0):
     L.orc_g_table(ncomp * nlam, P(F), P(g))
     rw_y, rw_phi = np.zeros(1000), np.zeros(1000)
     L.orc_rw_table(P(rw_y), P(rw_phi))
-    out = dict(Kp=Kp, KabsTot=KabsTot, KscaTot=KscaTot, KpCell=KpCell, sinthet=sinthet, cos2phi=cos2phi,
+    out = dict(kp_uniform=int(uniform), Kp=Kp, KabsTot=KabsTot, KscaTot=KscaTot, KpCell=KpCell, sinthet=sinthet, cos2phi=cos2phi,
                sin2phi=sin2phi, IF=IF, g=g, rw_y=rw_y, rw_phi=rw_phi, thick=None, KDext=None, KDabs=None)
-    if randomwalk:
+    if randomwalk and lazy_kd:
+        # thick flags only; DiffCoeffCell is evaluated lazily inside the run
+        thick = np.zeros(ncell, np.uint8)
+        keep = [np.ascontiguousarray(a, float) for a in (m.R, m.Theta, m.SinTheta, m.dens, m.V, m.lam, m.BB, m.Fstar,
+                                                         Ksca, m.F)]
+        om = OrcModel(m.nr, m.nt, P(keep[0]), P(keep[1]), P(keep[2]), P(keep[3]), P(keep[4]), None, nlam,
+                      P(keep[5]), P(nu), P(KabsTot), P(KscaTot), P(KpCell), int(uniform), P(keep[6]), P(keep[7]), float(m.Lstar),
+                      ncomp, P(comp_w), P(keep[8]), P(keep[9]), P(IF), P(sinthet), P(cos2phi), P(sin2phi), None, None,
+                      P(g), P(rw_y), P(rw_phi))
+        L.orc_init_random_walk(C.byref(om), int(m.scat_how), C.c_double(factRW), P(thick))
+        out.update(thick=thick)
+    elif randomwalk:
         scattering = int(m.scat_how != 0 and np.any(KscaTot != 0))
         KDext = np.zeros((ncell, TT))
         KDabs = np.zeros((ncell, TT))
@@ -199,11 +219,11 @@ def mcradiation(model, nphot, seed=1, randomwalk=False, factRW=10.0, maxinteract
     om = OrcModel(m.nr, m.nt, A("R", m.R), A("Theta", m.Theta), A("SinTheta", m.SinTheta), A("dens", m.dens),
                   A("V", m.V), A("thick", t["thick"], np.uint8) if t["thick"] is not None else None, m.nlam,
                   A("lam", m.lam), A("nu", m.nu), A("KabsTot", t["KabsTot"]), A("KscaTot", t["KscaTot"]),
-                  A("KpCell", t["KpCell"]), A("BB", m.BB), A("Fstar", m.Fstar), float(m.Lstar), m.ncomp,
+                  A("KpCell", t["KpCell"]), int(t["kp_uniform"]), A("BB", m.BB), A("Fstar", m.Fstar), float(m.Lstar), m.ncomp,
                   A("comp_w", m.comp_w), A("Ksca", m.Ksca), A("F", m.F), A("IF", t["IF"]),
                   A("sinthet", t["sinthet"]), A("cos2phi", t["cos2phi"]), A("sin2phi", t["sin2phi"]),
                   A("KDext", t["KDext"]) if t["KDext"] is not None else None,
-                  A("KDabs", t["KDabs"]) if t["KDabs"] is not None else None, A("rw_y", t["rw_y"]),
+                  A("KDabs", t["KDabs"]) if t["KDabs"] is not None else None, A("g", t["g"]), A("rw_y", t["rw_y"]),
                   A("rw_phi", t["rw_phi"]))
     run = OrcRun(int(nphot), int(seed), int(m.scat_how), int(bool(randomwalk)), float(factRW), int(maxinteract),
                  int(rng), int(idum))
