@@ -1,0 +1,70 @@
+"""Host-side set-up: keyword decks, refractive-index regridding, grids,
+densities and size distributions."""
+import math
+import os
+
+import numpy as np
+
+from mcmax_b200 import model as M
+
+
+def test_parse_deck_surface():
+    txt = """* a comment line
+Tstar=10000   * inline
+rstar = 2.5
+computepart01:file='dust.lnk'
+scattype='FULL'
+NRAD=100
+"""
+    d = M.parse_deck(txt, overrides=["nrad=200", "factrw=5"])
+    assert d["tstar"] == "10000" and d["rstar"] == "2.5"
+    assert d["computepart01:file"] == "dust.lnk"
+    assert d["scattype"] == "FULL"
+    assert d["nrad"] == "200" and M.deck_value(d, "factrw", 10.0) == 5.0
+    assert M.deck_value(d, "missing", 3.0) == 3.0
+
+
+def test_readrefind_regrid_and_extrapolation(tmp_path):
+    p = tmp_path / "a.lnk"
+    p.write_text("0.1 1.5 0.1\n1.0 1.6 0.05\n10.0 1.8 0.02\n")
+    grid = np.array([0.05, 0.1, 0.5, 1.0, 5.0, 10.0, 100.0])
+    n, k = M.readrefind(str(p), grid)
+    assert n[0] == 1.5 and k[0] == 0.1          # below the table: first row
+    assert n[3] == 1.6 and abs(k[3] - 0.05) < 1e-15
+    assert 1.5 < n[2] < 1.6                     # log-log interpolation
+    assert n[-1] == n[-2] and abs(k[-1] - k[-2] * 10 / 100) < 1e-15  # dielectric extrapolation
+
+
+def test_particle_file(tmp_path):
+    (tmp_path / "a.lnk").write_text("0.1 1.5 0.1\n10 1.6 0.05\n")
+    pf = tmp_path / "part.in"
+    pf.write_text("* sizes\n5\n20\n'a.lnk'\n1.0 3.0\n")
+    ns, nf, mats = M.read_particle_file(str(pf))
+    assert ns == 5 and nf == 20 and mats[0][1:] == (1.0, 3.0)
+    assert mats[0][0].endswith("a.lnk")
+
+
+def test_spatial_grid_and_density():
+    R, Th, thet, ST = M.spatial_grid(2.5 * M.RSUN, 0.5, 100.0, 20, 12)
+    assert R.size == 22 and Th.size == 13
+    assert Th[0] == 1.0 and Th[-1] == 0.0 and np.all(np.diff(Th) < 0)
+    assert np.all(np.diff(R) > 0) and abs(R[1] - 0.5) < 1e-12 and abs(R[-1] - 100) < 1e-9
+    dens, V = M.zones_density(R, Th, thet, [dict(rin=0.5, rout=100, mdust=1e-5, denspow=1, sh=0.07, rsh=1,
+                                                 shpow=1.125)])
+    mass = (dens[1:] * V[1:]).sum()
+    assert abs(mass / (1e-5 * M.MSUN) - 1) < 1e-6
+    assert np.all(dens[0] == 1e-60)
+    # cells cover one hemisphere and count its mirror (Init.f:3073): the
+    # volumes add up to the full spherical shell
+    vol = V.sum()
+    full = 4 * math.pi / 3 * (R[-1] ** 3 - R[0] ** 3) * M.AU ** 3
+    assert abs(vol / full - 1) < 1e-12
+
+
+def test_mrn_abundances():
+    bins = M.grain_bins(0.1, 1.0, 20)
+    assert abs(bins[0][0] - 0.1) < 1e-15 and abs(bins[-1][1] - 1.0) < 1e-12
+    rg = [math.sqrt(a * b) * 1e-4 for a, b in bins]
+    w = M.mrn_abundances(rg, 0.1e-4, 1e-4, 3.5)
+    assert abs(w.sum() - 1) < 1e-9 and np.all(w > 0)
+    assert w[-1] > w[0]  # a^-3.5: mass in the large grains
