@@ -1,6 +1,6 @@
-"""Packets/s of the MCMax photon-packet loop on B200 (configs[1] workload).
+"""Packets/s of the MCMax photon-packet loop on B200.
 
-Workload (configs[1], "precision" deck): star Teff = 10000 K, R* = 2.5 Rsun;
+Workload (the "precision" disk deck): star Teff = 10000 K, R* = 2.5 Rsun;
 ZONES disk Rin = 0.5 AU, Rout = 100 AU, Sigma ~ r^-1, Mdust = 1e-3 Msun,
 H/R = 0.05 at 1 AU (MCMax scale height sh = 0.05*sqrt(2)), flaring 1.125;
 grid nr = 200 x ntheta = 120 (+ the star cell), nlam = 200 from 0.1 to 3000
@@ -9,13 +9,19 @@ micron; one synthetic .lnk composition, MRN 0.1-1 micron in 20 bins (5 sizes,
 Mueller scattering, Bjorkman-Wood re-emission, modified random walk
 (factRW = 10).  Opacities come from the library's own DHS kernels.
 
-One step = one MCRadiation call over `--nphot` packets (default 1e7; the deck's
-1e8 packets are ten steps).  `value` is device time of the transport kernel
-with all tables resident in HBM; `e2e` times the reference-facing C-ABI
+One step = one MCRadiation call over the deck's 1e8 packets (`--nphot`), with
+the reference's overflow roulette switched on at maxinteract = 1e5 (keyword
+'maxinteract', MCRadiation.f:568-571: an energy-compensated kill with
+probability 1/maxinteract per interaction).  Without it a few packets
+trapped in the optically thick midplane take 1e8+ events each (the CPU
+reference pays the same events serially; on the GPU they become the critical
+path of the launch).  `value` is the device time of the transport kernel with
+all tables resident in HBM; `e2e` times the reference-facing C-ABI
 (mcg_set_model from host buffers + mcg_mcradiation + result copies to host).
 
---impl reference runs the CPU restatement of the reference's loop (the
-checker; the Fortran reference cannot be compiled here) on all host cores.
+--impl reference runs the oracle (the CPU restatement of the reference's
+loop; the Fortran reference cannot be compiled without a Fortran compiler) on
+all host cores.
 """
 import argparse
 import json
@@ -30,10 +36,10 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-NPHOT_DEFAULT = 10_000_000
+NPHOT_DEFAULT = 100_000_000
 WORKLOAD = dict(mdust=1e-3, nrad=200, ntheta=120, nlam=200, lam1=0.1, lam2=3000.0, ngrains=20, ns=5, nf=20,
                 fmax=0.8, blend=True, porosity=0.25, scat_how=2)
-RUN = dict(randomwalk=True, factRW=10.0)
+RUN = dict(randomwalk=True, factRW=10.0, maxinteract=100_000)
 METRIC = "packets/s (MCRadiation packet loop, 1 B200)"
 
 
@@ -44,7 +50,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nphot", type=int, default=NPHOT_DEFAULT)
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed", "exact"])
+    ap.add_argument("--compare-fp64", action="store_true", help="also time the FP64 form (one step)")
     ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -122,7 +129,8 @@ def cpu_baseline_sample(model, seconds, cores):
     total_n, total_t = 0, 0.0
     while total_t < seconds and total_n < 200000:
         t0 = time.perf_counter()
-        O.mcradiation(model, n, seed=1000 + total_n, randomwalk=RUN["randomwalk"], factRW=RUN["factRW"], tables=tab)
+        O.mcradiation(model, n, seed=1000 + total_n, randomwalk=RUN["randomwalk"], factRW=RUN["factRW"],
+                      maxinteract=RUN["maxinteract"], tables=tab)
         dt = time.perf_counter() - t0
         total_n += n
         total_t += dt
@@ -160,7 +168,7 @@ def run_reference(args, rank, world):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "packets/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(step_times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "configs[1]-deck precision disk (CPU restatement, packets per step %d)" % total,
+            "config": {"workload": "precision disk deck (CPU restatement of the reference loop, packets per step %d)" % total,
                        "nr": 200, "ntheta": 120, "nlam": 200, "packets_per_step": total},
             "cpu_baseline": {"value": value, "unit": "packets/s", "cores": cores, "kind": "port",
                              "sample": "%d packets per step on %d processes" % (total, cores)},
@@ -172,7 +180,7 @@ _REF = {}
 
 
 def _cpu_model():
-    """configs[1] model with opacities from the CPU checker."""
+    """The same deck with opacities from the oracle's ComputePart."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import models
     return models.small_disk(nrad=WORKLOAD["nrad"], ntheta=WORKLOAD["ntheta"], nlam=WORKLOAD["nlam"],
@@ -192,7 +200,8 @@ def _ref_init():
 def _ref_work(a):
     import oracle_ffi as O
     seed, n = a
-    O.mcradiation(_REF["m"], n, seed=seed, randomwalk=True, factRW=RUN["factRW"], tables=_REF["tab"])
+    O.mcradiation(_REF["m"], n, seed=seed, randomwalk=True, factRW=RUN["factRW"], maxinteract=RUN["maxinteract"],
+                  tables=_REF["tab"])
     return n
 
 
@@ -247,7 +256,7 @@ def main():
                                                                "nu", "Kabs", "Ksca", "F", "BB", "Fstar"))
     nc = model.ncell
     d2h = nc * (8 * 4 + 4) + model.nlam * 31 * (8 * 2 + 4)
-    e2e_steps = max(1, min(args.steps, 2))
+    e2e_steps = 1
     _barrier(dist)
     t1 = time.perf_counter()
     for s in range(e2e_steps):
@@ -255,6 +264,12 @@ def main():
         ctx.mcradiation(args.nphot, seed=rank * 7_000_001 + s + 1, precision=args.precision, fetch=True, **RUN)
     e2e_t = _max_over_ranks(dist, time.perf_counter() - t1)
     e2e_value = args.nphot * e2e_steps * world / e2e_t
+    fp64_line = None
+    if args.compare_fp64 and args.precision != "fp64":
+        _, o64 = ctx.mcradiation(args.nphot, seed=rank * 5_000_011 + 1, precision="fp64", fetch=False, **RUN)
+        t64 = _max_over_ranks(dist, o64["device_ms"] / 1e3)
+        fp64_line = {"value": args.nphot * world / t64, "unit": "packets/s", "steps": 1,
+                     "ms_per_step": 1e3 * t64}
     # roofline of the transport kernel against the measured HBM copy bandwidth
     peaks = {}
     try:
@@ -281,23 +296,27 @@ def main():
             "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic",
-            "config": {"workload": "configs[1] precision disk: Mdust 1e-3 Msun, nr 200 x ntheta 120, nlam 200, "
-                                   "random walk, full Mueller scattering, %s transport" % args.precision,
+            "config": {"workload": "precision disk deck: Mdust 1e-3 Msun, nr 200 x ntheta 120, nlam 200, "
+                                   "random walk (factRW 10), full Mueller scattering, maxinteract 1e5, %s transport"
+                                   % args.precision,
                        "packets_per_step": args.nphot, "precision": args.precision,
                        "parallelism": "replicas" if world > 1 else "single",
                        "l2": "model tables exceed L2 (126 MB): per-cell opacity rows, emission CDF, "
                              "random-walk tables"},
             "e2e": {"value": e2e_value, "unit": "packets/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
-            "gpu_launches": int(args.steps),
+            "gpu_launches": 2 * int(args.steps),  # transport kernel + per-run combine kernel per step
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,
                          "note": "algorithmic bytes from the event counters (crossings, absorptions, scatterings, "
                                  "random-walk steps) per launch / transport-kernel time; peak = measured HBM copy"},
+            "progress_ms_last_step": out["progress_ms"],
             "events_per_step": {"crossings": int(counters[8] // args.steps), "absorptions": int(counters[2] // args.steps),
                                 "scatterings": int(counters[3] // args.steps), "rw_steps": int(counters[4] // args.steps)},
             "wall_s": wall, "clocks": clk, "cpu_baseline": cpu,
         }
+        if fp64_line:
+            line["fp64_form"] = fp64_line
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist:

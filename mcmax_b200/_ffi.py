@@ -7,7 +7,7 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libmcmax_gpu.so")
+LIB_PATH = os.environ.get("MCMAX_GPU_LIB") or os.path.join(HERE, "libmcmax_gpu.so")
 
 TMAX = 10000
 TT = TMAX + 1

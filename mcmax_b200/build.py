@@ -2,7 +2,7 @@
 
 The library is plain CUDA C++ behind the C-ABI of include/mcmax_gpu.h.  The
 FP64 translation units are compiled with --fmad=false so that every a*b+c is
-rounded twice, as in the CPU checker; that is what makes the opacity tables
+rounded twice, as in the CPU oracle; that is what makes the opacity tables
 and the serial transport replay bit-identical.
 """
 import os

@@ -2,7 +2,7 @@
  * cplx.h -- double-complex arithmetic with a fixed evaluation order, usable
  * from host C/C++ and CUDA device code.
  *
- * The opacity kernels must round exactly like the CPU checker, so complex
+ * The opacity kernels must round exactly like the CPU oracle, so complex
  * multiply and divide are written out here instead of relying on C99
  * _Complex or thrust::complex (whose division algorithms differ between
  * compilers).  Division uses Smith's algorithm (R. L. Smith, CACM 5, 435,

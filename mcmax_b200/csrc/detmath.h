@@ -3,7 +3,7 @@
  * device (CUDA) code.
  *
  * Why this exists: the FP64 opacity path must produce bit-identical tables on
- * the GPU and in the CPU checker.  glibc's libm and CUDA's libdevice round
+ * the GPU and in the CPU oracle.  glibc's libm and CUDA's libdevice round
  * sin/cos/exp/log differently in the last bit, so every transcendental that
  * feeds an FP64 result on the bit-exact path goes through these functions
  * instead.  They use only IEEE-754 operations that are correctly rounded on

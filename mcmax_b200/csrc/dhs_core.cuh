@@ -2,7 +2,7 @@
  * dhs_core.cuh -- per-sample light-scattering cores of the opacity stage,
  * written once for the GPU (one warp per sample, NL = 32 lanes) and
  * compilable for the host (NL = 1) so the same source can be replayed on the
- * CPU against the checker.
+ * CPU against the oracle.
  *
  *   dhs_sample  coated sphere of Toon & Ackerman (1981), Appl. Opt. 20, 3657,
  *               in the formulation of ComputePart.f:1256-1711 (DMiLay):
@@ -16,7 +16,7 @@
  *               n, the angle sums in parallel over angles with pi_n/tau_n
  *               generated on the fly.
  *
- * Every floating-point operation keeps the order of the checker (oracle/) so
+ * Every floating-point operation keeps the order of the oracle (oracle/) so
  * that FP64 results agree bit for bit; this translation unit is compiled with
  * --fmad=false and all transcendentals come from detmath.h.
  */

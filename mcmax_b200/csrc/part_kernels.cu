@@ -19,7 +19,7 @@
  *            ComputePart.f:407-415, weighted sums :417-429) and writes
  *            Kabs/Ksca/Kext and the six normalised Mueller elements.
  * All FP64, compiled with --fmad=false: the result is bit-identical to the
- * CPU checker.  Scratch (down-recurrence arrays) lives in one device buffer
+ * CPU oracle.  Scratch (down-recurrence arrays) lives in one device buffer
  * sliced per resident warp.
  */
 #include <cuda_runtime.h>
@@ -236,7 +236,7 @@ __global__ void __launch_bounds__(128) accum_kernel(AccDev a) {
 /* ---------------- host side ---------------- */
 
 /* Bruggeman mixing, ComputePart.f:1177-1212 (same operation order as the
- * checker) */
+ * oracle) */
 void blender(const double *e1, const double *e2, const double *abun, int nm, double *e1out,
              double *e2out) {
   cx mm = cx_make(1.0, 0.0), me = mm;

@@ -7,7 +7,7 @@
  * (block index, 0, packet id low, packet id high).  One block yields four
  * 32-bit words = two uniform doubles with 53 random bits each.  The stream of
  * a packet therefore does not depend on which thread, warp or launch
- * processes it, which is what lets the GPU kernels and the CPU checker replay
+ * processes it, which is what lets the GPU kernels and the CPU oracle replay
  * identical random numbers.
  */
 #ifndef MCMAX_PHILOX_H

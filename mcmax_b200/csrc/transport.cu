@@ -4,7 +4,7 @@
  *
  * Table builders (what Init.f and the top of MCRadiation.f build, one thread
  * per output entry, each entry summed in the reference's order so the FP64
- * values equal the CPU checker's):
+ * values equal the CPU oracle's):
  *   kp_comp_kernel     Kp(q,iT) = integrate(BB(:,iT) Kabs_q)      Init.f:3783-3790
  *   cell_opac_kernel   KabsTot/KscaTot(c,l) = sum_q K_q(l) w_q     MCRadiation.f:199-236
  *   kp_cell_kernel     sum_q Kp(q,iT) w_q  (computeE)              Radiation.f:611-627

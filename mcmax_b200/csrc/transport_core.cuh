@@ -14,7 +14,7 @@
  * The source compiles for the device and, unchanged, for the host (one
  * thread, atomics become plain updates) so a run can be replayed on the CPU.
  * With one thread the packet order is the reference's serial order and the
- * result matches the CPU checker bit for bit (FP64 path, --fmad=false,
+ * result matches the CPU oracle bit for bit (FP64 path, --fmad=false,
  * detmath.h transcendentals).
  *
  * Reference map:

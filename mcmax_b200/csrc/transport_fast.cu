@@ -124,8 +124,11 @@ SmemPlan plan_smem(int nr, int nt, int nlam, int ncomp, bool uniform) {
   return p;
 }
 
+#ifndef F_MINBLOCKS
+#define F_MINBLOCKS 1
+#endif
 template <class R>
-__global__ void __launch_bounds__(256) transport_fast_kernel(const __grid_constant__ FModel<R> g,
+__global__ void __launch_bounds__(256, F_MINBLOCKS) transport_fast_kernel(const __grid_constant__ FModel<R> g,
                                                              const __grid_constant__ TAcc A, SmemPlan sp) {
   extern __shared__ __align__(16) unsigned char smem[];
   if (blockIdx.x == 0 && threadIdx.x == 0) A.tmark[5] = tp_globaltimer();

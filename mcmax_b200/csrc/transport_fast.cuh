@@ -28,7 +28,7 @@
  * Stokes parameters are carried as fractions of E (q = Q/E ...), which is
  * what the reference's renormalisation (Radiation.f:480-483) keeps invariant.
  * Results agree with the reference-order kernel up to floating-point
- * reassociation; the checks are statistical against the CPU checker and
+ * reassociation; the checks are statistical against the CPU oracle and
  * paired (identical Philox streams) against the reference-order kernel.
  */
 #ifndef MCMAX_TRANSPORT_FAST_CUH
@@ -67,6 +67,14 @@ struct FModel {
 };
 
 #define F_NGUIDE 32
+
+/* cold paths (interactions, random walk, emission) can be compiled out of
+ * line to keep the crossing loop small in the instruction cache */
+#if defined(__CUDACC__) && defined(F_COLD_NOINLINE)
+#define F_COLD __host__ __device__ __noinline__
+#else
+#define F_COLD TP_FN
+#endif
 
 /* first index i in [0,n) with f(i) > v (or >= when ge), starting from a
  * guess and walking; f is non-decreasing */
@@ -338,7 +346,7 @@ TP_FN double f_tinv(const double *kp, double E1, int lo, int *ibr) {
 
 /* ------------------------------------------------------------- interaction */
 template <class R>
-TP_FN void f_interact(const FModel<R> &m, const TAcc &A, px_stream *r, FPkt<R> &p, TLocal &L) {
+F_COLD void f_interact(const FModel<R> &m, const TAcc &A, px_stream *r, FPkt<R> &p, TLocal &L) {
   typedef FOps<R> O;
   const int c = p.i * m.nc + (p.j - 1);
   const int nlam = m.nlam;
@@ -474,7 +482,7 @@ TP_FN void f_interact(const FModel<R> &m, const TAcc &A, px_stream *r, FPkt<R> &
 
 /* ------------------------------------------------------------- random walk */
 template <class R>
-TP_FN int f_random_walk(const FModel<R> &m, const TAcc &A, px_stream *r, FPkt<R> &p, TLocal &L) {
+F_COLD int f_random_walk(const FModel<R> &m, const TAcc &A, px_stream *r, FPkt<R> &p, TLocal &L) {
   const int c = p.i * m.nc + (p.j - 1);
   const int row = m.kd_index[c];
   if (row < 0) return 0;

@@ -349,8 +349,8 @@ def disk_model(ctx, *, tstar=10000.0, rstar=2.5, rin=0.5, rout=100.0, mdust=1e-5
 
 
 CONFIGS = {
-    # the reference's CPU-runnable case
-    "cfg0_small": dict(mdust=1e-5, nrad=100, ntheta=60, nlam=100),
-    # thick disk exercising the random walk
-    "cfg1_thick": dict(mdust=1e-3, nrad=200, ntheta=120, nlam=200),
+    # small thin disk: the case a CPU run finishes quickly
+    "small_thin_disk": dict(mdust=1e-5, nrad=100, ntheta=60, nlam=100),
+    # precision disk: optically thick midplane exercising the random walk
+    "precision_disk": dict(mdust=1e-3, nrad=200, ntheta=120, nlam=200),
 }

@@ -1,6 +1,6 @@
 /*
  * oracle.h -- CPU restatement of the MCMax hot path, used ONLY as the test
- * checker (tests/, the smoke check and bench.py's CPU baseline).  It is not
+ * reference for parity tests (tests/, the smoke check and bench.py's CPU baseline).  It is not
  * part of the product and the product never links it.
  *
  * Parity status: UNPINNED against the reference binary.  MCMax is Fortran,

@@ -1,6 +1,6 @@
 /*
  * oracle_mc.c -- serial CPU restatement of MCMax's photon-packet loop.
- * Test infrastructure only (checker for the GPU transport kernels and the
+ * Test infrastructure only (parity reference for the GPU transport kernels and the
  * timed CPU baseline).
  *
  * Follows:

@@ -1,4 +1,4 @@
-"""Small test models built on the CPU (opacities from the checker), shared
+"""Small test models built on the CPU (opacities from the oracle), shared
 by the CPU and GPU tests."""
 import math
 

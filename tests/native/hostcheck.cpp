@@ -1,6 +1,6 @@
 // Host build of the device cores (dhs_core.cuh, transport_core.cuh) for the
 // CPU tests: the same source the GPU kernels run, executed by one host
-// thread, so it can be compared bit for bit with the checker without a GPU.
+// thread, so it can be compared bit for bit with the oracle without a GPU.
 // Test infrastructure only.
 #include <cstdint>
 #include <cstdlib>

@@ -1,4 +1,4 @@
-"""ctypes bindings of the CPU checker (oracle/liboracle_mcmax.so).  Test
+"""ctypes bindings of the CPU oracle (oracle/liboracle_mcmax.so).  Test
 infrastructure only."""
 import ctypes as C
 import os

@@ -1,5 +1,5 @@
 """The C-ABI library: loads without a GPU, exports every symbol the header
-declares, its host-side table builder matches the checker, and it reports
+declares, its host-side table builder matches the oracle, and it reports
 errors instead of aborting."""
 import ctypes as C
 import os
@@ -31,7 +31,7 @@ def test_every_declared_symbol_is_exported():
     assert set(names) <= set(_ffi.SIGNATURES), set(names) - set(_ffi.SIGNATURES)
 
 
-def test_planck_table_matches_checker():
+def test_planck_table_matches_oracle():
     from mcmax_b200 import api
     lam = np.geomspace(0.1, 3000, 37)
     assert np.array_equal(api.bb_table(lam), O.bb_table(lam))

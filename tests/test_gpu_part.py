@@ -1,4 +1,4 @@
-"""GPU ComputePart (DHS/Mie kernels through the C-ABI) against the checker and
+"""GPU ComputePart (DHS/Mie kernels through the C-ABI) against the oracle and
 the golden fixtures: bit-exact FP64 opacity tables."""
 import os
 

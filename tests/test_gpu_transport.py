@@ -1,6 +1,6 @@
-"""GPU packet loop through the C-ABI against the checker.
+"""GPU packet loop through the C-ABI against the oracle.
 
-Reference-order FP64 kernel with one thread: bit for bit the checker's
+Reference-order FP64 kernel with one thread: bit for bit the oracle's
 serial loop.  Parallel runs (all three forms): statistical agreement of the
 per-cell temperatures and energy bookkeeping."""
 import numpy as np
@@ -55,10 +55,10 @@ def test_energy_conservation(ctx, prec):
 
 
 @pytest.mark.parametrize("prec", ["exact", "fp64", "mixed"])
-def test_temperatures_statistically_match_checker(ctx, prec):
-    """Per-cell temperature of a parallel GPU run vs the serial checker:
+def test_temperatures_statistically_match_oracle(ctx, prec):
+    """Per-cell temperature of a parallel GPU run vs the serial oracle:
     cells with many packets agree within 3 sigma of the combined MC noise
-    (sigma from the independent-seed scatter of the checker)."""
+    (sigma from the independent-seed scatter of the oracle)."""
     m = models.small_disk(nrad=12, ntheta=8, nlam=24, ngrains=2, ns=2, nf=3)
     N = 4000
     ctx.set_model(m)
@@ -84,10 +84,12 @@ def test_temperatures_statistically_match_checker(ctx, prec):
     sig = np.sqrt((sr ** 2 + sg ** 2) / 4) + 1e-3 * mr
     z = np.abs(mr - mg) / sig
     assert np.mean(z < 3) > 0.95, np.sort(z)[-5:]
-    assert np.all(np.abs(mg / mr - 1) < 0.15)
+    well = sr < 0.02 * mr  # cells the oracle resolves to 2 %
+    assert well.sum() > 10
+    assert np.all(np.abs(mg / mr - 1)[well] < 0.1)
 
 
-def test_finalize_matches_checker_determine_t(ctx):
+def test_finalize_matches_oracle_determine_t(ctx):
     m = models.small_disk()
     ctx.set_model(m)
     _, g = ctx.mcradiation(2000, seed=3, precision="exact")

@@ -1,5 +1,5 @@
 """The device cores (dhs_core.cuh, transport_core.cuh, transport_fast.cuh)
-built for the host and replayed against the CPU checker.  Bit-exact for the
+built for the host and replayed against the CPU oracle.  Bit-exact for the
 opacity cores and for the reference-order transport; statistical for the
 GPU-ordered transport."""
 import math

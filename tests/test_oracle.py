@@ -1,4 +1,4 @@
-"""The CPU checker (oracle/) against published values, limits and
+"""The CPU oracle (oracle/) against published values, limits and
 identities of the reference's algorithms, and against the golden fixtures."""
 import math
 import os
