@@ -112,6 +112,31 @@ mcg_status mcg_compute_part(mcg_ctx *ctx, const mcg_part_in *in, mcg_part_out *o
 mcg_status mcg_compute_part_batch(mcg_ctx *ctx, int nparts, const mcg_part_in *in,
                                   mcg_part_out *out);
 
+/* Size of the device array behind mcg_compute_part_static (64 MiB). */
+#define MCG_STATIC_ARENA_BYTES (64u * 1024u * 1024u)
+
+/* One grain bin, as mcg_compute_part, without allocating device memory.
+ * No counterpart in the reference (ComputePart itself allocates nothing on a
+ * GPU); it exists for host programs that must not call cudaMalloc/cudaFree:
+ * a Fortran or C driver whose device memory is already handed to its own
+ * pool allocator (cudaMalloc then fails or fragments the pool), and code
+ * that runs while other streams do latency-critical work (cudaFree waits
+ * for the whole device).  Inputs and outputs are the same host arrays as for
+ * mcg_compute_part and the tables are bit-identical to it.
+ *
+ * All device working memory of the call lives in one static array of
+ * MCG_STATIC_ARENA_BYTES that every GPU loading this library holds until the
+ * process exits.  A bin is processed in chunks of wavelengths that fit the
+ * array; a bin whose single wavelength needs more (many sizes times filling
+ * fractions, or very large size parameters) is rejected with MCG_ERR_LIMIT
+ * and a message giving the bytes it would need.  The first call on each
+ * device looks up the array's device address (cudaGetSymbolAddress); make
+ * that first call before any stream capture.  Every call shares the one
+ * array: calls that overlap on the same GPU (two contexts used from two
+ * host threads at once) race and must be serialised by the caller; the call
+ * returns only after its own work has finished. */
+mcg_status mcg_compute_part_static(mcg_ctx *ctx, const mcg_part_in *in, mcg_part_out *out);
+
 /* ----------------------------------------------------------------------
  * Model: what Init.f builds and MCRadiation reads.
  * -------------------------------------------------------------------- */

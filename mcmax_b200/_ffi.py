@@ -14,6 +14,7 @@ TT = TMAX + 1
 NANG = 180
 NANGLE_SED = 30
 NCOUNTERS = 16
+STATIC_ARENA_BYTES = 64 * 1024 * 1024
 
 MCG_OK, MCG_ERR_ARG, MCG_ERR_CUDA, MCG_ERR_STATE, MCG_ERR_NOMEM, MCG_ERR_LIMIT, MCG_ERR_RUN = range(7)
 STATUS_NAMES = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_STATE", 4: "ERR_NOMEM", 5: "ERR_LIMIT", 6: "ERR_RUN"}
@@ -81,6 +82,7 @@ SIGNATURES = {
     "mcg_version": (C.c_int, []),
     "mcg_compute_part": (C.c_int, [C.c_void_p, C.POINTER(PartIn), C.POINTER(PartOut)]),
     "mcg_compute_part_batch": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(PartIn), C.POINTER(PartOut)]),
+    "mcg_compute_part_static": (C.c_int, [C.c_void_p, C.POINTER(PartIn), C.POINTER(PartOut)]),
     "mcg_bb_table": (C.c_int, [C.c_int, dp, dp]),
     "mcg_planck": (C.c_double, [C.c_double, C.c_double]),
     "mcg_set_model": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Opacity)]),

@@ -78,6 +78,12 @@ mcg_status mcg_compute_part_batch(mcg_ctx *ctx, int nparts, const mcg_part_in *i
   return mcg_part_batch_impl(ctx, nparts, in, out);
 }
 
+mcg_status mcg_compute_part_static(mcg_ctx *ctx, const mcg_part_in *in, mcg_part_out *out) {
+  if (!ctx) return MCG_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  return mcg_part_static_impl(ctx, in, out);
+}
+
 mcg_status mcg_set_model(mcg_ctx *ctx, const mcg_grid *grid, const mcg_opacity *opac) {
   if (!ctx) return MCG_ERR_ARG;
   cudaSetDevice(ctx->device);

@@ -27,6 +27,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "dhs_core.cuh"
@@ -690,5 +691,324 @@ mcg_status mcg_part_batch_impl(mcg_ctx *ctx, int nparts, const mcg_part_in *in, 
     out[p].mscale = H[p].mscale;
     out[p].rscale = H[p].rscale;
   }
+  return MCG_OK;
+}
+
+/* ------------------------------------------------------------------------
+ * ComputePart without device allocation (mcg_compute_part_static).
+ *
+ * For callers that must not allocate device memory themselves or through
+ * this library: every device buffer of the call (staged inputs, per-sample
+ * Mueller rows, Mie slots, recurrence scratch, outputs before the copy back)
+ * is carved out of one file-scope array of MCG_STATIC_ARENA_BYTES.  The
+ * array exists once per device for as long as the library is loaded.
+ *
+ * Wavelength rows are independent in ComputePart (ComputePart.f:318-447), so
+ * a bin is processed in chunks of rows that fit the array; the kernels and
+ * their per-row order are those of mcg_part_batch_impl, so the tables are
+ * bit-identical to mcg_compute_part.
+ *
+ * The array keeps whatever the previous call left in it.  The work counters
+ * and the Mie success flags are cleared on the stream before each chunk;
+ * everything else is written before it is read.  Two calls whose work
+ * overlaps on the GPU (two contexts on one device used from two host
+ * threads) share the array and race; the call synchronises its stream
+ * before returning, so calls made one after the other never overlap.
+ * ---------------------------------------------------------------------- */
+static __device__ __align__(256) unsigned char mcg_static_arena[MCG_STATIC_ARENA_BYTES];
+
+namespace {
+
+constexpr size_t kArenaBytes = (size_t)MCG_STATIC_ARENA_BYTES;
+constexpr int kArenaMaxDevices = 64;
+
+std::mutex g_arena_mutex;
+void *g_arena_dev_ptr[kArenaMaxDevices] = {};
+
+/* Device address of the array on `dev` (the current device).  In host code
+ * the symbol mcg_static_arena only names a host-side shadow; the kernels
+ * need the address the runtime reports for the device. */
+cudaError_t arena_address(int dev, unsigned char **out) {
+  std::lock_guard<std::mutex> lock(g_arena_mutex);
+  if (dev < 0 || dev >= kArenaMaxDevices) return cudaErrorInvalidDevice;
+  if (!g_arena_dev_ptr[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, mcg_static_arena);
+    if (e != cudaSuccess) return e;
+    g_arena_dev_ptr[dev] = p;
+  }
+  *out = (unsigned char *)g_arena_dev_ptr[dev];
+  return cudaSuccess;
+}
+
+/* bump allocator over the array, 256-byte aligned pieces */
+struct Carve {
+  unsigned char *base;
+  size_t off = 0, cap = 0;
+  template <typename T>
+  T *take(size_t n) {
+    size_t bytes = (std::max<size_t>(n, 1) * sizeof(T) + 255) & ~(size_t)255;
+    T *p = (T *)(base + off);
+    off += bytes;
+    return p;
+  }
+};
+
+inline size_t padded(size_t bytes) { return (std::max<size_t>(bytes, 1) + 255) & ~(size_t)255; }
+
+}  // namespace
+
+mcg_status mcg_part_static_impl(mcg_ctx *ctx, const mcg_part_in *in, mcg_part_out *out) {
+  if (!in || !out) return mcg_fail(ctx, MCG_ERR_ARG, "compute_part_static: non-null in/out required");
+  PartHost h;
+  {
+    std::string why;
+    if (!part_setup(*in, h, why)) return mcg_fail(ctx, MCG_ERR_ARG, "%s", why.c_str());
+  }
+  if (!out->kabs || !out->ksca || !out->kext || !out->F)
+    return mcg_fail(ctx, MCG_ERR_ARG, "compute_part_static: null output array");
+  const int nlam = h.nlam, nmc = h.nmc, ns = h.ns, nf = h.nf;
+  const long long per_row_samp = (long long)nmc * ns * nf, per_row_slot = (long long)nmc * ns;
+
+  double mu[90], sinw[NA], tot2 = 0.0;
+  for (int i = 1; i <= 90; ++i) mu[i - 1] = cos(((double)i - 0.5) / (double)(NA / 2) * DHS_PI / 2.0);
+  for (int j = 1; j <= NA; ++j) sinw[j - 1] = sin(DHS_PI * ((double)j - 0.5) / (double)NA);
+  for (int j = 0; j < NA; ++j) tot2 = tot2 + sinw[j];
+
+  /* recurrence lengths over the whole bin (as mcg_part_batch_impl) */
+  int maxnmx1 = 150, maxmie = 0;
+  for (int ilam = 0; ilam < nlam; ++ilam) {
+    const double wvno = 2.0 * DHS_PI / in->lam[ilam];
+    for (int l = 0; l < nmc; ++l) {
+      const double e1 = h.e1[(size_t)l * nlam + ilam], e2 = h.e2[(size_t)l * nlam + ilam];
+      for (int k = 0; k < ns; ++k) {
+        const double r1 = h.r1[k];
+        for (int i = 0; i < nf; ++i) {
+          const bool mie = h.f[i] == 0.0 || r1 * wvno > 10000.0 || h.frac[l] == 0.0;
+          if (!mie) maxnmx1 = std::max(maxnmx1, dhs_nmx1(h.rad[(size_t)k * nf + i], wvno, e1, -e2));
+        }
+        double lm = in->lam[ilam];
+        if (r1 / lm >= 5000.0) lm = r1 / 5000.0;
+        int nmax, nfi, nD;
+        mie_counts(r1, lm, e1, e2, &nmax, &nfi, &nD);
+        maxmie = std::max(maxmie, std::max(nfi, nD));
+      }
+    }
+  }
+  if (maxnmx1 + 1 > DHS_LL) maxnmx1 = DHS_LL;
+  const int dcap = maxnmx1 + 2, mcap = maxmie + 2;
+  if ((long long)mcap > 50000000LL)
+    return mcg_fail(ctx, MCG_ERR_LIMIT, "compute_part_static: Mie term count %d beyond the 5e7 limit", maxmie);
+  const size_t per_warp = std::max((size_t)4 * dcap * sizeof(cx), (size_t)8 * mcap * sizeof(double));
+
+  /* bytes: fixed part, per wavelength row, per warp of recurrence scratch */
+  std::vector<double> pflat;
+  pflat.insert(pflat.end(), h.frac.begin(), h.frac.begin() + nmc);
+  pflat.insert(pflat.end(), h.rho.begin(), h.rho.begin() + nmc);
+  pflat.insert(pflat.end(), h.r1.begin(), h.r1.end());
+  pflat.insert(pflat.end(), h.nr.begin(), h.nr.end());
+  pflat.insert(pflat.end(), h.wf.begin(), h.wf.begin() + nf);
+  const size_t fixed = padded(90 * 8) + padded(NA * 8) + padded(16) + padded(sizeof(PartDev)) +
+                       padded(pflat.size() * 8) + padded(8) /* rho_av */;
+  /* 5 staged doubles, status, 4x180 Mueller, 2 cross sections per sample;
+   * 4 staged doubles, need flag, 4x180 Mueller, 2 cross sections, ok flag
+   * per Mie slot; row map, 3 opacities, 6x180 Mueller per row; each of the
+   * 21 row-sized arrays may lose up to 255 bytes to alignment */
+  const size_t per_row = (size_t)per_row_samp * (5 * 8 + 1 + 4 * NA * 8 + 2 * 8) +
+                         (size_t)per_row_slot * (4 * 8 + 4 + 4 * NA * 8 + 2 * 8 + 1) + 4 + 3 * 8 + 6 * NA * 8;
+  const size_t align_slack = 21 * 256;
+  if (fixed + align_slack + per_row + 4 * per_warp > kArenaBytes)
+    return mcg_fail(ctx, MCG_ERR_LIMIT,
+                    "compute_part_static: one wavelength row needs %zu bytes of device working memory "
+                    "(%lld samples, %zu bytes of recurrence scratch for 4 warps); the static array holds %zu",
+                    fixed + align_slack + per_row + 4 * per_warp, per_row_samp, 4 * per_warp, kArenaBytes);
+  const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;
+  /* scratch for up to one warp per sample of a chunk, at most 32 warps per
+   * SM, at most half the array; the rest holds rows */
+  size_t want_warps = std::min<size_t>((size_t)sms * 32, (size_t)std::max<long long>(4, per_row_samp * nlam));
+  size_t scratch = std::min(want_warps * per_warp, kArenaBytes / 2);
+  scratch = std::max(scratch, 4 * per_warp);
+  size_t rows_fit = (kArenaBytes - fixed - align_slack - scratch) / per_row;
+  if (rows_fit < 1) {
+    scratch = 4 * per_warp;
+    rows_fit = (kArenaBytes - fixed - align_slack - scratch) / per_row;
+  }
+  const int nlc_max = (int)std::min<size_t>(rows_fit, (size_t)nlam);
+  const size_t rows_bytes = (size_t)nlc_max * per_row + align_slack;
+  int nw = (int)(std::min((kArenaBytes - fixed - rows_bytes) / per_warp, (size_t)sms * 32) / 4 * 4);
+  if (nw < 4) nw = 4;
+
+  unsigned char *arena = nullptr;
+  cudaError_t ce = arena_address(ctx->device, &arena);
+  if (ce != cudaSuccess)
+    return mcg_fail(ctx, MCG_ERR_CUDA, "compute_part_static: cudaGetSymbolAddress failed: %s",
+                    cudaGetErrorString(ce));
+  cudaStream_t st = ctx->stream;
+  Carve cv{arena, 0, kArenaBytes};
+  double *d_mu = cv.take<double>(90);
+  double *d_sinw = cv.take<double>(NA);
+  unsigned long long *d_next = cv.take<unsigned long long>(2);
+  PartDev *d_part = cv.take<PartDev>(1);
+  double *d_pflat = cv.take<double>(pflat.size());
+  double *d_rhoav = cv.take<double>(1);
+  const size_t chunk_base = cv.off;
+
+  cudaMemcpyAsync(d_mu, mu, sizeof mu, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(d_sinw, sinw, sizeof sinw, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(d_pflat, pflat.data(), pflat.size() * sizeof(double), cudaMemcpyHostToDevice, st);
+
+  int64_t n_dhs = 0, n_fail = 0, n_mie = 0;
+  std::vector<double> srcore, srshell, swvno, smre, smim, mrad, mlam, me1, me2;
+  std::vector<int8_t> sstat, stat, mok;
+  std::vector<int> mneed, rowpart;
+  for (int c0 = 0; c0 < nlam; c0 += nlc_max) {
+    const int nlc = std::min(nlc_max, nlam - c0);
+    srcore.clear(); srshell.clear(); swvno.clear(); smre.clear(); smim.clear(); sstat.clear();
+    mrad.clear(); mlam.clear(); me1.clear(); me2.clear(); mneed.clear();
+    for (int ilam = c0; ilam < c0 + nlc; ++ilam) {
+      const double wvno = 2.0 * DHS_PI / in->lam[ilam];
+      for (int l = 0; l < nmc; ++l) {
+        const double e1 = h.e1[(size_t)l * nlam + ilam], e2 = h.e2[(size_t)l * nlam + ilam];
+        for (int k = 0; k < ns; ++k) {
+          const double r1 = h.r1[k];
+          int need = 0;
+          for (int i = 0; i < nf; ++i) {
+            int8_t s8 = S_DHS;
+            if (h.f[i] == 0.0 || r1 * wvno > 10000.0) s8 = S_MIE;
+            if (h.frac[l] == 0.0) {
+              s8 = S_MIE;
+            } else if (s8 == S_MIE) {
+              need = 1;
+            }
+            srcore.push_back(h.rcore[(size_t)k * nf + i]);
+            srshell.push_back(h.rad[(size_t)k * nf + i]);
+            swvno.push_back(wvno);
+            smre.push_back(e1);
+            smim.push_back(e2);
+            sstat.push_back(s8);
+          }
+          double lm = in->lam[ilam];
+          if (r1 / lm >= 5000.0) lm = r1 / 5000.0;
+          mrad.push_back(r1);
+          mlam.push_back(lm);
+          me1.push_back(e1);
+          me2.push_back(e2);
+          mneed.push_back(need);
+        }
+      }
+    }
+    const int nsamp = (int)sstat.size(), nslot = (int)mneed.size();
+    cv.off = chunk_base;
+    double *d_rcore = cv.take<double>(nsamp), *d_rshell = cv.take<double>(nsamp);
+    double *d_wvno = cv.take<double>(nsamp), *d_mre = cv.take<double>(nsamp), *d_mim = cv.take<double>(nsamp);
+    int8_t *d_stat = cv.take<int8_t>(nsamp);
+    double *d_sF = cv.take<double>((size_t)nsamp * 4 * NA), *d_scs = cv.take<double>((size_t)nsamp * 2);
+    double *d_mrad = cv.take<double>(nslot), *d_mlam = cv.take<double>(nslot);
+    double *d_me1 = cv.take<double>(nslot), *d_me2 = cv.take<double>(nslot);
+    int *d_mneed = cv.take<int>(nslot);
+    double *d_mF = cv.take<double>((size_t)nslot * 4 * NA), *d_mcs = cv.take<double>((size_t)nslot * 2);
+    int8_t *d_mok = cv.take<int8_t>(nslot);
+    int *d_rowpart = cv.take<int>(nlc);
+    double *d_kabs = cv.take<double>(nlc), *d_ksca = cv.take<double>(nlc), *d_kext = cv.take<double>(nlc);
+    double *d_Fout = cv.take<double>((size_t)nlc * 6 * NA);
+    const size_t scratch_off = cv.off;
+    if (scratch_off + (size_t)nw * per_warp > kArenaBytes)
+      return mcg_fail(ctx, MCG_ERR_LIMIT, "compute_part_static: internal layout exceeds the static array");
+
+    /* the chunk's rows are local (0..nlc-1); offsets shift the absolute
+     * wavelength index ilam = row + c0 onto them */
+    PartDev pd;
+    pd.nlam = nlam;
+    pd.nmc = nmc;
+    pd.ns = ns;
+    pd.nf = nf;
+    pd.samp0 = -(int)(c0 * per_row_samp);
+    pd.mie0 = -(int)(c0 * per_row_slot);
+    pd.out0 = -c0;
+    pd.mscale = h.mscale;
+    pd.frac = d_pflat;
+    pd.rho = d_pflat + nmc;
+    pd.r1 = d_pflat + 2 * nmc;
+    pd.nr = d_pflat + 2 * nmc + ns;
+    pd.wf = d_pflat + 2 * nmc + ns + (size_t)nmc * ns;
+    rowpart.assign(nlc, 0);
+#define H2D(dst, src, n) cudaMemcpyAsync(dst, src, (size_t)(n) * sizeof(*(src)), cudaMemcpyHostToDevice, st)
+    H2D(d_rcore, srcore.data(), nsamp);
+    H2D(d_rshell, srshell.data(), nsamp);
+    H2D(d_wvno, swvno.data(), nsamp);
+    H2D(d_mre, smre.data(), nsamp);
+    H2D(d_mim, smim.data(), nsamp);
+    H2D(d_stat, sstat.data(), nsamp);
+    H2D(d_mrad, mrad.data(), nslot);
+    H2D(d_mlam, mlam.data(), nslot);
+    H2D(d_me1, me1.data(), nslot);
+    H2D(d_me2, me2.data(), nslot);
+    H2D(d_mneed, mneed.data(), nslot);
+    H2D(d_part, &pd, 1);
+    H2D(d_rowpart, rowpart.data(), nlc);
+#undef H2D
+    /* what the previous call or chunk left behind must not count */
+    cudaMemsetAsync(d_next, 0, 2 * sizeof(unsigned long long), st);
+    cudaMemsetAsync(d_mok, 0, nslot, st);
+
+    SampleDev sd{d_rcore, d_rshell, d_wvno, d_mre, d_mim, d_stat, d_sF, d_scs, d_mneed, nsamp};
+    const int nw_dhs = std::min(nw, (nsamp + 3) / 4 * 4);
+    dhs_kernel<<<(nw_dhs + 3) / 4, 128, 0, st>>>(sd, d_mu, (cx *)(arena + scratch_off), dcap, d_next);
+    stat.resize(nsamp);
+    cudaMemcpyAsync(stat.data(), d_stat, nsamp, cudaMemcpyDeviceToHost, st);
+    ce = cudaStreamSynchronize(st);
+    if (ce != cudaSuccess)
+      return mcg_fail(ctx, MCG_ERR_CUDA, "compute_part_static: DHS kernel failed: %s", cudaGetErrorString(ce));
+    bool changed = false;
+    for (int q = 0; q < nslot; ++q)
+      for (int i = 0; i < nf; ++i) {
+        const int8_t s8 = stat[(size_t)q * nf + i];
+        if (s8 == S_DHS) n_dhs++;
+        if (s8 == S_DHS_ERR) {
+          n_dhs++;
+          n_fail++;
+          if (!mneed[q]) {
+            mneed[q] = 1;
+            changed = true;
+          }
+        }
+      }
+    for (int q = 0; q < nslot; ++q) n_mie += mneed[q];
+    if (changed) cudaMemcpyAsync(d_mneed, mneed.data(), (size_t)nslot * sizeof(int), cudaMemcpyHostToDevice, st);
+    MieDev md{d_mrad, d_mlam, d_me1, d_me2, d_mneed, d_mF, d_mcs, d_mok, nslot};
+    const int nw_mie = std::min(nw, (nslot + 3) / 4 * 4);
+    mie_kernel<<<(nw_mie + 3) / 4, 128, 0, st>>>(md, (double *)(arena + scratch_off), mcap, d_next + 1);
+    AccDev ad{d_part, 1, d_rowpart, d_stat, d_sF, d_scs, d_mF, d_mcs, d_sinw, tot2,
+              d_kabs, d_ksca, d_kext, d_Fout, d_rhoav, nlc};
+    accum_kernel<<<(nlc + 3) / 4, 128, 0, st>>>(ad);
+    ce = cudaGetLastError();
+    if (ce != cudaSuccess)
+      return mcg_fail(ctx, MCG_ERR_CUDA, "compute_part_static: launch failed: %s", cudaGetErrorString(ce));
+    mok.resize(nslot);
+    cudaMemcpyAsync(out->kabs + c0, d_kabs, nlc * sizeof(double), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(out->ksca + c0, d_ksca, nlc * sizeof(double), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(out->kext + c0, d_kext, nlc * sizeof(double), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(out->F + (size_t)c0 * 6 * NA, d_Fout, (size_t)nlc * 6 * NA * sizeof(double),
+                    cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(mok.data(), d_mok, nslot, cudaMemcpyDeviceToHost, st);
+    ce = cudaStreamSynchronize(st);
+    if (ce != cudaSuccess)
+      return mcg_fail(ctx, MCG_ERR_CUDA, "compute_part_static: kernels failed: %s", cudaGetErrorString(ce));
+    for (int q = 0; q < nslot; ++q)
+      if (mneed[q] && !mok[q])
+        return mcg_fail(ctx, MCG_ERR_LIMIT, "compute_part_static: homogeneous-sphere fallback did not fit (slot %d)",
+                        q + (int)(c0 * per_row_slot));
+  }
+  double rho_av = 0.0;
+  cudaMemcpyAsync(&rho_av, d_rhoav, sizeof(double), cudaMemcpyDeviceToHost, st);
+  ce = cudaStreamSynchronize(st);
+  if (ce != cudaSuccess)
+    return mcg_fail(ctx, MCG_ERR_CUDA, "compute_part_static: copy failed: %s", cudaGetErrorString(ce));
+  out->rho_av = rho_av;
+  out->mscale = h.mscale;
+  out->rscale = h.rscale;
+  out->n_dhs = n_dhs;
+  out->n_dhs_fail = n_fail;
+  out->n_mie = n_mie;
   return MCG_OK;
 }
