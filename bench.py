@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--compare-fp64", action="store_true", help="also time the FP64 form (one step)")
     ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--maxinteract", type=int, default=RUN["maxinteract"],
+                    help="overflow roulette (keyword maxinteract); smaller values shorten the trapped-packet tail "
+                         "for profiling runs")
     return ap.parse_args()
 
 
@@ -207,6 +210,7 @@ def _ref_work(a):
 
 def main():
     args = parse()
+    RUN["maxinteract"] = args.maxinteract
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -297,8 +301,8 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic",
             "config": {"workload": "precision disk deck: Mdust 1e-3 Msun, nr 200 x ntheta 120, nlam 200, "
-                                   "random walk (factRW 10), full Mueller scattering, maxinteract 1e5, %s transport"
-                                   % args.precision,
+                                   "random walk (factRW 10), full Mueller scattering, maxinteract %g, %s transport"
+                                   % (args.maxinteract, args.precision),
                        "packets_per_step": args.nphot, "precision": args.precision,
                        "parallelism": "replicas" if world > 1 else "single",
                        "l2": "model tables exceed L2 (126 MB): per-cell opacity rows, emission CDF, "

@@ -201,7 +201,8 @@ typedef struct {
   int precision;          /* mcg_precision */
   int threads;            /* 0: persistent grid; n > 0: exactly n threads
                              (1 reproduces the serial packet order) */
-  int block;              /* threads per block, 0: default */
+  int block;              /* threads per block: 0 = default (256), else a
+                             multiple of 32 up to 256 */
 } mcg_run;
 
 typedef struct {

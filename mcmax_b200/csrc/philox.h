@@ -76,15 +76,41 @@ PX_FN void px_init(px_stream *s, uint64_t seed, uint64_t packet_id) {
   s->spare = 0.0;
 }
 
+#if defined(__CUDA_ARCH__)
+/* One Philox block for a device caller.  Kept out of line: the packet loops
+ * draw random numbers at dozens of places, and one shared copy of the ten
+ * rounds keeps those loops small in the instruction cache. */
+static __device__ __noinline__ uint4 px_block_dev(uint32_t block, uint32_t pid_lo, uint32_t pid_hi, uint32_t k0,
+                                                  uint32_t k1) {
+  const uint32_t c[4] = {block, 0u, pid_lo, pid_hi};
+  const uint32_t k[2] = {k0, k1};
+  uint32_t o[4];
+  px_philox4x32_10(c, k, o);
+  return make_uint4(o[0], o[1], o[2], o[3]);
+}
+#endif
+
 /* next uniform double in (0,1) of the packet's stream */
 PX_FN double px_next(px_stream *s) {
   if (s->have) {
     s->have = 0;
     return s->spare;
   }
-  uint32_t c[4] = {s->block, 0u, s->pid_lo, s->pid_hi};
   uint32_t o[4];
-  px_philox4x32_10(c, s->key, o);
+#if defined(__CUDA_ARCH__)
+  {
+    const uint4 w = px_block_dev(s->block, s->pid_lo, s->pid_hi, s->key[0], s->key[1]);
+    o[0] = w.x;
+    o[1] = w.y;
+    o[2] = w.z;
+    o[3] = w.w;
+  }
+#else
+  {
+    const uint32_t c[4] = {s->block, 0u, s->pid_lo, s->pid_hi};
+    px_philox4x32_10(c, s->key, o);
+  }
+#endif
   s->block += 1u;
   s->spare = px_u01(o[2], o[3]);
   s->have = 1;

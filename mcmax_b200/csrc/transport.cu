@@ -577,6 +577,8 @@ mcg_status mcg_mcradiation_impl(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot
   if (run->precision != MCG_PREC_FP64 && run->precision != MCG_PREC_MIXED && run->precision != MCG_PREC_EXACT)
     return mcg_fail(ctx, MCG_ERR_ARG, "mcradiation: unknown precision %d", run->precision);
   if (run->threads < 0 || run->block < 0) return mcg_fail(ctx, MCG_ERR_ARG, "mcradiation: threads/block must be >= 0");
+  if (run->block > 256 || run->block % 32 != 0)
+    return mcg_fail(ctx, MCG_ERR_ARG, "mcradiation: block must be 0 (default) or a multiple of 32 up to 256");
   mcg_status s;
   if ((s = ensure_run_buffers(ctx, nruns)) != MCG_OK) return s;
   if (run->randomwalk && (s = build_rw_tables(ctx, run->factRW)) != MCG_OK) return s;

@@ -124,11 +124,17 @@ SmemPlan plan_smem(int nr, int nt, int nlam, int ncomp, bool uniform) {
   return p;
 }
 
+#ifndef F_BLOCK
+#define F_BLOCK 256
+#endif
+/* two 256-thread blocks per SM (128 registers a thread): the packet loop is
+ * latency bound, and 16 resident warps per SM finish the bulk of a run 1.4x
+ * sooner than 8 */
 #ifndef F_MINBLOCKS
-#define F_MINBLOCKS 1
+#define F_MINBLOCKS 2
 #endif
 template <class R>
-__global__ void __launch_bounds__(256, F_MINBLOCKS) transport_fast_kernel(const __grid_constant__ FModel<R> g,
+__global__ void __launch_bounds__(F_BLOCK, F_MINBLOCKS) transport_fast_kernel(const __grid_constant__ FModel<R> g,
                                                              const __grid_constant__ TAcc A, SmemPlan sp) {
   extern __shared__ __align__(16) unsigned char smem[];
   if (blockIdx.x == 0 && threadIdx.x == 0) A.tmark[5] = tp_globaltimer();
@@ -274,7 +280,7 @@ mcg_status launch_fast(mcg_ctx *ctx, int pi, const TModel &tm, const TAcc &ta, i
   g.kd_index = m.kd_index; g.thick = m.thick;
   SmemPlan sp = plan_smem<R>(m.nr, m.nt, m.nlam, m.ncomp, m.uniform_mix);
   MCG_CUDA(ctx, cudaFuncSetAttribute(transport_fast_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.bytes));
-  const int b = block > 0 ? block : 256;
+  const int b = block > 0 ? block : F_BLOCK;
   int grid;
   if (threads > 0) {
     grid = (threads + b - 1) / b;

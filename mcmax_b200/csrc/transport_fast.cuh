@@ -203,19 +203,102 @@ TP_FN void f_pick(const FModel<R> &m, FPkt<R> &p, int i, double Lt, double Ltold
 }
 
 /* ------------------------------------------------------------- geometry */
+/* Distance to the next cell boundary (Trace2edge, MCRadiation.f:1150-1272),
+ * same values as tp_trace2edge.  tp_trace2edge evaluates only the
+ * intersections each entry edge needs, in five branches; lanes of a warp
+ * that entered their cells through different edges then run those branches
+ * one after the other.  Here the two sphere and two cone intersections are
+ * evaluated once for every lane and the entry-edge rules (skip the sphere or
+ * cone just crossed, the re-hit of the same sphere, the midplane plane, the
+ * same-cone re-hit) replace values afterwards.  The fall-back of the
+ * reference (nothing hit: evaluate all four plainly) is the plain values. */
 template <class R>
 TP_FN int f_trace2edge(const FModel<R> &m, FPkt<R> &p, double *v, int *inext, int *jnext) {
-  TPkt t; /* geometry in FP64 */
-  t.x = p.x; t.y = p.y; t.z = p.z;
-  t.vx = p.vx; t.vy = p.vy; t.vz = p.vz;
-  t.i = p.i; t.j = p.j; t.edgeNr = p.edgeNr; t.onEdge = p.onEdge;
-  TModel tm;
-  tm.nt = m.nt;
-  tm.R = m.Rr;
-  tm.Theta = m.Theta;
-  int r = tp_trace2edge(tm, t, v, inext, jnext);
-  p.edgeNr = t.edgeNr;
-  return r;
+  const int nt = m.nt;
+  TPkt t;
+  t.z = p.z;
+  t.vz = p.vz;
+  const double r = (p.x * p.x + p.y * p.y) + p.z * p.z;
+  const double Ra = m.Rr[p.i], Rb = m.Rr[p.i + 1];
+  const double Ta = m.Theta[p.j - 1], Tb = m.Theta[p.j];
+  const double R1 = Ra * Ra, R2 = Rb * Rb, T1 = Ta * Ta, T2 = Tb * Tb;
+  const double b = 2.0 * ((p.x * p.vx + p.y * p.vy) + p.z * p.vz);
+  double pvR1, pvR2, pvT1, pvT2;
+  const int phR1 = tp_hitR(R1, r, b, &pvR1);
+  const int phR2 = tp_hitR(R2, r, b, &pvR2);
+  const int phT1 = tp_hitT(t, T1, r, b, &pvT1);
+  const int phT2 = tp_hitT(t, T2, r, b, &pvT2);
+  int hR1 = phR1, hR2 = phR2, hT1 = phT1, hT2 = phT2;
+  double vR1 = pvR1, vR2 = pvR2, vT1 = pvT1, vT2 = pvT2;
+  if (p.onEdge) {
+    const int e = p.edgeNr;
+    if (e == 1) {
+      hR1 = 0;
+      vR1 = 1e200;
+    } else if (e == 2) {
+      hR2 = 1;
+      vR2 = -b;
+    } else if (e == 3) {
+      hT1 = 0;
+      vT1 = 1e200;
+      if (p.j == nt - 1) {
+        vT2 = -p.z / p.vz;
+        hT2 = vT2 > 0.0;
+      }
+    } else {
+      if (p.j == 1) {
+        hT1 = 0;
+        vT1 = 1e200;
+      }
+      if (p.j != nt - 1) {
+        hT2 = tp_hitTsame(t, T2, b, &vT2);
+      } else {
+        hT2 = 0;
+        vT2 = 1e200;
+      }
+    }
+  }
+  if (!hR1 && !hR2 && !hT1 && !hT2) {
+    hR1 = phR1; hR2 = phR2; hT1 = phT1; hT2 = phT2;
+    vR1 = pvR1; vR2 = pvR2; vT1 = pvT1; vT2 = pvT2;
+    if (!hR1 && !hR2 && !hT1 && !hT2) return 1;
+  }
+  *v = 1e200;
+  *inext = p.i;
+  *jnext = p.j;
+  if (hR1 && vR1 < *v) {
+    *v = vR1;
+    *inext = p.i - 1;
+    *jnext = p.j;
+    p.edgeNr = 2;
+  }
+  if (hR2 && vR2 < *v) {
+    *v = vR2;
+    *inext = p.i + 1;
+    *jnext = p.j;
+    p.edgeNr = 1;
+  }
+  if (hT1 && vT1 < *v) {
+    *v = vT1;
+    *inext = p.i;
+    *jnext = p.j - 1;
+    p.edgeNr = 4;
+  }
+  if (hT2 && vT2 < *v) {
+    *v = vT2;
+    *inext = p.i;
+    *jnext = p.j + 1;
+    p.edgeNr = 3;
+  }
+  if (*jnext == nt) {
+    *jnext = nt - 1;
+    p.edgeNr = 4;
+  }
+  if (*jnext == 0) {
+    *jnext = 1;
+    p.edgeNr = 3;
+  }
+  return 0;
 }
 
 /* ------------------------------------------------------------- rotations */
@@ -706,5 +789,6 @@ TP_FN void f_run_packet(const FModel<R> &m, const TAcc &A0, int64_t pid, TLocal 
     }
   }
 }
+
 
 #endif /* MCMAX_TRANSPORT_FAST_CUH */

@@ -161,9 +161,8 @@ double hc_tinv(const double *kp, double E1, int lo) {
 #include "../../mcmax_b200/csrc/transport_fast.cuh"
 
 template <class R>
-static int hc_fast_impl(const HcModel *h, int nruns_unused, double *EJv, double *EJv2, double *Eabs, double *T, int *Ni,
+static int hc_fast_impl(const HcModel *h, double *EJv, double *EJv2, double *Eabs, double *T, int *Ni,
                         double *spec, unsigned long long *counters, double *tautot, int64_t first, int64_t count) {
-  (void)nruns_unused;
   const int nc = h->nt - 1, ncell = h->nr * nc, nlam = h->nlam, n = nlam - 1, ncomp = h->ncomp;
   std::vector<double> dens(ncell), mass(ncell), dnu(n), star_cdf(n), wlam(nlam);
   for (int c = 0; c < ncell; ++c) {
@@ -293,6 +292,6 @@ static int hc_fast_impl(const HcModel *h, int nruns_unused, double *EJv, double 
 
 extern "C" int hc_fast(const HcModel *h, int mixed, double *EJv, double *EJv2, double *Eabs, double *T, int *Ni,
                        double *spec, unsigned long long *counters, double *tautot, int64_t first, int64_t count) {
-  if (mixed) return hc_fast_impl<float>(h, 1, EJv, EJv2, Eabs, T, Ni, spec, counters, tautot, first, count);
-  return hc_fast_impl<double>(h, 1, EJv, EJv2, Eabs, T, Ni, spec, counters, tautot, first, count);
+  if (mixed) return hc_fast_impl<float>(h, EJv, EJv2, Eabs, T, Ni, spec, counters, tautot, first, count);
+  return hc_fast_impl<double>(h, EJv, EJv2, Eabs, T, Ni, spec, counters, tautot, first, count);
 }
