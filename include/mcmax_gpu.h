@@ -232,6 +232,84 @@ mcg_status mcg_mcradiation(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot_inou
  * (any may be NULL).  Uses EJv/V and EJv2/V^2 of the last mcg_mcradiation. */
 mcg_status mcg_finalize_t(mcg_ctx *ctx, double *T, double *dT, double *dEJv);
 
+/* ----------------------------------------------------------------------
+ * Opacity-surrogate network.  No counterpart in the reference: it stands in
+ * for ComputePart's coated-sphere inner loop (ComputePart.f:318-447) inside
+ * a training box (see mcg_compute_part_surrogate).  6 normalised inputs ->
+ * 4 x 256 SiLU -> 32 outputs; the 256-wide layers run as BF16 tcgen05 MMAs
+ * with FP32 accumulation, forward and backward.
+ *
+ * Parameters are one flat FP32 vector of MCG_MLP_NPARAMS values:
+ *   W0[256][6], b0[256], W1..W3[3][256][256] (out, in), b1..b3[3][256],
+ *   W4[32][256], b4[32].
+ * -------------------------------------------------------------------- */
+#define MCG_MLP_NIN 6
+#define MCG_MLP_NOUT 32
+#define MCG_MLP_NPARAMS 207392
+#define MCG_MLP_MAX_EPOCH_LOG 256
+
+typedef struct {
+  int epochs;          /* passes over the data set */
+  int batch;           /* rows per Adam step, 128 .. 2^20 */
+  float lr, lr_min;    /* Adam step size, cosine decay from lr to lr_min */
+  uint64_t seed;       /* shuffling */
+} mcg_mlp_train_opts;
+
+typedef struct {
+  double final_loss;   /* weighted mean squared error of the last batch */
+  int64_t steps;
+  float device_ms;     /* training time on the device */
+  double epoch_loss[MCG_MLP_MAX_EPOCH_LOG]; /* last-batch loss per epoch */
+} mcg_mlp_train_report;
+
+/* Load / read the parameters; loading also resets the optimizer state. */
+mcg_status mcg_mlp_set_params(mcg_ctx *ctx, const float *params, int64_t nparams);
+mcg_status mcg_mlp_get_params(mcg_ctx *ctx, float *params, int64_t nparams);
+/* y[n][32] = network(x[n][6]), host arrays. */
+mcg_status mcg_mlp_forward(mcg_ctx *ctx, int64_t n, const float *x, float *y);
+/* Loss sum_o w[o] (y - t)^2 averaged over the n rows, and its gradient with
+ * respect to every parameter (flat layout above), for one batch. */
+mcg_status mcg_mlp_gradient(mcg_ctx *ctx, int64_t n, const float *x, const float *t, const float *w,
+                            float *grad, double *loss);
+/* Adam training on a data set of n rows (x[n][6], targets t[n][32], output
+ * weights w[32]), starting from the loaded parameters. */
+mcg_status mcg_mlp_train(mcg_ctx *ctx, int64_t n, const float *x, const float *t, const float *w,
+                         const mcg_mlp_train_opts *opts, mcg_mlp_train_report *report);
+/* D[128][N] = A[128][256] * B[N][256]^T on the tensor cores, BF16 inputs
+ * (raw 16-bit patterns), FP32 result: a self-check of the operand layout. */
+mcg_status mcg_mlp_gemm_check(mcg_ctx *ctx, int N, const uint16_t *A, const uint16_t *B, float *D);
+
+/* ----------------------------------------------------------------------
+ * ComputePart through the surrogate.  No counterpart in the reference.
+ *
+ * Network inputs are (log10 a [micron], log10 lambda [micron], n,
+ * log10 k, porosity, fmax), each mapped from its training box to [-1, 1]:
+ *   log10 a in [-2, 3], log10 lambda in [-1, log10 3000], n in [1.5, 3.5],
+ *   log10 k in [-3.5, log10 2], porosity in [0, 0.6], fmax in [0, 0.8].
+ * Outputs (per single grain size, physical units, see mcg_surrogate_targets):
+ *   [0] log10 kappa_abs, [1] log10 kappa_sca, [2..13] moments chi_1..chi_12
+ *   of F11, [14..26] moments beta_0..beta_12 of F12, [27..31] unused.
+ * -------------------------------------------------------------------- */
+
+/* Training targets: one ComputePart evaluation (same kernels and loop order
+ * as mcg_compute_part) per sample in6[n][6] = (a [micron], lambda [micron],
+ * n, k, porosity, fmax) for a single grain size, material density rho and
+ * nf DHS filling fractions; out[n][32] as above. */
+mcg_status mcg_surrogate_targets(mcg_ctx *ctx, int64_t n, const double *in6, double rho, int nf, float *out);
+
+/* ComputePart for nparts grain bins with the loaded network in place of the
+ * coated-sphere sums.  A bin qualifies when it has one material, no
+ * abundance normalisation, nf == nf_train and every (size, wavelength) input
+ * inside the training box; the others go through mcg_compute_part_batch
+ * (the DHS/Mie kernels).  used[p] (may be NULL) = 1 when the network served
+ * bin p.  Opacities are mass-weighted over the bin's sizes and scaled by
+ * rho_train / rho (kappa ~ 1 / material density); the Mueller matrix is
+ * rebuilt on the 180 bins from the scattering-weighted moments (F22 = F11,
+ * F33 = F44 = sqrt(F11^2 - F12^2), F34 = 0) and normalised as ComputePart
+ * normalises F11 (ComputePart.f:407-415). */
+mcg_status mcg_compute_part_surrogate(mcg_ctx *ctx, int nparts, const mcg_part_in *in, mcg_part_out *out,
+                                      double rho_train, int nf_train, int *used);
+
 #ifdef __cplusplus
 }
 #endif

@@ -74,6 +74,20 @@ class Result(C.Structure):
     ]
 
 
+MLP_NIN, MLP_NOUT, MLP_NPARAMS, MLP_MAX_EPOCH_LOG = 6, 32, 207392, 256
+fp = C.POINTER(C.c_float)
+
+
+class MlpTrainOpts(C.Structure):
+    _fields_ = [("epochs", C.c_int), ("batch", C.c_int), ("lr", C.c_float), ("lr_min", C.c_float),
+                ("seed", C.c_uint64)]
+
+
+class MlpTrainReport(C.Structure):
+    _fields_ = [("final_loss", C.c_double), ("steps", C.c_int64), ("device_ms", C.c_float),
+                ("epoch_loss", C.c_double * MLP_MAX_EPOCH_LOG)]
+
+
 # name -> (restype, argtypes): every symbol the header declares
 SIGNATURES = {
     "mcg_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int]),
@@ -88,6 +102,16 @@ SIGNATURES = {
     "mcg_set_model": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Opacity)]),
     "mcg_mcradiation": (C.c_int, [C.c_void_p, C.POINTER(Run), C.POINTER(C.c_int64), C.POINTER(Result)]),
     "mcg_finalize_t": (C.c_int, [C.c_void_p, dp, dp, dp]),
+    "mcg_mlp_set_params": (C.c_int, [C.c_void_p, fp, C.c_int64]),
+    "mcg_mlp_get_params": (C.c_int, [C.c_void_p, fp, C.c_int64]),
+    "mcg_mlp_forward": (C.c_int, [C.c_void_p, C.c_int64, fp, fp]),
+    "mcg_mlp_gradient": (C.c_int, [C.c_void_p, C.c_int64, fp, fp, fp, fp, C.POINTER(C.c_double)]),
+    "mcg_mlp_train": (C.c_int, [C.c_void_p, C.c_int64, fp, fp, fp, C.POINTER(MlpTrainOpts),
+                                C.POINTER(MlpTrainReport)]),
+    "mcg_surrogate_targets": (C.c_int, [C.c_void_p, C.c_int64, dp, C.c_double, C.c_int, fp]),
+    "mcg_compute_part_surrogate": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(PartIn), C.POINTER(PartOut), C.c_double,
+                                             C.c_int, ip]),
+    "mcg_mlp_gemm_check": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_uint16), C.POINTER(C.c_uint16), fp]),
 }
 
 _lib = None
@@ -120,4 +144,8 @@ def ptr(a):
         return a.ctypes.data_as(dp)
     if a.dtype == np.int32:
         return a.ctypes.data_as(ip)
+    if a.dtype == np.float32:
+        return a.ctypes.data_as(fp)
+    if a.dtype == np.uint16:
+        return a.ctypes.data_as(C.POINTER(C.c_uint16))
     raise TypeError("unsupported dtype %s" % a.dtype)

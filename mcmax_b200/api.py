@@ -226,3 +226,65 @@ def MCRadiation(ctx, model, NphotTot, niter=1, dofastvisc=False, **run):
     for k, v in out.items():
         setattr(model, k, v)
     return n
+
+
+# ---------------------------------------------------------------- surrogate network
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _mlp_methods():
+    """Context methods of the opacity-surrogate network (include/mcmax_gpu.h,
+    mcg_mlp_*)."""
+
+    def mlp_set_params(self, params):
+        p = _f32(params)
+        self._check(self.lib.mcg_mlp_set_params(self.h, _ffi.ptr(p), p.size))
+
+    def mlp_get_params(self):
+        p = np.zeros(_ffi.MLP_NPARAMS, np.float32)
+        self._check(self.lib.mcg_mlp_get_params(self.h, _ffi.ptr(p), p.size))
+        return p
+
+    def mlp_forward(self, x):
+        x = _f32(x).reshape(-1, _ffi.MLP_NIN)
+        y = np.zeros((x.shape[0], _ffi.MLP_NOUT), np.float32)
+        self._check(self.lib.mcg_mlp_forward(self.h, x.shape[0], _ffi.ptr(x), _ffi.ptr(y)))
+        return y
+
+    def mlp_gradient(self, x, t, w):
+        x = _f32(x).reshape(-1, _ffi.MLP_NIN)
+        t = _f32(t).reshape(-1, _ffi.MLP_NOUT)
+        w = _f32(w)
+        g = np.zeros(_ffi.MLP_NPARAMS, np.float32)
+        loss = C.c_double(0.0)
+        self._check(self.lib.mcg_mlp_gradient(self.h, x.shape[0], _ffi.ptr(x), _ffi.ptr(t), _ffi.ptr(w),
+                                              _ffi.ptr(g), C.byref(loss)))
+        return g, loss.value
+
+    def mlp_train(self, x, t, w, epochs=10, batch=16384, lr=2e-3, lr_min=2e-5, seed=1):
+        x = _f32(x).reshape(-1, _ffi.MLP_NIN)
+        t = _f32(t).reshape(-1, _ffi.MLP_NOUT)
+        w = _f32(w)
+        o = _ffi.MlpTrainOpts(int(epochs), int(batch), float(lr), float(lr_min), int(seed))
+        r = _ffi.MlpTrainReport()
+        self._check(self.lib.mcg_mlp_train(self.h, x.shape[0], _ffi.ptr(x), _ffi.ptr(t), _ffi.ptr(w), C.byref(o),
+                                           C.byref(r)))
+        ne = min(int(epochs), _ffi.MLP_MAX_EPOCH_LOG)
+        return dict(final_loss=r.final_loss, steps=r.steps, device_ms=r.device_ms,
+                    epoch_loss=list(r.epoch_loss[:ne]))
+
+    def mlp_gemm_check(self, a_bits, b_bits):
+        a = np.ascontiguousarray(a_bits, dtype=np.uint16)
+        b = np.ascontiguousarray(b_bits, dtype=np.uint16)
+        n = b.shape[0]
+        d = np.zeros((128, n), np.float32)
+        self._check(self.lib.mcg_mlp_gemm_check(self.h, n, _ffi.ptr(a), _ffi.ptr(b), _ffi.ptr(d)))
+        return d
+
+    return dict(mlp_set_params=mlp_set_params, mlp_get_params=mlp_get_params, mlp_forward=mlp_forward,
+                mlp_gradient=mlp_gradient, mlp_train=mlp_train, mlp_gemm_check=mlp_gemm_check)
+
+
+for _k, _v in _mlp_methods().items():
+    setattr(Context, _k, _v)

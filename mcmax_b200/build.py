@@ -23,9 +23,10 @@ UNITS = {
     "transport.cu": ["--fmad=false"],
     "host_tables.cu": ["--fmad=false"],
     "transport_fast.cu": [],
+    "mlp_kernels.cu": [],
 }
 HEADERS = ["detmath.h", "cplx.h", "philox.h", "dhs_core.cuh", "transport_core.cuh", "transport_fast.cuh",
-           "mcg_internal.h"]
+           "mcg_internal.h", "tc_sm100.cuh"]
 
 
 def _nvcc():

@@ -58,6 +58,7 @@ void mcg_destroy(mcg_ctx *ctx) {
   mcg_free_model(ctx->model);
   mcg_free_run(ctx->run);
   if (ctx->part_scratch.p) cudaFree(ctx->part_scratch.p);
+  mcg_free_mlp(ctx);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);

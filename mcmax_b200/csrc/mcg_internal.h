@@ -100,6 +100,8 @@ struct DevRun {
   std::vector<void *> owned;
 };
 
+struct MlpState;
+
 struct mcg_ctx {
   int device = 0;
   int sm_count = 0;
@@ -111,6 +113,8 @@ struct mcg_ctx {
   bool have_run = false;
   /* reusable scratch for ComputePart */
   DevBuf part_scratch;
+  /* opacity-surrogate network (created on first use) */
+  MlpState *mlp = nullptr;
 };
 
 /* error helpers */
@@ -125,6 +129,7 @@ mcg_status mcg_fail(mcg_ctx *ctx, mcg_status st, const char *fmt, ...);
 
 /* entry points implemented in the kernel translation units */
 mcg_status mcg_part_batch_impl(mcg_ctx *ctx, int nparts, const mcg_part_in *in, mcg_part_out *out);
+mcg_status mcg_surrogate_targets_impl(mcg_ctx *ctx, int64_t n, const double *in6, double rho, int nf, float *out);
 mcg_status mcg_part_static_impl(mcg_ctx *ctx, const mcg_part_in *in, mcg_part_out *out);
 mcg_status mcg_set_model_impl(mcg_ctx *ctx, const mcg_grid *grid, const mcg_opacity *opac);
 mcg_status mcg_mcradiation_impl(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot, mcg_result *res);
@@ -133,5 +138,6 @@ mcg_status mcg_fast_run(mcg_ctx *ctx, int precision, const void *tmodel, const v
                         int block, float *ms);
 void mcg_free_model(DevModel &m);
 void mcg_free_run(DevRun &r);
+void mcg_free_mlp(mcg_ctx *ctx);
 
 #endif /* MCG_INTERNAL_H */

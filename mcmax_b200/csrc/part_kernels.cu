@@ -1012,3 +1012,299 @@ mcg_status mcg_part_static_impl(mcg_ctx *ctx, const mcg_part_in *in, mcg_part_ou
   out->n_mie = n_mie;
   return MCG_OK;
 }
+
+/* ------------------------------------------------------------------------
+ * Training targets of the opacity surrogate (mcg_surrogate_targets).
+ *
+ * Each sample is one ComputePart call for a single grain size: one .lnk
+ * material (n, k at one wavelength) Bruggeman-blended with a vacuum
+ * fraction `porosity` (ComputePart.f:227-252), ns = 1, nf DHS filling
+ * fractions on [0.01, fmax] (ComputePart.f:266-274), no abundance
+ * normalisation.  The samples go through the same dhs_kernel, mie_kernel
+ * and accum_kernel as mcg_compute_part (one output row per sample), and
+ * moments_kernel reduces each row's Mueller elements to the targets:
+ *   [0] log10 kappa_abs, [1] log10 kappa_sca (cm^2/g),
+ *   [2 + l - 1] chi_l, l = 1..12  moments of F11: sum_j F11_j P_l(mu_j) w_j
+ *   [14 + l]    beta_l, l = 0..12 moments of F12, both / sum_j F11_j w_j,
+ *   mu_j = cos((j + 1/2) deg), w_j = sin((j + 1/2) deg); [27..31] = 0.
+ * ---------------------------------------------------------------------- */
+namespace {
+
+constexpr int SURR_L = 12;
+
+__global__ void __launch_bounds__(128) moments_kernel(int nrows, const double *kabs, const double *ksca,
+                                                      const double *Fout, float *out) {
+  const int lane = threadIdx.x & 31;
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (row >= nrows) return;
+  double s11[SURR_L + 1], s12[SURR_L + 1];
+#pragma unroll
+  for (int l = 0; l <= SURR_L; ++l) s11[l] = s12[l] = 0.0;
+  for (int j = lane; j < NA; j += WARP) {
+    const double th = DHS_PI * ((double)j + 0.5) / (double)NA;
+    const double mu = cos(th), w = sin(th);
+    const double f11 = Fout[((size_t)row * 6 + 0) * NA + j] * w;
+    const double f12 = Fout[((size_t)row * 6 + 1) * NA + j] * w;
+    double p0 = 1.0, p1 = mu;
+    s11[0] += f11;
+    s12[0] += f12;
+    s11[1] += f11 * p1;
+    s12[1] += f12 * p1;
+#pragma unroll
+    for (int l = 1; l < SURR_L; ++l) {
+      const double p2 = ((2.0 * l + 1.0) * mu * p1 - (double)l * p0) / (double)(l + 1);
+      s11[l + 1] += f11 * p2;
+      s12[l + 1] += f12 * p2;
+      p0 = p1;
+      p1 = p2;
+    }
+  }
+#pragma unroll
+  for (int l = 0; l <= SURR_L; ++l)
+    for (int s = 16; s > 0; s >>= 1) {
+      s11[l] += __shfl_down_sync(0xffffffffu, s11[l], s);
+      s12[l] += __shfl_down_sync(0xffffffffu, s12[l], s);
+    }
+  if (lane == 0) {
+    float *o = out + (size_t)row * 32;
+    o[0] = (float)log10(fmax(kabs[row], 1e-30));
+    o[1] = (float)log10(fmax(ksca[row], 1e-30));
+    const double inv = s11[0] > 0.0 ? 1.0 / s11[0] : 0.0;
+    for (int l = 1; l <= SURR_L; ++l) o[1 + l] = (float)(s11[l] * inv);
+    for (int l = 0; l <= SURR_L; ++l) o[14 + l] = (float)(s12[l] * inv);
+    for (int k = 27; k < 32; ++k) o[k] = 0.0f;
+  }
+}
+
+}  // namespace
+
+mcg_status mcg_surrogate_targets_impl(mcg_ctx *ctx, int64_t n, const double *in6, double rho, int nf, float *out) {
+  if (n < 1 || !in6 || !out || nf < 1 || nf > 64 || !(rho > 0.0))
+    return mcg_fail(ctx, MCG_ERR_ARG, "surrogate_targets: n >= 1, 1 <= nf <= 64, rho > 0 and non-null arrays");
+  for (int64_t s = 0; s < n; ++s) {
+    const double *q = in6 + 6 * s;
+    if (!(q[0] > 0.0) || !(q[1] > 0.0) || !(q[2] > 0.0) || !(q[3] >= 0.0) || !(q[4] >= 0.0) || !(q[4] < 1.0) ||
+        !(q[5] >= 0.0) || !(q[5] < 1.0))
+      return mcg_fail(ctx, MCG_ERR_ARG, "surrogate_targets: sample %lld outside the physical range", (long long)s);
+  }
+  /* order by size parameter so each chunk's recurrence lengths are alike */
+  std::vector<int64_t> order((size_t)n);
+  for (int64_t s = 0; s < n; ++s) order[(size_t)s] = s;
+  std::sort(order.begin(), order.end(), [&](int64_t a, int64_t b) {
+    return in6[6 * a] / in6[6 * a + 1] < in6[6 * b] / in6[6 * b + 1];
+  });
+  double mu[90], sinw[NA], tot2 = 0.0;
+  for (int i = 1; i <= 90; ++i) mu[i - 1] = cos(((double)i - 0.5) / (double)(NA / 2) * DHS_PI / 2.0);
+  for (int j = 1; j <= NA; ++j) sinw[j - 1] = sin(DHS_PI * ((double)j - 0.5) / (double)NA);
+  for (int j = 0; j < NA; ++j) tot2 = tot2 + sinw[j];
+  const int64_t CH = 65536;
+  cudaStream_t st = ctx->stream;
+  const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;
+  std::vector<float> tout;
+  for (int64_t c0 = 0; c0 < n; c0 += CH) {
+    const int m = (int)std::min<int64_t>(CH, n - c0);
+    std::vector<double> srcore, srshell, swvno, smre, smim, mrad, mlam, me1, me2, pflat;
+    std::vector<int8_t> sstat;
+    std::vector<int> mneed, rowpart(m);
+    std::vector<PartDev> pd(m);
+    std::vector<size_t> poff(m);
+    int maxnmx1 = 150, maxmie = 0;
+    for (int r = 0; r < m; ++r) {
+      const double *q = in6 + 6 * order[(size_t)(c0 + r)];
+      const double a = q[0], lam = q[1], por = q[4], fmx = q[5];
+      /* Bruggeman blend with vacuum (ComputePart.f:227-252), nm = 1 */
+      double e1b, e2b;
+      {
+        const double e1s[2] = {q[2], 1.0}, e2s[2] = {q[3], 0.0}, ab[2] = {1.0 - por, por};
+        blender(e1s, e2s, ab, 2, &e1b, &e2b);
+      }
+      const double rav = (1.0 - por) * rho;
+      /* filling fractions (ComputePart.f:266-274) */
+      int nfs = nf;
+      std::vector<double> f(nf, 0.0), wf(nf, 0.0);
+      if (fmx == 0.0) nfs = 1;
+      if (nfs > 1 && fmx > 0.01) {
+        gauleg2(0.01, fmx, f.data(), wf.data(), nfs);
+      } else if (fmx == 0.0) {
+        f[0] = 0.0;
+        wf[0] = 1.0;
+      } else {
+        nfs = 1;
+        f[0] = fmx;
+        wf[0] = 1.0;
+      }
+      const double wvno = 2.0 * DHS_PI / lam;
+      PartDev &d = pd[r];
+      d.nlam = 1;
+      d.nmc = 1;
+      d.ns = 1;
+      d.nf = nfs;
+      d.samp0 = (int)sstat.size();
+      d.mie0 = (int)mneed.size();
+      d.out0 = r;
+      d.mscale = 1.0;
+      poff[r] = pflat.size();
+      pflat.push_back(1.0); /* frac */
+      pflat.push_back(rav); /* rho */
+      pflat.push_back(a);   /* r1 */
+      pflat.push_back(1.0); /* nr */
+      for (int i = 0; i < nfs; ++i) pflat.push_back(wf[i]);
+      rowpart[r] = r;
+      int need = 0;
+      for (int i = 0; i < nfs; ++i) {
+        const double rad = a / pow(1.0 - f[i], 1.0 / 3.0);
+        int8_t s8 = S_DHS;
+        if (f[i] == 0.0 || a * wvno > 10000.0) {
+          s8 = S_MIE;
+          need = 1;
+        }
+        srcore.push_back(f[i] > 0.0 ? rad * pow(f[i], 1.0 / 3.0) : 0.0);
+        srshell.push_back(rad);
+        swvno.push_back(wvno);
+        smre.push_back(e1b);
+        smim.push_back(e2b);
+        sstat.push_back(s8);
+        if (s8 == S_DHS) maxnmx1 = std::max(maxnmx1, dhs_nmx1(rad, wvno, e1b, -e2b));
+      }
+      double lm = lam;
+      if (a / lm >= 5000.0) lm = a / 5000.0;
+      mrad.push_back(a);
+      mlam.push_back(lm);
+      me1.push_back(e1b);
+      me2.push_back(e2b);
+      mneed.push_back(need);
+      int nmax, nfi, nD;
+      mie_counts(a, lm, e1b, e2b, &nmax, &nfi, &nD);
+      maxmie = std::max(maxmie, std::max(nfi, nD));
+    }
+    const int nsamp = (int)sstat.size(), nslot = (int)mneed.size();
+    if (maxnmx1 + 1 > DHS_LL) maxnmx1 = DHS_LL;
+    const int dcap = maxnmx1 + 2, mcap = maxmie + 2;
+    if ((long long)mcap > 50000000LL)
+      return mcg_fail(ctx, MCG_ERR_LIMIT, "surrogate_targets: Mie term count %d beyond the 5e7 limit", maxmie);
+    std::vector<void *> own;
+    cudaError_t ce = cudaSuccess;
+    auto fail_free = [&](const char *what) {
+      for (void *p : own) cudaFree(p);
+      return mcg_fail(ctx, MCG_ERR_NOMEM, "surrogate_targets: cudaMalloc of %s failed: %s", what,
+                      cudaGetErrorString(ce));
+    };
+#define ALLOC(T, cnt, name)               \
+  dev_alloc<T>(own, (size_t)(cnt), ce);   \
+  if (ce != cudaSuccess) return fail_free(name)
+    double *d_rcore = ALLOC(double, nsamp, "rcore");
+    double *d_rshell = ALLOC(double, nsamp, "rshell");
+    double *d_wvno = ALLOC(double, nsamp, "wvno");
+    double *d_mre = ALLOC(double, nsamp, "mre");
+    double *d_mim = ALLOC(double, nsamp, "mim");
+    int8_t *d_stat = ALLOC(int8_t, nsamp, "status");
+    double *d_sF = ALLOC(double, (size_t)nsamp * 4 * NA, "sample F");
+    double *d_scs = ALLOC(double, (size_t)nsamp * 2, "sample cs");
+    double *d_mrad = ALLOC(double, nslot, "mie rad");
+    double *d_mlam = ALLOC(double, nslot, "mie lam");
+    double *d_me1 = ALLOC(double, nslot, "mie e1");
+    double *d_me2 = ALLOC(double, nslot, "mie e2");
+    int *d_mneed = ALLOC(int, nslot, "mie need");
+    double *d_mF = ALLOC(double, (size_t)nslot * 4 * NA, "mie F");
+    double *d_mcs = ALLOC(double, (size_t)nslot * 2, "mie cs");
+    int8_t *d_mok = ALLOC(int8_t, nslot, "mie ok");
+    double *d_mu = ALLOC(double, 90, "mu");
+    double *d_sinw = ALLOC(double, NA, "sinw");
+    unsigned long long *d_next = ALLOC(unsigned long long, 2, "counters");
+    PartDev *d_parts = ALLOC(PartDev, m, "parts");
+    int *d_rowpart = ALLOC(int, m, "row map");
+    double *d_kabs = ALLOC(double, m, "kabs");
+    double *d_ksca = ALLOC(double, m, "ksca");
+    double *d_kext = ALLOC(double, m, "kext");
+    double *d_Fout = ALLOC(double, (size_t)m * 6 * NA, "F out");
+    double *d_rhoav = ALLOC(double, m, "rho_av");
+    double *d_pflat = ALLOC(double, pflat.size(), "part tables");
+    float *d_out = ALLOC(float, (size_t)m * 32, "targets");
+#undef ALLOC
+    for (int r = 0; r < m; ++r) {
+      double *b = d_pflat + poff[r];
+      pd[r].frac = b;
+      pd[r].rho = b + 1;
+      pd[r].r1 = b + 2;
+      pd[r].nr = b + 3;
+      pd[r].wf = b + 4;
+    }
+#define H2D(dst, src, cnt) cudaMemcpyAsync(dst, src, (size_t)(cnt) * sizeof(*(src)), cudaMemcpyHostToDevice, st)
+    H2D(d_rcore, srcore.data(), nsamp);
+    H2D(d_rshell, srshell.data(), nsamp);
+    H2D(d_wvno, swvno.data(), nsamp);
+    H2D(d_mre, smre.data(), nsamp);
+    H2D(d_mim, smim.data(), nsamp);
+    H2D(d_stat, sstat.data(), nsamp);
+    H2D(d_mrad, mrad.data(), nslot);
+    H2D(d_mlam, mlam.data(), nslot);
+    H2D(d_me1, me1.data(), nslot);
+    H2D(d_me2, me2.data(), nslot);
+    H2D(d_mneed, mneed.data(), nslot);
+    H2D(d_mu, mu, 90);
+    H2D(d_sinw, sinw, NA);
+    H2D(d_parts, pd.data(), m);
+    H2D(d_rowpart, rowpart.data(), m);
+    H2D(d_pflat, pflat.data(), pflat.size());
+#undef H2D
+    cudaMemsetAsync(d_next, 0, 2 * sizeof(unsigned long long), st);
+    cudaMemsetAsync(d_mok, 0, nslot, st);
+    const size_t budget = (size_t)1 << 31;
+    auto warps_for = [&](size_t per_warp, int work) {
+      long long w = std::min<long long>((long long)sms * 32, (long long)work);
+      long long wb = (long long)(budget / std::max<size_t>(per_warp, 1));
+      return (int)std::max<long long>(1, std::min(w, wb));
+    };
+    const int nw_dhs = (warps_for((size_t)4 * dcap * sizeof(cx), nsamp) + 3) / 4 * 4;
+    const int nw_mie = (warps_for((size_t)8 * mcap * sizeof(double), nslot) + 3) / 4 * 4;
+    const size_t scratch_bytes =
+        std::max((size_t)nw_dhs * 4 * dcap * sizeof(cx), (size_t)nw_mie * 8 * mcap * sizeof(double));
+    if (ctx->part_scratch.bytes < scratch_bytes) {
+      if (ctx->part_scratch.p) cudaFree(ctx->part_scratch.p);
+      ctx->part_scratch.p = nullptr;
+      ctx->part_scratch.bytes = 0;
+      ce = cudaMalloc(&ctx->part_scratch.p, scratch_bytes);
+      if (ce != cudaSuccess) return fail_free("recurrence scratch");
+      ctx->part_scratch.bytes = scratch_bytes;
+    }
+    SampleDev sd{d_rcore, d_rshell, d_wvno, d_mre, d_mim, d_stat, d_sF, d_scs, d_mneed, nsamp};
+    dhs_kernel<<<(nw_dhs + 3) / 4, 128, 0, st>>>(sd, d_mu, (cx *)ctx->part_scratch.p, dcap, d_next);
+    std::vector<int8_t> stat(nsamp);
+    cudaMemcpyAsync(stat.data(), d_stat, nsamp, cudaMemcpyDeviceToHost, st);
+    ce = cudaStreamSynchronize(st);
+    if (ce != cudaSuccess) {
+      for (void *p : own) cudaFree(p);
+      return mcg_fail(ctx, MCG_ERR_CUDA, "surrogate_targets: DHS kernel failed: %s", cudaGetErrorString(ce));
+    }
+    bool changed = false;
+    for (int r = 0; r < m; ++r)
+      for (int i = 0; i < pd[r].nf; ++i)
+        if (stat[pd[r].samp0 + i] == S_DHS_ERR && !mneed[r]) {
+          mneed[r] = 1;
+          changed = true;
+        }
+    if (changed) cudaMemcpyAsync(d_mneed, mneed.data(), (size_t)nslot * sizeof(int), cudaMemcpyHostToDevice, st);
+    MieDev md{d_mrad, d_mlam, d_me1, d_me2, d_mneed, d_mF, d_mcs, d_mok, nslot};
+    mie_kernel<<<(nw_mie + 3) / 4, 128, 0, st>>>(md, (double *)ctx->part_scratch.p, mcap, d_next + 1);
+    AccDev ad{d_parts, m, d_rowpart, d_stat, d_sF, d_scs, d_mF, d_mcs, d_sinw, tot2,
+              d_kabs, d_ksca, d_kext, d_Fout, d_rhoav, m};
+    accum_kernel<<<(m + 3) / 4, 128, 0, st>>>(ad);
+    moments_kernel<<<(m + 3) / 4, 128, 0, st>>>(m, d_kabs, d_ksca, d_Fout, d_out);
+    ce = cudaGetLastError();
+    tout.resize((size_t)m * 32);
+    std::vector<int8_t> mok(nslot);
+    cudaMemcpyAsync(tout.data(), d_out, tout.size() * sizeof(float), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(mok.data(), d_mok, nslot, cudaMemcpyDeviceToHost, st);
+    cudaError_t se = cudaStreamSynchronize(st);
+    for (void *p : own) cudaFree(p);
+    if (ce != cudaSuccess || se != cudaSuccess)
+      return mcg_fail(ctx, MCG_ERR_CUDA, "surrogate_targets: kernels failed: %s",
+                      cudaGetErrorString(ce != cudaSuccess ? ce : se));
+    for (int q = 0; q < nslot; ++q)
+      if (mneed[q] && !mok[q])
+        return mcg_fail(ctx, MCG_ERR_LIMIT, "surrogate_targets: homogeneous-sphere fallback did not fit");
+    for (int r = 0; r < m; ++r)
+      memcpy(out + 32 * order[(size_t)(c0 + r)], tout.data() + (size_t)r * 32, 32 * sizeof(float));
+  }
+  return MCG_OK;
+}

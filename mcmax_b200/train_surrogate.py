@@ -1,0 +1,48 @@
+"""Train the opacity surrogate on the GPU and write its weights.
+
+    python -m mcmax_b200.train_surrogate --samples 2000000 --out surrogate.npz
+
+Samples: a scrambled Sobol sequence over the training box (see surrogate.py);
+targets: ComputePart on the GPU for each sample (one grain size, nf = 20,
+material density 3 g/cm^3); training: the tensor-core forward/backward
+kernels with Adam.  Prints the held-out error of the network."""
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import api
+from . import surrogate as S
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--samples", type=int, default=2_000_000)
+    ap.add_argument("--test", type=int, default=20_000)
+    ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--batch", type=int, default=8192)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--out", default="surrogate.npz")
+    a = ap.parse_args()
+    ctx = api.Context(0)
+    t0 = time.perf_counter()
+    X = S.sobol_samples(a.samples, seed=a.seed)
+    T = S.targets(ctx, X)
+    t_targets = time.perf_counter() - t0
+    params, info = S.train(ctx, X, T, epochs=a.epochs, batch=a.batch, lr=a.lr, seed=a.seed)
+    Xt = S.sobol_samples(a.test, seed=a.seed + 1000)
+    Tt = S.targets(ctx, Xt)
+    Y = ctx.mlp_forward(S.normalize(Xt))
+    err = np.abs(Y - Tt)
+    info.update(targets_s=t_targets, test_n=a.test,
+                test_median_dex_kabs=float(np.median(err[:, 0])), test_p95_dex_kabs=float(np.percentile(err[:, 0], 95)),
+                test_median_dex_ksca=float(np.median(err[:, 1])), test_p95_dex_ksca=float(np.percentile(err[:, 1], 95)),
+                test_median_g=float(np.median(err[:, 2])))
+    S.save(a.out, params, info)
+    print(json.dumps({k: (v.tolist() if isinstance(v, np.ndarray) else v) for k, v in info.items()}))
+
+
+if __name__ == "__main__":
+    main()
