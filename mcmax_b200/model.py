@@ -157,6 +157,23 @@ def wavelength_grid(lam1, lam2, nlam):
     return lam, nu
 
 
+def theta_centres(ntheta):
+    """cell-centre angles theta_av (radians, j = 1..ntheta, pole to
+    midplane) of the theta grid of Init.f:2779-2890 (no refinement)"""
+    nT = ntheta + 1
+    th = []
+    k = nT // 2
+    for j in range(1, k + 1):
+        th.append((j - 1) / (k - 1))
+        th.append(math.cos(0.5 * math.pi * j / (k + 1)))
+    i = len(th)
+    if i < nT:
+        for j in range(i + 1, nT + 1):
+            th.append((j - i + 1) / (nT - i + 1))
+    th = sorted(th)[:nT]
+    return np.array([math.acos((th[nT - i] + th[nT - i - 1]) / 2.0) for i in range(1, nT)])
+
+
 def spatial_grid(rstar_cm, rin, rout, nrad, ntheta):
     """Edges R[0..nR] (AU, R[0] = Rstar) and cos-theta edges Theta[0..nTheta-1]
     following Init.f:2779-2890 without refinement (ntspan = ntlev = 0)."""
@@ -232,6 +249,61 @@ def zones_density(R, Theta, thet, zones):
         total += zd
     dens[1:] = 1e-60 + total[1:]
     return dens, V
+
+
+def grain_rv(amin, amax, apow, ns):
+    """rv = sqrt(<a^2>) of a bin's ns sizes in cm (ComputePart.f:950-976;
+    number weights n(a) ~ a^(1 - apow) of ComputePart.f:276-292)"""
+    if ns == 1:
+        r = np.array([10 ** ((math.log10(amin) + math.log10(amax)) / 2)])
+        nr = np.ones(1)
+    else:
+        r = 10 ** (math.log10(amin) + (math.log10(amax) - math.log10(amin)) * np.arange(ns) / (ns - 1))
+        nr = r ** (1.0 - apow)
+    return math.sqrt((nr * r * r).sum() / nr.sum()) * 1e-4
+
+
+def fixed_mp_settling(R, Theta, ntheta, dens, V, w, rho_grain, rv, alpha, zone, gas2dust=100.0, gamma=2.0):
+    """Vertical settling of every grain in a fixed-structure zone.
+
+    FixedMPSettling (MPSettling.f:132-168): per ring i the gas surface
+    density and, per grain ii, hH = (1/(1+gamma))^(1/4) sqrt(alpha Sigma /
+    (sqrt(2 pi) rho_ii rv_ii)), scale factor hH / sqrt(1 + hH^2).  The
+    grain's density in the ring then takes the zone profile with the scale
+    height times that factor, renormalised to the grain's mass in the ring
+    (DiskStructure.f:345-380, fix_struct zones).  dens (nR, nc), V (nR, nc),
+    w (nR, nc, ngrains) are the unsettled dust density, cell volumes and
+    grain mass fractions; returns the settled dens and w."""
+    nR, nc = dens.shape
+    ng = w.shape[2]
+    R_av = AU * 10.0 ** ((np.log10(R[:-1]) + np.log10(R[1:])) / 2.0)
+    th = theta_centres(ntheta)
+    dens_new = dens.copy()
+    w_new = w.copy()
+    c1 = (1.0 / (1.0 + gamma)) ** 0.25
+    for i in range(1, nR):
+        rr = R_av[i] * np.sin(th) / AU
+        zz = R_av[i] * np.cos(th) / AU
+        sigma = (dens[i] * gas2dust * V[i]).sum() / (math.pi * (R[i + 1] ** 2 - R[i] ** 2) * AU ** 2)
+        rho_g = np.zeros((nc, ng))
+        for ii in range(ng):
+            hH = c1 * math.sqrt(alpha * sigma / (math.sqrt(2.0 * math.pi) * rho_grain[ii] * rv[ii]))
+            scale = hH / math.sqrt(1.0 + hH * hH)
+            hr = scale * zone["sh"] * (rr / zone["rsh"]) ** zone["shpow"]
+            prof = np.zeros(nc)
+            ok = rr > 0.0  # the polar cell (theta_av = 0) gets the density floor
+            f2 = -(zz[ok] / hr[ok]) ** 2
+            if ok[nc - 1]:
+                f2[-1] = 0.0
+            prof[ok] = np.exp(np.log(rr[ok] ** (-zone["denspow"]) / hr[ok]) + f2)
+            m0 = (dens[i] * V[i] * w[i, :, ii]).sum()
+            m1 = (prof * V[i]).sum()
+            rg = prof * (m0 / m1) if m1 > 0 else np.zeros(nc)
+            rho_g[:, ii] = np.maximum(rg, 1e-50)
+        d = rho_g.sum(1)
+        dens_new[i] = d
+        w_new[i] = rho_g / d[:, None]
+    return dens_new, w_new
 
 
 def mrn_abundances(rgrain, rmin, rmax, index):
@@ -346,6 +418,80 @@ def disk_model(ctx, *, tstar=10000.0, rstar=2.5, rin=0.5, rout=100.0, mdust=1e-5
                  V=V.reshape(-1), ncomp=ncomp, comp_w=comp_w, nlam=nlam, lam=lam, nu=nu, Kabs=Kabs, Ksca=Ksca,
                  F=F, BB=BB, Fstar=Fstar, Lstar=Lstar, Tstar=tstar, Rstar_cm=rstar_cm, scat_how=scat_how,
                  bins=bins, w=w)
+
+
+LEARNED_COMPOSITIONS = (
+    # k prefactor of the synthetic .lnk, porosity, DHS fmax
+    (0.003, 0.2, 0.8),
+    (0.03, 0.4, 0.5),
+    (0.3, 0.0, 0.8),
+)
+
+
+def learned_disk_parts(lam, ngrains=50, amin=0.01, amax=1000.0, apow=3.5, ns=5, nf=20, rho=3.0,
+                       compositions=LEARNED_COMPOSITIONS):
+    """ComputePart inputs of the learned-opacities deck: per composition
+    ngrains log bins from amin to amax (one synthetic .lnk each)"""
+    bins = grain_bins(amin, amax, ngrains)
+    parts = []
+    for kp, por, fmax in compositions:
+        n, k = synthetic_lnk(lam, kp)
+        for a, b in bins:
+            parts.append(dict(lam=lam, e1=np.array([n]), e2=np.array([k]), frac=np.ones(1), rho=np.full(1, rho),
+                              amin=a, amax=b, apow=apow, fmax=fmax, porosity=por, blend=True, ns=ns, nf=nf))
+    return parts, bins
+
+
+def learned_disk_model(ctx, *, opacity="dhs", params=None, tstar=10000.0, rstar=2.5, rin=0.5, rout=100.0,
+                       mdust=1e-3, sh=0.05 * math.sqrt(2.0), rsh=1.0, shpow=1.125, denspow=1.0, nrad=200,
+                       ntheta=120, lam1=0.1, lam2=3000.0, nlam=200, ngrains=50, amin=0.01, amax=1000.0, apow=3.5,
+                       ns=5, nf=20, rho=3.0, alpha=1e-3, scat_how=2, compositions=LEARNED_COMPOSITIONS):
+    """The learned-opacities deck: three compositions in ngrains log bins
+    each, equal mass per composition and MRN within it, vertically settled
+    with alpha (FixedMPSettling), opacities from the DHS kernels
+    (opacity='dhs') or from the surrogate network (opacity='surrogate').
+    Returns (model, opacity-stage seconds, bins served by the network)."""
+    import time
+    rstar_cm = rstar * RSUN
+    lam, nu = wavelength_grid(lam1, lam2, nlam)
+    R, Theta, thet, SinTheta = spatial_grid(rstar_cm, rin, rout, nrad, ntheta)
+    zone = dict(rin=rin, rout=rout, mdust=mdust, denspow=denspow, sh=sh, rsh=rsh, shpow=shpow)
+    dens, V = zones_density(R, Theta, thet, [zone])
+    BB = api.bb_table(lam)
+    Fstar = np.array([math.pi * rstar_cm ** 2 * api.planck(tstar, x) for x in lam])
+    Lstar = integrate(nu, Fstar)
+    parts, bins = learned_disk_parts(lam, ngrains, amin, amax, apow, ns, nf, rho, compositions)
+    t0 = time.perf_counter()
+    if opacity == "dhs":
+        res = ctx.compute_part_batch(parts)
+        served = 0
+    elif opacity == "surrogate":
+        from . import surrogate as S
+        res, used = S.compute_part_surrogate(ctx, parts, params)
+        served = int(used.sum())
+    else:
+        raise ValueError("opacity must be 'dhs' or 'surrogate'")
+    t_opac = time.perf_counter() - t0
+    Kabs = np.array([r["kabs"] for r in res])
+    Ksca = np.array([r["ksca"] for r in res])
+    F = np.array([r["F"] for r in res])
+    if scat_how == 0:
+        Ksca = np.zeros_like(Ksca)
+    ncomp = len(parts)
+    rg = [math.sqrt(a * b) * 1e-4 for a, b in bins]
+    wmrn = mrn_abundances(rg, amin * 1e-4, amax * 1e-4, apow)
+    w0 = np.concatenate([wmrn / len(compositions) for _ in compositions])
+    nr = R.size - 1
+    nc = Theta.size - 1
+    w = np.tile(w0, (nr, nc, 1))
+    rho_grain = np.array([r["rho_av"] for r in res])
+    rv = np.array([grain_rv(p["amin"], p["amax"], apow, ns) for p in parts])
+    dens2, w2 = fixed_mp_settling(R, Theta, ntheta, dens, V, w, rho_grain, rv, alpha, zone)
+    m = Model(nr=nr, nt=Theta.size, R=R, Theta=Theta, SinTheta=SinTheta, thet=thet, dens=dens2.reshape(-1),
+              V=V.reshape(-1), ncomp=ncomp, comp_w=w2.reshape(nr * nc, ncomp), nlam=nlam, lam=lam, nu=nu,
+              Kabs=Kabs, Ksca=Ksca, F=F, BB=BB, Fstar=Fstar, Lstar=Lstar, Tstar=tstar, Rstar_cm=rstar_cm,
+              scat_how=scat_how, bins=bins, w=w0)
+    return m, t_opac, served
 
 
 CONFIGS = {

@@ -27,7 +27,7 @@ RHO_TRAIN = 3.0
 NF_TRAIN = 20
 # loss weight per output: the two opacities, the F11 moments, the F12 moments
 OUT_WEIGHT = np.zeros(NOUT, np.float32)
-OUT_WEIGHT[0:2] = 4.0
+OUT_WEIGHT[0:2] = 16.0
 OUT_WEIGHT[2:14] = 1.0
 OUT_WEIGHT[14:27] = 0.5
 
@@ -84,7 +84,7 @@ def fold_output_scaling(params, mean, std):
     return p
 
 
-def train(ctx, samples, T, epochs=40, batch=16384, lr=2e-3, lr_min=2e-5, seed=1):
+def train(ctx, samples, T, epochs=300, batch=8192, lr=2e-3, lr_min=2e-5, seed=1):
     """Train on (samples, targets); returns (params, info).  Targets are
     standardised per output for training and the scaling is folded into
     the output layer, so the returned network outputs physical targets."""

@@ -18,9 +18,9 @@ from . import surrogate as S
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--samples", type=int, default=2_000_000)
+    ap.add_argument("--samples", type=int, default=1 << 21)
     ap.add_argument("--test", type=int, default=20_000)
-    ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--epochs", type=int, default=300)
     ap.add_argument("--batch", type=int, default=8192)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed", type=int, default=1)
@@ -31,7 +31,7 @@ def main():
     X = S.sobol_samples(a.samples, seed=a.seed)
     T = S.targets(ctx, X)
     t_targets = time.perf_counter() - t0
-    params, info = S.train(ctx, X, T, epochs=a.epochs, batch=a.batch, lr=a.lr, seed=a.seed)
+    params, info = S.train(ctx, X, T, epochs=a.epochs, batch=a.batch, lr=a.lr, lr_min=a.lr * 1e-2, seed=a.seed)
     Xt = S.sobol_samples(a.test, seed=a.seed + 1000)
     Tt = S.targets(ctx, Xt)
     Y = ctx.mlp_forward(S.normalize(Xt))
