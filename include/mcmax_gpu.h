@@ -228,6 +228,42 @@ typedef struct {
 mcg_status mcg_mcradiation(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot_inout,
                            mcg_result *res);
 
+/* ----------------------------------------------------------------------
+ * Many models in one launch (no counterpart in the reference, which runs
+ * one model per process).  Models registered with mcg_add_model keep their
+ * device tables; mcg_mcradiation_batch runs the packet loops of several of
+ * them in one persistent launch (packets of all models share one work
+ * counter), each model with its own run parameters, accumulators and result.
+ * -------------------------------------------------------------------- */
+#define MCG_BATCH_MAX 1024
+
+typedef struct {
+  int block;          /* threads per block (multiple of 32, <= 256); 0: tuned or 256 */
+  int blocks_per_sm;  /* resident blocks per SM in the persistent grid; 0: tuned or 2 */
+  int chunk;          /* packets a thread takes per visit of the work counter; 0: tuned or 1 */
+  int autotune;       /* 1: time candidate shapes on a short trial (1/50 of the packets)
+                         before the run and keep the fastest for later calls with the
+                         same models and packet counts */
+  int use_graph;      /* 1: capture the launch sequence (accumulator resets, the batched
+                         kernel, the per-model combination) in a CUDA graph and replay it
+                         on later calls with the same models, packet counts and shape */
+  float device_ms;    /* out: device time of the batched launch */
+} mcg_batch_opts;
+
+/* Build the tables of a model (as mcg_set_model) and keep them; *model_id
+ * names it in mcg_mcradiation_batch.  The model used by mcg_mcradiation is
+ * not affected. */
+mcg_status mcg_add_model(mcg_ctx *ctx, const mcg_grid *grid, const mcg_opacity *opac, int *model_id);
+/* One launch over nmodels kept models: model k runs runs[k] with
+ * nphot_inout[k] packets and writes results[k] (arrays as for
+ * mcg_mcradiation).  All runs use the same precision (FP64 or MIXED).
+ * runs[0].threads == 1 runs every packet on one thread in model order (the
+ * serial order of mcg_mcradiation with threads = 1, for replay checks: the
+ * same packets, equal up to floating-point contraction differences).
+ * opts may be NULL (defaults); the launch shape used is written back. */
+mcg_status mcg_mcradiation_batch(mcg_ctx *ctx, int nmodels, const int *model_ids, const mcg_run *runs,
+                                 int64_t *nphot_inout, mcg_result *results, mcg_batch_opts *opts);
+
 /* Temperatures from the last run (Main.f:498-549): T, dT, dEJv per cell
  * (any may be NULL).  Uses EJv/V and EJv2/V^2 of the last mcg_mcradiation. */
 mcg_status mcg_finalize_t(mcg_ctx *ctx, double *T, double *dT, double *dEJv);
@@ -275,6 +311,11 @@ mcg_status mcg_mlp_gradient(mcg_ctx *ctx, int64_t n, const float *x, const float
  * weights w[32]), starting from the loaded parameters. */
 mcg_status mcg_mlp_train(mcg_ctx *ctx, int64_t n, const float *x, const float *t, const float *w,
                          const mcg_mlp_train_opts *opts, mcg_mlp_train_report *report);
+/* Device time of one forward pass over n device-resident rows and of one
+ * training step (forward, backward, Adam) on `batch` rows, each averaged
+ * over `iters` repetitions after two untimed ones; the loaded parameters
+ * are restored afterwards (the optimizer state is reset). */
+mcg_status mcg_mlp_time(mcg_ctx *ctx, int64_t n, int iters, int batch, float *fwd_ms, float *step_ms);
 /* D[128][N] = A[128][256] * B[N][256]^T on the tensor cores, BF16 inputs
  * (raw 16-bit patterns), FP32 result: a self-check of the operand layout. */
 mcg_status mcg_mlp_gemm_check(mcg_ctx *ctx, int N, const uint16_t *A, const uint16_t *B, float *D);

@@ -88,6 +88,11 @@ class MlpTrainReport(C.Structure):
                 ("epoch_loss", C.c_double * MLP_MAX_EPOCH_LOG)]
 
 
+class BatchOpts(C.Structure):
+    _fields_ = [("block", C.c_int), ("blocks_per_sm", C.c_int), ("chunk", C.c_int), ("autotune", C.c_int),
+                ("use_graph", C.c_int), ("device_ms", C.c_float)]
+
+
 # name -> (restype, argtypes): every symbol the header declares
 SIGNATURES = {
     "mcg_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int]),
@@ -102,6 +107,9 @@ SIGNATURES = {
     "mcg_set_model": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Opacity)]),
     "mcg_mcradiation": (C.c_int, [C.c_void_p, C.POINTER(Run), C.POINTER(C.c_int64), C.POINTER(Result)]),
     "mcg_finalize_t": (C.c_int, [C.c_void_p, dp, dp, dp]),
+    "mcg_add_model": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Opacity), C.POINTER(C.c_int)]),
+    "mcg_mcradiation_batch": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(Run),
+                                        C.POINTER(C.c_int64), C.POINTER(Result), C.POINTER(BatchOpts)]),
     "mcg_mlp_set_params": (C.c_int, [C.c_void_p, fp, C.c_int64]),
     "mcg_mlp_get_params": (C.c_int, [C.c_void_p, fp, C.c_int64]),
     "mcg_mlp_forward": (C.c_int, [C.c_void_p, C.c_int64, fp, fp]),
@@ -111,6 +119,7 @@ SIGNATURES = {
     "mcg_surrogate_targets": (C.c_int, [C.c_void_p, C.c_int64, dp, C.c_double, C.c_int, fp]),
     "mcg_compute_part_surrogate": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(PartIn), C.POINTER(PartOut), C.c_double,
                                              C.c_int, ip]),
+    "mcg_mlp_time": (C.c_int, [C.c_void_p, C.c_int64, C.c_int, C.c_int, fp, fp]),
     "mcg_mlp_gemm_check": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_uint16), C.POINTER(C.c_uint16), fp]),
 }
 

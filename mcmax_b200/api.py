@@ -142,6 +142,70 @@ class Context:
                 out[k] = out[k].reshape(m.nlam, _ffi.NANGLE_SED + 1)
         return n.value, out
 
+    def _grid_opacity(self, m):
+        arrs = dict(R=_f64(m.R), Theta=_f64(m.Theta), SinTheta=_f64(m.SinTheta), dens=_f64(m.dens),
+                    V=_f64(m.V), comp_w=_f64(m.comp_w), lam=_f64(m.lam), nu=_f64(m.nu),
+                    Kabs=_f64(m.Kabs), Ksca=_f64(m.Ksca), F=_f64(m.F) if m.F is not None else None,
+                    BB=_f64(m.BB), Fstar=_f64(m.Fstar))
+        g = _ffi.Grid(m.nr, m.nt, _ffi.ptr(arrs["R"]), _ffi.ptr(arrs["Theta"]), _ffi.ptr(arrs["SinTheta"]),
+                      _ffi.ptr(arrs["dens"]), _ffi.ptr(arrs["V"]), m.ncomp, _ffi.ptr(arrs["comp_w"]))
+        o = _ffi.Opacity(m.nlam, _ffi.ptr(arrs["lam"]), _ffi.ptr(arrs["nu"]), m.ncomp, _ffi.ptr(arrs["Kabs"]),
+                         _ffi.ptr(arrs["Ksca"]), _ffi.ptr(arrs["F"]), _ffi.ptr(arrs["BB"]),
+                         _ffi.ptr(arrs["Fstar"]), float(m.Lstar), float(m.Tstar), float(m.Rstar_cm),
+                         int(m.scat_how))
+        return arrs, g, o
+
+    def add_model(self, model):
+        """Keep a model on the device for batched runs; returns its id."""
+        arrs, g, o = self._grid_opacity(model)
+        mid = C.c_int(-1)
+        self._check(self.lib.mcg_add_model(self.h, C.byref(g), C.byref(o), C.byref(mid)))
+        if not hasattr(self, "kept"):
+            self.kept = {}
+        self.kept[mid.value] = model
+        return mid.value
+
+    def mcradiation_batch(self, ids, nphot, seeds, precision="mixed", randomwalk=False, factRW=10.0,
+                          maxinteract=0, threads=0, block=0, blocks_per_sm=0, chunk=0, autotune=False,
+                          use_graph=False, fetch=True):
+        """One launch over kept models ids[k] with nphot[k] packets and seed
+        seeds[k]; returns (nphot_out, results, launch info)."""
+        n = len(ids)
+        prec = {"fp64": _ffi.PREC_FP64, "mixed": _ffi.PREC_MIXED}[precision]
+        runs = (_ffi.Run * n)()
+        for k in range(n):
+            runs[k] = _ffi.Run(int(seeds[k]), int(bool(randomwalk)), float(factRW), int(maxinteract), 1, prec,
+                               int(threads), 0)
+        cids = (C.c_int * n)(*[int(i) for i in ids])
+        cn = (C.c_int64 * n)(*[int(x) for x in nphot])
+        res = (_ffi.Result * n)()
+        outs = []
+        kept = getattr(self, "kept", {})
+        for k in range(n):
+            m = kept.get(ids[k])
+            out = {}
+            if fetch and m is not None:
+                nc = m.ncell
+                ns = m.nlam * (_ffi.NANGLE_SED + 1)
+                out = dict(EJv=np.zeros(nc), EJv2=np.zeros(nc), Eabs=np.zeros(nc), T=np.zeros(nc),
+                           Ni=np.zeros(nc, np.int32), spec=np.zeros(ns), scatspec=np.zeros(ns),
+                           ispec=np.zeros(ns, np.int32))
+                for key, v in out.items():
+                    setattr(res[k], key, _ffi.ptr(v))
+            outs.append(out)
+        opts = _ffi.BatchOpts(int(block), int(blocks_per_sm), int(chunk), int(bool(autotune)), int(bool(use_graph)),
+                              0.0)
+        self._check(self.lib.mcg_mcradiation_batch(self.h, n, cids, runs, cn, res, C.byref(opts)))
+        for k in range(n):
+            outs[k]["counters"] = np.array(res[k].counters[:], dtype=np.int64)
+            outs[k]["tautot"] = res[k].tautot
+            if fetch:
+                m = kept[ids[k]]
+                for key in ("spec", "scatspec", "ispec"):
+                    outs[k][key] = outs[k][key].reshape(m.nlam, _ffi.NANGLE_SED + 1)
+        info = dict(block=opts.block, blocks_per_sm=opts.blocks_per_sm, chunk=opts.chunk, device_ms=opts.device_ms)
+        return list(cn), outs, info
+
     def finalize_t(self):
         nc = self.model.ncell
         T, dT, dE = np.zeros(nc), np.zeros(nc), np.zeros(nc)

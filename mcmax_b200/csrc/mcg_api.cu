@@ -59,6 +59,7 @@ void mcg_destroy(mcg_ctx *ctx) {
   mcg_free_run(ctx->run);
   if (ctx->part_scratch.p) cudaFree(ctx->part_scratch.p);
   mcg_free_mlp(ctx);
+  mcg_free_batch(ctx);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -95,6 +96,19 @@ mcg_status mcg_mcradiation(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot_inou
   if (!ctx) return MCG_ERR_ARG;
   cudaSetDevice(ctx->device);
   return mcg_mcradiation_impl(ctx, run, nphot_inout, res);
+}
+
+mcg_status mcg_add_model(mcg_ctx *ctx, const mcg_grid *grid, const mcg_opacity *opac, int *model_id) {
+  if (!ctx) return MCG_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  return mcg_add_model_impl(ctx, grid, opac, model_id);
+}
+
+mcg_status mcg_mcradiation_batch(mcg_ctx *ctx, int nmodels, const int *model_ids, const mcg_run *runs,
+                                 int64_t *nphot_inout, mcg_result *results, mcg_batch_opts *opts) {
+  if (!ctx) return MCG_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  return mcg_batch_impl(ctx, nmodels, model_ids, runs, nphot_inout, results, opts);
 }
 
 mcg_status mcg_finalize_t(mcg_ctx *ctx, double *T, double *dT, double *dEJv) {

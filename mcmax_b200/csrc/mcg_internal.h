@@ -29,6 +29,7 @@ struct DevModel {
   int scattering = 0;       /* scat_how != 0 and some Ksca > 0 */
   int uniform_mix = 0;      /* all cells have the same comp_w row */
   double Lstar = 0.0, Tstar = 0.0, Rstar_cm = 0.0;
+  double R0 = 0.0;          /* R[0], the star radius in AU */
   /* geometry */
   double *R = nullptr, *Theta = nullptr, *SinTheta = nullptr;
   double *dens = nullptr;   /* floored at 1e-50 */
@@ -75,6 +76,7 @@ struct DevModel {
   unsigned short *emitG = nullptr; /* uniform: TMAX*32 guide table of emit_cdf rows */
   double *c2cum = nullptr, *s2cum = nullptr, *rw_logy = nullptr;
   double *KextTot = nullptr;  /* ncell*nlam, fp64 fast path, non-uniform */
+  double *BBT = nullptr;      /* TT*nlam: BB temperature-major, non-uniform mixtures */
   std::vector<void *> owned;
 };
 
@@ -115,6 +117,26 @@ struct mcg_ctx {
   DevBuf part_scratch;
   /* opacity-surrogate network (created on first use) */
   MlpState *mlp = nullptr;
+  /* models kept for batched runs (mcg_add_model) and their accumulators */
+  std::vector<DevModel> models;
+  std::vector<DevRun> runs;
+  /* batched launch: device copies of the per-model kernel arguments, the
+   * captured graph and the tuned launch shape */
+  DevBuf batch_args;
+  cudaGraphExec_t batch_graph = nullptr;
+  std::vector<long long> batch_graph_key;
+  int tuned_block = 0, tuned_bps = 0, tuned_chunk = 0;
+  std::vector<long long> tuned_key;
+};
+
+/* kernel arguments of one prepared run: the model tables and accumulators
+ * as the transport kernels see them (transport_core.cuh) */
+#include "transport_core.cuh"
+struct RunPrep {
+  TModel tm;
+  TAcc ta;
+  int nruns = 1;
+  size_t nc = 0, ns = 0;
 };
 
 /* error helpers */
@@ -134,10 +156,18 @@ mcg_status mcg_part_static_impl(mcg_ctx *ctx, const mcg_part_in *in, mcg_part_ou
 mcg_status mcg_set_model_impl(mcg_ctx *ctx, const mcg_grid *grid, const mcg_opacity *opac);
 mcg_status mcg_mcradiation_impl(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot, mcg_result *res);
 mcg_status mcg_finalize_impl(mcg_ctx *ctx, double *T, double *dT, double *dEJv);
+mcg_status mcg_run_prepare(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot, RunPrep *rp, bool zero);
+cudaError_t mcg_run_zero(mcg_ctx *ctx, size_t nb, size_t ns);
+void mcg_run_combine(mcg_ctx *ctx, const RunPrep &rp);
+mcg_status mcg_run_finish(mcg_ctx *ctx, const RunPrep &rp, float ms, mcg_result *res);
 mcg_status mcg_fast_run(mcg_ctx *ctx, int precision, const void *tmodel, const void *tacc, int threads,
                         int block, float *ms);
 void mcg_free_model(DevModel &m);
 void mcg_free_run(DevRun &r);
 void mcg_free_mlp(mcg_ctx *ctx);
+mcg_status mcg_add_model_impl(mcg_ctx *ctx, const mcg_grid *grid, const mcg_opacity *opac, int *id);
+mcg_status mcg_batch_impl(mcg_ctx *ctx, int n, const int *ids, const mcg_run *runs, int64_t *nphot,
+                          mcg_result *res, mcg_batch_opts *opts);
+void mcg_free_batch(mcg_ctx *ctx);
 
 #endif /* MCG_INTERNAL_H */

@@ -62,10 +62,12 @@ __device__ __forceinline__ uint32_t pack2(float a, float b) {
   return *reinterpret_cast<uint32_t *>(&v);
 }
 
-/* copy `bytes` (multiple of 16*NT) from global to shared, 16 B per access */
+/* copy `bytes` (multiple of 16*NT) from global to shared, 16 B per access,
+ * eight loads in flight per thread */
 __device__ __forceinline__ void copy16(unsigned char *dst, const unsigned char *src, uint32_t bytes) {
   const uint4 *s = reinterpret_cast<const uint4 *>(src);
   uint4 *d = reinterpret_cast<uint4 *>(dst);
+#pragma unroll 8
   for (uint32_t i = threadIdx.x; i < bytes / 16; i += NT) d[i] = s[i];
 }
 
@@ -101,7 +103,15 @@ __device__ __forceinline__ int run_gemm(Tc &tc, uint64_t *mbar, uint32_t a0, uin
 }
 
 /* ------------------------------------------------------------------ forward */
-__global__ void __launch_bounds__(NT, 1)
+/* Four warpgroups per CTA: the four warps that share a TMEM lane quarter
+ * (rows 32q..32q+31) split the 256 columns of every layer into quarters, so
+ * the CUDA-core work (input layer, bias + SiLU epilogues) has 16 warps per
+ * SM to hide its latency.  Weights reach shared memory by bulk copy: the
+ * copy of the next layer's weights starts as soon as the current MMA has
+ * finished reading them and runs while the epilogue works. */
+constexpr int NTF = 512;
+
+__global__ void __launch_bounds__(NTF, 1)
     mlp_fwd_kernel(Params P, const float *__restrict__ x, int n, float *__restrict__ y, float *__restrict__ zs,
                    __nv_bfloat16 *__restrict__ hs, int *err) {
   extern __shared__ __align__(1024) unsigned char smem[];
@@ -110,30 +120,49 @@ __global__ void __launch_bounds__(NT, 1)
   float *sW0 = reinterpret_cast<float *>(B + B_BYTES);
   float *sb = sW0 + H * IN;                 /* b0 | b1 | b2 | b3 | b4 */
   uint64_t *mbar = reinterpret_cast<uint64_t *>(sb + 4 * H + OUT);
-  uint32_t *slot = reinterpret_cast<uint32_t *>(mbar + 1);
+  uint64_t *mbar_w = mbar + 1;
+  uint32_t *slot = reinterpret_cast<uint32_t *>(mbar + 2);
   const int t = threadIdx.x, warp = t >> 5;
-  for (int i = t; i < H * IN; i += NT) sW0[i] = P.W0[i];
-  for (int i = t; i < H; i += NT) sb[i] = P.b0[i];
-  for (int i = t; i < 3 * H; i += NT) sb[H + i] = P.b123[i];
-  for (int i = t; i < OUT; i += NT) sb[4 * H + i] = P.b4[i];
-  if (t == 0) tc_mbar_init(mbar, 1);
+  const int row = t & (TILE - 1);   /* = 32 * (warp % 4) + lane: this thread's TMEM lane */
+  const int c0 = (t >> 7) * (H / 4); /* this thread's quarter of the columns */
+  for (int i = t; i < H * IN; i += NTF) sW0[i] = P.W0[i];
+  for (int i = t; i < H; i += NTF) sb[i] = P.b0[i];
+  for (int i = t; i < 3 * H; i += NTF) sb[H + i] = P.b123[i];
+  for (int i = t; i < OUT; i += NTF) sb[4 * H + i] = P.b4[i];
+  if (t == 0) {
+    tc_mbar_init(mbar, 1);
+    tc_mbar_init(mbar_w, 1);
+  }
   if (warp == 0) tc_alloc(slot, 256);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   Tc tc{*slot, 0u};
-  const uint32_t lane_base = tc.tmem + ((uint32_t)(warp * 32) << 16);
+  uint32_t wphase = 0u;
+  int w_in_flight = 0;
+  const uint32_t lane_base = tc.tmem + ((uint32_t)((warp & 3) * 32) << 16);
   const uint32_t a0 = tc_smem_addr(A), b0 = tc_smem_addr(B);
   const int ntiles = (n + TILE - 1) / TILE;
   int ok = 1;
+  auto issue_w = [&](const __nv_bfloat16 *src, uint32_t bytes) {
+    if (t == 0) tc_bulk_load(B, src, bytes, mbar_w);
+    w_in_flight = 1;
+  };
+  auto wait_w = [&]() {
+    const int w = tc_mbar_wait(mbar_w, wphase);
+    wphase ^= 1u;
+    w_in_flight = 0;
+    return __syncthreads_and(w);
+  };
+  if ((int)blockIdx.x < ntiles) issue_w(P.Wc, B_BYTES);
   for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-    const int g = tile * TILE + t;
+    const int g = tile * TILE + row;
     const bool live = g < n;
-    /* layer 0 on CUDA cores: this thread's row */
+    /* layer 0 on CUDA cores: this thread's row, its quarter of the units */
     float xi[IN];
 #pragma unroll
     for (int i = 0; i < IN; ++i) xi[i] = live ? x[(size_t)g * IN + i] : 0.0f;
-    for (int j0 = 0; j0 < H; j0 += 8) {
+    for (int j0 = c0; j0 < c0 + H / 4; j0 += 8) {
       float v[8];
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
@@ -143,19 +172,23 @@ __global__ void __launch_bounds__(NT, 1)
         if (zs && live) zs[((size_t)g * 4 + 0) * H + j0 + u] = z;
         v[u] = silu(z);
       }
-      store_row8(A, t, j0, v);
+      store_row8(A, row, j0, v);
       if (hs && live) {
-        uint4 q = *reinterpret_cast<uint4 *>(A + tc_kmaj_off(t, j0, H));
+        uint4 q = *reinterpret_cast<uint4 *>(A + tc_kmaj_off(row, j0, H));
         *reinterpret_cast<uint4 *>(hs + ((size_t)g * 4 + 0) * H + j0) = q;
       }
     }
     /* layers 1..3 on the tensor cores */
     for (int l = 0; l < 3 && ok; ++l) {
-      __syncthreads();
-      copy16(B, reinterpret_cast<const unsigned char *>(P.Wc + (size_t)l * H * H), B_BYTES);
+      ok = wait_w();
+      if (!ok) break;
       ok = run_gemm(tc, mbar, a0, b0, H, H);
       if (!ok) break;
-      for (int c = 0; c < H; c += 16) {
+      if (l < 2)
+        issue_w(P.Wc + (size_t)(l + 1) * H * H, B_BYTES);
+      else
+        issue_w(P.W4c, OUT * H * 2);
+      for (int c = c0; c < c0 + H / 4; c += 16) {
         float v[16];
         tc_ld16(lane_base + (uint32_t)c, v);
 #pragma unroll
@@ -164,24 +197,26 @@ __global__ void __launch_bounds__(NT, 1)
           if (zs && live) zs[((size_t)g * 4 + l + 1) * H + c + u] = z;
           v[u] = silu(z);
         }
-        store_row8(A, t, c, v);
-        store_row8(A, t, c + 8, v + 8);
+        store_row8(A, row, c, v);
+        store_row8(A, row, c + 8, v + 8);
         if (hs && live) {
           *reinterpret_cast<uint4 *>(hs + ((size_t)g * 4 + l + 1) * H + c) =
-              *reinterpret_cast<uint4 *>(A + tc_kmaj_off(t, c, H));
+              *reinterpret_cast<uint4 *>(A + tc_kmaj_off(row, c, H));
           *reinterpret_cast<uint4 *>(hs + ((size_t)g * 4 + l + 1) * H + c + 8) =
-              *reinterpret_cast<uint4 *>(A + tc_kmaj_off(t, c + 8, H));
+              *reinterpret_cast<uint4 *>(A + tc_kmaj_off(row, c + 8, H));
         }
       }
       tc_fence_before();
     }
     if (!ok) break;
-    /* output layer: N = 32 */
-    __syncthreads();
-    copy16(B, reinterpret_cast<const unsigned char *>(P.W4c), OUT * H * 2);
+    /* output layer: N = 32, read by the first two warpgroups */
+    ok = wait_w();
+    if (!ok) break;
     ok = run_gemm(tc, mbar, a0, b0, OUT, H);
     if (!ok) break;
-    for (int c = 0; c < OUT; c += 16) {
+    if (tile + (int)gridDim.x < ntiles) issue_w(P.Wc, B_BYTES);
+    if (t < 2 * TILE) {
+      const int c = (t >> 7) * 16;
       float v[16];
       tc_ld16(lane_base + (uint32_t)c, v);
       if (live) {
@@ -192,7 +227,8 @@ __global__ void __launch_bounds__(NT, 1)
     tc_fence_before();
   }
   if (!ok && t == 0) atomicExch(err, 1);
-  /* a timed-out MMA may still be running: give it one more bounded wait */
+  /* nothing may still write shared or tensor memory when the CTA leaves */
+  if (w_in_flight) (void)tc_mbar_wait(mbar_w, wphase);
   if (!ok) (void)tc_mbar_wait(mbar, tc.phase ^ 1u);
   __syncthreads();
   tc_fence_after();
@@ -225,6 +261,7 @@ __global__ void __launch_bounds__(NT, 1)
     const int g = tile * TILE + t;
     const bool live = g < n;
     __syncthreads();
+#pragma unroll 8
     for (int k0 = 0; k0 < H; k0 += 8) {
       uint4 q = make_uint4(0, 0, 0, 0);
       if (live) q = *reinterpret_cast<const uint4 *>(dz + (size_t)g * H + k0);
@@ -521,7 +558,7 @@ constexpr int64_t OFF_W0 = 0, OFF_B0 = OFF_W0 + H * IN, OFF_W123 = OFF_B0 + H, O
                   OFF_W4 = OFF_B123 + 3 * H, OFF_B4 = OFF_W4 + OUT * H, NPARAMS = OFF_B4 + OUT;
 static_assert(NPARAMS == MCG_MLP_NPARAMS, "parameter count");
 
-constexpr size_t SMEM_FWD = A_BYTES + B_BYTES + (H * IN + 4 * H + OUT) * 4 + 16;
+constexpr size_t SMEM_FWD = A_BYTES + B_BYTES + (H * IN + 4 * H + OUT) * 4 + 24;
 constexpr size_t SMEM_DX = A_BYTES + B_BYTES + 16;
 constexpr size_t SMEM_DW = 4 * 128 * 128 * 2 + 16;
 constexpr size_t SMEM_CHECK = A_BYTES + B_BYTES + 16;
@@ -632,7 +669,7 @@ int grid_tiles(mcg_ctx *ctx, int64_t n) {
 /* forward of rows already in s.xb; zs/hs kept when `keep` */
 void mlp_fwd_launch(mcg_ctx *ctx, int64_t n, bool keep) {
   MlpState &s = *ctx->mlp;
-  mlp_fwd_kernel<<<grid_tiles(ctx, n), NT, SMEM_FWD, ctx->stream>>>(mlp_params(s), s.xb, (int)n, s.yb,
+  mlp_fwd_kernel<<<grid_tiles(ctx, n), NTF, SMEM_FWD, ctx->stream>>>(mlp_params(s), s.xb, (int)n, s.yb,
                                                                      keep ? s.zs : nullptr,
                                                                      keep ? s.hs : nullptr, s.err);
 }
@@ -1059,4 +1096,62 @@ extern "C" mcg_status mcg_surrogate_targets(mcg_ctx *ctx, int64_t n, const doubl
   if (!ctx) return MCG_ERR_ARG;
   cudaSetDevice(ctx->device);
   return mcg_surrogate_targets_impl(ctx, n, in6, rho, nf, out);
+}
+
+/* Device timing of the network: forward passes over n device-resident rows
+ * and training steps (forward + backward + Adam) on batches of `batch` rows,
+ * CUDA events on the context's stream.  The parameters are saved and
+ * restored around the training steps. */
+extern "C" mcg_status mcg_mlp_time(mcg_ctx *ctx, int64_t n, int iters, int batch, float *fwd_ms, float *step_ms) {
+  if (!ctx) return MCG_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  mcg_status st = mlp_ready(ctx, "mlp_time");
+  if (st != MCG_OK) return st;
+  if (n < TILE || n > ((int64_t)1 << 24) || iters < 1 || iters > 1000 || batch < TILE || batch > (1 << 20) || !fwd_ms ||
+      !step_ms)
+    return mcg_fail(ctx, MCG_ERR_ARG, "mlp_time: 128 <= n <= 2^24, 1 <= iters <= 1000, 128 <= batch <= 2^20");
+  MlpState &s = *ctx->mlp;
+  const int64_t rows = std::max<int64_t>(n, batch);
+  if ((st = mlp_reserve(ctx, rows)) != MCG_OK) return st;
+  cudaStream_t cs = ctx->stream;
+  std::vector<float> P((size_t)NPARAMS);
+  MCG_CUDA(ctx, cudaMemcpyAsync(P.data(), s.P, NPARAMS * sizeof(float), cudaMemcpyDeviceToHost, cs));
+  /* inputs in [-1, 1] and zero targets, generated on the host once */
+  {
+    std::vector<float> x((size_t)rows * IN), w(OUT, 1.0f);
+    std::mt19937 rng(7);
+    std::uniform_real_distribution<float> u(-1.0f, 1.0f);
+    for (auto &v : x) v = u(rng);
+    MCG_CUDA(ctx, cudaMemcpyAsync(s.xb, x.data(), x.size() * sizeof(float), cudaMemcpyHostToDevice, cs));
+    MCG_CUDA(ctx, cudaMemsetAsync(s.tb, 0, (size_t)rows * OUT * sizeof(float), cs));
+    MCG_CUDA(ctx, cudaMemcpyAsync(s.wout, w.data(), OUT * sizeof(float), cudaMemcpyHostToDevice, cs));
+    MCG_CUDA(ctx, cudaStreamSynchronize(cs));
+  }
+  for (int w = 0; w < 2; ++w) mlp_fwd_launch(ctx, n, false);
+  cudaEventRecord(ctx->ev0, cs);
+  for (int i = 0; i < iters; ++i) mlp_fwd_launch(ctx, n, false);
+  cudaEventRecord(ctx->ev1, cs);
+  MCG_CUDA(ctx, cudaEventSynchronize(ctx->ev1));
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  *fwd_ms = ms / (float)iters;
+  const float b1 = 0.9f, b2 = 0.999f;
+  auto step = [&]() {
+    mlp_backward_launch(ctx, batch);
+    ++s.step;
+    const float c1 = 1.0f - powf(b1, (float)s.step), c2 = 1.0f - powf(b2, (float)s.step);
+    mlp_adam_kernel<<<nblk(NPARAMS, 256), 256, 0, cs>>>(s.P, s.G, s.M, s.V, (int)NPARAMS, 1e-6f, b1, b2, 1e-8f, c1, c2);
+    mlp_pack(ctx);
+  };
+  for (int w = 0; w < 2; ++w) step();
+  cudaEventRecord(ctx->ev0, cs);
+  for (int i = 0; i < iters; ++i) step();
+  cudaEventRecord(ctx->ev1, cs);
+  MCG_CUDA(ctx, cudaEventSynchronize(ctx->ev1));
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  *step_ms = ms / (float)iters;
+  /* restore the parameters and a fresh optimizer state */
+  st = mcg_mlp_set_params(ctx, P.data(), NPARAMS);
+  if (st != MCG_OK) return st;
+  return mlp_check_err(ctx, "mlp_time");
 }

@@ -102,6 +102,29 @@ __device__ __forceinline__ int tc_mbar_wait(uint64_t *mbar, uint32_t parity) {
   return 0;
 }
 
+/* Asynchronous bulk copy global -> shared (the copy engine of the SM, no
+ * multicast) that completes `bytes` of transaction count on the mbarrier.
+ * The issuing thread first announces the total with tc_expect_tx.  Both
+ * addresses 16-byte aligned, sizes multiples of 16. */
+__device__ __forceinline__ void tc_expect_tx(uint64_t *mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc_smem_addr(mbar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void tc_bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   tc_smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(tc_smem_addr(mbar))
+               : "memory");
+}
+/* one thread: announce and issue a copy of `bytes` in pieces of 32 KB */
+__device__ __forceinline__ void tc_bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *mbar) {
+  tc_expect_tx(mbar, bytes);
+  for (uint32_t o = 0; o < bytes; o += 32768u) {
+    const uint32_t n = bytes - o < 32768u ? bytes - o : 32768u;
+    tc_bulk_g2s((unsigned char *)dst + o, (const unsigned char *)src + o, n, mbar);
+  }
+}
+
 /* 16 consecutive FP32 accumulator columns of this thread's TMEM lane: warp w
  * of the warpgroup reads lanes 32w..32w+31, lane = row of the 128-row tile */
 __device__ __forceinline__ void tc_ld16(uint32_t taddr, float *v) {

@@ -275,6 +275,7 @@ mcg_status mcg_set_model_impl(mcg_ctx *ctx, const mcg_grid *g, const mcg_opacity
   m.scat_how = o->scat_how;
   m.Lstar = o->Lstar;
   m.Tstar = o->Tstar;
+  m.R0 = g->R[0];
   m.Rstar_cm = o->Rstar_cm;
   m.scattering = 0;
   if (o->scat_how != 0)
@@ -566,8 +567,10 @@ __global__ static void combine_runs_kernel(int nc, int nruns, const double *EJv,
   NiTot[c] = n;
 }
 
-mcg_status mcg_mcradiation_impl(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot, mcg_result *res) {
-  if (!run || !nphot || !res) return mcg_fail(ctx, MCG_ERR_ARG, "mcradiation: null argument");
+/* validation, run buffers and tables, zeroed accumulators and the kernel
+ * arguments of one run of the current model (ctx->model / ctx->run) */
+mcg_status mcg_run_prepare(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot, RunPrep *rp, bool zero) {
+  if (!run || !nphot || !rp) return mcg_fail(ctx, MCG_ERR_ARG, "mcradiation: null argument");
   DevModel &m = ctx->model;
   if (!m.valid) return mcg_fail(ctx, MCG_ERR_STATE, "mcradiation: mcg_set_model has not been called");
   if (*nphot < 1) return mcg_fail(ctx, MCG_ERR_ARG, "mcradiation: NphotTot must be >= 1");
@@ -589,23 +592,12 @@ mcg_status mcg_mcradiation_impl(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot
   if (Nphot * nruns > (int64_t)2000000000)
     return mcg_fail(ctx, MCG_ERR_LIMIT, "mcradiation: at most 2e9 packets per call (packet numbers are int32)");
   const size_t nc = m.ncell, nb = (size_t)m.ncell * nruns, ns = (size_t)m.nlam * (TP_NANG + 1);
-  MCG_CUDA(ctx, cudaMemsetAsync(R.EJv, 0, nb * 8, st));
-  MCG_CUDA(ctx, cudaMemsetAsync(R.EJv2, 0, nb * 8, st));
-  MCG_CUDA(ctx, cudaMemsetAsync(R.Eabs, 0, nb * 8, st));
-  MCG_CUDA(ctx, cudaMemsetAsync(R.T, 0, nb * 8, st));
-  MCG_CUDA(ctx, cudaMemsetAsync(R.Ni, 0, nb * 4, st));
-  MCG_CUDA(ctx, cudaMemsetAsync(R.lastphot, 0, nb * 4, st));
-  MCG_CUDA(ctx, cudaMemsetAsync(R.kp_hint, 0, nb * 4, st));
-  MCG_CUDA(ctx, cudaMemsetAsync(R.spec, 0, ns * 8, st));
-  MCG_CUDA(ctx, cudaMemsetAsync(R.scatspec, 0, ns * 8, st));
-  MCG_CUDA(ctx, cudaMemsetAsync(R.ispec, 0, ns * 4, st));
-  MCG_CUDA(ctx, cudaMemsetAsync(R.counters, 0, MCG_NCOUNTERS * 8, st));
-  MCG_CUDA(ctx, cudaMemsetAsync(R.tautot, 0, 8, st));
-  MCG_CUDA(ctx, cudaMemsetAsync(R.next_packet, 0, 8, st));
-  MCG_CUDA(ctx, cudaMemsetAsync(R.done, 0, 8, st));
-  MCG_CUDA(ctx, cudaMemsetAsync(R.tmark, 0, 8 * 8, st));
+  rp->nruns = nruns;
+  rp->nc = nc;
+  rp->ns = ns;
+  if (zero) MCG_CUDA(ctx, mcg_run_zero(ctx, nb, ns));
 
-  TModel tm;
+  TModel &tm = rp->tm;
   memset(&tm, 0, sizeof tm);
   tm.nr = m.nr; tm.nt = m.nt; tm.nc = m.nc; tm.ncell = m.ncell; tm.nlam = m.nlam; tm.ncomp = m.ncomp;
   tm.scattering = m.scattering; tm.scat_how = m.scat_how; tm.uniform_mix = m.uniform_mix;
@@ -625,12 +617,8 @@ mcg_status mcg_mcradiation_impl(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot
   tm.sinthet = m.sinthet; tm.cos2phi = m.cos2phi; tm.sin2phi = m.sin2phi;
   tm.KDext = m.KDext; tm.KDabs = m.KDabs; tm.rw_y = m.rw_y; tm.rw_phi = m.rw_phi;
   tm.kd_index = m.kd_index; tm.thick = m.thick;
-  {
-    double R0;
-    MCG_CUDA(ctx, cudaMemcpy(&R0, m.R, sizeof(double), cudaMemcpyDeviceToHost));
-    tm.R0 = R0;
-  }
-  TAcc ta;
+  tm.R0 = m.R0;
+  TAcc &ta = rp->ta;
   memset(&ta, 0, sizeof ta);
   ta.EJv = R.EJv; ta.EJv2 = R.EJv2; ta.Eabs = R.Eabs; ta.T = R.T; ta.Ni = R.Ni; ta.lastphot = R.lastphot;
   ta.kp_hint = R.kp_hint;
@@ -648,10 +636,84 @@ mcg_status mcg_mcradiation_impl(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot
       ta.thresh[k] = t < 1ULL ? 1ULL : (t > tot ? tot : t);
     }
   }
+  return MCG_OK;
+}
 
+/* zero the accumulators of the current run buffers (nb per-cell entries per
+ * array, ns spectrum bins); capturable into a CUDA graph */
+cudaError_t mcg_run_zero(mcg_ctx *ctx, size_t nb, size_t ns) {
+  DevRun &R = ctx->run;
+  cudaStream_t st = ctx->stream;
+  cudaError_t e = cudaSuccess;
+  if (e == cudaSuccess) e = cudaMemsetAsync(R.EJv, 0, nb * 8, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(R.EJv2, 0, nb * 8, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(R.Eabs, 0, nb * 8, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(R.T, 0, nb * 8, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(R.Ni, 0, nb * 4, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(R.lastphot, 0, nb * 4, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(R.kp_hint, 0, nb * 4, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(R.spec, 0, ns * 8, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(R.scatspec, 0, ns * 8, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(R.ispec, 0, ns * 4, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(R.counters, 0, MCG_NCOUNTERS * 8, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(R.tautot, 0, 8, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(R.next_packet, 0, 8, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(R.done, 0, 8, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(R.tmark, 0, 8 * 8, st);
+  return e;
+}
+
+/* per-run combination of the current run (nruns averages) */
+void mcg_run_combine(mcg_ctx *ctx, const RunPrep &rp) {
+  DevRun &R = ctx->run;
+  combine_runs_kernel<<<(int)((rp.nc + 255) / 256), 256, 0, ctx->stream>>>((int)rp.nc, rp.nruns, R.EJv, R.EJv2, R.Ni,
+                                                                            R.EJvTot, R.EJv2Tot, R.NiTot);
+}
+
+/* results of the current run to the caller's arrays */
+mcg_status mcg_run_finish(mcg_ctx *ctx, const RunPrep &rp, float ms, mcg_result *res) {
+  DevRun &R = ctx->run;
+  cudaStream_t st = ctx->stream;
+  const size_t nc = rp.nc, ns = rp.ns;
+  MCG_CUDA(ctx, cudaGetLastError());
+  res->device_ms = ms;
+  unsigned long long cnt[MCG_NCOUNTERS], tmk[8];
+  MCG_CUDA(ctx, cudaMemcpyAsync(cnt, R.counters, sizeof cnt, cudaMemcpyDeviceToHost, st));
+  MCG_CUDA(ctx, cudaMemcpyAsync(tmk, R.tmark, sizeof tmk, cudaMemcpyDeviceToHost, st));
+  MCG_CUDA(ctx, cudaMemcpyAsync(&res->tautot, R.tautot, 8, cudaMemcpyDeviceToHost, st));
+  const size_t last = (size_t)(rp.nruns - 1) * nc;
+#define DN(dst, src, n) \
+  if (dst) MCG_CUDA(ctx, cudaMemcpyAsync(dst, src, (size_t)(n) * sizeof(*(dst)), cudaMemcpyDeviceToHost, st))
+  DN(res->EJv, R.EJvTot, nc);
+  DN(res->EJv2, R.EJv2Tot, nc);
+  DN(res->Eabs, R.Eabs + last, nc);
+  DN(res->T, R.T + last, nc);
+  DN(res->Ni, R.NiTot, nc);
+  DN(res->spec, R.spec, ns);
+  DN(res->scatspec, R.scatspec, ns);
+  DN(res->ispec, R.ispec, ns);
+#undef DN
+  MCG_CUDA(ctx, cudaStreamSynchronize(st));
+  for (int k = 0; k < MCG_NCOUNTERS; ++k) res->counters[k] = (int64_t)cnt[k];
+  /* progress marks relative to the kernel start (tmark[5]) */
+  for (int k = 0; k < 5; ++k)
+    res->progress_ms[k] = (tmk[k] && tmk[5] && tmk[k] >= tmk[5]) ? (float)((double)(tmk[k] - tmk[5]) * 1e-6) : -1.0f;
+  ctx->have_run = true;
+  if (cnt[TC_GEOFAIL] > 0)
+    return mcg_fail(ctx, MCG_ERR_RUN, "mcradiation: %llu packets found no cell boundary to hit", cnt[TC_GEOFAIL]);
+  return MCG_OK;
+}
+
+mcg_status mcg_mcradiation_impl(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot, mcg_result *res) {
+  if (!res) return mcg_fail(ctx, MCG_ERR_ARG, "mcradiation: null argument");
+  RunPrep rp;
+  mcg_status s = mcg_run_prepare(ctx, run, nphot, &rp, true);
+  if (s != MCG_OK) return s;
+  TModel &tm = rp.tm;
+  TAcc &ta = rp.ta;
+  cudaStream_t st = ctx->stream;
   const int block = run->block > 0 ? run->block : 128;
   float ms = 0.0f;
-  unsigned long long t_host_start = 0;
   if (run->precision == MCG_PREC_EXACT) {
     int grid;
     if (run->threads > 0) {
@@ -675,36 +737,8 @@ mcg_status mcg_mcradiation_impl(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot
                                  run->block, &ms);
     if (fs != MCG_OK) return fs;
   }
-  (void)t_host_start;
-  combine_runs_kernel<<<(int)((nc + 255) / 256), 256, 0, st>>>((int)nc, nruns, R.EJv, R.EJv2, R.Ni, R.EJvTot,
-                                                             R.EJv2Tot, R.NiTot);
-  MCG_CUDA(ctx, cudaGetLastError());
-  res->device_ms = ms;
-  unsigned long long cnt[MCG_NCOUNTERS], tmk[8];
-  MCG_CUDA(ctx, cudaMemcpyAsync(cnt, R.counters, sizeof cnt, cudaMemcpyDeviceToHost, st));
-  MCG_CUDA(ctx, cudaMemcpyAsync(tmk, R.tmark, sizeof tmk, cudaMemcpyDeviceToHost, st));
-  MCG_CUDA(ctx, cudaMemcpyAsync(&res->tautot, R.tautot, 8, cudaMemcpyDeviceToHost, st));
-  const size_t last = (size_t)(nruns - 1) * nc;
-#define DN(dst, src, n) \
-  if (dst) MCG_CUDA(ctx, cudaMemcpyAsync(dst, src, (size_t)(n) * sizeof(*(dst)), cudaMemcpyDeviceToHost, st))
-  DN(res->EJv, R.EJvTot, nc);
-  DN(res->EJv2, R.EJv2Tot, nc);
-  DN(res->Eabs, R.Eabs + last, nc);
-  DN(res->T, R.T + last, nc);
-  DN(res->Ni, R.NiTot, nc);
-  DN(res->spec, R.spec, ns);
-  DN(res->scatspec, R.scatspec, ns);
-  DN(res->ispec, R.ispec, ns);
-#undef DN
-  MCG_CUDA(ctx, cudaStreamSynchronize(st));
-  for (int k = 0; k < MCG_NCOUNTERS; ++k) res->counters[k] = (int64_t)cnt[k];
-  /* progress marks relative to the kernel start (tmark[5]) */
-  for (int k = 0; k < 5; ++k)
-    res->progress_ms[k] = (tmk[k] && tmk[5] && tmk[k] >= tmk[5]) ? (float)((double)(tmk[k] - tmk[5]) * 1e-6) : -1.0f;
-  ctx->have_run = true;
-  if (cnt[TC_GEOFAIL] > 0)
-    return mcg_fail(ctx, MCG_ERR_RUN, "mcradiation: %llu packets found no cell boundary to hit", cnt[TC_GEOFAIL]);
-  return MCG_OK;
+  mcg_run_combine(ctx, rp);
+  return mcg_run_finish(ctx, rp, ms, res);
 }
 
 mcg_status mcg_finalize_impl(mcg_ctx *ctx, double *T, double *dT, double *dEJv) {

@@ -79,6 +79,14 @@ __global__ void emit_guide_kernel(int n, const double *D, unsigned short *G) {
   }
 }
 
+/* BBT[iT*nlam + l] = BB[l*TT + iT]: one Planck row per temperature */
+__global__ void bbt_kernel(int nlam, const double *BB, double *BBT) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)TP_TT * nlam) return;
+  const int iT = (int)(i / nlam), l = (int)(i % nlam);
+  BBT[i] = BB[(size_t)l * TP_TT + iT];
+}
+
 template <class R>
 __global__ void cast_kernel(long long n, const double *a, R *b) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -217,6 +225,11 @@ mcg_status build_fast_tables(mcg_ctx *ctx, int pi) {
     MCG_CUDA(ctx, cudaMemcpyAsync(m.c2cum, c2.data(), 181 * 8, cudaMemcpyHostToDevice, st));
     MCG_CUDA(ctx, cudaMemcpyAsync(m.s2cum, s2.data(), 181 * 8, cudaMemcpyHostToDevice, st));
     MCG_CUDA(ctx, cudaMemcpyAsync(m.rw_logy, ly.data(), TP_NY * 8, cudaMemcpyHostToDevice, st));
+    if (!m.uniform_mix) {
+      if ((e = alloc((size_t)TP_TT * nlam * 8, (void **)&m.BBT)) != cudaSuccess)
+        return mcg_fail(ctx, MCG_ERR_NOMEM, "fast tables: %s", cudaGetErrorString(e));
+      bbt_kernel<<<nblk((long long)TP_TT * nlam, 256), 256, 0, st>>>(nlam, m.BB, m.BBT);
+    }
     if (m.uniform_mix) {
       if ((e = alloc((size_t)TP_TT * (nlam - 1) * 8, (void **)&m.Ccum)) != cudaSuccess)
         return mcg_fail(ctx, MCG_ERR_NOMEM, "fast tables: %s", cudaGetErrorString(e));
@@ -255,13 +268,11 @@ mcg_status build_fast_tables(mcg_ctx *ctx, int pi) {
   return MCG_OK;
 }
 
+/* the GPU-ordered kernels' view of the current model (global pointers) */
 template <class R>
-mcg_status launch_fast(mcg_ctx *ctx, int pi, const TModel &tm, const TAcc &ta, int threads, int block, float *ms) {
-  mcg_status s = build_fast_tables<R>(ctx, pi);
-  if (s != MCG_OK) return s;
+void fill_fmodel(mcg_ctx *ctx, int pi, const TModel &tm, FModel<R> &g) {
   DevModel &m = ctx->model;
   DevModel::Fast &f = m.fast[pi];
-  FModel<R> g;
   memset(&g, 0, sizeof g);
   g.nr = tm.nr; g.nt = tm.nt; g.nc = tm.nc; g.ncell = tm.ncell; g.nlam = tm.nlam; g.ncomp = tm.ncomp;
   g.scattering = tm.scattering; g.scat_how = tm.scat_how; g.uniform_mix = tm.uniform_mix; g.rw = tm.rw;
@@ -272,12 +283,21 @@ mcg_status launch_fast(mcg_ctx *ctx, int pi, const TModel &tm, const TAcc &ta, i
   g.c2cum = m.c2cum; g.s2cum = m.s2cum;
   g.dens = tm.dens; g.mass = tm.mass; g.wlam = tm.wlam;
   g.KabsTotR = (const R *)f.KabsTotR; g.KextTotR = (const R *)f.KextTotR; g.KabsTot = m.KabsTot;
-  g.BB = m.BB; g.dnu_half = m.dnu_half; g.KpCell = m.KpCell;
+  g.BB = m.BB; g.BBT = m.BBT; g.dnu_half = m.dnu_half; g.KpCell = m.KpCell;
   g.Ccum = m.Ccum; g.Dcum = m.emit_cdf; g.comp_w = m.comp_w;
   g.scatA = (const R *)f.scatA; g.scatB = (const R *)f.scatB; g.F6 = (const R *)f.F6; g.IF_c = m.IF_c;
   g.scatG = f.scatG; g.emitG = m.emitG;
   g.KDext = m.KDext; g.KDabs = m.KDabs; g.rw_logy = m.rw_logy; g.rw_phi = m.rw_phi;
   g.kd_index = m.kd_index; g.thick = m.thick;
+}
+
+template <class R>
+mcg_status launch_fast(mcg_ctx *ctx, int pi, const TModel &tm, const TAcc &ta, int threads, int block, float *ms) {
+  mcg_status s = build_fast_tables<R>(ctx, pi);
+  if (s != MCG_OK) return s;
+  DevModel &m = ctx->model;
+  FModel<R> g;
+  fill_fmodel<R>(ctx, pi, tm, g);
   SmemPlan sp = plan_smem<R>(m.nr, m.nt, m.nlam, m.ncomp, m.uniform_mix);
   MCG_CUDA(ctx, cudaFuncSetAttribute(transport_fast_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.bytes));
   const int b = block > 0 ? block : F_BLOCK;
@@ -309,4 +329,316 @@ mcg_status mcg_fast_run(mcg_ctx *ctx, int precision, const void *tmodel, const v
   const TAcc &ta = *(const TAcc *)tacc;
   if (precision == 1) return launch_fast<float>(ctx, 1, tm, ta, threads, block, ms);
   return launch_fast<double>(ctx, 0, tm, ta, threads, block, ms);
+}
+
+/* ========================================================================
+ * Many models in one launch (mcg_add_model, mcg_mcradiation_batch).
+ *
+ * Packets of all models are numbered consecutively (model k owns
+ * [off[k], off[k+1])) and taken from one work counter, `chunk` at a time;
+ * a thread finds a packet's model by bisection in the offsets (shared
+ * memory) and runs it with that model's tables and accumulators, through
+ * the same per-packet code as the single-model kernel.  A packet keeps its
+ * own Philox stream (its model's seed, its number within the model), so a
+ * model's packets are the same packets whether it runs alone or in a batch
+ * (the two kernels are compiled separately, so FMA contraction may round a
+ * few operations differently).
+ * ====================================================================== */
+namespace {
+
+template <class R>
+__global__ void __launch_bounds__(F_BLOCK, F_MINBLOCKS)
+    transport_batch_kernel(const FModel<R> *__restrict__ models, const TAcc *__restrict__ accs,
+                           const long long *__restrict__ off, int nmodels, unsigned long long *next, int chunk) {
+  __shared__ long long soff[MCG_BATCH_MAX + 1];
+  for (int i = threadIdx.x; i <= nmodels; i += blockDim.x) soff[i] = off[i];
+  if (blockIdx.x == 0)
+    for (int i = threadIdx.x; i < nmodels; i += blockDim.x) accs[i].tmark[5] = tp_globaltimer();
+  __syncthreads();
+  const long long total = soff[nmodels];
+  TLocal L;
+  auto clear = [&]() {
+#pragma unroll
+    for (int k = 0; k < TC_N; ++k) L.cnt[k] = 0u;
+    L.tautot = 0.0;
+  };
+  auto flush = [&](const TAcc &A) {
+#pragma unroll
+    for (int k = 0; k < TC_N; ++k)
+      if (L.cnt[k]) atomicAdd(&A.counters[k], (unsigned long long)L.cnt[k]);
+    if (L.tautot != 0.0) atomicAdd(A.tautot, L.tautot);
+  };
+  clear();
+  int cur = -1;
+  for (;;) {
+    const unsigned long long k0 = atomicAdd(next, (unsigned long long)chunk);
+    if (k0 >= (unsigned long long)total) break;
+    const long long k1 = (long long)k0 + chunk < total ? (long long)k0 + chunk : total;
+    for (long long k = (long long)k0; k < k1; ++k) {
+      int lo = 0, hi = nmodels;
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (soff[mid] <= k)
+          lo = mid;
+        else
+          hi = mid;
+      }
+      if (lo != cur) {
+        if (cur >= 0) flush(accs[cur]);
+        clear();
+        cur = lo;
+      }
+      const FModel<R> &m = models[lo];
+      f_run_packet<R>(m, accs[lo], (int64_t)(k - soff[lo]) + m.pid0, L);
+      tp_packet_done(accs[lo]);
+    }
+  }
+  if (cur >= 0) flush(accs[cur]);
+}
+
+/* swap kept model `id` in as the context's current model (and back) */
+struct ModelSlot {
+  mcg_ctx *ctx;
+  int id;
+  ModelSlot(mcg_ctx *c, int i) : ctx(c), id(i) {
+    std::swap(ctx->model, ctx->models[id]);
+    std::swap(ctx->run, ctx->runs[id]);
+  }
+  ~ModelSlot() {
+    std::swap(ctx->model, ctx->models[id]);
+    std::swap(ctx->run, ctx->runs[id]);
+  }
+};
+
+struct Shape {
+  int block, bps, chunk;
+};
+
+template <class R>
+mcg_status batch_run_t(mcg_ctx *ctx, int pi, int n, const int *ids, const mcg_run *runs, int64_t *nphot,
+                       mcg_result *res, mcg_batch_opts *opts) {
+  cudaStream_t st = ctx->stream;
+  /* runs[0].threads == 1: one thread takes every packet in order (the
+   * serial order of the single-model kernel with threads = 1) */
+  const bool serial = runs[0].threads == 1;
+  const bool use_graph = opts && opts->use_graph && !serial;
+  std::vector<RunPrep> rp(n);
+  std::vector<FModel<R>> fm(n);
+  std::vector<TAcc> ta(n);
+  std::vector<long long> off(n + 1, 0);
+  mcg_status s;
+  for (int i = 0; i < n; ++i) {
+    ModelSlot slot(ctx, ids[i]);
+    if ((s = mcg_run_prepare(ctx, &runs[i], &nphot[i], &rp[i], false)) != MCG_OK) return s;
+    if ((s = build_fast_tables<R>(ctx, pi)) != MCG_OK) return s;
+    fill_fmodel<R>(ctx, pi, rp[i].tm, fm[i]);
+    ta[i] = rp[i].ta;
+    off[i + 1] = off[i] + (long long)rp[i].tm.nphot;
+  }
+  /* kernel arguments in one device buffer: models | accumulators | offsets | counter */
+  const size_t b_fm = ((size_t)n * sizeof(FModel<R>) + 255) & ~(size_t)255;
+  const size_t b_ta = ((size_t)n * sizeof(TAcc) + 255) & ~(size_t)255;
+  const size_t b_off = ((size_t)(n + 1) * sizeof(long long) + 255) & ~(size_t)255;
+  const size_t need = b_fm + b_ta + b_off + 256;
+  if (ctx->batch_args.bytes < need) {
+    if (ctx->batch_graph) {
+      cudaGraphExecDestroy(ctx->batch_graph);
+      ctx->batch_graph = nullptr;
+      ctx->batch_graph_key.clear();
+    }
+    if (ctx->batch_args.p) cudaFree(ctx->batch_args.p);
+    ctx->batch_args.p = nullptr;
+    ctx->batch_args.bytes = 0;
+    cudaError_t e = cudaMalloc(&ctx->batch_args.p, need);
+    if (e != cudaSuccess) return mcg_fail(ctx, MCG_ERR_NOMEM, "mcradiation_batch: %s", cudaGetErrorString(e));
+    ctx->batch_args.bytes = need;
+  }
+  unsigned char *base = (unsigned char *)ctx->batch_args.p;
+  FModel<R> *d_fm = (FModel<R> *)base;
+  TAcc *d_ta = (TAcc *)(base + b_fm);
+  long long *d_off = (long long *)(base + b_fm + b_ta);
+  unsigned long long *d_next = (unsigned long long *)(base + b_fm + b_ta + b_off);
+  MCG_CUDA(ctx, cudaMemcpyAsync(d_fm, fm.data(), (size_t)n * sizeof(FModel<R>), cudaMemcpyHostToDevice, st));
+  MCG_CUDA(ctx, cudaMemcpyAsync(d_ta, ta.data(), (size_t)n * sizeof(TAcc), cudaMemcpyHostToDevice, st));
+  MCG_CUDA(ctx, cudaMemcpyAsync(d_off, off.data(), (size_t)(n + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));
+
+  const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;
+  std::vector<long long> key;
+  key.push_back(pi);
+  for (int i = 0; i < n; ++i) {
+    key.push_back(ids[i]);
+    key.push_back((long long)rp[i].tm.nphot);
+    key.push_back(rp[i].nruns);
+  }
+  /* launch shape: explicit, tuned before, tuned now, or the default */
+  Shape sh{256, 2, 1};
+  if (ctx->tuned_block && ctx->tuned_key == key) sh = Shape{ctx->tuned_block, ctx->tuned_bps, ctx->tuned_chunk};
+  if (opts && opts->autotune && !serial && !(ctx->tuned_block && ctx->tuned_key == key)) {
+    /* short trial runs: 1/50 of every model's packets (at least 200) */
+    std::vector<FModel<R>> tf = fm;
+    std::vector<long long> toff(n + 1, 0);
+    for (int i = 0; i < n; ++i) {
+      const long long np = std::max<long long>(200, (long long)rp[i].tm.nphot / 50);
+      tf[i].nphot = np;
+      toff[i + 1] = toff[i] + np;
+    }
+    const Shape cand[] = {{256, 2, 1}, {128, 4, 1}, {256, 2, 4}, {128, 4, 4}, {256, 1, 1}};
+    float best = -1.0f;
+    for (const Shape &c : cand) {
+      for (int i = 0; i < n; ++i) {
+        ModelSlot slot(ctx, ids[i]);
+        MCG_CUDA(ctx, mcg_run_zero(ctx, (size_t)rp[i].nc * rp[i].nruns, rp[i].ns));
+      }
+      MCG_CUDA(ctx, cudaMemcpyAsync(d_fm, tf.data(), (size_t)n * sizeof(FModel<R>), cudaMemcpyHostToDevice, st));
+      MCG_CUDA(ctx, cudaMemcpyAsync(d_off, toff.data(), (size_t)(n + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));
+      MCG_CUDA(ctx, cudaMemsetAsync(d_next, 0, 8, st));
+      MCG_CUDA(ctx, cudaEventRecord(ctx->ev0, st));
+      transport_batch_kernel<R><<<sms * c.bps, c.block, 0, st>>>(d_fm, d_ta, d_off, n, d_next, c.chunk);
+      MCG_CUDA(ctx, cudaGetLastError());
+      MCG_CUDA(ctx, cudaEventRecord(ctx->ev1, st));
+      MCG_CUDA(ctx, cudaEventSynchronize(ctx->ev1));
+      float ms = 0.0f;
+      MCG_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+      if (best < 0.0f || ms < best) {
+        best = ms;
+        sh = c;
+      }
+    }
+    ctx->tuned_block = sh.block;
+    ctx->tuned_bps = sh.bps;
+    ctx->tuned_chunk = sh.chunk;
+    ctx->tuned_key = key;
+    MCG_CUDA(ctx, cudaMemcpyAsync(d_fm, fm.data(), (size_t)n * sizeof(FModel<R>), cudaMemcpyHostToDevice, st));
+    MCG_CUDA(ctx, cudaMemcpyAsync(d_off, off.data(), (size_t)(n + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));
+  }
+  if (opts && opts->block > 0) sh.block = opts->block;
+  if (opts && opts->blocks_per_sm > 0) sh.bps = opts->blocks_per_sm;
+  if (opts && opts->chunk > 0) sh.chunk = opts->chunk;
+  if (sh.block > F_BLOCK || sh.block % 32 != 0 || sh.bps < 1 || sh.bps > 8 || sh.chunk < 1 || sh.chunk > 64)
+    return mcg_fail(ctx, MCG_ERR_ARG, "mcradiation_batch: block <= %d (multiple of 32), 1 <= blocks_per_sm <= 8, "
+                    "1 <= chunk <= 64", F_BLOCK);
+  key.push_back(sh.block);
+  key.push_back(sh.bps);
+  key.push_back(sh.chunk);
+
+  /* the launch sequence: resets, the batched kernel, per-model combination */
+  auto enqueue = [&](bool timed) -> mcg_status {
+    for (int i = 0; i < n; ++i) {
+      ModelSlot slot(ctx, ids[i]);
+      MCG_CUDA(ctx, mcg_run_zero(ctx, (size_t)rp[i].nc * rp[i].nruns, rp[i].ns));
+    }
+    MCG_CUDA(ctx, cudaMemsetAsync(d_next, 0, 8, st));
+    if (timed) MCG_CUDA(ctx, cudaEventRecord(ctx->ev0, st));
+    if (serial)
+      transport_batch_kernel<R><<<1, 1, 0, st>>>(d_fm, d_ta, d_off, n, d_next, 1);
+    else
+      transport_batch_kernel<R><<<sms * sh.bps, sh.block, 0, st>>>(d_fm, d_ta, d_off, n, d_next, sh.chunk);
+    MCG_CUDA(ctx, cudaGetLastError());
+    if (timed) MCG_CUDA(ctx, cudaEventRecord(ctx->ev1, st));
+    for (int i = 0; i < n; ++i) {
+      ModelSlot slot(ctx, ids[i]);
+      mcg_run_combine(ctx, rp[i]);
+    }
+    MCG_CUDA(ctx, cudaGetLastError());
+    return MCG_OK;
+  };
+  float ms = 0.0f;
+  if (use_graph) {
+    if (!ctx->batch_graph || ctx->batch_graph_key != key) {
+      if (ctx->batch_graph) {
+        cudaGraphExecDestroy(ctx->batch_graph);
+        ctx->batch_graph = nullptr;
+      }
+      cudaGraph_t g = nullptr;
+      MCG_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      s = enqueue(false);
+      cudaError_t e = cudaStreamEndCapture(st, &g);
+      if (s != MCG_OK) {
+        if (g) cudaGraphDestroy(g);
+        return s;
+      }
+      if (e != cudaSuccess) return mcg_fail(ctx, MCG_ERR_CUDA, "mcradiation_batch: capture: %s", cudaGetErrorString(e));
+      e = cudaGraphInstantiate(&ctx->batch_graph, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) {
+        ctx->batch_graph = nullptr;
+        return mcg_fail(ctx, MCG_ERR_CUDA, "mcradiation_batch: graph: %s", cudaGetErrorString(e));
+      }
+      ctx->batch_graph_key = key;
+    }
+    MCG_CUDA(ctx, cudaEventRecord(ctx->ev0, st));
+    MCG_CUDA(ctx, cudaGraphLaunch(ctx->batch_graph, st));
+    MCG_CUDA(ctx, cudaEventRecord(ctx->ev1, st));
+  } else {
+    if ((s = enqueue(true)) != MCG_OK) return s;
+  }
+  MCG_CUDA(ctx, cudaEventSynchronize(ctx->ev1));
+  MCG_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  if (opts) {
+    opts->block = sh.block;
+    opts->blocks_per_sm = sh.bps;
+    opts->chunk = sh.chunk;
+    opts->device_ms = ms;
+  }
+  mcg_status first_err = MCG_OK;
+  for (int i = 0; i < n; ++i) {
+    ModelSlot slot(ctx, ids[i]);
+    s = mcg_run_finish(ctx, rp[i], ms, &res[i]);
+    if (s != MCG_OK && first_err == MCG_OK) first_err = s;
+  }
+  return first_err;
+}
+
+}  // namespace
+
+mcg_status mcg_add_model_impl(mcg_ctx *ctx, const mcg_grid *grid, const mcg_opacity *opac, int *id) {
+  if (!id) return mcg_fail(ctx, MCG_ERR_ARG, "add_model: null model_id");
+  if ((int)ctx->models.size() >= 65536) return mcg_fail(ctx, MCG_ERR_LIMIT, "add_model: at most 65536 kept models");
+  DevModel keep_model;
+  DevRun keep_run;
+  const bool keep_have = ctx->have_run;
+  std::swap(keep_model, ctx->model);
+  std::swap(keep_run, ctx->run);
+  mcg_status s = mcg_set_model_impl(ctx, grid, opac);
+  if (s == MCG_OK) {
+    ctx->models.push_back(DevModel());
+    ctx->runs.push_back(DevRun());
+    std::swap(ctx->models.back(), ctx->model);
+    *id = (int)ctx->models.size() - 1;
+  } else {
+    mcg_free_model(ctx->model);
+  }
+  std::swap(keep_model, ctx->model);
+  std::swap(keep_run, ctx->run);
+  ctx->have_run = keep_have;
+  return s;
+}
+
+mcg_status mcg_batch_impl(mcg_ctx *ctx, int n, const int *ids, const mcg_run *runs, int64_t *nphot, mcg_result *res,
+                          mcg_batch_opts *opts) {
+  if (n < 1 || n > MCG_BATCH_MAX || !ids || !runs || !nphot || !res)
+    return mcg_fail(ctx, MCG_ERR_ARG, "mcradiation_batch: 1 <= nmodels <= %d and non-null arrays", MCG_BATCH_MAX);
+  const int prec = runs[0].precision;
+  if (prec != MCG_PREC_FP64 && prec != MCG_PREC_MIXED)
+    return mcg_fail(ctx, MCG_ERR_ARG, "mcradiation_batch: precision must be FP64 or MIXED");
+  for (int i = 0; i < n; ++i) {
+    if (ids[i] < 0 || ids[i] >= (int)ctx->models.size())
+      return mcg_fail(ctx, MCG_ERR_ARG, "mcradiation_batch: unknown model id %d", ids[i]);
+    if (runs[i].precision != prec) return mcg_fail(ctx, MCG_ERR_ARG, "mcradiation_batch: mixed precisions");
+    for (int j = 0; j < i; ++j)
+      if (ids[j] == ids[i]) return mcg_fail(ctx, MCG_ERR_ARG, "mcradiation_batch: model %d listed twice", ids[i]);
+  }
+  if (prec == MCG_PREC_MIXED) return batch_run_t<float>(ctx, 1, n, ids, runs, nphot, res, opts);
+  return batch_run_t<double>(ctx, 0, n, ids, runs, nphot, res, opts);
+}
+
+void mcg_free_batch(mcg_ctx *ctx) {
+  if (ctx->batch_graph) cudaGraphExecDestroy(ctx->batch_graph);
+  ctx->batch_graph = nullptr;
+  if (ctx->batch_args.p) cudaFree(ctx->batch_args.p);
+  ctx->batch_args = DevBuf();
+  for (auto &m : ctx->models) mcg_free_model(m);
+  for (auto &r : ctx->runs) mcg_free_run(r);
+  ctx->models.clear();
+  ctx->runs.clear();
 }

@@ -53,6 +53,7 @@ struct FModel {
   const R *KabsTotR, *KextTotR; /* ncell*nlam (non-uniform mixtures) */
   const double *KabsTot;        /* ncell*nlam, for the per-cell scan */
   const double *BB, *dnu_half;
+  const double *BBT;            /* non-uniform mixtures: BB temperature-major */
   const double *KpCell;         /* uniform: 1 row, else ncell rows */
   const double *Ccum, *Dcum;    /* uniform mixture: TT*(nlam-1) */
   const double *comp_w;
@@ -503,24 +504,41 @@ F_COLD void f_interact(const FModel<R> &m, const TAcc &A, px_stream *r, FPkt<R> 
         f_pick<R>(m, p, lo, lo < n ? cum(lo) : 0.0, lo > 0 ? cum(lo - 1) : 0.0, Lr);
       }
     } else {
-      /* per-cell spectrum: sequential scan (Radiation.f:187-213) */
+      /* per-cell spectrum: sequential scan (Radiation.f:187-213), the
+       * additions in the reference's order; the Planck rows are read
+       * temperature-major and eight wavelengths at a time, so the loads of
+       * a block are issued together */
       const double *Ka = m.KabsTot + (size_t)c * nlam;
+      const double *P0 = m.BBT + (size_t)iT0 * nlam, *P0p = P0 + nlam;
+      const double *P1 = m.BBT + (size_t)iT1 * nlam, *P1p = P1 + nlam;
       auto spec = [&](int l) {
-        const double *Bl = m.BB + (size_t)l * TP_TT;
-        if (iT0 == iT1) return (Bl[iT0 + 1] - Bl[iT0]) * Ka[l];
-        return (((e1 * Bl[iT1 + 1] + (1.0 - e1) * Bl[iT1]) - e0 * Bl[iT0 + 1]) - (1.0 - e0) * Bl[iT0]) * Ka[l];
+        if (iT0 == iT1) return (P0p[l] - P0[l]) * Ka[l];
+        return (((e1 * P1p[l] + (1.0 - e1) * P1[l]) - e0 * P0p[l]) - (1.0 - e0) * P0[l]) * Ka[l];
       };
       double kpe = iT0 == iT1 ? kp[iT0 + 1] - kp[iT0]
                               : ((e1 * kp[iT1 + 1] + (1.0 - e1) * kp[iT1]) - e0 * kp[iT0 + 1]) - (1.0 - e0) * kp[iT0];
       const double Lr = xi * kpe;
       double Lt = 0.0, Ltold = 0.0, s0 = spec(0);
-      int i = 0;
-      for (; i < n; ++i) {
-        double s1 = spec(i + 1);
-        Lt = Lt + m.dnu_half[i] * (s0 + s1);
-        if (Lt >= Lr) break;
-        Ltold = Lt;
-        s0 = s1;
+      int i = n;
+      for (int i0 = 0; i0 < n && i == n; i0 += 8) {
+        double sb[8], dn[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int l = i0 + u;
+          sb[u] = l < n ? spec(l + 1) : 0.0;
+          dn[u] = l < n ? m.dnu_half[l] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          if (i0 + u >= n) break;
+          Lt = Lt + dn[u] * (s0 + sb[u]);
+          if (Lt >= Lr) {
+            i = i0 + u;
+            break;
+          }
+          Ltold = Lt;
+          s0 = sb[u];
+        }
       }
       f_pick<R>(m, p, i, Lt, Ltold, Lr);
     }
@@ -537,22 +555,35 @@ F_COLD void f_interact(const FModel<R> &m, const TAcc &A, px_stream *r, FPkt<R> 
       R KscaR = O::u(px_next(r)) * ksca;
       const double *w = m.comp_w + (size_t)c * m.ncomp;
       int mat = -1, qlast = 0, llast = l1;
-      for (int q = 0; q < m.ncomp; ++q) {
-        const R wq = (R)w[q];
-        const R w2 = wq * p.wl2 * m.Ksca_c[q * nlam + l1 + 1];
-        KscaR -= w2;
-        if (KscaR < (R)0) {
-          mat = q * nlam + l1 + 1;
-          break;
+      /* the reference's order (Radiation.f:273-290): per component the
+       * l1+1 term, then the l1 term; weights and opacities of four
+       * components are loaded together */
+      for (int q0 = 0; q0 < m.ncomp && mat < 0; q0 += 4) {
+        R w2b[4], w1b[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int q = q0 + u;
+          const R wq = q < m.ncomp ? (R)w[q] : (R)0;
+          w2b[u] = q < m.ncomp ? wq * p.wl2 * m.Ksca_c[q * nlam + l1 + 1] : (R)0;
+          w1b[u] = q < m.ncomp ? wq * p.wl1 * m.Ksca_c[q * nlam + l1] : (R)0;
         }
-        const R w1 = wq * p.wl1 * m.Ksca_c[q * nlam + l1];
-        KscaR -= w1;
-        if (KscaR < (R)0) {
-          mat = q * nlam + l1;
-          break;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int q = q0 + u;
+          if (q >= m.ncomp) break;
+          KscaR -= w2b[u];
+          if (KscaR < (R)0) {
+            mat = q * nlam + l1 + 1;
+            break;
+          }
+          KscaR -= w1b[u];
+          if (KscaR < (R)0) {
+            mat = q * nlam + l1;
+            break;
+          }
+          if (w2b[u] > (R)0) { qlast = q; llast = l1 + 1; }
+          if (w1b[u] > (R)0) { qlast = q; llast = l1; }
         }
-        if (w2 > (R)0) { qlast = q; llast = l1 + 1; }
-        if (w1 > (R)0) { qlast = q; llast = l1; }
       }
       if (mat < 0) {
         L.cnt[TC_AVGMAT]++;

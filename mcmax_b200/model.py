@@ -208,48 +208,42 @@ def spatial_grid(rstar_cm, rin, rout, nrad, ntheta):
 
 
 def cell_volumes(R, Theta):
-    nR = R.size - 1
-    nc = Theta.size - 1
-    V = np.zeros((nR, nc))
-    for i in range(nR):
-        for j in range(nc):
-            V[i, j] = (4.0 * math.pi / 3.0) * (R[i + 1] ** 3 - R[i] ** 3) * (Theta[j] - Theta[j + 1]) * AU ** 3
-    return V
+    R = np.asarray(R, float)
+    Theta = np.asarray(Theta, float)
+    return (4.0 * math.pi / 3.0) * (R[1:, None] ** 3 - R[:-1, None] ** 3) * (Theta[None, :-1] - Theta[None, 1:]) \
+        * AU ** 3
 
 
 def zones_density(R, Theta, thet, zones):
     """'ZONES' dust density (Init.f:3054-3139).  zones: list of dicts with
-    rin, rout, mdust (Msun), denspow, sh, rsh, shpow.  Cell i = 0 gets 1e-60
+    rin, rout, mdust (Msun), denspow, sh, rsh, shpow.  Each cell averages the
+    zone profile over 10 sub-angles; cell i = 0 gets 1e-60
     (Init.f:2932-2938)."""
     nR = R.size - 1
     nc = Theta.size - 1
     V = cell_volumes(R, Theta)
     R_av = AU * 10.0 ** ((np.log10(R[:-1]) + np.log10(R[1:])) / 2.0)
+    thet = np.asarray(thet, float)
     dens = np.full((nR, nc), 1e-60)
     total = np.zeros((nR, nc))
     for z in zones:
-        zd = np.zeros((nR, nc))
-        tot = 0.0
-        for i in range(1, nR):
-            if not (R_av[i] >= z["rin"] * AU and R_av[i] <= z["rout"] * AU):
-                continue
-            for j in range(nc):
-                acc = 0.0
-                for jj in range(1, 11):
-                    theta = thet[j] + (thet[j + 1] - thet[j]) * jj / 11.0
-                    r = R_av[i] * math.sin(theta) / AU
-                    zz = R_av[i] * math.cos(theta) / AU
-                    hr = z["sh"] * (r / z["rsh"]) ** z["shpow"]
-                    f1 = r ** (-z["denspow"])
-                    f2 = math.exp(-(zz / hr) ** 2)
-                    acc += f1 * f2 / hr / 10.0
-                zd[i, j] = acc
-                tot += acc * V[i, j]
+        inside = (R_av >= z["rin"] * AU) & (R_av <= z["rout"] * AU)
+        inside[0] = False
+        acc = np.zeros((nR, nc))
+        for jj in range(1, 11):
+            theta = thet[:-1] + (thet[1:] - thet[:-1]) * jj / 11.0
+            r = R_av[:, None] * np.sin(theta)[None, :] / AU
+            zz = R_av[:, None] * np.cos(theta)[None, :] / AU
+            hr = z["sh"] * (r / z["rsh"]) ** z["shpow"]
+            f1 = r ** (-z["denspow"])
+            f2 = np.exp(-(zz / hr) ** 2)
+            acc = acc + f1 * f2 / hr / 10.0
+        zd = np.where(inside[:, None], acc, 0.0)
+        tot = (zd * V).sum()
         zd *= z["mdust"] * MSUN / tot
         total += zd
     dens[1:] = 1e-60 + total[1:]
     return dens, V
-
 
 def grain_rv(amin, amax, apow, ns):
     """rv = sqrt(<a^2>) of a bin's ns sizes in cm (ComputePart.f:950-976;
