@@ -19,6 +19,13 @@ path of the launch).  `value` is the device time of the transport kernel with
 all tables resident in HBM; `e2e` times the reference-facing C-ABI
 (mcg_set_model from host buffers + mcg_mcradiation + result copies to host).
 
+The same line carries `learned_deck`: the learned-opacities deck (three
+compositions in 50 bins from 0.01 to 1000 micron, vertically settled) in its
+plain form (FP64 transport on DHS opacities) and in its fast form (mixed
+transport on the opacity surrogate's tables), with opacity-stage time,
+packets/s, end-to-end time per step and the agreement of per-cell
+temperatures and SEDs with the plain form on identical Philox streams.
+
 --impl reference runs the oracle (the CPU restatement of the reference's
 loop; the Fortran reference cannot be compiled without a Fortran compiler) on
 all host cores.
@@ -54,6 +61,8 @@ def parse():
     ap.add_argument("--compare-fp64", action="store_true", help="also time the FP64 form (one step)")
     ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--learned-nphot", type=int, default=30_000_000,
+                    help="packets per run of the learned-opacities comparison (0 skips it)")
     ap.add_argument("--maxinteract", type=int, default=RUN["maxinteract"],
                     help="overflow roulette (keyword maxinteract); smaller values shorten the trapped-packet tail "
                          "for profiling runs")
@@ -141,6 +150,58 @@ def cpu_baseline_sample(model, seconds, cores):
         if n <= 0:
             break
     return total_n / total_t, total_n, total_t
+
+
+def learned_deck_comparison(ctx, nphot, seed0):
+    """The learned-opacities deck (three compositions in 50 bins from 0.01 to
+    1000 micron, settled with alpha = 1e-3, nr 200 x ntheta 120, nlam 200)
+    in its two forms: plain FP64 transport on DHS opacities and mixed
+    transport on surrogate opacities.  Both runs use the same Philox seed;
+    a second FP64 run with another seed gives the Monte Carlo noise floor
+    of the agreement figures.  Per step: opacity stage (ComputePart of the
+    150 bins), mcg_set_model from host arrays, the packet loop, results to
+    the host."""
+    import numpy as np
+    from mcmax_b200 import model as M
+    from mcmax_b200 import surrogate as S
+    params, sinfo = S.load(os.path.join(ROOT, "mcmax_b200", "data", "surrogate_nf20.npz"))
+    out = {"workload": "learned-opacities deck: 3 compositions x 50 bins 0.01-1000 micron (ns 5, nf 20), "
+                       "settling alpha 1e-3, Mdust 1e-3 Msun, nr 200 x ntheta 120, nlam 200, random walk, "
+                       "maxinteract %g, %d packets per run" % (RUN["maxinteract"], nphot)}
+    runs = {}
+    for tag, opac, prec, seed in (("fp64_dhs", "dhs", "fp64", seed0), ("mixed_surrogate", "surrogate", "mixed", seed0),
+                                  ("fp64_dhs_seed2", "dhs", "fp64", seed0 + 1)):
+        t0 = time.perf_counter()
+        m, t_opac, served = M.learned_disk_model(ctx, opacity=opac, params=params if opac == "surrogate" else None)
+        ctx.set_model(m)
+        t_setup = time.perf_counter() - t0
+        t1 = time.perf_counter()
+        _, o = ctx.mcradiation(nphot, seed=seed, precision=prec, fetch=True, **RUN)
+        T, _, _ = ctx.finalize_t()
+        t_run = time.perf_counter() - t1
+        runs[tag] = dict(T=T, spec=o["spec"], Ni=o["Ni"])
+        out[tag] = {"opacity_stage_s": t_opac, "setup_s": t_setup, "transport_device_ms": o["device_ms"],
+                    "packets_per_s": nphot / (o["device_ms"] / 1e3), "run_s": t_run,
+                    "e2e_step_s": t_setup + t_run, "bins_served_by_network": served,
+                    "progress_ms": o["progress_ms"]}
+    ref = runs["fp64_dhs"]
+    sel = (ref["Ni"] >= 1000) & (ref["T"] > 0)
+    for tag in ("mixed_surrogate", "fp64_dhs_seed2"):
+        r = runs[tag]
+        rel = np.abs(r["T"][sel] / ref["T"][sel] - 1)
+        sr, sp = ref["spec"][:, 1:].sum(1), r["spec"][:, 1:].sum(1)
+        ok = sr > 0
+        sed = np.abs(sp[ok] / sr[ok] - 1)
+        out[tag]["agreement_with_fp64_dhs"] = {
+            "cells_Ni_ge_1e3": int(sel.sum()), "T_within_1pct": float(np.mean(rel < 0.01)),
+            "T_median_rel": float(np.median(rel)), "T_p95_rel": float(np.percentile(rel, 95)),
+            "sed_median_rel": float(np.median(sed))}
+    out["speedup_e2e_step"] = out["fp64_dhs"]["e2e_step_s"] / out["mixed_surrogate"]["e2e_step_s"]
+    out["speedup_transport"] = out["mixed_surrogate"]["packets_per_s"] / out["fp64_dhs"]["packets_per_s"]
+    out["surrogate"] = {"train_samples": int(sinfo["n"]), "epochs": int(sinfo["epochs"]),
+                        "bins_median_dex_kabs": float(sinfo["bins_median_dex_kabs"]),
+                        "bins_median_dex_ksca": float(sinfo["bins_median_dex_ksca"])}
+    return out
 
 
 def build_model(ctx):
@@ -274,6 +335,9 @@ def main():
         t64 = _max_over_ranks(dist, o64["device_ms"] / 1e3)
         fp64_line = {"value": args.nphot * world / t64, "unit": "packets/s", "steps": 1,
                      "ms_per_step": 1e3 * t64}
+    learned = None
+    if rank == 0 and world == 1 and args.learned_nphot > 0:
+        learned = learned_deck_comparison(ctx, args.learned_nphot, 7_000_003)
     # roofline of the transport kernel against the measured HBM copy bandwidth
     peaks = {}
     try:
@@ -321,6 +385,8 @@ def main():
         }
         if fp64_line:
             line["fp64_form"] = fp64_line
+        if learned:
+            line["learned_deck"] = learned
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist:
@@ -331,16 +397,19 @@ def main():
 def _barrier(dist):
     if dist:
         import torch
-        torch.cuda.synchronize()
+        if dist.get_backend() == "nccl":
+            torch.cuda.synchronize()
         dist.barrier()
     return True
 
 
 def _max_over_ranks(dist, v):
+    """the largest value over the ranks (timings: the slowest rank)"""
     if not dist:
         return v
     import torch
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 

@@ -55,6 +55,8 @@ struct DevModel {
   /* random walk */
   double *KDext = nullptr, *KDabs = nullptr; /* nthick_alloc*TT */
   int *kd_index = nullptr;  /* ncell -> row of KDext/KDabs or -1 */
+  double *rw_dmin = nullptr; /* ncell: factRW x the shortest mean free path of the
+                                cell's diffusion table (1e300 when not thick) */
   unsigned char *thick = nullptr;
   double *rw_y = nullptr, *rw_phi = nullptr; /* 1000 each */
   int kd_rows = 0;

@@ -429,6 +429,23 @@ mcg_status mcg_set_model_impl(mcg_ctx *ctx, const mcg_grid *g, const mcg_opacity
   return MCG_OK;
 }
 
+/* per thick cell: factRW / (AU * max_iT KDext * dens), the bound below which
+ * no random-walk jump can be taken at any temperature (one warp per row) */
+__global__ void rw_dmin_kernel(int nrows, const int *cells, const double *KDext, const double *dens, double factRW,
+                               double *rw_dmin) {
+  const int lane = threadIdx.x & 31;
+  const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (r >= nrows) return;
+  double kmax = 0.0;
+  for (int iT = 1 + lane; iT <= TP_TMAX - 1; iT += 32) kmax = fmax(kmax, KDext[(size_t)r * TP_TT + iT]);
+  for (int s = 16; s > 0; s >>= 1) kmax = fmax(kmax, __shfl_down_sync(0xffffffffu, kmax, s));
+  if (lane == 0) {
+    const int c = cells[r];
+    const double lr = 1.0 / ((TP_AU * kmax) * dens[c]);
+    rw_dmin[c] = kmax > 0.0 ? factRW * lr : 1e300;
+  }
+}
+
 /* thick flags (InitRandomWalk, RandomWalk.f:172-190) and the diffusion
  * tables of the thick cells for all iT */
 static mcg_status build_rw_tables(mcg_ctx *ctx, double factRW) {
@@ -498,6 +515,21 @@ static mcg_status build_rw_tables(mcg_ctx *ctx, double factRW) {
   }
   MCG_CUDA(ctx, cudaMemcpyAsync(m.thick, thick.data(), ncell, cudaMemcpyHostToDevice, st));
   MCG_CUDA(ctx, cudaMemcpyAsync(m.kd_index, idx.data(), sizeof(int) * ncell, cudaMemcpyHostToDevice, st));
+  if (!m.rw_dmin) {
+    e = cudaMalloc(&m.rw_dmin, sizeof(double) * (size_t)ncell);
+    if (e != cudaSuccess) {
+      cudaFree(den); cudaFree(kd4e); cudaFree(kd4a); cudaFree(cells);
+      return mcg_fail(ctx, MCG_ERR_NOMEM, "random walk: %s", cudaGetErrorString(e));
+    }
+    m.owned.push_back(m.rw_dmin);
+  }
+  {
+    std::vector<double> lim(ncell, 1e300);
+    MCG_CUDA(ctx, cudaMemcpyAsync(m.rw_dmin, lim.data(), sizeof(double) * ncell, cudaMemcpyHostToDevice, st));
+    MCG_CUDA(ctx, cudaStreamSynchronize(st));
+  }
+  if (nrows > 0)
+    rw_dmin_kernel<<<nblk((long long)nrows * 32, B), B, 0, st>>>(nrows, cells, m.KDext, m.dens, factRW, m.rw_dmin);
   MCG_CUDA(ctx, cudaGetLastError());
   MCG_CUDA(ctx, cudaStreamSynchronize(st));
   cudaFree(den);

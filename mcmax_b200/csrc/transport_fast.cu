@@ -288,7 +288,7 @@ void fill_fmodel(mcg_ctx *ctx, int pi, const TModel &tm, FModel<R> &g) {
   g.scatA = (const R *)f.scatA; g.scatB = (const R *)f.scatB; g.F6 = (const R *)f.F6; g.IF_c = m.IF_c;
   g.scatG = f.scatG; g.emitG = m.emitG;
   g.KDext = m.KDext; g.KDabs = m.KDabs; g.rw_logy = m.rw_logy; g.rw_phi = m.rw_phi;
-  g.kd_index = m.kd_index; g.thick = m.thick;
+  g.kd_index = m.kd_index; g.thick = m.thick; g.rw_dmin = m.rw_dmin;
 }
 
 template <class R>

@@ -65,6 +65,7 @@ struct FModel {
   const double *KDext, *KDabs, *rw_logy, *rw_phi;
   const int *kd_index;
   const unsigned char *thick;
+  const double *rw_dmin;        /* factRW x the cell's shortest mean free path */
 };
 
 #define F_NGUIDE 32
@@ -598,8 +599,6 @@ F_COLD void f_interact(const FModel<R> &m, const TAcc &A, px_stream *r, FPkt<R> 
 template <class R>
 F_COLD int f_random_walk(const FModel<R> &m, const TAcc &A, px_stream *r, FPkt<R> &p, TLocal &L) {
   const int c = p.i * m.nc + (p.j - 1);
-  const int row = m.kd_index[c];
-  if (row < 0) return 0;
   /* distance to the nearest face (MinDist, RandomWalk.f:15-43) */
   double rho = p.x * p.x + p.y * p.y;
   const double rr = sqrt(rho + p.z * p.z);
@@ -612,6 +611,12 @@ F_COLD int f_random_walk(const FModel<R> &m, const TAcc &A, px_stream *r, FPkt<R
   if (t < dmin) dmin = t;
   t = fabs(m.Theta[p.j] * rho - m.SinTheta[p.j] * z);
   if (t < dmin) dmin = t;
+  /* no jump at any temperature: dmin is within factRW of the cell's
+   * shortest mean free path (the test below at the current temperature
+   * would fail too), so the table lookups are skipped */
+  if (m.rw_dmin && dmin <= m.rw_dmin[c]) return 0;
+  const int row = m.kd_index[c];
+  if (row < 0) return 0;
   int iT = (int)A.T[c];
   if (iT < 1) iT = 1;
   if (iT > TP_TMAX - 1) iT = TP_TMAX - 1;
