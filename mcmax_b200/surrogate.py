@@ -93,6 +93,10 @@ def train(ctx, samples, T, epochs=300, batch=8192, lr=2e-3, lr_min=2e-5, seed=1)
     mean = T.mean(0)
     std = T.std(0)
     std[std < 1e-6] = 1.0
+    # powers of two: folding them into the output layer commutes with the
+    # BF16 rounding of its weights, so the folded network computes exactly
+    # what was trained
+    std = (2.0 ** np.round(np.log2(std))).astype(np.float32)
     Ts = ((T - mean) / std).astype(np.float32)
     ctx.mlp_set_params(init_params(seed))
     t0 = time.perf_counter()

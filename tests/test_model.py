@@ -68,3 +68,40 @@ def test_mrn_abundances():
     w = M.mrn_abundances(rg, 0.1e-4, 1e-4, 3.5)
     assert abs(w.sum() - 1) < 1e-9 and np.all(w > 0)
     assert w[-1] > w[0]  # a^-3.5: mass in the large grains
+
+
+def test_settling_conserves_each_grain_mass_and_settles_large_grains():
+    R, Th, thet, ST = M.spatial_grid(2.5 * M.RSUN, 0.5, 100.0, 24, 16)
+    zone = dict(rin=0.5, rout=100, mdust=1e-3, denspow=1.0, sh=0.05 * math.sqrt(2.0), rsh=1.0, shpow=1.125)
+    dens, V = M.zones_density(R, Th, thet, [zone])
+    ng = 5
+    w = np.tile(np.full(ng, 1.0 / ng), (dens.shape[0], dens.shape[1], 1))
+    rv = np.array([1e-6, 1e-5, 1e-4, 1e-3, 1e-2])
+    d2, w2 = M.fixed_mp_settling(R, Th, 16, dens, V, w, np.full(ng, 3.0), rv, 1e-3, zone)
+    assert np.allclose(w2.sum(2), 1.0)
+    for ii in range(ng):
+        m0 = (dens[1:] * V[1:] * w[1:, :, ii]).sum()
+        m1 = (d2[1:] * V[1:] * w2[1:, :, ii]).sum()
+        assert abs(m1 / m0 - 1) < 1e-12
+    i = 12
+    nc = w2.shape[1]
+    # an upper cell that still holds dust: the big grains have left it
+    upper = [j for j in range(nc - 3) if d2[i, j] * w2[i, j, 0] > 1e-40][-1]
+    assert w2[i, upper, -1] < 0.1 * w2[i, upper, 0]
+    assert w2[i, nc - 1, -1] > w2[i, nc - 1, 0]   # and collect at the midplane
+
+
+def test_grain_rv_and_theta_centres():
+    assert abs(M.grain_rv(0.5, 0.5, 3.5, 1) - 0.5e-4) < 1e-16
+    rv = M.grain_rv(0.1, 1.0, 3.5, 5)
+    assert 0.1e-4 < rv < 1.0e-4
+    th = M.theta_centres(60)
+    assert th.size == 60 and np.all(np.diff(th) > 0) and th[-1] < math.pi / 2
+
+
+def test_learned_deck_parts():
+    lam, _ = M.wavelength_grid(0.1, 3000.0, 12)
+    parts, bins = M.learned_disk_parts(lam, ngrains=5)
+    assert len(parts) == 15 and len(bins) == 5
+    assert abs(bins[0][0] - 0.01) < 1e-12 and abs(bins[-1][1] - 1000.0) < 1e-9
+    assert {p["porosity"] for p in parts} == {0.0, 0.2, 0.4}
