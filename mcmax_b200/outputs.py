@@ -1,0 +1,148 @@
+"""The reference's ASCII output files, written from the library's results so
+that MCMax's own readers and plotting scripts take them unchanged.
+
+    write_denstemp(path, model, T)        denstemp.dat (outputstruct,
+                                          InputOutput.f:6-227, format 5 with
+                                          DENS, TEMP, COMP, GASDENS, DENS0 as
+                                          Main.f:605 writes it)
+    read_denstemp(path)                   the same file back
+    write_mcspec(outdir, model, result)   MCSpec<angle>.dat per inclination
+                                          bin and MCSpec.dat
+                                          (MCRadiation.f:738-762)
+
+Cells are written for ir = 1..nR-1 (the star cell is left out) and it =
+1..nTheta-1, radius and angle at the cell middles (D%R_av in cm, D%theta_av
+in radians from the pole).  Numbers are written in free format, one or a
+row per line, as list-directed Fortran output is read back.
+"""
+import math
+import os
+
+import numpy as np
+
+from . import model as M
+
+PARSEC = 3.08568025e18
+
+
+def _r_av_cm(R):
+    R = np.asarray(R, float)
+    return M.AU * 10.0 ** ((np.log10(R[:-1]) + np.log10(R[1:])) / 2.0)
+
+
+def _num(x):
+    return " %.16E" % float(x)
+
+
+def write_denstemp(path, model, T, dens0=None, gas2dust=100.0):
+    """denstemp.dat of a model and its cell temperatures T (ncell, the
+    library's cell order c = i*(nt-1) + (j-1)).  dens0: the dust density
+    before settling (defaults to the model's density); the gas density is
+    written as dens0 * gas2dust (C%gasdens*gas2dust)."""
+    nr, nc = model.nr, model.nt - 1
+    ng = model.ncomp
+    dens = np.asarray(model.dens, float).reshape(nr, nc)
+    T = np.asarray(T, float).reshape(nr, nc)
+    comp = np.asarray(model.comp_w, float).reshape(nr, nc, ng)
+    d0 = dens if dens0 is None else np.asarray(dens0, float).reshape(nr, nc)
+    r_av = _r_av_cm(model.R)
+    th = M.theta_centres(nc)
+    with open(path, "w") as f:
+        f.write("# Format number\n")
+        f.write("%6d\n" % 5)
+        f.write("# NR, NT, NGRAINS, NGRAINS2\n")
+        f.write("%6d%6d%6d%6d\n" % (nr - 1, nc, ng, 1))
+        f.write("# Spherical radius grid [cm] (middle of cell)\n")
+        for i in range(1, nr):
+            f.write(_num(r_av[i]) + "\n")
+        f.write("# Theta grid [rad, from pole] (middle of cell)\n")
+        for j in range(nc):
+            f.write(_num(th[j]) + "\n")
+        blocks = (("# Density array (for ir=0,nr-1 do for it=0,nt-1 do ...)", dens),
+                  ("# Temperature array (for ir=0,nr-1 do for it=0,nt-1 do ...)", T))
+        for title, a in blocks:
+            f.write(title + "\n")
+            for i in range(1, nr):
+                for j in range(nc):
+                    f.write(_num(a[i, j]) + "\n")
+        f.write("# Composition array (for ir=0,nr-1 do for it=0,nt-1 do ...)\n")
+        for i in range(1, nr):
+            for j in range(nc):
+                f.write("".join(_num(v) for v in comp[i, j]) + "\n")
+        f.write("# Gas density array (for ir=0,nr-1 do for it=0,nt-1 do ...)\n")
+        for i in range(1, nr):
+            for j in range(nc):
+                f.write(_num(d0[i, j] * gas2dust) + "\n")
+        f.write("# Density0 array (for ir=0,nr-1 do for it=0,nt-1 do ...)\n")
+        for i in range(1, nr):
+            for j in range(nc):
+                f.write(_num(d0[i, j]) + "\n")
+
+
+def read_denstemp(path):
+    """dict with r_av, theta_av, dens, T, comp, gasdens, dens0 ((nr-1, nt-1)
+    arrays) from a format-5 denstemp.dat"""
+    with open(path) as f:
+        lines = [ln for ln in f.read().splitlines() if ln.strip() and not ln.lstrip().startswith("#")]
+    fmt = int(lines[0])
+    if fmt != 5:
+        raise ValueError("denstemp format %d: only format 5 is read" % fmt)
+    nr, nt, ng, ng2 = (int(x) for x in lines[1].split())
+    k = 2
+    r_av = np.array([float(x) for x in lines[k:k + nr]])
+    k += nr
+    th = np.array([float(x) for x in lines[k:k + nt]])
+    k += nt
+
+    def block(width=1):
+        nonlocal k
+        rows = [[float(x) for x in ln.split()] for ln in lines[k:k + nr * nt]]
+        k += nr * nt
+        a = np.array(rows)
+        return a.reshape(nr, nt, width) if width > 1 else a.reshape(nr, nt)
+
+    dens = block()
+    T = block()
+    comp = block(ng)
+    gas = block()
+    dens0 = block()
+    return dict(r_av=r_av, theta_av=th, dens=dens, T=T, comp=comp, gasdens=gas, dens0=dens0, ngrains=ng)
+
+
+def mcspec_name(j, nangle=30):
+    """file name of inclination bin j = 1..nangle (MCRadiation.f:741-743):
+    the bin's angle written as one digit of tens and f3.1 of the rest"""
+    angle = 180.0 * math.acos((j - 0.5) / nangle) / math.pi
+    tens = int(angle / 10.0)
+    return "MCSpec%d%3.1f.dat" % (tens, angle - 10.0 * tens)
+
+
+def write_mcspec(outdir, model, result, distance_pc=100.0, nangle=30):
+    """MCSpec<angle>.dat for the nangle inclination bins and MCSpec.dat.
+
+    Columns (MCRadiation.f:752-753): wavelength [micron], flux density
+    [Jy] spec/d^2, its Monte Carlo error spec/sqrt(ispec)/d^2, the scattered
+    part scatspec/d^2, a scattered-packet count, and the stellar flux
+    1e23 Fstar/d^2; no interstellar extinction.  The library counts
+    escaping packets per bin (ispec) but not the scattered ones separately,
+    so the fifth column is 0.  It does not fill the narrow observer bin 0
+    (MCRadiation.f:610-612), so MCSpec.dat holds zeros."""
+    os.makedirs(outdir, exist_ok=True)
+    d2 = (distance_pc * PARSEC) ** 2
+    spec = np.asarray(result["spec"], float).reshape(model.nlam, nangle + 1)
+    scat = np.asarray(result["scatspec"], float).reshape(model.nlam, nangle + 1)
+    ispec = np.asarray(result["ispec"]).reshape(model.nlam, nangle + 1)
+    names = []
+    for j in range(1, nangle + 1):
+        name = mcspec_name(j, nangle)
+        names.append(name)
+        with open(os.path.join(outdir, name), "w") as f:
+            for i in range(model.nlam):
+                n = int(ispec[i, j])
+                dspec = spec[i, j] / math.sqrt(n) if n > 0 else 0.0
+                f.write("%s%s%s%s %d%s\n" % (_num(model.lam[i]), _num(spec[i, j] / d2), _num(dspec / d2),
+                                            _num(scat[i, j] / d2), 0, _num(1e23 * model.Fstar[i] / d2)))
+    with open(os.path.join(outdir, "MCSpec.dat"), "w") as f:
+        for i in range(model.nlam):
+            f.write("%s%s\n" % (_num(model.lam[i]), _num(spec[i, 0] / d2)))
+    return names

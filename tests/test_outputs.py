@@ -1,0 +1,46 @@
+"""The reference's output files written from library results: denstemp.dat
+(format 5) round trip, and the MCSpec file names and columns."""
+import math
+import os
+
+import numpy as np
+
+import models
+from mcmax_b200 import outputs as OUT
+
+
+def test_denstemp_round_trip(tmp_path):
+    m = models.small_disk()
+    rng = np.random.default_rng(2)
+    T = rng.uniform(10, 1500, m.ncell)
+    p = os.path.join(tmp_path, "denstemp.dat")
+    OUT.write_denstemp(p, m, T)
+    d = OUT.read_denstemp(p)
+    nr, nc = m.nr, m.nt - 1
+    assert d["dens"].shape == (nr - 1, nc) and d["ngrains"] == m.ncomp
+    assert np.array_equal(d["T"], T.reshape(nr, nc)[1:])
+    assert np.array_equal(d["dens"], m.dens.reshape(nr, nc)[1:])
+    assert np.array_equal(d["comp"], m.comp_w.reshape(nr, nc, m.ncomp)[1:])
+    assert np.allclose(d["gasdens"], 100.0 * d["dens0"], rtol=1e-15)
+    assert np.all(np.diff(d["r_av"]) > 0) and np.all(np.diff(d["theta_av"]) > 0)
+    assert abs(d["r_av"][0] / 1.49598e13 - math.sqrt(m.R[1] * m.R[2])) < 1e-9 * d["r_av"][0] / 1.49598e13
+
+
+def test_mcspec_names_and_columns(tmp_path):
+    names = [OUT.mcspec_name(j) for j in range(1, 31)]
+    assert names[0] == "MCSpec89.0.dat" and names[-1] == "MCSpec10.5.dat"
+    assert len(set(names)) == 30
+    m = models.small_disk()
+    ns = m.nlam * 31
+    rng = np.random.default_rng(1)
+    res = dict(spec=rng.uniform(0, 1, ns), scatspec=rng.uniform(0, 0.1, ns), ispec=rng.integers(0, 50, ns))
+    OUT.write_mcspec(str(tmp_path), m, res, distance_pc=140.0)
+    a = np.loadtxt(os.path.join(tmp_path, names[5]))
+    assert a.shape == (m.nlam, 6)
+    d2 = (140.0 * OUT.PARSEC) ** 2
+    sp = res["spec"].reshape(m.nlam, 31)[:, 6]
+    assert np.allclose(a[:, 0], m.lam) and np.allclose(a[:, 1], sp / d2, rtol=1e-15)
+    n = res["ispec"].reshape(m.nlam, 31)[:, 6]
+    ok = n > 0
+    assert np.allclose(a[ok, 2], sp[ok] / np.sqrt(n[ok]) / d2, rtol=1e-14)
+    assert os.path.exists(os.path.join(tmp_path, "MCSpec.dat"))
