@@ -488,6 +488,141 @@ def learned_disk_model(ctx, *, opacity="dhs", params=None, tstar=10000.0, rstar=
     return m, t_opac, served
 
 
+def deck_model(ctx, deck, overrides=(), compute_parts=None):
+    """Model and run parameters from an MCMax input deck: the keywords the
+    packet loop and ComputePart read (Init.f:462-1240), with the reference's
+    defaults (Init.f:66-384).
+
+    Keywords used: startype ('PLANCK'), tstar, rstar [Rsun]; rin, rout, nrad,
+    ntheta; denstype ('ZONES') with zoneN:rin, rout, mdust, denspow, sh,
+    rsh, shpow; lam1, lam2, nlam; scattype (NONE, ISOTROPIC, FULL);
+    computepartNN:file (particle file: ns, nf, then per material an .lnk
+    path and 'frac rho'), amin, amax, apow, fmax, ngrains, blend,
+    porosity, norm_abun, standard ('FILE'), with amin, amax, apow (micron)
+    as the deck-wide defaults; abunNN (relative mass of computepart entry
+    NN); fixmpset, alphaturb (settling of a one-zone
+    disk); randomwalk, factrw, maxinteract, nruns, idum.  A value that
+    selects physics outside the packet loop (another startype or denstype,
+    scattype RAYLEIGH, tcontact false) raises ValueError.
+
+    deck: a path or the deck text; overrides: 'key=value' strings applied
+    after the file (the -s switches).  compute_parts(parts) returns the
+    ComputePart results of a list of grain bins (default: the library's
+    DHS kernels, ctx.compute_part_batch).  Returns (model, run) with run =
+    dict(seed, randomwalk, factRW, maxinteract, nruns) for mcradiation."""
+    base = "."
+    if os.path.exists(str(deck)):
+        base = os.path.dirname(os.path.abspath(deck))
+        with open(deck) as f:
+            text = f.read()
+    else:
+        text = deck
+    d = parse_deck(text, overrides)
+
+    def v(key, default, cast=float):
+        return deck_value(d, key, default, cast)
+
+    if v("startype", "PLANCK", str).upper() != "PLANCK":
+        raise ValueError("startype: only 'PLANCK' stars")
+    if v("denstype", "ZONES", str).upper() != "ZONES":
+        raise ValueError("denstype: only 'ZONES' densities")
+    if not v("tcontact", True, bool):
+        raise ValueError("tcontact: only thermal contact (Bjorkman-Wood with one temperature per cell)")
+    scat = {"NONE": 0, "ISOTROPIC": 1, "FULL": 2}.get(v("scattype", "ISOTROPIC", str).upper())
+    if scat is None:
+        raise ValueError("scattype: NONE, ISOTROPIC or FULL")
+    tstar, rstar = v("tstar", 10000.0), v("rstar", 2.1)
+    rin, rout = v("rin", 0.5), v("rout", 1000.0)
+    nrad, ntheta = v("nrad", 70, int), v("ntheta", 60, int)
+    lam1, lam2, nlam = v("lam1", 0.1), v("lam2", 10000.0), v("nlam", 100, int)
+    zones = []
+    for iz in range(1, 11):
+        kz = "zone%d:" % iz
+        if not any(k.startswith(kz) for k in d):
+            continue
+        zones.append(dict(rin=v(kz + "rin", rin), rout=v(kz + "rout", rout), mdust=v(kz + "mdust", 1e-5),
+                          denspow=v(kz + "denspow", 1.0), sh=v(kz + "sh", 0.01), rsh=v(kz + "rsh", 1.0),
+                          shpow=v(kz + "shpow", 1.1)))
+    if not zones:
+        raise ValueError("no zoneN:* keywords")
+    # grain bins of every computepart entry (Init.f:746-789, 1323-1420)
+    entries = sorted({int(k[len("computepart"):k.index(":")]) for k in d if k.startswith("computepart")
+                      and ":" in k})
+    if not entries:
+        raise ValueError("no computepartNN:* keywords")
+    rstar_cm = rstar * RSUN
+    lam, nu = wavelength_grid(lam1, lam2, nlam)
+    parts, weights = [], []
+    abun = np.array([v("abun%02d" % e, v("abun%d" % e, 1.0)) for e in entries])
+    abun = abun / abun.sum()
+    for e, ab in zip(entries, abun):
+        kp = "computepart%02d:" % e if any(k.startswith("computepart%02d:" % e) for k in d) else \
+            "computepart%d:" % e
+        if v(kp + "standard", "FILE", str).upper() != "FILE":
+            raise ValueError(kp + "standard: only 'FILE' particle files")
+        pfile = v(kp + "file", None, str)
+        if not pfile:
+            raise ValueError(kp + "file missing")
+        if not os.path.isabs(pfile):
+            pfile = os.path.join(base, pfile)
+        ns, nf, mats = read_particle_file(pfile)
+        e1, e2, frac, rho = [], [], [], []
+        for lnk, fr, rh in mats:
+            n_, k_ = readrefind(lnk, lam)
+            e1.append(n_)
+            e2.append(k_)
+            frac.append(fr)
+            rho.append(rh)
+        # unset sizes fall back to the deck-wide size distribution
+        # (Init.f:1155-1163, 1320-1322; defaults Init.f:174-176)
+        amin, amax = v(kp + "amin", -1.0), v(kp + "amax", -1.0)
+        apow, ngr = v(kp + "apow", 1e5), v(kp + "ngrains", 1, int)
+        if amin <= 0:
+            amin = v("amin", v("mrn_rmin", 0.01))
+        if amax <= 0:
+            amax = v("amax", v("mrn_rmax", 1000.0))
+        if apow > 100:
+            apow = v("apow", v("mrn_index", 3.5))
+        bins = grain_bins(amin, amax, ngr) if ngr > 1 else [(amin, amax)]
+        rg = [math.sqrt(a * b) * 1e-4 for a, b in bins]
+        wmrn = mrn_abundances(rg, amin * 1e-4, amax * 1e-4, apow) if ngr > 1 else np.ones(1)
+        for (a, b), wb in zip(bins, wmrn):
+            parts.append(dict(lam=lam, e1=np.array(e1), e2=np.array(e2), frac=np.array(frac), rho=np.array(rho),
+                              amin=a, amax=b, apow=apow, fmax=v(kp + "fmax", 0.0), porosity=v(kp + "porosity", 0.25),
+                              blend=v(kp + "blend", True, bool), ns=ns, nf=nf,
+                              normalize_abun=v(kp + "norm_abun", -1.0)))
+            weights.append(ab * wb)
+    res = (compute_parts or ctx.compute_part_batch)(parts)
+    Kabs = np.array([r["kabs"] for r in res])
+    Ksca = np.array([r["ksca"] for r in res])
+    F = np.array([r["F"] for r in res])
+    if scat == 0:
+        Ksca = np.zeros_like(Ksca)
+    if scat == 1:
+        F = np.ones_like(F)
+    R, Theta, thet, SinTheta = spatial_grid(rstar_cm, rin, rout, nrad, ntheta)
+    dens, V = zones_density(R, Theta, thet, zones)
+    BB = api.bb_table(lam)
+    Fstar = np.array([math.pi * rstar_cm ** 2 * api.planck(tstar, x) for x in lam])
+    Lstar = integrate(nu, Fstar)
+    nr, nt = R.size - 1, Theta.size
+    w0 = np.array(weights)
+    w = np.tile(w0, (nr, nt - 1, 1))
+    if v("fixmpset", False, bool):
+        if len(zones) != 1:
+            raise ValueError("fixmpset: settling of a one-zone disk")
+        rv = np.array([grain_rv(p["amin"], p["amax"], p["apow"], p["ns"]) for p in parts])
+        rho_g = np.array([r["rho_av"] for r in res])
+        dens, w = fixed_mp_settling(R, Theta, ntheta, dens, V, w, rho_g, rv, v("alphaturb", 1e-4), zones[0])
+    m = Model(nr=nr, nt=nt, R=R, Theta=Theta, SinTheta=SinTheta, thet=thet, dens=dens.reshape(-1), V=V.reshape(-1),
+              ncomp=len(parts), comp_w=w.reshape(nr * (nt - 1), len(parts)), nlam=nlam, lam=lam, nu=nu, Kabs=Kabs,
+              Ksca=Ksca, F=F, BB=BB, Fstar=Fstar, Lstar=Lstar, Tstar=tstar, Rstar_cm=rstar_cm, scat_how=scat,
+              bins=[(p["amin"], p["amax"]) for p in parts], w=w0, distance=v("distance", 100.0))
+    run = dict(seed=abs(v("idum", -42, int)), randomwalk=v("randomwalk", False, bool), factRW=v("factrw", 10.0),
+               maxinteract=v("maxinteract", 1000000, int), nruns=v("nruns", 1, int))
+    return m, run
+
+
 CONFIGS = {
     # small thin disk: the case a CPU run finishes quickly
     "small_thin_disk": dict(mdust=1e-5, nrad=100, ntheta=60, nlam=100),

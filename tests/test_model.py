@@ -4,6 +4,7 @@ import math
 import os
 
 import numpy as np
+import pytest
 
 from mcmax_b200 import model as M
 
@@ -105,3 +106,58 @@ def test_learned_deck_parts():
     assert len(parts) == 15 and len(bins) == 5
     assert abs(bins[0][0] - 0.01) < 1e-12 and abs(bins[-1][1] - 1000.0) < 1e-9
     assert {p["porosity"] for p in parts} == {0.0, 0.2, 0.4}
+
+
+def test_deck_model_builds_the_disk_model_of_its_keywords(tmp_path):
+    import oracle_ffi as O
+    lam_tab = np.geomspace(0.05, 5000.0, 80)
+    n, k = M.synthetic_lnk(lam_tab, 0.03)
+    (tmp_path / "syn.lnk").write_text("".join("%g %g %g\n" % t for t in zip(lam_tab, n, k)))
+    (tmp_path / "dust.particle").write_text("2\n3\n'syn.lnk'\n1.0 3.0\n")
+    deck = tmp_path / "disk.in"
+    deck.write_text("""* a passive disk
+tstar=10000
+rstar=2.5
+startype='PLANCK'
+rin=0.5
+rout=100
+nrad=12
+ntheta=8
+lam1=0.1
+lam2=3000
+nlam=20
+denstype='ZONES'
+zone1:rin=0.5
+zone1:rout=100
+zone1:mdust=1d-5
+zone1:denspow=1
+zone1:sh=0.0707
+zone1:rsh=1
+zone1:shpow=1.125
+scattype='FULL'
+computepart01:file='dust.particle'
+amin=0.1
+computepart01:amax=1.0
+computepart01:ngrains=3
+computepart01:fmax=0.8
+computepart01:porosity=0.25
+randomwalk=.true.
+factrw=5
+idum=-7
+""")
+
+    def oracle_parts(parts):
+        return [O.compute_part(p["lam"], p["e1"][0], p["e2"][0], p["frac"], p["rho"], p["amin"], p["amax"],
+                               p["apow"], p["fmax"], p["blend"], p["porosity"], p["ns"], p["nf"]) for p in parts]
+
+    m, run = M.deck_model(None, str(deck), overrides=["maxinteract=20000"], compute_parts=oracle_parts)
+    assert (m.nr, m.nt, m.nlam, m.ncomp, m.scat_how) == (13, 9, 20, 3, 2)
+    assert run == dict(seed=7, randomwalk=True, factRW=5.0, maxinteract=20000, nruns=1)
+    assert np.allclose(m.comp_w.sum(1), 1.0)
+    ref = M.disk_model(None, nrad=12, ntheta=8, nlam=20, lam2=3000.0, mdust=1e-5, sh=0.0707, ngrains=3,
+                       opacities=(m.Kabs, m.Ksca, m.F))
+    for key in ("R", "Theta", "dens", "V", "comp_w", "lam", "BB", "Fstar"):
+        assert np.allclose(getattr(m, key), getattr(ref, key), rtol=1e-12, atol=0), key
+    assert abs(m.Lstar / ref.Lstar - 1) < 1e-12
+    with pytest.raises(ValueError):
+        M.deck_model(None, str(deck), overrides=["scattype='RAYLEIGH'"], compute_parts=oracle_parts)
