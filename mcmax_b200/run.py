@@ -1,0 +1,78 @@
+"""Command-line run of the packet loop on an MCMax input deck, writing the
+reference's result files:
+
+    python -m mcmax_b200.run input.in Nphot [-o outdir] [-s key=value]...
+                             [--precision mixed|fp64|exact] [--opacity dhs|surrogate]
+
+The arguments follow the reference's command line (Main.f:60-72 for -o,
+Init.f:462-478 for -s): the deck, the packet count, an output directory
+(created if missing) and keyword overrides applied after the deck.  One
+pass of MCRadiation with the deck's run keywords (randomwalk, factrw,
+maxinteract, nruns, idum), the post-Monte-Carlo temperatures
+(Main.f:498-549), then denstemp.dat (format 5, InputOutput.f:6-227) and
+the MCSpec<angle>.dat files (MCRadiation.f:738-762) in the output
+directory.  --opacity surrogate serves the grain bins inside the network's
+training box from the committed surrogate weights."""
+import argparse
+import os
+import sys
+
+from . import model as M
+from . import outputs
+
+
+def _surrogate_parts(ctx):
+    from . import surrogate as S
+    params, _ = S.load(os.path.join(os.path.dirname(__file__), "data", "surrogate_nf20.npz"))
+    return lambda parts: S.compute_part_surrogate(ctx, parts, params)[0]
+
+
+def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opacity="dhs", compute_parts=None):
+    """Build the deck's model, run the packet loop and write the result
+    files; returns dict(model, run, nphot, result, T, files)."""
+    if compute_parts is None and opacity == "surrogate":
+        compute_parts = _surrogate_parts(ctx)
+    elif opacity not in ("dhs", "surrogate"):
+        raise ValueError("opacity: 'dhs' or 'surrogate'")
+    m, run = M.deck_model(ctx, deck, overrides, compute_parts=compute_parts)
+    ctx.set_model(m)
+    n, res = ctx.mcradiation(int(nphot), precision=precision, **run)
+    T, dT, dE = ctx.finalize_t()
+    os.makedirs(outdir, exist_ok=True)
+    files = [os.path.join(outdir, "denstemp.dat")]
+    outputs.write_denstemp(files[0], m, T)
+    names = outputs.write_mcspec(outdir, m, res, distance_pc=m.distance)
+    files += [os.path.join(outdir, x) for x in names + ["MCSpec.dat"]]
+    return dict(model=m, run=run, nphot=n, result=res, T=T, files=files)
+
+
+def parse_args(argv):
+    ap = argparse.ArgumentParser(prog="python -m mcmax_b200.run", description=__doc__.split("\n\n")[0])
+    ap.add_argument("deck")
+    ap.add_argument("nphot", type=lambda s: int(float(s)))
+    ap.add_argument("-o", dest="outdir", default=".")
+    ap.add_argument("-s", dest="overrides", action="append", default=[], metavar="key=value")
+    ap.add_argument("--precision", choices=("mixed", "fp64", "exact"), default="mixed")
+    ap.add_argument("--opacity", choices=("dhs", "surrogate"), default="dhs")
+    ap.add_argument("--device", type=int, default=0)
+    return ap.parse_args(argv)
+
+
+def main(argv=None, context=None):
+    a = parse_args(sys.argv[1:] if argv is None else argv)
+    if context is None:
+        from .api import Context
+        context = Context
+    ctx = context(a.device)
+    try:
+        r = run_deck(ctx, a.deck, a.nphot, a.outdir, a.overrides, a.precision, a.opacity)
+    finally:
+        ctx.close()
+    print("packets %d, %d cells, T %.1f-%.1f K, wrote %s" % (r["nphot"], r["T"].size, r["T"].min(), r["T"].max(),
+                                                             ", ".join(os.path.basename(f) for f in r["files"][:2])
+                                                             + ", ..."))
+    return r
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,107 @@
+"""The command-line runner's wiring on CPU: deck keywords reach the packet
+loop's run parameters, the result files are written and read back.  The
+context is a stand-in that records the calls; the transport itself is
+covered by the GPU tests."""
+import os
+
+import numpy as np
+
+import oracle_ffi as O
+from mcmax_b200 import model as M
+from mcmax_b200 import outputs, run as R
+
+DECK = """tstar=5000
+rstar=2
+rin=1
+rout=50
+nrad=6
+ntheta=6
+lam1=0.2
+lam2=1000
+nlam=12
+zone1:rin=1
+zone1:rout=50
+zone1:mdust=1d-6
+scattype='ISOTROPIC'
+computepart01:file='dust.particle'
+computepart01:amin=0.1
+computepart01:amax=0.5
+computepart01:ngrains=2
+maxinteract=5000
+nruns=2
+idum=-11
+"""
+
+
+def _oracle_parts(parts):
+    return [O.compute_part(p["lam"], p["e1"][0], p["e2"][0], p["frac"], p["rho"], p["amin"], p["amax"],
+                           p["apow"], p["fmax"], p["blend"], p["porosity"], p["ns"], p["nf"]) for p in parts]
+
+
+class FakeContext:
+    def __init__(self, device=0):
+        self.calls = []
+        self.closed = False
+
+    def compute_part_batch(self, parts):
+        return _oracle_parts(parts)
+
+    def set_model(self, m):
+        self.model = m
+
+    def mcradiation(self, nphot, **run):
+        self.calls.append(dict(nphot=nphot, **run))
+        m = self.model
+        rng = np.random.default_rng(0)
+        ns = (m.nlam, 31)
+        return nphot, dict(spec=rng.uniform(1e20, 1e21, ns), scatspec=np.zeros(ns),
+                           ispec=rng.integers(1, 100, ns).astype(np.int32))
+
+    def finalize_t(self):
+        T = np.linspace(20.0, 900.0, self.model.ncell)
+        return T, 0 * T, 0 * T
+
+    def close(self):
+        self.closed = True
+
+
+def _write_inputs(d):
+    lam_tab = np.geomspace(0.05, 5000.0, 60)
+    n, k = M.synthetic_lnk(lam_tab, 0.03)
+    (d / "syn.lnk").write_text("".join("%g %g %g\n" % t for t in zip(lam_tab, n, k)))
+    (d / "dust.particle").write_text("1\n1\n'syn.lnk'\n1.0 3.0\n")
+    (d / "disk.in").write_text(DECK)
+    return str(d / "disk.in")
+
+
+def test_command_line_runs_the_deck_and_writes_result_files(tmp_path):
+    deck = _write_inputs(tmp_path)
+    out = tmp_path / "out"
+    made = []
+
+    def factory(device):
+        made.append(FakeContext(device))
+        return made[-1]
+
+    r = R.main([deck, "2e4", "-o", str(out), "-s", "randomwalk=.true.", "-s", "factrw=4",
+                "--precision", "fp64"], context=factory)
+    ctx = made[0]
+    assert ctx.closed
+    assert ctx.calls == [dict(nphot=20000, precision="fp64", seed=11, randomwalk=True, factRW=4.0,
+                              maxinteract=5000, nruns=2)]
+    assert len(r["files"]) == 32 and all(os.path.exists(f) for f in r["files"])
+    d = outputs.read_denstemp(str(out / "denstemp.dat"))
+    m = r["model"]
+    assert d["T"].shape == (m.nr - 1, m.nt - 1)
+    assert np.allclose(d["T"].ravel(), r["T"].reshape(m.nr, m.nt - 1)[1:].ravel(), rtol=1e-15)
+    assert np.allclose(d["dens"].ravel(), m.dens.reshape(m.nr, m.nt - 1)[1:].ravel(), rtol=1e-15)
+    assert np.allclose(d["comp"].sum(-1), 1.0)
+    # isotropic scattering: the phase matrices are unit, sizes from the deck
+    assert m.scat_how == 1 and m.bins[0][0] == 0.1 and abs(m.bins[-1][1] - 0.5) < 1e-12
+
+
+def test_command_line_arguments():
+    a = R.parse_args(["x.in", "1e6"])
+    assert (a.nphot, a.outdir, a.overrides, a.precision, a.opacity) == (1000000, ".", [], "mixed", "dhs")
+    a = R.parse_args(["x.in", "300", "-o", "o", "-s", "a=1", "-s", "b=2", "--opacity", "surrogate"])
+    assert (a.nphot, a.outdir, a.overrides, a.opacity) == (300, "o", ["a=1", "b=2"], "surrogate")
