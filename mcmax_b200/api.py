@@ -14,6 +14,7 @@ Both go through libmcmax_gpu.so (include/mcmax_gpu.h); errors raise McgError
 with the library's message, the counterpart of the reference's `stop`.
 """
 import ctypes as C
+import math
 import os
 
 import numpy as np
@@ -243,15 +244,22 @@ class Particle:
         self.rho = np.zeros(nopac)
         self.mscale = np.ones(nopac)
         self.rscale = np.ones(nopac)
+        self.rv = np.zeros(nopac)
         self.counters = [None] * nopac
 
 
 def ComputePart(ctx, p, ii, input, amin, amax, apow, fmax, blend, porosity, inp_abun, iopac,
-                normalize_abun, standard, nsubgrains, lam):
+                normalize_abun, standard, nsubgrains, lam, particledir=None, abun_in_name=0):
     """ComputePart.f:1 for standard='FILE': `input` is a particle file (ns,
     nf, then per material an .lnk path and 'frac rho').  iopac is 1-based as
-    in the reference.  `lam` is the wavelength grid (module global there)."""
+    in the reference.  `lam` is the wavelength grid (module global there).
+
+    particledir (the reference's `dirparticle`, a module global there):
+    when given, a cached particleNNNN.fits(.gz) made for the same grain
+    (ComputePart.f:160-205) is read instead of computing, and a computed
+    bin is written as particle<ii>.fits.gz (ComputePart.f:529)."""
     from .model import read_particle_file, readrefind
+    from . import particle_fits as PF
     if standard != "FILE":
         raise McgError(_ffi.MCG_ERR_ARG, "standard=%r: only 'FILE' particle files are supported" % standard)
     ns, nf, mats = read_particle_file(input)
@@ -264,10 +272,21 @@ def ComputePart(ctx, p, ii, input, amin, amax, apow, fmax, blend, porosity, inp_
         e2.append(k_)
         frac.append(fr)
         rho.append(rh)
+    io = iopac - 1
+    lnkfiles = [m[0] for m in mats]
+    if particledir is not None:
+        hit = PF.find_particle_file(particledir, ii, amin, amax, apow, ns, fmax, blend, porosity, frac, rho,
+                                    lnkfiles, iopac, abun_in_name)
+        if hit is not None:
+            res = PF.read_particle_fits(hit, lam)
+            p.Kabs[io], p.Ksca[io], p.Kext[io], p.F[io] = res["kabs"], res["ksca"], res["kext"], res["F"]
+            p.rho[io] = res["rho_av"]
+            p.rv[io] = res["rv"]
+            p.counters[io] = None
+            return p
     res = ctx.compute_part_batch([dict(lam=lam, e1=np.array(e1), e2=np.array(e2), frac=frac, rho=rho,
                                        amin=amin, amax=amax, apow=apow, fmax=fmax, porosity=porosity,
                                        blend=blend, ns=ns, nf=nf, normalize_abun=normalize_abun)])[0]
-    io = iopac - 1
     p.Kabs[io] = res["kabs"]
     p.Ksca[io] = res["ksca"]
     p.Kext[io] = res["kext"]
@@ -276,6 +295,11 @@ def ComputePart(ctx, p, ii, input, amin, amax, apow, fmax, blend, porosity, inp_
     p.mscale[io] = res["mscale"]
     p.rscale[io] = res["rscale"]
     p.counters[io] = (res["n_dhs"], res["n_mie"], res["n_dhs_fail"])
+    p.rv[io] = math.sqrt(PF.dust_moments(amin, amax, apow, ns)[1]) * 1e-4
+    if particledir is not None:
+        fr = np.asarray(frac, float) / np.sum(frac)
+        PF.write_particle_fits(PF.particle_file_name(particledir, ii, iopac, fr, abun_in_name), lam, res, amin, amax,
+                               apow, fmax, blend, porosity, frac, rho, lnkfiles, ns)
     return p
 
 
