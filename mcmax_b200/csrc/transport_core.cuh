@@ -48,7 +48,10 @@
 
 #define TP_TMAX 10000
 #define TP_TT (TP_TMAX + 1)
-#define TP_AU 1.49598e13
+/* the reference declares AU real*8 but gives it a default-real literal,
+ * parameter(AU=1.49598e13) (Modules.f:4,8): its value is the single-precision
+ * number nearest 1.49598e13, widened */
+#define TP_AU ((double)1.49598e13f)
 #define TP_PI 3.14159265358979323846
 #define TP_NY 1000
 #define TP_NANG 30

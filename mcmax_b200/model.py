@@ -26,10 +26,13 @@ import numpy as np
 from . import api
 from ._ffi import TT, NANG
 
-AU = 1.49598e13
-RSUN = 6.9599e10
-MSUN = 1.98892e33
-LSUN = 3.846e33
+# Modules.f:4-10 declares these real*8 but writes them as default-real
+# (single-precision) literals, so the reference computes with the float
+# nearest each decimal value, widened to double
+AU = float(np.float32(1.49598e13))
+RSUN = float(np.float32(6.9599e10))
+MSUN = float(np.float32(1.98892e33))
+LSUN = float(np.float32(3.846e33))
 CLIGHT_MICRON = 2.9979e14
 
 

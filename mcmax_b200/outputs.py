@@ -22,7 +22,8 @@ import numpy as np
 
 from . import model as M
 
-PARSEC = 3.08568025e18
+# single-precision literal widened to real*8, as Modules.f:9 holds it
+PARSEC = float(np.float32(3.08568025e18))
 
 
 def _r_av_cm(R):

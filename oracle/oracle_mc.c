@@ -43,7 +43,9 @@
 #include "../mcmax_b200/csrc/detmath.h"
 #include "../mcmax_b200/csrc/philox.h"
 
-#define AU_CM 1.49598e13
+/* AU as the reference holds it: a single-precision literal widened to
+ * real*8 (Modules.f:4,8) */
+#define AU_CM ((double)1.49598e13f)
 #define PI_D 3.14159265358979323846
 #define NY_RW 1000
 

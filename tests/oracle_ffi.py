@@ -11,6 +11,7 @@ ORACLE_DIR = os.path.join(ROOT, "oracle")
 ORACLE_LIB = os.path.join(ORACLE_DIR, "liboracle_mcmax.so")
 TMAX = 10000
 TT = TMAX + 1
+AU = float(np.float32(1.49598e13))   # Modules.f:8, a single-precision literal
 dp = C.POINTER(C.c_double)
 ip = C.POINTER(C.c_int32)
 u8p = C.POINTER(C.c_uint8)
@@ -199,7 +200,7 @@ def transport_tables(model, randomwalk=False, factRW=10.0, lazy_kd=False):
                                  P(KDext[c]), P(KDabs[c]))
             if i >= 1:
                 for iT in (100, 600, 1100, 1600):
-                    lr = 1.0 / ((1.49598e13 * KDext[c, iT]) * dens[c])
+                    lr = 1.0 / ((AU * KDext[c, iT]) * dens[c])
                     if (m.R[i + 1] - m.R[i]) > factRW * lr:
                         thick[c] = 1
         out.update(KDext=KDext, KDabs=KDabs, thick=thick)

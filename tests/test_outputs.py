@@ -6,6 +6,7 @@ import os
 import numpy as np
 
 import models
+from mcmax_b200 import model as M
 from mcmax_b200 import outputs as OUT
 
 
@@ -23,7 +24,7 @@ def test_denstemp_round_trip(tmp_path):
     assert np.array_equal(d["comp"], m.comp_w.reshape(nr, nc, m.ncomp)[1:])
     assert np.allclose(d["gasdens"], 100.0 * d["dens0"], rtol=1e-15)
     assert np.all(np.diff(d["r_av"]) > 0) and np.all(np.diff(d["theta_av"]) > 0)
-    assert abs(d["r_av"][0] / 1.49598e13 - math.sqrt(m.R[1] * m.R[2])) < 1e-9 * d["r_av"][0] / 1.49598e13
+    assert abs(d["r_av"][0] / M.AU - math.sqrt(m.R[1] * m.R[2])) < 1e-9 * d["r_av"][0] / M.AU
 
 
 def test_mcspec_names_and_columns(tmp_path):
