@@ -23,7 +23,8 @@
  *                in the reference.
  *
  *   mcg_finalize_t replaces the temperature step that follows the call
- *   (Main.f:498-549: EJv/V, EJv2/V^2, determineT, dEJv, dT).
+ *   (Main.f:498-549: EJv/V, EJv2/V^2, determineT, dEJv, dT), and
+ *   mcg_diffuse the diffusion step after it (Diffuse, Diffusion.f:9).
  *
  * Layout conventions (all arrays are plain host pointers, row-major):
  *   cells      (i,j), i = 0..nr-1 (i = 0 is the star-to-Rin cell),
@@ -267,6 +268,24 @@ mcg_status mcg_mcradiation_batch(mcg_ctx *ctx, int nmodels, const int *model_ids
 /* Temperatures from the last run (Main.f:498-549): T, dT, dEJv per cell
  * (any may be NULL).  Uses EJv/V and EJv2/V^2 of the last mcg_mcradiation. */
 mcg_status mcg_finalize_t(mcg_ctx *ctx, double *T, double *dT, double *dEJv);
+
+/* Diffuse (Diffusion.f:9-330, called as Diffuse(NPhotDiffuse, dTDiffuse)
+ * from Main.f:561-563 after the temperature step): cells with fewer than
+ * nphotmin packets or a relative error dT/T above dtmax that are optically
+ * thick (or saw at most one packet) take their temperature from the
+ * diffusion equation for T^4 over them and their neighbours, three passes.
+ * The reference's defaults are nphotmin = 25, dtmax = 1 (Init.f:140-141).
+ * Thick flags are InitRandomWalk's test with factRW (RandomWalk.f:172-190);
+ * the clearing of Diffusion.f:136 applies inside this call only.
+ * Ni, dT: per cell, from mcg_mcradiation and mcg_finalize_t of the current
+ * model; T: in/out (the temperatures of mcg_finalize_t); EJv: out, may be
+ * NULL, written only for the cells given a diffusion temperature (the
+ * Planck-mean emission sum w*wopac*Kp(iT) the reference stores in C%EJv).
+ * ncells (may be NULL): [0] cells selected, [1] unknowns of the system,
+ * [2] cells solved in the last pass, [3] passes whose elimination met a zero
+ * pivot (their temperatures are kept, as after DGESV's INFO > 0). */
+mcg_status mcg_diffuse(mcg_ctx *ctx, int32_t nphotmin, double dtmax, double factRW, const int32_t *Ni,
+                       const double *dT, double *T, double *EJv, int32_t *ncells);
 
 /* ----------------------------------------------------------------------
  * Opacity-surrogate network.  No counterpart in the reference: it stands in

@@ -107,6 +107,8 @@ SIGNATURES = {
     "mcg_set_model": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Opacity)]),
     "mcg_mcradiation": (C.c_int, [C.c_void_p, C.POINTER(Run), C.POINTER(C.c_int64), C.POINTER(Result)]),
     "mcg_finalize_t": (C.c_int, [C.c_void_p, dp, dp, dp]),
+    "mcg_diffuse": (C.c_int, [C.c_void_p, C.c_int32, C.c_double, C.c_double, C.POINTER(C.c_int32), dp, dp, dp,
+                              C.POINTER(C.c_int32)]),
     "mcg_add_model": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Opacity), C.POINTER(C.c_int)]),
     "mcg_mcradiation_batch": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(Run),
                                         C.POINTER(C.c_int64), C.POINTER(Result), C.POINTER(BatchOpts)]),

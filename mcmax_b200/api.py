@@ -213,6 +213,22 @@ class Context:
         self._check(self.lib.mcg_finalize_t(self.h, _ffi.ptr(T), _ffi.ptr(dT), _ffi.ptr(dE)))
         return T, dT, dE
 
+    def diffuse(self, Ni, dT, T, nphotmin=25, dtmax=1.0, factRW=10.0):
+        """mcg_diffuse on the current model: returns (T, EJv, counts) with
+        EJv NaN where no diffusion temperature was given and counts =
+        (selected, unknowns, solved in the last pass, failed passes)."""
+        nc = self.model.ncell
+        Ni = np.ascontiguousarray(Ni, dtype=np.int32).reshape(-1)
+        dT = _f64(dT).reshape(-1)
+        T = np.array(T, dtype=np.float64).reshape(-1)
+        if Ni.size != nc or dT.size != nc or T.size != nc:
+            raise McgError(_ffi.MCG_ERR_ARG, "diffuse: Ni, dT and T need one value per cell (%d)" % nc)
+        EJv = np.full(nc, np.nan)
+        counts = np.zeros(4, np.int32)
+        self._check(self.lib.mcg_diffuse(self.h, int(nphotmin), float(dtmax), float(factRW), _ffi.ptr(Ni),
+                                         _ffi.ptr(dT), _ffi.ptr(T), _ffi.ptr(EJv), _ffi.ptr(counts)))
+        return T, EJv, tuple(int(x) for x in counts)
+
 
 def bb_table(lam):
     """Planck table BB[l, iT] (Init.f:2616-2622) built by the library."""
@@ -314,6 +330,20 @@ def MCRadiation(ctx, model, NphotTot, niter=1, dofastvisc=False, **run):
     for k, v in out.items():
         setattr(model, k, v)
     return n
+
+
+def Diffuse(ctx, model, NPhotMin=25, dTMax=1.0, factRW=10.0):
+    """Diffusion.f:9 after MCRadiation on `model`: the post-MC temperatures
+    (Main.f:498-549), then the diffusion step for the thick cells that too
+    few packets reached (defaults NphotDiffuse = 25, dTDiffuse = 1,
+    Init.f:140-141).  Stores T, dT and the diffused cells' EJv on the model;
+    returns (selected, unknowns, solved, failed passes)."""
+    if getattr(ctx, "model", None) is not model:
+        raise McgError(_ffi.MCG_ERR_STATE, "Diffuse: run MCRadiation on this model first")
+    T, dT, _ = ctx.finalize_t()
+    T, EJv, counts = ctx.diffuse(model.Ni, dT, T, NPhotMin, dTMax, factRW)
+    model.T, model.dT, model.EJvDiffuse = T, dT, EJv
+    return counts
 
 
 # ---------------------------------------------------------------- surrogate network

@@ -24,9 +24,10 @@ UNITS = {
     "host_tables.cu": ["--fmad=false"],
     "transport_fast.cu": [],
     "mlp_kernels.cu": [],
+    "diffuse.cu": ["--fmad=false"],
 }
 HEADERS = ["detmath.h", "cplx.h", "philox.h", "dhs_core.cuh", "transport_core.cuh", "transport_fast.cuh",
-           "mcg_internal.h", "tc_sm100.cuh"]
+           "mcg_internal.h", "tc_sm100.cuh", "diffuse_core.cuh"]
 
 
 def _nvcc():

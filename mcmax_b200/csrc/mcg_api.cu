@@ -117,4 +117,11 @@ mcg_status mcg_finalize_t(mcg_ctx *ctx, double *T, double *dT, double *dEJv) {
   return mcg_finalize_impl(ctx, T, dT, dEJv);
 }
 
+mcg_status mcg_diffuse(mcg_ctx *ctx, int32_t nphotmin, double dtmax, double factRW, const int32_t *Ni,
+                       const double *dT, double *T, double *EJv, int32_t *ncells) {
+  if (!ctx) return MCG_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  return mcg_diffuse_impl(ctx, nphotmin, dtmax, factRW, Ni, dT, T, EJv, ncells);
+}
+
 }  // extern "C"

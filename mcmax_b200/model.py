@@ -504,7 +504,8 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
     porosity, norm_abun, standard ('FILE'), with amin, amax, apow (micron)
     as the deck-wide defaults; abunNN (relative mass of computepart entry
     NN); fixmpset, alphaturb (settling of a one-zone
-    disk); randomwalk, factrw, maxinteract, nruns, idum.  A value that
+    disk); randomwalk, factrw, maxinteract, nruns, idum; nphotdiffuse,
+    dtdiffuse (the diffusion step after the run).  A value that
     selects physics outside the packet loop (another startype or denstype,
     scattype RAYLEIGH, tcontact false) raises ValueError.
 
@@ -512,7 +513,8 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
     after the file (the -s switches).  compute_parts(parts) returns the
     ComputePart results of a list of grain bins (default: the library's
     DHS kernels, ctx.compute_part_batch).  Returns (model, run) with run =
-    dict(seed, randomwalk, factRW, maxinteract, nruns) for mcradiation."""
+    dict(seed, randomwalk, factRW, maxinteract, nruns) for mcradiation plus
+    nphotdiffuse, dtdiffuse (defaults 25 and 1, Init.f:140-141)."""
     base = "."
     if os.path.exists(str(deck)):
         base = os.path.dirname(os.path.abspath(deck))
@@ -622,7 +624,8 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
               Ksca=Ksca, F=F, BB=BB, Fstar=Fstar, Lstar=Lstar, Tstar=tstar, Rstar_cm=rstar_cm, scat_how=scat,
               bins=[(p["amin"], p["amax"]) for p in parts], w=w0, distance=v("distance", 100.0))
     run = dict(seed=abs(v("idum", -42, int)), randomwalk=v("randomwalk", False, bool), factRW=v("factrw", 10.0),
-               maxinteract=v("maxinteract", 1000000, int), nruns=v("nruns", 1, int))
+               maxinteract=v("maxinteract", 1000000, int), nruns=v("nruns", 1, int),
+               nphotdiffuse=v("nphotdiffuse", 25, int), dtdiffuse=v("dtdiffuse", 1.0))
     return m, run
 
 

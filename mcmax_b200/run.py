@@ -9,7 +9,9 @@ Init.f:462-478 for -s): the deck, the packet count, an output directory
 (created if missing) and keyword overrides applied after the deck.  One
 pass of MCRadiation with the deck's run keywords (randomwalk, factrw,
 maxinteract, nruns, idum), the post-Monte-Carlo temperatures
-(Main.f:498-549), then denstemp.dat (format 5, InputOutput.f:6-227) and
+(Main.f:498-549), the diffusion step for poorly sampled thick cells when
+nphotdiffuse > 0 or dtdiffuse < 1 (Main.f:561-563, on by default), then
+denstemp.dat (format 5, InputOutput.f:6-227) and
 the MCSpec<angle>.dat files (MCRadiation.f:738-762) in the output
 directory.  --opacity surrogate serves the grain bins inside the network's
 training box from the committed surrogate weights."""
@@ -28,22 +30,27 @@ def _surrogate_parts(ctx):
 
 
 def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opacity="dhs", compute_parts=None):
-    """Build the deck's model, run the packet loop and write the result
-    files; returns dict(model, run, nphot, result, T, files)."""
+    """Build the deck's model, run the packet loop and the diffusion step
+    and write the result files; returns dict(model, run, nphot, result, T,
+    diffused (the counts of mcg_diffuse, or None), files)."""
     if compute_parts is None and opacity == "surrogate":
         compute_parts = _surrogate_parts(ctx)
     elif opacity not in ("dhs", "surrogate"):
         raise ValueError("opacity: 'dhs' or 'surrogate'")
     m, run = M.deck_model(ctx, deck, overrides, compute_parts=compute_parts)
     ctx.set_model(m)
-    n, res = ctx.mcradiation(int(nphot), precision=precision, **run)
+    rad = {k: run[k] for k in ("seed", "randomwalk", "factRW", "maxinteract", "nruns")}
+    n, res = ctx.mcradiation(int(nphot), precision=precision, **rad)
     T, dT, dE = ctx.finalize_t()
+    diffused = None
+    if run["nphotdiffuse"] > 0 or run["dtdiffuse"] < 1.0:
+        T, _, diffused = ctx.diffuse(res["Ni"], dT, T, run["nphotdiffuse"], run["dtdiffuse"], run["factRW"])
     os.makedirs(outdir, exist_ok=True)
     files = [os.path.join(outdir, "denstemp.dat")]
     outputs.write_denstemp(files[0], m, T)
     names = outputs.write_mcspec(outdir, m, res, distance_pc=m.distance)
     files += [os.path.join(outdir, x) for x in names + ["MCSpec.dat"]]
-    return dict(model=m, run=run, nphot=n, result=res, T=T, files=files)
+    return dict(model=m, run=run, nphot=n, result=res, T=T, diffused=diffused, files=files)
 
 
 def parse_args(argv):

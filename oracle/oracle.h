@@ -154,6 +154,17 @@ double orc_determine_t(const double *kp, double E1, double Tcur);
 /* Bjorkman-Wood upward scan, Radiation.f:537-562 */
 double orc_increase_t(const double *kp, double E1, double Tcur);
 
+/* Diffuse (Diffusion.f:9-330) on the dense system with DGESV's elimination.
+ * KDext: ncell*(TMAX+1) DiffCoeffCell tables (orc_diffcoeff_cell); KpCell as
+ * in orc_model; thick: InitRandomWalk flags, cleared in place as
+ * Diffusion.f:136 does; T in/out; EJv written for the solved cells.
+ * stats: [0] cells selected, [1] unknowns, [2] cells solved in the last pass,
+ * [3] passes whose DGESV returned INFO > 0. */
+int orc_diffuse(int nr, int nt, const double *R, const double *Theta, const double *dens, int ncomp,
+                const double *comp_w, const double *KDext, const double *KpCell, int kp_uniform, uint8_t *thick,
+                int nphotmin, double dtmax, const int32_t *Ni, const double *dT, double *T, double *EJv,
+                int *stats);
+
 /* ran1 (Numerical Recipes minimal standard + shuffle), Subroutines.f:1481-1509 */
 double orc_ran1(int32_t *idum, int32_t *iv, int32_t *iy);
 

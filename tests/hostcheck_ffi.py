@@ -12,7 +12,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "native", "hostcheck.cpp")
 LIB = os.path.join(HERE, "native", "libhostcheck.so")
 DEPS = [SRC] + [os.path.join(HERE, "..", "mcmax_b200", "csrc", f) for f in
-                ("dhs_core.cuh", "transport_core.cuh", "transport_fast.cuh", "detmath.h", "cplx.h", "philox.h")]
+                ("dhs_core.cuh", "transport_core.cuh", "transport_fast.cuh", "diffuse_core.cuh", "detmath.h", "cplx.h",
+                 "philox.h")]
 
 
 class HcModel(C.Structure):
@@ -97,3 +98,36 @@ def mcradiation(model, tables, nphot, seed=1, randomwalk=False, factRW=10.0, max
     for k in ("spec", "scatspec", "ispec"):
         out[k] = out[k].reshape(m.nlam, 31)
     return out
+
+
+class HcDiffuseTables(C.Structure):
+    _fields_ = [("nlam", C.c_int), ("ncomp", C.c_int), ("scattering", C.c_int), ("uniform_mix", C.c_int)] + \
+               [(n, dp) for n in ("comp_w", "g_c", "Ksca_c", "KabsTot", "KscaTot", "nu", "BB", "KpCell")]
+
+
+def diffuse(model, tables, Ni, dT, T, nphotmin=25, dtmax=1.0, factRW=10.0):
+    """the host logic of mcg_diffuse with serial loops in place of its
+    kernels; returns (T, EJv, stats [selected, unknowns, solved, failed
+    passes, box rows, half-bandwidth])"""
+    L = load()
+    m = model
+    arrs = [np.ascontiguousarray(a, float) for a in (m.comp_w, tables["g"], m.Ksca, tables["KabsTot"],
+                                                     tables["KscaTot"], m.nu, m.BB, tables["KpCell"])]
+    scattering = int(m.scat_how != 0 and np.any(np.asarray(tables["KscaTot"]) != 0))
+    t = HcDiffuseTables(m.nlam, m.ncomp, scattering, int(tables["kp_uniform"]), *[P(a) for a in arrs])
+    T = np.array(T, float)
+    EJv = np.full(m.ncell, np.nan)
+    stats = np.zeros(6, np.int32)
+    geo = [np.ascontiguousarray(a, float) for a in (m.R, m.Theta, m.dens)]
+    L.hc_diffuse(m.nr, m.nt, P(geo[0]), P(geo[1]), P(geo[2]), C.byref(t), int(nphotmin), C.c_double(dtmax),
+                 C.c_double(factRW), P(np.ascontiguousarray(Ni, np.int32)), P(np.ascontiguousarray(dT, float)), P(T),
+                 P(EJv), P(stats))
+    return T, EJv, stats
+
+
+def band_solve(nb, w, coef, rhs):
+    L = load()
+    x = np.zeros(nb)
+    code = L.hc_band_solve(int(nb), int(w), P(np.ascontiguousarray(coef, float)), P(np.ascontiguousarray(rhs, float)),
+                           P(x))
+    return code, x

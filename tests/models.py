@@ -12,7 +12,7 @@ def small_disk(nrad=20, ntheta=12, nlam=30, ngrains=3, ns=2, nf=4, mdust=1e-5, s
                amin=0.1, amax=1.0, tstar=10000.0, rstar=2.5, rin=0.5, rout=100.0, blend=True, porosity=0.25,
                fmax=0.8, cache={}):
     key = (nrad, ntheta, nlam, ngrains, ns, nf, mdust, scat_how, lam2, kpref, amin, amax, tstar, rstar, rin, rout,
-           blend, porosity, fmax)
+           blend, porosity, fmax, M.AU, M.RSUN, M.MSUN)
     if key in cache:
         return cache[key]
     import hashlib

@@ -9,6 +9,7 @@
 
 #include "../../mcmax_b200/csrc/dhs_core.cuh"
 #include "../../mcmax_b200/csrc/transport_core.cuh"
+#include "../../mcmax_b200/csrc/diffuse_core.cuh"
 
 extern "C" {
 
@@ -294,4 +295,58 @@ extern "C" int hc_fast(const HcModel *h, int mixed, double *EJv, double *EJv2, d
                        double *spec, unsigned long long *counters, double *tautot, int64_t first, int64_t count) {
   if (mixed) return hc_fast_impl<float>(h, EJv, EJv2, Eabs, T, Ni, spec, counters, tautot, first, count);
   return hc_fast_impl<double>(h, EJv, EJv2, Eabs, T, Ni, spec, counters, tautot, first, count);
+}
+
+/* Diffuse on the host: the host logic of mcg_diffuse with a backend of
+ * serial loops over the kernels' per-element functions */
+struct HcDiffuseTables {
+  int nlam, ncomp, scattering, uniform_mix;
+  const double *comp_w, *g_c, *Ksca_c, *KabsTot, *KscaTot, *nu, *BB, *KpCell;
+};
+
+struct HostDiffuseBackend {
+  const HcDiffuseTables *t;
+  std::vector<double> dnu_half;
+  bool kd(int n, const int *cells, const int *iTs, double *out) {
+    for (int k = 0; k < n; ++k)
+      out[k] = df_kd_ext(cells[k], iTs[k], t->nlam, t->ncomp, t->scattering, t->comp_w, t->g_c, t->Ksca_c,
+                         t->KabsTot, t->KscaTot, dnu_half.data(), t->BB);
+    return true;
+  }
+  bool kp(int n, const int *cells, const int *iTs, double *out) {
+    for (int k = 0; k < n; ++k) out[k] = t->KpCell[(t->uniform_mix ? (size_t)0 : (size_t)cells[k] * DF_TT) + iTs[k]];
+    return true;
+  }
+  bool solve(int nb, int w, const double *coef, const double *rhs, double *x, int *code) {
+    *code = df_band_solve_host(nb, w, coef, rhs, x);
+    return true;
+  }
+};
+
+extern "C" int hc_diffuse(int nr, int nt, const double *R, const double *Theta, const double *dens_in,
+                          const HcDiffuseTables *t, int nphotmin, double dtmax, double factRW, const int *Ni,
+                          const double *dT, double *T, double *EJv, int *stats) {
+  const int ncell = nr * (nt - 1);
+  std::vector<double> dens(ncell);
+  for (int c = 0; c < ncell; ++c) dens[c] = dens_in[c] <= 1e-50 ? 1e-50 : dens_in[c];
+  HostDiffuseBackend be;
+  be.t = t;
+  be.dnu_half.resize(t->nlam > 1 ? t->nlam - 1 : 1);
+  for (int i = 0; i < t->nlam - 1; ++i) be.dnu_half[i] = std::fabs(t->nu[i] - t->nu[i + 1]) * 0.5;
+  DfGrid g{nr, nt, R, Theta, dens.data(), t->ncomp, t->comp_w};
+  DfStats st;
+  df_diffuse(g, be, nphotmin, dtmax, factRW, (const int32_t *)Ni, dT, T, EJv, &st);
+  stats[0] = st.ncor;
+  stats[1] = st.nunknown;
+  stats[2] = st.nsolved;
+  stats[3] = st.failed;
+  stats[4] = st.nb;
+  stats[5] = st.w;
+  return 0;
+}
+
+/* the band solve alone: coef nb*5 stencil slots, rhs nb -> x nb; returns
+ * 0 or 1 + the first step with a zero or non-finite pivot */
+extern "C" int hc_band_solve(int nb, int w, const double *coef, const double *rhs, double *x) {
+  return df_band_solve_host(nb, w, coef, rhs, x);
 }

@@ -240,3 +240,21 @@ def mcradiation(model, nphot, seed=1, randomwalk=False, factRW=10.0, maxinteract
     for k in ("spec", "scatspec", "ispec"):
         out[k] = out[k].reshape(m.nlam, 31)
     return out
+
+
+def diffuse(model, tables, Ni, dT, T, nphotmin=25, dtmax=1.0):
+    """orc_diffuse on (Ni, dT, T); tables from transport_tables(model,
+    randomwalk=True) (KDext, thick).  Returns (T, EJv, thick, stats)."""
+    L = load()
+    m = model
+    T = np.array(T, float)
+    EJv = np.full(m.ncell, np.nan)
+    thick = np.array(tables["thick"], np.uint8)
+    stats = np.zeros(4, np.int32)
+    Ni = np.ascontiguousarray(Ni, np.int32)
+    dT = np.ascontiguousarray(dT, float)
+    keep = [np.ascontiguousarray(a, float) for a in (m.R, m.Theta, m.dens, m.comp_w)]
+    L.orc_diffuse(m.nr, m.nt, P(keep[0]), P(keep[1]), P(keep[2]), m.ncomp, P(keep[3]), P(tables["KDext"]),
+                  P(tables["KpCell"]), int(tables["kp_uniform"]), P(thick), int(nphotmin), C.c_double(dtmax),
+                  P(Ni), P(dT), P(T), P(EJv), P(stats))
+    return T, EJv, thick, stats

@@ -152,7 +152,8 @@ idum=-7
 
     m, run = M.deck_model(None, str(deck), overrides=["maxinteract=20000"], compute_parts=oracle_parts)
     assert (m.nr, m.nt, m.nlam, m.ncomp, m.scat_how) == (13, 9, 20, 3, 2)
-    assert run == dict(seed=7, randomwalk=True, factRW=5.0, maxinteract=20000, nruns=1)
+    assert run == dict(seed=7, randomwalk=True, factRW=5.0, maxinteract=20000, nruns=1, nphotdiffuse=25,
+                       dtdiffuse=1.0)
     assert np.allclose(m.comp_w.sum(1), 1.0)
     ref = M.disk_model(None, nrad=12, ntheta=8, nlam=20, lam2=3000.0, mdust=1e-5, sh=0.0707, ngrains=3,
                        opacities=(m.Kabs, m.Ksca, m.F))

@@ -55,7 +55,13 @@ class FakeContext:
         rng = np.random.default_rng(0)
         ns = (m.nlam, 31)
         return nphot, dict(spec=rng.uniform(1e20, 1e21, ns), scatspec=np.zeros(ns),
-                           ispec=rng.integers(1, 100, ns).astype(np.int32))
+                           ispec=rng.integers(1, 100, ns).astype(np.int32), Ni=np.full(m.ncell, 7, np.int32))
+
+    def diffuse(self, Ni, dT, T, nphotmin, dtmax, factRW):
+        self.diffuse_args = (int(Ni[0]), nphotmin, dtmax, factRW)
+        T = np.array(T)
+        T[-1] = 555.0
+        return T, np.full(T.size, np.nan), (1, 5, 1, 0)
 
     def finalize_t(self):
         T = np.linspace(20.0, 900.0, self.model.ncell)
@@ -89,6 +95,7 @@ def test_command_line_runs_the_deck_and_writes_result_files(tmp_path):
     assert ctx.closed
     assert ctx.calls == [dict(nphot=20000, precision="fp64", seed=11, randomwalk=True, factRW=4.0,
                               maxinteract=5000, nruns=2)]
+    assert ctx.diffuse_args == (7, 25, 1.0, 4.0) and r["diffused"] == (1, 5, 1, 0)
     assert len(r["files"]) == 32 and all(os.path.exists(f) for f in r["files"])
     d = outputs.read_denstemp(str(out / "denstemp.dat"))
     m = r["model"]
