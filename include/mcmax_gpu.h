@@ -287,6 +287,39 @@ mcg_status mcg_finalize_t(mcg_ctx *ctx, double *T, double *dT, double *dEJv);
 mcg_status mcg_diffuse(mcg_ctx *ctx, int32_t nphotmin, double dtmax, double factRW, const int32_t *Ni,
                        const double *dT, double *T, double *EJv, int32_t *ncells);
 
+/* Vertical structure (DiskStructure, DiskStructure.f:85-468, with
+ * CheckMinimumDensity and CheckCells): per ring and species (gas, then each
+ * grain) the density along theta from hydrostatic equilibrium in the
+ * temperatures Temp (the TempAverage of DiskStructure.f:25, >= 2.7 K), by the
+ * reference's adaptive Cash-Karp integration (Subroutines.f:1933-2090),
+ * renormalised to the species' mass in the ring; rings inside a zone with a
+ * fixed structure keep the zone's analytic profile.  Then every cell's dust
+ * and gas densities and abundances are rebuilt from the profiles.  All
+ * grains have the 'DISK' scale-height type; no radiation pressure, gaps or
+ * halo.  Cell arrays in the cell order above, w and w0 with ngrains values
+ * per cell (C%w, C%w0), all in/out: dens (C%dens), dens0 (C%dens0, the
+ * condensable total), gasdens (C%gasdens, in dust-density units). */
+typedef struct {
+  double rin, rout;               /* AU */
+  double sh, rsh, shpow, denspow; /* Zone(iz)%sh, Rsh, shpow, denspow */
+  int32_t fix_struct;             /* 1: the zone keeps its analytic structure */
+} mcg_zone;
+
+typedef struct {
+  int32_t nr, nt, ngrains;        /* D%nR, D%nTheta, grains */
+  const double *R;                /* nr+1 radial edges, AU */
+  const double *Theta;            /* nt cos(theta) edges */
+  const double *V;                /* cell volumes, nr*(nt-1) */
+  double Mstar;                   /* stellar mass, g */
+  int32_t nzones;
+  const mcg_zone *zones;
+  const double *shscale;          /* nr scale-height factors per ring, or NULL (1) */
+  const double *grain_scale;      /* ngrains*nr settling factors Grain(ii)%shscale(i), or NULL */
+} mcg_structure;
+
+mcg_status mcg_disk_structure(mcg_ctx *ctx, const mcg_structure *s, const double *Temp, double *dens, double *dens0,
+                              double *gasdens, double *w, double *w0);
+
 /* ----------------------------------------------------------------------
  * Opacity-surrogate network.  No counterpart in the reference: it stands in
  * for ComputePart's coated-sphere inner loop (ComputePart.f:318-447) inside

@@ -41,6 +41,18 @@ class PartOut(C.Structure):
     ]
 
 
+class Zone(C.Structure):
+    _fields_ = [("rin", C.c_double), ("rout", C.c_double), ("sh", C.c_double), ("rsh", C.c_double),
+                ("shpow", C.c_double), ("denspow", C.c_double), ("fix_struct", C.c_int32)]
+
+
+class Structure(C.Structure):
+    _fields_ = [("nr", C.c_int32), ("nt", C.c_int32), ("ngrains", C.c_int32), ("R", C.POINTER(C.c_double)),
+                ("Theta", C.POINTER(C.c_double)), ("V", C.POINTER(C.c_double)), ("Mstar", C.c_double),
+                ("nzones", C.c_int32), ("zones", C.POINTER(Zone)), ("shscale", C.POINTER(C.c_double)),
+                ("grain_scale", C.POINTER(C.c_double))]
+
+
 class Grid(C.Structure):
     _fields_ = [
         ("nr", C.c_int), ("nt", C.c_int), ("R", dp), ("Theta", dp), ("SinTheta", dp),
@@ -107,6 +119,7 @@ SIGNATURES = {
     "mcg_set_model": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Opacity)]),
     "mcg_mcradiation": (C.c_int, [C.c_void_p, C.POINTER(Run), C.POINTER(C.c_int64), C.POINTER(Result)]),
     "mcg_finalize_t": (C.c_int, [C.c_void_p, dp, dp, dp]),
+    "mcg_disk_structure": (C.c_int, [C.c_void_p, C.POINTER(Structure), dp, dp, dp, dp, dp, dp]),
     "mcg_diffuse": (C.c_int, [C.c_void_p, C.c_int32, C.c_double, C.c_double, C.POINTER(C.c_int32), dp, dp, dp,
                               C.POINTER(C.c_int32)]),
     "mcg_add_model": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Opacity), C.POINTER(C.c_int)]),

@@ -213,6 +213,30 @@ class Context:
         self._check(self.lib.mcg_finalize_t(self.h, _ffi.ptr(T), _ffi.ptr(dT), _ffi.ptr(dE)))
         return T, dT, dE
 
+    def disk_structure(self, R, Theta, V, Mstar, zones, Temp, dens, dens0, gasdens, w, w0, shscale=None,
+                       grain_scale=None):
+        """mcg_disk_structure: zones is a list of (rin, rout, sh, rsh, shpow,
+        denspow, fix_struct); cell arrays in the library's cell order, w and
+        w0 (ncell, ngrains).  Returns the new (dens, dens0, gasdens, w, w0)."""
+        R, Theta, V, Temp = _f64(R), _f64(Theta), _f64(V), _f64(Temp)
+        nr, nt = R.size - 1, Theta.size
+        ncell = nr * (nt - 1)
+        out = [np.array(a, dtype=np.float64) for a in (dens, dens0, gasdens, w, w0)]
+        ng = out[3].size // ncell
+        if any(a.size != ncell for a in out[:3]) or out[3].size != ncell * ng or out[4].size != ncell * ng or \
+                V.size != ncell or Temp.size != ncell:
+            raise McgError(_ffi.MCG_ERR_ARG, "disk_structure: cell arrays need %d cells" % ncell)
+        zs = (_ffi.Zone * max(len(zones), 1))()
+        for k, z in enumerate(zones):
+            zs[k] = _ffi.Zone(*[float(x) for x in z[:6]], int(bool(z[6])))
+        keep = [None if a is None else _f64(a) for a in (shscale, grain_scale)]
+        st = _ffi.Structure(nr, nt, ng, _ffi.ptr(R), _ffi.ptr(Theta), _ffi.ptr(V), float(Mstar), len(zones), zs,
+                            _ffi.ptr(keep[0]), _ffi.ptr(keep[1]))
+        self._check(self.lib.mcg_disk_structure(self.h, C.byref(st), _ffi.ptr(Temp), *[_ffi.ptr(a) for a in out]))
+        out[3] = out[3].reshape(ncell, ng)
+        out[4] = out[4].reshape(ncell, ng)
+        return tuple(out)
+
     def diffuse(self, Ni, dT, T, nphotmin=25, dtmax=1.0, factRW=10.0):
         """mcg_diffuse on the current model: returns (T, EJv, counts) with
         EJv NaN where no diffusion temperature was given and counts =

@@ -25,9 +25,11 @@ UNITS = {
     "transport_fast.cu": [],
     "mlp_kernels.cu": [],
     "diffuse.cu": ["--fmad=false"],
+    "dstruct.cu": ["--fmad=false"],
 }
 HEADERS = ["detmath.h", "cplx.h", "philox.h", "dhs_core.cuh", "transport_core.cuh", "transport_fast.cuh",
-           "mcg_internal.h", "tc_sm100.cuh", "diffuse_core.cuh"]
+           "mcg_internal.h", "tc_sm100.cuh", "diffuse_core.cuh",
+           "dstruct_core.cuh"]
 
 
 def _nvcc():

@@ -117,6 +117,13 @@ mcg_status mcg_finalize_t(mcg_ctx *ctx, double *T, double *dT, double *dEJv) {
   return mcg_finalize_impl(ctx, T, dT, dEJv);
 }
 
+mcg_status mcg_disk_structure(mcg_ctx *ctx, const mcg_structure *s, const double *Temp, double *dens, double *dens0,
+                              double *gasdens, double *w, double *w0) {
+  if (!ctx) return MCG_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  return mcg_disk_structure_impl(ctx, s, Temp, dens, dens0, gasdens, w, w0);
+}
+
 mcg_status mcg_diffuse(mcg_ctx *ctx, int32_t nphotmin, double dtmax, double factRW, const int32_t *Ni,
                        const double *dT, double *T, double *EJv, int32_t *ncells) {
   if (!ctx) return MCG_ERR_ARG;

@@ -505,7 +505,8 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
     as the deck-wide defaults; abunNN (relative mass of computepart entry
     NN); fixmpset, alphaturb (settling of a one-zone
     disk); randomwalk, factrw, maxinteract, nruns, idum; nphotdiffuse,
-    dtdiffuse (the diffusion step after the run).  A value that
+    dtdiffuse (the diffusion step after the run); zoneN:fix, mstar,
+    maxiter, epsiter (structure iterations).  A value that
     selects physics outside the packet loop (another startype or denstype,
     scattype RAYLEIGH, tcontact false) raises ValueError.
 
@@ -514,7 +515,9 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
     ComputePart results of a list of grain bins (default: the library's
     DHS kernels, ctx.compute_part_batch).  Returns (model, run) with run =
     dict(seed, randomwalk, factRW, maxinteract, nruns) for mcradiation plus
-    nphotdiffuse, dtdiffuse (defaults 25 and 1, Init.f:140-141)."""
+    nphotdiffuse, dtdiffuse (defaults 25 and 1, Init.f:140-141) and the
+    structure-iteration inputs zones (rin, rout, sh, rsh, shpow, denspow,
+    fix), Mstar [g], maxiter, epsiter (defaults 10 and 3, Init.f:113-114)."""
     base = "."
     if os.path.exists(str(deck)):
         base = os.path.dirname(os.path.abspath(deck))
@@ -547,7 +550,7 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
             continue
         zones.append(dict(rin=v(kz + "rin", rin), rout=v(kz + "rout", rout), mdust=v(kz + "mdust", 1e-5),
                           denspow=v(kz + "denspow", 1.0), sh=v(kz + "sh", 0.01), rsh=v(kz + "rsh", 1.0),
-                          shpow=v(kz + "shpow", 1.1)))
+                          shpow=v(kz + "shpow", 1.1), fix=v(kz + "fix", False, bool)))
     if not zones:
         raise ValueError("no zoneN:* keywords")
     # grain bins of every computepart entry (Init.f:746-789, 1323-1420)
@@ -625,7 +628,9 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
               bins=[(p["amin"], p["amax"]) for p in parts], w=w0, distance=v("distance", 100.0))
     run = dict(seed=abs(v("idum", -42, int)), randomwalk=v("randomwalk", False, bool), factRW=v("factrw", 10.0),
                maxinteract=v("maxinteract", 1000000, int), nruns=v("nruns", 1, int),
-               nphotdiffuse=v("nphotdiffuse", 25, int), dtdiffuse=v("dtdiffuse", 1.0))
+               nphotdiffuse=v("nphotdiffuse", 25, int), dtdiffuse=v("dtdiffuse", 1.0),
+               zones=[(z["rin"], z["rout"], z["sh"], z["rsh"], z["shpow"], z["denspow"], z["fix"]) for z in zones],
+               Mstar=v("mstar", 2.5) * MSUN, maxiter=v("maxiter", 10, int), epsiter=v("epsiter", 3.0))
     return m, run
 
 

@@ -10,7 +10,10 @@ Init.f:462-478 for -s): the deck, the packet count, an output directory
 pass of MCRadiation with the deck's run keywords (randomwalk, factrw,
 maxinteract, nruns, idum), the post-Monte-Carlo temperatures
 (Main.f:498-549), the diffusion step for poorly sampled thick cells when
-nphotdiffuse > 0 or dtdiffuse < 1 (Main.f:561-563, on by default), then
+nphotdiffuse > 0 or dtdiffuse < 1 (Main.f:561-563, on by default); when a
+zone has no fixed structure (zoneN:fix, false by default) these passes
+repeat with the hydrostatic vertical structure rebuilt in between
+(mcmax_b200.structure) until the temperatures converge; then
 denstemp.dat (format 5, InputOutput.f:6-227) and
 the MCSpec<angle>.dat files (MCRadiation.f:738-762) in the output
 directory.  --opacity surrogate serves the grain bins inside the network's
@@ -38,19 +41,27 @@ def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opac
     elif opacity not in ("dhs", "surrogate"):
         raise ValueError("opacity: 'dhs' or 'surrogate'")
     m, run = M.deck_model(ctx, deck, overrides, compute_parts=compute_parts)
-    ctx.set_model(m)
     rad = {k: run[k] for k in ("seed", "randomwalk", "factRW", "maxinteract", "nruns")}
-    n, res = ctx.mcradiation(int(nphot), precision=precision, **rad)
-    T, dT, dE = ctx.finalize_t()
-    diffused = None
-    if run["nphotdiffuse"] > 0 or run["dtdiffuse"] < 1.0:
-        T, _, diffused = ctx.diffuse(res["Ni"], dT, T, run["nphotdiffuse"], run["dtdiffuse"], run["factRW"])
+    diffused = structure = None
+    if any(not z[6] for z in run["zones"]):
+        # a zone without a fixed structure: structure iterations (Init.f:1519)
+        from . import structure as S
+        structure = S.iterate(ctx, m, run["zones"], run["Mstar"], nphot, run=rad, maxiter=run["maxiter"],
+                              epsiter=run["epsiter"], nphotdiffuse=run["nphotdiffuse"], dtdiffuse=run["dtdiffuse"],
+                              precision=precision)
+        T, n, res = structure["T"], structure["nphot"], structure["result"]
+    else:
+        ctx.set_model(m)
+        n, res = ctx.mcradiation(int(nphot), precision=precision, **rad)
+        T, dT, dE = ctx.finalize_t()
+        if run["nphotdiffuse"] > 0 or run["dtdiffuse"] < 1.0:
+            T, _, diffused = ctx.diffuse(res["Ni"], dT, T, run["nphotdiffuse"], run["dtdiffuse"], run["factRW"])
     os.makedirs(outdir, exist_ok=True)
     files = [os.path.join(outdir, "denstemp.dat")]
     outputs.write_denstemp(files[0], m, T)
     names = outputs.write_mcspec(outdir, m, res, distance_pc=m.distance)
     files += [os.path.join(outdir, x) for x in names + ["MCSpec.dat"]]
-    return dict(model=m, run=run, nphot=n, result=res, T=T, diffused=diffused, files=files)
+    return dict(model=m, run=run, nphot=n, result=res, T=T, diffused=diffused, structure=structure, files=files)
 
 
 def parse_args(argv):

@@ -165,6 +165,15 @@ int orc_diffuse(int nr, int nt, const double *R, const double *Theta, const doub
                 int nphotmin, double dtmax, const int32_t *Ni, const double *dT, double *T, double *EJv,
                 int *stats);
 
+/* DiskStructure (DiskStructure.f:85-468) for 'DISK' grains with
+ * CheckMinimumDensity and CheckCells.  zones: 7 values per zone (rin, rout
+ * [AU], sh, rsh, shpow, denspow, fix_struct as 0/1); shscale (nR) and
+ * grain_scale (ng*nR) may be NULL.  Cell arrays in/out as mcg_disk_structure. */
+int orc_disk_structure(int nR, int nTheta, int ng, const double *R, const double *Theta, const double *V,
+                       double Mstar, int nzones, const double *zones, const double *shscale,
+                       const double *grain_scale, const double *Temp, double *dens, double *dens0, double *gasdens,
+                       double *w, double *w0);
+
 /* ran1 (Numerical Recipes minimal standard + shuffle), Subroutines.f:1481-1509 */
 double orc_ran1(int32_t *idum, int32_t *iv, int32_t *iy);
 

@@ -12,8 +12,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "native", "hostcheck.cpp")
 LIB = os.path.join(HERE, "native", "libhostcheck.so")
 DEPS = [SRC] + [os.path.join(HERE, "..", "mcmax_b200", "csrc", f) for f in
-                ("dhs_core.cuh", "transport_core.cuh", "transport_fast.cuh", "diffuse_core.cuh", "detmath.h", "cplx.h",
-                 "philox.h")]
+                ("dhs_core.cuh", "transport_core.cuh", "transport_fast.cuh", "diffuse_core.cuh", "dstruct_core.cuh",
+                 "detmath.h", "cplx.h", "philox.h")]
 
 
 class HcModel(C.Structure):
@@ -131,3 +131,23 @@ def band_solve(nb, w, coef, rhs):
     code = L.hc_band_solve(int(nb), int(w), P(np.ascontiguousarray(coef, float)), P(np.ascontiguousarray(rhs, float)),
                            P(x))
     return code, x
+
+
+def _structure_call(fn, st, Temp, dens, dens0, gasdens, w, w0):
+    """st: dict(nr, nt, ng, R, Theta, V, Mstar, zones [(rin, rout, sh, rsh,
+    shpow, denspow, fix)], shscale, grain_scale).  Returns the updated
+    (dens, dens0, gasdens, w, w0)."""
+    out = [np.array(a, dtype=np.float64) for a in (dens, dens0, gasdens, w, w0)]
+    zones = np.ascontiguousarray(np.array(st.get("zones", []), dtype=np.float64).reshape(-1))
+    arrs = [np.ascontiguousarray(st[k], float) for k in ("R", "Theta", "V")]
+    sh = None if st.get("shscale") is None else np.ascontiguousarray(st["shscale"], float)
+    gs = None if st.get("grain_scale") is None else np.ascontiguousarray(st["grain_scale"], float)
+    rc = fn(int(st["nr"]), int(st["nt"]), int(st["ng"]), P(arrs[0]), P(arrs[1]), P(arrs[2]), C.c_double(st["Mstar"]),
+            len(st.get("zones", [])), P(zones) if zones.size else None, P(sh), P(gs),
+            P(np.ascontiguousarray(Temp, float)), *[P(a) for a in out])
+    assert rc == 0
+    return tuple(out)
+
+
+def disk_structure(st, Temp, dens, dens0, gasdens, w, w0):
+    return _structure_call(load().hc_disk_structure, st, Temp, dens, dens0, gasdens, w, w0)

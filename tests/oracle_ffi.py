@@ -258,3 +258,9 @@ def diffuse(model, tables, Ni, dT, T, nphotmin=25, dtmax=1.0):
                   P(tables["KpCell"]), int(tables["kp_uniform"]), P(thick), int(nphotmin), C.c_double(dtmax),
                   P(Ni), P(dT), P(T), P(EJv), P(stats))
     return T, EJv, thick, stats
+
+
+def disk_structure(st, Temp, dens, dens0, gasdens, w, w0):
+    """orc_disk_structure; arguments as hostcheck_ffi.disk_structure"""
+    import hostcheck_ffi as H
+    return H._structure_call(load().orc_disk_structure, st, Temp, dens, dens0, gasdens, w, w0)

@@ -1,0 +1,226 @@
+"""The vertical structure step (DiskStructure, DiskStructure.f:85-468) on
+CPU: the host logic of mcg_disk_structure with its kernels replaced by
+serial loops over the same per-column and per-cell functions
+(tests/native/hostcheck.cpp) against the oracle's restatement in the
+reference's loop order (oracle/oracle_dstruct.c), bit for bit, and against
+closed forms of hydrostatic equilibrium."""
+import math
+
+import numpy as np
+import pytest
+
+import hostcheck_ffi as H
+import models
+import oracle_ffi as O
+from mcmax_b200 import model as M
+
+MU, G, KB = float(np.float32(2.3)) * 1.67262158e-24, 6.67300e-8, 1.3806503e-16
+SH = 0.05 * math.sqrt(2.0)
+
+
+@pytest.fixture(scope="module")
+def disk():
+    m = models.small_disk(nrad=20, ntheta=14, nlam=16, mdust=1e-4, ngrains=2)
+    dens = np.maximum(m.dens, 1e-50)
+    state = dict(dens=dens.copy(), dens0=dens.copy(), gasdens=dens.copy(), w=m.comp_w.copy(), w0=m.comp_w.copy())
+    return m, state
+
+
+def _st(m, zones, **kw):
+    d = dict(nr=m.nr, nt=m.nt, ng=m.ncomp, R=m.R, Theta=m.Theta, V=m.V, Mstar=2.5 * M.MSUN, zones=zones)
+    d.update(kw)
+    return d
+
+
+def _temp(m, vertical=0.5):
+    nc = m.nt - 1
+    R_av = np.sqrt(m.R[:-1] * m.R[1:])
+    return np.maximum((300.0 * R_av[:, None] ** -0.5 * (1 + vertical * np.linspace(1, 0, nc))[None, :]).ravel(), 2.7)
+
+
+def _run(fn, st, T, s):
+    return dict(zip(("dens", "dens0", "gasdens", "w", "w0"),
+                    fn(st, T, s["dens"], s["dens0"], s["gasdens"], s["w"], s["w0"])))
+
+
+def _geometry(m):
+    nc = m.nt - 1
+    R_av = M.AU * 10 ** ((np.log10(m.R[:-1]) + np.log10(m.R[1:])) / 2)
+    th = np.arccos((m.Theta[:-1] + m.Theta[1:]) / 2)
+    return R_av, th, nc
+
+
+@pytest.mark.parametrize("fix", [0, 1])
+def test_replay_matches_oracle_and_keeps_ring_masses(disk, fix):
+    m, s = disk
+    st = _st(m, [(0.5, 100.0, SH, 1.0, 1.125, 1.0, fix)])
+    T = _temp(m)
+    o = _run(O.disk_structure, st, T, s)
+    h = _run(H.disk_structure, st, T, s)
+    for k in o:
+        assert np.array_equal(o[k], h[k]), k
+    nc = m.nt - 1
+    V = m.V.reshape(m.nr, nc)
+    for name, new, old in (("gas", h["gasdens"], s["gasdens"]), ("condensable", h["dens0"], s["dens0"])):
+        r = (new.reshape(m.nr, nc) * V).sum(1)[1:] / (old.reshape(m.nr, nc) * V).sum(1)[1:]
+        assert np.allclose(r, 1.0, rtol=1e-12, atol=0), name
+    assert np.allclose(h["w"].reshape(-1, m.ncomp).sum(1), 1.0, rtol=1e-12)
+
+
+def test_isothermal_column_is_gaussian(disk):
+    """constant T: ln rho = -mu G M z^2 / (2 k T R^3) + const"""
+    m, s = disk
+    st = _st(m, [(0.5, 100.0, SH, 1.0, 1.125, 1.0, 0)])
+    T = np.full(m.ncell, 3000.0)
+    h = _run(H.disk_structure, st, T, s)
+    R_av, th, nc = _geometry(m)
+    gas = h["gasdens"].reshape(m.nr, nc)
+    for i in (8, 15, 19):
+        z = R_av[i] * np.cos(th)
+        lnr = -MU * G * st["Mstar"] * z ** 2 / (2 * KB * 3000.0 * R_av[i] ** 3)
+        got = np.log(gas[i] / gas[i, -1])
+        ok = gas[i] > 1e-45
+        assert ok.sum() >= 3
+        err = np.abs(got[ok] - (lnr[ok] - lnr[-1]))
+        assert np.all(err < 1e-5 * np.maximum(1.0, np.abs(lnr[ok]))), (i, err)
+
+
+def test_settling_factor_narrows_a_grain(disk):
+    """a grain with scale-height factor f follows the gas profile with z/f"""
+    m, s = disk
+    gs = np.ones((m.ncomp, m.nr))
+    gs[1] = 0.5
+    st = _st(m, [(0.5, 100.0, SH, 1.0, 1.125, 1.0, 0)], grain_scale=gs)
+    T = np.full(m.ncell, 3000.0)
+    o = _run(O.disk_structure, st, T, s)
+    h = _run(H.disk_structure, st, T, s)
+    for k in o:
+        assert np.array_equal(o[k], h[k]), k
+    R_av, th, nc = _geometry(m)
+    i = 19
+    z = R_av[i] * np.cos(th)
+    d1 = (h["dens0"] * h["w0"][:, 1]).reshape(m.nr, nc)[i]
+    lnr = -MU * G * st["Mstar"] * z ** 2 / (2 * KB * 3000.0 * R_av[i] ** 3 * 0.25)
+    ok = d1 > 1e-45
+    assert ok.sum() >= 2
+    got = np.log(d1[ok] / d1[-1])
+    assert np.all(np.abs(got - (lnr[ok] - lnr[-1])) < 1e-5 * np.maximum(1.0, np.abs(lnr[ok])))
+
+
+def test_fixed_zone_profile(disk):
+    """a fixed-structure zone keeps rho ~ r^-p / h exp(-(z/h)^2), h = sh (r/Rsh)^q,
+    renormalised per ring (DiskStructure.f:360-386)"""
+    m, s = disk
+    st = _st(m, [(0.5, 100.0, SH, 1.0, 1.125, 1.0, 1)])
+    h = _run(H.disk_structure, st, _temp(m), s)
+    R_av, th, nc = _geometry(m)
+    i = 10
+    rr = R_av[i] * np.sin(th) / M.AU
+    zz = R_av[i] * np.cos(th) / M.AU
+    hr = SH * rr ** 1.125
+    prof = rr ** -1.0 / hr * np.exp(-(zz / hr) ** 2 * (np.arange(nc) != nc - 1))
+    prof = prof / (prof * m.V.reshape(m.nr, nc)[i]).sum()
+    got = h["gasdens"].reshape(m.nr, nc)[i]
+    got = got / (got * m.V.reshape(m.nr, nc)[i]).sum()
+    big = prof > 1e-40
+    assert np.allclose(got[big], prof[big], rtol=1e-12)
+
+
+def test_wedge_zone_and_ring_factors(disk):
+    m, s = disk
+    shs = np.linspace(0.8, 1.2, m.nr)
+    st = _st(m, [(0.5, 10.0, -30.0, 1.0, 1.0, 1.0, 1), (10.0, 100.0, SH, 1.0, 1.125, 1.0, 0)], shscale=shs)
+    T = _temp(m)
+    o = _run(O.disk_structure, st, T, s)
+    h = _run(H.disk_structure, st, T, s)
+    for k in o:
+        assert np.array_equal(o[k], h[k]), k
+    R_av, th, nc = _geometry(m)
+    inner = np.nonzero((R_av > 0.5 * M.AU) & (R_av < 10 * M.AU))[0][1]
+    g = h["gasdens"].reshape(m.nr, nc)[inner]
+    open_ = 180 * th[:-1] / np.pi > 30.0
+    assert np.allclose(g[:-1][open_], g[-1], rtol=1e-12)
+    assert np.all(g[:-1][~open_] < 1e-20 * g[-1])
+
+
+# ---------------------------------------------------------------- the iteration driver
+from mcmax_b200 import structure as S  # noqa: E402
+
+
+def test_temp_average_and_compare_cells():
+    T0 = np.array([10.0, 2.0, 5.0])
+    assert np.array_equal(S.temp_average(None, T0, 0.5), T0)
+    assert np.allclose(S.temp_average(T0, [20.0, 1.0, 5.0], 0.5), [15.0, 2.35, 5.0])
+    nr, nt = 3, 3          # 3 rings x 2 theta cells; ring 0 is left out
+    T1 = np.array([1, 1, 10, 10, 20, 20.0])
+    T2 = np.array([1, 1, 12, 10, 20, 23.0])
+    dT = np.ones(6)
+    dT2 = dT.copy()
+    dT2[5] = 0.0           # no error estimate: cell left out
+    err = S.compare_cells(T1, dT, T2, dT2, nr, nt)
+    assert abs(err - (4.0 / 2.0) / (2 * 2 - 1)) < 1e-15
+
+
+class _FakeRun:
+    """packet loop stand-in: the temperatures it returns are set by the
+    test; the structure step is the host replay of mcg_disk_structure"""
+
+    def __init__(self, temps):
+        self.temps = list(temps)
+        self.calls = dict(mc=0, ds=0, diffuse=0)
+        self.dens_seen = []
+
+    def set_model(self, m):
+        self.model = m
+        self.dens_seen.append(np.array(m.dens))
+
+    def mcradiation(self, nphot, **kw):
+        self.calls["mc"] += 1
+        return nphot, dict(Ni=np.full(self.model.ncell, 1000, np.int32))
+
+    def finalize_t(self):
+        T = self.temps[min(self.calls["mc"], len(self.temps)) - 1]
+        return T.copy(), np.ones_like(T), np.zeros_like(T)
+
+    def diffuse(self, Ni, dT, T, nphotmin, dtmax, factRW):
+        self.calls["diffuse"] += 1
+        return T, None, (0, 0, 0, 0)
+
+    def disk_structure(self, R, Theta, V, Mstar, zones, Temp, dens, dens0, gasdens, w, w0, shscale=None,
+                       grain_scale=None):
+        self.calls["ds"] += 1
+        st = dict(nr=R.size - 1, nt=Theta.size, ng=np.asarray(w).shape[1], R=R, Theta=Theta, V=V, Mstar=Mstar,
+                  zones=zones, shscale=shscale, grain_scale=grain_scale)
+        out = H.disk_structure(st, Temp, dens, dens0, gasdens, np.ravel(w), np.ravel(w0))
+        ncell = np.asarray(dens).size
+        return out[0], out[1], out[2], out[3].reshape(ncell, -1), out[4].reshape(ncell, -1)
+
+
+def _driver_model():
+    m = models.small_disk(nrad=20, ntheta=14, nlam=16, mdust=1e-4, ngrains=2)
+    return M.Model(**dict(m.__dict__, dens=np.maximum(m.dens, 1e-50).copy(), comp_w=m.comp_w.copy()))
+
+
+def test_iterations_stop_after_two_agreeing_passes():
+    m = _driver_model()
+    T = _temp(m)
+    fake = _FakeRun([T])
+    zones = [(0.5, 100.0, SH, 1.0, 1.125, 1.0, 0)]
+    r = S.iterate(fake, m, zones, 2.5 * M.MSUN, 1000)
+    # pass 1 has no previous temperatures (errT 0), pass 2 agrees, then one last run
+    assert [h["niter"] for h in r["history"]] == [1, 2]
+    assert fake.calls == dict(mc=3, ds=2, diffuse=3)
+    assert not np.array_equal(fake.dens_seen[1], fake.dens_seen[0])
+    assert np.array_equal(m.dens, r["state"]["dens"])
+
+
+def test_iterations_stop_at_maxiter():
+    m = _driver_model()
+    T = _temp(m)
+    fake = _FakeRun([T, T + 10.0, T, T + 10.0, T, T + 10.0])
+    r = S.iterate(fake, m, [(0.5, 100.0, SH, 1.0, 1.125, 1.0, 0)], 2.5 * M.MSUN, 1000, maxiter=3)
+    assert [h["niter"] for h in r["history"]] == [1, 2, 3, 4]
+    assert all(h["errT"] > 3.0 for h in r["history"][1:])
+    assert fake.calls["mc"] == 5 and fake.calls["ds"] == 4
+    # the structure temperature averages the passes with weight f_weight = 0.5
+    assert np.allclose(r["Temp"], 0.5 * (0.5 * (0.5 * T + 0.5 * (T + 10)) + 0.5 * T) + 0.5 * (T + 10), rtol=1e-12)

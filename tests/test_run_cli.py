@@ -22,6 +22,7 @@ nlam=12
 zone1:rin=1
 zone1:rout=50
 zone1:mdust=1d-6
+zone1:fix=.true.
 scattype='ISOTROPIC'
 computepart01:file='dust.particle'
 computepart01:amin=0.1
