@@ -341,6 +341,110 @@ def grain_bins(amin, amax, ngrains):
 
 
 # ---------------------------------------------------------------- model
+def luminosity(T, R):
+    """Luminosity of a blackbody sphere, T [K], R [cm] (Subroutines.f:24-35,
+    with its constants; pi there is a single-precision literal)"""
+    k, c, h = 1.3807e-16, 2.9979e10, 6.6261e-27
+    pi = float(np.float32(3.1415926536))
+    p4, k4 = (pi * pi) * (pi * pi), (k * k) * (k * k)
+    return (((((2.0 * p4) * k4) / ((15.0 * ((h * h) * h)) * (c * c))) * ((T * T) * (T * T))) * pi) * (R * R)
+
+
+def _read_pairs(path):
+    xs, ys = [], []
+    with open(path) as f:
+        for line in f:
+            parts = line.replace("d", "e").replace("D", "E").split()
+            if len(parts) < 2:
+                continue
+            try:
+                x, y = float(parts[0]), float(parts[1])
+            except ValueError:
+                continue
+            xs.append(x)
+            ys.append(y)
+    return np.array(xs), np.array(ys)
+
+
+def read_star(path, grid):
+    """A stellar spectrum file (wavelength [micron], flux; one pair per
+    line) on the wavelength grid (readstar, Subroutines.f:130-216): the
+    file's points inside a grid bin (edges at the geometric midpoints) are
+    averaged with weights |d(1/lambda)|; bins without a point take the
+    log-log interpolation of readstar_interpol (Subroutines.f:219-258), and
+    points beyond the file fall off as lambda^-2 from its last point.
+
+    The bin edges are the reference's: its last assignment puts the upper
+    edge of bin n-1 at grid(n)^2 / edge(n-1) and leaves the upper edge of
+    bin n unset, zero under its -finit-local-zero build, so bin n-1 reaches
+    up to grid(n) times the half-step and bin n always interpolates."""
+    grid = np.asarray(grid, float)
+    n = grid.size
+    if n < 3:
+        raise ValueError("read_star: at least three wavelengths")
+    xe = np.empty(n + 1)
+    xe[1:n] = np.sqrt(grid[:-1] * grid[1:])
+    xe[0] = grid[0] ** 2 / xe[1]
+    xe[n - 1] = grid[n - 1] ** 2 / xe[n - 2]
+    xe[n] = 0.0
+    ls, Fs = _read_pairs(path)
+    nls = ls.size
+    if nls < 3:
+        raise ValueError("%s: fewer than three points" % path)
+    dls = np.empty(nls)
+    dls[1:-1] = (1.0 / ls[:-2] - 1.0 / ls[2:]) / 2.0
+    dls[0], dls[-1] = dls[1], dls[-2]
+    y, tot = np.zeros(n), np.zeros(n)
+    done = np.zeros(n, bool)
+    j = 0
+    for i in range(nls):
+        while True:
+            if ls[i] < xe[j]:
+                break
+            if ls[i] > xe[j + 1]:
+                j += 1
+                if j >= n:
+                    break
+                continue
+            y[j] = y[j] + Fs[i] * dls[i]
+            tot[j] = tot[j] + dls[i]
+            done[j] = True
+            break
+        if j >= n:
+            break
+    y[done] = y[done] / tot[done]
+    if not done.all():
+        y[~done] = _star_interpol(ls, Fs, grid[~done])
+    return y
+
+
+def _star_interpol(ls, Fs, grid):
+    """readstar_interpol (Subroutines.f:219-258) on the grid points given"""
+    n = grid.size
+    y = np.zeros(n)
+    i = 0
+    x0, y0 = ls[0], Fs[0]
+    while i < n and x0 >= grid[i]:
+        y[i] = y0
+        i += 1
+    x1, y1 = x0, y0
+    for k in range(1, ls.size):
+        x1, y1 = ls[k], Fs[k]
+        while i < n and x0 < grid[i] <= x1:
+            if y1 > 1e-60 and y0 > 1e-60:
+                y[i] = 10.0 ** (math.log10(y1) + (math.log10(grid[i]) - math.log10(x1)) *
+                                (math.log10(y0) - math.log10(y1)) / (math.log10(x0) - math.log10(x1)))
+            else:
+                y[i] = y1 + (grid[i] - x1) * (y0 - y1) / (x0 - x1)
+            i += 1
+        if i >= n:
+            return y
+        x0, y0 = x1, y1
+    for j in range(i, n):
+        y[j] = y1 * x1 ** 2 / grid[j] ** 2
+    return y
+
+
 def integrate(nu, spec):
     """Trapezoid over frequency in the reference's order (Radiation.f:1-18)."""
     L = 0.0
@@ -496,7 +600,8 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
     packet loop and ComputePart read (Init.f:462-1240), with the reference's
     defaults (Init.f:66-384).
 
-    Keywords used: startype ('PLANCK'), tstar, rstar [Rsun]; rin, rout, nrad,
+    Keywords used: startype ('PLANCK', or 'FILE' with starfile and lstar
+    [Lsun]), tstar, rstar [Rsun]; rin, rout, nrad,
     ntheta; denstype ('ZONES') with zoneN:rin, rout, mdust, denspow, sh,
     rsh, shpow; lam1, lam2, nlam; scattype (NONE, ISOTROPIC, FULL);
     computepartNN:file (particle file: ns, nf, then per material an .lnk
@@ -530,8 +635,9 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
     def v(key, default, cast=float):
         return deck_value(d, key, default, cast)
 
-    if v("startype", "PLANCK", str).upper() != "PLANCK":
-        raise ValueError("startype: only 'PLANCK' stars")
+    startype = v("startype", "PLANCK", str).upper()
+    if startype not in ("PLANCK", "FILE"):
+        raise ValueError("startype: 'PLANCK' or 'FILE' stars")
     if v("denstype", "ZONES", str).upper() != "ZONES":
         raise ValueError("denstype: only 'ZONES' densities")
     if not v("tcontact", True, bool):
@@ -611,8 +717,19 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
     R, Theta, thet, SinTheta = spatial_grid(rstar_cm, rin, rout, nrad, ntheta)
     dens, V = zones_density(R, Theta, thet, zones)
     BB = api.bb_table(lam)
-    Fstar = np.array([math.pi * rstar_cm ** 2 * api.planck(tstar, x) for x in lam])
-    Lstar = integrate(nu, Fstar)
+    if startype == "FILE":
+        # the file's spectrum scaled to lstar solar luminosities (Init.f:504-509, 2677-2682)
+        if "lstar" not in d:
+            raise ValueError("startype 'FILE' needs lstar")
+        sfile = v("starfile", "", str)
+        if not os.path.isabs(sfile):
+            sfile = os.path.join(base, sfile)
+        Fstar = read_star(sfile, lam)
+        Lstar = v("lstar", 1.0) * luminosity(5778.0, RSUN)
+        Fstar = Lstar * Fstar / integrate(nu, Fstar)
+    else:
+        Fstar = np.array([math.pi * rstar_cm ** 2 * api.planck(tstar, x) for x in lam])
+        Lstar = integrate(nu, Fstar)
     nr, nt = R.size - 1, Theta.size
     w0 = np.array(weights)
     w = np.tile(w0, (nr, nt - 1, 1))

@@ -165,3 +165,53 @@ idum=-7
     assert abs(m.Lstar / ref.Lstar - 1) < 1e-12
     with pytest.raises(ValueError):
         M.deck_model(None, str(deck), overrides=["scattype='RAYLEIGH'"], compute_parts=oracle_parts)
+
+
+def test_read_star_bins_and_interpolates(tmp_path):
+    lam = M.wavelength_grid(0.1, 100.0, 30)[0]
+    fine = np.geomspace(0.05, 50.0, 4000)
+    f = lambda x: x ** -2.0 * np.exp(-0.05 / x)
+    (tmp_path / "star.dat").write_text("* a spectrum\n" + "".join("%.9e %.9e\n" % (x, f(x)) for x in fine))
+    got = M.read_star(str(tmp_path / "star.dat"), lam)
+    inside = lam < 30.0
+    # bin averages of a smooth spectrum sampled densely: close to its value
+    assert np.allclose(got[inside], f(lam[inside]), rtol=0.03)
+    # beyond the file: lambda^-2 from the last point
+    beyond = lam > 50.0 * 1.0001
+    assert np.allclose(got[beyond], f(fine[-1]) * fine[-1] ** 2 / lam[beyond] ** 2, rtol=1e-9)
+    # a coarse file: a bin holding one of its points takes that point's value,
+    # a bin holding none the log-log interpolation between its points
+    coarse = np.geomspace(0.05, 50.0, 7)
+    (tmp_path / "coarse.dat").write_text("".join("%.12e %.12e\n" % (x, x ** -3.0) for x in coarse))
+    got = M.read_star(str(tmp_path / "coarse.dat"), lam)
+    interp = np.isclose(got, lam ** -3.0, rtol=1e-9)
+    point = np.array([np.any(np.isclose(g, coarse ** -3.0, rtol=1e-9)) for g in got])
+    assert np.all((interp | point)[lam < 50.0])
+    assert interp.sum() >= 15 and point.sum() >= 4
+
+
+def test_deck_model_file_star(tmp_path):
+    import oracle_ffi as O
+    lam_tab = np.geomspace(0.05, 5000.0, 80)
+    n, k = M.synthetic_lnk(lam_tab, 0.03)
+    (tmp_path / "syn.lnk").write_text("".join("%g %g %g\n" % t for t in zip(lam_tab, n, k)))
+    (tmp_path / "dust.particle").write_text("1\n1\n'syn.lnk'\n1.0 3.0\n")
+    fine = np.geomspace(0.05, 5000.0, 3000)
+    (tmp_path / "spec.dat").write_text("".join("%.9e %.9e\n" % (x, x ** -2 * np.exp(-0.3 / x)) for x in fine))
+    deck = tmp_path / "d.in"
+    deck.write_text("startype='FILE'\nstarfile='spec.dat'\nlstar=20\nnrad=8\nntheta=6\nnlam=15\n"
+                    "zone1:rin=1\nzone1:rout=50\nzone1:fix=.true.\ncomputepart01:file='dust.particle'\n")
+
+    def oracle_parts(parts):
+        return [O.compute_part(p["lam"], p["e1"][0], p["e2"][0], p["frac"], p["rho"], p["amin"], p["amax"],
+                               p["apow"], p["fmax"], p["blend"], p["porosity"], p["ns"], p["nf"]) for p in parts]
+
+    m, run = M.deck_model(None, str(deck), compute_parts=oracle_parts)
+    Lsun = M.luminosity(5778.0, M.RSUN)
+    # the reference's luminosity unit is per steradian over pi: sigma T^4 R^2,
+    # as the integral of Fstar = pi R^2 B_nu is for a Planck star
+    assert abs(Lsun / (5.6704e-5 * 5778.0 ** 4 * M.RSUN ** 2) - 1) < 1e-3
+    assert abs(m.Lstar / (20 * Lsun) - 1) < 1e-14
+    assert abs(M.integrate(m.nu, m.Fstar) / m.Lstar - 1) < 1e-12
+    with pytest.raises(ValueError):
+        M.deck_model(None, str(deck), overrides=["startype='KURUCZ'"], compute_parts=oracle_parts)
