@@ -320,6 +320,33 @@ typedef struct {
 mcg_status mcg_disk_structure(mcg_ctx *ctx, const mcg_structure *s, const double *Temp, double *dens, double *dens0,
                               double *gasdens, double *w, double *w0);
 
+/* Ray-traced spectrum at one inclination: the 'SPECTRUM' observation of
+ * Telescope.f:137-160 -- TracePath (TraceMono.f:2032) once, then TraceFlux
+ * (TraceMono.f:8) per wavelength -- for the thermal emission of the dust
+ * (thermal contact, cell temperatures T) and the star seen through the
+ * disk, on the current model.  The scattering field of TraceMono's second
+ * Monte Carlo is not included (flux as with no scattered light), and a
+ * component's extinction is Kabs + Ksca as uploaded.  The image has nphi
+ * angles over half the plane and radii from the tau = 0.1 radius at
+ * lam_path, the fixed radii Rfix, nr points per radial cell (nr < 0: one
+ * point every -nr cells), 30 over the stellar disk and the outer edge.
+ * flux[k] is the reference's image%flux at lam_obs[k] (0 outside the
+ * wavelength grid): multiply by 1e23 / distance^2 [cm] for Jy.  info (may
+ * be NULL): [0] image radii, [1] rays ended by a geometry failure. */
+typedef struct {
+  double angle;       /* inclination, rad */
+  int32_t nphi;       /* image angles over half the plane (Telescope default 45) */
+  int32_t nr;         /* image points per radial cell (default 2) */
+  int32_t nRfix;      /* fixed radii: zone and gap edges inside the grid, AU */
+  const double *Rfix;
+  double lam_path;    /* micron; 0.55 for a spectrum */
+  int32_t tracestar;  /* 1: add the star behind the disk */
+  double dimstar;     /* factor on the star (1) */
+} mcg_trace_opts;
+
+mcg_status mcg_trace_spectrum(mcg_ctx *ctx, const mcg_trace_opts *opts, const double *T, int32_t nobs,
+                              const double *lam_obs, double *flux, int32_t *info);
+
 /* ----------------------------------------------------------------------
  * Opacity-surrogate network.  No counterpart in the reference: it stands in
  * for ComputePart's coated-sphere inner loop (ComputePart.f:318-447) inside

@@ -53,6 +53,12 @@ class Structure(C.Structure):
                 ("grain_scale", C.POINTER(C.c_double))]
 
 
+class TraceOpts(C.Structure):
+    _fields_ = [("angle", C.c_double), ("nphi", C.c_int32), ("nr", C.c_int32), ("nRfix", C.c_int32),
+                ("Rfix", C.POINTER(C.c_double)), ("lam_path", C.c_double), ("tracestar", C.c_int32),
+                ("dimstar", C.c_double)]
+
+
 class Grid(C.Structure):
     _fields_ = [
         ("nr", C.c_int), ("nt", C.c_int), ("R", dp), ("Theta", dp), ("SinTheta", dp),
@@ -119,6 +125,8 @@ SIGNATURES = {
     "mcg_set_model": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Opacity)]),
     "mcg_mcradiation": (C.c_int, [C.c_void_p, C.POINTER(Run), C.POINTER(C.c_int64), C.POINTER(Result)]),
     "mcg_finalize_t": (C.c_int, [C.c_void_p, dp, dp, dp]),
+    "mcg_trace_spectrum": (C.c_int, [C.c_void_p, C.POINTER(TraceOpts), dp, C.c_int32, dp, dp,
+                                     C.POINTER(C.c_int32)]),
     "mcg_disk_structure": (C.c_int, [C.c_void_p, C.POINTER(Structure), dp, dp, dp, dp, dp, dp]),
     "mcg_diffuse": (C.c_int, [C.c_void_p, C.c_int32, C.c_double, C.c_double, C.POINTER(C.c_int32), dp, dp, dp,
                               C.POINTER(C.c_int32)]),

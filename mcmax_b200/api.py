@@ -213,6 +213,24 @@ class Context:
         self._check(self.lib.mcg_finalize_t(self.h, _ffi.ptr(T), _ffi.ptr(dT), _ffi.ptr(dE)))
         return T, dT, dE
 
+    def trace_spectrum(self, T, lam_obs, angle, nphi=45, nr=2, Rfix=(), lam_path=0.55, tracestar=True,
+                       dimstar=1.0):
+        """mcg_trace_spectrum on the current model: the ray-traced flux at
+        inclination `angle` [rad] for each wavelength of lam_obs, from the
+        cell temperatures T.  Returns (flux, info) with flux in the
+        reference's units (x 1e23 / distance^2 for Jy) and info = (image
+        radii, rays ended by a geometry failure)."""
+        T = _f64(T).reshape(-1)
+        lam_obs = _f64(np.atleast_1d(lam_obs))
+        Rfix = _f64(np.atleast_1d(np.asarray(Rfix, float)))
+        o = _ffi.TraceOpts(float(angle), int(nphi), int(nr), int(Rfix.size), _ffi.ptr(Rfix) if Rfix.size else None,
+                           float(lam_path), int(bool(tracestar)), float(dimstar))
+        flux = np.zeros(lam_obs.size)
+        info = np.zeros(2, np.int32)
+        self._check(self.lib.mcg_trace_spectrum(self.h, C.byref(o), _ffi.ptr(T), lam_obs.size, _ffi.ptr(lam_obs),
+                                                _ffi.ptr(flux), _ffi.ptr(info)))
+        return flux, (int(info[0]), int(info[1]))
+
     def disk_structure(self, R, Theta, V, Mstar, zones, Temp, dens, dens0, gasdens, w, w0, shscale=None,
                        grain_scale=None):
         """mcg_disk_structure: zones is a list of (rin, rout, sh, rsh, shpow,

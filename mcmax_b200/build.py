@@ -26,10 +26,11 @@ UNITS = {
     "mlp_kernels.cu": [],
     "diffuse.cu": ["--fmad=false"],
     "dstruct.cu": ["--fmad=false"],
+    "raytrace.cu": ["--fmad=false"],
 }
 HEADERS = ["detmath.h", "cplx.h", "philox.h", "dhs_core.cuh", "transport_core.cuh", "transport_fast.cuh",
            "mcg_internal.h", "tc_sm100.cuh", "diffuse_core.cuh",
-           "dstruct_core.cuh"]
+           "dstruct_core.cuh", "rt_core.cuh"]
 
 
 def _nvcc():

@@ -117,6 +117,13 @@ mcg_status mcg_finalize_t(mcg_ctx *ctx, double *T, double *dT, double *dEJv) {
   return mcg_finalize_impl(ctx, T, dT, dEJv);
 }
 
+mcg_status mcg_trace_spectrum(mcg_ctx *ctx, const mcg_trace_opts *opts, const double *T, int32_t nobs,
+                              const double *lam_obs, double *flux, int32_t *info) {
+  if (!ctx) return MCG_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  return mcg_trace_spectrum_impl(ctx, opts, T, nobs, lam_obs, flux, info);
+}
+
 mcg_status mcg_disk_structure(mcg_ctx *ctx, const mcg_structure *s, const double *Temp, double *dens, double *dens0,
                               double *gasdens, double *w, double *w0) {
   if (!ctx) return MCG_ERR_ARG;

@@ -79,6 +79,8 @@ struct DevModel {
   double *c2cum = nullptr, *s2cum = nullptr, *rw_logy = nullptr;
   double *KextTot = nullptr;  /* ncell*nlam, fp64 fast path, non-uniform */
   double *BBT = nullptr;      /* TT*nlam: BB temperature-major, non-uniform mixtures */
+  /* host copies of the wavelength grid and the stellar spectrum */
+  std::vector<double> lam_h, Fstar_h;
   std::vector<void *> owned;
 };
 
@@ -158,6 +160,8 @@ mcg_status mcg_part_static_impl(mcg_ctx *ctx, const mcg_part_in *in, mcg_part_ou
 mcg_status mcg_set_model_impl(mcg_ctx *ctx, const mcg_grid *grid, const mcg_opacity *opac);
 mcg_status mcg_mcradiation_impl(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot, mcg_result *res);
 mcg_status mcg_finalize_impl(mcg_ctx *ctx, double *T, double *dT, double *dEJv);
+mcg_status mcg_trace_spectrum_impl(mcg_ctx *ctx, const mcg_trace_opts *o, const double *T, int32_t nobs,
+                                   const double *lam_obs, double *flux, int32_t *info);
 mcg_status mcg_disk_structure_impl(mcg_ctx *ctx, const mcg_structure *s, const double *Temp, double *dens,
                                    double *dens0, double *gasdens, double *w, double *w0);
 mcg_status mcg_diffuse_impl(mcg_ctx *ctx, int32_t nphotmin, double dtmax, double factRW, const int32_t *Ni,

@@ -391,6 +391,8 @@ mcg_status mcg_set_model_impl(mcg_ctx *ctx, const mcg_grid *g, const mcg_opacity
   UP(m.V, g->V, ncell);
   UP(m.comp_w, g->comp_w, (size_t)ncell * ncomp);
   UP(m.nu, o->nu, nlam);
+  m.lam_h.assign(o->lam, o->lam + nlam);
+  m.Fstar_h.assign(o->Fstar, o->Fstar + nlam);
   UP(m.dnu_half, dnu_half.data(), nlam - 1);
   UP(m.BB, o->BB, (size_t)nlam * TP_TT);
   UP(m.star_cdf, star_cdf.data(), nlam - 1);

@@ -174,6 +174,15 @@ int orc_disk_structure(int nR, int nTheta, int ng, const double *R, const double
                        const double *grain_scale, const double *Temp, double *dens, double *dens0, double *gasdens,
                        double *w, double *w0);
 
+/* Ray-traced spectrum without a scattering field (TracePath + TraceFlux,
+ * TraceMono.f:2032-2297 and 8-497): Kabs_c, Ksca_c per component (ncomp*nlam),
+ * T per cell; the model's dens is used as given.  info: [0] image radii,
+ * [1] rays ended by a geometry failure. */
+int orc_trace_spectrum(const orc_model *m, const double *Kabs_c, const double *Ksca_c, const double *T,
+                       int scat_how, double angle, int nphi, int nj0, int nRfix, const double *Rfix,
+                       double lam_path, int tracestar, double dimstar, int nobs, const double *lam_obs, double *flux,
+                       int *info);
+
 /* ran1 (Numerical Recipes minimal standard + shuffle), Subroutines.f:1481-1509 */
 double orc_ran1(int32_t *idum, int32_t *iv, int32_t *iy);
 

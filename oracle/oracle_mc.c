@@ -889,3 +889,314 @@ void orc_init_random_walk(const orc_model *m, int scat_how, double factRW, uint8
     }
   }
 }
+
+/* ---------------------------------------------------------------- ray-traced spectrum
+ * TracePath + TraceFlux (TraceMono.f:2032-2297, 8-497) for the thermal
+ * emission and the star, without a scattering field, as the reference
+ * orders it: the paths of all image rays are traced and stored first
+ * (count2dpath, trace2dpath), then integrated per wavelength.  The tau =
+ * 0.1 radius uses the opacities at lam_path (the reference's trace reads
+ * the last packet's opacities).  exp, cos and sin of the ray set-up and the
+ * attenuation are detmath's. */
+
+typedef struct {
+  int n, cap, hitstar;
+  int *i, *j;
+  double *v;
+} orc_path;
+
+static void path_push(orc_path *p, int i, int j, double v) {
+  if (p->n == p->cap) {
+    p->cap = p->cap ? 2 * p->cap : 64;
+    p->i = (int *)realloc(p->i, sizeof(int) * p->cap);
+    p->j = (int *)realloc(p->j, sizeof(int) * p->cap);
+    p->v = (double *)realloc(p->v, sizeof(double) * p->cap);
+  }
+  p->i[p->n] = i;
+  p->j[p->n] = j;
+  p->v[p->n] = v;
+  p->n++;
+}
+
+static void rt_cells(const orc_model *m, const double *Kabs_c, const double *Ksca_c, const double *T, double lam0,
+                     double *kext, double *emis) {
+  const int nlam = m->nlam, ncell = m->nr * (m->nt - 1), TT = ORC_TMAX + 1;
+  int l1 = 0, l2 = 1;
+  double w1 = 1.0, w2 = 0.0;
+  for (int i = 0; i < nlam - 1; ++i)
+    if (lam0 >= m->lam[i] && lam0 <= m->lam[i + 1]) {
+      l1 = i;
+      l2 = i + 1;
+      w1 = (m->lam[i + 1] - lam0) / (m->lam[i + 1] - m->lam[i]);
+      w2 = (lam0 - m->lam[i]) / (m->lam[i + 1] - m->lam[i]);
+    }
+  if (lam0 >= m->lam[nlam - 1]) {
+    l1 = nlam - 2;
+    l2 = nlam - 1;
+    w1 = 0.0;
+    w2 = 1.0;
+  }
+  for (int c = 0; c < ncell; ++c) {
+    const double *w = m->comp_w + (size_t)c * m->ncomp;
+    double Kabs = 0.0, Kext = 0.0, Ksca = 0.0;
+    for (int q = 0; q < m->ncomp; ++q) {
+      const double *Ka = Kabs_c + (size_t)q * nlam, *Ks = Ksca_c + (size_t)q * nlam;
+      Kabs = Kabs + (w1 * Ka[l1] + w2 * Ka[l2]) * w[q];
+      Kext = Kext + (w1 * (Ka[l1] + Ks[l1]) + w2 * (Ka[l2] + Ks[l2])) * w[q];
+      Ksca = Ksca + (w1 * Ks[l1] + w2 * Ks[l2]) * w[q];
+    }
+    const double albedo = Ksca / Kext;
+    int iT = (int)(T[c] / 1.0);
+    const double wT1 = (double)(iT + 1) - T[c] / 1.0, wT2 = T[c] / 1.0 - (double)iT;
+    if (iT < 1) iT = 1;
+    if (iT > ORC_TMAX - 1) iT = ORC_TMAX - 1;
+    double e = 0.0;
+    for (int q = 0; q < m->ncomp; ++q) {
+      const double *Ka = Kabs_c + (size_t)q * nlam;
+      e = e + (((w1 * (wT1 * m->BB[(size_t)l1 * TT + iT] + wT2 * m->BB[(size_t)l1 * TT + iT + 1])) * Ka[l1] +
+                (w2 * (wT1 * m->BB[(size_t)l2 * TT + iT] + wT2 * m->BB[(size_t)l2 * TT + iT + 1])) * Ka[l2]) *
+               w[q]) / Kabs;
+    }
+    kext[c] = Kext;
+    emis[c] = e * (1.0 - albedo);
+  }
+}
+
+static void sel_sort(double *x, int n) { /* sort, Subroutines.f:1907-1927 */
+  for (int j = 0; j < n - 1; ++j) {
+    double mn = x[j];
+    int im = j;
+    for (int i = j; i < n; ++i)
+      if (x[i] < mn) {
+        mn = x[i];
+        im = i;
+      }
+    mn = x[j];
+    x[j] = x[im];
+    x[im] = mn;
+  }
+}
+
+int orc_trace_spectrum(const orc_model *m, const double *Kabs_c, const double *Ksca_c, const double *T,
+                       int scat_how, double angle, int nphi, int nj0, int nRfix, const double *Rfix,
+                       double lam_path, int tracestar, double dimstar, int nobs, const double *lam_obs, double *flux,
+                       int *info) {
+  const int nR = m->nr, nTheta = m->nt, nc = nTheta - 1, ncell = nR * nc, nstar = 30;
+  mc_t s;
+  memset(&s, 0, sizeof s);
+  s.m = m;
+  s.nc = nc;
+  double *kext = (double *)malloc(sizeof(double) * ncell), *emis = (double *)malloc(sizeof(double) * ncell);
+  /* tau01R, midplane direction */
+  rt_cells(m, Kabs_c, Ksca_c, T, lam_path, kext, emis);
+  double R01;
+  {
+    const double r = m->R[1], ct = (m->Theta[nc - 1] + m->Theta[nc]) / 2.0;
+    orc_phot p;
+    memset(&p, 0, sizeof p);
+    p.x = sqrt(1.0 - ct * ct) * r;
+    p.z = ct * r;
+    p.edgeNr = 1;
+    p.onEdge = 1;
+    p.vx = p.x / r;
+    p.vz = p.z / r;
+    p.i = 1;
+    p.j = nc;
+    double tau = 0.0, v;
+    int escape = 0, inext, jnext;
+    for (int n = 0; n < 1000000; ++n) {
+      if (trace2edge(&s, &p, &v, &inext, &jnext) != 0) break;
+      const int c = p.i * nc + (p.j - 1);
+      const double tau1 = ((kext[c] * v) * m->dens[c]) * AU_CM;
+      if (tau + tau1 > 0.1) {
+        v = v * (0.1 - tau) / tau1;
+        p.x = p.x + p.vx * v;
+        p.y = p.y + p.vy * v;
+        p.z = p.z + p.vz * v;
+        break;
+      }
+      p.x = p.x + p.vx * v;
+      p.y = p.y + p.vy * v;
+      p.z = p.z + p.vz * v;
+      p.onEdge = 1;
+      tau = tau + tau1;
+      if (inext >= nR || inext < 0) {
+        escape = 1;
+        break;
+      }
+      p.i = inext;
+      p.j = jnext;
+    }
+    if (escape) p.z = 0.0;
+    R01 = sqrt(p.x * p.x + p.z * p.z);
+    if (R01 > m->R[nR - 1]) R01 = m->R[1];
+  }
+  /* image radii (TraceMono.f:2108-2222) */
+  int nimg = (nj0 > 0 ? nj0 * (nR - 1) : (nR - 2) / (-nj0) + 1) + nc * 2 * (nRfix + 2) + 1 + nstar;
+  if (scat_how == 2) nimg += 180 * (nRfix + 1);
+  double *Ri = (double *)calloc((size_t)nimg, sizeof(double));
+  double *ta = (double *)malloc(sizeof(double) * (nTheta + 1));
+  for (int j = 1; j <= nc; ++j) ta[j] = acos((m->Theta[j - 1] + m->Theta[j]) / 2.0);
+  int nj = 0;
+  for (int j = 1; j <= nc; ++j) {
+    Ri[nj++] = R01 * fabs(cos(PI_D / 2.0 - ta[j] + angle));
+    Ri[nj++] = fabs(R01 * cos(ta[j] - PI_D / 2.0 + angle));
+  }
+  for (int j = 1; j <= nc; ++j) {
+    Ri[nj++] = R01 * fabs(cos(PI_D / 2.0 - ta[j]));
+    Ri[nj++] = fabs(R01 * cos(ta[j] - PI_D / 2.0));
+  }
+  if (scat_how == 2)
+    for (int j = 1; j <= 180; ++j) {
+      const double theta = (double)(float)j * (PI_D / 2.0) / 181.0;
+      Ri[nj++] = m->R[1] * fabs(cos(PI_D / 2.0 - theta));
+      for (int i = 0; i < nRfix; ++i) Ri[nj++] = Rfix[i] * fabs(cos(PI_D / 2.0 - theta));
+    }
+  for (int i = 0; i < nRfix; ++i)
+    for (int j = 1; j <= nc; ++j) {
+      Ri[nj++] = Rfix[i] * fabs(cos(PI_D / 2.0 - ta[j] + angle));
+      Ri[nj++] = fabs(Rfix[i] * cos(ta[j] - PI_D / 2.0 + angle));
+    }
+  sel_sort(Ri, nj);
+  if (nj0 > 0) {
+    for (int i = 1; i <= nR - 1; ++i)
+      for (int j = 1; j <= nj0; ++j)
+        Ri[nj++] = m->R[i] + (m->R[i + 1] - m->R[i]) * ((double)(float)j - 0.5) / (double)(float)nj0;
+  } else {
+    for (int i = 1; i <= nR - 1; i += -nj0) Ri[nj++] = pow(10.0, log10(m->R[i] * m->R[i + 1]) / 2.0);
+  }
+  for (int i = 1; i <= nstar - 1; ++i) Ri[nj++] = ((0.999 * m->R[0]) * (double)(float)(i - 1)) / (double)(float)(nstar - 2);
+  Ri[nj++] = m->R[0] * (double)1.001f;
+  Ri[nimg - 1] = m->R[nR] * (double)0.9999f;
+  sel_sort(Ri, nimg);
+  {
+    int k = 0;
+  restart:
+    k = k + 1;
+    for (int i = nimg - 1; i >= 1; --i)
+      if (Ri[i] == Ri[i - 1]) {
+        if (i != nimg - 1)
+          Ri[i] = (Ri[i + 1] + Ri[i]) / 2.0;
+        else
+          Ri[i - 1] = (Ri[i - 1] + Ri[i]) / 2.0;
+        if (k < nimg * 10) goto restart;
+      }
+  }
+  /* paths (TraceMono.f:2236-2290, trace2dpath) */
+  orc_path *paths = (orc_path *)calloc((size_t)nimg * nphi, sizeof(orc_path));
+  double *phi = (double *)malloc(sizeof(double) * nphi);
+  int bad = 0;
+  for (int i = 0; i < nimg; ++i)
+    for (int k = 1; k <= nphi; ++k) {
+      phi[k - 1] = 1e-5 + PI_D * (double)((float)k - 0.5f) / (double)(float)nphi;
+      const double Rad = Ri[i], Rout = m->R[nR];
+      orc_phot p;
+      memset(&p, 0, sizeof p);
+      p.x = Rad * dm_cos(phi[k - 1]);
+      p.y = Rad * dm_sin(phi[k - 1]);
+      p.z = sqrt(Rout * Rout - Rad * Rad);
+      p.edgeNr = 2;
+      p.onEdge = 1;
+      rotate(&p.x, &p.y, &p.z, 0.0, 1.0, 0.0, angle);
+      const double ct = fabs(p.z) / Rout;
+      p.i = nR - 1;
+      p.j = 1;
+      for (int j = 1; j <= nc; ++j)
+        if (ct < m->Theta[j - 1] && ct >= m->Theta[j]) p.j = j;
+      p.vx = 0.0;
+      p.vy = 0.0;
+      p.vz = -1.0;
+      rotate(&p.vx, &p.vy, &p.vz, 0.0, 1.0, 0.0, angle);
+      orc_path *pa = &paths[(size_t)i * nphi + (k - 1)];
+      for (int n = 0;; ++n) {
+        double v;
+        int inext, jnext;
+        if (n >= (1 << 20) || trace2edge(&s, &p, &v, &inext, &jnext) != 0) {
+          bad++;
+          break;
+        }
+        p.onEdge = 1;
+        path_push(pa, p.i, p.j, v);
+        p.x = p.x + p.vx * v;
+        p.y = p.y + p.vy * v;
+        p.z = p.z + p.vz * v;
+        if (inext >= nR) break;
+        if (inext < 0) {
+          pa->hitstar = 1;
+          break;
+        }
+        p.i = inext;
+        p.j = jnext;
+      }
+    }
+  /* TraceFlux per wavelength */
+  double *image = (double *)malloc(sizeof(double) * (size_t)nimg * nphi);
+  for (int l = 0; l < nobs; ++l) {
+    const double lam0 = lam_obs[l];
+    flux[l] = 0.0;
+    if (lam0 < m->lam[0] || lam0 > m->lam[m->nlam - 1]) continue;
+    int l1 = 0, l2 = 1;
+    double w1 = 1.0, w2 = 0.0;
+    for (int i = 0; i < m->nlam - 1; ++i)
+      if (lam0 >= m->lam[i] && lam0 <= m->lam[i + 1]) {
+        l1 = i;
+        l2 = i + 1;
+        w1 = (m->lam[i + 1] - lam0) / (m->lam[i + 1] - m->lam[i]);
+        w2 = (lam0 - m->lam[i]) / (m->lam[i + 1] - m->lam[i]);
+      }
+    if (lam0 >= m->lam[m->nlam - 1]) {
+      l1 = m->nlam - 2;
+      l2 = m->nlam - 1;
+      w1 = 0.0;
+      w2 = 1.0;
+    }
+    rt_cells(m, Kabs_c, Ksca_c, T, lam0, kext, emis);
+    for (int i = 0; i < nimg; ++i)
+      for (int k = 0; k < nphi; ++k) {
+        const orc_path *pa = &paths[(size_t)i * nphi + k];
+        double I = 0.0, tau = 0.0, fact = 1.0;
+        int stopped = 0;
+        for (int q = 0; q < pa->n; ++q) {
+          const int ip = pa->i[q], jp = pa->j[q];
+          if (ip != 0) {
+            const int c = ip * nc + (jp - 1);
+            const double tau_e = ((pa->v[q] * m->dens[c]) * kext[c]) * AU_CM;
+            if (tau_e < 1e-6) {
+              I = I + (emis[c] * tau_e) * fact;
+              fact = fact * (1.0 - tau_e);
+            } else {
+              const double ex = dm_exp(-tau_e);
+              I = I + (emis[c] * (1.0 - ex)) * fact;
+              fact = fact * ex;
+            }
+            tau = tau + tau_e;
+          }
+          if (tau > 1e8) {
+            stopped = 1;
+            break;
+          }
+        }
+        if (!stopped && pa->hitstar && tracestar)
+          I = I + (((m->Fstar[l1] * w1 + m->Fstar[l2] * w2) * fact) * dimstar) /
+                      (PI_D * ((m->R[0] * AU_CM) * (m->R[0] * AU_CM)));
+        image[(size_t)i * nphi + k] = I;
+      }
+    double f = 0.0;
+    for (int i = 0; i < nimg - 1; ++i)
+      for (int k = 0; k < nphi; ++k) {
+        const double w1a = (((2.0 * PI_D) * fabs(Ri[i])) * (AU_CM * AU_CM)) / (double)(float)nphi;
+        const double w2a = (((2.0 * PI_D) * fabs(Ri[i + 1])) * (AU_CM * AU_CM)) / (double)(float)nphi;
+        f = f + ((Ri[i + 1] - Ri[i]) * (w1a * image[(size_t)i * nphi + k] + w2a * image[(size_t)(i + 1) * nphi + k])) / 2.0;
+      }
+    flux[l] = f;
+  }
+  info[0] = nimg;
+  info[1] = bad;
+  for (int q = 0; q < nimg * nphi; ++q) {
+    free(paths[q].i);
+    free(paths[q].j);
+    free(paths[q].v);
+  }
+  free(paths); free(phi); free(image); free(Ri); free(ta); free(kext); free(emis);
+  return 0;
+}

@@ -13,7 +13,7 @@ SRC = os.path.join(HERE, "native", "hostcheck.cpp")
 LIB = os.path.join(HERE, "native", "libhostcheck.so")
 DEPS = [SRC] + [os.path.join(HERE, "..", "mcmax_b200", "csrc", f) for f in
                 ("dhs_core.cuh", "transport_core.cuh", "transport_fast.cuh", "diffuse_core.cuh", "dstruct_core.cuh",
-                 "detmath.h", "cplx.h", "philox.h")]
+                 "rt_core.cuh", "detmath.h", "cplx.h", "philox.h")]
 
 
 class HcModel(C.Structure):
@@ -151,3 +151,28 @@ def _structure_call(fn, st, Temp, dens, dens0, gasdens, w, w0):
 
 def disk_structure(st, Temp, dens, dens0, gasdens, w, w0):
     return _structure_call(load().hc_disk_structure, st, Temp, dens, dens0, gasdens, w, w0)
+
+
+def trace_spectrum(model, T, lam_obs, angle, nphi=45, nj0=2, Rfix=(), lam_path=0.55, tracestar=1, dimstar=1.0,
+                   dens=None, cap=20000):
+    """the host logic of mcg_trace_spectrum with its kernels as loops;
+    returns (flux, R_image, image (nr, nphi) of the last wavelength, bad rays)"""
+    L = load()
+    m = model
+    dens = np.maximum(np.asarray(m.dens, float), 1e-50) if dens is None else np.asarray(dens, float)
+    arrs = [np.ascontiguousarray(a, float) for a in (m.R, m.Theta, dens, m.comp_w, m.Kabs, m.Ksca, m.BB, m.lam,
+                                                     m.Fstar, T)]
+    lam_obs = np.ascontiguousarray(lam_obs, float)
+    Rfix = np.ascontiguousarray(Rfix, float)
+    flux = np.zeros(lam_obs.size)
+    info = np.zeros(2, np.int32)
+    Rimg = np.zeros(cap)
+    image = np.zeros(cap * nphi)
+    rc = L.hc_trace_spectrum(m.nr, m.nt, P(arrs[0]), P(arrs[1]), P(arrs[2]), int(m.scat_how), m.ncomp, m.nlam,
+                             P(arrs[3]), P(arrs[4]), P(arrs[5]), P(arrs[6]), P(arrs[7]), P(arrs[8]), P(arrs[9]),
+                             C.c_double(angle), int(nphi), int(nj0), int(Rfix.size), P(Rfix) if Rfix.size else None,
+                             C.c_double(lam_path), int(tracestar), C.c_double(dimstar), int(lam_obs.size), P(lam_obs),
+                             P(flux), P(info), P(Rimg), int(cap), P(image))
+    assert rc == 0
+    nr = int(info[0])
+    return flux, Rimg[:nr], image[:nr * nphi].reshape(nr, nphi), int(info[1])

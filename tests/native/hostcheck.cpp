@@ -11,6 +11,7 @@
 #include "../../mcmax_b200/csrc/transport_core.cuh"
 #include "../../mcmax_b200/csrc/diffuse_core.cuh"
 #include "../../mcmax_b200/csrc/dstruct_core.cuh"
+#include "../../mcmax_b200/csrc/rt_core.cuh"
 
 extern "C" {
 
@@ -380,4 +381,78 @@ extern "C" int hc_disk_structure(int nR, int nTheta, int ng, const double *R, co
   DsGrid g{nR, nTheta, ng, R, Theta, V, Mstar, nzones, zs.data(), shscale, grain_scale};
   HostStructBackend be;
   return ds_disk_structure(g, be, Temp, dens, dens0, gasdens, w, w0) ? 0 : 1;
+}
+
+/* the ray-traced spectrum on the host: the host logic of
+ * mcg_trace_spectrum with its kernels replaced by loops over rt_cell and
+ * rt_ray.  dens is used as given (the library floors it at 1e-50). */
+struct HostRtBackend {
+  TModel m;
+  int ncomp, nlam;
+  const double *comp_w, *Kabs_c, *Ksca_c, *BB, *lam, *T, *dens;
+  std::vector<double> kext, emis;
+  bool cells(double lam0, double *kx, double *em) {
+    int l1, l2;
+    double w1, w2;
+    rt_lam(nlam, lam, lam0, &l1, &l2, &w1, &w2);
+    const int ncell = m.nr * (m.nt - 1);
+    kext.resize(ncell);
+    emis.resize(ncell);
+    for (int c = 0; c < ncell; ++c)
+      rt_cell(c, ncomp, nlam, comp_w, Kabs_c, Ksca_c, BB, T[c], l1, l2, w1, w2, &kext[c], &emis[c]);
+    std::copy(kext.begin(), kext.end(), kx);
+    std::copy(emis.begin(), emis.end(), em);
+    return true;
+  }
+  bool rays(const std::vector<double> &R, const std::vector<double> &phi, double fstar, const RtOptions &o,
+            double *image, int *bad) {
+    const int nr = (int)R.size(), nphi = (int)phi.size();
+    *bad = 0;
+    for (int i = 0; i < nr; ++i)
+      for (int k = 0; k < nphi; ++k) {
+        int steps;
+        image[(size_t)i * nphi + k] = rt_ray(m, dens, kext.data(), emis.data(), R[i], phi[k], o.angle, fstar,
+                                              o.dimstar, o.tracestar, 1 << 20, &steps);
+        if (steps < 0) ++*bad;
+      }
+    return true;
+  }
+};
+
+extern "C" int hc_trace_spectrum(int nr, int nt, const double *R, const double *Theta, const double *dens,
+                                 int scat_how, int ncomp, int nlam, const double *comp_w, const double *Kabs_c,
+                                 const double *Ksca_c, const double *BB, const double *lam, const double *Fstar,
+                                 const double *T, double angle, int nphi, int nj0, int nRfix, const double *Rfix,
+                                 double lam_path, int tracestar, double dimstar, int nobs, const double *lam_obs,
+                                 double *flux, int *info, double *Rimg_out, int Rimg_cap, double *image_out) {
+  TModel m;
+  memset(&m, 0, sizeof m);
+  m.nr = nr;
+  m.nt = nt;
+  m.nc = nt - 1;
+  m.ncell = nr * (nt - 1);
+  m.scat_how = scat_how;
+  m.R = R;
+  m.Theta = Theta;
+  HostRtBackend be;
+  be.m = m;
+  be.ncomp = ncomp;
+  be.nlam = nlam;
+  be.comp_w = comp_w;
+  be.Kabs_c = Kabs_c;
+  be.Ksca_c = Ksca_c;
+  be.BB = BB;
+  be.lam = lam;
+  be.T = T;
+  be.dens = dens;
+  RtOptions o{angle, nphi, nj0, nRfix, Rfix, lam_path, tracestar, dimstar};
+  std::vector<double> Rimg, image;
+  int bad = 0;
+  if (!rt_spectrum(m, be, o, nlam, lam, Fstar, dens, nobs, lam_obs, flux, &Rimg, &image, &bad)) return 1;
+  info[0] = (int)Rimg.size();
+  info[1] = bad;
+  for (int i = 0; i < (int)Rimg.size() && i < Rimg_cap; ++i) Rimg_out[i] = Rimg[i];
+  if (image_out && (int)Rimg.size() <= Rimg_cap)
+    std::copy(image.begin(), image.end(), image_out);
+  return 0;
 }

@@ -264,3 +264,24 @@ def disk_structure(st, Temp, dens, dens0, gasdens, w, w0):
     """orc_disk_structure; arguments as hostcheck_ffi.disk_structure"""
     import hostcheck_ffi as H
     return H._structure_call(load().orc_disk_structure, st, Temp, dens, dens0, gasdens, w, w0)
+
+
+def trace_spectrum(model, T, lam_obs, angle, nphi=45, nj0=2, Rfix=(), lam_path=0.55, tracestar=1, dimstar=1.0,
+                   dens=None):
+    """orc_trace_spectrum; returns (flux, image radii count, bad rays)"""
+    L = load()
+    m = model
+    dens = np.maximum(np.asarray(m.dens, float), 1e-50) if dens is None else np.asarray(dens, float)
+    keep = [np.ascontiguousarray(a, float) for a in (m.R, m.Theta, m.SinTheta, dens, m.V, m.lam, m.nu, m.BB, m.Fstar,
+                                                     m.comp_w, m.Kabs, m.Ksca, T)]
+    om = OrcModel(m.nr, m.nt, P(keep[0]), P(keep[1]), P(keep[2]), P(keep[3]), P(keep[4]), None, m.nlam, P(keep[5]),
+                  P(keep[6]), None, None, None, 0, P(keep[7]), P(keep[8]), float(m.Lstar), m.ncomp, P(keep[9]), None,
+                  None, None, None, None, None, None, None, None, None, None)
+    lam_obs = np.ascontiguousarray(lam_obs, float)
+    Rfix = np.ascontiguousarray(Rfix, float)
+    flux = np.zeros(lam_obs.size)
+    info = np.zeros(2, np.int32)
+    L.orc_trace_spectrum(C.byref(om), P(keep[10]), P(keep[11]), P(keep[12]), int(m.scat_how), C.c_double(angle),
+                         int(nphi), int(nj0), int(Rfix.size), P(Rfix) if Rfix.size else None, C.c_double(lam_path),
+                         int(tracestar), C.c_double(dimstar), int(lam_obs.size), P(lam_obs), P(flux), P(info))
+    return flux, int(info[0]), int(info[1])
