@@ -9,6 +9,10 @@ that MCMax's own readers and plotting scripts take them unchanged.
     write_mcspec(outdir, model, result)   MCSpec<angle>.dat per inclination
                                           bin and MCSpec.dat
                                           (MCRadiation.f:738-762)
+    spectrum_wavelengths(lam, lam1, lam2) the wavelengths of a ray-traced
+                                          spectrum (Telescope.f:40-52)
+    write_spectrum(outdir, angle, ...)    spectrum<angle>.dat of a ray-traced
+                                          spectrum (Telescope.f:140-160)
 
 Cells are written for ir = 1..nR-1 (the star cell is left out) and it =
 1..nTheta-1, radius and angle at the cell middles (D%R_av in cm, D%theta_av
@@ -147,3 +151,57 @@ def write_mcspec(outdir, model, result, distance_pc=100.0, nangle=30):
         for i in range(model.nlam):
             f.write("%s%s\n" % (_num(model.lam[i]), _num(spec[i, 0] / d2)))
     return names
+
+
+def spectrum_wavelengths(lam, lam1, lam2):
+    """lam1, the model's wavelengths strictly between lam1 and lam2, lam2
+    (the default grid of a spectrum observation, Telescope.f:40-52)"""
+    lam = np.asarray(lam, float)
+    return np.concatenate([[lam1], lam[(lam > lam1) & (lam < lam2)], [lam2]])
+
+
+def _arrinterpol_log(x, xarr, yarr):
+    """arrinterpol(..., log=1) as Subroutines.f:2506-2535 evaluates it: at
+    or beyond either end it returns the end's abscissa, and inside, its scan
+    keeps the last interval, so the value is the power law through the
+    grid's last two points"""
+    n = len(xarr)
+    if x <= xarr[0]:
+        return float(xarr[0])
+    if x >= xarr[n - 1]:
+        return float(xarr[n - 1])
+    x1, x2, y1, y2 = xarr[n - 2], xarr[n - 1], yarr[n - 2], yarr[n - 1]
+    p = math.log10(y2 / y1) / math.log10(x2 / x1)
+    return y1 * (x / x1) ** p
+
+
+def spectrum_name(angle_deg, flag=""):
+    """spectrum<angle><flag>.dat: the angle as one digit of tens and f3.1
+    of the rest (Telescope.f:143-144)"""
+    tens = int(angle_deg / 10.0)
+    return "spectrum%d%3.1f%s.dat" % (tens, angle_deg - 10.0 * tens, flag)
+
+
+def write_spectrum(outdir, angle_deg, lam_obs, flux, lam, Fstar, distance_pc=100.0, scatflux=None, flag="",
+                   star_column="reference"):
+    """spectrum<angle>.dat of a ray-traced spectrum (Telescope.f:140-160):
+    wavelength [micron], flux [Jy], its scattered part [Jy], the star [Jy],
+    with no interstellar extinction (Av = 0).  star_column "reference"
+    writes the star as the reference's arrinterpol gives it (see
+    _arrinterpol_log); "interpolated" writes the log-log interpolation of
+    the stellar spectrum instead.  Returns the path."""
+    os.makedirs(outdir, exist_ok=True)
+    d2 = (distance_pc * PARSEC) ** 2
+    lam = np.asarray(lam, float)
+    Fstar = np.asarray(Fstar, float)
+    scat = np.zeros(len(lam_obs)) if scatflux is None else np.asarray(scatflux, float)
+    path = os.path.join(outdir, spectrum_name(angle_deg, flag))
+    with open(path, "w") as f:
+        for j, l0 in enumerate(lam_obs):
+            if star_column == "reference":
+                fs = _arrinterpol_log(l0, lam, Fstar)
+            else:
+                fs = float(np.exp(np.interp(np.log(l0), np.log(lam), np.log(Fstar))))
+            f.write("%s%s%s%s\n" % (_num(l0), _num(1e23 * flux[j] / d2), _num(1e23 * scat[j] / d2),
+                                    _num(1e23 * fs / d2)))
+    return path

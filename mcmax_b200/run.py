@@ -3,6 +3,7 @@ reference's result files:
 
     python -m mcmax_b200.run input.in Nphot [-o outdir] [-s key=value]...
                              [--precision mixed|fp64|exact] [--opacity dhs|surrogate]
+                             [--spectrum DEG]...
 
 The arguments follow the reference's command line (Main.f:60-72 for -o,
 Init.f:462-478 for -s): the deck, the packet count, an output directory
@@ -32,10 +33,24 @@ def _surrogate_parts(ctx):
     return lambda parts: S.compute_part_surrogate(ctx, parts, params)[0]
 
 
-def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opacity="dhs", compute_parts=None):
+def fixed_radii(zones, rin, rout):
+    """zone edges strictly inside the grid, each once, sorted (D%Rfix,
+    Init.f:1511-1517)"""
+    out = []
+    for z in zones:
+        for r in (z[0], z[1]):
+            if rin < r < rout and r not in out:
+                out.append(r)
+    return sorted(out)
+
+
+def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opacity="dhs", compute_parts=None,
+             spectra=(), spectrum_nphi=45, spectrum_nr=2):
     """Build the deck's model, run the packet loop and the diffusion step
-    and write the result files; returns dict(model, run, nphot, result, T,
-    diffused (the counts of mcg_diffuse, or None), files)."""
+    and write the result files; for each inclination in `spectra` [deg]
+    also the ray-traced spectrum (mcg_trace_spectrum) as
+    spectrum<angle>.dat.  Returns dict(model, run, nphot, result, T,
+    diffused (the counts of mcg_diffuse, or None), structure, files)."""
     if compute_parts is None and opacity == "surrogate":
         compute_parts = _surrogate_parts(ctx)
     elif opacity not in ("dhs", "surrogate"):
@@ -61,6 +76,14 @@ def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opac
     outputs.write_denstemp(files[0], m, T)
     names = outputs.write_mcspec(outdir, m, res, distance_pc=m.distance)
     files += [os.path.join(outdir, x) for x in names + ["MCSpec.dat"]]
+    if spectra:
+        import math
+        lam_obs = outputs.spectrum_wavelengths(m.lam, m.lam[0], m.lam[-1])
+        rfix = fixed_radii(run["zones"], m.R[1], m.R[-1])
+        for ang in spectra:
+            flux, _ = ctx.trace_spectrum(T, lam_obs, math.radians(ang), nphi=spectrum_nphi, nr=spectrum_nr,
+                                         Rfix=rfix)
+            files.append(outputs.write_spectrum(outdir, ang, lam_obs, flux, m.lam, m.Fstar, m.distance))
     return dict(model=m, run=run, nphot=n, result=res, T=T, diffused=diffused, structure=structure, files=files)
 
 
@@ -72,6 +95,10 @@ def parse_args(argv):
     ap.add_argument("-s", dest="overrides", action="append", default=[], metavar="key=value")
     ap.add_argument("--precision", choices=("mixed", "fp64", "exact"), default="mixed")
     ap.add_argument("--opacity", choices=("dhs", "surrogate"), default="dhs")
+    ap.add_argument("--spectrum", dest="spectra", action="append", type=float, default=[], metavar="DEG",
+                    help="write the ray-traced spectrum at this inclination (repeatable)")
+    ap.add_argument("--spectrum-nphi", type=int, default=45)
+    ap.add_argument("--spectrum-nr", type=int, default=2)
     ap.add_argument("--device", type=int, default=0)
     return ap.parse_args(argv)
 
@@ -83,7 +110,8 @@ def main(argv=None, context=None):
         context = Context
     ctx = context(a.device)
     try:
-        r = run_deck(ctx, a.deck, a.nphot, a.outdir, a.overrides, a.precision, a.opacity)
+        r = run_deck(ctx, a.deck, a.nphot, a.outdir, a.overrides, a.precision, a.opacity, spectra=a.spectra,
+                     spectrum_nphi=a.spectrum_nphi, spectrum_nr=a.spectrum_nr)
     finally:
         ctx.close()
     print("packets %d, %d cells, T %.1f-%.1f K, wrote %s" % (r["nphot"], r["T"].size, r["T"].min(), r["T"].max(),

@@ -45,3 +45,25 @@ def test_mcspec_names_and_columns(tmp_path):
     ok = n > 0
     assert np.allclose(a[ok, 2], sp[ok] / np.sqrt(n[ok]) / d2, rtol=1e-14)
     assert os.path.exists(os.path.join(tmp_path, "MCSpec.dat"))
+
+
+def test_spectrum_file(tmp_path):
+    lam = np.geomspace(0.1, 1000.0, 12)
+    Fstar = lam ** -2.0 * np.exp(-0.5 / lam)
+    lo = OUT.spectrum_wavelengths(lam, 0.2, 500.0)
+    assert lo[0] == 0.2 and lo[-1] == 500.0 and np.all(np.diff(lo) > 0) and lo.size == 2 + np.sum((lam > 0.2) & (lam < 500))
+    flux = np.linspace(1.0, 2.0, lo.size)
+    path = OUT.write_spectrum(str(tmp_path), 45.0, lo, flux, lam, Fstar, distance_pc=100.0)
+    assert os.path.basename(path) == "spectrum45.0.dat"
+    rows = np.loadtxt(path)
+    d2 = (100.0 * OUT.PARSEC) ** 2
+    assert np.allclose(rows[:, 0], lo) and np.allclose(rows[:, 1], 1e23 * flux / d2, rtol=1e-15)
+    assert np.all(rows[:, 2] == 0.0)
+    # the reference's star column: the abscissa at the ends, the last-interval power law inside
+    p = math.log10(Fstar[-1] / Fstar[-2]) / math.log10(lam[-1] / lam[-2])
+    inner = Fstar[-2] * (lo[1:-1] / lam[-2]) ** p
+    assert np.allclose(rows[1:-1, 3], 1e23 * inner / d2, rtol=1e-12)
+    p2 = OUT.write_spectrum(str(tmp_path), 7.5, lo, flux, lam, Fstar, star_column="interpolated", flag="_b")
+    assert os.path.basename(p2) == "spectrum07.5_b.dat"
+    r2 = np.loadtxt(p2)
+    assert np.allclose(r2[1:-1, 3], 1e23 * np.exp(np.interp(np.log(lo[1:-1]), np.log(lam), np.log(Fstar))) / d2)

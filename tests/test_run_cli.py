@@ -68,6 +68,10 @@ class FakeContext:
         T = np.linspace(20.0, 900.0, self.model.ncell)
         return T, 0 * T, 0 * T
 
+    def trace_spectrum(self, T, lam_obs, angle, nphi=45, nr=2, Rfix=()):
+        self.trace_args = (angle, nphi, nr, tuple(Rfix))
+        return np.full(len(lam_obs), 1e20), (100, 0)
+
     def close(self):
         self.closed = True
 
@@ -91,13 +95,15 @@ def test_command_line_runs_the_deck_and_writes_result_files(tmp_path):
         return made[-1]
 
     r = R.main([deck, "2e4", "-o", str(out), "-s", "randomwalk=.true.", "-s", "factrw=4",
-                "--precision", "fp64"], context=factory)
+                "--precision", "fp64", "--spectrum", "30", "--spectrum-nphi", "20"], context=factory)
     ctx = made[0]
     assert ctx.closed
     assert ctx.calls == [dict(nphot=20000, precision="fp64", seed=11, randomwalk=True, factRW=4.0,
                               maxinteract=5000, nruns=2)]
     assert ctx.diffuse_args == (7, 25, 1.0, 4.0) and r["diffused"] == (1, 5, 1, 0)
-    assert len(r["files"]) == 32 and all(os.path.exists(f) for f in r["files"])
+    assert len(r["files"]) == 33 and all(os.path.exists(f) for f in r["files"])
+    assert os.path.basename(r["files"][-1]) == "spectrum30.0.dat"
+    assert made[0].trace_args[1:] == (20, 2, ()) and abs(made[0].trace_args[0] - np.radians(30)) < 1e-15
     d = outputs.read_denstemp(str(out / "denstemp.dat"))
     m = r["model"]
     assert d["T"].shape == (m.nr - 1, m.nt - 1)
