@@ -4,6 +4,6 @@ the DHS/Mie opacity stage (ComputePart) and the photon-packet transport
 
     from mcmax_b200 import Context, ComputePart, MCRadiation
 """
-from .api import Context, McgError, ComputePart, MCRadiation, Particle, bb_table, planck  # noqa: F401
+from .api import Context, McgError, ComputePart, MCRadiation, Diffuse, Particle, bb_table, planck  # noqa: F401
 
-__all__ = ["Context", "McgError", "ComputePart", "MCRadiation", "Particle", "bb_table", "planck"]
+__all__ = ["Context", "McgError", "ComputePart", "MCRadiation", "Diffuse", "Particle", "bb_table", "planck"]
