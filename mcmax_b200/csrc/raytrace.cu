@@ -133,7 +133,7 @@ mcg_status mcg_trace_spectrum_impl(mcg_ctx *ctx, const mcg_trace_opts *o, const 
     return mcg_fail(ctx, MCG_ERR_ARG, "trace_spectrum: nphi >= 1, nr != 0, lam_path > 0 required");
   const int ncell = m.ncell;
   for (int c = 0; c < ncell; ++c)
-    if (!(T[c] >= 0.0) || !(T[c] < 1e30)) return mcg_fail(ctx, MCG_ERR_ARG, "trace_spectrum: T[%d] = %g", c, T[c]);
+    if (!(T[c] >= 0.0) || !(T[c] < 1e6)) return mcg_fail(ctx, MCG_ERR_ARG, "trace_spectrum: T[%d] = %g", c, T[c]);
   cudaStream_t st = ctx->stream;
   std::vector<double> R(m.nr + 1), Theta(m.nt), dens(ncell), lam(m.nlam), Fstar(m.nlam);
   MCG_CUDA(ctx, cudaMemcpyAsync(R.data(), m.R, sizeof(double) * R.size(), cudaMemcpyDeviceToHost, st));
