@@ -171,6 +171,9 @@ mcg_status mcg_diffuse_impl(mcg_ctx *ctx, int32_t nphotmin, double dtmax, double
   if (!Ni || !dT || !T) return mcg_fail(ctx, MCG_ERR_ARG, "diffuse: Ni, dT and T are required");
   if (!(factRW > 0.0) || !(dtmax == dtmax)) return mcg_fail(ctx, MCG_ERR_ARG, "diffuse: factRW > 0 and a dtmax");
   if (m.nc > DF_MAX_W) return mcg_fail(ctx, MCG_ERR_ARG, "diffuse: %d theta cells, at most %d", m.nc, DF_MAX_W);
+  for (int c = 0; c < m.ncell; ++c)
+    if (!(T[c] >= 0.0) || !(T[c] < 1e6))
+      return mcg_fail(ctx, MCG_ERR_ARG, "diffuse: T[%d] = %g is outside 0..1e6 K", c, T[c]);
   cudaStream_t st = ctx->stream;
   const int ncell = m.ncell;
   std::vector<double> R(m.nr + 1), Theta(m.nt), dens(ncell), comp_w((size_t)ncell * m.ncomp);
