@@ -47,3 +47,34 @@ def test_invalid_arguments_do_not_abort():
     assert lib.mcg_set_model(None, None, None) == _ffi.MCG_ERR_ARG
     assert lib.mcg_mcradiation(None, None, None, None) == _ffi.MCG_ERR_ARG
     assert lib.mcg_version() >= 100
+
+
+PAIRS = [("mcg_part_in", "PartIn"), ("mcg_part_out", "PartOut"), ("mcg_grid", "Grid"), ("mcg_opacity", "Opacity"),
+         ("mcg_run", "Run"), ("mcg_result", "Result"), ("mcg_batch_opts", "BatchOpts"), ("mcg_zone", "Zone"),
+         ("mcg_structure", "Structure"), ("mcg_trace_opts", "TraceOpts"),
+         ("mcg_mlp_train_opts", "MlpTrainOpts"), ("mcg_mlp_train_report", "MlpTrainReport")]
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """every struct of the header: size and field offsets as the C compiler
+    lays it out, against the ctypes mirror"""
+    import subprocess
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "mcmax_gpu.h"', "int main(void) {"]
+    for cname, pname in PAIRS:
+        st = getattr(_ffi, pname)
+        lines.append('printf("%s %%zu\\n", sizeof(%s));' % (cname, cname))
+        for f in st._fields_:
+            lines.append('printf("%s.%s %%zu\\n", offsetof(%s, %s));' % (cname, f[0], cname, f[0]))
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include", str(src), "-o",
+                    str(exe)], check=True)
+    got = dict(ln.split() for ln in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                   check=True).stdout.splitlines())
+    for cname, pname in PAIRS:
+        st = getattr(_ffi, pname)
+        assert int(got[cname]) == C.sizeof(st), cname
+        for f in st._fields_:
+            assert int(got["%s.%s" % (cname, f[0])]) == getattr(st, f[0]).offset, (cname, f[0])
