@@ -210,6 +210,37 @@ def spatial_grid(rstar_cm, rin, rout, nrad, ntheta):
     return R, Theta, thet, SinTheta
 
 
+def grid_from_centres(rstar_cm, rin, rout, r_av_cm, theta_av):
+    """Edges rebuilt from the cell centres of a density file
+    (Init.f:2727-2752 for the radii, Init.f:2876-2889 for theta): R[1] = rin,
+    each next edge the mirror of the previous one about the centre in log r
+    (or the midpoint of the two centres when that falls outside them),
+    R[nR] = rout; theta edges halfway between the centre angles.  Returns
+    (R, Theta, thet, SinTheta) as spatial_grid."""
+    r_av = np.asarray(r_av_cm, float) / AU
+    n = r_av.size
+    R = np.zeros(n + 2)
+    R[0] = rstar_cm / AU
+    R[1] = rin
+    for i in range(2, n + 1):
+        R[i] = 10.0 ** (2.0 * math.log10(r_av[i - 2]) - math.log10(R[i - 1]))
+        if r_av[i - 1] < R[i] or r_av[i - 2] > R[i]:
+            R[i] = (r_av[i - 2] + r_av[i - 1]) / 2.0
+    R[n + 1] = rout
+    R[1:n + 1] = np.sort(R[1:n + 1])
+    ta = np.asarray(theta_av, float)
+    nT = ta.size + 1
+    Theta = np.zeros(nT)
+    thet = np.zeros(nT)
+    Theta[0] = 1.0
+    for i in range(2, nT):
+        thet[i - 1] = (ta[i - 2] + ta[i - 1]) / 2.0
+        Theta[i - 1] = math.cos((ta[i - 2] + ta[i - 1]) / 2.0)
+    Theta[nT - 1] = 0.0
+    thet[nT - 1] = math.pi / 2.0
+    return R, Theta, thet, np.sin(thet)
+
+
 def cell_volumes(R, Theta):
     R = np.asarray(R, float)
     Theta = np.asarray(Theta, float)
@@ -609,7 +640,9 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
     porosity, norm_abun, standard ('FILE'), with amin, amax, apow (micron)
     as the deck-wide defaults; abunNN (relative mass of computepart entry
     NN); fixmpset, alphaturb (settling of a one-zone
-    disk); randomwalk, factrw, maxinteract, nruns, idum; nphotdiffuse,
+    disk); denstype 'FILE' with densfile (a denstemp.dat: its dust density
+    and the grid rebuilt from its cell centres; rin and rout still give the
+    outer edges); randomwalk, factrw, maxinteract, nruns, idum; nphotdiffuse,
     dtdiffuse (the diffusion step after the run); zoneN:fix, mstar,
     maxiter, epsiter (structure iterations).  A value that
     selects physics outside the packet loop (another startype or denstype,
@@ -638,8 +671,9 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
     startype = v("startype", "PLANCK", str).upper()
     if startype not in ("PLANCK", "FILE"):
         raise ValueError("startype: 'PLANCK' or 'FILE' stars")
-    if v("denstype", "ZONES", str).upper() != "ZONES":
-        raise ValueError("denstype: only 'ZONES' densities")
+    denstype = v("denstype", "ZONES", str).upper()
+    if denstype not in ("ZONES", "FILE"):
+        raise ValueError("denstype: 'ZONES' or 'FILE' densities")
     if not v("tcontact", True, bool):
         raise ValueError("tcontact: only thermal contact (Bjorkman-Wood with one temperature per cell)")
     scat = {"NONE": 0, "ISOTROPIC": 1, "FULL": 2}.get(v("scattype", "ISOTROPIC", str).upper())
@@ -657,7 +691,7 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
         zones.append(dict(rin=v(kz + "rin", rin), rout=v(kz + "rout", rout), mdust=v(kz + "mdust", 1e-5),
                           denspow=v(kz + "denspow", 1.0), sh=v(kz + "sh", 0.01), rsh=v(kz + "rsh", 1.0),
                           shpow=v(kz + "shpow", 1.1), fix=v(kz + "fix", False, bool)))
-    if not zones:
+    if not zones and denstype == "ZONES":
         raise ValueError("no zoneN:* keywords")
     # grain bins of every computepart entry (Init.f:746-789, 1323-1420)
     entries = sorted({int(k[len("computepart"):k.index(":")]) for k in d if k.startswith("computepart")
@@ -714,8 +748,21 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
         Ksca = np.zeros_like(Ksca)
     if scat == 1:
         F = np.ones_like(F)
-    R, Theta, thet, SinTheta = spatial_grid(rstar_cm, rin, rout, nrad, ntheta)
-    dens, V = zones_density(R, Theta, thet, zones)
+    if denstype == "FILE":
+        # the dust density of a denstemp file and the grid rebuilt from its
+        # cell centres (Init.f:2727-2752, readstruct InputOutput.f:579)
+        from .outputs import read_denstemp
+        dfile = v("densfile", "", str)
+        if not os.path.isabs(dfile):
+            dfile = os.path.join(base, dfile)
+        dt = read_denstemp(dfile)
+        R, Theta, thet, SinTheta = grid_from_centres(rstar_cm, rin, rout, dt["r_av"], dt["theta_av"])
+        V = cell_volumes(R, Theta)
+        dens = np.full(V.shape, 1e-60)
+        dens[1:] = dt["dens"]
+    else:
+        R, Theta, thet, SinTheta = spatial_grid(rstar_cm, rin, rout, nrad, ntheta)
+        dens, V = zones_density(R, Theta, thet, zones)
     BB = api.bb_table(lam)
     if startype == "FILE":
         # the file's spectrum scaled to lstar solar luminosities (Init.f:504-509, 2677-2682)

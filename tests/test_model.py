@@ -215,3 +215,30 @@ def test_deck_model_file_star(tmp_path):
     assert abs(M.integrate(m.nu, m.Fstar) / m.Lstar - 1) < 1e-12
     with pytest.raises(ValueError):
         M.deck_model(None, str(deck), overrides=["startype='KURUCZ'"], compute_parts=oracle_parts)
+
+
+def test_deck_model_file_density_restarts_from_denstemp(tmp_path):
+    import oracle_ffi as O
+    from mcmax_b200 import outputs as OUT
+    lam_tab = np.geomspace(0.05, 5000.0, 80)
+    n, k = M.synthetic_lnk(lam_tab, 0.03)
+    (tmp_path / "syn.lnk").write_text("".join("%g %g %g\n" % t for t in zip(lam_tab, n, k)))
+    (tmp_path / "dust.particle").write_text("1\n1\n'syn.lnk'\n1.0 3.0\n")
+    common = "rin=0.5\nrout=100\nnlam=15\ncomputepart01:file='dust.particle'\n"
+    (tmp_path / "a.in").write_text(common + "nrad=14\nntheta=10\nzone1:rin=0.5\nzone1:rout=100\nzone1:fix=.true.\n"
+                                   "zone1:mdust=1d-4\n")
+
+    def oracle_parts(parts):
+        return [O.compute_part(p["lam"], p["e1"][0], p["e2"][0], p["frac"], p["rho"], p["amin"], p["amax"],
+                               p["apow"], p["fmax"], p["blend"], p["porosity"], p["ns"], p["nf"]) for p in parts]
+
+    a, _ = M.deck_model(None, str(tmp_path / "a.in"), compute_parts=oracle_parts)
+    T = np.linspace(20, 900, a.ncell)
+    OUT.write_denstemp(str(tmp_path / "denstemp.dat"), a, T)
+    (tmp_path / "b.in").write_text(common + "denstype='FILE'\ndensfile='denstemp.dat'\n")
+    b, run = M.deck_model(None, str(tmp_path / "b.in"), compute_parts=oracle_parts)
+    assert (b.nr, b.nt) == (a.nr, a.nt) and run["zones"] == []
+    nc = a.nt - 1
+    assert np.array_equal(b.dens.reshape(b.nr, nc)[1:], a.dens.reshape(a.nr, nc)[1:])
+    assert np.allclose(b.R, a.R, rtol=1e-12) and np.allclose(b.Theta, a.Theta, rtol=0, atol=1e-14)
+    assert np.allclose(b.V, a.V, rtol=1e-10)
