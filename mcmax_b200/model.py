@@ -794,7 +794,8 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
                maxinteract=v("maxinteract", 1000000, int), nruns=v("nruns", 1, int),
                nphotdiffuse=v("nphotdiffuse", 25, int), dtdiffuse=v("dtdiffuse", 1.0),
                zones=[(z["rin"], z["rout"], z["sh"], z["rsh"], z["shpow"], z["denspow"], z["fix"]) for z in zones],
-               Mstar=v("mstar", 2.5) * MSUN, maxiter=v("maxiter", 10, int), epsiter=v("epsiter", 3.0))
+               Mstar=v("mstar", 2.5) * MSUN, maxiter=v("maxiter", 10, int), epsiter=v("epsiter", 3.0),
+               incangle=v("incangle", 45.0))
     return m, run
 
 

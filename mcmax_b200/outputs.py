@@ -153,11 +153,65 @@ def write_mcspec(outdir, model, result, distance_pc=100.0, nangle=30):
     return names
 
 
-def spectrum_wavelengths(lam, lam1, lam2):
-    """lam1, the model's wavelengths strictly between lam1 and lam2, lam2
-    (the default grid of a spectrum observation, Telescope.f:40-52)"""
+def spectrum_wavelengths(lam, lam1, lam2, nlam=-1, lamfile=None):
+    """The wavelengths of a spectrum observation (Telescope.f:40-71): from
+    lamfile when given (one per line); else with nlam < 0, lam1, the model's
+    wavelengths strictly between lam1 and lam2, and lam2; else nlam
+    log-spaced points (at most the model's count)."""
     lam = np.asarray(lam, float)
-    return np.concatenate([[lam1], lam[(lam > lam1) & (lam < lam2)], [lam2]])
+    if lamfile:
+        out = []
+        with open(lamfile) as f:
+            for line in f:
+                try:
+                    out.append(float(line.split()[0].replace("d", "e").replace("D", "E")))
+                except (ValueError, IndexError):
+                    continue
+        return np.array(out)
+    if nlam < 0:
+        return np.concatenate([[lam1], lam[(lam > lam1) & (lam < lam2)], [lam2]])
+    n = min(int(nlam), lam.size)
+    if n == 1:
+        return np.array([lam1])
+    return 10.0 ** (math.log10(lam1) + math.log10(lam2 / lam1) * np.arange(n) / (n - 1))
+
+
+def read_observations(path, lam, incangle=45.0):
+    """The observations of an MCMax observation file (Telescope.f:583-1100):
+    keywords before the first type= line set the defaults, each type= line
+    starts an observation whose own keywords follow.  Returns a list of
+    dicts with kind, inc [deg], lam1, lam2, nlam, lamfile, nphi, nrad, flag
+    (and the other keywords as given, lower-case).  Defaults: inc from the
+    deck's incangle, lam1/lam2 the model's range, nphi 45, nrad 2."""
+    lam = np.asarray(lam, float)
+    default = dict(inc=float(incangle), lam1=float(lam[0]), lam2=float(lam[-1]), nlam=-1, lamfile="", nphi=45,
+                   nrad=2, flag="")
+    obs, cur = [], default
+    base = os.path.dirname(os.path.abspath(path))
+    with open(path) as f:
+        for line in f:
+            t = line.strip()
+            if not t or t.startswith("*") or "=" not in t:
+                continue
+            key, val = t.split("=", 1)
+            key = key.strip().lower()
+            val = val.strip()
+            if val[:1] in ("'", '"'):
+                val = val[1:-1] if len(val) > 1 and val[-1] == val[0] else val[1:]
+            if key == "type":
+                cur = dict(default, kind=val.upper())
+                obs.append(cur)
+                continue
+            if key in ("nphi", "nrad", "nlam"):
+                cur[key] = int(float(val.replace("d", "e").replace("D", "E")))
+            elif key in ("inc", "lam1", "lam2", "lam"):
+                x = float(val.replace("d", "e").replace("D", "E"))
+                cur["lam1" if key == "lam" else key] = x
+            elif key == "lamfile":
+                cur[key] = val if os.path.isabs(val) else os.path.join(base, val)
+            else:
+                cur[key] = val
+    return obs
 
 
 def _arrinterpol_log(x, xarr, yarr):

@@ -1,7 +1,7 @@
 """Command-line run of the packet loop on an MCMax input deck, writing the
 reference's result files:
 
-    python -m mcmax_b200.run input.in Nphot [-o outdir] [-s key=value]...
+    python -m mcmax_b200.run input.in Nphot [observation files] [-o outdir] [-s key=value]...
                              [--precision mixed|fp64|exact] [--opacity dhs|surrogate]
                              [--spectrum DEG]...
 
@@ -45,12 +45,15 @@ def fixed_radii(zones, rin, rout):
 
 
 def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opacity="dhs", compute_parts=None,
-             spectra=(), spectrum_nphi=45, spectrum_nr=2):
+             spectra=(), spectrum_nphi=45, spectrum_nr=2, observations=()):
     """Build the deck's model, run the packet loop and the diffusion step
     and write the result files; for each inclination in `spectra` [deg]
     also the ray-traced spectrum (mcg_trace_spectrum) as
     spectrum<angle>.dat.  Returns dict(model, run, nphot, result, T,
-    diffused (the counts of mcg_diffuse, or None), structure, files)."""
+    diffused (the counts of mcg_diffuse, or None), structure, files).
+    observations: MCMax observation files; their SPECTRUM observations are
+    ray-traced the same way, other kinds are skipped and listed in
+    'skipped'."""
     if compute_parts is None and opacity == "surrogate":
         compute_parts = _surrogate_parts(ctx)
     elif opacity not in ("dhs", "surrogate"):
@@ -76,21 +79,30 @@ def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opac
     outputs.write_denstemp(files[0], m, T)
     names = outputs.write_mcspec(outdir, m, res, distance_pc=m.distance)
     files += [os.path.join(outdir, x) for x in names + ["MCSpec.dat"]]
-    if spectra:
+    todo = [dict(inc=a, lam1=m.lam[0], lam2=m.lam[-1], nlam=-1, lamfile="", nphi=spectrum_nphi, nrad=spectrum_nr,
+                 flag="") for a in spectra]
+    skipped = []
+    for path in observations:
+        for ob in outputs.read_observations(path, m.lam, run.get("incangle", 45.0)):
+            (todo if ob["kind"] == "SPECTRUM" else skipped).append(ob)
+    if todo:
         import math
-        lam_obs = outputs.spectrum_wavelengths(m.lam, m.lam[0], m.lam[-1])
         rfix = fixed_radii(run["zones"], m.R[1], m.R[-1])
-        for ang in spectra:
-            flux, _ = ctx.trace_spectrum(T, lam_obs, math.radians(ang), nphi=spectrum_nphi, nr=spectrum_nr,
+        for ob in todo:
+            lam_obs = outputs.spectrum_wavelengths(m.lam, ob["lam1"], ob["lam2"], ob["nlam"], ob["lamfile"] or None)
+            flux, _ = ctx.trace_spectrum(T, lam_obs, math.radians(ob["inc"]), nphi=ob["nphi"], nr=ob["nrad"],
                                          Rfix=rfix)
-            files.append(outputs.write_spectrum(outdir, ang, lam_obs, flux, m.lam, m.Fstar, m.distance))
-    return dict(model=m, run=run, nphot=n, result=res, T=T, diffused=diffused, structure=structure, files=files)
+            files.append(outputs.write_spectrum(outdir, ob["inc"], lam_obs, flux, m.lam, m.Fstar, m.distance,
+                                                flag=ob["flag"]))
+    return dict(model=m, run=run, nphot=n, result=res, T=T, diffused=diffused, structure=structure, files=files,
+                skipped=[ob["kind"] for ob in skipped])
 
 
 def parse_args(argv):
     ap = argparse.ArgumentParser(prog="python -m mcmax_b200.run", description=__doc__.split("\n\n")[0])
     ap.add_argument("deck")
     ap.add_argument("nphot", type=lambda s: int(float(s)))
+    ap.add_argument("observations", nargs="*", help="MCMax observation files (SPECTRUM observations are traced)")
     ap.add_argument("-o", dest="outdir", default=".")
     ap.add_argument("-s", dest="overrides", action="append", default=[], metavar="key=value")
     ap.add_argument("--precision", choices=("mixed", "fp64", "exact"), default="mixed")
@@ -111,7 +123,7 @@ def main(argv=None, context=None):
     ctx = context(a.device)
     try:
         r = run_deck(ctx, a.deck, a.nphot, a.outdir, a.overrides, a.precision, a.opacity, spectra=a.spectra,
-                     spectrum_nphi=a.spectrum_nphi, spectrum_nr=a.spectrum_nr)
+                     spectrum_nphi=a.spectrum_nphi, spectrum_nr=a.spectrum_nr, observations=a.observations)
     finally:
         ctx.close()
     print("packets %d, %d cells, T %.1f-%.1f K, wrote %s" % (r["nphot"], r["T"].size, r["T"].min(), r["T"].max(),

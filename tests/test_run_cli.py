@@ -114,8 +114,28 @@ def test_command_line_runs_the_deck_and_writes_result_files(tmp_path):
     assert m.scat_how == 1 and m.bins[0][0] == 0.1 and abs(m.bins[-1][1] - 0.5) < 1e-12
 
 
+def test_observation_files_drive_spectra(tmp_path):
+    deck = _write_inputs(tmp_path)
+    (tmp_path / "Spectrum.out").write_text("nphi=30\nnrad=1\n*****\ntype='SPECTRUM'\ninc=60\nflag='_a'\n"
+                                           "type='IMAGE'\nlam=0.6\ntype='SPECTRUM'\nlam1=1\nlam2=100\nnlam=5\n")
+    made = []
+
+    def factory(device):
+        made.append(FakeContext(device))
+        return made[-1]
+
+    r = R.main([deck, "1e3", str(tmp_path / "Spectrum.out"), "-o", str(tmp_path / "o")], context=factory)
+    names = [os.path.basename(f) for f in r["files"] if "spectrum" in f]
+    assert names == ["spectrum60.0_a.dat", "spectrum45.0.dat"]
+    assert r["skipped"] == ["IMAGE"]
+    rows = np.loadtxt(str(tmp_path / "o" / "spectrum45.0.dat"))
+    assert rows.shape[0] == 5 and np.allclose(rows[[0, -1], 0], [1.0, 100.0])
+    assert made[0].trace_args[1:3] == (30, 1)
+
+
 def test_command_line_arguments():
     a = R.parse_args(["x.in", "1e6"])
     assert (a.nphot, a.outdir, a.overrides, a.precision, a.opacity) == (1000000, ".", [], "mixed", "dhs")
-    a = R.parse_args(["x.in", "300", "-o", "o", "-s", "a=1", "-s", "b=2", "--opacity", "surrogate"])
-    assert (a.nphot, a.outdir, a.overrides, a.opacity) == (300, "o", ["a=1", "b=2"], "surrogate")
+    a = R.parse_args(["x.in", "300", "obs.out", "-o", "o", "-s", "a=1", "-s", "b=2", "--opacity", "surrogate"])
+    assert (a.nphot, a.outdir, a.overrides, a.opacity, a.observations) == (300, "o", ["a=1", "b=2"], "surrogate",
+                                                                            ["obs.out"])
