@@ -751,11 +751,11 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
     if denstype == "FILE":
         # the dust density of a denstemp file and the grid rebuilt from its
         # cell centres (Init.f:2727-2752, readstruct InputOutput.f:579)
-        from .outputs import read_denstemp
+        from .outputs import read_denstemp, read_denstemp_fits
         dfile = v("densfile", "", str)
         if not os.path.isabs(dfile):
             dfile = os.path.join(base, dfile)
-        dt = read_denstemp(dfile)
+        dt = read_denstemp_fits(dfile) if ".fits" in os.path.basename(dfile) else read_denstemp(dfile)
         R, Theta, thet, SinTheta = grid_from_centres(rstar_cm, rin, rout, dt["r_av"], dt["theta_av"])
         V = cell_volumes(R, Theta)
         dens = np.full(V.shape, 1e-60)
@@ -795,7 +795,7 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
                nphotdiffuse=v("nphotdiffuse", 25, int), dtdiffuse=v("dtdiffuse", 1.0),
                zones=[(z["rin"], z["rout"], z["sh"], z["rsh"], z["shpow"], z["denspow"], z["fix"]) for z in zones],
                Mstar=v("mstar", 2.5) * MSUN, maxiter=v("maxiter", 10, int), epsiter=v("epsiter", 3.0),
-               incangle=v("incangle", 45.0))
+               incangle=v("incangle", 45.0), outputfits=v("outputfits", False, bool))
     return m, run
 
 

@@ -6,6 +6,10 @@ that MCMax's own readers and plotting scripts take them unchanged.
                                           DENS, TEMP, COMP, GASDENS, DENS0 as
                                           Main.f:605 writes it)
     read_denstemp(path)                   the same file back
+    write_denstemp_fits(path, model, T)   denstemp.fits.gz, the same arrays as
+                                          FITS images (outputstruct_fits,
+                                          InputOutput.f:230-574)
+    read_denstemp_fits(path)              the same file back
     write_mcspec(outdir, model, result)   MCSpec<angle>.dat per inclination
                                           bin and MCSpec.dat
                                           (MCRadiation.f:738-762)
@@ -112,6 +116,68 @@ def read_denstemp(path):
     gas = block()
     dens0 = block()
     return dict(r_av=r_av, theta_av=th, dens=dens, T=T, comp=comp, gasdens=gas, dens0=dens0, ngrains=ng)
+
+
+def write_denstemp_fits(path, model, T, dens0=None, gas2dust=100.0, rin=None, rout=None, nlam=None):
+    """denstemp.fits(.gz) as outputstruct_fits writes it (InputOutput.f:230-
+    574) for DENS, TEMP, COMP, GASDENS, DENS0: a primary image (nR-1) x
+    (nTheta-1) x 2 of the cell-centre radius [AU] and angle, with the
+    keywords RIN, ROUT, NR, NTHETA, NGRAINS, NGRAINS2, NLAM, NHDU and
+    'HDU n' naming the extensions, then one image per quantity (COMP: w and
+    wopac, (nR-1) x (nTheta-1) x ngrains x 2).  A name ending in .fits gets
+    .gz as in the reference."""
+    from . import particle_fits as PF
+    if path.endswith(".fits"):
+        path = path + ".gz"
+    nr, nc, ng = model.nr, model.nt - 1, model.ncomp
+    dens = np.asarray(model.dens, float).reshape(nr, nc)[1:]
+    T = np.asarray(T, float).reshape(nr, nc)[1:]
+    comp = np.asarray(model.comp_w, float).reshape(nr, nc, ng)[1:]
+    d0 = dens if dens0 is None else np.asarray(dens0, float).reshape(nr, nc)[1:]
+    r_av = _r_av_cm(model.R)[1:] / M.AU
+    th = M.theta_centres(nc)
+    vars_ = ["DENS", "TEMP", "COMP", "GASDENS", "DENS0"]
+    cards = [PF._card("SIMPLE", True, "file does conform to FITS standard"),
+             PF._card("BITPIX", -64, "number of bits per data pixel"), PF._card("NAXIS", 3, "number of data axes"),
+             PF._card("NAXIS1", nr - 1, "length of data axis 1"), PF._card("NAXIS2", nc, "length of data axis 2"),
+             PF._card("NAXIS3", 2, "length of data axis 3"),
+             PF._card("EXTEND", True, "FITS dataset may contain extensions"),
+             PF._card("Rin", float(model.R[1] if rin is None else rin), "[AU]"),
+             PF._card("Rout", float(model.R[-1] if rout is None else rout), "[AU]"),
+             PF._card("nR", nr - 1), PF._card("nTheta", nc), PF._card("ngrains", ng), PF._card("ngrains2", 1),
+             PF._card("nlam", int(model.nlam if nlam is None else nlam)), PF._card("nHDU", len(vars_))]
+    cards += [PF._card("HDU%2d" % (i + 1), v) for i, v in enumerate(vars_)]
+    grid = np.stack([np.broadcast_to(r_av[None, :], (nc, nr - 1)), np.broadcast_to(th[:, None], (nc, nr - 1))])
+    raw = PF._header(cards) + PF._data(grid)
+    comp4 = np.stack([comp.transpose(2, 1, 0), np.ones((ng, nc, nr - 1))])      # (2, ng, nc, nr-1)
+    blocks = {"DENS": dens.T, "TEMP": T.T, "COMP": comp4, "GASDENS": (d0 * gas2dust).T, "DENS0": d0.T}
+    for v in vars_:
+        a = blocks[v]
+        ext = [PF._card("XTENSION", "IMAGE", "IMAGE extension"), PF._card("BITPIX", -64),
+               PF._card("NAXIS", a.ndim)]
+        ext += [PF._card("NAXIS%d" % (k + 1), a.shape[a.ndim - 1 - k]) for k in range(a.ndim)]
+        ext += [PF._card("PCOUNT", 0), PF._card("GCOUNT", 1)]
+        raw += PF._header(ext) + PF._data(a)
+    import gzip
+    with open(path, "wb") as f:
+        f.write(gzip.compress(raw) if path.endswith(".gz") else raw)
+    return path
+
+
+def read_denstemp_fits(path):
+    """dict as read_denstemp from a denstemp.fits(.gz) file"""
+    from . import particle_fits as PF
+    hdus = PF._read_hdus(PF._open(path))
+    hdr, grid = hdus[0]
+    names = [str(hdr.get("HDU%2d" % (i + 1), "")).strip() for i in range(int(hdr.get("NHDU", len(hdus) - 1)))]
+    out = dict(r_av=grid[0, 0, :] * M.AU, theta_av=grid[1, :, 0], ngrains=int(hdr["NGRAINS"]))
+    key = {"DENS": "dens", "TEMP": "T", "GASDENS": "gasdens", "DENS0": "dens0"}
+    for name, (h, a) in zip(names, hdus[1:]):
+        if name == "COMP":
+            out["comp"] = a[0].transpose(2, 1, 0)
+        elif name in key:
+            out[key[name]] = a.T
+    return out
 
 
 def mcspec_name(j, nangle=30):

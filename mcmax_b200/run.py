@@ -75,8 +75,11 @@ def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opac
         if run["nphotdiffuse"] > 0 or run["dtdiffuse"] < 1.0:
             T, _, diffused = ctx.diffuse(res["Ni"], dT, T, run["nphotdiffuse"], run["dtdiffuse"], run["factRW"])
     os.makedirs(outdir, exist_ok=True)
-    files = [os.path.join(outdir, "denstemp.dat")]
-    outputs.write_denstemp(files[0], m, T)
+    if run.get("outputfits"):
+        files = [outputs.write_denstemp_fits(os.path.join(outdir, "denstemp.fits.gz"), m, T)]
+    else:
+        files = [os.path.join(outdir, "denstemp.dat")]
+        outputs.write_denstemp(files[0], m, T)
     names = outputs.write_mcspec(outdir, m, res, distance_pc=m.distance)
     files += [os.path.join(outdir, x) for x in names + ["MCSpec.dat"]]
     todo = [dict(inc=a, lam1=m.lam[0], lam2=m.lam[-1], nlam=-1, lamfile="", nphi=spectrum_nphi, nrad=spectrum_nr,

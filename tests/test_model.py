@@ -156,7 +156,7 @@ idum=-7
     assert zones == [(0.5, 100.0, 0.0707, 1.0, 1.125, 1.0, False)]
     assert abs(run.pop("Mstar") / (2.5 * M.MSUN) - 1) < 1e-15
     assert run == dict(seed=7, randomwalk=True, factRW=5.0, maxinteract=20000, nruns=1, nphotdiffuse=25,
-                       dtdiffuse=1.0, maxiter=10, epsiter=3.0, incangle=45.0)
+                       dtdiffuse=1.0, maxiter=10, epsiter=3.0, incangle=45.0, outputfits=False)
     assert np.allclose(m.comp_w.sum(1), 1.0)
     ref = M.disk_model(None, nrad=12, ntheta=8, nlam=20, lam2=3000.0, mdust=1e-5, sh=0.0707, ngrains=3,
                        opacities=(m.Kabs, m.Ksca, m.F))
@@ -242,3 +242,27 @@ def test_deck_model_file_density_restarts_from_denstemp(tmp_path):
     assert np.array_equal(b.dens.reshape(b.nr, nc)[1:], a.dens.reshape(a.nr, nc)[1:])
     assert np.allclose(b.R, a.R, rtol=1e-12) and np.allclose(b.Theta, a.Theta, rtol=0, atol=1e-14)
     assert np.allclose(b.V, a.V, rtol=1e-10)
+
+
+def test_deck_model_file_density_from_fits(tmp_path):
+    import oracle_ffi as O
+    from mcmax_b200 import outputs as OUT
+    lam_tab = np.geomspace(0.05, 5000.0, 80)
+    n, k = M.synthetic_lnk(lam_tab, 0.03)
+    (tmp_path / "syn.lnk").write_text("".join("%g %g %g\n" % t for t in zip(lam_tab, n, k)))
+    (tmp_path / "dust.particle").write_text("1\n1\n'syn.lnk'\n1.0 3.0\n")
+    common = "rin=0.5\nrout=100\nnlam=12\ncomputepart01:file='dust.particle'\n"
+    (tmp_path / "a.in").write_text(common + "nrad=9\nntheta=8\nzone1:rin=0.5\nzone1:rout=100\nzone1:fix=.true.\n")
+
+    def oracle_parts(parts):
+        return [O.compute_part(p["lam"], p["e1"][0], p["e2"][0], p["frac"], p["rho"], p["amin"], p["amax"],
+                               p["apow"], p["fmax"], p["blend"], p["porosity"], p["ns"], p["nf"]) for p in parts]
+
+    a, _ = M.deck_model(None, str(tmp_path / "a.in"), compute_parts=oracle_parts)
+    OUT.write_denstemp_fits(str(tmp_path / "denstemp.fits.gz"), a, np.full(a.ncell, 50.0))
+    (tmp_path / "b.in").write_text(common + "denstype='FILE'\ndensfile='denstemp.fits.gz'\noutputfits=.true.\n")
+    b, run = M.deck_model(None, str(tmp_path / "b.in"), compute_parts=oracle_parts)
+    nc = a.nt - 1
+    assert run["outputfits"] is True
+    assert np.array_equal(b.dens.reshape(b.nr, nc)[1:], a.dens.reshape(a.nr, nc)[1:])
+    assert np.allclose(b.R, a.R, rtol=1e-12)

@@ -67,3 +67,20 @@ def test_spectrum_file(tmp_path):
     assert os.path.basename(p2) == "spectrum07.5_b.dat"
     r2 = np.loadtxt(p2)
     assert np.allclose(r2[1:-1, 3], 1e23 * np.exp(np.interp(np.log(lo[1:-1]), np.log(lam), np.log(Fstar))) / d2)
+
+
+def test_denstemp_fits_round_trip(tmp_path):
+    m = models.small_disk(nrad=10, ntheta=8, nlam=12, mdust=1e-5)
+    T = np.linspace(10.0, 500.0, m.ncell)
+    p = OUT.write_denstemp_fits(str(tmp_path / "denstemp.fits"), m, T)
+    assert p.endswith(".fits.gz") and os.path.exists(p)
+    d = OUT.read_denstemp_fits(p)
+    OUT.write_denstemp(str(tmp_path / "denstemp.dat"), m, T)
+    t = OUT.read_denstemp(str(tmp_path / "denstemp.dat"))
+    for k in ("dens", "T", "gasdens", "dens0", "comp"):
+        assert np.array_equal(d[k], t[k]), k
+    assert np.allclose(d["r_av"], t["r_av"], rtol=1e-15) and np.array_equal(d["theta_av"], t["theta_av"])
+    from mcmax_b200 import particle_fits as PF
+    hdr = PF._read_hdus(PF._open(p))[0][0]
+    assert (hdr["NR"], hdr["NTHETA"], hdr["NGRAINS"], hdr["NHDU"]) == (m.nr - 1, m.nt - 1, m.ncomp, 5)
+    assert hdr["HDU 3"] == "COMP"
