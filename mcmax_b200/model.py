@@ -638,8 +638,9 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
     computepartNN:file (particle file: ns, nf, then per material an .lnk
     path and 'frac rho'), amin, amax, apow, fmax, ngrains, blend,
     porosity, norm_abun, standard ('FILE'), with amin, amax, apow (micron)
-    as the deck-wide defaults; abunNN (relative mass of computepart entry
-    NN); fixmpset, alphaturb (settling of a one-zone
+    as the deck-wide defaults; fitspartNN (a particle FITS file) and opacNN
+    (an opacity table) as grains taken as given; abunNN (relative mass of
+    grain entry NN); fixmpset, alphaturb (settling of a one-zone
     disk); denstype 'FILE' with densfile (a denstemp.dat: its dust density
     and the grid rebuilt from its cell centres; rin and rout still give the
     outer edges); randomwalk, factrw, maxinteract, nruns, idum; nphotdiffuse,
@@ -694,16 +695,41 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
     if not zones and denstype == "ZONES":
         raise ValueError("no zoneN:* keywords")
     # grain bins of every computepart entry (Init.f:746-789, 1323-1420)
-    entries = sorted({int(k[len("computepart"):k.index(":")]) for k in d if k.startswith("computepart")
-                      and ":" in k})
+    # grains by index NN: computepartNN:* (computed, then split into size
+    # bins), fitspartNN (a particle FITS file, ReadParticleFits) and opacNN
+    # (an opacity table, readopacity) (Init.f:697-740, 3333-3400)
+    kinds = {}
+    for k in d:
+        if k.startswith("computepart") and ":" in k and k[11:k.index(":")].isdigit():
+            kinds[int(k[11:k.index(":")])] = "computepart"
+        elif k.startswith("fitspart") and k[8:].isdigit():
+            kinds[int(k[8:])] = "fitspart"
+        elif k.startswith("opac") and k[4:].isdigit():
+            kinds[int(k[4:])] = "opac"
+    entries = sorted(kinds)
     if not entries:
-        raise ValueError("no computepartNN:* keywords")
+        raise ValueError("no grains: computepartNN:*, fitspartNN or opacNN keywords")
     rstar_cm = rstar * RSUN
     lam, nu = wavelength_grid(lam1, lam2, nlam)
-    parts, weights = [], []
+    parts, weights, slots = [], [], []
     abun = np.array([v("abun%02d" % e, v("abun%d" % e, 1.0)) for e in entries])
     abun = abun / abun.sum()
+
+    def path_of(val):
+        return val if os.path.isabs(val) else os.path.join(base, val)
+
     for e, ab in zip(entries, abun):
+        if kinds[e] != "computepart":
+            key = ("%s%02d" % (kinds[e], e)) if ("%s%02d" % (kinds[e], e)) in d else "%s%d" % (kinds[e], e)
+            from . import particle_fits as PF
+            if kinds[e] == "fitspart":
+                r = PF.read_particle_fits(path_of(v(key, "", str)), lam)
+            else:
+                r = PF.read_opacity_file(path_of(v(key, "", str)), lam)
+                r.update(rho_av=float("nan"), rv=float("nan"), amin=float("nan"), amax=float("nan"))
+            slots.append(("file", r))
+            weights.append(ab)
+            continue
         kp = "computepart%02d:" % e if any(k.startswith("computepart%02d:" % e) for k in d) else \
             "computepart%d:" % e
         if v(kp + "standard", "FILE", str).upper() != "FILE":
@@ -711,9 +737,7 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
         pfile = v(kp + "file", None, str)
         if not pfile:
             raise ValueError(kp + "file missing")
-        if not os.path.isabs(pfile):
-            pfile = os.path.join(base, pfile)
-        ns, nf, mats = read_particle_file(pfile)
+        ns, nf, mats = read_particle_file(path_of(pfile))
         e1, e2, frac, rho = [], [], [], []
         for lnk, fr, rh in mats:
             n_, k_ = readrefind(lnk, lam)
@@ -735,12 +759,22 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
         rg = [math.sqrt(a * b) * 1e-4 for a, b in bins]
         wmrn = mrn_abundances(rg, amin * 1e-4, amax * 1e-4, apow) if ngr > 1 else np.ones(1)
         for (a, b), wb in zip(bins, wmrn):
+            slots.append(("part", len(parts)))
             parts.append(dict(lam=lam, e1=np.array(e1), e2=np.array(e2), frac=np.array(frac), rho=np.array(rho),
                               amin=a, amax=b, apow=apow, fmax=v(kp + "fmax", 0.0), porosity=v(kp + "porosity", 0.25),
                               blend=v(kp + "blend", True, bool), ns=ns, nf=nf,
                               normalize_abun=v(kp + "norm_abun", -1.0)))
             weights.append(ab * wb)
-    res = (compute_parts or ctx.compute_part_batch)(parts)
+    computed = (compute_parts or ctx.compute_part_batch)(parts) if parts else []
+    res, grain_info = [], []
+    for kind, x in slots:
+        if kind == "part":
+            p = parts[x]
+            res.append(computed[x])
+            grain_info.append(((p["amin"], p["amax"]), grain_rv(p["amin"], p["amax"], p["apow"], p["ns"])))
+        else:
+            res.append(x)
+            grain_info.append(((x["amin"], x["amax"]), x["rv"]))
     Kabs = np.array([r["kabs"] for r in res])
     Ksca = np.array([r["ksca"] for r in res])
     F = np.array([r["F"] for r in res])
@@ -783,13 +817,15 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
     if v("fixmpset", False, bool):
         if len(zones) != 1:
             raise ValueError("fixmpset: settling of a one-zone disk")
-        rv = np.array([grain_rv(p["amin"], p["amax"], p["apow"], p["ns"]) for p in parts])
+        rv = np.array([g[1] for g in grain_info])
         rho_g = np.array([r["rho_av"] for r in res])
+        if not (np.all(np.isfinite(rv)) and np.all(np.isfinite(rho_g))):
+            raise ValueError("fixmpset: an opacNN grain has no size or density to settle")
         dens, w = fixed_mp_settling(R, Theta, ntheta, dens, V, w, rho_g, rv, v("alphaturb", 1e-4), zones[0])
     m = Model(nr=nr, nt=nt, R=R, Theta=Theta, SinTheta=SinTheta, thet=thet, dens=dens.reshape(-1), V=V.reshape(-1),
-              ncomp=len(parts), comp_w=w.reshape(nr * (nt - 1), len(parts)), nlam=nlam, lam=lam, nu=nu, Kabs=Kabs,
+              ncomp=len(res), comp_w=w.reshape(nr * (nt - 1), len(res)), nlam=nlam, lam=lam, nu=nu, Kabs=Kabs,
               Ksca=Ksca, F=F, BB=BB, Fstar=Fstar, Lstar=Lstar, Tstar=tstar, Rstar_cm=rstar_cm, scat_how=scat,
-              bins=[(p["amin"], p["amax"]) for p in parts], w=w0, distance=v("distance", 100.0))
+              bins=[g[0] for g in grain_info], w=w0, distance=v("distance", 100.0))
     run = dict(seed=abs(v("idum", -42, int)), randomwalk=v("randomwalk", False, bool), factRW=v("factrw", 10.0),
                maxinteract=v("maxinteract", 1000000, int), nruns=v("nruns", 1, int),
                nphotdiffuse=v("nphotdiffuse", 25, int), dtdiffuse=v("dtdiffuse", 1.0),

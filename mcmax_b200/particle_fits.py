@@ -262,25 +262,19 @@ def check_particle_file(path, amin, amax, apow, ns, fmax, blend, porosity, frac,
     return True
 
 
-def read_particle_fits(path, lam):
-    """ReadParticleFits without the Rayleigh and Henyey-Greenstein options:
-    the file's opacities and matrices on the wavelength grid lam.
-
-    Below the file's first wavelength the first entry is taken; inside its
-    range every quantity (Kext too) is linear in wavelength between the
-    bracketing entries; beyond its last wavelength Ksca falls as lam^-4,
-    Kabs as lam^-2, Kext = Kabs + Ksca and F is held.  Every matrix is then
-    renormalised so that sum F11 sin(theta) = sum sin(theta) over the 180
-    bins.  Returns dict(kabs, ksca, kext, F (nlam, 6, 180), rho_av, a1, a2,
-    a3, rv [cm])."""
-    (hdr, a), (_, m) = _read_hdus(_open(path))[:2]
+def _regrid(L, Kx, Ka, Ks, M, lam):
+    """opacities and matrices of a tabulated grain on the wavelength grid
+    lam, as ReadParticleFits (ReadParticleFits.f:112-222) and readopacity
+    (Init.f:4929-4972) regrid them: below the table's first wavelength the
+    first entry; inside, linear in wavelength between the bracketing entries
+    (Kext too); beyond the last, Ksca ~ lam^-4, Kabs ~ lam^-2, Kext = Kabs +
+    Ksca and F held; then every matrix renormalised so that sum F11
+    sin(theta) = sum sin(theta) over the 180 bins.  M: (nl, 6, 180)."""
     lam = np.asarray(lam, float)
     nlam = lam.size
-    L, Kx, Ka, Ks = a
-    M = m.transpose(2, 1, 0)                       # (nl_read, 6, 180)
-    nl = L.size
     kext, kabs, ksca = np.zeros(nlam), np.zeros(nlam), np.zeros(nlam)
     F = np.zeros((nlam, 6, NANG))
+    nl = L.size
     i = 0
     while i < nlam and L[0] >= lam[i]:
         kext[i], kabs[i], ksca[i], F[i] = Kx[0], Ka[0], Ks[0], M[0]
@@ -301,13 +295,55 @@ def read_particle_fits(path, lam):
         kext[j] = kabs[j] + ksca[j]
         F[j] = F[i - 1]
     elif i == 0:
-        raise ValueError("%s: the wavelength grid starts above the file's range" % path)
+        raise ValueError("the wavelength grid starts above the table's range")
     s = np.sin(math.pi * (np.arange(1, NANG + 1) - 0.5) / 180.0)
     tot = (F[:, 0, :] * s).sum(1)
     F *= (s.sum() / tot)[:, None, None]
+    return kext, kabs, ksca, F
+
+
+def read_particle_fits(path, lam):
+    """ReadParticleFits without the Rayleigh and Henyey-Greenstein options:
+    the file's opacities and matrices on the wavelength grid lam (see
+    _regrid).  Returns dict(kabs, ksca, kext, F (nlam, 6, 180), rho_av, a1,
+    a2, a3, rv [cm])."""
+    (hdr, a), (_, m) = _read_hdus(_open(path))[:2]
+    L, Kx, Ka, Ks = a
+    kext, kabs, ksca, F = _regrid(L, Kx, Ka, Ks, m.transpose(2, 1, 0), lam)
     a2 = float(hdr["A2"])
     return dict(kabs=kabs, ksca=ksca, kext=kext, F=F, rho_av=float(hdr["DENSITY"]), a1=float(hdr["A1"]), a2=a2,
-                a3=float(hdr["A3"]), rv=math.sqrt(a2) * 1e-4)
+                a3=float(hdr["A3"]), rv=math.sqrt(a2) * 1e-4, amin=float(hdr.get("R_MIN", float("nan"))),
+                amax=float(hdr.get("R_MAX", float("nan"))))
+
+
+def rayleigh_matrix():
+    """the scattering matrix readopacity gives a tabulated grain
+    (Init.f:4920-4927): Rayleigh-like, (6, 180)"""
+    th = (np.arange(1, NANG + 1) - 0.5) * math.pi / 180.0
+    c = np.cos(th)
+    return np.stack([(1 + c * c) / 2, -(1 - c * c) / 2, (1 + c * c) / 2, c, np.zeros(NANG), c])
+
+
+def read_opacity_file(path, lam):
+    """readopacity (Init.f:4886-4990): an ASCII table of wavelength
+    [micron], Kext, Kabs, Ksca [cm^2/g] per line, with the Rayleigh-like
+    matrix, on the wavelength grid lam.  Returns dict(kabs, ksca, kext, F)."""
+    rows = []
+    with open(path) as f:
+        for line in f:
+            parts = line.replace("d", "e").replace("D", "E").split()
+            if len(parts) < 4:
+                continue
+            try:
+                rows.append([float(x) for x in parts[:4]])
+            except ValueError:
+                continue
+    if len(rows) < 2:
+        raise ValueError("%s: fewer than two wavelengths" % path)
+    t = np.array(rows)
+    M = np.broadcast_to(rayleigh_matrix(), (t.shape[0], 6, NANG))
+    kext, kabs, ksca, F = _regrid(t[:, 0], t[:, 1], t[:, 2], t[:, 3], M, lam)
+    return dict(kabs=kabs, ksca=ksca, kext=kext, F=F)
 
 
 def find_particle_file(particledir, ii, amin, amax, apow, ns, fmax, blend, porosity, frac, rho, lnkfiles, iopac=1,

@@ -266,3 +266,35 @@ def test_deck_model_file_density_from_fits(tmp_path):
     assert run["outputfits"] is True
     assert np.array_equal(b.dens.reshape(b.nr, nc)[1:], a.dens.reshape(a.nr, nc)[1:])
     assert np.allclose(b.R, a.R, rtol=1e-12)
+
+
+def test_deck_grains_from_particle_fits_and_opacity_tables(tmp_path):
+    import oracle_ffi as O
+    from mcmax_b200 import particle_fits as PF
+    lam_tab = np.geomspace(0.05, 5000.0, 80)
+    n, k = M.synthetic_lnk(lam_tab, 0.03)
+    (tmp_path / "syn.lnk").write_text("".join("%g %g %g\n" % t for t in zip(lam_tab, n, k)))
+    (tmp_path / "dust.particle").write_text("2\n2\n'syn.lnk'\n1.0 3.0\n")
+    common = "rin=0.5\nrout=100\nnrad=8\nntheta=6\nnlam=14\nzone1:rin=0.5\nzone1:rout=100\nzone1:fix=.true.\n"
+    (tmp_path / "a.in").write_text(common + "computepart01:file='dust.particle'\ncomputepart01:amin=0.2\n"
+                                   "computepart01:amax=0.8\n")
+
+    def oracle_parts(parts):
+        return [O.compute_part(p["lam"], p["e1"][0], p["e2"][0], p["frac"], p["rho"], p["amin"], p["amax"],
+                               p["apow"], p["fmax"], p["blend"], p["porosity"], p["ns"], p["nf"]) for p in parts]
+
+    a, _ = M.deck_model(None, str(tmp_path / "a.in"), compute_parts=oracle_parts)
+    # the particle cache file of that grain, and an opacity table of it
+    res = dict(kabs=a.Kabs[0], ksca=a.Ksca[0], kext=a.Kabs[0] + a.Ksca[0], F=a.F[0], rho_av=2.25)
+    PF.write_particle_fits(str(tmp_path / "p.fits.gz"), a.lam, res, 0.2, 0.8, 3.5, 0.0, True, 0.25, [1.0], [3.0],
+                           ["syn.lnk"], 2)
+    (tmp_path / "o.dat").write_text("".join("%.17e %.17e %.17e %.17e\n" % (l, ka + ks, ka, ks)
+                                            for l, ka, ks in zip(a.lam, a.Kabs[0], a.Ksca[0])))
+    (tmp_path / "b.in").write_text(common + "fitspart01='p.fits.gz'\nopac02='o.dat'\nabun01=3\nabun02=1\n")
+    b, _ = M.deck_model(None, str(tmp_path / "b.in"), compute_parts=oracle_parts)
+    assert b.ncomp == 2 and np.allclose(b.comp_w[0], [0.75, 0.25])
+    assert np.array_equal(b.Kabs[0], a.Kabs[0]) and np.array_equal(b.Ksca[1], a.Ksca[0])
+    assert np.allclose(b.F[0], a.F[0], rtol=1e-12, atol=1e-300)
+    s = np.sin(np.pi * (np.arange(1, 181) - 0.5) / 180.0)
+    assert np.allclose((b.F[1][:, 0, :] * s).sum(1), s.sum(), rtol=1e-13)      # the normalised Rayleigh matrix
+    assert np.allclose(b.bins[0], (0.2, 0.8), rtol=1e-7)      # R_MIN, R_MAX of the file (single precision)
