@@ -638,8 +638,9 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
     computepartNN:file (particle file: ns, nf, then per material an .lnk
     path and 'frac rho'), amin, amax, apow, fmax, ngrains, blend,
     porosity, norm_abun, standard ('FILE'), with amin, amax, apow (micron)
-    as the deck-wide defaults; fitspartNN (a particle FITS file) and opacNN
-    (an opacity table) as grains taken as given; abunNN (relative mass of
+    as the deck-wide defaults; fitspartNN (a particle FITS file), partNN (an
+    ASCII particle file) and opacNN (an opacity table) as grains taken as
+    given; abunNN (relative mass of
     grain entry NN); fixmpset, alphaturb (settling of a one-zone
     disk); denstype 'FILE' with densfile (a denstemp.dat: its dust density
     and the grid rebuilt from its cell centres; rin and rout still give the
@@ -696,8 +697,9 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
         raise ValueError("no zoneN:* keywords")
     # grain bins of every computepart entry (Init.f:746-789, 1323-1420)
     # grains by index NN: computepartNN:* (computed, then split into size
-    # bins), fitspartNN (a particle FITS file, ReadParticleFits) and opacNN
-    # (an opacity table, readopacity) (Init.f:697-740, 3333-3400)
+    # bins), fitspartNN (a particle FITS file, ReadParticleFits), opacNN (an
+    # opacity table, readopacity) and partNN (an ASCII particle file,
+    # readparticle) (Init.f:697-740, 3333-3400)
     kinds = {}
     for k in d:
         if k.startswith("computepart") and ":" in k and k[11:k.index(":")].isdigit():
@@ -706,6 +708,8 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
             kinds[int(k[8:])] = "fitspart"
         elif k.startswith("opac") and k[4:].isdigit():
             kinds[int(k[4:])] = "opac"
+        elif k.startswith("part") and k[4:].isdigit():
+            kinds[int(k[4:])] = "part"
     entries = sorted(kinds)
     if not entries:
         raise ValueError("no grains: computepartNN:*, fitspartNN or opacNN keywords")
@@ -725,7 +729,8 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
             if kinds[e] == "fitspart":
                 r = PF.read_particle_fits(path_of(v(key, "", str)), lam)
             else:
-                r = PF.read_opacity_file(path_of(v(key, "", str)), lam)
+                read = PF.read_opacity_file if kinds[e] == "opac" else PF.read_particle_ascii
+                r = read(path_of(v(key, "", str)), lam)
                 r.update(rho_av=float("nan"), rv=float("nan"), amin=float("nan"), amax=float("nan"))
             slots.append(("file", r))
             weights.append(ab)

@@ -4,6 +4,7 @@ has computed before instead of computing them again, and so that MCMax
 itself reads the files this library writes.
 
     particle_file_name(dir, ii, iopac, frac, abun_in_name)   ComputePart.f:161-187, 906-938
+    read_opacity_file(path, lam), read_particle_ascii(...)   readopacity, readparticle (Init.f:4664-4990)
     dust_moments(amin, amax, apow, ns)                       ComputePart.f:276-292, 950-976
     write_particle_fits(path, lam, res, ...)                 ParticleFITS, ComputePart.f:884-1093
     check_particle_file(path, ...)                           checkparticlefile, ComputePart.f:559-688
@@ -343,6 +344,45 @@ def read_opacity_file(path, lam):
     t = np.array(rows)
     M = np.broadcast_to(rayleigh_matrix(), (t.shape[0], 6, NANG))
     kext, kabs, ksca, F = _regrid(t[:, 0], t[:, 1], t[:, 2], t[:, 3], M, lam)
+    return dict(kabs=kabs, ksca=ksca, kext=kext, F=F)
+
+
+def read_particle_ascii(path, lam):
+    """readparticle (Init.f:4664-4780): an ASCII particle file of records
+    'wavelength Kext Kabs Ksca' followed by F11, F12, F22, F33, F34, F44 of
+    180 values each.  As the reference's list-directed reads, every read
+    starts on a new line and takes as many lines as its values need, the
+    rest of its last line unread.  Regridded as _regrid.  Returns dict(kabs,
+    ksca, kext, F)."""
+    with open(path) as f:
+        lines = [ln.replace("d", "e").replace("D", "E").split() for ln in f]
+    lines = [ln for ln in lines if ln]
+    k = 0
+    L, Kx, Ka, Ks, Ms = [], [], [], [], []
+    while k < len(lines):
+        head = lines[k]
+        k += 1
+        if len(head) < 4:
+            break
+        M6 = []
+        for _ in range(6):
+            vals = []
+            while len(vals) < NANG and k < len(lines):
+                vals += lines[k]
+                k += 1
+            if len(vals) < NANG:
+                break
+            M6.append([float(x) for x in vals[:NANG]])
+        if len(M6) < 6:
+            break
+        L.append(float(head[0]))
+        Kx.append(float(head[1]))
+        Ka.append(float(head[2]))
+        Ks.append(float(head[3]))
+        Ms.append(M6)
+    if len(L) < 1:
+        raise ValueError("%s: no complete wavelength record" % path)
+    kext, kabs, ksca, F = _regrid(np.array(L), np.array(Kx), np.array(Ka), np.array(Ks), np.array(Ms), lam)
     return dict(kabs=kabs, ksca=ksca, kext=kext, F=F)
 
 

@@ -290,9 +290,18 @@ def test_deck_grains_from_particle_fits_and_opacity_tables(tmp_path):
                            ["syn.lnk"], 2)
     (tmp_path / "o.dat").write_text("".join("%.17e %.17e %.17e %.17e\n" % (l, ka + ks, ka, ks)
                                             for l, ka, ks in zip(a.lam, a.Kabs[0], a.Ksca[0])))
-    (tmp_path / "b.in").write_text(common + "fitspart01='p.fits.gz'\nopac02='o.dat'\nabun01=3\nabun02=1\n")
+    with open(tmp_path / "q.dat", "w") as f:    # the ASCII particle format: 8 values per line for the matrices
+        for li, l in enumerate(a.lam):
+            f.write("%.17e %.17e %.17e %.17e\n" % (l, a.Kabs[0][li] + a.Ksca[0][li], a.Kabs[0][li], a.Ksca[0][li]))
+            for e in range(6):
+                row = a.F[0][li, e]
+                for c0 in range(0, 180, 8):
+                    f.write(" ".join("%.17e" % x for x in row[c0:c0 + 8]) + "\n")
+    (tmp_path / "b.in").write_text(common + "fitspart01='p.fits.gz'\nopac02='o.dat'\npart3='q.dat'\nabun01=3\n"
+                                   "abun02=1\n")
     b, _ = M.deck_model(None, str(tmp_path / "b.in"), compute_parts=oracle_parts)
-    assert b.ncomp == 2 and np.allclose(b.comp_w[0], [0.75, 0.25])
+    assert b.ncomp == 3 and np.allclose(b.comp_w[0], [0.6, 0.2, 0.2])
+    assert np.array_equal(b.Kabs[2], a.Kabs[0]) and np.allclose(b.F[2], a.F[0], rtol=1e-12, atol=1e-300)
     assert np.array_equal(b.Kabs[0], a.Kabs[0]) and np.array_equal(b.Ksca[1], a.Ksca[0])
     assert np.allclose(b.F[0], a.F[0], rtol=1e-12, atol=1e-300)
     s = np.sin(np.pi * (np.arange(1, 181) - 0.5) / 180.0)
