@@ -634,7 +634,9 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
     Keywords used: startype ('PLANCK', or 'FILE' with starfile and lstar
     [Lsun]), tstar, rstar [Rsun]; rin, rout, nrad,
     ntheta; denstype ('ZONES') with zoneN:rin, rout, mdust, denspow, sh,
-    rsh, shpow; lam1, lam2, nlam; scattype (NONE, ISOTROPIC, FULL);
+    rsh, shpow; lam1, lam2, nlam; scattype (NONE, ISOTROPIC, FULL, and
+    RAYLEIGH: the Henyey-Greenstein/Rayleigh matrices of asymNN, asymbNN,
+    wasymbNN, pmaxNN for partNN and fitspartNN grains);
     computepartNN:file (particle file: ns, nf, then per material an .lnk
     path and 'frac rho'), amin, amax, apow, fmax, ngrains, blend,
     porosity, norm_abun, standard ('FILE'), with amin, amax, apow (micron)
@@ -648,7 +650,7 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
     dtdiffuse (the diffusion step after the run); zoneN:fix, mstar,
     maxiter, epsiter (structure iterations).  A value that
     selects physics outside the packet loop (another startype or denstype,
-    scattype RAYLEIGH, tcontact false) raises ValueError.
+    tcontact false) raises ValueError.
 
     deck: a path or the deck text; overrides: 'key=value' strings applied
     after the file (the -s switches).  compute_parts(parts) returns the
@@ -678,9 +680,10 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
         raise ValueError("denstype: 'ZONES' or 'FILE' densities")
     if not v("tcontact", True, bool):
         raise ValueError("tcontact: only thermal contact (Bjorkman-Wood with one temperature per cell)")
-    scat = {"NONE": 0, "ISOTROPIC": 1, "FULL": 2}.get(v("scattype", "ISOTROPIC", str).upper())
+    scattype = v("scattype", "ISOTROPIC", str).upper()
+    scat = {"NONE": 0, "ISOTROPIC": 1, "FULL": 2, "RAYLEIGH": 2}.get(scattype)
     if scat is None:
-        raise ValueError("scattype: NONE, ISOTROPIC or FULL")
+        raise ValueError("scattype: NONE, ISOTROPIC, FULL or RAYLEIGH")
     tstar, rstar = v("tstar", 10000.0), v("rstar", 2.1)
     rin, rout = v("rin", 0.5), v("rout", 1000.0)
     nrad, ntheta = v("nrad", 70, int), v("ntheta", 60, int)
@@ -726,11 +729,20 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
         if kinds[e] != "computepart":
             key = ("%s%02d" % (kinds[e], e)) if ("%s%02d" % (kinds[e], e)) in d else "%s%d" % (kinds[e], e)
             from . import particle_fits as PF
+            mat = None
+            if scattype == "RAYLEIGH" and kinds[e] != "opac":
+                # Henyey-Greenstein / Rayleigh matrices (Init.f:3336-3348, 928-955)
+                mat = PF.rayleigh_hg_matrix(v("asym%02d" % e, v("asym%d" % e, 2.0)),
+                                            v("asymb%02d" % e, v("asymb%d" % e, 2.0)),
+                                            v("wasymb%02d" % e, v("wasymb%d" % e, 0.0)),
+                                            v("pmax%02d" % e, v("pmax%d" % e, 1.0)))
             if kinds[e] == "fitspart":
-                r = PF.read_particle_fits(path_of(v(key, "", str)), lam)
+                r = PF.read_particle_fits(path_of(v(key, "", str)), lam, matrix=mat)
+            elif kinds[e] == "part":
+                r = PF.read_particle_ascii(path_of(v(key, "", str)), lam, matrix=mat)
             else:
-                read = PF.read_opacity_file if kinds[e] == "opac" else PF.read_particle_ascii
-                r = read(path_of(v(key, "", str)), lam)
+                r = PF.read_opacity_file(path_of(v(key, "", str)), lam)
+            if kinds[e] != "fitspart":
                 r.update(rho_av=float("nan"), rv=float("nan"), amin=float("nan"), amax=float("nan"))
             slots.append(("file", r))
             weights.append(ab)

@@ -303,18 +303,51 @@ def _regrid(L, Kx, Ka, Ks, M, lam):
     return kext, kabs, ksca, F
 
 
-def read_particle_fits(path, lam):
-    """ReadParticleFits without the Rayleigh and Henyey-Greenstein options:
-    the file's opacities and matrices on the wavelength grid lam (see
-    _regrid).  Returns dict(kabs, ksca, kext, F (nlam, 6, 180), rho_av, a1,
-    a2, a3, rv [cm])."""
+def read_particle_fits(path, lam, matrix=None):
+    """ReadParticleFits: the file's opacities and matrices on the wavelength
+    grid lam (see _regrid); matrix (6, 180), when given, replaces the file's
+    at every wavelength (the Rayleigh / Henyey-Greenstein option, see
+    rayleigh_hg_matrix).  Returns dict(kabs, ksca, kext, F (nlam, 6, 180),
+    rho_av, a1, a2, a3, rv [cm], amin, amax)."""
     (hdr, a), (_, m) = _read_hdus(_open(path))[:2]
     L, Kx, Ka, Ks = a
-    kext, kabs, ksca, F = _regrid(L, Kx, Ka, Ks, m.transpose(2, 1, 0), lam)
+    M = m.transpose(2, 1, 0) if matrix is None else np.broadcast_to(matrix, (L.size, 6, NANG))
+    kext, kabs, ksca, F = _regrid(L, Kx, Ka, Ks, M, lam)
     a2 = float(hdr["A2"])
     return dict(kabs=kabs, ksca=ksca, kext=kext, F=F, rho_av=float(hdr["DENSITY"]), a1=float(hdr["A1"]), a2=a2,
                 a3=float(hdr["A3"]), rv=math.sqrt(a2) * 1e-4, amin=float(hdr.get("R_MIN", float("nan"))),
                 amax=float(hdr.get("R_MAX", float("nan"))))
+
+
+def hg_binned(g, theta):
+    """HG (Init.f:5594-5612): the Henyey-Greenstein phase function averaged
+    with sin(t) weights over 1000 angles across the one-degree bin at theta,
+    the offsets formed in single precision as there"""
+    n = 1000
+    i = np.arange(1, n + 1, dtype=np.float32)
+    off = ((i - np.float32(1)) / np.float32(n - 1) - np.float32(0.5)) * np.float32(3.1415926536)
+    t = theta + off.astype(np.float64) / 180.0
+    f = (1.0 - g * g) / (1.0 - 2.0 * g * np.cos(t) + g * g) ** 1.5 / 2.0
+    return float(np.sum(f * np.sin(t)) / np.sum(np.sin(t)))
+
+
+def rayleigh_hg_matrix(asym=2.0, asym2=2.0, wasym2=0.0, pmax=1.0):
+    """the matrix readparticle and ReadParticleFits put in place of a file's
+    under scattype 'RAYLEIGH' (Init.f:4689-4707, ReadParticleFits.f:
+    125-143): Henyey-Greenstein F11 (plus wasym2 of a second one) with a
+    Rayleigh-shaped polarisation Pmax when |asym| < 1, else Rayleigh.
+    Returns (6, 180)."""
+    th = (np.arange(1, NANG + 1) - 0.5) * math.pi / 180.0
+    c = np.cos(th)
+    if -1.0 < asym < 1.0:
+        F11 = np.array([hg_binned(asym, x) for x in th])
+        if wasym2 != 0.0:
+            F11 = F11 + wasym2 * np.array([hg_binned(asym2, x) for x in th])
+        F12 = -pmax * F11 * (1.0 - c * c) / (1.0 + c * c)
+    else:
+        F11 = (1.0 + c * c) / 2.0
+        F12 = -(1.0 - c * c) / 2.0
+    return np.stack([F11, F12, F11, c * F11 / (1.0 + c * c), np.zeros(NANG), c * F11 / (1.0 + c * c)])
 
 
 def rayleigh_matrix():
@@ -347,13 +380,13 @@ def read_opacity_file(path, lam):
     return dict(kabs=kabs, ksca=ksca, kext=kext, F=F)
 
 
-def read_particle_ascii(path, lam):
+def read_particle_ascii(path, lam, matrix=None):
     """readparticle (Init.f:4664-4780): an ASCII particle file of records
     'wavelength Kext Kabs Ksca' followed by F11, F12, F22, F33, F34, F44 of
     180 values each.  As the reference's list-directed reads, every read
     starts on a new line and takes as many lines as its values need, the
-    rest of its last line unread.  Regridded as _regrid.  Returns dict(kabs,
-    ksca, kext, F)."""
+    rest of its last line unread.  Regridded as _regrid; matrix as in
+    read_particle_fits.  Returns dict(kabs, ksca, kext, F)."""
     with open(path) as f:
         lines = [ln.replace("d", "e").replace("D", "E").split() for ln in f]
     lines = [ln for ln in lines if ln]
@@ -382,7 +415,8 @@ def read_particle_ascii(path, lam):
         Ms.append(M6)
     if len(L) < 1:
         raise ValueError("%s: no complete wavelength record" % path)
-    kext, kabs, ksca, F = _regrid(np.array(L), np.array(Kx), np.array(Ka), np.array(Ks), np.array(Ms), lam)
+    Ms = np.array(Ms) if matrix is None else np.broadcast_to(matrix, (len(L), 6, NANG))
+    kext, kabs, ksca, F = _regrid(np.array(L), np.array(Kx), np.array(Ka), np.array(Ks), Ms, lam)
     return dict(kabs=kabs, ksca=ksca, kext=kext, F=F)
 
 

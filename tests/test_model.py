@@ -164,7 +164,7 @@ idum=-7
         assert np.allclose(getattr(m, key), getattr(ref, key), rtol=1e-12, atol=0), key
     assert abs(m.Lstar / ref.Lstar - 1) < 1e-12
     with pytest.raises(ValueError):
-        M.deck_model(None, str(deck), overrides=["scattype='RAYLEIGH'"], compute_parts=oracle_parts)
+        M.deck_model(None, str(deck), overrides=["scattype='ANISOTROPIC'"], compute_parts=oracle_parts)
 
 
 def test_read_star_bins_and_interpolates(tmp_path):
@@ -307,3 +307,25 @@ def test_deck_grains_from_particle_fits_and_opacity_tables(tmp_path):
     s = np.sin(np.pi * (np.arange(1, 181) - 0.5) / 180.0)
     assert np.allclose((b.F[1][:, 0, :] * s).sum(1), s.sum(), rtol=1e-13)      # the normalised Rayleigh matrix
     assert np.allclose(b.bins[0], (0.2, 0.8), rtol=1e-7)      # R_MIN, R_MAX of the file (single precision)
+
+
+def test_rayleigh_scattype_matrices_for_file_grains(tmp_path):
+    from mcmax_b200 import particle_fits as PF
+    th = (np.arange(1, 181) - 0.5) * np.pi / 180.0
+    hg = lambda g: (1 - g * g) / (1 - 2 * g * np.cos(th) + g * g) ** 1.5 / 2
+    # the one-degree bin average is the closed form to second order in the bin width
+    assert np.allclose([PF.hg_binned(0.5, x) for x in th], hg(0.5), rtol=2e-3)
+    lam = M.wavelength_grid(0.1, 1000.0, 10)[0]
+    res = dict(kabs=np.linspace(1, 2, 10), ksca=np.linspace(2, 3, 10), kext=np.linspace(3, 5, 10),
+               F=np.ones((10, 6, 180)), rho_av=3.0)
+    PF.write_particle_fits(str(tmp_path / "p.fits"), lam, res, 0.1, 1.0, 3.5, 0.0, False, 0.0, [1.0], [3.0], ["x"], 1)
+    r = PF.read_particle_fits(str(tmp_path / "p.fits"), lam, matrix=PF.rayleigh_hg_matrix(0.5, pmax=0.3))
+    s = np.sin(th)
+    F11 = r["F"][3, 0]
+    assert np.allclose(F11 / F11[0], np.array([PF.hg_binned(0.5, x) for x in th]) / PF.hg_binned(0.5, th[0]),
+                       rtol=1e-12)
+    assert abs((F11 * s).sum() / s.sum() - 1) < 1e-13
+    c = np.cos(th)
+    assert np.allclose(r["F"][3, 1], -0.3 * F11 * (1 - c * c) / (1 + c * c), rtol=1e-12)
+    ray = PF.read_particle_fits(str(tmp_path / "p.fits"), lam, matrix=PF.rayleigh_hg_matrix())
+    assert np.allclose(ray["F"][0, 0] / ray["F"][0, 0][0], ((1 + c * c) / 2) / ((1 + c[0] ** 2) / 2), rtol=1e-12)
