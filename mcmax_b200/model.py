@@ -736,10 +736,13 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
                                             v("asymb%02d" % e, v("asymb%d" % e, 2.0)),
                                             v("wasymb%02d" % e, v("wasymb%d" % e, 0.0)),
                                             v("pmax%02d" % e, v("pmax%d" % e, 1.0)))
+            extra = dict(nspike=v("nspike", 0, int) if scat == 2 else 0,
+                         wasym2=v("wasymb%02d" % e, v("wasymb%d" % e, 0.0)),
+                         asym2=v("asymb%02d" % e, v("asymb%d" % e, 2.0)))
             if kinds[e] == "fitspart":
-                r = PF.read_particle_fits(path_of(v(key, "", str)), lam, matrix=mat)
+                r = PF.read_particle_fits(path_of(v(key, "", str)), lam, matrix=mat, **extra)
             elif kinds[e] == "part":
-                r = PF.read_particle_ascii(path_of(v(key, "", str)), lam, matrix=mat)
+                r = PF.read_particle_ascii(path_of(v(key, "", str)), lam, matrix=mat, **extra)
             else:
                 r = PF.read_opacity_file(path_of(v(key, "", str)), lam)
             if kinds[e] != "fitspart":

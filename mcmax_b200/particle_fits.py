@@ -263,14 +263,22 @@ def check_particle_file(path, amin, amax, apow, ns, fmax, blend, porosity, frac,
     return True
 
 
-def _regrid(L, Kx, Ka, Ks, M, lam):
+def _regrid(L, Kx, Ka, Ks, M, lam, nspike=0, spike="min", wasym2=0.0, asym2=2.0):
     """opacities and matrices of a tabulated grain on the wavelength grid
     lam, as ReadParticleFits (ReadParticleFits.f:112-222) and readopacity
     (Init.f:4929-4972) regrid them: below the table's first wavelength the
     first entry; inside, linear in wavelength between the bracketing entries
     (Kext too); beyond the last, Ksca ~ lam^-4, Kabs ~ lam^-2, Kext = Kabs +
     Ksca and F held; then every matrix renormalised so that sum F11
-    sin(theta) = sum sin(theta) over the 180 bins.  M: (nl, 6, 180)."""
+    sin(theta) = sum sin(theta) over the 180 bins.  M: (nl, 6, 180).
+
+    nspike > 0 (with full scattering) makes the first nspike degrees flat:
+    F11 there takes the smallest F11 of bins 1..nspike+1 (spike "min",
+    ReadParticleFits.f:224-270) or F11 of bin nspike+1 (spike "next",
+    readparticle, Init.f:4816-4845), the other elements scaled alike; Ksca
+    drops by the removed part and the matrix is renormalised.  wasym2 != 0
+    mixes a Henyey-Greenstein F11 of asymmetry asym2 in with that weight
+    (ReadParticleFits.f:272-285)."""
     lam = np.asarray(lam, float)
     nlam = lam.size
     kext, kabs, ksca = np.zeros(nlam), np.zeros(nlam), np.zeros(nlam)
@@ -300,19 +308,33 @@ def _regrid(L, Kx, Ka, Ks, M, lam):
     s = np.sin(math.pi * (np.arange(1, NANG + 1) - 0.5) / 180.0)
     tot = (F[:, 0, :] * s).sum(1)
     F *= (s.sum() / tot)[:, None, None]
+    if 0 < nspike < NANG:
+        for j in range(nlam):
+            lvl = F[j, 0, :nspike + 1].min() if spike == "min" else F[j, 0, nspike]
+            f = lvl / F[j, 0, :nspike]
+            F[j, 1:, :nspike] *= f[None, :]
+            F[j, 0, :nspike] = lvl
+            t = (F[j, 0] * s).sum()
+            ksca[j] = ksca[j] * t / s.sum()
+            kext[j] = kabs[j] + ksca[j]
+            F[j] *= s.sum() / t
+    if wasym2 != 0.0:
+        th = (np.arange(1, NANG + 1) - 0.5) * math.pi / 180.0
+        hg = np.array([hg_binned(asym2, x) for x in th])
+        F[:, 0, :] = F[:, 0, :] * (1.0 - wasym2) + wasym2 * hg[None, :]
     return kext, kabs, ksca, F
 
 
-def read_particle_fits(path, lam, matrix=None):
+def read_particle_fits(path, lam, matrix=None, nspike=0, wasym2=0.0, asym2=2.0):
     """ReadParticleFits: the file's opacities and matrices on the wavelength
     grid lam (see _regrid); matrix (6, 180), when given, replaces the file's
     at every wavelength (the Rayleigh / Henyey-Greenstein option, see
-    rayleigh_hg_matrix).  Returns dict(kabs, ksca, kext, F (nlam, 6, 180),
+    rayleigh_hg_matrix); nspike, wasym2, asym2 as _regrid.  Returns dict(kabs, ksca, kext, F (nlam, 6, 180),
     rho_av, a1, a2, a3, rv [cm], amin, amax)."""
     (hdr, a), (_, m) = _read_hdus(_open(path))[:2]
     L, Kx, Ka, Ks = a
     M = m.transpose(2, 1, 0) if matrix is None else np.broadcast_to(matrix, (L.size, 6, NANG))
-    kext, kabs, ksca, F = _regrid(L, Kx, Ka, Ks, M, lam)
+    kext, kabs, ksca, F = _regrid(L, Kx, Ka, Ks, M, lam, nspike, "min", 0.0 if matrix is not None else wasym2, asym2)
     a2 = float(hdr["A2"])
     return dict(kabs=kabs, ksca=ksca, kext=kext, F=F, rho_av=float(hdr["DENSITY"]), a1=float(hdr["A1"]), a2=a2,
                 a3=float(hdr["A3"]), rv=math.sqrt(a2) * 1e-4, amin=float(hdr.get("R_MIN", float("nan"))),
@@ -380,7 +402,7 @@ def read_opacity_file(path, lam):
     return dict(kabs=kabs, ksca=ksca, kext=kext, F=F)
 
 
-def read_particle_ascii(path, lam, matrix=None):
+def read_particle_ascii(path, lam, matrix=None, nspike=0, wasym2=0.0, asym2=2.0):
     """readparticle (Init.f:4664-4780): an ASCII particle file of records
     'wavelength Kext Kabs Ksca' followed by F11, F12, F22, F33, F34, F44 of
     180 values each.  As the reference's list-directed reads, every read
@@ -416,7 +438,8 @@ def read_particle_ascii(path, lam, matrix=None):
     if len(L) < 1:
         raise ValueError("%s: no complete wavelength record" % path)
     Ms = np.array(Ms) if matrix is None else np.broadcast_to(matrix, (len(L), 6, NANG))
-    kext, kabs, ksca, F = _regrid(np.array(L), np.array(Kx), np.array(Ka), np.array(Ks), Ms, lam)
+    kext, kabs, ksca, F = _regrid(np.array(L), np.array(Kx), np.array(Ka), np.array(Ks), Ms, lam, nspike, "next",
+                                  0.0 if matrix is not None else wasym2, asym2)
     return dict(kabs=kabs, ksca=ksca, kext=kext, F=F)
 
 

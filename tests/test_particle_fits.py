@@ -168,3 +168,22 @@ def test_compute_part_reads_its_cache(tmp_path):
     # the first grain is found again under index 2's lookup (particle0001 .. particle0002)
     api.ComputePart(ctx, api.Particle(lam.size), 2, *args, particledir=cache)
     assert ctx.calls == 2
+
+
+def test_nspike_flattens_the_forward_peak(tmp_path):
+    lam = np.geomspace(0.1, 3000, 8)
+    res = _result(lam, 9)
+    res["F"][:, 0, :5] *= 50.0          # a forward spike
+    path = str(tmp_path / "p.fits")
+    PF.write_particle_fits(path, lam, res, **GRAIN)
+    plain = PF.read_particle_fits(path, lam)
+    flat = PF.read_particle_fits(path, lam, nspike=4)
+    s = np.sin(np.pi * (np.arange(1, 181) - 0.5) / 180.0)
+    for j in range(lam.size):
+        F11 = flat["F"][j, 0]
+        assert np.allclose(F11[:4], F11[0]) and abs((F11 * s).sum() / s.sum() - 1) < 1e-13
+        # the removed forward part leaves Ksca, the extinction follows
+        assert flat["ksca"][j] < plain["ksca"][j] and abs(flat["kext"][j] - flat["kabs"][j] - flat["ksca"][j]) < 1e-9 * flat["kext"][j]
+    mixed = PF.read_particle_fits(path, lam, wasym2=0.3, asym2=0.6)
+    hg = np.array([PF.hg_binned(0.6, x) for x in (np.arange(1, 181) - 0.5) * np.pi / 180.0])
+    assert np.allclose(mixed["F"][2, 0], 0.7 * plain["F"][2, 0] + 0.3 * hg, rtol=1e-12)
