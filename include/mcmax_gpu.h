@@ -347,6 +347,41 @@ typedef struct {
 mcg_status mcg_trace_spectrum(mcg_ctx *ctx, const mcg_trace_opts *opts, const double *T, int32_t nobs,
                               const double *lam_obs, double *flux, int32_t *info);
 
+/* Rectangular image at one wavelength: the 'IMAGE' observation of
+ * Telescope.f:162-182 -- TracePath at lam0 (opts->lam_path = lam0 as the
+ * reference passes it), TraceFlux at lam0, then MakeImage
+ * (TraceMono.f:2759-3001) without convolution, noise, planets or
+ * polarisation.  Each image cell (between two image radii and two of the
+ * nphi angles) gets nint random points; at each the ray intensities are
+ * interpolated (log-linear, or linear with `linear`) and
+ * I * 2 pi AU^2 dR R / (nphi 2 nint) is added to the pixel of the point and
+ * of its mirror below the major axis.  Pixel (ix, iy), 1-based, covers
+ * x = -R cos(phi + pa), y = R sin(phi + pa) in [-Rmax, Rmax] split into
+ * npixel; im[(ix-1)*npixel + (iy-1)] (the order of the reference's FITS data
+ * stream) is in erg/s/Hz per pixel at unit distance: multiply by
+ * 1e23 zscale / distance^2 [cm] as the reference does.  The random points
+ * come from Philox4x32-10 with key `seed` and counter (0, 1, s_lo, s_hi),
+ * s = (i nphi + j) nint + k the point's index (the reference draws ran2 in
+ * loop order); the pixel sums are accumulated in point order.  flux[0] is
+ * TraceFlux's flux at lam0.  When cap > 0, Rimg[0..nr) and rphi[nr*nphi]
+ * receive the image radii (AU) and the ray intensities (radius-major);
+ * cap must then be at least the number of image radii.  info (may be NULL):
+ * [0] image radii, [1] rays ended by a geometry failure. */
+typedef struct {
+  int32_t npixel;     /* pixels per side (npix keyword, Telescope default 500) */
+  int32_t nint;       /* random points per image cell (nint keyword, default 1000) */
+  double Rmax;        /* half the field of view, AU */
+  double pa;          /* position angle, degrees (posangle keyword) */
+  uint64_t seed;      /* key of the points' random numbers */
+  int32_t linear;     /* 1: linear interpolation of the intensities; 0: log-linear */
+  int32_t cap;        /* capacity of Rimg in radii (0: not written) */
+  double *Rimg;       /* out: image radii [cap] */
+  double *rphi;       /* out: intensities [cap * nphi] */
+} mcg_image_opts;
+
+mcg_status mcg_trace_image(mcg_ctx *ctx, const mcg_trace_opts *opts, const double *T, double lam0,
+                           const mcg_image_opts *io, double *flux, double *im, int32_t *info);
+
 /* ----------------------------------------------------------------------
  * Opacity-surrogate network.  No counterpart in the reference: it stands in
  * for ComputePart's coated-sphere inner loop (ComputePart.f:318-447) inside

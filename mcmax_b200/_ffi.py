@@ -59,6 +59,12 @@ class TraceOpts(C.Structure):
                 ("dimstar", C.c_double)]
 
 
+class ImageOpts(C.Structure):
+    _fields_ = [("npixel", C.c_int32), ("nint", C.c_int32), ("Rmax", C.c_double), ("pa", C.c_double),
+                ("seed", C.c_uint64), ("linear", C.c_int32), ("cap", C.c_int32), ("Rimg", C.POINTER(C.c_double)),
+                ("rphi", C.POINTER(C.c_double))]
+
+
 class Grid(C.Structure):
     _fields_ = [
         ("nr", C.c_int), ("nt", C.c_int), ("R", dp), ("Theta", dp), ("SinTheta", dp),
@@ -127,6 +133,8 @@ SIGNATURES = {
     "mcg_finalize_t": (C.c_int, [C.c_void_p, dp, dp, dp]),
     "mcg_trace_spectrum": (C.c_int, [C.c_void_p, C.POINTER(TraceOpts), dp, C.c_int32, dp, dp,
                                      C.POINTER(C.c_int32)]),
+    "mcg_trace_image": (C.c_int, [C.c_void_p, C.POINTER(TraceOpts), dp, C.c_double, C.POINTER(ImageOpts), dp, dp,
+                                  C.POINTER(C.c_int32)]),
     "mcg_disk_structure": (C.c_int, [C.c_void_p, C.POINTER(Structure), dp, dp, dp, dp, dp, dp]),
     "mcg_diffuse": (C.c_int, [C.c_void_p, C.c_int32, C.c_double, C.c_double, C.POINTER(C.c_int32), dp, dp, dp,
                               C.POINTER(C.c_int32)]),

@@ -231,6 +231,43 @@ class Context:
                                                 _ffi.ptr(flux), _ffi.ptr(info)))
         return flux, (int(info[0]), int(info[1]))
 
+    def trace_image(self, T, lam0, angle, npixel=500, nint=1000, Rmax=None, pa=0.0, nphi=45, nr=2, Rfix=(),
+                    tracestar=True, dimstar=1.0, seed=42, linear=None):
+        """mcg_trace_image on the current model: the rectangular image at
+        wavelength lam0 [micron] and inclination `angle` [rad] (MakeImage).
+        Rmax: half the field of view [AU], by default the grid's outer radius
+        (the reference's default fov is twice that); pa: position angle
+        [deg]; linear: interpolate the ray intensities linearly (default:
+        as the reference does for the model's scattering, linear for the
+        full Mueller matrix, log-linear otherwise).  Returns dict(image
+        (npixel, npixel) indexed [ix-1, iy-1] in the reference's units per
+        pixel (x 1e23 zscale / distance^2 for Jy), flux at lam0, R (image
+        radii, AU), rphi (nr, nphi) ray intensities, info)."""
+        m = self.model
+        T = _f64(T).reshape(-1)
+        Rfix = _f64(np.atleast_1d(np.asarray(Rfix, float)))
+        if Rmax is None:
+            Rmax = float(np.asarray(m.R)[-1])
+        if linear is None:
+            linear = int(m.scat_how) == 2
+        nRfix = int(Rfix.size)
+        cap = nr * (m.nr - 1) if nr > 0 else (m.nr - 2) // (-nr) + 1
+        cap += (m.nt - 1) * 2 * (nRfix + 2) + 1 + 30 + (180 * (nRfix + 1) if int(m.scat_how) == 2 else 0)
+        Rimg = np.zeros(cap)
+        rphi = np.zeros(cap * int(nphi))
+        o = _ffi.TraceOpts(float(angle), int(nphi), int(nr), nRfix, _ffi.ptr(Rfix) if nRfix else None, float(lam0),
+                           int(bool(tracestar)), float(dimstar))
+        io = _ffi.ImageOpts(int(npixel), int(nint), float(Rmax), float(pa), int(seed) & (2 ** 64 - 1),
+                            int(bool(linear)), int(cap), _ffi.ptr(Rimg), _ffi.ptr(rphi))
+        flux = np.zeros(1)
+        im = np.zeros(int(npixel) * int(npixel))
+        info = np.zeros(2, np.int32)
+        self._check(self.lib.mcg_trace_image(self.h, C.byref(o), _ffi.ptr(T), float(lam0), C.byref(io),
+                                             _ffi.ptr(flux), _ffi.ptr(im), _ffi.ptr(info)))
+        n = int(info[0])
+        return dict(image=im.reshape(int(npixel), int(npixel)), flux=float(flux[0]), R=Rimg[:n].copy(),
+                    rphi=rphi[:n * int(nphi)].reshape(n, int(nphi)).copy(), info=(n, int(info[1])))
+
     def disk_structure(self, R, Theta, V, Mstar, zones, Temp, dens, dens0, gasdens, w, w0, shscale=None,
                        grain_scale=None):
         """mcg_disk_structure: zones is a list of (rin, rout, sh, rsh, shpow,

@@ -124,6 +124,13 @@ mcg_status mcg_trace_spectrum(mcg_ctx *ctx, const mcg_trace_opts *opts, const do
   return mcg_trace_spectrum_impl(ctx, opts, T, nobs, lam_obs, flux, info);
 }
 
+mcg_status mcg_trace_image(mcg_ctx *ctx, const mcg_trace_opts *opts, const double *T, double lam0,
+                           const mcg_image_opts *io, double *flux, double *im, int32_t *info) {
+  if (!ctx) return MCG_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  return mcg_trace_image_impl(ctx, opts, T, lam0, io, flux, im, info);
+}
+
 mcg_status mcg_disk_structure(mcg_ctx *ctx, const mcg_structure *s, const double *Temp, double *dens, double *dens0,
                               double *gasdens, double *w, double *w0) {
   if (!ctx) return MCG_ERR_ARG;

@@ -9,9 +9,21 @@
  *                   through the cells and the formal solution
  * The image grid, the tau = 0.1 radius and the flux sum are host logic
  * shared with the test replay.
+ *
+ * mcg_trace_image adds the rectangular image of one wavelength:
+ *   rt_image_sample_kernel  one thread per sample point: the interpolated
+ *                           intensity and the pixels of the point and its
+ *                           mirror (rt_image_sample)
+ *   stable radix sort of (pixel, amount) pairs, in sample order
+ *   rt_image_add_kernel     one thread per pixel: adds its run of amounts in
+ *                           sample order, so that every pixel holds the same
+ *                           sum, bit for bit, as the sequential loop
+ * The samples are processed in chunks of RT_IMG_CHUNK; the pixel sums carry
+ * over from chunk to chunk.
  */
 #include <cuda_runtime.h>
 
+#include <cub/device/device_radix_sort.cuh>
 #include <vector>
 
 #include "mcg_internal.h"
@@ -39,6 +51,43 @@ __global__ void rt_ray_kernel(const __grid_constant__ TModel m, const double *de
   int steps;
   image[t] = rt_ray(m, dens, kext, emis, Rimg[i], phi[k], angle, fstar, dimstar, tracestar, RT_MAXSTEPS, &steps);
   if (steps < 0) atomicAdd(bad, 1u);
+}
+
+__global__ void rt_image_sample_kernel(long long s0, long long n, int nphi, int nint, const double *R,
+                                       const double *image, unsigned long long seed, double Rmax, double pa_deg,
+                                       int npix, int linear, uint32_t *keys, double *vals) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  uint32_t key[2];
+  double v;
+  rt_image_sample(s0 + t, nphi, nint, R, image, (uint64_t)seed, Rmax, pa_deg, npix, linear, key, &v);
+  keys[2 * t] = key[0];
+  keys[2 * t + 1] = key[1];
+  vals[2 * t] = v;
+  vals[2 * t + 1] = v;
+}
+
+/* first index q in [0, n) with keys[q] >= p (n when none) */
+__device__ __forceinline__ long long rt_lower_bound(const uint32_t *keys, long long n, uint32_t p) {
+  long long lo = 0, hi = n;
+  while (lo < hi) {
+    const long long mid = (lo + hi) >> 1;
+    if (keys[mid] < p)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+__global__ void rt_image_add_kernel(int npix2, long long n, const uint32_t *keys, const double *vals, double *im) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npix2) return;
+  const long long lo = rt_lower_bound(keys, n, (uint32_t)p), hi = rt_lower_bound(keys, n, (uint32_t)p + 1u);
+  if (lo == hi) return;
+  double a = im[p];
+  for (long long q = lo; q < hi; ++q) a = a + vals[q];
+  im[p] = a;
 }
 
 inline int nblk(long long n, int b) { return (int)((n + b - 1) / b); }
@@ -122,18 +171,22 @@ struct RtDeviceBackend {
 
 }  // namespace
 
-mcg_status mcg_trace_spectrum_impl(mcg_ctx *ctx, const mcg_trace_opts *o, const double *T, int32_t nobs,
-                                   const double *lam_obs, double *flux, int32_t *info) {
+/* the ray-traced flux at nobs wavelengths (shared by both entry points):
+ * validation, the image rays and the formal solution; Rimg and image_last
+ * receive the image radii and the last wavelength's intensities */
+static mcg_status rt_trace(mcg_ctx *ctx, const char *who, const mcg_trace_opts *o, const double *T, int32_t nobs,
+                           const double *lam_obs, double *flux, std::vector<double> *Rimg,
+                           std::vector<double> *image_last, int *bad) {
   DevModel &m = ctx->model;
-  if (!m.valid) return mcg_fail(ctx, MCG_ERR_STATE, "trace_spectrum: no model set");
+  if (!m.valid) return mcg_fail(ctx, MCG_ERR_STATE, "%s: no model set", who);
   if (!o || !T || (nobs > 0 && (!lam_obs || !flux)) || nobs < 0)
-    return mcg_fail(ctx, MCG_ERR_ARG, "trace_spectrum: missing argument");
+    return mcg_fail(ctx, MCG_ERR_ARG, "%s: missing argument", who);
   if (o->nphi < 1 || o->nr == 0 || o->nphi > 100000 || (o->nRfix > 0 && !o->Rfix) || o->nRfix < 0 ||
       !(o->lam_path > 0.0))
-    return mcg_fail(ctx, MCG_ERR_ARG, "trace_spectrum: nphi >= 1, nr != 0, lam_path > 0 required");
+    return mcg_fail(ctx, MCG_ERR_ARG, "%s: nphi >= 1, nr != 0, lam_path > 0 required", who);
   const int ncell = m.ncell;
   for (int c = 0; c < ncell; ++c)
-    if (!(T[c] >= 0.0) || !(T[c] < 1e6)) return mcg_fail(ctx, MCG_ERR_ARG, "trace_spectrum: T[%d] = %g", c, T[c]);
+    if (!(T[c] >= 0.0) || !(T[c] < 1e6)) return mcg_fail(ctx, MCG_ERR_ARG, "%s: T[%d] = %g", who, c, T[c]);
   cudaStream_t st = ctx->stream;
   std::vector<double> R(m.nr + 1), Theta(m.nt), dens(ncell), lam(m.nlam), Fstar(m.nlam);
   MCG_CUDA(ctx, cudaMemcpyAsync(R.data(), m.R, sizeof(double) * R.size(), cudaMemcpyDeviceToHost, st));
@@ -141,7 +194,7 @@ mcg_status mcg_trace_spectrum_impl(mcg_ctx *ctx, const mcg_trace_opts *o, const 
   MCG_CUDA(ctx, cudaMemcpyAsync(dens.data(), m.dens, sizeof(double) * ncell, cudaMemcpyDeviceToHost, st));
   MCG_CUDA(ctx, cudaStreamSynchronize(st));
   if (m.lam_h.size() != (size_t)m.nlam || m.Fstar_h.size() != (size_t)m.nlam)
-    return mcg_fail(ctx, MCG_ERR_STATE, "trace_spectrum: the model's wavelengths are not kept");
+    return mcg_fail(ctx, MCG_ERR_STATE, "%s: the model's wavelengths are not kept", who);
   lam = m.lam_h;
   Fstar = m.Fstar_h;
   RtMem mem;
@@ -156,7 +209,7 @@ mcg_status mcg_trace_spectrum_impl(mcg_ctx *ctx, const mcg_trace_opts *o, const 
   if (e == cudaSuccess) e = mem.alloc(&be.kext, (size_t)ncell);
   if (e == cudaSuccess) e = mem.alloc(&be.emis, (size_t)ncell);
   if (e == cudaSuccess) e = cudaMemcpyAsync(dT, T, sizeof(double) * ncell, cudaMemcpyHostToDevice, st);
-  if (e != cudaSuccess) return mcg_fail(ctx, MCG_ERR_CUDA, "trace_spectrum: %s", cudaGetErrorString(e));
+  if (e != cudaSuccess) return mcg_fail(ctx, MCG_ERR_CUDA, "%s: %s", who, cudaGetErrorString(e));
   be.T = dT;
   TModel hm;
   memset(&hm, 0, sizeof hm);
@@ -171,14 +224,97 @@ mcg_status mcg_trace_spectrum_impl(mcg_ctx *ctx, const mcg_trace_opts *o, const 
   be.tm.R = m.R;
   be.tm.Theta = m.Theta;
   RtOptions ro{o->angle, o->nphi, o->nr, o->nRfix, o->Rfix, o->lam_path, o->tracestar, o->dimstar};
+  *bad = 0;
+  if (!rt_spectrum(hm, be, ro, m.nlam, lam.data(), Fstar.data(), dens.data(), nobs, lam_obs, flux, Rimg, image_last,
+                   bad))
+    return mcg_fail(ctx, MCG_ERR_CUDA, "%s", be.err.c_str());
+  return MCG_OK;
+}
+
+mcg_status mcg_trace_spectrum_impl(mcg_ctx *ctx, const mcg_trace_opts *o, const double *T, int32_t nobs,
+                                   const double *lam_obs, double *flux, int32_t *info) {
   std::vector<double> Rimg;
   int bad = 0;
-  if (!rt_spectrum(hm, be, ro, m.nlam, lam.data(), Fstar.data(), dens.data(), nobs, lam_obs, flux, &Rimg, nullptr,
-                   &bad))
-    return mcg_fail(ctx, MCG_ERR_CUDA, "%s", be.err.c_str());
+  const mcg_status rc = rt_trace(ctx, "trace_spectrum", o, T, nobs, lam_obs, flux, &Rimg, nullptr, &bad);
+  if (rc != MCG_OK) return rc;
   if (info) {
     info[0] = (int32_t)Rimg.size();
     info[1] = bad;
   }
+  return MCG_OK;
+}
+
+constexpr long long RT_IMG_CHUNK = 1LL << 23; /* samples per sort (2^24 pairs, 192 MB with the sort buffers) */
+
+mcg_status mcg_trace_image_impl(mcg_ctx *ctx, const mcg_trace_opts *o, const double *T, double lam0,
+                                const mcg_image_opts *io, double *flux, double *im, int32_t *info) {
+  if (!io || !im || !flux) return mcg_fail(ctx, MCG_ERR_ARG, "trace_image: missing argument");
+  if (io->npixel < 1 || io->npixel > 8192 || io->nint < 1 || io->nint > 1000000 || !(io->Rmax > 0.0) ||
+      !(io->Rmax < 1e30) || !(fabs(io->pa) < 1e6) || io->cap < 0 || (io->cap > 0 && (!io->Rimg || !io->rphi)))
+    return mcg_fail(ctx, MCG_ERR_ARG,
+                    "trace_image: 1 <= npixel <= 8192, 1 <= nint <= 1e6, 0 < Rmax < 1e30, |pa| < 1e6 and the "
+                    "radius buffers required");
+  std::vector<double> Rimg, rphi;
+  int bad = 0;
+  mcg_status rc = rt_trace(ctx, "trace_image", o, T, 1, &lam0, flux, &Rimg, &rphi, &bad);
+  if (rc != MCG_OK) return rc;
+  const int nr = (int)Rimg.size(), nphi = o->nphi, npix = io->npixel;
+  if (info) {
+    info[0] = nr;
+    info[1] = bad;
+  }
+  if (io->cap > 0) {
+    if (io->cap < nr) return mcg_fail(ctx, MCG_ERR_ARG, "trace_image: cap %d < %d image radii", io->cap, nr);
+    memcpy(io->Rimg, Rimg.data(), sizeof(double) * nr);
+    memcpy(io->rphi, rphi.data(), sizeof(double) * (size_t)nr * nphi);
+  }
+  const int npix2 = npix * npix;
+  const long long nsamp = (long long)(nr - 1) * nphi * io->nint;
+  const long long chunk = nsamp < RT_IMG_CHUNK ? nsamp : RT_IMG_CHUNK;
+  cudaStream_t st = ctx->stream;
+  RtMem mem;
+  double *dR, *dI, *dim, *vals, *vals_s;
+  uint32_t *keys, *keys_s;
+  cudaError_t e = mem.alloc(&dR, (size_t)nr);
+  if (e == cudaSuccess) e = mem.alloc(&dI, (size_t)nr * nphi);
+  if (e == cudaSuccess) e = mem.alloc(&dim, (size_t)npix2);
+  if (e == cudaSuccess) e = mem.alloc(&keys, (size_t)(2 * chunk));
+  if (e == cudaSuccess) e = mem.alloc(&keys_s, (size_t)(2 * chunk));
+  if (e == cudaSuccess) e = mem.alloc(&vals, (size_t)(2 * chunk));
+  if (e == cudaSuccess) e = mem.alloc(&vals_s, (size_t)(2 * chunk));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dR, Rimg.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(dI, rphi.data(), sizeof(double) * (size_t)nr * nphi, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(dim, 0, sizeof(double) * npix2, st);
+  if (e != cudaSuccess) return mcg_fail(ctx, MCG_ERR_CUDA, "trace_image: %s", cudaGetErrorString(e));
+  int end_bit = 1;
+  while (end_bit < 32 && (1ull << end_bit) <= (unsigned long long)npix2) ++end_bit; /* keys 0..npix2 */
+  size_t tmp_bytes = 0;
+  e = cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys, keys_s, vals, vals_s, (int)(2 * chunk), 0, end_bit,
+                                      st);
+  char *tmp = nullptr;
+  if (e == cudaSuccess) e = mem.alloc(&tmp, tmp_bytes);
+  if (e != cudaSuccess) return mcg_fail(ctx, MCG_ERR_CUDA, "trace_image: sort setup: %s", cudaGetErrorString(e));
+  for (long long s0 = 0; s0 < nsamp; s0 += chunk) {
+    const long long n = nsamp - s0 < chunk ? nsamp - s0 : chunk;
+    rt_image_sample_kernel<<<nblk(n, 256), 256, 0, st>>>(s0, n, nphi, io->nint, dR, dI,
+                                                         (unsigned long long)io->seed, io->Rmax, io->pa, npix,
+                                                         io->linear ? 1 : 0, keys, vals);
+    e = cudaGetLastError();
+    size_t need = 0;
+    if (e == cudaSuccess)
+      e = cub::DeviceRadixSort::SortPairs(nullptr, need, keys, keys_s, vals, vals_s, (int)(2 * n), 0, end_bit, st);
+    if (e == cudaSuccess && need > tmp_bytes)
+      return mcg_fail(ctx, MCG_ERR_CUDA, "trace_image: sort needs %zu bytes, %zu held", need, tmp_bytes);
+    if (e == cudaSuccess)
+      e = cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys, keys_s, vals, vals_s, (int)(2 * n), 0, end_bit, st);
+    if (e == cudaSuccess) {
+      rt_image_add_kernel<<<nblk(npix2, 256), 256, 0, st>>>(npix2, 2 * n, keys_s, vals_s, dim);
+      e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) return mcg_fail(ctx, MCG_ERR_CUDA, "trace_image: image pass: %s", cudaGetErrorString(e));
+  }
+  MCG_CUDA(ctx, cudaMemcpyAsync(im, dim, sizeof(double) * npix2, cudaMemcpyDeviceToHost, st));
+  MCG_CUDA(ctx, cudaStreamSynchronize(st));
   return MCG_OK;
 }

@@ -358,4 +358,86 @@ bool rt_spectrum(const TModel &m, Backend &be, const RtOptions &o, int nlam, con
   return true;
 }
 
+/* ---- rectangular image (MakeImage, TraceMono.f:2759-3001) ----
+ *
+ * Sample s = (ring i, angle column j, draw k), s = (i nphi + j) nint + k,
+ * places one point at a uniform position in the image cell between radii
+ * R[i], R[i+1] and angles pi j/nphi, pi (j+1)/nphi, interpolates the ray
+ * intensities there (bilinear in radius and angle, the angle neighbour being
+ * the column on the point's side, TraceMono.f:2841-2861) and adds
+ * I w2 R / (2 nint) to the pixel of the point and of its mirror image
+ * -phi (TraceMono.f:2963-3001), w2 = 2 pi AU^2 (R[i+1] - R[i]) / nphi.
+ *
+ * The interpolation is log-linear (TraceMono.f:2931-2934, the 10**() of
+ * interpolated log10 I, written here with natural logarithms) or, with
+ * linear set, linear: the form the reference reaches for scattering with
+ * the full Mueller matrix when the image carries no polarisation (its
+ * polarised branch divides U by 2 a_l a_r = 0, number_invalid turns the
+ * NaN into the linear interpolation, TraceMono.f:2862-2920).
+ *
+ * The two uniforms of a sample are one Philox block with key = seed and
+ * counter (0, 1, s_lo, s_hi), where the reference draws ran2 in loop order.
+ * key[0], key[1]: the pixel index (ix - 1) npix + (iy - 1) of the point and
+ * of its mirror, npix^2 when the point falls outside the image; *val the
+ * amount added to each. */
+RT_HD void rt_image_sample(long long s, int nphi, int nint, const double *R, const double *image, uint64_t seed,
+                           double Rmax, double pa_deg, int npix, int linear, uint32_t key[2], double *val) {
+  const long long per_ring = (long long)nphi * nint;
+  const int i = (int)(s / per_ring);
+  const int jf = (int)((s / nint) % nphi) + 1; /* Fortran column 1..nphi */
+  const uint32_t ctr[4] = {0u, 1u, (uint32_t)(unsigned long long)s, (uint32_t)((unsigned long long)s >> 32)};
+  const uint32_t kk[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+  uint32_t o[4];
+  px_philox4x32_10(ctr, kk, o);
+  const double ranR = px_u01(o[0], o[1]), ranPhi = px_u01(o[2], o[3]);
+  const double w2 = (((2.0 * RT_PI) * (RT_AU * RT_AU)) * (R[i + 1] - R[i])) / (double)(float)nphi;
+  const double Rs = R[i] + (R[i + 1] - R[i]) * ranR;
+  const double phi = (RT_PI * ((double)(float)(jf - 1) + ranPhi)) / (double)(float)nphi;
+  int jp1, jp2 = jf;
+  double wp1, wp2;
+  if (ranPhi < 0.5) {
+    wp1 = 0.5 - ranPhi;
+    jp1 = jf - 1;
+    if (jp1 == 0) jp1 = 1;
+    wp2 = ranPhi + 0.5;
+  } else {
+    wp1 = ranPhi - 0.5;
+    jp1 = jf + 1;
+    if (jp1 == nphi + 1) jp1 = nphi;
+    wp2 = 1.5 - ranPhi;
+  }
+  const double wr1 = 1.0 - ranR, wr2 = ranR;
+  const double *r1 = image + (size_t)i * nphi, *r2 = image + (size_t)(i + 1) * nphi;
+  const double I11 = r1[jp1 - 1], I12 = r1[jp2 - 1], I21 = r2[jp1 - 1], I22 = r2[jp2 - 1];
+  double f;
+  if (linear) {
+    f = ((wr1 * (wp1 * I11 + wp2 * I12) + wr2 * (wp1 * I21 + wp2 * I22)) * w2) * Rs;
+  } else {
+    const double e = wr1 * (wp1 * dm_log(I11) + wp2 * dm_log(I12)) + wr2 * (wp1 * dm_log(I21) + wp2 * dm_log(I22));
+    f = (dm_exp(e) * w2) * Rs;
+  }
+  *val = f / (double)(float)(2 * nint);
+  const double pa = (pa_deg * RT_PI) / 180.0;
+  const double npf = (double)(float)npix;
+  for (int m = 0; m < 2; ++m) {
+    const double a = m == 0 ? phi + pa : -phi + pa;
+    const double x = (npf * (-Rs * dm_cos(a) + Rmax)) / (2.0 * Rmax) + 1.0;
+    const double y = (npf * (Rs * dm_sin(a) + Rmax)) / (2.0 * Rmax) + 1.0;
+    /* Fortran's ix = x truncates; ix in 1..npix  <=>  1 <= x < npix + 1 */
+    if (x >= 1.0 && x < npf + 1.0 && y >= 1.0 && y < npf + 1.0)
+      key[m] = (uint32_t)(((int)x - 1) * npix + ((int)y - 1));
+    else
+      key[m] = (uint32_t)npix * (uint32_t)npix;
+  }
+}
+
+/* image radii count for the rectangular image's buffers: the size of
+ * rt_image_radii's list (the model's nr, nt; nj0; nRfix; scat_how) */
+static inline long long rt_image_radii_count(int nr, int nt, int nj0, int nRfix, int scat_how) {
+  long long n = (nj0 > 0 ? (long long)nj0 * (nr - 1) : (long long)(nr - 2) / (-nj0) + 1);
+  n += (long long)(nt - 1) * 2 * (nRfix + 2) + 1 + RT_NSTAR;
+  if (scat_how == 2) n += 180LL * (nRfix + 1);
+  return n;
+}
+
 #endif /* MCMAX_RT_CORE_CUH */

@@ -242,18 +242,26 @@ def spectrum_wavelengths(lam, lam1, lam2, nlam=-1, lamfile=None):
     return 10.0 ** (math.log10(lam1) + math.log10(lam2 / lam1) * np.arange(n) / (n - 1))
 
 
-def read_observations(path, lam, incangle=45.0):
+def read_observations(path, lam, incangle=45.0, rout=None):
     """The observations of an MCMax observation file (Telescope.f:583-1100):
     keywords before the first type= line set the defaults, each type= line
     starts an observation whose own keywords follow.  Returns a list of
-    dicts with kind, inc [deg], lam1, lam2, nlam, lamfile, nphi, nrad, flag
-    (and the other keywords as given, lower-case).  Defaults: inc from the
-    deck's incangle, lam1/lam2 the model's range, nphi 45, nrad 2."""
+    dicts with kind, inc [deg], lam1, lam2, nlam, lamfile, nphi, nrad, flag,
+    npix, nint, fov (list, AU or arcsec), scaletype (and the other keywords
+    as given, lower-case).  Defaults: inc from the deck's incangle, lam1/lam2
+    the model's range, nphi 45, nrad 2, npix 500, nint 1000, fov twice the
+    grid's outer radius `rout`, scaletype 1.  An IMAGE observation's lam1 is
+    the default-level `lam`, else the middle of the wavelength range
+    (Telescope.f:591,710-712); a `lam` among an observation's own keywords
+    sets its lam1."""
     lam = np.asarray(lam, float)
     default = dict(inc=float(incangle), lam1=float(lam[0]), lam2=float(lam[-1]), nlam=-1, lamfile="", nphi=45,
-                   nrad=2, flag="")
+                   nrad=2, flag="", npix=500, nint=1000, fov=[] if rout is None else [2.0 * float(rout)],
+                   scaletype=1)
+    deflam = (float(lam[0]) + float(lam[-1])) / 2.0
     obs, cur = [], default
     base = os.path.dirname(os.path.abspath(path))
+    num = lambda v: float(v.replace("d", "e").replace("D", "E"))
     with open(path) as f:
         for line in f:
             t = line.strip()
@@ -265,18 +273,28 @@ def read_observations(path, lam, incangle=45.0):
             if val[:1] in ("'", '"'):
                 val = val[1:-1] if len(val) > 1 and val[-1] == val[0] else val[1:]
             if key == "type":
-                cur = dict(default, kind=val.upper())
+                cur = dict(default, kind=val.upper(), fov=list(default["fov"]))
+                if cur["kind"] == "IMAGE":
+                    cur["lam1"] = deflam
                 obs.append(cur)
                 continue
-            if key in ("nphi", "nrad", "nlam"):
-                cur[key] = int(float(val.replace("d", "e").replace("D", "E")))
+            if key in ("nphi", "nrad", "nlam", "npix", "nint", "scaletype"):
+                cur[key] = int(num(val))
+            elif key == "lam" and cur is default:
+                deflam = num(val)
             elif key in ("inc", "lam1", "lam2", "lam"):
-                x = float(val.replace("d", "e").replace("D", "E"))
-                cur["lam1" if key == "lam" else key] = x
+                cur["lam1" if key == "lam" else key] = num(val)
+            elif key[:3] == "fov":
+                i = int(key[3:]) if len(key) > 3 else 1
+                while len(cur["fov"]) < i:
+                    cur["fov"].append(None)
+                cur["fov"][i - 1] = num(val)
             elif key == "lamfile":
                 cur[key] = val if os.path.isabs(val) else os.path.join(base, val)
             else:
                 cur[key] = val
+    for ob in obs:
+        ob["fov"] = [x for x in ob["fov"] if x is not None]
     return obs
 
 
@@ -324,4 +342,142 @@ def write_spectrum(outdir, angle_deg, lam_obs, flux, lam, Fstar, distance_pc=100
                 fs = float(np.exp(np.interp(np.log(l0), np.log(lam), np.log(Fstar))))
             f.write("%s%s%s%s\n" % (_num(l0), _num(1e23 * flux[j] / d2), _num(1e23 * scat[j] / d2),
                                     _num(1e23 * fs / d2)))
+    return path
+
+
+def _fortran_f(x, w, d):
+    """Fortran fw.d: asterisks when the number does not fit"""
+    t = "%*.*f" % (w, d, x)
+    return "*" * w if len(t) > w else t
+
+
+def _fortran_i1(n):
+    return str(n) if 0 <= n <= 9 else "*"
+
+
+def _angle_tag(angle_rad):
+    """i1,f3.1 of the inclination in degrees as FITSImage forms it from the
+    angle in radians, tenths of 9.95 and up carried (TraceMono.f:3475-3480)"""
+    a = (180.0 * angle_rad) / math.pi
+    i10 = int(a / 10.0)
+    i1 = a - 10.0 * i10
+    if i1 >= 9.95:
+        i1 = i1 - 9.95
+        i10 = i10 + 1
+    return _fortran_i1(i10) + _fortran_f(i1, 3, 1)
+
+
+def _lam_tag(lam0):
+    """4(i1),f4.2 of the wavelength (TraceMono.f:3482-3486)"""
+    a = int(lam0 / 10000.0)
+    b = int((lam0 - 10000.0 * a) / 1000.0)
+    c = int((lam0 - 1000.0 * b - 10000.0 * a) / 100.0)
+    d = int((lam0 - 100.0 * c - 1000.0 * b - 10000.0 * a) / 10.0)
+    e = lam0 - 10.0 * d - 100.0 * c - 1000.0 * b - 10000.0 * a
+    return "".join(_fortran_i1(v) for v in (a, b, c, d)) + _fortran_f(e, 4, 2)
+
+
+def _fov_tag(Rmax):
+    """4(i1),f3.1 of the field of view 2 Rmax with the carries of
+    TraceMono.f:3488-3509"""
+    r = 2.0 * Rmax
+    a = int(r / 10000.0)
+    b = int((r - 10000.0 * a) / 1000.0)
+    c = int((r - 1000.0 * b - 10000.0 * a) / 100.0)
+    d = int((r - 100.0 * c - 1000.0 * b - 10000.0 * a) / 10.0)
+    e = r - 10.0 * d - 100.0 * c - 1000.0 * b - 10000.0 * a
+    if e >= 9.95:
+        d, e = d + 1, e - 9.95
+    if d >= 10:
+        c, d = c + 1, d - 10
+    if c >= 10:
+        b, c = b + 1, c - 10
+    if b >= 10:
+        a, b = a + 1, b - 10
+    return "".join(_fortran_i1(v) for v in (a, b, c, d)) + _fortran_f(e, 3, 1)
+
+
+def image_name(kind, angle_rad, lam0, Rmax, flag=""):
+    """Image<kind>_i<angle>_l<lam>_fov<2 Rmax><flag>.fits (TraceMono.f:3511-3512)"""
+    return "Image%s_i%s_l%s_fov%s%s.fits" % (kind, _angle_tag(angle_rad), _lam_tag(lam0), _fov_tag(Rmax), flag)
+
+
+def rimage_name(angle_rad, lam0, flag=""):
+    """RImage_i<angle>_l<lam><flag>.dat (TraceMono.f:3399-3400)"""
+    return "RImage_i%s_l%s%s.dat" % (_angle_tag(angle_rad), _lam_tag(lam0), flag)
+
+
+def write_image_fits(path, im, Rmax, rscale=1.0, scaletype=1):
+    """an image as FITSImage writes it (TraceMono.f:3446-3570): a primary
+    npix x npix BITPIX -64 image whose data stream is im[ix-1, iy-1] with iy
+    running fastest, then CTYPE1/2, CRPIX1/2 = 0.5, CRVAL1/2 = -Rmax rscale
+    (the corner), CDELT1/2 = 2 Rmax rscale / npix; AU for scaletype 1,
+    arcsec for 2.  Returns the path."""
+    from . import particle_fits as PF
+    im = np.asarray(im, float)
+    n = im.shape[0]
+    unit = "AU" if scaletype == 1 else "arcsec"
+    cards = [PF._card("SIMPLE", True, "file does conform to FITS standard"),
+             PF._card("BITPIX", -64, "number of bits per data pixel"), PF._card("NAXIS", 2, "number of data axes"),
+             PF._card("NAXIS1", n, "length of data axis 1"), PF._card("NAXIS2", n, "length of data axis 2"),
+             PF._card("EXTEND", True, "FITS dataset may contain extensions")]
+    if scaletype in (1, 2):
+        cards += [PF._card("CTYPE1", "X [%s]" % unit, "X-coordinate"),
+                  PF._card("CTYPE2", "Y [%s]" % unit, "Y-coordinate")]
+    corner = -Rmax * rscale
+    pix = 2.0 * Rmax * rscale / float(np.float32(n))
+    cards += [PF._card("CRPIX1", 0.5, "reference pixel: the image corner", 10),
+              PF._card("CRPIX2", 0.5, "reference pixel: the image corner", 10),
+              PF._card("CRVAL1", corner, "coordinate of the corner", 10),
+              PF._card("CRVAL2", corner, "coordinate of the corner", 10)]
+    if scaletype in (1, 2):
+        cards += [PF._card("CDELT1", pix, "pixel size (%s)" % unit, 10),
+                  PF._card("CDELT2", pix, "pixel size (%s)" % unit, 10)]
+    if os.path.exists(path):
+        os.remove(path)
+    with open(path, "wb") as f:
+        f.write(PF._header(cards) + PF._data(im))
+    return path
+
+
+def read_image_fits(path):
+    """(header dict, image [ix-1, iy-1]) of an image written by write_image_fits"""
+    from . import particle_fits as PF
+    hdr, a = PF._read_hdus(PF._open(path))[0]
+    return hdr, np.asarray(a, float)
+
+
+def write_rimage(path, R, rphi, rscale, zscale, distance_cm, fov_au, npixel, polarised=False):
+    """the radial profile file of RImage (TraceMono.f:3375-3443): per image
+    radius R[i] (i < nr-1) the radius x rscale, the flux inside the ring's
+    outer edge [Jy at the distance] (the running trapezoid sum over the
+    rings) and the intensity at angle column nphi/2 x scaling, scaling =
+    zscale 1e23 / d^2 fov^2 AU^2 / npix^2; then the same for the last
+    radius with the total flux.  With polarisation (full Mueller matrix) the
+    Q, U and polarised columns are written as zeros: the image carries no
+    polarisation.  Returns the path."""
+    R = np.asarray(R, float)
+    rphi = np.asarray(rphi, float)
+    nr, nphi = rphi.shape
+    d2 = distance_cm ** 2
+    scaling = (zscale * 1e23 / d2) * (fov_au ** 2 * M.AU ** 2) / float(npixel ** 2)
+    kc = max(nphi // 2, 1) - 1
+    flux = 0.0
+    lines = []
+    for i in range(nr - 1):
+        w1 = 2.0 * math.pi * abs(R[i]) * M.AU ** 2 / float(np.float32(nphi))
+        w2 = 2.0 * math.pi * abs(R[i + 1]) * M.AU ** 2 / float(np.float32(nphi))
+        for k in range(nphi):
+            flux = flux + (R[i + 1] - R[i]) * (w1 * rphi[i, k] + w2 * rphi[i + 1, k]) / 2.0
+        row = [R[i] * rscale, flux * 1e23 / d2, scaling * rphi[i, kc]]
+        if polarised:
+            row += [0.0, 0.0, 0.0]
+        lines.append(row)
+    row = [R[nr - 1] * rscale, flux * 1e23 / d2, scaling * rphi[nr - 1, kc]]
+    if polarised:
+        row += [0.0]
+    lines.append(row)
+    with open(path, "w") as f:
+        for row in lines:
+            f.write("".join(_num(x) for x in row) + "\n")
     return path

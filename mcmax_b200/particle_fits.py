@@ -87,7 +87,7 @@ def _string_cards(key, value, comment=""):
     return "".join(cards)
 
 
-def _card(key, value=None, comment=""):
+def _card(key, value=None, comment="", decimals=8):
     if isinstance(value, str):
         return _string_cards(key, value, comment)
     if value is None:
@@ -98,7 +98,7 @@ def _card(key, value=None, comment=""):
         elif isinstance(value, (int, np.integer)):
             v = str(int(value)).rjust(20)
         else:
-            v = ("%.8E" % float(value)).rjust(20)
+            v = ("%.*E" % (decimals, float(value))).rjust(20)
         c = key.upper().ljust(8)[:8] + "= " + v
         if comment:
             c += " / " + comment

@@ -1,8 +1,11 @@
 """The steps after the packet loop on the precision disk deck's grid:
-Diffuse (mcg_diffuse), the vertical structure (mcg_disk_structure) and the
-ray-traced spectrum (mcg_trace_spectrum), each timed through the C-ABI.
+Diffuse (mcg_diffuse), the vertical structure (mcg_disk_structure), the
+ray-traced spectrum (mcg_trace_spectrum) and the rectangular image
+(mcg_trace_image: 500 x 500 pixels, 1000 points per image cell, at the
+observation file's default wavelength, the middle of the grid's range),
+each timed through the C-ABI.
 
-    python -m mcmax_b200.postmc_bench [--nphot 2e7] [--angles 20,45,80] [--reps 3]
+    python -m mcmax_b200.postmc_bench [--nphot 2e7] [--angles 20,45,80] [--reps 3] [--npix 500] [--nint 1000]
 
 Deck: Mdust 1e-3 Msun ZONES disk, nr 200 (+ star cell) x ntheta 120, nlam
 200 from 0.1 to 3000 micron, MRN 0.1-1 micron in 20 DHS bins, full Mueller
@@ -40,6 +43,8 @@ def main():
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--nphi", type=int, default=45)
     ap.add_argument("--nr", type=int, default=2)
+    ap.add_argument("--npix", type=int, default=500)
+    ap.add_argument("--nint", type=int, default=1000)
     a = ap.parse_args()
     ctx = api.Context(0)
     m = M.disk_model(ctx, nrad=200, ntheta=120, nlam=200, mdust=1e-3, ngrains=20)
@@ -69,6 +74,15 @@ def main():
                         "rays_per_wavelength": info[0] * a.nphi, "bad_rays": info[1],
                         "rays_per_s": info[0] * a.nphi * lam_obs.size / t})
     out["trace_spectrum"] = spectra
+    lam_img = (m.lam[0] + m.lam[-1]) / 2.0
+    images = []
+    for ang in [float(x) for x in a.angles.split(",") if x]:
+        r, t = _time(lambda: ctx.trace_image(Td, lam_img, math.radians(ang), npixel=a.npix, nint=a.nint,
+                                             nphi=a.nphi, nr=a.nr), a.reps)
+        pts = (r["info"][0] - 1) * a.nphi * a.nint
+        images.append({"angle_deg": ang, "s": t, "lam": lam_img, "pixels": a.npix * a.npix, "image_radii": r["info"][0],
+                       "points": pts, "points_per_s": pts / t, "sum_over_flux": float(r["image"].sum() / r["flux"])})
+    out["trace_image"] = images
     print(json.dumps(out))
     ctx.close()
 

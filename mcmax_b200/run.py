@@ -20,6 +20,7 @@ the MCSpec<angle>.dat files (MCRadiation.f:738-762) in the output
 directory.  --opacity surrogate serves the grain bins inside the network's
 training box from the committed surrogate weights."""
 import argparse
+import math
 import os
 import sys
 
@@ -44,6 +45,39 @@ def fixed_radii(zones, rin, rout):
     return sorted(out)
 
 
+def observe_image(ctx, m, T, ob, outdir, rfix=(), seed=42, posangle=0.0):
+    """An IMAGE observation (Telescope.f:162-182) without convolution,
+    noise or opening: the rays traced at the observation's wavelength
+    (mcg_trace_image), the radial profile RImage_*.dat and, per field of
+    view, the rectangular image ImageAI_*.fits in Jy/pixel and AU
+    (scaletype 1) or mJy/arcsec^2 and arcsec (scaletype 2), with no
+    interstellar extinction.  Returns the files written."""
+    from .outputs import PARSEC
+    angle = (math.pi * ob["inc"]) / 180.0
+    lam0 = ob["lam1"]
+    dcm = m.distance * PARSEC
+    fovs = ob["fov"] or [2.0 * float(m.R[-1])]
+    scaletype = int(ob.get("scaletype", 1))
+    files = []
+    for n, fov in enumerate(fovs):
+        if scaletype == 2:
+            fov = fov * dcm / PARSEC
+            rscale, zscale = PARSEC / dcm, 1e3 * ((ob["npix"] / fov) * dcm / PARSEC) ** 2
+        else:
+            rscale, zscale = 1.0, 1.0
+        r = ctx.trace_image(T, lam0, angle, npixel=ob["npix"], nint=ob["nint"], Rmax=fov / 2.0, pa=posangle,
+                            nphi=ob["nphi"], nr=ob["nrad"], Rfix=rfix, seed=seed + n)
+        if n == 0:
+            files.append(outputs.write_rimage(os.path.join(outdir, outputs.rimage_name(angle, lam0, ob["flag"])),
+                                              r["R"], r["rphi"], rscale, zscale, dcm, fov, ob["npix"],
+                                              polarised=int(m.scat_how) == 2))
+        im = r["image"] * 1e23 * zscale / dcm ** 2
+        files.append(outputs.write_image_fits(
+            os.path.join(outdir, outputs.image_name("AI", angle, lam0, fov / 2.0, ob["flag"])), im, fov / 2.0,
+            rscale, scaletype))
+    return files
+
+
 def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opacity="dhs", compute_parts=None,
              spectra=(), spectrum_nphi=45, spectrum_nr=2, observations=()):
     """Build the deck's model, run the packet loop and the diffusion step
@@ -52,8 +86,9 @@ def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opac
     spectrum<angle>.dat.  Returns dict(model, run, nphot, result, T,
     diffused (the counts of mcg_diffuse, or None), structure, files).
     observations: MCMax observation files; their SPECTRUM observations are
-    ray-traced the same way, other kinds are skipped and listed in
-    'skipped'."""
+    ray-traced the same way, their IMAGE observations give RImage_*.dat
+    and ImageAI_*.fits (observe_image); other kinds are skipped and listed
+    in 'skipped'."""
     if compute_parts is None and opacity == "surrogate":
         compute_parts = _surrogate_parts(ctx)
     elif opacity not in ("dhs", "surrogate"):
@@ -84,19 +119,18 @@ def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opac
     files += [os.path.join(outdir, x) for x in names + ["MCSpec.dat"]]
     todo = [dict(inc=a, lam1=m.lam[0], lam2=m.lam[-1], nlam=-1, lamfile="", nphi=spectrum_nphi, nrad=spectrum_nr,
                  flag="") for a in spectra]
-    skipped = []
+    skipped, images = [], []
     for path in observations:
-        for ob in outputs.read_observations(path, m.lam, run.get("incangle", 45.0)):
-            (todo if ob["kind"] == "SPECTRUM" else skipped).append(ob)
-    if todo:
-        import math
-        rfix = fixed_radii(run["zones"], m.R[1], m.R[-1])
-        for ob in todo:
-            lam_obs = outputs.spectrum_wavelengths(m.lam, ob["lam1"], ob["lam2"], ob["nlam"], ob["lamfile"] or None)
-            flux, _ = ctx.trace_spectrum(T, lam_obs, math.radians(ob["inc"]), nphi=ob["nphi"], nr=ob["nrad"],
-                                         Rfix=rfix)
-            files.append(outputs.write_spectrum(outdir, ob["inc"], lam_obs, flux, m.lam, m.Fstar, m.distance,
-                                                flag=ob["flag"]))
+        for ob in outputs.read_observations(path, m.lam, run.get("incangle", 45.0), rout=m.R[-1]):
+            {"SPECTRUM": todo, "IMAGE": images}.get(ob["kind"], skipped).append(ob)
+    rfix = fixed_radii(run["zones"], m.R[1], m.R[-1])
+    for ob in todo:
+        lam_obs = outputs.spectrum_wavelengths(m.lam, ob["lam1"], ob["lam2"], ob["nlam"], ob["lamfile"] or None)
+        flux, _ = ctx.trace_spectrum(T, lam_obs, math.radians(ob["inc"]), nphi=ob["nphi"], nr=ob["nrad"], Rfix=rfix)
+        files.append(outputs.write_spectrum(outdir, ob["inc"], lam_obs, flux, m.lam, m.Fstar, m.distance,
+                                            flag=ob["flag"]))
+    for ob in images:
+        files += observe_image(ctx, m, T, ob, outdir, rfix, seed=run["seed"], posangle=run.get("posangle", 0.0))
     return dict(model=m, run=run, nphot=n, result=res, T=T, diffused=diffused, structure=structure, files=files,
                 skipped=[ob["kind"] for ob in skipped])
 
@@ -105,7 +139,7 @@ def parse_args(argv):
     ap = argparse.ArgumentParser(prog="python -m mcmax_b200.run", description=__doc__.split("\n\n")[0])
     ap.add_argument("deck")
     ap.add_argument("nphot", type=lambda s: int(float(s)))
-    ap.add_argument("observations", nargs="*", help="MCMax observation files (SPECTRUM observations are traced)")
+    ap.add_argument("observations", nargs="*", help="MCMax observation files (SPECTRUM and IMAGE observations are traced)")
     ap.add_argument("-o", dest="outdir", default=".")
     ap.add_argument("-s", dest="overrides", action="append", default=[], metavar="key=value")
     ap.add_argument("--precision", choices=("mixed", "fp64", "exact"), default="mixed")

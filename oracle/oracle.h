@@ -183,6 +183,14 @@ int orc_trace_spectrum(const orc_model *m, const double *Kabs_c, const double *K
                        double lam_path, int tracestar, double dimstar, int nobs, const double *lam_obs, double *flux,
                        int *info);
 
+/* MakeImage without polarisation, planets or convolution: npix^2 image
+ * im[(ix-1) npix + (iy-1)], flux[0] at lam0; the points' uniforms from
+ * Philox (key seed, counter (0, 1, s_lo, s_hi)) */
+int orc_trace_image(const orc_model *m, const double *Kabs_c, const double *Ksca_c, const double *T, int scat_how,
+                    double angle, int nphi, int nj0, int nRfix, const double *Rfix, int tracestar, double dimstar,
+                    double lam0, int npix, int nint, double Rmax, double pa, uint64_t seed, int linear, double *flux,
+                    double *im, int *info);
+
 /* ran1 (Numerical Recipes minimal standard + shuffle), Subroutines.f:1481-1509 */
 double orc_ran1(int32_t *idum, int32_t *iv, int32_t *iy);
 

@@ -977,10 +977,26 @@ static void sel_sort(double *x, int n) { /* sort, Subroutines.f:1907-1927 */
   }
 }
 
+static int trace_run(const orc_model *m, const double *Kabs_c, const double *Ksca_c, const double *T, int scat_how,
+                     double angle, int nphi, int nj0, int nRfix, const double *Rfix, double lam_path, int tracestar,
+                     double dimstar, int nobs, const double *lam_obs, double *flux, int *info, double **Ri_out,
+                     double **image_out);
+
 int orc_trace_spectrum(const orc_model *m, const double *Kabs_c, const double *Ksca_c, const double *T,
                        int scat_how, double angle, int nphi, int nj0, int nRfix, const double *Rfix,
                        double lam_path, int tracestar, double dimstar, int nobs, const double *lam_obs, double *flux,
                        int *info) {
+  return trace_run(m, Kabs_c, Ksca_c, T, scat_how, angle, nphi, nj0, nRfix, Rfix, lam_path, tracestar, dimstar, nobs,
+                   lam_obs, flux, info, NULL, NULL);
+}
+
+/* TracePath + TraceFlux (TraceMono.f:2032-2297, 8-497); when Ri_out and
+ * image_out are given they receive (malloc'ed) the image radii and the last
+ * wavelength's intensities, radius-major */
+static int trace_run(const orc_model *m, const double *Kabs_c, const double *Ksca_c, const double *T, int scat_how,
+                     double angle, int nphi, int nj0, int nRfix, const double *Rfix, double lam_path, int tracestar,
+                     double dimstar, int nobs, const double *lam_obs, double *flux, int *info, double **Ri_out,
+                     double **image_out) {
   const int nR = m->nr, nTheta = m->nt, nc = nTheta - 1, ncell = nR * nc, nstar = 30;
   mc_t s;
   memset(&s, 0, sizeof s);
@@ -1130,7 +1146,7 @@ int orc_trace_spectrum(const orc_model *m, const double *Kabs_c, const double *K
       }
     }
   /* TraceFlux per wavelength */
-  double *image = (double *)malloc(sizeof(double) * (size_t)nimg * nphi);
+  double *image = (double *)calloc((size_t)nimg * nphi, sizeof(double));
   for (int l = 0; l < nobs; ++l) {
     const double lam0 = lam_obs[l];
     flux[l] = 0.0;
@@ -1197,6 +1213,89 @@ int orc_trace_spectrum(const orc_model *m, const double *Kabs_c, const double *K
     free(paths[q].j);
     free(paths[q].v);
   }
-  free(paths); free(phi); free(image); free(Ri); free(ta); free(kext); free(emis);
+  free(paths); free(phi); free(ta); free(kext); free(emis);
+  if (Ri_out && image_out) {
+    *Ri_out = Ri;
+    *image_out = image;
+  } else {
+    free(Ri);
+    free(image);
+  }
+  return 0;
+}
+
+/* MakeImage (TraceMono.f:2759-3001) for an image without polarisation,
+ * planets or convolution.  Loop order i (image ring), j (angle column), k
+ * (point), as the reference's single-threaded run; point s = (i nphi + j)
+ * nint + k takes its two uniforms from one Philox block with key seed and
+ * counter (0, 1, s_lo, s_hi).  The interpolation is the 10**() of the
+ * interpolated log10 I (TraceMono.f:2931-2934), evaluated as exp of the
+ * interpolated natural logarithm, or linear (linear != 0: the value the
+ * polarised branch falls back to when Q = U = V = 0, TraceMono.f:2901-2920).
+ * im[(ix-1) npix + (iy-1)]. */
+int orc_trace_image(const orc_model *m, const double *Kabs_c, const double *Ksca_c, const double *T, int scat_how,
+                    double angle, int nphi, int nj0, int nRfix, const double *Rfix, int tracestar, double dimstar,
+                    double lam0, int npix, int nint, double Rmax, double pa, uint64_t seed, int linear, double *flux,
+                    double *im, int *info) {
+  double *Ri = NULL, *image = NULL;
+  trace_run(m, Kabs_c, Ksca_c, T, scat_how, angle, nphi, nj0, nRfix, Rfix, lam0, tracestar, dimstar, 1, &lam0, flux,
+            info, &Ri, &image);
+  const int nimg = info[0];
+  memset(im, 0, sizeof(double) * (size_t)npix * npix);
+  const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+  long long s = 0;
+  for (int i = 1; i <= nimg - 1; ++i)
+    for (int j = 1; j <= nphi; ++j) {
+      const double w2 = (((2.0 * PI_D) * (AU_CM * AU_CM)) * (Ri[i] - Ri[i - 1])) / (double)(float)nphi;
+      for (int k = 1; k <= nint; ++k, ++s) {
+        const uint32_t ctr[4] = {0u, 1u, (uint32_t)s, (uint32_t)((unsigned long long)s >> 32)};
+        uint32_t o[4];
+        px_philox4x32_10(ctr, key, o);
+        const double ranR = px_u01(o[0], o[1]), ranPhi = px_u01(o[2], o[3]);
+        const double R = Ri[i - 1] + (Ri[i] - Ri[i - 1]) * ranR;
+        const double phi = (PI_D * ((double)(float)(j - 1) + ranPhi)) / (double)(float)nphi;
+        int jp1, jp2;
+        double wp1, wp2;
+        if (ranPhi < 0.5) {
+          wp1 = 0.5 - ranPhi;
+          jp1 = j - 1;
+          if (jp1 == 0) jp1 = 1;
+          wp2 = ranPhi + 0.5;
+          jp2 = j;
+        } else {
+          wp1 = ranPhi - 0.5;
+          jp1 = j + 1;
+          if (jp1 == nphi + 1) jp1 = nphi;
+          wp2 = 1.5 - ranPhi;
+          jp2 = j;
+        }
+        const double wr1 = 1.0 - ranR, wr2 = ranR;
+        /* image(ir, jp) of the reference, ir = i, i+1 (1-based) */
+        const double I11 = image[(size_t)(i - 1) * nphi + (jp1 - 1)], I12 = image[(size_t)(i - 1) * nphi + (jp2 - 1)];
+        const double I21 = image[(size_t)i * nphi + (jp1 - 1)], I22 = image[(size_t)i * nphi + (jp2 - 1)];
+        double f;
+        if (linear) {
+          f = ((wr1 * (wp1 * I11 + wp2 * I12) + wr2 * (wp1 * I21 + wp2 * I22)) * w2) * R;
+        } else {
+          f = wr1 * (wp1 * dm_log(I11) + wp2 * dm_log(I12)) + wr2 * (wp1 * dm_log(I21) + wp2 * dm_log(I22));
+          f = (dm_exp(f) * w2) * R;
+        }
+        const double add = f / (double)(float)(2 * nint);
+        for (int side = 0; side < 2; ++side) {
+          const double a = side == 0 ? phi + (pa * PI_D) / 180.0 : -phi + (pa * PI_D) / 180.0;
+          double x = -R * dm_cos(a);
+          x = (((double)(float)npix * (x + Rmax)) / (2.0 * Rmax)) + 1.0;
+          double y = R * dm_sin(a);
+          y = (((double)(float)npix * (y + Rmax)) / (2.0 * Rmax)) + 1.0;
+          /* ix = x truncates toward zero; kept when 1 <= ix <= npix */
+          if (x >= 1.0 && x < (double)npix + 1.0 && y >= 1.0 && y < (double)npix + 1.0) {
+            const int ix = (int)x, iy = (int)y;
+            im[(size_t)(ix - 1) * npix + (iy - 1)] = im[(size_t)(ix - 1) * npix + (iy - 1)] + add;
+          }
+        }
+      }
+    }
+  free(Ri);
+  free(image);
   return 0;
 }

@@ -176,3 +176,25 @@ def trace_spectrum(model, T, lam_obs, angle, nphi=45, nj0=2, Rfix=(), lam_path=0
     assert rc == 0
     nr = int(info[0])
     return flux, Rimg[:nr], image[:nr * nphi].reshape(nr, nphi), int(info[1])
+
+
+def trace_image(model, T, lam0, angle, npix, nint, Rmax, pa=0.0, seed=42, linear=0, nphi=45, nj0=2, Rfix=(),
+                tracestar=1, dimstar=1.0, dens=None):
+    """the host logic of mcg_trace_image with its kernels as one loop over
+    the points; returns (image (npix, npix), flux, image radii, bad rays)"""
+    L = load()
+    m = model
+    dens = np.maximum(np.asarray(m.dens, float), 1e-50) if dens is None else np.asarray(dens, float)
+    arrs = [np.ascontiguousarray(a, float) for a in (m.R, m.Theta, dens, m.comp_w, m.Kabs, m.Ksca, m.BB, m.lam,
+                                                     m.Fstar, T)]
+    Rfix = np.ascontiguousarray(Rfix, float)
+    flux = np.zeros(1)
+    im = np.zeros(npix * npix)
+    info = np.zeros(2, np.int32)
+    rc = L.hc_trace_image(m.nr, m.nt, P(arrs[0]), P(arrs[1]), P(arrs[2]), int(m.scat_how), m.ncomp, m.nlam,
+                          P(arrs[3]), P(arrs[4]), P(arrs[5]), P(arrs[6]), P(arrs[7]), P(arrs[8]), P(arrs[9]),
+                          C.c_double(angle), int(nphi), int(nj0), int(Rfix.size), P(Rfix) if Rfix.size else None,
+                          int(tracestar), C.c_double(dimstar), C.c_double(lam0), int(npix), int(nint),
+                          C.c_double(Rmax), C.c_double(pa), C.c_ulonglong(seed), int(linear), P(flux), P(im), P(info))
+    assert rc == 0
+    return im.reshape(npix, npix), float(flux[0]), int(info[0]), int(info[1])

@@ -456,3 +456,31 @@ extern "C" int hc_trace_spectrum(int nr, int nt, const double *R, const double *
     std::copy(image.begin(), image.end(), image_out);
   return 0;
 }
+
+/* the rectangular image on the host: mcg_trace_image's host logic with the
+ * sample and pixel kernels replaced by one loop over the points in order */
+extern "C" int hc_trace_image(int nr, int nt, const double *R, const double *Theta, const double *dens, int scat_how,
+                              int ncomp, int nlam, const double *comp_w, const double *Kabs_c, const double *Ksca_c,
+                              const double *BB, const double *lam, const double *Fstar, const double *T, double angle,
+                              int nphi, int nj0, int nRfix, const double *Rfix, int tracestar, double dimstar,
+                              double lam0, int npix, int nint, double Rmax, double pa, unsigned long long seed,
+                              int linear, double *flux, double *im, int *info) {
+  const int cap = (int)rt_image_radii_count(nr, nt, nj0, nRfix, scat_how);
+  std::vector<double> Rimg(cap), image((size_t)cap * nphi);
+  if (hc_trace_spectrum(nr, nt, R, Theta, dens, scat_how, ncomp, nlam, comp_w, Kabs_c, Ksca_c, BB, lam, Fstar, T,
+                        angle, nphi, nj0, nRfix, Rfix, lam0, tracestar, dimstar, 1, &lam0, flux, info, Rimg.data(),
+                        cap, image.data()) != 0)
+    return 1;
+  const int ni = info[0];
+  if (ni > cap) return 2;
+  std::fill(im, im + (size_t)npix * npix, 0.0);
+  const long long ns = (long long)(ni - 1) * nphi * nint;
+  for (long long s = 0; s < ns; ++s) {
+    uint32_t key[2];
+    double v;
+    rt_image_sample(s, nphi, nint, Rimg.data(), image.data(), (uint64_t)seed, Rmax, pa, npix, linear, key, &v);
+    for (int m = 0; m < 2; ++m)
+      if (key[m] < (uint32_t)npix * (uint32_t)npix) im[key[m]] = im[key[m]] + v;
+  }
+  return 0;
+}

@@ -285,3 +285,25 @@ def trace_spectrum(model, T, lam_obs, angle, nphi=45, nj0=2, Rfix=(), lam_path=0
                          int(nphi), int(nj0), int(Rfix.size), P(Rfix) if Rfix.size else None, C.c_double(lam_path),
                          int(tracestar), C.c_double(dimstar), int(lam_obs.size), P(lam_obs), P(flux), P(info))
     return flux, int(info[0]), int(info[1])
+
+
+def trace_image(model, T, lam0, angle, npix, nint, Rmax, pa=0.0, seed=42, linear=0, nphi=45, nj0=2, Rfix=(),
+                tracestar=1, dimstar=1.0, dens=None):
+    """orc_trace_image; returns (image (npix, npix), flux, image radii, bad rays)"""
+    L = load()
+    m = model
+    dens = np.maximum(np.asarray(m.dens, float), 1e-50) if dens is None else np.asarray(dens, float)
+    keep = [np.ascontiguousarray(a, float) for a in (m.R, m.Theta, m.SinTheta, dens, m.V, m.lam, m.nu, m.BB, m.Fstar,
+                                                     m.comp_w, m.Kabs, m.Ksca, T)]
+    om = OrcModel(m.nr, m.nt, P(keep[0]), P(keep[1]), P(keep[2]), P(keep[3]), P(keep[4]), None, m.nlam, P(keep[5]),
+                  P(keep[6]), None, None, None, 0, P(keep[7]), P(keep[8]), float(m.Lstar), m.ncomp, P(keep[9]), None,
+                  None, None, None, None, None, None, None, None, None, None)
+    Rfix = np.ascontiguousarray(Rfix, float)
+    flux = np.zeros(1)
+    im = np.zeros(npix * npix)
+    info = np.zeros(2, np.int32)
+    L.orc_trace_image(C.byref(om), P(keep[10]), P(keep[11]), P(keep[12]), int(m.scat_how), C.c_double(angle),
+                      int(nphi), int(nj0), int(Rfix.size), P(Rfix) if Rfix.size else None, int(tracestar),
+                      C.c_double(dimstar), C.c_double(lam0), int(npix), int(nint), C.c_double(Rmax), C.c_double(pa),
+                      C.c_uint64(seed), int(linear), P(flux), P(im), P(info))
+    return im.reshape(npix, npix), float(flux[0]), int(info[0]), int(info[1])

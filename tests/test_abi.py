@@ -51,7 +51,7 @@ def test_invalid_arguments_do_not_abort():
 
 PAIRS = [("mcg_part_in", "PartIn"), ("mcg_part_out", "PartOut"), ("mcg_grid", "Grid"), ("mcg_opacity", "Opacity"),
          ("mcg_run", "Run"), ("mcg_result", "Result"), ("mcg_batch_opts", "BatchOpts"), ("mcg_zone", "Zone"),
-         ("mcg_structure", "Structure"), ("mcg_trace_opts", "TraceOpts"),
+         ("mcg_structure", "Structure"), ("mcg_trace_opts", "TraceOpts"), ("mcg_image_opts", "ImageOpts"),
          ("mcg_mlp_train_opts", "MlpTrainOpts"), ("mcg_mlp_train_report", "MlpTrainReport")]
 
 

@@ -25,3 +25,38 @@ def test_trace_spectrum_matches_replay(ctx, deg):
     fh, Rimg, _, bad = H.trace_spectrum(m, T, lam, math.radians(deg), nphi=30, nj0=2)
     assert info == (Rimg.size, bad) and bad == 0
     assert np.array_equal(fg, fh)
+
+
+@pytest.mark.parametrize("deg,pa,linear", [(45.0, 20.0, 0), (80.0, 0.0, 1)])
+def test_trace_image_matches_replay(ctx, deg, pa, linear):
+    """the sample kernel, the stable sort and the per-pixel sums give the
+    sequential loop's image bit for bit"""
+    m = models.small_disk(nrad=20, ntheta=12, nlam=30, mdust=1e-5)
+    nc = m.nt - 1
+    R_av = np.sqrt(m.R[:-1] * m.R[1:])
+    T = np.maximum((400.0 * R_av[:, None] ** -0.5 * np.ones(nc)[None, :]).ravel(), 3.0)
+    ctx.set_model(m)
+    Rmax = 0.6 * float(m.R[-1])
+    g = ctx.trace_image(T, 10.0, math.radians(deg), npixel=64, nint=50, Rmax=Rmax, pa=pa, nphi=30, nr=2, seed=9,
+                        linear=bool(linear))
+    ih, fh, nh, bh = H.trace_image(m, T, 10.0, math.radians(deg), 64, 50, Rmax, pa=pa, seed=9, linear=linear,
+                                   nphi=30, nj0=2)
+    assert g["info"] == (nh, bh) and bh == 0
+    assert g["flux"] == fh
+    assert np.array_equal(g["image"], ih)
+    _, Rimg, rphi, _ = H.trace_spectrum(m, T, [10.0], math.radians(deg), nphi=30, nj0=2, lam_path=10.0)
+    assert np.array_equal(g["R"], Rimg) and np.array_equal(g["rphi"], rphi)
+
+
+def test_trace_image_in_chunks(ctx):
+    """more points than one sort chunk (2^23): the pixel sums carry over"""
+    m = models.small_disk(nrad=12, ntheta=8, nlam=20, mdust=1e-5)
+    nc = m.nt - 1
+    R_av = np.sqrt(m.R[:-1] * m.R[1:])
+    T = np.maximum((300.0 * R_av[:, None] ** -0.5 * np.ones(nc)[None, :]).ravel(), 3.0)
+    ctx.set_model(m)
+    g = ctx.trace_image(T, 3.0, math.radians(30.0), npixel=32, nint=800, nphi=45, nr=2, seed=3)
+    n = (g["info"][0] - 1) * 45 * 800
+    assert n > (1 << 23)
+    ih, fh, _, _ = H.trace_image(m, T, 3.0, math.radians(30.0), 32, 800, float(m.R[-1]), seed=3, nphi=45, nj0=2)
+    assert np.array_equal(g["image"], ih)

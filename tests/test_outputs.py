@@ -84,3 +84,45 @@ def test_denstemp_fits_round_trip(tmp_path):
     hdr = PF._read_hdus(PF._open(p))[0][0]
     assert (hdr["NR"], hdr["NTHETA"], hdr["NGRAINS"], hdr["NHDU"]) == (m.nr - 1, m.nt - 1, m.ncomp, 5)
     assert hdr["HDU 3"] == "COMP"
+
+
+def test_image_file_names_follow_the_reference_formats():
+    deg = lambda a: math.pi * a / 180.0
+    assert OUT.image_name("AI", deg(45.0), 0.6, 50.0) == "ImageAI_i45.0_l00000.60_fov00100.0.fits"
+    assert OUT.rimage_name(deg(30.0), 1234.5678, "_x") == "RImage_i30.0_l01234.57_x.dat"
+    # tenths of 9.95 and up carry into the tens (angle and field of view)
+    assert OUT._angle_tag(deg(39.97)) == "40.0"
+    assert OUT._fov_tag(99.97 / 2.0) == "00100.0"
+    # a value that does not fit f4.2 prints as asterisks, as Fortran does
+    assert OUT._lam_tag(9.999) == "0000****"
+
+
+def test_image_fits_round_trip(tmp_path):
+    im = np.arange(12.0 * 12.0).reshape(12, 12) * 1e-3
+    p = OUT.write_image_fits(str(tmp_path / "ImageAI_x.fits"), im, 25.0, rscale=0.01, scaletype=2)
+    raw = open(p, "rb").read()
+    assert len(raw) % 2880 == 0
+    hdr, back = OUT.read_image_fits(p)
+    assert np.array_equal(back, im)
+    assert hdr["NAXIS1"] == 12 and hdr["BITPIX"] == -64
+    assert hdr["CRPIX1"] == 0.5 and abs(hdr["CRVAL2"] + 0.25) < 1e-12 and abs(hdr["CDELT1"] - 0.5 / 12) < 1e-12
+    assert hdr["CTYPE2"].strip() == "Y [arcsec]"
+
+
+def test_rimage_profile(tmp_path):
+    """running trapezoid flux per image radius, the total on the last row,
+    the intensity at column nphi/2 times the pixel scaling"""
+    R = np.array([0.0, 1.0, 2.5, 4.0])
+    rphi = np.outer([4.0, 3.0, 2.0, 1.0], np.ones(6)) * 1e-10
+    d = 140.0 * OUT.PARSEC
+    p = OUT.write_rimage(str(tmp_path / "RImage.dat"), R, rphi, 1.0, 1.0, d, 10.0, 100)
+    rows = np.loadtxt(p)
+    AU = M.AU
+    ring = [(R[i + 1] - R[i]) * math.pi * AU ** 2 * (R[i] * rphi[i, 0] + R[i + 1] * rphi[i + 1, 0])
+            for i in range(3)]
+    assert rows.shape == (4, 3)
+    assert np.allclose(rows[:, 0], R)
+    assert np.allclose(rows[:3, 1], np.cumsum(ring) * 1e23 / d ** 2, rtol=1e-12)
+    assert rows[3, 1] == rows[2, 1]
+    scaling = 1e23 / d ** 2 * 10.0 ** 2 * AU ** 2 / 100 ** 2
+    assert np.allclose(rows[:, 2], scaling * rphi[:, 2], rtol=1e-12)

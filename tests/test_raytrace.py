@@ -78,3 +78,54 @@ def test_wavelengths_outside_the_grid_give_zero():
     m = models.small_disk(nrad=20, ntheta=12, nlam=30, mdust=1e-5)
     f, _, _, _ = H.trace_spectrum(m, _temps(m), [0.01, 1e5, 1.0], 0.3)
     assert f[0] == 0.0 and f[1] == 0.0 and f[2] > 0.0
+
+
+@pytest.mark.parametrize("deg,pa,linear,nj0", [(45.0, 20.0, 0, 2), (80.0, 0.0, 1, 2), (10.0, -35.0, 0, -2)])
+def test_image_replay_matches_oracle(deg, pa, linear, nj0):
+    """MakeImage: the host logic of mcg_trace_image (per-point function of
+    the sample kernel, points summed in order) against the oracle's own
+    loop, bit for bit"""
+    m = models.small_disk(nrad=20, ntheta=12, nlam=30, mdust=1e-5)
+    T = _temps(m)
+    Rmax = 0.7 * float(m.R[-1])
+    io, fo, no, bo = O.trace_image(m, T, 10.0, math.radians(deg), 48, 20, Rmax, pa=pa, seed=5, linear=linear,
+                                   nphi=30, nj0=nj0)
+    ih, fh, nh, bh = H.trace_image(m, T, 10.0, math.radians(deg), 48, 20, Rmax, pa=pa, seed=5, linear=linear,
+                                   nphi=30, nj0=nj0)
+    assert (no, bo) == (nh, bh) and bo == 0
+    assert fo == fh and np.array_equal(io, ih)
+    assert np.all(np.isfinite(ih)) and np.all(ih >= 0) and (ih > 0).sum() > 100
+
+
+@pytest.mark.parametrize("linear,tol", [(1, 0.01), (0, 0.03)])
+def test_image_total_is_the_flux(linear, tol):
+    """a field of view around the whole grid collects every point: the
+    pixel sum is the Monte Carlo estimate of the flux the trapezoid gives
+    (the log-linear interpolation lies a little below the linear one)"""
+    m = models.small_disk(nrad=20, ntheta=12, nlam=30, mdust=1e-5)
+    T = _temps(m)
+    im, f, n, _ = H.trace_image(m, T, 10.0, math.radians(45.0), 64, 40, 1.01 * float(m.R[-1]), seed=1,
+                                linear=linear, nphi=30)
+    assert abs(im.sum() / f - 1.0) < tol, im.sum() / f
+
+
+def test_image_is_mirror_symmetric():
+    """every point also lands at -phi: with no position angle the image is
+    symmetric under y -> -y up to points on a pixel edge"""
+    m = models.small_disk(nrad=20, ntheta=12, nlam=30, mdust=1e-5)
+    im, f, _, _ = H.trace_image(m, _temps(m), 10.0, math.radians(60.0), 40, 30, float(m.R[-1]), seed=2, nphi=30)
+    assert abs(im.sum() - im[:, ::-1].sum()) <= 1e-12 * im.sum()
+    same = np.isclose(im, im[:, ::-1], rtol=1e-12, atol=0)
+    assert same.mean() > 0.98, same.mean()
+
+
+def test_image_rotates_with_the_position_angle():
+    """pa = 90 degrees turns the image by a quarter: a point at (x, y)
+    moves to (y, -x), so b[i, j] = a[n-1-j, i] in 0-based pixels"""
+    m = models.small_disk(nrad=20, ntheta=12, nlam=30, mdust=1e-5)
+    T = _temps(m)
+    R = float(m.R[-1])
+    a, _, _, _ = H.trace_image(m, T, 10.0, math.radians(60.0), 40, 30, R, pa=0.0, seed=2, nphi=30)
+    b, _, _, _ = H.trace_image(m, T, 10.0, math.radians(60.0), 40, 30, R, pa=90.0, seed=2, nphi=30)
+    assert abs(b.sum() / a.sum() - 1.0) < 1e-12
+    assert np.isclose(b, a[::-1].T, rtol=1e-9, atol=0).mean() > 0.97

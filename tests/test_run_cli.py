@@ -72,6 +72,14 @@ class FakeContext:
         self.trace_args = (angle, nphi, nr, tuple(Rfix))
         return np.full(len(lam_obs), 1e20), (100, 0)
 
+    def trace_image(self, T, lam0, angle, npixel=500, nint=1000, Rmax=None, pa=0.0, nphi=45, nr=2, Rfix=(),
+                    seed=42):
+        self.image_args = dict(lam0=lam0, angle=angle, npixel=npixel, nint=nint, Rmax=Rmax, pa=pa, nphi=nphi, nr=nr,
+                               seed=seed)
+        R = np.linspace(0.0, 50.0, 11)
+        return dict(image=np.full((npixel, npixel), 2.0), flux=1.0, R=R, rphi=np.ones((R.size, nphi)),
+                    info=(R.size, 0))
+
     def close(self):
         self.closed = True
 
@@ -117,7 +125,9 @@ def test_command_line_runs_the_deck_and_writes_result_files(tmp_path):
 def test_observation_files_drive_spectra(tmp_path):
     deck = _write_inputs(tmp_path)
     (tmp_path / "Spectrum.out").write_text("nphi=30\nnrad=1\n*****\ntype='SPECTRUM'\ninc=60\nflag='_a'\n"
-                                           "type='IMAGE'\nlam=0.6\ntype='SPECTRUM'\nlam1=1\nlam2=100\nnlam=5\n")
+                                           "type='IMAGE'\nlam=0.6\nnpix=16\nnint=3\n"
+                                           "type='SPECTRUM'\nlam1=1\nlam2=100\nnlam=5\n"
+                                           "type='VISIBILITY'\n")
     made = []
 
     def factory(device):
@@ -127,7 +137,17 @@ def test_observation_files_drive_spectra(tmp_path):
     r = R.main([deck, "1e3", str(tmp_path / "Spectrum.out"), "-o", str(tmp_path / "o")], context=factory)
     names = [os.path.basename(f) for f in r["files"] if "spectrum" in f]
     assert names == ["spectrum60.0_a.dat", "spectrum45.0.dat"]
-    assert r["skipped"] == ["IMAGE"]
+    assert r["skipped"] == ["VISIBILITY"]
+    images = [os.path.basename(f) for f in r["files"] if "Image" in f]
+    assert images == ["RImage_i45.0_l00000.60.dat", "ImageAI_i45.0_l00000.60_fov00100.0.fits"]
+    a = made[0].image_args
+    rout = float(r["model"].R[-1])
+    assert (a["lam0"], a["npixel"], a["nint"], a["Rmax"], a["nphi"], a["nr"], a["pa"]) == (0.6, 16, 3, rout, 30, 1, 0.0)
+    hdr, im = outputs.read_image_fits(str(tmp_path / "o" / images[1]))
+    d = 100.0 * outputs.PARSEC
+    assert im.shape == (16, 16) and np.allclose(im, 2.0 * 1e23 / d ** 2, rtol=1e-15)
+    assert abs(hdr["CRVAL1"] / -rout - 1) < 1e-10 and abs(hdr["CDELT2"] / (2 * rout / 16) - 1) < 1e-10
+    assert hdr["CTYPE1"].strip() == "X [AU]"
     rows = np.loadtxt(str(tmp_path / "o" / "spectrum45.0.dat"))
     assert rows.shape[0] == 5 and np.allclose(rows[[0, -1], 0], [1.0, 100.0])
     assert made[0].trace_args[1:3] == (30, 1)
