@@ -55,8 +55,10 @@ def test_trace_image_in_chunks(ctx):
     R_av = np.sqrt(m.R[:-1] * m.R[1:])
     T = np.maximum((300.0 * R_av[:, None] ** -0.5 * np.ones(nc)[None, :]).ravel(), 3.0)
     ctx.set_model(m)
-    g = ctx.trace_image(T, 3.0, math.radians(30.0), npixel=32, nint=800, nphi=45, nr=2, seed=3)
+    g = ctx.trace_image(T, 3.0, math.radians(30.0), npixel=32, nint=800, nphi=45, nr=2, seed=3, linear=False)
     n = (g["info"][0] - 1) * 45 * 800
     assert n > (1 << 23)
-    ih, fh, _, _ = H.trace_image(m, T, 3.0, math.radians(30.0), 32, 800, float(m.R[-1]), seed=3, nphi=45, nj0=2)
+    ih, fh, _, _ = H.trace_image(m, T, 3.0, math.radians(30.0), 32, 800, float(m.R[-1]), seed=3, linear=0, nphi=45,
+                                 nj0=2)
+    assert g["flux"] == fh
     assert np.array_equal(g["image"], ih)
