@@ -279,6 +279,93 @@ def zones_density(R, Theta, thet, zones):
     dens[1:] = 1e-60 + total[1:]
     return dens, V
 
+ANALYTIC_DENSITIES = ("PASCUCCI", "MIN", "PARAMETERIZED", "PINTE", "SHELL", "WEDGE")
+
+
+def analytic_density(denstype, R, Theta, thet, p, lam=None, kext=None):
+    """The closed-form dust densities of Init.f:3142-3240 that need no
+    initial structure iteration: PASCUCCI (the radiative-transfer benchmark
+    disk, scaled to the midplane optical depth tau550 at 0.55 micron,
+    Init.f:3992-4026), MIN and PINTE (Gaussian vertical profile of scale
+    height sh1AU r^shpow; PINTE cut at r = Rexp), PARAMETERIZED (the same,
+    averaged over 10 sub-angles), SHELL ((AU/R)^denspow) and WEDGE (the
+    cells within wedgeopen degrees of the midplane, 10 sub-angles).  r and z
+    are taken at the cell centre (R_av, theta_av); cell i = 0 is empty.
+
+    p: dict of the deck's rin, rout [AU], denspow, shpow, sh1au, rexp,
+    tau550, wedgeopen, and mtot [g] with mdustscale (mdust given).  lam,
+    kext (ngrains, nlam) are needed for PASCUCCI: its tau550 uses the sum
+    of the grains' Kext at 0.55 micron, unweighted, as the reference forms
+    it.  Then the mass normalisation of Init.f:3242-3264: the densities are
+    scaled to mtot when mdust was given (never for PASCUCCI), else kept.
+    Densities below 1e-60 are raised to 1e-60, the floor the 'ZONES' cells
+    start from.  Returns (dens (nR, ncells per ring), V)."""
+    nR = R.size - 1
+    nc = Theta.size - 1
+    V = cell_volumes(R, Theta)
+    R_av = AU * 10.0 ** ((np.log10(R[:-1]) + np.log10(R[1:])) / 2.0)
+    Theta = np.asarray(Theta, float)
+    thet = np.asarray(thet, float)
+    theta_av = np.arccos((Theta[:-1] + Theta[1:]) / 2.0)
+    r = R_av[:, None] * np.sin(theta_av)[None, :] / AU
+    z = R_av[:, None] * np.cos(theta_av)[None, :] / AU
+    rin, rout = p["rin"], p["rout"]
+    mtot = p["mtot"]
+    mdustscale = p["mdustscale"]
+    with np.errstate(over="ignore", under="ignore", divide="ignore"):
+        if denstype == "PASCUCCI":
+            # Init.f:3992-4026: the tau550 form replaces the mass-scaled one
+            l55 = float(np.float32(0.55))
+            lam = np.asarray(lam, float)
+            il1, w1, w2 = 0, 1.0, 0.0
+            for i in range(lam.size - 1):
+                if lam[i] <= l55 <= lam[i + 1]:
+                    il1 = i
+                    w1 = (lam[i + 1] - l55) / (lam[i + 1] - lam[i])
+                    w2 = (l55 - lam[i]) / (lam[i + 1] - lam[i])
+            kext = np.atleast_2d(np.asarray(kext, float))
+            k550 = 0.0
+            for row in kext:
+                k550 = k550 + row[il1] * w1 + row[il1 + 1] * w2
+            rd, zd = rout / 2.0, rout / 8.0
+            scale = p["tau550"] / (rd * math.log(rout / rin) * k550)
+            hr = zd * (r / rd) ** 1.125
+            dens = (r / rd) ** (-1.0) * np.exp(-(math.pi / 4.0) * (z / hr) ** 2) * scale / AU
+            mdustscale = False
+        elif denstype in ("MIN", "PINTE"):
+            hr = p["sh1au"] * r ** p["shpow"]
+            scale = mtot / (AU ** 3 * 2.0 * math.pi * p["sh1au"] * math.sqrt(math.pi) * (rout - rin))
+            dens = scale * r ** (-p["denspow"]) * np.exp(-(z / hr) ** 2) * r ** (-p["shpow"])
+            if denstype == "PINTE":
+                dens = np.where(r < p["rexp"], dens, 1e-60)
+        elif denstype == "PARAMETERIZED":
+            scale = mtot / (AU ** 3 * 2.0 * math.pi * p["sh1au"] * math.sqrt(math.pi) * (rout - rin))
+            dens = np.zeros((nR, nc))
+            for jj in range(1, 11):
+                theta = thet[:-1] + (thet[1:] - thet[:-1]) * jj / 11.0
+                rr = R_av[:, None] * np.sin(theta)[None, :] / AU
+                zz = R_av[:, None] * np.cos(theta)[None, :] / AU
+                hr = p["sh1au"] * rr ** p["shpow"]
+                dens = dens + scale * rr ** (-p["denspow"]) * np.exp(-(zz / hr) ** 2) / hr / 10.0
+        elif denstype == "SHELL":
+            dens = np.broadcast_to(((AU / R_av) ** p["denspow"])[:, None], (nR, nc)).copy()
+        elif denstype == "WEDGE":
+            dens = np.full((nR, nc), 1e-200)
+            for jj in range(1, 11):
+                theta = thet[:-1] + (thet[1:] - thet[:-1]) * jj / 11.0
+                inside = (180.0 * (math.pi / 2.0 - theta) / math.pi) < p["wedgeopen"]
+                dens = dens + np.where(inside[None, :], ((AU / R_av) ** (p["denspow"] + 1.0))[:, None], 0.0)
+        else:
+            raise ValueError("denstype %r is not a closed-form density" % denstype)
+    dens = np.array(dens, float)
+    dens[0] = 1e-60
+    mass = float((dens[1:] * V[1:]).sum())
+    if not mdustscale:
+        mtot = mass
+    dens[1:] = dens[1:] * (mtot / mass)
+    return np.maximum(dens, 1e-60), V
+
+
 def grain_rv(amin, amax, apow, ns):
     """rv = sqrt(<a^2>) of a bin's ns sizes in cm (ComputePart.f:950-976;
     number weights n(a) ~ a^(1 - apow) of ComputePart.f:276-292)"""
@@ -646,7 +733,9 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
     grain entry NN); fixmpset, alphaturb (settling of a one-zone
     disk); denstype 'FILE' with densfile (a denstemp.dat: its dust density
     and the grid rebuilt from its cell centres; rin and rout still give the
-    outer edges); randomwalk, factrw, maxinteract, nruns, idum; nphotdiffuse,
+    outer edges); the closed-form denstypes of analytic_density (PASCUCCI,
+    MIN, PARAMETERIZED, PINTE, SHELL, WEDGE) with denspow, shpow, sh1au,
+    rexp, tau550, wedgeopen and mdust [Msun]; randomwalk, factrw, maxinteract, nruns, idum; nphotdiffuse,
     dtdiffuse (the diffusion step after the run); zoneN:fix, mstar,
     maxiter, epsiter (structure iterations).  A value that
     selects physics outside the packet loop (another startype or denstype,
@@ -676,8 +765,11 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
     if startype not in ("PLANCK", "FILE"):
         raise ValueError("startype: 'PLANCK' or 'FILE' stars")
     denstype = v("denstype", "ZONES", str).upper()
-    if denstype not in ("ZONES", "FILE"):
-        raise ValueError("denstype: 'ZONES' or 'FILE' densities")
+    if denstype not in ("ZONES", "FILE") + ANALYTIC_DENSITIES:
+        raise ValueError("denstype: 'ZONES', 'FILE' or one of %s (the types that start from an optically thin "
+                         "structure iteration are not built)" % ", ".join(ANALYTIC_DENSITIES))
+    if denstype == "PARAMETERIZED" and ("scalesh" in d or "rimscale" in d):
+        raise ValueError("PARAMETERIZED: scale-height factors (scalesh, rimscale) are not built")
     if not v("tcontact", True, bool):
         raise ValueError("tcontact: only thermal contact (Bjorkman-Wood with one temperature per cell)")
     scattype = v("scattype", "ISOTROPIC", str).upper()
@@ -696,6 +788,8 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
         zones.append(dict(rin=v(kz + "rin", rin), rout=v(kz + "rout", rout), mdust=v(kz + "mdust", 1e-5),
                           denspow=v(kz + "denspow", 1.0), sh=v(kz + "sh", 0.01), rsh=v(kz + "rsh", 1.0),
                           shpow=v(kz + "shpow", 1.1), fix=v(kz + "fix", False, bool)))
+    if zones and denstype in ANALYTIC_DENSITIES:
+        raise ValueError("denstype %s takes no zoneN:* keywords" % denstype)
     if not zones and denstype == "ZONES":
         raise ValueError("no zoneN:* keywords")
     # grain bins of every computepart entry (Init.f:746-789, 1323-1420)
@@ -814,6 +908,13 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
         V = cell_volumes(R, Theta)
         dens = np.full(V.shape, 1e-60)
         dens[1:] = dt["dens"]
+    elif denstype in ANALYTIC_DENSITIES:
+        R, Theta, thet, SinTheta = spatial_grid(rstar_cm, rin, rout, nrad, ntheta)
+        kext = [r["kext"] if "kext" in r else np.asarray(r["kabs"]) + np.asarray(r["ksca"]) for r in res]
+        dens, V = analytic_density(denstype, R, Theta, thet, dict(
+            rin=rin, rout=rout, denspow=v("denspow", 1.0), shpow=v("shpow", 1.3), sh1au=v("sh1au", 0.03),
+            rexp=v("rexp", 1e10), tau550=v("tau550", 100.0), wedgeopen=v("wedgeopen", 5.0),
+            mtot=v("mdust", 1e-15) * MSUN, mdustscale="mdust" in d), lam=lam, kext=kext)
     else:
         R, Theta, thet, SinTheta = spatial_grid(rstar_cm, rin, rout, nrad, ntheta)
         dens, V = zones_density(R, Theta, thet, zones)

@@ -329,3 +329,85 @@ def test_rayleigh_scattype_matrices_for_file_grains(tmp_path):
     assert np.allclose(r["F"][3, 1], -0.3 * F11 * (1 - c * c) / (1 + c * c), rtol=1e-12)
     ray = PF.read_particle_fits(str(tmp_path / "p.fits"), lam, matrix=PF.rayleigh_hg_matrix())
     assert np.allclose(ray["F"][0, 0] / ray["F"][0, 0][0], ((1 + c * c) / 2) / ((1 + c[0] ** 2) / 2), rtol=1e-12)
+
+
+def _analytic_deck(tmp_path, body):
+    import oracle_ffi as O
+    lam_tab = np.geomspace(0.05, 5000.0, 80)
+    n, k = M.synthetic_lnk(lam_tab, 0.03)
+    (tmp_path / "syn.lnk").write_text("".join("%g %g %g\n" % t for t in zip(lam_tab, n, k)))
+    (tmp_path / "dust.particle").write_text("1\n1\n'syn.lnk'\n1.0 3.0\n")
+    deck = tmp_path / "d.in"
+    deck.write_text("rin=0.1\nrout=1000\nnrad=30\nntheta=20\nlam1=0.1\nlam2=3000\nnlam=25\n"
+                    "computepart01:file='dust.particle'\n" + body)
+
+    def oracle_parts(parts):
+        return [O.compute_part(p["lam"], p["e1"][0], p["e2"][0], p["frac"], p["rho"], p["amin"], p["amax"],
+                               p["apow"], p["fmax"], p["blend"], p["porosity"], p["ns"], p["nf"]) for p in parts]
+
+    return str(deck), oracle_parts
+
+
+def _cells(m):
+    nc = m.nt - 1
+    dens = m.dens.reshape(m.nr, nc)
+    V = m.V.reshape(m.nr, nc)
+    R_av = M.AU * 10.0 ** ((np.log10(m.R[:-1]) + np.log10(m.R[1:])) / 2.0)
+    th = np.arccos((m.Theta[:-1] + m.Theta[1:]) / 2.0)
+    return dens, V, R_av[:, None] * np.sin(th)[None, :] / M.AU, R_av[:, None] * np.cos(th)[None, :] / M.AU
+
+
+def test_pascucci_density_has_the_midplane_optical_depth(tmp_path):
+    """the benchmark disk: rho ~ (r/rd)^-1 exp(-pi/4 (z/h)^2), h = rd/4
+    (r/rd)^1.125, scaled so that the midplane's radial optical depth at
+    0.55 micron, from rin to rout, is tau550"""
+    deck, parts = _analytic_deck(tmp_path, "denstype='PASCUCCI'\ntau550=100\n")
+    m, run = M.deck_model(None, deck, compute_parts=parts)
+    dens, V, r, z = _cells(m)
+    rd = 500.0
+    h = rd / 4.0 * (r / rd) ** 1.125
+    shape = (r / rd) ** -1.0 * np.exp(-(math.pi / 4.0) * (z / h) ** 2)
+    sel = dens[1:] > 1e-40          # cells above the 1e-60 floor
+    ratio = dens[1:][sel] / shape[1:][sel]
+    assert np.allclose(ratio, ratio[0], rtol=1e-12)
+    # the midplane tau of the closed form: Kext550 * scale * rd * ln(rout/rin)
+    k550 = np.interp(0.55, m.lam, m.Kabs[0] + m.Ksca[0])
+    tau = k550 * ratio[0] * M.AU * rd * math.log(1000.0 / 0.1)
+    assert abs(tau / 100.0 - 1.0) < 1e-3, tau
+    assert run["zones"] == []
+
+
+@pytest.mark.parametrize("kind", ["MIN", "PARAMETERIZED", "PINTE"])
+def test_gaussian_disks_hold_the_dust_mass(kind, tmp_path):
+    deck, parts = _analytic_deck(tmp_path, "denstype='%s'\nmdust=2d-4\nsh1au=0.05\nshpow=1.2\ndenspow=0.8\n"
+                                           "rexp=100\n" % kind)
+    m, _ = M.deck_model(None, deck, compute_parts=parts)
+    dens, V, r, z = _cells(m)
+    assert abs((dens[1:] * V[1:]).sum() / (2e-4 * M.MSUN) - 1.0) < 1e-12
+    if kind == "MIN":
+        f = r ** -0.8 * np.exp(-(z / (0.05 * r ** 1.2)) ** 2) * r ** -1.2
+        sel = dens[1:] > 1e-40
+        ratio = dens[1:][sel] / f[1:][sel]
+        assert np.allclose(ratio, ratio[0], rtol=1e-10)
+    if kind == "PINTE":
+        # outside rexp: 1e-60 times the mass scaling, as the reference scales every cell
+        assert np.all(dens[1:][r[1:] >= 100.0] < 1e-55) and np.any(dens[1:][r[1:] < 100.0] > 1e-30)
+
+
+def test_shell_and_wedge_densities(tmp_path):
+    deck, parts = _analytic_deck(tmp_path, "denstype='SHELL'\ndenspow=2\nmdust=1d-5\n")
+    m, _ = M.deck_model(None, deck, compute_parts=parts)
+    dens, V, r, z = _cells(m)
+    R_av = M.AU * 10.0 ** ((np.log10(m.R[:-1]) + np.log10(m.R[1:])) / 2.0)
+    assert np.allclose(dens[1:] * (R_av[1:, None] / M.AU) ** 2, dens[1, 0] * (R_av[1] / M.AU) ** 2, rtol=1e-12)
+    deck, parts = _analytic_deck(tmp_path, "denstype='WEDGE'\nwedgeopen=20\n")
+    m, _ = M.deck_model(None, deck, compute_parts=parts)
+    dens, V, r, z = _cells(m)
+    thet = np.asarray(m.thet)
+    lo = 90.0 - np.degrees(thet[1:])      # elevation of a cell's lower edge above the midplane
+    assert np.all(dens[1:, lo > 20.5] <= 1e-60)          # at the floor
+    assert np.all(dens[1:, -1] > 1e-40)
+    with pytest.raises(ValueError):
+        M.deck_model(None, deck, overrides=["denstype='POW'"], compute_parts=parts)
+    with pytest.raises(ValueError):
+        M.deck_model(None, deck, overrides=["zone1:rin=1"], compute_parts=parts)
