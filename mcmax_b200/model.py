@@ -280,6 +280,9 @@ def zones_density(R, Theta, thet, zones):
     return dens, V
 
 ANALYTIC_DENSITIES = ("PASCUCCI", "MIN", "PARAMETERIZED", "PINTE", "SHELL", "WEDGE")
+# radial power laws whose vertical structure the reference builds from the
+# optically thin temperatures before the first pass (Init.f:3924-3960)
+THIN_START_DENSITIES = ("POW", "DOUBLEPOW", "SIMILARITY", "DOUBLEPOWSIM")
 
 
 def analytic_density(denstype, R, Theta, thet, p, lam=None, kext=None):
@@ -291,6 +294,10 @@ def analytic_density(denstype, R, Theta, thet, p, lam=None, kext=None):
     averaged over 10 sub-angles), SHELL ((AU/R)^denspow) and WEDGE (the
     cells within wedgeopen degrees of the midplane, 10 sub-angles).  r and z
     are taken at the cell centre (R_av, theta_av); cell i = 0 is empty.
+    Also the radial power laws of THIN_START_DENSITIES (POW, DOUBLEPOW,
+    SIMILARITY, DOUBLEPOWSIM, with denspow2, rpow2, rpow3, rexp,
+    gamma_exp), whose vertical structure the caller then builds
+    (structure.thin_start).
 
     p: dict of the deck's rin, rout [AU], denspow, shpow, sh1au, rexp,
     tau550, wedgeopen, and mtot [g] with mdustscale (mdust given).  lam,
@@ -349,6 +356,21 @@ def analytic_density(denstype, R, Theta, thet, p, lam=None, kext=None):
                 dens = dens + scale * rr ** (-p["denspow"]) * np.exp(-(zz / hr) ** 2) / hr / 10.0
         elif denstype == "SHELL":
             dens = np.broadcast_to(((AU / R_av) ** p["denspow"])[:, None], (nR, nc)).copy()
+        elif denstype in THIN_START_DENSITIES:
+            ra = R_av / AU
+            g = p["gamma_exp"] if p["gamma_exp"] >= 0.0 else 2.0 - p["denspow"]   # Init.f:1568
+            if denstype == "POW":
+                d1 = (AU / R_av) ** (p["denspow"] + 1.0)
+            elif denstype == "SIMILARITY":
+                d1 = (AU / R_av) ** (p["denspow"] + 1.0) * np.exp(-(R_av / (AU * p["rexp"])) ** g)
+            elif denstype == "DOUBLEPOW":
+                inner = (ra < p["rpow2"]) & (ra > p["rpow3"])
+                d1 = np.where(inner, (p["rpow2"] * AU / R_av) ** (p["denspow"] + 1.0),
+                              (p["rpow2"] * AU / R_av) ** (p["denspow2"] + 1.0))
+            else:
+                d1 = np.where(ra < p["rpow2"], (p["rpow2"] * AU / R_av) ** (p["denspow"] + 1.0),
+                              (p["rpow2"] * AU / R_av) ** (p["denspow2"] + 1.0) * np.exp(-(R_av / (AU * p["rexp"])) ** g))
+            dens = np.broadcast_to(d1[:, None], (nR, nc)).copy()
         elif denstype == "WEDGE":
             dens = np.full((nR, nc), 1e-200)
             for jj in range(1, 11):
@@ -765,9 +787,9 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
     if startype not in ("PLANCK", "FILE"):
         raise ValueError("startype: 'PLANCK' or 'FILE' stars")
     denstype = v("denstype", "ZONES", str).upper()
-    if denstype not in ("ZONES", "FILE") + ANALYTIC_DENSITIES:
-        raise ValueError("denstype: 'ZONES', 'FILE' or one of %s (the types that start from an optically thin "
-                         "structure iteration are not built)" % ", ".join(ANALYTIC_DENSITIES))
+    if denstype not in ("ZONES", "FILE") + ANALYTIC_DENSITIES + THIN_START_DENSITIES:
+        raise ValueError("denstype: 'ZONES', 'FILE' or one of %s"
+                         % ", ".join(ANALYTIC_DENSITIES + THIN_START_DENSITIES))
     if denstype == "PARAMETERIZED" and ("scalesh" in d or "rimscale" in d):
         raise ValueError("PARAMETERIZED: scale-height factors (scalesh, rimscale) are not built")
     if not v("tcontact", True, bool):
@@ -788,7 +810,7 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
         zones.append(dict(rin=v(kz + "rin", rin), rout=v(kz + "rout", rout), mdust=v(kz + "mdust", 1e-5),
                           denspow=v(kz + "denspow", 1.0), sh=v(kz + "sh", 0.01), rsh=v(kz + "rsh", 1.0),
                           shpow=v(kz + "shpow", 1.1), fix=v(kz + "fix", False, bool)))
-    if zones and denstype in ANALYTIC_DENSITIES:
+    if zones and denstype in ANALYTIC_DENSITIES + THIN_START_DENSITIES:
         raise ValueError("denstype %s takes no zoneN:* keywords" % denstype)
     if not zones and denstype == "ZONES":
         raise ValueError("no zoneN:* keywords")
@@ -908,12 +930,14 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
         V = cell_volumes(R, Theta)
         dens = np.full(V.shape, 1e-60)
         dens[1:] = dt["dens"]
-    elif denstype in ANALYTIC_DENSITIES:
+    elif denstype in ANALYTIC_DENSITIES + THIN_START_DENSITIES:
         R, Theta, thet, SinTheta = spatial_grid(rstar_cm, rin, rout, nrad, ntheta)
         kext = [r["kext"] if "kext" in r else np.asarray(r["kabs"]) + np.asarray(r["ksca"]) for r in res]
         dens, V = analytic_density(denstype, R, Theta, thet, dict(
             rin=rin, rout=rout, denspow=v("denspow", 1.0), shpow=v("shpow", 1.3), sh1au=v("sh1au", 0.03),
             rexp=v("rexp", 1e10), tau550=v("tau550", 100.0), wedgeopen=v("wedgeopen", 5.0),
+            denspow2=v("denspow2", 1.0), rpow2=v("rpow2", 1e10), rpow3=v("rpow3", 0.0),
+            gamma_exp=v("gamma_exp", -1.0),
             mtot=v("mdust", 1e-15) * MSUN, mdustscale="mdust" in d), lam=lam, kext=kext)
     else:
         R, Theta, thet, SinTheta = spatial_grid(rstar_cm, rin, rout, nrad, ntheta)
@@ -953,6 +977,11 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
                zones=[(z["rin"], z["rout"], z["sh"], z["rsh"], z["shpow"], z["denspow"], z["fix"]) for z in zones],
                Mstar=v("mstar", 2.5) * MSUN, maxiter=v("maxiter", 10, int), epsiter=v("epsiter", 3.0),
                incangle=v("incangle", 45.0), outputfits=v("outputfits", False, bool), posangle=v("posangle", 0.0))
+    # the structure loop runs for zones without a fixed structure or with
+    # iter=.true. (Init.f:563,1519); it and the power-law densities start
+    # from the optically thin structure (Init.f:3924-3960)
+    run["iterate"] = any(not z["fix"] for z in zones) or v("iter", False, bool)
+    run["thin_start"] = run["iterate"] or denstype in THIN_START_DENSITIES
     return m, run
 
 

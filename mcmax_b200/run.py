@@ -96,14 +96,20 @@ def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opac
     m, run = M.deck_model(ctx, deck, overrides, compute_parts=compute_parts)
     rad = {k: run[k] for k in ("seed", "randomwalk", "factRW", "maxinteract", "nruns")}
     diffused = structure = None
-    if any(not z[6] for z in run["zones"]):
-        # a zone without a fixed structure: structure iterations (Init.f:1519)
+    if run.get("iterate", any(not z[6] for z in run["zones"])):
+        # a zone without a fixed structure, or iter=.true.: structure
+        # iterations (Init.f:563,1519) from the optically thin structure
         from . import structure as S
         structure = S.iterate(ctx, m, run["zones"], run["Mstar"], nphot, run=rad, maxiter=run["maxiter"],
                               epsiter=run["epsiter"], nphotdiffuse=run["nphotdiffuse"], dtdiffuse=run["dtdiffuse"],
-                              precision=precision)
+                              precision=precision, thin=True)
         T, n, res = structure["T"], structure["nphot"], structure["result"]
     else:
+        if run.get("thin_start"):
+            # a power-law density: its vertical structure at the optically
+            # thin temperatures, then one pass (Init.f:3924-3960)
+            from . import structure as S
+            S.thin_start(ctx, m, run["zones"], run["Mstar"])
         ctx.set_model(m)
         n, res = ctx.mcradiation(int(nphot), precision=precision, **rad)
         T, dT, dE = ctx.finalize_t()

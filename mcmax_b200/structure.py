@@ -13,9 +13,16 @@ the final structure (Main.f:778-790).
     temp_average(Temp, T, fw)                 TempAverage
     compare_cells(T1, dT1, T2, dT2, nr, nt)   compareCells (errT)
     initial_state(model)                      dens0 = dens, w0 = w, gasdens = dens (Init.f:3904)
+    planck_means(model)                       Kp(iT) and Kpabsstar of every grain (Init.f:3785-3798)
+    thin_temperature(model)                   OpticallyThin's temperatures (Radiation.f:1253-1370)
+    thin_start(ctx, model, zones, Mstar)      the structure the first pass starts from (Init.f:3924-3960)
     iterate(ctx, model, zones, Mstar, nphot)  the loop
 """
+import math
+
 import numpy as np
+
+TMAX = 10000
 
 
 def temp_average(Temp, T, fw):
@@ -51,17 +58,112 @@ def initial_state(model):
     return dict(dens=dens, dens0=dens.copy(), gasdens=dens.copy(), w=w, w0=w.copy())
 
 
+def planck_means(model):
+    """Per grain (component) the Planck-mean table Kp[k, iT] =
+    integrate(BB(:, iT) Kabs) on the 1 K grid and Kpabsstar[k] =
+    integrate(Fstar Kabs) / Lstar (Init.f:3785-3798), each trapezoid summed
+    in the reference's order (Radiation.f:1-18)."""
+    nu = np.asarray(model.nu, float)
+    BB = np.asarray(model.BB, float).reshape(model.nlam, TMAX + 1)
+    Kabs = np.asarray(model.Kabs, float).reshape(model.ncomp, model.nlam)
+    Fstar = np.asarray(model.Fstar, float)
+    Kp = np.zeros((model.ncomp, TMAX + 1))
+    ks = np.zeros(model.ncomp)
+    for i in range(model.nlam - 1):
+        c = abs(nu[i] - nu[i + 1]) * 0.5
+        Kp = Kp + c * (BB[i][None, :] * Kabs[:, i][:, None] + BB[i + 1][None, :] * Kabs[:, i + 1][:, None])
+        ks = ks + c * (Fstar[i] * Kabs[:, i] + Fstar[i + 1] * Kabs[:, i + 1])
+    return Kp, ks / model.Lstar
+
+
+def _cell_energy(Kp, w, iT):
+    """computeE_QHP (Radiation.f:924-936): sum over the grains of Kp(iT) w,
+    in grain order, for each cell's own iT"""
+    E = np.zeros(w.shape[0])
+    for k in range(w.shape[1]):
+        E = E + Kp[k, iT] * w[:, k]
+    return E
+
+
+def thin_temperature(model, Kp=None, kpabsstar=None):
+    """The optically thin temperatures OpticallyThin(.false.) gives at the
+    start (Radiation.f:1253-1370, thermal contact, no viscous heating): each
+    cell absorbs the dilute stellar field, E = W Lstar / (pi Rstar^2)
+    sum_ii Kpabsstar w / sum_ii w with W = (1 - sqrt(1 - (Rstar/r)^2)) / 2
+    at the cell's inner radius (the grid's inner edge for the star cell),
+    and T solves sum_ii Kp(T) w = E as computeT_QHP does (Radiation.f:848-
+    921): the bracketing 1 K steps around E, T^4 interpolated between them
+    (in FP64), 1 K below the table and TMAX - 1 above it, 3 K for NaN.  The
+    back-warming factors of the reference's three inner passes do not enter
+    when OpticallyThin is called with BW false, so one pass is the same.
+    Returns T per cell (the library's cell order)."""
+    from .model import AU
+    if Kp is None or kpabsstar is None:
+        Kp, kpabsstar = planck_means(model)
+    nr, nc = model.nr, model.nt - 1
+    w = np.asarray(model.comp_w, float).reshape(model.ncell, model.ncomp)
+    R = np.asarray(model.R, float)
+    r = np.repeat(np.where(np.arange(nr) == 0, R[1], R[:nr]) * AU, nc)
+    W = 0.5 * (1.0 - np.sqrt(1.0 - (model.Rstar_cm / r) ** 2))
+    E = np.zeros(model.ncell)
+    for k in range(model.ncomp):
+        E = E + kpabsstar[k] * w[:, k]
+    E = W * E * model.Lstar / (math.pi * model.Rstar_cm ** 2) / w.sum(1)
+    Emin, Emax = _cell_energy(Kp, w, np.ones(model.ncell, int)), _cell_energy(Kp, w, np.full(model.ncell, TMAX, int))
+    lo = np.ones(model.ncell, int)
+    hi = np.full(model.ncell, TMAX, int)
+    while np.any(hi - lo > 1):
+        mid = (lo + hi) // 2
+        Em = _cell_energy(Kp, w, mid)
+        up = Em <= E
+        lo = np.where(up & (hi - lo > 1), mid, lo)
+        hi = np.where(~up & (hi - lo > 1), mid, hi)
+    E0, E1 = _cell_energy(Kp, w, lo), _cell_energy(Kp, w, hi)
+    t4 = lambda i: (i.astype(float) ** 2) ** 2
+    with np.errstate(invalid="ignore", divide="ignore"):
+        T = np.sqrt(np.sqrt(t4(lo) + ((t4(hi) - t4(lo)) * (E - E0)) / (E1 - E0)))
+    T = np.where(E1 == E0, lo.astype(float), T)
+    T = np.where(E > Emax, float(TMAX - 1), T)
+    T = np.where(E < Emin, 1.0, T)
+    return np.where(np.isnan(E), 3.0, T)
+
+
+def thin_start(ctx, model, zones, Mstar, shscale=None, grain_scale=None):
+    """The vertical structure the first Monte Carlo pass starts from
+    (Init.f:3924-3960): dens0 = gasdens = dens, the optically thin
+    temperatures (BackWarming(1) changes nothing before the first pass:
+    no cell has absorbed packets yet), their average (the first
+    TempAverage copies them) and three DiskStructure passes on them.
+    Regridding in theta and dead zones are not built.  Updates the model's
+    dens and comp_w; returns dict(state, Temp)."""
+    state = initial_state(model)
+    Temp = temp_average(None, thin_temperature(model), 1.0)
+    for _ in range(3):
+        out = ctx.disk_structure(model.R, model.Theta, model.V, Mstar, zones, Temp, state["dens"], state["dens0"],
+                                 state["gasdens"], state["w"], state["w0"], shscale, grain_scale)
+        state = dict(zip(("dens", "dens0", "gasdens", "w", "w0"), out))
+    model.dens = state["dens"]
+    model.comp_w = state["w"].reshape(model.ncell, -1)
+    return dict(state=state, Temp=Temp)
+
+
 def iterate(ctx, model, zones, Mstar, nphot, run=None, maxiter=10, epsiter=3.0, f_weight=0.5, niter0=1000,
-            nphotdiffuse=25, dtdiffuse=1.0, shscale=None, grain_scale=None, precision="mixed", log=None):
+            nphotdiffuse=25, dtdiffuse=1.0, shscale=None, grain_scale=None, precision="mixed", log=None,
+            thin=False):
     """Run the structure iterations on `model` (one opacity set per grain:
     comp_w holds the grains' abundances).  zones: (rin, rout, sh, rsh,
     shpow, denspow, fix_struct) per zone; Mstar in g; run: the keyword
-    arguments of Context.mcradiation.  The model's dens and comp_w are
+    arguments of Context.mcradiation.  thin: start from the optically thin
+    structure (thin_start), as the reference does before its first pass;
+    otherwise from the model's densities.  The model's dens and comp_w are
     updated in place.  Returns dict(T, dT, Temp, state, history, nphot,
     result) with one history entry (niter, errT, packets) per structure
     pass and the last packet run's count and result."""
     run = dict(run or {})
-    state = initial_state(model)
+    if thin:
+        state = thin_start(ctx, model, zones, Mstar, shscale, grain_scale)["state"]
+    else:
+        state = initial_state(model)
     Temp = None
     niter = 0
     finaliter = lastiter = False

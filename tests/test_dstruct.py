@@ -224,3 +224,64 @@ def test_iterations_stop_at_maxiter():
     assert fake.calls["mc"] == 5 and fake.calls["ds"] == 4
     # the structure temperature averages the passes with weight f_weight = 0.5
     assert np.allclose(r["Temp"], 0.5 * (0.5 * (0.5 * T + 0.5 * (T + 10)) + 0.5 * T) + 0.5 * (T + 10), rtol=1e-12)
+
+
+def test_thin_temperatures_follow_determine_t():
+    """OpticallyThin's cell temperatures: the absorbed dilute stellar field
+    inverted on each cell's Planck-mean table with determineT's bracket and
+    T^4 interpolation; the oracle's determineT on the same table gives the
+    same bits"""
+    m = _driver_model()
+    Kp, kps = S.planck_means(m)
+    T = S.thin_temperature(m, Kp, kps)
+    w = m.comp_w.reshape(m.ncell, m.ncomp)
+    nc = m.nt - 1
+    R = np.asarray(m.R)
+    for c in range(0, m.ncell, 7):
+        i = c // nc
+        r = (R[1] if i == 0 else R[i]) * M.AU
+        W = 0.5 * (1.0 - math.sqrt(1.0 - (m.Rstar_cm / r) ** 2))
+        E = 0.0
+        for k in range(m.ncomp):
+            E = E + kps[k] * w[c, k]
+        E = W * E * m.Lstar / (math.pi * m.Rstar_cm ** 2) / w[c].sum()
+        kp = np.zeros(S.TMAX + 1)
+        for k in range(m.ncomp):
+            kp = kp + Kp[k] * w[c, k]
+        kp = np.ascontiguousarray(kp)
+        assert T[c] == O.load().orc_determine_t(O.P(kp), E, 100.0), c
+    # hotter inside, and below the star
+    Tr = T.reshape(m.nr, nc)[:, -1]
+    assert np.all(np.diff(Tr[1:]) < 0) and Tr[1] < m.Tstar
+
+
+def test_thin_temperature_of_a_grey_grain():
+    """with a wavelength-independent opacity, sum Kp(T) = W sum Kpabsstar
+    gives int B(T) = W int B(Tstar) on the grid: T = W^(1/4) Tstar where
+    the grid holds both Planck curves"""
+    m = _driver_model()
+    m = M.Model(**dict(m.__dict__, Kabs=np.ones_like(m.Kabs)))
+    T = S.thin_temperature(m).reshape(m.nr, m.nt - 1)
+    R = np.asarray(m.R)
+    for i in (3, 8, 15):
+        W = 0.5 * (1.0 - math.sqrt(1.0 - (m.Rstar_cm / (R[i] * M.AU)) ** 2))
+        assert abs(T[i, 0] / (W ** 0.25 * m.Tstar) - 1.0) < 0.02, (i, T[i, 0], W ** 0.25 * m.Tstar)
+
+
+def test_thin_start_runs_three_structure_passes():
+    m = _driver_model()
+    T = _temp(m)
+    fake = _FakeRun([T])
+    zones = [(0.5, 100.0, SH, 1.0, 1.125, 1.0, 0)]
+    thin = S.thin_temperature(m)
+    st = S.thin_start(fake, m, zones, 2.5 * M.MSUN)
+    assert fake.calls["ds"] == 3 and np.array_equal(st["Temp"], thin)
+    assert np.array_equal(m.dens, st["state"]["dens"])
+    # the ring masses survive the passes
+    V = m.V.reshape(m.nr, -1)
+    d0 = _driver_model().dens.reshape(m.nr, -1)
+    d1 = m.dens.reshape(m.nr, -1)
+    assert np.allclose((d1 * V).sum(1)[1:], (d0 * V).sum(1)[1:], rtol=1e-10)
+    fake2 = _FakeRun([T])
+    r = S.iterate(fake2, _driver_model(), zones, 2.5 * M.MSUN, 1000, thin=True)
+    assert fake2.calls["ds"] == 3 + len(r["history"])

@@ -156,7 +156,8 @@ idum=-7
     assert zones == [(0.5, 100.0, 0.0707, 1.0, 1.125, 1.0, False)]
     assert abs(run.pop("Mstar") / (2.5 * M.MSUN) - 1) < 1e-15
     assert run == dict(seed=7, randomwalk=True, factRW=5.0, maxinteract=20000, nruns=1, nphotdiffuse=25,
-                       dtdiffuse=1.0, maxiter=10, epsiter=3.0, incangle=45.0, outputfits=False, posangle=0.0)
+                       dtdiffuse=1.0, maxiter=10, epsiter=3.0, incangle=45.0, outputfits=False, posangle=0.0,
+                       iterate=True, thin_start=True)
     assert np.allclose(m.comp_w.sum(1), 1.0)
     ref = M.disk_model(None, nrad=12, ntheta=8, nlam=20, lam2=3000.0, mdust=1e-5, sh=0.0707, ngrains=3,
                        opacities=(m.Kabs, m.Ksca, m.F))
@@ -408,6 +409,30 @@ def test_shell_and_wedge_densities(tmp_path):
     assert np.all(dens[1:, lo > 20.5] <= 1e-60)          # at the floor
     assert np.all(dens[1:, -1] > 1e-40)
     with pytest.raises(ValueError):
-        M.deck_model(None, deck, overrides=["denstype='POW'"], compute_parts=parts)
+        M.deck_model(None, deck, overrides=["denstype='MASSLOSS'"], compute_parts=parts)
     with pytest.raises(ValueError):
         M.deck_model(None, deck, overrides=["zone1:rin=1"], compute_parts=parts)
+
+
+@pytest.mark.parametrize("kind", ["POW", "SIMILARITY", "DOUBLEPOW", "DOUBLEPOWSIM"])
+def test_power_law_densities(kind, tmp_path):
+    """the radial power laws start from (AU/R)^(denspow+1), independent of
+    theta, scaled to mdust; their vertical structure comes from the
+    optically thin start"""
+    deck, parts = _analytic_deck(tmp_path, "denstype='%s'\nmdust=1d-4\ndenspow=1.5\ndenspow2=3\nrpow2=30\n"
+                                           "rexp=50\n" % kind)
+    m, run = M.deck_model(None, deck, compute_parts=parts)
+    dens, V, r, z = _cells(m)
+    assert abs((dens[1:] * V[1:]).sum() / (1e-4 * M.MSUN) - 1.0) < 1e-12
+    assert np.all(dens[1:] == dens[1:, :1])
+    R_av = 10.0 ** ((np.log10(m.R[:-1]) + np.log10(m.R[1:])) / 2.0)
+    f = R_av ** -2.5
+    if kind == "SIMILARITY":
+        f = f * np.exp(-(R_av / 50.0) ** 0.5)        # gamma_exp defaults to 2 - denspow
+    if kind in ("DOUBLEPOW", "DOUBLEPOWSIM"):
+        f = np.where(R_av < 30.0, (30.0 / R_av) ** 2.5, (30.0 / R_av) ** 4.0)
+        if kind == "DOUBLEPOWSIM":
+            f = np.where(R_av < 30.0, f, f * np.exp(-(R_av / 50.0) ** 0.5))
+    ratio = dens[1:, 0] / f[1:]
+    assert np.allclose(ratio, ratio[0], rtol=1e-10)
+    assert run["thin_start"] and not run["iterate"] and run["zones"] == []

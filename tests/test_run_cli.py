@@ -72,6 +72,12 @@ class FakeContext:
         self.trace_args = (angle, nphi, nr, tuple(Rfix))
         return np.full(len(lam_obs), 1e20), (100, 0)
 
+    def disk_structure(self, R, Theta, V, Mstar, zones, Temp, dens, dens0, gasdens, w, w0, shscale=None,
+                       grain_scale=None):
+        self.structure_calls = getattr(self, "structure_calls", 0) + 1
+        self.structure_zones = zones
+        return (np.array(dens), np.array(dens0), np.array(gasdens), np.array(w), np.array(w0))
+
     def trace_image(self, T, lam0, angle, npixel=500, nint=1000, Rmax=None, pa=0.0, nphi=45, nr=2, Rfix=(),
                     seed=42):
         self.image_args = dict(lam0=lam0, angle=angle, npixel=npixel, nint=nint, Rmax=Rmax, pa=pa, nphi=nphi, nr=nr,
@@ -159,3 +165,19 @@ def test_command_line_arguments():
     a = R.parse_args(["x.in", "300", "obs.out", "-o", "o", "-s", "a=1", "-s", "b=2", "--opacity", "surrogate"])
     assert (a.nphot, a.outdir, a.overrides, a.opacity, a.observations) == (300, "o", ["a=1", "b=2"], "surrogate",
                                                                             ["obs.out"])
+
+
+def test_power_law_deck_starts_from_the_thin_structure(tmp_path):
+    deck = _write_inputs(tmp_path)
+    made = []
+
+    def factory(device):
+        made.append(FakeContext(device))
+        return made[-1]
+
+    body = open(deck).read().replace("zone1:rin=1\nzone1:rout=50\nzone1:mdust=1d-6\nzone1:fix=.true.\n", "")
+    (tmp_path / "pow.in").write_text(body + "denstype='POW'\nmdust=1d-6\n")
+    r = R.main([str(tmp_path / "pow.in"), "1e3", "-o", str(tmp_path / "o")], context=factory)
+    # three structure passes before the one packet run, no zones
+    assert made[0].structure_calls == 3 and made[0].structure_zones == []
+    assert len(made[0].calls) == 1 and r["structure"] is None
