@@ -279,7 +279,7 @@ def zones_density(R, Theta, thet, zones):
     dens[1:] = 1e-60 + total[1:]
     return dens, V
 
-ANALYTIC_DENSITIES = ("PASCUCCI", "MIN", "PARAMETERIZED", "PINTE", "SHELL", "WEDGE")
+ANALYTIC_DENSITIES = ("PASCUCCI", "MIN", "PARAMETERIZED", "PINTE", "SHELL", "WEDGE", "MASSLOSS", "INFALL")
 # radial power laws whose vertical structure the reference builds from the
 # optically thin temperatures before the first pass (Init.f:3924-3960)
 THIN_START_DENSITIES = ("POW", "DOUBLEPOW", "SIMILARITY", "DOUBLEPOWSIM")
@@ -292,7 +292,10 @@ def analytic_density(denstype, R, Theta, thet, p, lam=None, kext=None):
     Init.f:3992-4026), MIN and PINTE (Gaussian vertical profile of scale
     height sh1AU r^shpow; PINTE cut at r = Rexp), PARAMETERIZED (the same,
     averaged over 10 sub-angles), SHELL ((AU/R)^denspow) and WEDGE (the
-    cells within wedgeopen degrees of the midplane, 10 sub-angles).  r and z
+    cells within wedgeopen degrees of the midplane, 10 sub-angles), MASSLOSS
+    (a wind Mdot / (gas2dust 4 pi R^2 v(R)), v = vexp2 (1 - (1 - (vexp1 /
+    vexp2)^(1/bexp)) Rstar / R)^bexp) and INFALL (rotating infall of
+    Minfall onto radius rexp around Mstar).  r and z
     are taken at the cell centre (R_av, theta_av); cell i = 0 is empty.
     Also the radial power laws of THIN_START_DENSITIES (POW, DOUBLEPOW,
     SIMILARITY, DOUBLEPOWSIM, with denspow2, rpow2, rpow3, rexp,
@@ -356,6 +359,32 @@ def analytic_density(denstype, R, Theta, thet, p, lam=None, kext=None):
                 dens = dens + scale * rr ** (-p["denspow"]) * np.exp(-(zz / hr) ** 2) / hr / 10.0
         elif denstype == "SHELL":
             dens = np.broadcast_to(((AU / R_av) ** p["denspow"])[:, None], (nR, nc)).copy()
+        elif denstype == "MASSLOSS":
+            # a stationary wind with a beta velocity law; the 1. literals
+            # are exact in single precision
+            v2, v1 = p["vexp2"], p["vexp1"]
+            vexp = v2 * (1.0 - (1.0 - (v1 / v2) ** (1.0 / p["bexp"])) * p["rstar_cm"] / R_av) ** p["bexp"]
+            d1 = p["mdot"] / (p["gas2dust"] * 4.0 * math.pi * R_av ** 2 * vexp)
+            dens = np.broadcast_to(d1[:, None], (nR, nc)).copy()
+            mdustscale = False
+        elif denstype == "INFALL":
+            # rotating infall onto a disk of radius rexp: mu0 of each
+            # streamline by solve_mu0's scan of 1000 values (Init.f:5747-5764)
+            mu1 = (np.arange(1000, dtype=np.float32) / np.float32(999)).astype(float)
+            dens = np.zeros((nR, nc))
+            Gc = 6.67300e-8
+            for i in range(1, nR):
+                rr = R_av[i] / (AU * p["rexp"])
+                for j in range(nc):
+                    mu = math.cos(theta_av[j])
+                    d = np.abs((1.0 - mu1 ** 2) - rr * (1.0 - mu / mu1))
+                    d = np.where(np.isnan(d), np.inf, d)
+                    k = int(np.argmin(d)) if np.min(d) < 1e200 else None
+                    mu0 = mu1[k] if k is not None else 0.0
+                    dens[i, j] = ((p["minfall"] / (4.0 * math.pi * math.sqrt(Gc * p["mstar"] * R_av[i] ** 3)))
+                                  * (1.0 + mu / mu0) ** (-0.5)
+                                  * (mu / mu0 + 2.0 * mu0 ** 2 * p["rexp"] * AU / R_av[i]) ** (-1.0)) / p["gas2dust"]
+            mdustscale = False
         elif denstype in THIN_START_DENSITIES:
             ra = R_av / AU
             g = p["gamma_exp"] if p["gamma_exp"] >= 0.0 else 2.0 - p["denspow"]   # Init.f:1568
@@ -938,6 +967,11 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
             rexp=v("rexp", 1e10), tau550=v("tau550", 100.0), wedgeopen=v("wedgeopen", 5.0),
             denspow2=v("denspow2", 1.0), rpow2=v("rpow2", 1e10), rpow3=v("rpow3", 0.0),
             gamma_exp=v("gamma_exp", -1.0),
+            mdot=v("mdot", 1e-8) * MSUN / (365.25 * 24.0 * 60.0 * 60.0),
+            minfall=(v("minfall", -1.0) if v("minfall", -1.0) >= 0.0 else v("mdot", 1e-8)) * MSUN / (365.25 * 24.0 * 60.0 * 60.0),
+            vexp1=v("vexp1", v("vexp", 10.0)) * 100000.0,
+            vexp2=(v("vexp2", -10.0) if v("vexp2", -10.0) > 0.0 else v("vexp1", v("vexp", 10.0))) * 100000.0,
+            bexp=v("bexp", 0.5), gas2dust=v("gas2dust", 100.0), mstar=v("mstar", 2.5) * MSUN, rstar_cm=rstar_cm,
             mtot=v("mdust", 1e-15) * MSUN, mdustscale="mdust" in d), lam=lam, kext=kext)
     else:
         R, Theta, thet, SinTheta = spatial_grid(rstar_cm, rin, rout, nrad, ntheta)

@@ -409,7 +409,7 @@ def test_shell_and_wedge_densities(tmp_path):
     assert np.all(dens[1:, lo > 20.5] <= 1e-60)          # at the floor
     assert np.all(dens[1:, -1] > 1e-40)
     with pytest.raises(ValueError):
-        M.deck_model(None, deck, overrides=["denstype='MASSLOSS'"], compute_parts=parts)
+        M.deck_model(None, deck, overrides=["denstype='MEIXNER'"], compute_parts=parts)
     with pytest.raises(ValueError):
         M.deck_model(None, deck, overrides=["zone1:rin=1"], compute_parts=parts)
 
@@ -436,3 +436,26 @@ def test_power_law_densities(kind, tmp_path):
     ratio = dens[1:, 0] / f[1:]
     assert np.allclose(ratio, ratio[0], rtol=1e-10)
     assert run["thin_start"] and not run["iterate"] and run["zones"] == []
+
+
+def test_massloss_and_infall_densities(tmp_path):
+    """MASSLOSS at constant speed is Mdot / (gas2dust 4 pi R^2 v); INFALL far
+    outside its disk radius tends to free fall, Minfall / (4 pi sqrt(2 G
+    Mstar R^3)) / gas2dust, whatever the angle"""
+    yr = 365.25 * 24 * 3600.0
+    deck, parts = _analytic_deck(tmp_path, "denstype='MASSLOSS'\nmdot=1d-6\nvexp=15\n")
+    m, _ = M.deck_model(None, deck, compute_parts=parts)
+    dens, V, r, z = _cells(m)
+    R_av = M.AU * 10.0 ** ((np.log10(m.R[:-1]) + np.log10(m.R[1:])) / 2.0)
+    want = 1e-6 * M.MSUN / yr / (100.0 * 4.0 * math.pi * R_av ** 2 * 15e5)
+    assert np.allclose(dens[1:], want[1:, None], rtol=1e-12)
+    deck, parts = _analytic_deck(tmp_path, "denstype='INFALL'\nmdot=1d-6\nrexp=0.5\nmstar=1\n")
+    m, _ = M.deck_model(None, deck, compute_parts=parts)
+    dens, V, r, z = _cells(m)
+    R_av = M.AU * 10.0 ** ((np.log10(m.R[:-1]) + np.log10(m.R[1:])) / 2.0)
+    ff = 1e-6 * M.MSUN / yr / (4.0 * math.pi * np.sqrt(2.0 * 6.673e-8 * M.MSUN * R_av ** 3)) / 100.0
+    far = R_av / M.AU > 200.0
+    assert np.allclose(dens[far], ff[far, None], rtol=0.05)
+    # nearer in, the flow piles up toward the midplane
+    i = int(np.searchsorted(R_av / M.AU, 1.0))
+    assert dens[i, -1] > dens[i, 0]
