@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--compare-fp64", action="store_true", help="also time the FP64 form (one step)")
     ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-post-mc", action="store_true",
+                    help="skip the timing of the steps after the packet loop (Diffuse, structure, spectrum, image)")
     ap.add_argument("--learned-nphot", type=int, default=30_000_000,
                     help="packets per run of the learned-opacities comparison (0 skips it)")
     ap.add_argument("--maxinteract", type=int, default=RUN["maxinteract"],
@@ -204,6 +206,48 @@ def learned_deck_comparison(ctx, nphot, seed0):
     return out
 
 
+def post_mc_steps(ctx, model, res):
+    """The steps after the packet loop on the same deck and the packet
+    run's result, each C-ABI call timed on the host (every call ends with a
+    device synchronisation): the temperatures (mcg_finalize_t), Diffuse
+    (mcg_diffuse), one vertical-structure pass on the zone taken as not
+    fixed (mcg_disk_structure), the ray-traced spectrum at 45 degrees on the
+    grid's wavelengths (mcg_trace_spectrum) and a 500 x 500 image with 1000
+    points per image cell at the middle of the wavelength range
+    (mcg_trace_image).  Not part of the headline metric."""
+    import math
+    import numpy as np
+    from mcmax_b200 import model as M
+    from mcmax_b200 import outputs
+    from mcmax_b200 import structure as S
+
+    def timed(fn):
+        t0 = time.perf_counter()
+        r = fn()
+        return r, time.perf_counter() - t0
+
+    out = {}
+    (T, dT, _), t = timed(ctx.finalize_t)
+    out["finalize_t_s"] = t
+    (Td, _, counts), t = timed(lambda: ctx.diffuse(res["Ni"], dT, T))
+    out["diffuse"] = {"s": t, "selected_cells": int(counts[0]), "unknowns": int(counts[1])}
+    st = S.initial_state(model)
+    zones = [(0.5, 100.0, 0.05 * math.sqrt(2.0), 1.0, 1.125, 1.0, 0)]
+    _, t = timed(lambda: ctx.disk_structure(model.R, model.Theta, model.V, 2.5 * M.MSUN, zones, np.maximum(Td, 2.7),
+                                            st["dens"], st["dens0"], st["gasdens"], st["w"], st["w0"]))
+    out["disk_structure"] = {"s": t, "columns": int((model.nr - 1) * (model.ncomp + 1))}
+    lam_obs = outputs.spectrum_wavelengths(model.lam, model.lam[0], model.lam[-1])
+    (flux, info), t = timed(lambda: ctx.trace_spectrum(Td, lam_obs, math.radians(45.0)))
+    out["trace_spectrum"] = {"s": t, "wavelengths": int(lam_obs.size), "image_radii": info[0],
+                             "rays_per_s": info[0] * 45 * lam_obs.size / t, "bad_rays": info[1]}
+    lam0 = (model.lam[0] + model.lam[-1]) / 2.0
+    img, t = timed(lambda: ctx.trace_image(Td, lam0, math.radians(45.0), npixel=500, nint=1000))
+    pts = (img["info"][0] - 1) * 45 * 1000
+    out["trace_image"] = {"s": t, "points": int(pts), "points_per_s": pts / t,
+                          "sum_over_flux": float(img["image"].sum() / img["flux"])}
+    return out
+
+
 def build_model(ctx):
     from mcmax_b200 import model as M
     return M.disk_model(ctx, **WORKLOAD)
@@ -326,8 +370,15 @@ def main():
     t1 = time.perf_counter()
     for s in range(e2e_steps):
         ctx.set_model(model)
-        ctx.mcradiation(args.nphot, seed=rank * 7_000_001 + s + 1, precision=args.precision, fetch=True, **RUN)
+        _, e2e_res = ctx.mcradiation(args.nphot, seed=rank * 7_000_001 + s + 1, precision=args.precision,
+                                     fetch=True, **RUN)
     e2e_t = _max_over_ranks(dist, time.perf_counter() - t1)
+    post_mc = None
+    if rank == 0 and world == 1 and not args.no_post_mc:
+        try:
+            post_mc = post_mc_steps(ctx, model, e2e_res)
+        except Exception as e:  # the extra timings must not sink the GPU line
+            post_mc = {"failed": str(e)}
     e2e_value = args.nphot * e2e_steps * world / e2e_t
     fp64_line = None
     if args.compare_fp64 and args.precision != "fp64":
@@ -387,6 +438,8 @@ def main():
             line["fp64_form"] = fp64_line
         if learned:
             line["learned_deck"] = learned
+        if post_mc:
+            line["post_mc"] = post_mc
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist:
