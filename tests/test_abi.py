@@ -46,6 +46,10 @@ def test_invalid_arguments_do_not_abort():
     assert lib.mcg_bb_table(0, None, None) == _ffi.MCG_ERR_ARG
     assert lib.mcg_set_model(None, None, None) == _ffi.MCG_ERR_ARG
     assert lib.mcg_mcradiation(None, None, None, None) == _ffi.MCG_ERR_ARG
+    assert lib.mcg_diffuse(None, 25, 1.0, 10.0, None, None, None, None, None) == _ffi.MCG_ERR_ARG
+    assert lib.mcg_disk_structure(None, None, None, None, None, None, None, None) == _ffi.MCG_ERR_ARG
+    assert lib.mcg_trace_spectrum(None, None, None, 0, None, None, None) == _ffi.MCG_ERR_ARG
+    assert lib.mcg_trace_image(None, None, None, 1.0, None, None, None, None) == _ffi.MCG_ERR_ARG
     assert lib.mcg_version() >= 100
 
 

@@ -62,3 +62,17 @@ def test_trace_image_in_chunks(ctx):
                                  nj0=2)
     assert g["flux"] == fh
     assert np.array_equal(g["image"], ih)
+
+
+def test_trace_image_rejects_bad_sizes(ctx):
+    """sizes outside the documented limits come back as errors before any
+    device work; the context stays usable"""
+    from mcmax_b200.api import McgError
+    m = models.small_disk(nrad=12, ntheta=8, nlam=20, mdust=1e-5)
+    ctx.set_model(m)
+    T = np.full(m.ncell, 100.0)
+    for kw in (dict(npixel=0), dict(npixel=9000), dict(nint=0), dict(Rmax=-1.0), dict(Rmax=0.0)):
+        with pytest.raises(McgError):
+            ctx.trace_image(T, 3.0, 0.5, **dict(dict(npixel=16, nint=2), **kw))
+    g = ctx.trace_image(T, 3.0, 0.5, npixel=16, nint=2)
+    assert np.all(np.isfinite(g["image"])) and g["image"].sum() > 0
