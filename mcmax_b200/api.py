@@ -232,7 +232,7 @@ class Context:
         return flux, (int(info[0]), int(info[1]))
 
     def trace_image(self, T, lam0, angle, npixel=500, nint=1000, Rmax=None, pa=0.0, nphi=45, nr=2, Rfix=(),
-                    tracestar=True, dimstar=1.0, seed=42, linear=None):
+                    tracestar=True, dimstar=1.0, seed=42, linear=None, lam_path=None):
         """mcg_trace_image on the current model: the rectangular image at
         wavelength lam0 [micron] and inclination `angle` [rad] (MakeImage).
         Rmax: half the field of view [AU], by default the grid's outer radius
@@ -242,7 +242,9 @@ class Context:
         full Mueller matrix, log-linear otherwise).  Returns dict(image
         (npixel, npixel) indexed [ix-1, iy-1] in the reference's units per
         pixel (x 1e23 zscale / distance^2 for Jy), flux at lam0, R (image
-        radii, AU), rphi (nr, nphi) ray intensities, info)."""
+        radii, AU), rphi (nr, nphi) ray intensities, info).  lam_path: the
+        wavelength of the tau = 0.1 radius that places the image rays (an
+        IMAGE observation traces at lam0, the default; an IFU at 0.55)."""
         m = self.model
         T = _f64(T).reshape(-1)
         Rfix = _f64(np.atleast_1d(np.asarray(Rfix, float)))
@@ -255,7 +257,8 @@ class Context:
         cap += (m.nt - 1) * 2 * (nRfix + 2) + 1 + 30 + (180 * (nRfix + 1) if int(m.scat_how) == 2 else 0)
         Rimg = np.zeros(cap)
         rphi = np.zeros(cap * int(nphi))
-        o = _ffi.TraceOpts(float(angle), int(nphi), int(nr), nRfix, _ffi.ptr(Rfix) if nRfix else None, float(lam0),
+        lam_path = float(lam0) if lam_path is None else float(lam_path)
+        o = _ffi.TraceOpts(float(angle), int(nphi), int(nr), nRfix, _ffi.ptr(Rfix) if nRfix else None, lam_path,
                            int(bool(tracestar)), float(dimstar))
         io = _ffi.ImageOpts(int(npixel), int(nint), float(Rmax), float(pa), int(seed) & (2 ** 64 - 1),
                             int(bool(linear)), int(cap), _ffi.ptr(Rimg), _ffi.ptr(rphi))

@@ -78,6 +78,38 @@ def observe_image(ctx, m, T, ob, outdir, rfix=(), seed=42, posangle=0.0):
     return files
 
 
+def observe_ifu(ctx, m, T, ob, outdir, rfix=(), seed=42, posangle=0.0):
+    """An IFU observation (Telescope.f:184-199): the image rays placed with
+    the tau = 0.1 radius at 0.55 micron, then per wavelength of the
+    observation (as a SPECTRUM's) and per field of view a rectangular image
+    ImageAI_*.fits (mcg_trace_image with lam_path 0.55).  As in the
+    reference, the fields of view of scaletype 2 are not converted from
+    arcsec before they set the image size, only rscale and zscale change.
+    Returns the files written."""
+    from .outputs import PARSEC
+    angle = (math.pi * ob["inc"]) / 180.0
+    dcm = m.distance * PARSEC
+    fovs = ob["fov"] or [2.0 * float(m.R[-1])]
+    scaletype = int(ob.get("scaletype", 1))
+    lam_obs = outputs.spectrum_wavelengths(m.lam, ob["lam1"], ob["lam2"], ob["nlam"], ob["lamfile"] or None)
+    files = []
+    n = 0
+    for lam0 in lam_obs:
+        for fov in fovs:
+            if scaletype == 2:
+                rscale, zscale = PARSEC / dcm, 1e3 * ((ob["npix"] / fov) * dcm / PARSEC) ** 2
+            else:
+                rscale, zscale = 1.0, 1.0
+            r = ctx.trace_image(T, lam0, angle, npixel=ob["npix"], nint=ob["nint"], Rmax=fov / 2.0, pa=posangle,
+                                nphi=ob["nphi"], nr=ob["nrad"], Rfix=rfix, seed=seed + n, lam_path=0.55)
+            n += 1
+            im = r["image"] * 1e23 * zscale / dcm ** 2
+            files.append(outputs.write_image_fits(
+                os.path.join(outdir, outputs.image_name("AI", angle, lam0, fov / 2.0, ob["flag"])), im, fov / 2.0,
+                rscale, scaletype))
+    return files
+
+
 def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opacity="dhs", compute_parts=None,
              spectra=(), spectrum_nphi=45, spectrum_nr=2, observations=()):
     """Build the deck's model, run the packet loop and the diffusion step
@@ -87,8 +119,9 @@ def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opac
     diffused (the counts of mcg_diffuse, or None), structure, files).
     observations: MCMax observation files; their SPECTRUM observations are
     ray-traced the same way, their IMAGE observations give RImage_*.dat
-    and ImageAI_*.fits (observe_image); other kinds are skipped and listed
-    in 'skipped'."""
+    and ImageAI_*.fits (observe_image), IFU observations one ImageAI_*.fits
+    per wavelength (observe_ifu); other kinds are skipped and listed in
+    'skipped'."""
     if compute_parts is None and opacity == "surrogate":
         compute_parts = _surrogate_parts(ctx)
     elif opacity not in ("dhs", "surrogate"):
@@ -128,7 +161,7 @@ def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opac
     skipped, images = [], []
     for path in observations:
         for ob in outputs.read_observations(path, m.lam, run.get("incangle", 45.0), rout=m.R[-1]):
-            {"SPECTRUM": todo, "IMAGE": images}.get(ob["kind"], skipped).append(ob)
+            {"SPECTRUM": todo, "IMAGE": images, "IFU": images}.get(ob["kind"], skipped).append(ob)
     rfix = fixed_radii(run["zones"], m.R[1], m.R[-1])
     for ob in todo:
         lam_obs = outputs.spectrum_wavelengths(m.lam, ob["lam1"], ob["lam2"], ob["nlam"], ob["lamfile"] or None)
@@ -136,7 +169,8 @@ def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opac
         files.append(outputs.write_spectrum(outdir, ob["inc"], lam_obs, flux, m.lam, m.Fstar, m.distance,
                                             flag=ob["flag"]))
     for ob in images:
-        files += observe_image(ctx, m, T, ob, outdir, rfix, seed=run["seed"], posangle=run.get("posangle", 0.0))
+        observe = observe_ifu if ob["kind"] == "IFU" else observe_image
+        files += observe(ctx, m, T, ob, outdir, rfix, seed=run["seed"], posangle=run.get("posangle", 0.0))
     return dict(model=m, run=run, nphot=n, result=res, T=T, diffused=diffused, structure=structure, files=files,
                 skipped=[ob["kind"] for ob in skipped])
 

@@ -79,9 +79,10 @@ class FakeContext:
         return (np.array(dens), np.array(dens0), np.array(gasdens), np.array(w), np.array(w0))
 
     def trace_image(self, T, lam0, angle, npixel=500, nint=1000, Rmax=None, pa=0.0, nphi=45, nr=2, Rfix=(),
-                    seed=42):
+                    seed=42, lam_path=None):
         self.image_args = dict(lam0=lam0, angle=angle, npixel=npixel, nint=nint, Rmax=Rmax, pa=pa, nphi=nphi, nr=nr,
-                               seed=seed)
+                               seed=seed, lam_path=lam_path)
+        self.image_calls = getattr(self, "image_calls", []) + [self.image_args]
         R = np.linspace(0.0, 50.0, 11)
         return dict(image=np.full((npixel, npixel), 2.0), flux=1.0, R=R, rphi=np.ones((R.size, nphi)),
                     info=(R.size, 0))
@@ -181,3 +182,22 @@ def test_power_law_deck_starts_from_the_thin_structure(tmp_path):
     # three structure passes before the one packet run, no zones
     assert made[0].structure_calls == 3 and made[0].structure_zones == []
     assert len(made[0].calls) == 1 and r["structure"] is None
+
+
+def test_ifu_observation_writes_one_image_per_wavelength(tmp_path):
+    deck = _write_inputs(tmp_path)
+    (tmp_path / "ifu.out").write_text("type='IFU'\nlam1=1\nlam2=100\nnlam=3\nnpix=8\nnint=2\nfov=40\n")
+    made = []
+
+    def factory(device):
+        made.append(FakeContext(device))
+        return made[-1]
+
+    r = R.main([deck, "1e3", str(tmp_path / "ifu.out"), "-o", str(tmp_path / "o")], context=factory)
+    names = [os.path.basename(f) for f in r["files"] if "Image" in f]
+    assert names == ["ImageAI_i45.0_l00001.00_fov00040.0.fits", "ImageAI_i45.0_l00010.00_fov00040.0.fits",
+                     "ImageAI_i45.0_l00100.00_fov00040.0.fits"]
+    calls = made[0].image_calls
+    assert [c["lam0"] for c in calls] == [1.0, 10.0, 100.0]
+    assert all(c["lam_path"] == 0.55 and c["Rmax"] == 20.0 and c["npixel"] == 8 for c in calls)
+    assert len({c["seed"] for c in calls}) == 3
