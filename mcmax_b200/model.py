@@ -282,7 +282,75 @@ def zones_density(R, Theta, thet, zones):
 ANALYTIC_DENSITIES = ("PASCUCCI", "MIN", "PARAMETERIZED", "PINTE", "SHELL", "WEDGE", "MASSLOSS", "INFALL")
 # radial power laws whose vertical structure the reference builds from the
 # optically thin temperatures before the first pass (Init.f:3924-3960)
-THIN_START_DENSITIES = ("POW", "DOUBLEPOW", "SIMILARITY", "DOUBLEPOWSIM")
+THIN_START_DENSITIES = ("POW", "DOUBLEPOW", "SIMILARITY", "DOUBLEPOWSIM", "SURFFILE")
+
+
+def regridlog(path, grid):
+    """A two-column table (x, y) on the grid as regridlog reads it
+    (Subroutines.f:82-123): grid points up to the first x take its y,
+    points inside the table the log-log interpolation of their interval
+    (an entry y <= 0 read as 1e-50 of the one before), points beyond it
+    the last value times grid(last)/grid (1/x); values that are still <= 0
+    become 1e-60 of the last entry read.  Lines before the first readable
+    pair are skipped."""
+    grid = np.asarray(grid, float)
+    n = grid.size
+    pairs = []
+    with open(path) as f:
+        for line in f:
+            t = line.replace("d", "e").replace("D", "E").split()
+            try:
+                pairs.append((float(t[0]), float(t[1])))
+            except (IndexError, ValueError):
+                if pairs:
+                    raise ValueError("%s: unreadable line %r" % (path, line))
+    if not pairs:
+        raise ValueError("%s: no (x, y) pairs" % path)
+    y = np.zeros(n)
+    x0, y0 = pairs[0]
+    i = 0
+    while i < n and x0 >= grid[i]:
+        y[i] = y0
+        i += 1
+    for x1, y1 in pairs[1:]:
+        if i >= n:
+            break
+        if y1 <= 0.0:
+            y1 = y0 * 1e-50
+        while i < n and x0 < grid[i] <= x1:
+            y[i] = 10.0 ** (math.log10(y1) + math.log10(grid[i] / x1) * math.log10(y0 / y1) / math.log10(x0 / x1))
+            i += 1
+        x0, y0 = x1, y1
+    if i == 0:
+        raise ValueError("%s: the table starts beyond the grid" % path)
+    for j in range(i, n):
+        y[j] = y[i - 1] * grid[i - 1] / grid[j]
+    return np.where(y <= 0.0, y0 * 1e-60, y)
+
+
+def surface_density(R, Theta, path, gaspath=None, gas2dust=100.0, mtot=None):
+    """'SURFFILE' densities (Init.f:2966-3003): the file's surface density
+    regridded on the cell centres (regridlog), spread evenly over each
+    ring, dens = Sigma (R_i+1^2 - R_i^2) / V in the reference's mixed units
+    (radii in AU, volumes in cm^3), then scaled to mtot [g] when mdust was
+    given, else kept (Init.f:3242-3264).  gaspath: the gas surface density,
+    gasdens = Sigma_gas pi (R_i+1^2 - R_i^2) AU^2 / V / (nTheta - 1) /
+    gas2dust, not scaled.  Returns (dens, V, gasdens or None)."""
+    R = np.asarray(R, float)
+    nR, nc = R.size - 1, np.asarray(Theta).size - 1
+    V = cell_volumes(R, Theta)
+    R_av = 10.0 ** ((np.log10(R[:-1]) + np.log10(R[1:])) / 2.0)
+    ring = (R[2:] ** 2 - R[1:-1] ** 2)[:, None]
+    dens = np.full((nR, nc), 1e-60)
+    dens[1:] = regridlog(path, R_av[1:])[:, None] * ring / V[1:]
+    mass = float((dens[1:] * V[1:]).sum())
+    dens[1:] = dens[1:] * ((mass if mtot is None else mtot) / mass)
+    gas = None
+    if gaspath:
+        gas = np.full((nR, nc), 1e-60)
+        gas[1:] = regridlog(gaspath, R_av[1:])[:, None] * math.pi * ring * AU ** 2 / V[1:] / float(
+            np.float32(nc)) / gas2dust
+    return np.maximum(dens, 1e-60), V, gas
 
 
 def analytic_density(denstype, R, Theta, thet, p, lam=None, kext=None):
@@ -385,7 +453,7 @@ def analytic_density(denstype, R, Theta, thet, p, lam=None, kext=None):
                                   * (1.0 + mu / mu0) ** (-0.5)
                                   * (mu / mu0 + 2.0 * mu0 ** 2 * p["rexp"] * AU / R_av[i]) ** (-1.0)) / p["gas2dust"]
             mdustscale = False
-        elif denstype in THIN_START_DENSITIES:
+        elif denstype in ("POW", "DOUBLEPOW", "SIMILARITY", "DOUBLEPOWSIM"):
             ra = R_av / AU
             g = p["gamma_exp"] if p["gamma_exp"] >= 0.0 else 2.0 - p["denspow"]   # Init.f:1568
             if denstype == "POW":
@@ -947,6 +1015,7 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
         Ksca = np.zeros_like(Ksca)
     if scat == 1:
         F = np.ones_like(F)
+    gasdens = None
     if denstype == "FILE":
         # the dust density of a denstemp file and the grid rebuilt from its
         # cell centres (Init.f:2727-2752, readstruct InputOutput.f:579)
@@ -959,6 +1028,12 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
         V = cell_volumes(R, Theta)
         dens = np.full(V.shape, 1e-60)
         dens[1:] = dt["dens"]
+    elif denstype == "SURFFILE":
+        R, Theta, thet, SinTheta = spatial_grid(rstar_cm, rin, rout, nrad, ntheta)
+        gfile = v("gasdensfile", "", str)
+        dens, V, gasdens = surface_density(
+            R, Theta, path_of(v("densfile", "", str)), path_of(gfile) if gfile else None, v("gas2dust", 100.0),
+            v("mdust", 1e-15) * MSUN if "mdust" in d else None)
     elif denstype in ANALYTIC_DENSITIES + THIN_START_DENSITIES:
         R, Theta, thet, SinTheta = spatial_grid(rstar_cm, rin, rout, nrad, ntheta)
         kext = [r["kext"] if "kext" in r else np.asarray(r["kabs"]) + np.asarray(r["ksca"]) for r in res]
@@ -1004,7 +1079,8 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
     m = Model(nr=nr, nt=nt, R=R, Theta=Theta, SinTheta=SinTheta, thet=thet, dens=dens.reshape(-1), V=V.reshape(-1),
               ncomp=len(res), comp_w=w.reshape(nr * (nt - 1), len(res)), nlam=nlam, lam=lam, nu=nu, Kabs=Kabs,
               Ksca=Ksca, F=F, BB=BB, Fstar=Fstar, Lstar=Lstar, Tstar=tstar, Rstar_cm=rstar_cm, scat_how=scat,
-              bins=[g[0] for g in grain_info], w=w0, distance=v("distance", 100.0))
+              bins=[g[0] for g in grain_info], w=w0, distance=v("distance", 100.0),
+              gasdens=None if gasdens is None else gasdens.reshape(-1))
     run = dict(seed=abs(v("idum", -42, int)), randomwalk=v("randomwalk", False, bool), factRW=v("factrw", 10.0),
                maxinteract=v("maxinteract", 1000000, int), nruns=v("nruns", 1, int),
                nphotdiffuse=v("nphotdiffuse", 25, int), dtdiffuse=v("dtdiffuse", 1.0),

@@ -52,10 +52,13 @@ def compare_cells(T1, dT1, T2, dT2, nr, nt):
 def initial_state(model):
     """cell arrays of the structure step at the start: the unsettled
     condensable density and abundances equal the dust's, and the gas
-    density (in dust-density units) equals the dust density (Init.f:3904)"""
+    density (in dust-density units) equals the dust density, unless the
+    model carries its own (a gas surface-density file, Init.f:3904)"""
     dens = np.asarray(model.dens, float).copy()
     w = np.asarray(model.comp_w, float).reshape(model.ncell, -1).copy()
-    return dict(dens=dens, dens0=dens.copy(), gasdens=dens.copy(), w=w, w0=w.copy())
+    gas = getattr(model, "gasdens", None)
+    gas = dens.copy() if gas is None else np.asarray(gas, float).copy()
+    return dict(dens=dens, dens0=dens.copy(), gasdens=gas, w=w, w0=w.copy())
 
 
 def planck_means(model):

@@ -459,3 +459,39 @@ def test_massloss_and_infall_densities(tmp_path):
     # nearer in, the flow piles up toward the midplane
     i = int(np.searchsorted(R_av / M.AU, 1.0))
     assert dens[i, -1] > dens[i, 0]
+
+
+def test_regridlog_follows_the_reference_reader(tmp_path):
+    p = tmp_path / "s.dat"
+    p.write_text("# r sigma\n1.0 10.0\n2.0 5.0\n4.0 0.0\n8.0 1.0\n")
+    grid = np.array([0.5, 1.0, 1.5, 3.0, 6.0, 16.0, 32.0])
+    y = M.regridlog(str(p), grid)
+    assert y[0] == 10.0 and y[1] == 10.0                     # at or below the first x
+    assert abs(y[2] - 10.0 * 1.5 ** -1.0) < 1e-12            # log-log inside: Sigma ~ 1/r here
+    # an entry <= 0 is read as 1e-50 of the one before
+    assert abs(math.log10(y[3] / 5.0) - math.log10(5e-50 / 5.0) * math.log10(3.0 / 2.0) / math.log10(2.0)) < 1e-9
+    assert y[5] == y[4] * 6.0 / 16.0 or abs(y[5] / (1.0 * 8.0 / 16.0) - 1) < 1e-12
+    assert abs(y[6] / y[5] - 0.5) < 1e-12                    # beyond the table: 1/r from the last point
+
+
+def test_surface_density_file(tmp_path):
+    r = np.geomspace(0.05, 2000.0, 60)
+    (tmp_path / "sigma.dat").write_text("".join("%.8e %.8e\n" % (a, 100.0 * a ** -1.0) for a in r))
+    (tmp_path / "gas.dat").write_text("".join("%.8e %.8e\n" % (a, 1e4 * a ** -1.0) for a in r))
+    deck, parts = _analytic_deck(tmp_path, "denstype='SURFFILE'\ndensfile='sigma.dat'\nmdust=1d-4\n"
+                                           "gasdensfile='gas.dat'\n")
+    m, run = M.deck_model(None, deck, compute_parts=parts)
+    dens, V, r_, z_ = _cells(m)
+    assert abs((dens[1:] * V[1:]).sum() / (1e-4 * M.MSUN) - 1.0) < 1e-12
+    R = np.asarray(m.R)
+    R_av = 10.0 ** ((np.log10(R[:-1]) + np.log10(R[1:])) / 2.0)
+    # each ring's mass goes as Sigma(R_av) (R_i+1^2 - R_i^2), spread evenly over its cells
+    ringmass = (dens * V).sum(1)[1:]
+    want = R_av[1:] ** -1.0 * (R[2:] ** 2 - R[1:-1] ** 2)
+    assert np.allclose(ringmass / want, ringmass[0] / want[0], rtol=1e-7)   # the table has 9 digits
+    assert np.allclose(dens[1:], dens[1:, :1], rtol=1e-12)
+    gas = m.gasdens.reshape(m.nr, -1)
+    want_gas = 1e4 * R_av[1:, None] ** -1.0 * math.pi * (R[2:] ** 2 - R[1:-1] ** 2)[:, None] * M.AU ** 2 / V[1:] / \
+        (m.nt - 1) / 100.0
+    assert np.allclose(gas[1:], want_gas, rtol=1e-7)
+    assert run["thin_start"] and not run["iterate"]
