@@ -884,7 +884,7 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
     if startype not in ("PLANCK", "FILE"):
         raise ValueError("startype: 'PLANCK' or 'FILE' stars")
     denstype = v("denstype", "ZONES", str).upper()
-    if denstype not in ("ZONES", "FILE") + ANALYTIC_DENSITIES + THIN_START_DENSITIES:
+    if denstype not in ("ZONES", "FILE", "SHELLFILE") + ANALYTIC_DENSITIES + THIN_START_DENSITIES:
         raise ValueError("denstype: 'ZONES', 'FILE' or one of %s"
                          % ", ".join(ANALYTIC_DENSITIES + THIN_START_DENSITIES))
     if denstype == "PARAMETERIZED" and ("scalesh" in d or "rimscale" in d):
@@ -907,7 +907,7 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
         zones.append(dict(rin=v(kz + "rin", rin), rout=v(kz + "rout", rout), mdust=v(kz + "mdust", 1e-5),
                           denspow=v(kz + "denspow", 1.0), sh=v(kz + "sh", 0.01), rsh=v(kz + "rsh", 1.0),
                           shpow=v(kz + "shpow", 1.1), fix=v(kz + "fix", False, bool)))
-    if zones and denstype in ANALYTIC_DENSITIES + THIN_START_DENSITIES:
+    if zones and denstype in ("SHELLFILE",) + ANALYTIC_DENSITIES + THIN_START_DENSITIES:
         raise ValueError("denstype %s takes no zoneN:* keywords" % denstype)
     if not zones and denstype == "ZONES":
         raise ValueError("no zoneN:* keywords")
@@ -1028,6 +1028,14 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
         V = cell_volumes(R, Theta)
         dens = np.full(V.shape, 1e-60)
         dens[1:] = dt["dens"]
+    elif denstype == "SHELLFILE":
+        # a radial density table taken as the cells' density, not scaled
+        # to a dust mass (Init.f:3005-3023)
+        R, Theta, thet, SinTheta = spatial_grid(rstar_cm, rin, rout, nrad, ntheta)
+        V = cell_volumes(R, Theta)
+        R_av = 10.0 ** ((np.log10(R[:-1]) + np.log10(R[1:])) / 2.0)
+        dens = np.full(V.shape, 1e-60)
+        dens[1:] = np.maximum(regridlog(path_of(v("densfile", "", str)), R_av[1:]), 1e-60)[:, None]
     elif denstype == "SURFFILE":
         R, Theta, thet, SinTheta = spatial_grid(rstar_cm, rin, rout, nrad, ntheta)
         gfile = v("gasdensfile", "", str)

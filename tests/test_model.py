@@ -495,3 +495,16 @@ def test_surface_density_file(tmp_path):
         (m.nt - 1) / 100.0
     assert np.allclose(gas[1:], want_gas, rtol=1e-7)
     assert run["thin_start"] and not run["iterate"]
+
+
+def test_shell_density_file(tmp_path):
+    r = np.geomspace(0.05, 2000.0, 40)
+    (tmp_path / "shell.dat").write_text("".join("%.12e %.12e\n" % (a, 1e-18 * a ** -2.0) for a in r))
+    deck, parts = _analytic_deck(tmp_path, "denstype='SHELLFILE'\ndensfile='shell.dat'\nmdust=1d-4\n")
+    m, run = M.deck_model(None, deck, compute_parts=parts)
+    dens, V, _, _ = _cells(m)
+    R = np.asarray(m.R)
+    R_av = 10.0 ** ((np.log10(R[:-1]) + np.log10(R[1:])) / 2.0)
+    # the table's values, not scaled to mdust
+    assert np.allclose(dens[1:], 1e-18 * R_av[1:, None] ** -2.0, rtol=1e-9)
+    assert not run["thin_start"]
