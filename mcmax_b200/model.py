@@ -279,7 +279,8 @@ def zones_density(R, Theta, thet, zones):
     dens[1:] = 1e-60 + total[1:]
     return dens, V
 
-ANALYTIC_DENSITIES = ("PASCUCCI", "MIN", "PARAMETERIZED", "PINTE", "SHELL", "WEDGE", "MASSLOSS", "INFALL")
+ANALYTIC_DENSITIES = ("PASCUCCI", "MIN", "PARAMETERIZED", "PINTE", "SHELL", "WEDGE", "MASSLOSS", "INFALL",
+                      "MEIXNER")
 # radial power laws whose vertical structure the reference builds from the
 # optically thin temperatures before the first pass (Init.f:3924-3960)
 THIN_START_DENSITIES = ("POW", "DOUBLEPOW", "SIMILARITY", "DOUBLEPOWSIM", "SURFFILE")
@@ -362,8 +363,9 @@ def analytic_density(denstype, R, Theta, thet, p, lam=None, kext=None):
     averaged over 10 sub-angles), SHELL ((AU/R)^denspow) and WEDGE (the
     cells within wedgeopen degrees of the midplane, 10 sub-angles), MASSLOSS
     (a wind Mdot / (gas2dust 4 pi R^2 v(R)), v = vexp2 (1 - (1 - (vexp1 /
-    vexp2)^(1/bexp)) Rstar / R)^bexp) and INFALL (rotating infall of
-    Minfall onto radius rexp around Mstar).  r and z
+    vexp2)^(1/bexp)) Rstar / R)^bexp), INFALL (rotating infall of
+    Minfall onto radius rexp around Mstar) and MEIXNER (meixa..meixf,
+    meixrsw, meixrin, timeshift).  r and z
     are taken at the cell centre (R_av, theta_av); cell i = 0 is empty.
     Also the radial power laws of THIN_START_DENSITIES (POW, DOUBLEPOW,
     SIMILARITY, DOUBLEPOWSIM, with denspow2, rpow2, rpow3, rexp,
@@ -435,6 +437,20 @@ def analytic_density(denstype, R, Theta, thet, p, lam=None, kext=None):
             d1 = p["mdot"] / (p["gas2dust"] * 4.0 * math.pi * R_av ** 2 * vexp)
             dens = np.broadcast_to(d1[:, None], (nR, nc)).copy()
             mdustscale = False
+        elif denstype == "MEIXNER":
+            # the axisymmetric superwind shell of Meixner et al. (2002) as
+            # Init.f:3226-3238 writes it, r shifted by timeshift vexp1
+            ra = R_av / AU
+            rr = ra - p["timeshift"] * p["vexp1"] * 0.210944839e-5
+            rin_m, rsw = p["meixrin"], p["meixrsw"]
+            st, ct = np.sin(theta_av)[None, :], np.cos(theta_av)[None, :]
+            rc = rr[:, None]
+            dens = ((rc / rin_m) ** (-p["meixb"] * (1.0 + p["meixc"] * st ** p["meixf"]
+                                                     * np.exp(-(rc / rsw) ** p["meixd"] + (rin_m / rsw) ** p["meixd"]))))
+            dens = dens * (1.0 + p["meixa"] * (1.0 - ct) ** p["meixf"]
+                           * np.exp(-(rc / rsw) ** p["meixe"] + (rin_m / rsw) ** p["meixe"]))
+            dens = dens * (rc / ra[:, None]) ** 2
+            dens = np.where(rc > rin_m, dens, 1e-60)
         elif denstype == "INFALL":
             # rotating infall onto a disk of radius rexp: mu0 of each
             # streamline by solve_mu0's scan of 1000 values (Init.f:5747-5764)
@@ -1055,6 +1071,9 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
             vexp1=v("vexp1", v("vexp", 10.0)) * 100000.0,
             vexp2=(v("vexp2", -10.0) if v("vexp2", -10.0) > 0.0 else v("vexp1", v("vexp", 10.0))) * 100000.0,
             bexp=v("bexp", 0.5), gas2dust=v("gas2dust", 100.0), mstar=v("mstar", 2.5) * MSUN, rstar_cm=rstar_cm,
+            meixa=v("meixa", 8.0), meixb=v("meixb", 2.0), meixc=v("meixc", 2.0), meixd=v("meixd", 1.0),
+            meixe=v("meixe", 3.0), meixf=v("meixf", 1.0), meixrsw=v("meixrsw", 1800.0),
+            meixrin=v("meixrin", -1.0) if v("meixrin", -1.0) > 0.0 else rin, timeshift=v("timeshift", 0.0),
             mtot=v("mdust", 1e-15) * MSUN, mdustscale="mdust" in d), lam=lam, kext=kext)
     else:
         R, Theta, thet, SinTheta = spatial_grid(rstar_cm, rin, rout, nrad, ntheta)

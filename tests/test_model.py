@@ -508,3 +508,21 @@ def test_shell_density_file(tmp_path):
     # the table's values, not scaled to mdust
     assert np.allclose(dens[1:], 1e-18 * R_av[1:, None] ** -2.0, rtol=1e-9)
     assert not run["thin_start"]
+
+
+def test_meixner_shell(tmp_path):
+    """at the inner radius the profile is 1 + A (1 - cos theta)^F; with
+    C = 0 it falls as r^-B times the equatorial factor"""
+    deck, parts = _analytic_deck(tmp_path, "denstype='MEIXNER'\nmdust=1d-5\nmeixc=0\nmeixrin=1\n")
+    m, _ = M.deck_model(None, deck, compute_parts=parts)
+    dens, V, _, _ = _cells(m)
+    R = np.asarray(m.R)
+    ra = 10.0 ** ((np.log10(R[:-1]) + np.log10(R[1:])) / 2.0)
+    th = np.arccos((m.Theta[:-1] + m.Theta[1:]) / 2.0)
+    f = (ra[:, None] / 1.0) ** -2.0 * (1.0 + 8.0 * (1.0 - np.cos(th))[None, :]
+                                        * np.exp(-(ra[:, None] / 1800.0) ** 3 + (1.0 / 1800.0) ** 3))
+    sel = ra[1:] > 1.0
+    ratio = dens[1:][sel] / f[1:][sel]
+    assert np.allclose(ratio, ratio[0, 0], rtol=1e-10)
+    assert np.all(dens[1:][~sel] < 1e-55)
+    assert abs((dens[1:] * V[1:]).sum() / (1e-5 * M.MSUN) - 1) < 1e-12
