@@ -409,7 +409,7 @@ def test_shell_and_wedge_densities(tmp_path):
     assert np.all(dens[1:, lo > 20.5] <= 1e-60)          # at the floor
     assert np.all(dens[1:, -1] > 1e-40)
     with pytest.raises(ValueError):
-        M.deck_model(None, deck, overrides=["denstype='MEIXNER'"], compute_parts=parts)
+        M.deck_model(None, deck, overrides=["denstype='PRODIMO'"], compute_parts=parts)
     with pytest.raises(ValueError):
         M.deck_model(None, deck, overrides=["zone1:rin=1"], compute_parts=parts)
 
