@@ -922,7 +922,8 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
             continue
         zones.append(dict(rin=v(kz + "rin", rin), rout=v(kz + "rout", rout), mdust=v(kz + "mdust", 1e-5),
                           denspow=v(kz + "denspow", 1.0), sh=v(kz + "sh", 0.01), rsh=v(kz + "rsh", 1.0),
-                          shpow=v(kz + "shpow", 1.1), fix=v(kz + "fix", False, bool)))
+                          shpow=v(kz + "shpow", 1.1), fix=v(kz + "fix", False, bool),
+                          alphaturb=v(kz + "alphaturb", v("alphaturb", 1e-4))))
     if zones and denstype in ("SHELLFILE",) + ANALYTIC_DENSITIES + THIN_START_DENSITIES:
         raise ValueError("denstype %s takes no zoneN:* keywords" % denstype)
     if not zones and denstype == "ZONES":
@@ -1117,8 +1118,24 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
     # the structure loop runs for zones without a fixed structure or with
     # iter=.true. (Init.f:563,1519); it and the power-law densities start
     # from the optically thin structure (Init.f:3924-3960)
-    run["iterate"] = any(not z["fix"] for z in zones) or v("iter", False, bool)
-    run["thin_start"] = run["iterate"] or denstype in THIN_START_DENSITIES
+    mpset = v("mpset", False, bool)
+    if mpset and v("fixmpset", False, bool):
+        raise ValueError("mpset and fixmpset: one settling prescription at a time")
+    run["iterate"] = any(not z["fix"] for z in zones) or v("iter", False, bool) or (mpset and bool(zones))
+    run["settling"] = None
+    if mpset:
+        # MPSettling's inputs (Init.f:2906, 3070: the zones' alphaturb on their rings)
+        R_av = AU * 10.0 ** ((np.log10(R[:-1]) + np.log10(R[1:])) / 2.0)
+        alpha = np.full(nr, v("alphaturb", 1e-4))
+        for z in zones:
+            alpha[(R_av >= z["rin"] * AU) & (R_av <= z["rout"] * AU)] = z["alphaturb"]
+        rv = np.array([g[1] for g in grain_info])
+        rho_g = np.array([r["rho_av"] for r in res])
+        if not (np.all(np.isfinite(rv)) and np.all(np.isfinite(rho_g))):
+            raise ValueError("mpset: an opacNN grain has no size or density to settle")
+        run["settling"] = dict(rho=rho_g, rv=rv, alpha=alpha,
+                               rscale=np.array([r.get("rscale", 1.0) for r in res]), gas2dust=v("gas2dust", 100.0))
+    run["thin_start"] = run["iterate"] or denstype in THIN_START_DENSITIES or mpset
     return m, run
 
 

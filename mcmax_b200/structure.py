@@ -131,17 +131,69 @@ def thin_temperature(model, Kp=None, kpabsstar=None):
     return np.where(np.isnan(E), 3.0, T)
 
 
-def thin_start(ctx, model, zones, Mstar, shscale=None, grain_scale=None):
+def mp_settling(model, state, T, Mstar, rho, rv, alpha, rscale=None, gas2dust=100.0):
+    """Dust scale-height factors of MPSettling (MPSettling.f:8-121, after
+    Dubrulle et al. 1995), recomputed before every structure pass: per grain
+    ii and ring i, the stopping time of the midplane cell, tau_f =
+    <rho_ii rv_ii rscale> / (c_s rho_gas) (the grain's density-weighted
+    mean over the ring's cells, rho_gas from the midplane gas density, or
+    the dust's times gas2dust when that is below 1e-5 of the dust's), with
+    c_s = sqrt(k T / (2.3 amu)) at the midplane temperature, Omega =
+    sqrt(G Mstar / R^3), h = (1/3)^(1/4) sqrt(alpha / (Omega tau_f)) and
+    the factor h / sqrt(1 + h^2).  The reference's constants are kept: G =
+    6.672e-8, mu = 2.3 as a single-precision literal.  rho, rv [cm],
+    rscale: per grain; alpha: per ring (the zone's alphaturb).  Returns the
+    grain_scale array (ngrains, nr) of mcg_disk_structure (ring 0 unused,
+    1)."""
+    from .model import AU
+    nr, nc = model.nr, model.nt - 1
+    ng = model.ncomp
+    dens = np.asarray(state["dens"], float).reshape(nr, nc)
+    gas = np.asarray(state["gasdens"], float).reshape(nr, nc)
+    w = np.asarray(state["w"], float).reshape(nr, nc, ng)
+    T = np.asarray(T, float).reshape(nr, nc)
+    rscale = np.ones(ng) if rscale is None else np.asarray(rscale, float)
+    R = np.asarray(model.R, float)
+    R_av = AU * 10.0 ** ((np.log10(R[:-1]) + np.log10(R[1:])) / 2.0)
+    GG, amu, kb, mu, gamma = 6.672e-8, 1.66053886e-24, 1.3806503e-16, float(np.float32(2.3)), 2.0
+    omega_r = math.sqrt(GG * Mstar)
+    cs_T = math.sqrt(kb / (mu * amu))
+    prefac = (1.0 / (1.0 + gamma)) ** 0.25
+    scale = np.ones((ng, nr))
+    for ii in range(ng):
+        for i in range(1, nr):
+            t, tot = 0.0, 0.0
+            for j in range(nc):
+                t = t + dens[i, j] * w[i, j, ii] * rho[ii] * rv[ii] * rscale[ii]
+                tot = tot + dens[i, j] * w[i, j, ii]
+            t = t / tot if tot > 1e-100 else rho[ii] * rv[ii]
+            rho_g = gas[i, nc - 1] * gas2dust
+            if rho_g < dens[i, nc - 1] / 1e5:
+                rho_g = dens[i, nc - 1] * gas2dust
+            cs = cs_T * math.sqrt(T[i, nc - 1])
+            omegatau = (omega_r / R_av[i] ** 1.5) * (t / (cs * rho_g))
+            h = prefac * math.sqrt(alpha[i] / omegatau)
+            scale[ii, i] = h * (1.0 + h ** 2) ** (-0.5)
+    return scale
+
+
+def thin_start(ctx, model, zones, Mstar, shscale=None, grain_scale=None, settling=None):
     """The vertical structure the first Monte Carlo pass starts from
     (Init.f:3924-3960): dens0 = gasdens = dens, the optically thin
     temperatures (BackWarming(1) changes nothing before the first pass:
     no cell has absorbed packets yet), their average (the first
     TempAverage copies them) and three DiskStructure passes on them.
+    settling: the keyword arguments of mp_settling (rho, rv, alpha,
+    rscale, gas2dust) when the grains settle (mpset); their factors are
+    then recomputed before every pass, at the thin temperatures.
     Regridding in theta and dead zones are not built.  Updates the model's
     dens and comp_w; returns dict(state, Temp)."""
     state = initial_state(model)
-    Temp = temp_average(None, thin_temperature(model), 1.0)
+    Tthin = thin_temperature(model)
+    Temp = temp_average(None, Tthin, 1.0)
     for _ in range(3):
+        if settling:
+            grain_scale = mp_settling(model, state, Tthin, Mstar, **settling)
         out = ctx.disk_structure(model.R, model.Theta, model.V, Mstar, zones, Temp, state["dens"], state["dens0"],
                                  state["gasdens"], state["w"], state["w0"], shscale, grain_scale)
         state = dict(zip(("dens", "dens0", "gasdens", "w", "w0"), out))
@@ -152,19 +204,22 @@ def thin_start(ctx, model, zones, Mstar, shscale=None, grain_scale=None):
 
 def iterate(ctx, model, zones, Mstar, nphot, run=None, maxiter=10, epsiter=3.0, f_weight=0.5, niter0=1000,
             nphotdiffuse=25, dtdiffuse=1.0, shscale=None, grain_scale=None, precision="mixed", log=None,
-            thin=False):
+            thin=False, settling=None):
     """Run the structure iterations on `model` (one opacity set per grain:
     comp_w holds the grains' abundances).  zones: (rin, rout, sh, rsh,
     shpow, denspow, fix_struct) per zone; Mstar in g; run: the keyword
     arguments of Context.mcradiation.  thin: start from the optically thin
     structure (thin_start), as the reference does before its first pass;
-    otherwise from the model's densities.  The model's dens and comp_w are
-    updated in place.  Returns dict(T, dT, Temp, state, history, nphot,
-    result) with one history entry (niter, errT, packets) per structure
-    pass and the last packet run's count and result."""
+    otherwise from the model's densities.  settling: mp_settling's keyword
+    arguments when the grains settle (mpset): the factors are recomputed
+    from the current state and temperatures before every structure pass.
+    The model's dens and comp_w are updated in place.  Returns dict(T, dT,
+    Temp, state, history, nphot, result) with one history entry (niter,
+    errT, packets) per structure pass and the last packet run's count and
+    result."""
     run = dict(run or {})
     if thin:
-        state = thin_start(ctx, model, zones, Mstar, shscale, grain_scale)["state"]
+        state = thin_start(ctx, model, zones, Mstar, shscale, grain_scale, settling)["state"]
     else:
         state = initial_state(model)
     Temp = None
@@ -190,6 +245,8 @@ def iterate(ctx, model, zones, Mstar, nphot, run=None, maxiter=10, epsiter=3.0, 
         else:
             fw = 1.0
         Temp = temp_average(Temp, T, fw)
+        if settling:
+            grain_scale = mp_settling(model, state, T, Mstar, **settling)
         out = ctx.disk_structure(model.R, model.Theta, model.V, Mstar, zones, Temp, state["dens"], state["dens0"],
                                  state["gasdens"], state["w"], state["w0"], shscale, grain_scale)
         state = dict(zip(("dens", "dens0", "gasdens", "w", "w0"), out))

@@ -285,3 +285,45 @@ def test_thin_start_runs_three_structure_passes():
     fake2 = _FakeRun([T])
     r = S.iterate(fake2, _driver_model(), zones, 2.5 * M.MSUN, 1000, thin=True)
     assert fake2.calls["ds"] == 3 + len(r["history"])
+
+
+def test_mp_settling_factors():
+    """MPSettling's factor h / sqrt(1 + h^2), h = (1/3)^(1/4) sqrt(alpha /
+    (Omega tau_f)), tau_f = rho_grain rv / (c_s rho_gas) at the midplane:
+    near 1 for small grains, small for large ones"""
+    m = _driver_model()
+    st = S.initial_state(m)
+    T = _temp(m)
+    nr, nc = m.nr, m.nt - 1
+    rho = np.array([3.0, 3.0])
+    rv = np.array([1e-5, 1e-1])
+    alpha = np.full(nr, 1e-3)
+    sc = S.mp_settling(m, st, T, 2.5 * M.MSUN, rho, rv, alpha)
+    assert sc.shape == (m.ncomp, nr) and np.all(sc[:, 0] == 1.0)
+    assert np.all(sc[0, 1:] > 0.9) and np.all(sc[1, 1:] < sc[0, 1:])
+    R_av = M.AU * 10.0 ** ((np.log10(m.R[:-1]) + np.log10(m.R[1:])) / 2.0)
+    d = st["dens"].reshape(nr, nc)
+    for i in (3, 10):
+        cs = math.sqrt(1.3806503e-16 * T.reshape(nr, nc)[i, -1] / (float(np.float32(2.3)) * 1.66053886e-24))
+        tauf = rho[1] * rv[1] / (cs * d[i, -1] * 100.0)
+        om = math.sqrt(6.672e-8 * 2.5 * M.MSUN / R_av[i] ** 3)
+        h = (1.0 / 3.0) ** 0.25 * math.sqrt(1e-3 / (om * tauf))
+        assert abs(sc[1, i] / (h / math.sqrt(1 + h * h)) - 1) < 1e-10
+
+
+def test_settling_factors_reach_each_structure_pass():
+    m = _driver_model()
+    T = _temp(m)
+    seen = []
+
+    class Fake(_FakeRun):
+        def disk_structure(self, *a, **kw):
+            seen.append(a[12] if len(a) > 12 else kw.get("grain_scale"))
+            return super().disk_structure(*a, **kw)
+
+    fake = Fake([T])
+    zones = [(0.5, 100.0, SH, 1.0, 1.125, 1.0, 0)]
+    settling = dict(rho=np.array([3.0, 3.0]), rv=np.array([1e-5, 1e-2]), alpha=np.full(m.nr, 1e-4))
+    S.iterate(fake, m, zones, 2.5 * M.MSUN, 1000, thin=True, settling=settling)
+    assert len(seen) == fake.calls["ds"] and all(g is not None and g.shape == (2, m.nr) for g in seen)
+    assert all(np.all(g[1, 1:] < g[0, 1:]) for g in seen)
