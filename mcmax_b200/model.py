@@ -1116,8 +1116,9 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
                Mstar=v("mstar", 2.5) * MSUN, maxiter=v("maxiter", 10, int), epsiter=v("epsiter", 3.0),
                incangle=v("incangle", 45.0), outputfits=v("outputfits", False, bool), posangle=v("posangle", 0.0))
     # the structure loop runs for zones without a fixed structure or with
-    # iter=.true. (Init.f:563,1519); it and the power-law densities start
-    # from the optically thin structure (Init.f:3924-3960)
+    # iter=.true. (Init.f:563,1519); it, the power-law densities and every
+    # deck with zones start from the optically thin structure
+    # (Init.f:3924-3960)
     mpset = v("mpset", False, bool)
     if mpset and v("fixmpset", False, bool):
         raise ValueError("mpset and fixmpset: one settling prescription at a time")
@@ -1135,7 +1136,11 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
             raise ValueError("mpset: an opacNN grain has no size or density to settle")
         run["settling"] = dict(rho=rho_g, rv=rv, alpha=alpha,
                                rscale=np.array([r.get("rscale", 1.0) for r in res]), gas2dust=v("gas2dust", 100.0))
-    run["thin_start"] = run["iterate"] or denstype in THIN_START_DENSITIES or mpset
+    # the reference runs the start whenever the deck has zones (nzones /= 0):
+    # its structure pass rebuilds a fixed zone's profile at the cell
+    # centres.  With fixmpset the settled zone above is that rebuild already.
+    run["thin_start"] = (run["iterate"] or denstype in THIN_START_DENSITIES or mpset
+                         or (bool(zones) and not v("fixmpset", False, bool)))
     return m, run
 
 

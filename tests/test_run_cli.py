@@ -116,6 +116,9 @@ def test_command_line_runs_the_deck_and_writes_result_files(tmp_path):
     assert ctx.calls == [dict(nphot=20000, precision="fp64", seed=11, randomwalk=True, factRW=4.0,
                               maxinteract=5000, nruns=2)]
     assert ctx.diffuse_args == (7, 25, 1.0, 4.0) and r["diffused"] == (1, 5, 1, 0)
+    # a deck with zones starts from three structure passes (a fixed zone's
+    # profile rebuilt at the cell centres), as the reference's Init does
+    assert ctx.structure_calls == 3 and ctx.structure_zones == [(1.0, 50.0, 0.01, 1.0, 1.1, 1.0, True)]
     assert len(r["files"]) == 33 and all(os.path.exists(f) for f in r["files"])
     assert os.path.basename(r["files"][-1]) == "spectrum30.0.dat"
     assert made[0].trace_args[1:] == (20, 2, ()) and abs(made[0].trace_args[0] - np.radians(30)) < 1e-15
