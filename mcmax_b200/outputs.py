@@ -321,10 +321,12 @@ def spectrum_name(angle_deg, flag=""):
 
 
 def write_spectrum(outdir, angle_deg, lam_obs, flux, lam, Fstar, distance_pc=100.0, scatflux=None, flag="",
-                   star_column="reference"):
+                   star_column="reference", polarised=False):
     """spectrum<angle>.dat of a ray-traced spectrum (Telescope.f:140-160):
     wavelength [micron], flux [Jy], its scattered part [Jy], the star [Jy],
-    with no interstellar extinction (Av = 0).  star_column "reference"
+    with no interstellar extinction (Av = 0); with polarised (scattering
+    with the full Mueller matrix) a fifth column, the Q flux [Jy], zero
+    here: the traced flux carries no polarisation.  star_column "reference"
     writes the star as the reference's arrinterpol gives it (see
     _arrinterpol_log); "interpolated" writes the log-log interpolation of
     the stellar spectrum instead.  Returns the path."""
@@ -340,8 +342,8 @@ def write_spectrum(outdir, angle_deg, lam_obs, flux, lam, Fstar, distance_pc=100
                 fs = _arrinterpol_log(l0, lam, Fstar)
             else:
                 fs = float(np.exp(np.interp(np.log(l0), np.log(lam), np.log(Fstar))))
-            f.write("%s%s%s%s\n" % (_num(l0), _num(1e23 * flux[j] / d2), _num(1e23 * scat[j] / d2),
-                                    _num(1e23 * fs / d2)))
+            f.write("%s%s%s%s%s\n" % (_num(l0), _num(1e23 * flux[j] / d2), _num(1e23 * scat[j] / d2),
+                                      _num(1e23 * fs / d2), _num(0.0) if polarised else ""))
     return path
 
 

@@ -167,7 +167,7 @@ def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opac
         lam_obs = outputs.spectrum_wavelengths(m.lam, ob["lam1"], ob["lam2"], ob["nlam"], ob["lamfile"] or None)
         flux, _ = ctx.trace_spectrum(T, lam_obs, math.radians(ob["inc"]), nphi=ob["nphi"], nr=ob["nrad"], Rfix=rfix)
         files.append(outputs.write_spectrum(outdir, ob["inc"], lam_obs, flux, m.lam, m.Fstar, m.distance,
-                                            flag=ob["flag"]))
+                                            flag=ob["flag"], polarised=int(m.scat_how) == 2))
     for ob in images:
         observe = observe_ifu if ob["kind"] == "IFU" else observe_image
         files += observe(ctx, m, T, ob, outdir, rfix, seed=run["seed"], posangle=run.get("posangle", 0.0))

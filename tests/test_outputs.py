@@ -67,6 +67,11 @@ def test_spectrum_file(tmp_path):
     assert os.path.basename(p2) == "spectrum07.5_b.dat"
     r2 = np.loadtxt(p2)
     assert np.allclose(r2[1:-1, 3], 1e23 * np.exp(np.interp(np.log(lo[1:-1]), np.log(lam), np.log(Fstar))) / d2)
+    # full Mueller scattering: a fifth column for the Q flux
+    p3 = OUT.write_spectrum(str(tmp_path), 30.0, lo, flux, lam, Fstar, polarised=True)
+    r3 = np.loadtxt(p3)
+    assert rows.shape[1] == 4 and r3.shape == (lo.size, 5)
+    assert np.all(r3[:, 4] == 0.0) and np.array_equal(r3[:, :4], rows[:, :4])
 
 
 def test_denstemp_fits_round_trip(tmp_path):
