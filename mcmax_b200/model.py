@@ -1114,7 +1114,8 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
                nphotdiffuse=v("nphotdiffuse", 25, int), dtdiffuse=v("dtdiffuse", 1.0),
                zones=[(z["rin"], z["rout"], z["sh"], z["rsh"], z["shpow"], z["denspow"], z["fix"]) for z in zones],
                Mstar=v("mstar", 2.5) * MSUN, maxiter=v("maxiter", 10, int), epsiter=v("epsiter", 3.0),
-               incangle=v("incangle", 45.0), outputfits=v("outputfits", False, bool), posangle=v("posangle", 0.0))
+               incangle=v("incangle", 45.0), outputfits=v("outputfits", False, bool), posangle=v("posangle", 0.0),
+               vis_norm_fov=v("vis_norm_fov", True, bool))
     # the structure loop runs for zones without a fixed structure or with
     # iter=.true. (Init.f:563,1519); it, the power-law densities and every
     # deck with zones start from the optically thin structure

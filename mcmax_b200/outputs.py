@@ -247,7 +247,9 @@ def read_observations(path, lam, incangle=45.0, rout=None):
     keywords before the first type= line set the defaults, each type= line
     starts an observation whose own keywords follow.  Returns a list of
     dicts with kind, inc [deg], lam1, lam2, nlam, lamfile, nphi, nrad, flag,
-    npix, nint, fov (list, AU or arcsec), scaletype (and the other keywords
+    npix, nint, fov (list, AU or arcsec), scaletype, the VISIBILITY
+    baselines b [m] and theta [deg] (default one of 100 m at 0), d (the
+    telescope diameter, m) (and the other keywords
     as given, lower-case).  Defaults: inc from the deck's incangle, lam1/lam2
     the model's range, nphi 45, nrad 2, npix 500, nint 1000, fov twice the
     grid's outer radius `rout`, scaletype 1.  An IMAGE observation's lam1 is
@@ -257,7 +259,7 @@ def read_observations(path, lam, incangle=45.0, rout=None):
     lam = np.asarray(lam, float)
     default = dict(inc=float(incangle), lam1=float(lam[0]), lam2=float(lam[-1]), nlam=-1, lamfile="", nphi=45,
                    nrad=2, flag="", npix=500, nint=1000, fov=[] if rout is None else [2.0 * float(rout)],
-                   scaletype=1)
+                   scaletype=1, b=[100.0], theta=[0.0], d=-1.0)
     deflam = (float(lam[0]) + float(lam[-1])) / 2.0
     obs, cur = [], default
     base = os.path.dirname(os.path.abspath(path))
@@ -273,7 +275,8 @@ def read_observations(path, lam, incangle=45.0, rout=None):
             if val[:1] in ("'", '"'):
                 val = val[1:-1] if len(val) > 1 and val[-1] == val[0] else val[1:]
             if key == "type":
-                cur = dict(default, kind=val.upper(), fov=list(default["fov"]))
+                cur = dict(default, kind=val.upper(), fov=list(default["fov"]), b=list(default["b"]),
+                           theta=list(default["theta"]))
                 if cur["kind"] == "IMAGE":
                     cur["lam1"] = deflam
                 obs.append(cur)
@@ -284,6 +287,16 @@ def read_observations(path, lam, incangle=45.0, rout=None):
                 deflam = num(val)
             elif key in ("inc", "lam1", "lam2", "lam"):
                 cur["lam1" if key == "lam" else key] = num(val)
+            elif cur is not default and cur["kind"] == "VISIBILITY" and (
+                    (key[:4] == "base" and key[4:].isdigit()) or (key[:5] == "angle" and key[5:].isdigit())):
+                # baseN [m] and angleN [deg] of the baselines (Telescope.f:1067-1127)
+                i = int(key[4:] if key[:4] == "base" else key[5:])
+                while len(cur["b"]) < i:
+                    cur["b"].append(0.0)
+                    cur["theta"].append(0.0)
+                cur["b" if key[:4] == "base" else "theta"][i - 1] = num(val)
+            elif key == "d":
+                cur["d"] = num(val)
             elif key[:3] == "fov":
                 i = int(key[3:]) if len(key) > 3 else 1
                 while len(cur["fov"]) < i:
@@ -482,4 +495,110 @@ def write_rimage(path, R, rphi, rscale, zscale, distance_cm, fov_au, npixel, pol
     with open(path, "w") as f:
         for row in lines:
             f.write("".join(_num(x) for x in row) + "\n")
+    return path
+
+
+def image_phi(nphi):
+    """the angles of the image columns, 1e-5 + pi (k - 1/2) / nphi with the
+    single-precision k - 0.5 of TraceMono.f:2237"""
+    k = np.arange(1, nphi + 1, dtype=np.float32)
+    return 1e-5 + (math.pi * (k - np.float32(0.5)).astype(float)) / float(np.float32(nphi))
+
+
+def _vis_half(R, rphi, phi_c, nphi, theta, k, Rsigma, vis_norm_fov, sign):
+    """one half of the image plane (+phi or -phi) of Visibility.f:36-150:
+    per ring segment and angle column the closed-form Fourier integral of
+    an intensity linear in r and constant in phi; returns (cV, Ftot)"""
+    r1 = R[:-1, None]
+    r2 = R[1:, None]
+    I1 = rphi[:-1]
+    I2 = rphi[1:]
+    Rs2 = np.float64(Rsigma) ** 2 if Rsigma < 1e150 else np.inf   # 1e200^2 is infinite, as in the reference
+    t1 = I1 * np.exp(-r1 ** 2 / (2.0 * Rs2))
+    t2 = I2 * np.exp(-r2 ** 2 / (2.0 * Rs2))
+    n1, n2 = (t1, t2) if vis_norm_fov else (I1, I2)
+    half = 0.5 * math.pi / float(np.float32(nphi))
+    phi1 = sign * phi_c[None, :] - half
+    phi2 = sign * phi_c[None, :] + half
+    c1 = np.cos(theta + phi1)
+    b1 = np.sin((phi1 + phi2) / 2.0 + theta)
+    a1 = c1 + 2.0 * np.sin((phi1 - phi2) / 2.0) * b1
+    cI = 1j
+    with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
+        far = (np.abs(k * r2) > 0.1) | (np.abs(k * r1) > 0.1)
+        ea1, ea2 = np.exp(-cI * k * r1 * a1), np.exp(-cI * k * r2 * a1)
+        ec1, ec2 = np.exp(-cI * k * r1 * c1), np.exp(-cI * k * r2 * c1)
+        J1f = (-1.0 / (k ** 2 * b1)) * ((ea2 - ea1) / a1 - (ec2 - ec1) / c1)
+        J2f = (-1.0 / (cI * k ** 3 * b1)) * ((1.0 + cI * k * a1 * r2) * ea2 / a1 ** 2 - (1.0 + cI * k * c1 * r2) * ec2 / c1 ** 2
+                                             - (1.0 + cI * k * a1 * r1) * ea1 / a1 ** 2 + (1.0 + cI * k * c1 * r1) * ec1 / c1 ** 2)
+        J1s = ((r2 ** 2 - r1 ** 2) * (a1 - c1) / (2.0 * b1) - (cI * (r2 ** 3 - r1 ** 3) * (a1 ** 2 - c1 ** 2) / (6.0 * b1)) * k
+               - ((r2 ** 4 - r1 ** 4) * (a1 ** 3 - c1 ** 3) / (24.0 * b1)) * k ** 2
+               + (cI * (r2 ** 5 - r1 ** 5) * (a1 ** 4 - c1 ** 4) / (120.0 * b1)) * k ** 3
+               + ((r2 ** 6 - r1 ** 6) * (a1 ** 5 - c1 ** 5) / (720.0 * b1)) * k ** 4
+               - (cI * (r2 ** 7 - r1 ** 7) * (a1 ** 6 - c1 ** 6) / (5040.0 * b1)) * k ** 5
+               - ((r2 ** 8 - r1 ** 8) * (a1 ** 7 - c1 ** 7) / (40320.0 * b1)) * k ** 6)
+        J2s = ((r2 ** 3 - r1 ** 3) * (a1 - c1) / (3.0 * b1) - (cI * (r2 ** 4 - r1 ** 4) * (a1 ** 2 - c1 ** 2) / (8.0 * b1)) * k
+               - ((r2 ** 5 - r1 ** 5) * (a1 ** 3 - c1 ** 3) / (30.0 * b1)) * k ** 2
+               + (cI * (r2 ** 6 - r1 ** 6) * (a1 ** 4 - c1 ** 4) / (144.0 * b1)) * k ** 3
+               + ((r2 ** 7 - r1 ** 7) * (a1 ** 5 - c1 ** 5) / (840.0 * b1)) * k ** 4
+               - (cI * (r2 ** 8 - r1 ** 8) * (a1 ** 6 - c1 ** 6) / (5760.0 * b1)) * k ** 5
+               - ((r2 ** 9 - r1 ** 9) * (a1 ** 7 - c1 ** 7) / (45360.0 * b1)) * k ** 6)
+        J1 = np.where(far, J1f, J1s)
+        J2 = np.where(far, J2f, J2s)
+        dr = r2 - r1
+        cV = t1 * ((1.0 + r1 / dr) * J1 - J2 / dr) + t2 * (J2 - r1 * J1) / dr
+        K1 = (r2 ** 2 - r1 ** 2) * (a1 - c1) / (2.0 * b1)
+        K2 = (r2 ** 3 - r1 ** 3) * (a1 - c1) / (3.0 * b1)
+        F = -(n1 * ((1.0 + r1 / dr) * K1 - K2 / dr)) - n2 * (K2 - r1 * K1) / dr
+    keep = np.broadcast_to(r1 != r2, cV.shape)
+    return np.sum(np.where(keep, cV, 0.0)), np.sum(np.where(keep, F, 0.0))
+
+
+def visibility(R, rphi, b, theta_b, lam0, distance_cm, diam=-1.0, pa=0.0, vis_norm_fov=True):
+    """Visibility amplitude and phase of the ray image at one baseline
+    (Visibility.f:1-163): R the image radii [AU], rphi (nr, nphi) their
+    intensities, b the baseline [m], theta_b its angle [rad], lam0
+    [micron], the distance [cm], diam the telescope diameter [m] (a
+    Gaussian taper of 0.42 lam/D when positive), pa the position angle
+    [deg].  The image is linear in r between image radii and constant over
+    each angle column, mirrored to -phi; the integrals are the reference's
+    closed forms (its series below k r = 0.1), evaluated in complex128
+    where the reference uses quad-precision complex, and summed with NumPy
+    rather than in the reference's loop order.  Returns (V, phase)."""
+    R = np.asarray(R, float)
+    rphi = np.asarray(rphi, float)
+    nphi = rphi.shape[1]
+    dpc = distance_cm / PARSEC
+    if abs(theta_b) < math.pi / 360.0:
+        theta = math.pi / 2.0 - math.pi / 360.0 + pa * math.pi / 180.0
+    else:
+        theta = math.pi / 2.0 - theta_b + pa * math.pi / 180.0
+    k = 2.0 * math.pi * b / (lam0 * dpc)
+    k = k * 1e6 * math.pi / (180.0 * 3600.0)
+    if diam > 0.0:
+        Rsigma = float(np.float32(0.42)) * lam0 * 1e-6 / diam * 180.0 / math.pi * 3600.0 * dpc
+    else:
+        Rsigma = 1e200
+    phi_c = image_phi(nphi)
+    cV1, F1 = _vis_half(R, rphi, phi_c, nphi, theta, k, Rsigma, vis_norm_fov, 1.0)
+    cV2, F2 = _vis_half(R, rphi, phi_c, nphi, theta, k, Rsigma, vis_norm_fov, -1.0)
+    z = (cV1 + cV2) / (F1 + F2)
+    return float(abs(z)), float(math.atan2(z.imag, z.real))
+
+
+def write_visibility(outdir, angle_deg, lam_obs, spec_jy, b, theta_deg, V, phase, flag=""):
+    """visibility<angle><flag>.dat (Telescope.f:214-240): the header naming
+    the columns, then per wavelength the wavelength, the flux [Jy], the
+    visibilities of each baseline and their phases.  Returns the path."""
+    os.makedirs(outdir, exist_ok=True)
+    tens = int(angle_deg / 10.0)
+    path = os.path.join(outdir, "visibility%d%3.1f%s.dat" % (tens, angle_deg - 10.0 * tens, flag))
+    nb = len(b)
+    with open(path, "w") as f:
+        f.write("# column   1: wavelength\n# column   2: full disk\n")
+        for kk in range(nb):
+            f.write("# column %3d and %3d: vis and phase for: baseline %10.3f, angle %10.3f\n"
+                    % (kk + 3, kk + 3 + nb, b[kk], theta_deg[kk]))
+        for j, l0 in enumerate(lam_obs):
+            f.write("".join(_num(x) for x in [l0, spec_jy[j]] + list(V[j]) + list(phase[j])) + "\n")
     return path

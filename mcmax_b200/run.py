@@ -110,6 +110,29 @@ def observe_ifu(ctx, m, T, ob, outdir, rfix=(), seed=42, posangle=0.0):
     return files
 
 
+def observe_visibility(ctx, m, T, ob, outdir, rfix=(), seed=42, posangle=0.0, vis_norm_fov=True):
+    """A VISIBILITY observation (Telescope.f:200-245): the image rays placed
+    at 0.55 micron, then per wavelength (as a SPECTRUM's) the flux and, per
+    baseline, the visibility and phase of the ray image (outputs.visibility;
+    the rays come from mcg_trace_image with a one-pixel image).  Writes
+    visibility<angle>.dat; returns its path."""
+    from .outputs import PARSEC
+    angle = (math.pi * ob["inc"]) / 180.0
+    dcm = m.distance * PARSEC
+    lam_obs = outputs.spectrum_wavelengths(m.lam, ob["lam1"], ob["lam2"], ob["nlam"], ob["lamfile"] or None)
+    b, th = list(ob["b"]), list(ob["theta"])
+    spec, V, ph = [], [], []
+    for n, lam0 in enumerate(lam_obs):
+        r = ctx.trace_image(T, lam0, angle, npixel=1, nint=1, nphi=ob["nphi"], nr=ob["nrad"], Rfix=rfix,
+                            seed=seed + n, lam_path=0.55)
+        spec.append(1e23 * r["flux"] / dcm ** 2)
+        vp = [outputs.visibility(r["R"], r["rphi"], bk, math.pi * tk / 180.0, lam0, dcm, ob["d"], posangle,
+                                 vis_norm_fov) for bk, tk in zip(b, th)]
+        V.append([x[0] for x in vp])
+        ph.append([x[1] for x in vp])
+    return outputs.write_visibility(outdir, ob["inc"], lam_obs, spec, b, th, V, ph, ob["flag"])
+
+
 def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opacity="dhs", compute_parts=None,
              spectra=(), spectrum_nphi=45, spectrum_nr=2, observations=()):
     """Build the deck's model, run the packet loop and the diffusion step
@@ -161,7 +184,8 @@ def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opac
     skipped, images = [], []
     for path in observations:
         for ob in outputs.read_observations(path, m.lam, run.get("incangle", 45.0), rout=m.R[-1]):
-            {"SPECTRUM": todo, "IMAGE": images, "IFU": images}.get(ob["kind"], skipped).append(ob)
+            {"SPECTRUM": todo, "IMAGE": images, "IFU": images, "VISIBILITY": images}.get(ob["kind"],
+                                                                                        skipped).append(ob)
     rfix = fixed_radii(run["zones"], m.R[1], m.R[-1])
     for ob in todo:
         lam_obs = outputs.spectrum_wavelengths(m.lam, ob["lam1"], ob["lam2"], ob["nlam"], ob["lamfile"] or None)
@@ -169,6 +193,11 @@ def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opac
         files.append(outputs.write_spectrum(outdir, ob["inc"], lam_obs, flux, m.lam, m.Fstar, m.distance,
                                             flag=ob["flag"], polarised=int(m.scat_how) == 2))
     for ob in images:
+        if ob["kind"] == "VISIBILITY":
+            files.append(observe_visibility(ctx, m, T, ob, outdir, rfix, seed=run["seed"],
+                                            posangle=run.get("posangle", 0.0),
+                                            vis_norm_fov=run.get("vis_norm_fov", True)))
+            continue
         observe = observe_ifu if ob["kind"] == "IFU" else observe_image
         files += observe(ctx, m, T, ob, outdir, rfix, seed=run["seed"], posangle=run.get("posangle", 0.0))
     return dict(model=m, run=run, nphot=n, result=res, T=T, diffused=diffused, structure=structure, files=files,

@@ -131,3 +131,22 @@ def test_rimage_profile(tmp_path):
     assert rows[3, 1] == rows[2, 1]
     scaling = 1e23 / d ** 2 * 10.0 ** 2 * AU ** 2 / 100 ** 2
     assert np.allclose(rows[:, 2], scaling * rphi[:, 2], rtol=1e-12)
+
+
+def test_visibility_of_a_uniform_disk():
+    """a face-on disk of constant intensity out to R: V = |2 J1(x) / x|,
+    x = k R with k = 2 pi b / lambda in rad per AU at the distance; V = 1
+    at zero baseline"""
+    from scipy.special import j1
+    R = np.linspace(0.0, 10.0, 201)
+    rphi = np.ones((R.size, 45))
+    d = 140.0 * OUT.PARSEC
+    for b in (0.0, 20.0, 60.0, 120.0):
+        V, ph = OUT.visibility(R, rphi, b, 0.3, 2.0, d)
+        k = 2.0 * math.pi * b / (2.0 * 140.0) * 1e6 * math.pi / (180.0 * 3600.0)
+        x = k * 10.0
+        want = 1.0 if b == 0.0 else abs(2.0 * j1(x) / x)
+        assert abs(V - want) < 2e-3, (b, V, want)
+    # a telescope taper (diameter d) only lowers the long-baseline response
+    V1, _ = OUT.visibility(R, rphi, 60.0, 0.3, 2.0, d, diam=8.0)
+    assert 0.0 <= V1 <= 1.0 + 1e-12

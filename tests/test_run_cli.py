@@ -137,7 +137,7 @@ def test_observation_files_drive_spectra(tmp_path):
     (tmp_path / "Spectrum.out").write_text("nphi=30\nnrad=1\n*****\ntype='SPECTRUM'\ninc=60\nflag='_a'\n"
                                            "type='IMAGE'\nlam=0.6\nnpix=16\nnint=3\n"
                                            "type='SPECTRUM'\nlam1=1\nlam2=100\nnlam=5\n"
-                                           "type='VISIBILITY'\n")
+                                           "type='LINE'\n")
     made = []
 
     def factory(device):
@@ -147,7 +147,7 @@ def test_observation_files_drive_spectra(tmp_path):
     r = R.main([deck, "1e3", str(tmp_path / "Spectrum.out"), "-o", str(tmp_path / "o")], context=factory)
     names = [os.path.basename(f) for f in r["files"] if "spectrum" in f]
     assert names == ["spectrum60.0_a.dat", "spectrum45.0.dat"]
-    assert r["skipped"] == ["VISIBILITY"]
+    assert r["skipped"] == ["LINE"]
     images = [os.path.basename(f) for f in r["files"] if "Image" in f]
     assert images == ["RImage_i45.0_l00000.60.dat", "ImageAI_i45.0_l00000.60_fov00100.0.fits"]
     a = made[0].image_args
@@ -204,3 +204,24 @@ def test_ifu_observation_writes_one_image_per_wavelength(tmp_path):
     assert [c["lam0"] for c in calls] == [1.0, 10.0, 100.0]
     assert all(c["lam_path"] == 0.55 and c["Rmax"] == 20.0 and c["npixel"] == 8 for c in calls)
     assert len({c["seed"] for c in calls}) == 3
+
+
+def test_visibility_observation(tmp_path):
+    deck = _write_inputs(tmp_path)
+    (tmp_path / "vis.out").write_text("type='VISIBILITY'\nlam1=1\nlam2=100\nnlam=3\nbase1=50\nbase2=200\n"
+                                      "angle2=30\n")
+    made = []
+
+    def factory(device):
+        made.append(FakeContext(device))
+        return made[-1]
+
+    r = R.main([deck, "1e3", str(tmp_path / "vis.out"), "-o", str(tmp_path / "o")], context=factory)
+    path = [f for f in r["files"] if os.path.basename(f).startswith("visibility")]
+    assert [os.path.basename(p) for p in path] == ["visibility45.0.dat"]
+    rows = np.loadtxt(path[0])
+    assert rows.shape == (3, 2 + 2 + 2)
+    assert np.all((rows[:, 2:4] >= 0.0) & (rows[:, 2:4] <= 1.0 + 1e-12))
+    head = open(path[0]).read().splitlines()[:4]
+    assert head[3].startswith("# column   4 and   6: vis and phase for: baseline    200.000, angle     30.000")
+    assert all(c["lam_path"] == 0.55 and c["npixel"] == 1 for c in made[0].image_calls)
