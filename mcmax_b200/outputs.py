@@ -277,17 +277,26 @@ def read_observations(path, lam, incangle=45.0, rout=None):
             if key == "type":
                 cur = dict(default, kind=val.upper(), fov=list(default["fov"]), b=list(default["b"]),
                            theta=list(default["theta"]))
-                if cur["kind"] == "IMAGE":
+                if cur["kind"] in ("IMAGE", "BASEVIS"):
                     cur["lam1"] = deflam
                 obs.append(cur)
                 continue
             if key in ("nphi", "nrad", "nlam", "npix", "nint", "scaletype"):
                 cur[key] = int(num(val))
+            elif cur is not default and cur["kind"] == "BASEVIS" and key[:3] == "lam" and key[3:].isdigit():
+                # lamN: the wavelengths of a BASEVIS observation (Telescope.f:1129-1133)
+                i = int(key[3:])
+                lams = cur.setdefault("lams", [])
+                while len(lams) < i:
+                    lams.append(0.0)
+                lams[i - 1] = num(val)
+                if i == 1:
+                    cur["lam1"] = lams[0]
             elif key == "lam" and cur is default:
                 deflam = num(val)
             elif key in ("inc", "lam1", "lam2", "lam"):
                 cur["lam1" if key == "lam" else key] = num(val)
-            elif cur is not default and cur["kind"] == "VISIBILITY" and (
+            elif cur is not default and cur["kind"] in ("VISIBILITY", "BASEVIS") and (
                     (key[:4] == "base" and key[4:].isdigit()) or (key[:5] == "angle" and key[5:].isdigit())):
                 # baseN [m] and angleN [deg] of the baselines (Telescope.f:1067-1127)
                 i = int(key[4:] if key[:4] == "base" else key[5:])
@@ -601,4 +610,23 @@ def write_visibility(outdir, angle_deg, lam_obs, spec_jy, b, theta_deg, V, phase
                     % (kk + 3, kk + 3 + nb, b[kk], theta_deg[kk]))
         for j, l0 in enumerate(lam_obs):
             f.write("".join(_num(x) for x in [l0, spec_jy[j]] + list(V[j]) + list(phase[j])) + "\n")
+    return path
+
+
+def write_basevis(outdir, angle_deg, base, lams, theta_deg, flux_jy, V, phase, flag=""):
+    """basevis<angle><flag>.dat (Telescope.f:246-291): the header naming the
+    columns, then per baseline [m] the flux of the last wavelength [Jy] and
+    the visibilities and phases at each wavelength.  Returns the path."""
+    os.makedirs(outdir, exist_ok=True)
+    tens = int(angle_deg / 10.0)
+    path = os.path.join(outdir, "basevis%d%3.1f%s.dat" % (tens, angle_deg - 10.0 * tens, flag))
+    nl = len(lams)
+    with open(path, "w") as f:
+        f.write("# column   1: baseline\n# column   2: full disk (only last wavelength)\n")
+        for j in range(nl):
+            f.write("# column %3d and %3d: vis and phase for wavelength %10.3f, angle %10.3f\n"
+                    % (j + 3, j + 3 + nl, lams[j], theta_deg[j]))
+        for k, b in enumerate(base):
+            f.write("".join(_num(x) for x in [b, flux_jy] + [V[j][k] for j in range(nl)]
+                            + [phase[j][k] for j in range(nl)]) + "\n")
     return path

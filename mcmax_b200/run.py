@@ -133,6 +133,33 @@ def observe_visibility(ctx, m, T, ob, outdir, rfix=(), seed=42, posangle=0.0, vi
     return outputs.write_visibility(outdir, ob["inc"], lam_obs, spec, b, th, V, ph, ob["flag"])
 
 
+def observe_basevis(ctx, m, T, ob, outdir, rfix=(), seed=42, posangle=0.0, vis_norm_fov=True):
+    """A BASEVIS observation (Telescope.f:246-291): the image rays placed at
+    lam1, then for each wavelength lamN (traced again only when it differs
+    from the one before) the visibility and phase on 100 baselines from
+    base1 to base2, at the baseline angle angleN of that wavelength.
+    Writes basevis<angle>.dat; returns its path."""
+    from .outputs import PARSEC
+    angle = (math.pi * ob["inc"]) / 180.0
+    dcm = m.distance * PARSEC
+    lams = list(ob.get("lams") or [ob["lam1"]])
+    b = list(ob["b"]) + [0.0] * max(0, 2 - len(ob["b"]))
+    th = list(ob["theta"]) + [0.0] * max(0, len(lams) - len(ob["theta"]))
+    base = [b[0] + (b[1] - b[0]) * ((k - 1.0) / 99.0) for k in range(1, 101)]
+    V, ph = [], []
+    r = None
+    for j, lam0 in enumerate(lams):
+        if j == 0 or lam0 != lams[j - 1]:
+            r = ctx.trace_image(T, lam0, angle, npixel=1, nint=1, nphi=ob["nphi"], nr=ob["nrad"], Rfix=rfix,
+                                seed=seed + j, lam_path=ob["lam1"])
+        vp = [outputs.visibility(r["R"], r["rphi"], bk, math.pi * th[j] / 180.0, lam0, dcm, ob["d"], posangle,
+                                 vis_norm_fov) for bk in base]
+        V.append([x[0] for x in vp])
+        ph.append([x[1] for x in vp])
+    return outputs.write_basevis(outdir, ob["inc"], base, lams, th[:len(lams)], 1e23 * r["flux"] / dcm ** 2, V, ph,
+                                 ob["flag"])
+
+
 def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opacity="dhs", compute_parts=None,
              spectra=(), spectrum_nphi=45, spectrum_nr=2, observations=()):
     """Build the deck's model, run the packet loop and the diffusion step
@@ -184,8 +211,8 @@ def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opac
     skipped, images = [], []
     for path in observations:
         for ob in outputs.read_observations(path, m.lam, run.get("incangle", 45.0), rout=m.R[-1]):
-            {"SPECTRUM": todo, "IMAGE": images, "IFU": images, "VISIBILITY": images}.get(ob["kind"],
-                                                                                        skipped).append(ob)
+            {"SPECTRUM": todo, "IMAGE": images, "IFU": images, "VISIBILITY": images,
+             "BASEVIS": images}.get(ob["kind"], skipped).append(ob)
     rfix = fixed_radii(run["zones"], m.R[1], m.R[-1])
     for ob in todo:
         lam_obs = outputs.spectrum_wavelengths(m.lam, ob["lam1"], ob["lam2"], ob["nlam"], ob["lamfile"] or None)
@@ -193,6 +220,11 @@ def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opac
         files.append(outputs.write_spectrum(outdir, ob["inc"], lam_obs, flux, m.lam, m.Fstar, m.distance,
                                             flag=ob["flag"], polarised=int(m.scat_how) == 2))
     for ob in images:
+        if ob["kind"] == "BASEVIS":
+            files.append(observe_basevis(ctx, m, T, ob, outdir, rfix, seed=run["seed"],
+                                         posangle=run.get("posangle", 0.0),
+                                         vis_norm_fov=run.get("vis_norm_fov", True)))
+            continue
         if ob["kind"] == "VISIBILITY":
             files.append(observe_visibility(ctx, m, T, ob, outdir, rfix, seed=run["seed"],
                                             posangle=run.get("posangle", 0.0),

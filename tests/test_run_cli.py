@@ -225,3 +225,25 @@ def test_visibility_observation(tmp_path):
     head = open(path[0]).read().splitlines()[:4]
     assert head[3].startswith("# column   4 and   6: vis and phase for: baseline    200.000, angle     30.000")
     assert all(c["lam_path"] == 0.55 and c["npixel"] == 1 for c in made[0].image_calls)
+
+
+def test_basevis_observation(tmp_path):
+    deck = _write_inputs(tmp_path)
+    (tmp_path / "bv.out").write_text("type='BASEVIS'\nlam1=2\nlam2=2\nlam3=10\nbase1=10\nbase2=110\nangle3=45\n")
+    made = []
+
+    def factory(device):
+        made.append(FakeContext(device))
+        return made[-1]
+
+    r = R.main([deck, "1e3", str(tmp_path / "bv.out"), "-o", str(tmp_path / "o")], context=factory)
+    path = [f for f in r["files"] if os.path.basename(f).startswith("basevis")]
+    assert [os.path.basename(p) for p in path] == ["basevis45.0.dat"]
+    rows = np.loadtxt(path[0])
+    assert rows.shape == (100, 2 + 3 + 3)
+    assert rows[0, 0] == 10.0 and rows[-1, 0] == 110.0
+    # the same wavelength twice is traced once
+    calls = made[0].image_calls
+    assert [c["lam0"] for c in calls] == [2.0, 10.0] and all(c["lam_path"] == 2.0 for c in calls)
+    head = open(path[0]).read().splitlines()
+    assert head[4].startswith("# column   5 and   8: vis and phase for wavelength     10.000, angle     45.000")
