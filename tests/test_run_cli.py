@@ -247,3 +247,25 @@ def test_basevis_observation(tmp_path):
     assert [c["lam0"] for c in calls] == [2.0, 10.0] and all(c["lam_path"] == 2.0 for c in calls)
     head = open(path[0]).read().splitlines()
     assert head[4].startswith("# column   5 and   8: vis and phase for wavelength     10.000, angle     45.000")
+
+
+def test_image_in_arcsec(tmp_path):
+    """scaletype 2: the field of view in arcsec becomes AU at the distance
+    (100 pc), the header counts arcsec and the image is in mJy/arcsec^2"""
+    deck = _write_inputs(tmp_path)
+    (tmp_path / "im.out").write_text("type='IMAGE'\nlam=1\nnpix=10\nnint=2\nfov=0.4\nscaletype=2\n")
+    made = []
+
+    def factory(device):
+        made.append(FakeContext(device))
+        return made[-1]
+
+    r = R.main([deck, "1e3", str(tmp_path / "im.out"), "-o", str(tmp_path / "o")], context=factory)
+    a = made[0].image_args
+    assert abs(a["Rmax"] - 0.4 * 100.0 / 2.0) < 1e-9
+    fits = [f for f in r["files"] if os.path.basename(f).startswith("ImageAI")]
+    hdr, im = outputs.read_image_fits(fits[0])
+    assert hdr["CTYPE1"].strip() == "X [arcsec]" and abs(hdr["CDELT1"] - 0.4 / 10) < 1e-12
+    d = 100.0 * outputs.PARSEC
+    zscale = 1e3 * (10 / 0.4) ** 2
+    assert np.allclose(im, 2.0 * 1e23 * zscale / d ** 2, rtol=1e-12)
