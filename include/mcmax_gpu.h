@@ -130,9 +130,11 @@ mcg_status mcg_compute_part_batch(mcg_ctx *ctx, int nparts, const mcg_part_in *i
  * process exits.  A bin is processed in chunks of wavelengths that fit the
  * array; a bin whose single wavelength needs more (many sizes times filling
  * fractions, or very large size parameters) is rejected with MCG_ERR_LIMIT
- * and a message giving the bytes it would need.  The first call on each
- * device looks up the array's device address (cudaGetSymbolAddress); make
- * that first call before any stream capture.  Every call shares the one
+ * and a message giving the bytes it would need.  Every call looks up the
+ * array's device address on the context's device (cudaGetSymbolAddress),
+ * so the call stays valid after a device reset; the first lookup on a
+ * device loads the library's device code, so make the first call on each
+ * device before any stream capture.  Every call shares the one
  * array: calls that overlap on the same GPU (two contexts used from two
  * host threads at once) race and must be serialised by the caller; the call
  * returns only after its own work has finished. */

@@ -27,7 +27,6 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
-#include <mutex>
 #include <vector>
 
 #include "dhs_core.cuh"
@@ -720,24 +719,20 @@ static __device__ __align__(256) unsigned char mcg_static_arena[MCG_STATIC_ARENA
 namespace {
 
 constexpr size_t kArenaBytes = (size_t)MCG_STATIC_ARENA_BYTES;
-constexpr int kArenaMaxDevices = 64;
 
-std::mutex g_arena_mutex;
-void *g_arena_dev_ptr[kArenaMaxDevices] = {};
-
-/* Device address of the array on `dev` (the current device).  In host code
- * the symbol mcg_static_arena only names a host-side shadow; the kernels
- * need the address the runtime reports for the device. */
-cudaError_t arena_address(int dev, unsigned char **out) {
-  std::lock_guard<std::mutex> lock(g_arena_mutex);
-  if (dev < 0 || dev >= kArenaMaxDevices) return cudaErrorInvalidDevice;
-  if (!g_arena_dev_ptr[dev]) {
-    void *p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, mcg_static_arena);
-    if (e != cudaSuccess) return e;
-    g_arena_dev_ptr[dev] = p;
-  }
-  *out = (unsigned char *)g_arena_dev_ptr[dev];
+/* Device address of the array on the current device.  In host code the
+ * symbol mcg_static_arena only names a host-side shadow; the kernels need
+ * the address the runtime reports for the device.  It is looked up on every
+ * call (a cheap runtime query) rather than cached for the process: after a
+ * cudaDeviceReset, or when the primary context is released and created
+ * again, the module is loaded anew and the array may sit at another
+ * address.  The first lookup on a device loads the module, which is why the
+ * first call on a device belongs before any stream capture. */
+cudaError_t arena_address(unsigned char **out) {
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, mcg_static_arena);
+  if (e != cudaSuccess) return e;
+  *out = (unsigned char *)p;
   return cudaSuccess;
 }
 
@@ -839,7 +834,7 @@ mcg_status mcg_part_static_impl(mcg_ctx *ctx, const mcg_part_in *in, mcg_part_ou
   if (nw < 4) nw = 4;
 
   unsigned char *arena = nullptr;
-  cudaError_t ce = arena_address(ctx->device, &arena);
+  cudaError_t ce = arena_address(&arena);
   if (ce != cudaSuccess)
     return mcg_fail(ctx, MCG_ERR_CUDA, "compute_part_static: cudaGetSymbolAddress failed: %s",
                     cudaGetErrorString(ce));

@@ -1060,7 +1060,22 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
             R, Theta, path_of(v("densfile", "", str)), path_of(gfile) if gfile else None, v("gas2dust", 100.0),
             v("mdust", 1e-15) * MSUN if "mdust" in d else None)
     elif denstype in ANALYTIC_DENSITIES + THIN_START_DENSITIES:
-        R, Theta, thet, SinTheta = spatial_grid(rstar_cm, rin, rout, nrad, ntheta)
+        meixrin = v("meixrin", -1.0) if v("meixrin", -1.0) > 0.0 else rin
+        meixd, meixe = v("meixd", 1.0), v("meixe", 3.0)
+        if meixd <= 0.0:     # Init.f:1529-1530, in this order
+            meixd = meixe
+        if meixe <= 0.0:
+            meixe = meixd
+        timeshift = v("timeshift", 0.0)
+        rin_g, rout_g = rin, rout
+        if denstype == "MEIXNER" and timeshift != 0.0:
+            # the shell has expanded for timeshift years at vexp1 km/s: the
+            # grid's edges move out by timeshift vexp1 0.210944839 AU
+            # (Init.f:1634-1636), while the shell's own inner radius stays
+            # at the unshifted rin (MeixRin is set before, Init.f:1528)
+            shift = timeshift * v("vexp1", v("vexp", 10.0)) * 0.210944839
+            rin_g, rout_g = rin + shift, rout + shift
+        R, Theta, thet, SinTheta = spatial_grid(rstar_cm, rin_g, rout_g, nrad, ntheta)
         kext = [r["kext"] if "kext" in r else np.asarray(r["kabs"]) + np.asarray(r["ksca"]) for r in res]
         dens, V = analytic_density(denstype, R, Theta, thet, dict(
             rin=rin, rout=rout, denspow=v("denspow", 1.0), shpow=v("shpow", 1.3), sh1au=v("sh1au", 0.03),
@@ -1072,9 +1087,9 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
             vexp1=v("vexp1", v("vexp", 10.0)) * 100000.0,
             vexp2=(v("vexp2", -10.0) if v("vexp2", -10.0) > 0.0 else v("vexp1", v("vexp", 10.0))) * 100000.0,
             bexp=v("bexp", 0.5), gas2dust=v("gas2dust", 100.0), mstar=v("mstar", 2.5) * MSUN, rstar_cm=rstar_cm,
-            meixa=v("meixa", 8.0), meixb=v("meixb", 2.0), meixc=v("meixc", 2.0), meixd=v("meixd", 1.0),
-            meixe=v("meixe", 3.0), meixf=v("meixf", 1.0), meixrsw=v("meixrsw", 1800.0),
-            meixrin=v("meixrin", -1.0) if v("meixrin", -1.0) > 0.0 else rin, timeshift=v("timeshift", 0.0),
+            meixa=v("meixa", 8.0), meixb=v("meixb", 2.0), meixc=v("meixc", 2.0), meixd=meixd,
+            meixe=meixe, meixf=v("meixf", 1.0), meixrsw=v("meixrsw", 1800.0),
+            meixrin=meixrin, timeshift=timeshift,
             mtot=v("mdust", 1e-15) * MSUN, mdustscale="mdust" in d), lam=lam, kext=kext)
     else:
         R, Theta, thet, SinTheta = spatial_grid(rstar_cm, rin, rout, nrad, ntheta)

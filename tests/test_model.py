@@ -526,3 +526,30 @@ def test_meixner_shell(tmp_path):
     assert np.allclose(ratio, ratio[0, 0], rtol=1e-10)
     assert np.all(dens[1:][~sel] < 1e-55)
     assert abs((dens[1:] * V[1:]).sum() / (1e-5 * M.MSUN) - 1) < 1e-12
+
+
+def test_meixner_timeshift_moves_the_grid_and_the_profile(tmp_path):
+    """timeshift t [yr] at vexp1 v [km/s]: the grid's inner and outer radii
+    move out by t v 0.210944839 AU (Init.f:1634-1636), the profile is
+    evaluated at r - t v 0.210944839 AU with the shell's inner radius kept
+    at the unshifted rin (Init.f:1528, 3231); meixd <= 0 takes meixe
+    (Init.f:1529)"""
+    deck, parts = _analytic_deck(tmp_path, "denstype='MEIXNER'\nmdust=1d-5\nmeixd=-1\ntimeshift=100\n"
+                                           "vexp1=15\n")
+    m, _ = M.deck_model(None, deck, compute_parts=parts)
+    shift = 100.0 * 15.0 * 0.210944839
+    R = np.asarray(m.R)
+    assert abs(R[1] / (0.1 + shift) - 1) < 1e-12
+    assert abs(R[-1] / (1000.0 + shift) - 1) < 1e-12
+    dens, V, _, _ = _cells(m)
+    ra = 10.0 ** ((np.log10(R[:-1]) + np.log10(R[1:])) / 2.0)
+    th = np.arccos((m.Theta[:-1] + m.Theta[1:]) / 2.0)
+    rr = (ra[1:] - 100.0 * 15e5 * 0.210944839e-5)[:, None]   # the disk's rings (not the star cell)
+    st, ct = np.sin(th)[None, :], np.cos(th)[None, :]
+    D = E = 3.0
+    f = (rr / 0.1) ** (-2.0 * (1.0 + 2.0 * st * np.exp(-(rr / 1800.0) ** D + (0.1 / 1800.0) ** D)))
+    f = f * (1.0 + 8.0 * (1.0 - ct) * np.exp(-(rr / 1800.0) ** E + (0.1 / 1800.0) ** E)) * (rr / ra[1:, None]) ** 2
+    ratio = dens[1:] / f
+    assert np.all(rr > 0.1)
+    assert np.allclose(ratio, ratio[0, 0], rtol=1e-10)
+    assert abs((dens[1:] * V[1:]).sum() / (1e-5 * M.MSUN) - 1) < 1e-12

@@ -6,8 +6,9 @@ code that cannot afford cudaFree's device-wide wait).
 Called through the C-ABI with ctypes, it must give the same opacity tables,
 bit for bit, as mcg_compute_part on the same bin, on consecutive calls that
 reuse the array: first a bin that fits in one pass, then one that is split
-into several wavelength chunks.  A bin whose single wavelength needs more
-than the array holds is refused before anything runs on the GPU.
+into several wavelength chunks.  Repeated calls must leave the device's free
+memory where it was.  A bin whose single wavelength needs more than the
+array holds is refused before anything runs on the GPU.
 
 The file name sorts last so that a run stopping at the first failure has run
 every other test first."""
@@ -81,6 +82,32 @@ def test_static_matches_allocating_entry_point_on_consecutive_calls(handle):
     ref0 = _call(lib, h, "mcg_compute_part", bins[0])
     for key in ("kabs", "ksca", "kext", "F"):
         assert np.array_equal(ref0[key], again[key]), key
+
+
+def _device_free_bytes():
+    """Free device memory of the current context (cuMemGetInfo of the
+    driver API; the library's calls made its device's primary context
+    current on this thread)."""
+    drv = C.CDLL("libcuda.so.1")
+    free, total = C.c_size_t(), C.c_size_t()
+    assert drv.cuMemGetInfo_v2(C.byref(free), C.byref(total)) == 0
+    return free.value
+
+
+def test_static_calls_leave_device_memory_unchanged(handle):
+    # the premise of the entry point: no device allocation.  A first pass
+    # over both bins loads the kernels and looks up the array's address;
+    # after it, the device's free memory must be the same before and after
+    # further calls (an allocation that is still held, or a cached buffer,
+    # would lower it)
+    lib, h = handle
+    bins = [part_inputs(PART_CASES[0]), _chunked_bin()]
+    for p in bins:
+        assert _call(lib, h, "mcg_compute_part_static", p)["status"] == _ffi.MCG_OK, lib.mcg_last_error(h)
+    before = _device_free_bytes()
+    for p in bins + bins:
+        assert _call(lib, h, "mcg_compute_part_static", p)["status"] == _ffi.MCG_OK, lib.mcg_last_error(h)
+    assert _device_free_bytes() == before
 
 
 def test_static_refuses_a_bin_beyond_the_array(handle):
