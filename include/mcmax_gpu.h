@@ -206,6 +206,18 @@ typedef struct {
                              (1 reproduces the serial packet order) */
   int block;              /* threads per block: 0 = default (256), else a
                              multiple of 32 up to 256 */
+  double maxruntime;      /* keyword 'maxruntime' (Init.f:1094, default -1 =
+                             off), seconds.  > 0: when a packet starts after
+                             more than maxruntime seconds of the run, or once
+                             a tenth of the packets have started and the run
+                             projects to more than 5 maxruntime, with under 90 %
+                             started, the run stops, NphotTot shrinks to
+                             NphotTot (maxruntime / t) (0.5 i / Nphot) (at
+                             least 10; i packets started after t seconds) and
+                             the run starts over with that many packets, as
+                             MCRadiation.f:323-342 does; *nphot_inout returns
+                             the count that ran.  Time is measured on the
+                             device from the kernel's start. */
 } mcg_run;
 
 typedef struct {
@@ -218,13 +230,21 @@ typedef struct {
   /* 0 emissions (nemit), 1 interactions, 2 absorptions, 3 scatterings,
    * 4 random-walk steps, 5 star hits, 6 abandoned traces, 7 overflow
    * kills, 8 cell crossings, 9 escapes, 10 averaged-matrix scatterings,
-   * 11 geometry failures */
+   * 11 geometry failures; FP64/MIXED forms with the warp scheduler:
+   * 12 scheduled warp phases, 13 lanes served by them, 14 warp crossing
+   * steps, 15 lanes that crossed in them (13/12 and 15/14 are the mean
+   * lanes per phase and per crossing step) */
   int64_t counters[MCG_NCOUNTERS];
   double tautot;
   float device_ms;        /* transport kernel time of the call */
   float progress_ms[5];   /* time at which 50, 90, 99, 99.9, 100 % of the
                              packets had finished (the rest is the tail of
                              the heaviest packets) */
+  int32_t *Nabs;          /* ncell: absorption events (Bjorkman-Wood
+                             re-emissions) per cell, summed over the nruns
+                             sub-runs; NULL skips the copy.  Not a reference
+                             output: the count behind the accuracy criterion
+                             "cells with >= 1e3 absorption events". */
 } mcg_result;
 
 /* The packet loop (MCRadiation.f:6-887).  *nphot_inout = NphotTot. */

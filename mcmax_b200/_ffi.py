@@ -85,7 +85,7 @@ class Run(C.Structure):
     _fields_ = [
         ("seed", C.c_uint64), ("randomwalk", C.c_int), ("factRW", C.c_double),
         ("maxinteract", C.c_int64), ("nruns", C.c_int), ("precision", C.c_int),
-        ("threads", C.c_int), ("block", C.c_int),
+        ("threads", C.c_int), ("block", C.c_int), ("maxruntime", C.c_double),
     ]
 
 
@@ -94,7 +94,7 @@ class Result(C.Structure):
         ("EJv", dp), ("EJv2", dp), ("Eabs", dp), ("T", dp), ("Ni", ip),
         ("spec", dp), ("scatspec", dp), ("ispec", ip),
         ("counters", C.c_int64 * NCOUNTERS), ("tautot", C.c_double), ("device_ms", C.c_float),
-        ("progress_ms", C.c_float * 5),
+        ("progress_ms", C.c_float * 5), ("Nabs", ip),
     ]
 
 

@@ -116,12 +116,13 @@ class Context:
         self.model = m
 
     def mcradiation(self, nphot, seed=1, randomwalk=False, factRW=10.0, maxinteract=0, nruns=1,
-                    precision="exact", threads=0, block=0, fetch=True):
-        """Run the packet loop; returns (nphot_out, result dict)."""
+                    precision="exact", threads=0, block=0, fetch=True, maxruntime=-1.0):
+        """Run the packet loop; returns (nphot_out, result dict).  nphot_out
+        is smaller than nphot when maxruntime (seconds, > 0) cut the run."""
         m = self.model
         prec = {"fp64": _ffi.PREC_FP64, "mixed": _ffi.PREC_MIXED, "exact": _ffi.PREC_EXACT}[precision]
         run = _ffi.Run(int(seed), int(bool(randomwalk)), float(factRW), int(maxinteract), int(nruns), prec,
-                       int(threads), int(block))
+                       int(threads), int(block), float(maxruntime))
         out = {}
         res = _ffi.Result()
         if fetch:
@@ -129,7 +130,7 @@ class Context:
             ns = m.nlam * (_ffi.NANGLE_SED + 1)
             out = dict(EJv=np.zeros(nc), EJv2=np.zeros(nc), Eabs=np.zeros(nc), T=np.zeros(nc),
                        Ni=np.zeros(nc, np.int32), spec=np.zeros(ns), scatspec=np.zeros(ns),
-                       ispec=np.zeros(ns, np.int32))
+                       ispec=np.zeros(ns, np.int32), Nabs=np.zeros(nc, np.int32))
             for k, v in out.items():
                 setattr(res, k, _ffi.ptr(v))
         n = C.c_int64(int(nphot))

@@ -29,7 +29,7 @@ UNITS = {
     "raytrace.cu": ["--fmad=false"],
 }
 HEADERS = ["detmath.h", "cplx.h", "philox.h", "dhs_core.cuh", "transport_core.cuh", "transport_fast.cuh",
-           "mcg_internal.h", "tc_sm100.cuh", "diffuse_core.cuh",
+           "mcg_internal.h", "tc_sm100.cuh", "diffuse_core.cuh", "transport_event.cuh",
            "dstruct_core.cuh", "rt_core.cuh"]
 
 

@@ -103,6 +103,9 @@ struct DevRun {
   /* nruns accumulation */
   double *EJvTot = nullptr, *EJv2Tot = nullptr;
   int *kp_hint = nullptr;
+  /* absorption events per cell (nruns*ncell) and their sum over runs */
+  int *Nabs = nullptr, *NabsTot = nullptr;
+  unsigned long long *stop = nullptr; /* maxruntime record, 2 entries */
   std::vector<void *> owned;
 };
 

@@ -170,9 +170,11 @@ __global__ void __launch_bounds__(128) transport_fp64_kernel(const __grid_consta
 #pragma unroll
   for (int k = 0; k < TC_N; ++k) L.cnt[k] = 0u;
   L.tautot = 0.0;
+  const unsigned long long t0 = tp_globaltimer();
   for (;;) {
     unsigned long long pid = atomicAdd(A.next, 1ULL);
     if (pid >= (unsigned long long)m.nphot) break;
+    if (tp_runtime_stop(A, m.maxruntime, m.nphot, pid, t0)) break;
     tp_run_packet(m, A, (int64_t)pid + m.pid0, L);
     tp_packet_done(A);
   }
@@ -431,25 +433,36 @@ mcg_status mcg_set_model_impl(mcg_ctx *ctx, const mcg_grid *g, const mcg_opacity
   return MCG_OK;
 }
 
-/* per thick cell: factRW / (AU * max_iT KDext * dens), the bound below which
- * no random-walk jump can be taken at any temperature (one warp per row) */
-__global__ void rw_dmin_kernel(int nrows, const int *cells, const double *KDext, const double *dens, double factRW,
-                               double *rw_dmin) {
+/* largest KDext over iT of each diffusion-table row (one warp per row) */
+__global__ void kd_max_kernel(int nrows, const double *KDext, double *kmax_row) {
   const int lane = threadIdx.x & 31;
   const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (r >= nrows) return;
   double kmax = 0.0;
   for (int iT = 1 + lane; iT <= TP_TMAX - 1; iT += 32) kmax = fmax(kmax, KDext[(size_t)r * TP_TT + iT]);
   for (int s = 16; s > 0; s >>= 1) kmax = fmax(kmax, __shfl_down_sync(0xffffffffu, kmax, s));
-  if (lane == 0) {
-    const int c = cells[r];
-    const double lr = 1.0 / ((TP_AU * kmax) * dens[c]);
-    rw_dmin[c] = kmax > 0.0 ? factRW * lr : 1e300;
-  }
+  if (lane == 0) kmax_row[r] = kmax;
+}
+
+/* per thick cell: factRW / (AU * max_iT KDext * dens), the bound below which
+ * no random-walk jump can be taken at any temperature */
+__global__ void rw_dmin_kernel(int ncell, const int *kd_index, const double *kmax_row, const double *dens,
+                               double factRW, double *rw_dmin) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  const int r = kd_index[c];
+  if (r < 0) return;
+  const double kmax = kmax_row[r];
+  const double lr = 1.0 / ((TP_AU * kmax) * dens[c]);
+  rw_dmin[c] = kmax > 0.0 ? factRW * lr : 1e300;
 }
 
 /* thick flags (InitRandomWalk, RandomWalk.f:172-190) and the diffusion
- * tables of the thick cells for all iT */
+ * tables of the thick cells for all iT.  DiffCoeffCell (Dtable.f:97-182)
+ * depends on the cell only through its grain mixture (KabsTot, KscaTot and
+ * the mean asymmetry), so cells with the same mixture share one row: a
+ * uniform mixture needs a single row, which is what lets models with many
+ * thick cells (massive disks of a parameter sweep) keep the random walk. */
 static mcg_status build_rw_tables(mcg_ctx *ctx, double factRW) {
   DevModel &m = ctx->model;
   if (m.kd_factRW == factRW) return MCG_OK;
@@ -487,8 +500,12 @@ static mcg_status build_rw_tables(mcg_ctx *ctx, double factRW) {
       if ((R[i + 1] - R[i]) > factRW * lr) thick[c] = 1;
     }
     if (thick[c]) {
-      idx[c] = (int)rows.size();
-      rows.push_back(c);
+      if (m.uniform_mix && !rows.empty()) {
+        idx[c] = 0; /* the same mixture: the same row, bit for bit */
+      } else {
+        idx[c] = (int)rows.size();
+        rows.push_back(c);
+      }
     }
   }
   /* full tables for the thick cells */
@@ -530,8 +547,13 @@ static mcg_status build_rw_tables(mcg_ctx *ctx, double factRW) {
     MCG_CUDA(ctx, cudaMemcpyAsync(m.rw_dmin, lim.data(), sizeof(double) * ncell, cudaMemcpyHostToDevice, st));
     MCG_CUDA(ctx, cudaStreamSynchronize(st));
   }
-  if (nrows > 0)
-    rw_dmin_kernel<<<nblk((long long)nrows * 32, B), B, 0, st>>>(nrows, cells, m.KDext, m.dens, factRW, m.rw_dmin);
+  if (nrows > 0) {
+    /* the row maxima go into the 4-temperature buffer (no longer needed;
+     * ncell*4 >= nrows entries) */
+    double *kmax_row = kd4a;
+    kd_max_kernel<<<nblk((long long)nrows * 32, B), B, 0, st>>>(nrows, m.KDext, kmax_row);
+    rw_dmin_kernel<<<nblk(ncell, B), B, 0, st>>>(ncell, m.kd_index, kmax_row, m.dens, factRW, m.rw_dmin);
+  }
   MCG_CUDA(ctx, cudaGetLastError());
   MCG_CUDA(ctx, cudaStreamSynchronize(st));
   cudaFree(den);
@@ -566,6 +588,9 @@ static mcg_status ensure_run_buffers(mcg_ctx *ctx, int nruns) {
   r.Ni = (int *)A(nb * 4);
   r.lastphot = (int *)A(nb * 4);
   r.kp_hint = (int *)A(nb * 4);
+  r.Nabs = (int *)A(nb * 4);
+  r.NabsTot = (int *)A(nc * 4);
+  r.stop = (unsigned long long *)A(2 * 8);
   r.EJvTot = (double *)A(nc * 8);
   r.EJv2Tot = (double *)A(nc * 8);
   r.NiTot = (int *)A(nc * 4);
@@ -586,19 +611,22 @@ static mcg_status ensure_run_buffers(mcg_ctx *ctx, int nruns) {
 
 /* run averages in the reference's order: Tot = sum_r (EJv_r / nruns) */
 __global__ static void combine_runs_kernel(int nc, int nruns, const double *EJv, const double *EJv2, const int *Ni,
-                                           double *EJvTot, double *EJv2Tot, int *NiTot) {
+                                           const int *Nabs, double *EJvTot, double *EJv2Tot, int *NiTot,
+                                           int *NabsTot) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
   double a = 0.0, b = 0.0;
-  int n = 0;
+  int n = 0, na = 0;
   for (int r = 0; r < nruns; ++r) {
     a = a + EJv[(size_t)r * nc + c] / (double)nruns;
     b = b + EJv2[(size_t)r * nc + c] / (double)nruns;
     n += Ni[(size_t)r * nc + c];
+    na += Nabs[(size_t)r * nc + c];
   }
   EJvTot[c] = a;
   EJv2Tot[c] = b;
   NiTot[c] = n;
+  NabsTot[c] = na;
 }
 
 /* validation, run buffers and tables, zeroed accumulators and the kernel
@@ -652,6 +680,7 @@ mcg_status mcg_run_prepare(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot, Run
   tm.KDext = m.KDext; tm.KDabs = m.KDabs; tm.rw_y = m.rw_y; tm.rw_phi = m.rw_phi;
   tm.kd_index = m.kd_index; tm.thick = m.thick;
   tm.R0 = m.R0;
+  tm.maxruntime = run->maxruntime;
   TAcc &ta = rp->ta;
   memset(&ta, 0, sizeof ta);
   ta.EJv = R.EJv; ta.EJv2 = R.EJv2; ta.Eabs = R.Eabs; ta.T = R.T; ta.Ni = R.Ni; ta.lastphot = R.lastphot;
@@ -662,6 +691,8 @@ mcg_status mcg_run_prepare(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot, Run
   ta.ncell = m.ncell;
   ta.done = R.done;
   ta.tmark = R.tmark;
+  ta.Nabs = R.Nabs;
+  ta.stop = R.stop;
   {
     const unsigned long long tot = (unsigned long long)(Nphot * nruns);
     const double f[5] = {0.5, 0.9, 0.99, 0.999, 1.0};
@@ -686,6 +717,8 @@ cudaError_t mcg_run_zero(mcg_ctx *ctx, size_t nb, size_t ns) {
   if (e == cudaSuccess) e = cudaMemsetAsync(R.Ni, 0, nb * 4, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(R.lastphot, 0, nb * 4, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(R.kp_hint, 0, nb * 4, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(R.Nabs, 0, nb * 4, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(R.stop, 0, 2 * 8, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(R.spec, 0, ns * 8, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(R.scatspec, 0, ns * 8, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(R.ispec, 0, ns * 4, st);
@@ -700,8 +733,8 @@ cudaError_t mcg_run_zero(mcg_ctx *ctx, size_t nb, size_t ns) {
 /* per-run combination of the current run (nruns averages) */
 void mcg_run_combine(mcg_ctx *ctx, const RunPrep &rp) {
   DevRun &R = ctx->run;
-  combine_runs_kernel<<<(int)((rp.nc + 255) / 256), 256, 0, ctx->stream>>>((int)rp.nc, rp.nruns, R.EJv, R.EJv2, R.Ni,
-                                                                            R.EJvTot, R.EJv2Tot, R.NiTot);
+  combine_runs_kernel<<<(int)((rp.nc + 255) / 256), 256, 0, ctx->stream>>>(
+      (int)rp.nc, rp.nruns, R.EJv, R.EJv2, R.Ni, R.Nabs, R.EJvTot, R.EJv2Tot, R.NiTot, R.NabsTot);
 }
 
 /* results of the current run to the caller's arrays */
@@ -723,6 +756,7 @@ mcg_status mcg_run_finish(mcg_ctx *ctx, const RunPrep &rp, float ms, mcg_result 
   DN(res->Eabs, R.Eabs + last, nc);
   DN(res->T, R.T + last, nc);
   DN(res->Ni, R.NiTot, nc);
+  DN(res->Nabs, R.NabsTot, nc);
   DN(res->spec, R.spec, ns);
   DN(res->scatspec, R.scatspec, ns);
   DN(res->ispec, R.ispec, ns);
@@ -738,8 +772,26 @@ mcg_status mcg_run_finish(mcg_ctx *ctx, const RunPrep &rp, float ms, mcg_result 
   return MCG_OK;
 }
 
+static mcg_status mcg_mcradiation_once(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot, mcg_result *res,
+                                       float *ms_out, bool *stopped);
+
 mcg_status mcg_mcradiation_impl(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot, mcg_result *res) {
   if (!res) return mcg_fail(ctx, MCG_ERR_ARG, "mcradiation: null argument");
+  /* maxruntime: a stopped run starts over with fewer packets (the
+   * reference's `goto 6`); each restart at least halves NphotTot */
+  for (int attempt = 0;; ++attempt) {
+    float ms = 0.0f;
+    bool stopped = false;
+    mcg_status s = mcg_mcradiation_once(ctx, run, nphot, res, &ms, &stopped);
+    if (s != MCG_OK || !stopped) return s;
+    if (attempt >= 64) return mcg_fail(ctx, MCG_ERR_RUN, "mcradiation: maxruntime restarts did not converge");
+  }
+}
+
+/* one pass of the packet loop; *stopped when maxruntime stopped it (then
+ * *nphot holds the reduced count for the restart) */
+static mcg_status mcg_mcradiation_once(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot, mcg_result *res,
+                                       float *ms_out, bool *stopped) {
   RunPrep rp;
   mcg_status s = mcg_run_prepare(ctx, run, nphot, &rp, true);
   if (s != MCG_OK) return s;
@@ -770,6 +822,25 @@ mcg_status mcg_mcradiation_impl(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot
     mcg_status fs = mcg_fast_run(ctx, run->precision == MCG_PREC_MIXED ? 1 : 0, &tm, &ta, run->threads,
                                  run->block, &ms);
     if (fs != MCG_OK) return fs;
+  }
+  *ms_out = ms;
+  if (run->maxruntime > 0.0) {
+    unsigned long long rec[2] = {0ULL, 0ULL};
+    MCG_CUDA(ctx, cudaMemcpyAsync(rec, ctx->run.stop, sizeof rec, cudaMemcpyDeviceToHost, st));
+    MCG_CUDA(ctx, cudaStreamSynchronize(st));
+    if (rec[0] != 0ULL) {
+      /* NphotTot = NphotTot (maxruntime / checktime) (0.5 i / Nphot), at
+       * least 10 (MCRadiation.f:333-334); i packets had started */
+      const double checktime = (double)rec[1] * 1e-9 > 0.0 ? (double)rec[1] * 1e-9 : 1e-9;
+      const double ntot = (double)tm.nphot;
+      const double nn = (double)*nphot * (run->maxruntime / checktime) * (0.5 * (double)rec[0] / ntot);
+      int64_t n = nn < 9e18 ? (int64_t)nn : *nphot;
+      if (n < 10) n = 10;
+      if (n >= *nphot) n = *nphot / 2 > 10 ? *nphot / 2 : 10;
+      *nphot = n;
+      *stopped = true;
+      return MCG_OK;
+    }
   }
   mcg_run_combine(ctx, rp);
   return mcg_run_finish(ctx, rp, ms, res);

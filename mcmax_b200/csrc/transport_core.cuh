@@ -79,6 +79,7 @@ struct TModel {
   const double *KDext, *KDabs, *rw_y, *rw_phi;
   const int *kd_index;
   const unsigned char *thick;
+  double maxruntime; /* seconds; > 0: the run-time limit of MCRadiation.f:323-342 */
 };
 
 /* accumulators */
@@ -99,6 +100,9 @@ struct TAcc {
    * done, [5] = kernel start */
   unsigned long long *done, *tmark;
   unsigned long long thresh[5];
+  int *Nabs;                /* absorption events per cell (may be null) */
+  unsigned long long *stop; /* maxruntime: [0] packets started when the run
+                               stopped (0: running), [1] elapsed ns then */
 };
 
 /* accumulators of the run that packet pid belongs to */
@@ -112,6 +116,7 @@ TP_FN TAcc tp_run_acc(const TAcc &A, int64_t pid) {
   R.Ni += off;
   R.lastphot += off;
   R.kp_hint += off;
+  if (R.Nabs) R.Nabs += off;
   return R;
 }
 
@@ -147,6 +152,32 @@ TP_FN double tp_add(double *p, double v) {
   return o;
 #endif
 }
+/* The run-time limit of MCRadiation.f:323-342, checked when the run's
+ * packet k (0-based) is about to start, t0 the caller's start time
+ * (globaltimer, ns): the run stops when more than maxruntime seconds have
+ * passed, or when more than a tenth of the packets have started and the run
+ * projects to more than 5 maxruntime -- in both cases only with under 90 %
+ * of the packets started.  The first thread to see it records the packet
+ * count and the elapsed time; returns 1 when the run is stopping. */
+TP_FN int tp_runtime_stop(const TAcc &A, double maxruntime, int64_t nphot, unsigned long long k,
+                          unsigned long long t0) {
+#if defined(__CUDA_ARCH__)
+  if (!(maxruntime > 0.0) || nphot <= 10 || !A.stop) return 0;
+  if (*(volatile unsigned long long *)A.stop) return 1;
+  const double t = (double)(tp_globaltimer() - t0) * 1e-9;
+  const unsigned long long i = k + 1ULL;
+  const double di = (double)i, dn = (double)nphot;
+  if ((t > maxruntime || (i > (unsigned long long)(nphot / 10) && t * dn / di > 5.0 * maxruntime)) && di / dn < 0.9) {
+    if (atomicCAS(A.stop, 0ULL, i) == 0ULL) A.stop[1] = (unsigned long long)(t * 1e9);
+    return 1;
+  }
+  return 0;
+#else
+  (void)A; (void)maxruntime; (void)nphot; (void)k; (void)t0;
+  return 0;
+#endif
+}
+
 TP_FN void tp_addi(int *p, int v) {
 #if defined(__CUDA_ARCH__)
   atomicAdd(p, v);
@@ -594,6 +625,7 @@ TP_FN void tp_interact(const TModel &m, const TAcc &A, px_stream *r, TPkt &p, TL
   L.cnt[TC_INTERACT]++;
   if (!m.scattering || tp_rnd(r) > Albedo) {
     L.cnt[TC_ABSORB]++;
+    if (A.Nabs) tp_addi(&A.Nabs[c], 1);
     p.scatt = 0;
     p.pol = 0;
     p.Q = 0.0;

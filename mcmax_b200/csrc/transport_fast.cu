@@ -13,11 +13,12 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
 #include "mcg_internal.h"
-#include "transport_fast.cuh"
+#include "transport_event.cuh"
 
 namespace {
 
@@ -141,7 +142,11 @@ SmemPlan plan_smem(int nr, int nt, int nlam, int ncomp, bool uniform) {
 #ifndef F_MINBLOCKS
 #define F_MINBLOCKS 2
 #endif
-template <class R>
+/* EVENT: the warp scheduler over packet events (transport_event.cuh); the
+ * block must be whole warps.  Otherwise every thread runs its packets to
+ * completion one after the other (the one-thread launch replays the serial
+ * packet order). */
+template <class R, bool EVENT>
 __global__ void __launch_bounds__(F_BLOCK, F_MINBLOCKS) transport_fast_kernel(const __grid_constant__ FModel<R> g,
                                                              const __grid_constant__ TAcc A, SmemPlan sp) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -183,11 +188,17 @@ __global__ void __launch_bounds__(F_BLOCK, F_MINBLOCKS) transport_fast_kernel(co
 #pragma unroll
   for (int k = 0; k < TC_N; ++k) L.cnt[k] = 0u;
   L.tautot = 0.0;
-  for (;;) {
-    unsigned long long pid = atomicAdd(A.next, 1ULL);
-    if (pid >= (unsigned long long)m.nphot) break;
-    f_run_packet<R>(m, A, (int64_t)pid + m.pid0, L);
-    tp_packet_done(A);
+  if (EVENT) {
+    fe_event_loop<R>(m, A, L);
+  } else {
+    const unsigned long long t0 = tp_globaltimer();
+    for (;;) {
+      unsigned long long pid = atomicAdd(A.next, 1ULL);
+      if (pid >= (unsigned long long)m.nphot) break;
+      if (tp_runtime_stop(A, m.maxruntime, m.nphot, pid, t0)) break;
+      f_run_packet<R>(m, A, (int64_t)pid + m.pid0, L);
+      tp_packet_done(A);
+    }
   }
 #pragma unroll
   for (int k = 0; k < TC_N; ++k)
@@ -289,6 +300,7 @@ void fill_fmodel(mcg_ctx *ctx, int pi, const TModel &tm, FModel<R> &g) {
   g.scatG = f.scatG; g.emitG = m.emitG;
   g.KDext = m.KDext; g.KDabs = m.KDabs; g.rw_logy = m.rw_logy; g.rw_phi = m.rw_phi;
   g.kd_index = m.kd_index; g.thick = m.thick; g.rw_dmin = m.rw_dmin;
+  g.maxruntime = tm.maxruntime;
 }
 
 template <class R>
@@ -299,21 +311,28 @@ mcg_status launch_fast(mcg_ctx *ctx, int pi, const TModel &tm, const TAcc &ta, i
   FModel<R> g;
   fill_fmodel<R>(ctx, pi, tm, g);
   SmemPlan sp = plan_smem<R>(m.nr, m.nt, m.nlam, m.ncomp, m.uniform_mix);
-  MCG_CUDA(ctx, cudaFuncSetAttribute(transport_fast_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.bytes));
+  /* the per-lane loop for the one-thread serial replay; the warp scheduler
+   * otherwise (MCG_PACKET_LOOP=lane selects the per-lane loop for
+   * comparisons) */
+  const char *env = getenv("MCG_PACKET_LOOP");
+  const bool event = threads != 1 && !(env && strcmp(env, "lane") == 0);
+  auto kern = event ? transport_fast_kernel<R, true> : transport_fast_kernel<R, false>;
+  MCG_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp.bytes));
   const int b = block > 0 ? block : F_BLOCK;
+  if (event && b % 32 != 0) return mcg_fail(ctx, MCG_ERR_ARG, "mcradiation: block must be a multiple of 32");
   int grid;
   if (threads > 0) {
     grid = (threads + b - 1) / b;
   } else {
     int per_sm = 0;
-    MCG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, transport_fast_kernel<R>, b, sp.bytes));
+    MCG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, b, sp.bytes));
     grid = ctx->sm_count * std::max(per_sm, 1);
   }
   MCG_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
   if (threads == 1)
-    transport_fast_kernel<R><<<1, 1, sp.bytes, ctx->stream>>>(g, ta, sp);
+    kern<<<1, 1, sp.bytes, ctx->stream>>>(g, ta, sp);
   else
-    transport_fast_kernel<R><<<grid, b, sp.bytes, ctx->stream>>>(g, ta, sp);
+    kern<<<grid, b, sp.bytes, ctx->stream>>>(g, ta, sp);
   MCG_CUDA(ctx, cudaGetLastError());
   MCG_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
   MCG_CUDA(ctx, cudaEventSynchronize(ctx->ev1));

@@ -66,9 +66,17 @@ struct FModel {
   const int *kd_index;
   const unsigned char *thick;
   const double *rw_dmin;        /* factRW x the cell's shortest mean free path */
+  double maxruntime;            /* seconds; > 0: MCRadiation.f:323-342 */
 };
 
 #define F_NGUIDE 32
+
+/* member functions of the table functors (TP_FN is `static` on the host) */
+#if defined(__CUDACC__)
+#define F_MFN __host__ __device__ __forceinline__
+#else
+#define F_MFN inline
+#endif
 
 /* cold paths (interactions, random walk, emission) can be compiled out of
  * line to keep the crossing loop small in the instruction cache */
@@ -104,6 +112,7 @@ struct FPkt {
   R Sx, Sy, Sz;
   R wl1, wl2;
   R kabs, kext; /* at the packet wavelength, uniform mixture */
+  R kabs_i, ksca_i; /* at the interaction point (set when a trace ends inside a cell) */
   int ilam1, i, j, edgeNr, onEdge, scatt, pol, pid1;
   int cprev1, cprev2; /* last two cells this packet entered */
 };
@@ -429,175 +438,504 @@ TP_FN double f_tinv(const double *kp, double E1, int lo, int *ibr) {
   return tp_tinv(kp, E1, lo, ibr);
 }
 
-/* ------------------------------------------------------------- interaction */
+/* ------------------------------------------------------------- event steps
+ * The packet's life as a sequence of events.  One event advances one packet
+ * by one step of the reference's loop and consumes the same random numbers
+ * in the same order, so a packet is the same packet whether its events run
+ * back to back (f_run_packet: the host replay and the batched kernel) or
+ * interleaved with other packets' events by the warp scheduler of the
+ * single-model kernel.
+ *
+ *   FS_EMIT     star emission (MCRadiation.f:353-382) and the first tau
+ *   FS_RW       one modified-random-walk jump, or none (RandomWalk.f:47-147)
+ *   FS_TRACE    one cell crossing of trace2d (MCRadiation.f:941-1138)
+ *   FS_ABSORB   absorption + Bjorkman-Wood re-emission (Radiation.f:41-258)
+ *   FS_SCATTER  scattering (Radiation.f:259-355, 381-495)
+ * An interaction ends with the overflow roulette and the next tau
+ * (MCRadiation.f:554-573); a crossing can end the packet (escape: SED bin,
+ * :576-646) or send it back to the star (re-emission of the same packet). */
+enum { FS_NEW = 0, FS_EMIT, FS_RW, FS_TRACE, FS_ABSORB, FS_SCATTER, FS_DEAD, FS_NKIND };
+/* outcome of a crossing */
+enum { FX_CONT = 0, FX_INSIDE, FX_ESCAPE, FX_STAR, FX_GEOFAIL };
+
+/* the current trace: optical depth to travel, travelled so far, crossings */
+struct FTrace {
+  double tau0, tau;
+  int ntrace;
+};
+
+/* the per-cell accumulator updates of one crossing, applied by the caller
+ * (directly, or aggregated over the lanes of a warp that share the cell) */
+struct FDep {
+  int c;       /* cell, -1 when nothing is deposited */
+  int ni;      /* 1: the cell is not one of the packet's last two: exchange
+                  lastphotnr and count the packet in Ni when another packet's
+                  number was there (MCRadiation.f:943-946) */
+  double ej;   /* EJv += */
+  double ej2;  /* EJv2 += (cell exit only) */
+};
+
+TP_FN void f_apply_dep(const TAcc &A, size_t off, const FDep &d, int pid1) {
+  if (d.c < 0) return;
+  if (d.ni && tp_exch(&A.lastphot[off + d.c], pid1) != pid1) tp_addi(&A.Ni[off + d.c], 1);
+  if (d.ej2 != 0.0) tp_add(&A.EJv2[off + d.c], d.ej2);
+  tp_add(&A.EJv[off + d.c], d.ej);
+}
+
+/* accumulator offset of the sub-run packet pid belongs to (nruns) */
+TP_FN size_t f_run_off(const TAcc &A, int64_t pid) { return (size_t)(pid / A.run_packets) * (size_t)A.ncell; }
+
 template <class R>
-F_COLD void f_interact(const FModel<R> &m, const TAcc &A, px_stream *r, FPkt<R> &p, TLocal &L) {
-  typedef FOps<R> O;
-  const int c = p.i * m.nc + (p.j - 1);
+TP_FN void f_packet_init(FPkt<R> &p, int64_t pid) {
+  p.pid1 = (int)(pid + 1);
+  p.q = p.u = p.v = (R)0;
+  p.pol = 0;
+  p.scatt = 0;
+  p.cprev1 = p.cprev2 = -1;
+}
+
+/* star emission (MCRadiation.f:353-382) and the packet's first tau */
+template <class R>
+F_COLD void f_emit_star(const FModel<R> &m, px_stream *r, FPkt<R> &p, FTrace &t, TLocal &L) {
+  p.nEJv = 0.0;
+  (void)px_next(r); /* where_emit */
+  R x, y, z;
+  f_randomdirection<R>(r, &x, &y, &z);
+  p.x = m.R0 * (double)x;
+  p.y = m.R0 * (double)y;
+  p.z = m.R0 * (double)z;
+  L.cnt[TC_EMIT]++;
+  {
+    R ux, uy, uz;
+    f_randomdirection<R>(r, &ux, &uy, &uz);
+    f_set_dir<R>(p, ux, uy, uz);
+  }
+  p.scatt = 0;
+  p.pol = 0;
+  f_set_s<R>(p);
+  {
+    const double Lr = px_next(r) * m.Lstar;
+    const int n = m.nlam - 1;
+    int i = f_lower_bound(m.star_cdf, n, Lr);
+    f_pick<R>(m, p, i, i < n ? m.star_cdf[i] : 0.0, i > 0 ? m.star_cdf[i - 1] : 0.0, Lr);
+  }
+  f_set_lambda<R>(m, p);
+  p.E = m.Epkt;
+  {
+    R ux, uy, uz;
+    f_randomdirection<R>(r, &ux, &uy, &uz);
+    f_set_dir<R>(p, ux, uy, uz);
+  }
+  if (p.x * p.vx + p.y * p.vy + p.z * p.vz < 0.0) {
+    p.vx = -p.vx;
+    p.vy = -p.vy;
+    p.vz = -p.vz;
+  }
+  p.edgeNr = 1;
+  p.onEdge = 1;
+  const double ct = fabs(p.z) / m.R0;
+  p.i = 0;
+  p.j = m.nt - 1;
+  for (int j = 1; j <= m.nt - 1; ++j)
+    if (ct >= m.Theta[j]) {
+      p.j = j;
+      break;
+    }
+  if (m.scattering) {
+    p.pol = 0;
+    p.scatt = 0;
+    p.q = p.u = p.v = (R)0;
+    f_set_s<R>(p);
+  }
+  t.tau0 = -log(px_next(r));
+  t.tau = 0.0;
+  t.ntrace = 0;
+}
+
+/* the state a trace starts in: the random walk first when the packet sits
+ * inside a thick cell (MCRadiation.f:916) */
+template <class R>
+TP_FN int f_trace_state(const FModel<R> &m, const FPkt<R> &p) {
+  return (m.rw && !p.onEdge && m.thick[p.i * m.nc + (p.j - 1)]) ? FS_RW : FS_TRACE;
+}
+
+/* SED bin of an escaping packet (MCRadiation.f:576-646) */
+template <class R>
+TP_FN void f_escape(const FModel<R> &m, const TAcc &A, const FPkt<R> &p, TLocal &L) {
+  L.cnt[TC_ESCAPE]++;
+  const double av = fabs(p.vz);
+  int ia = (int)(av * (double)TP_NANG + 1.0);
+  if (ia > TP_NANG) ia = TP_NANG;
+  const int il = (p.wl1 > p.wl2) ? p.ilam1 : p.ilam1 + 1;
+  const size_t k = (size_t)il * (TP_NANG + 1) + ia;
+  const double wangle = 1.0 / ((double)ia / (double)TP_NANG - (double)(ia - 1) / (double)TP_NANG);
+  const double add = ((wangle * p.E) * m.wlam[il]) / m.nruns_d;
+  tp_add(&A.spec[k], add);
+  tp_addi(&A.ispec[k], 1);
+  if (p.scatt) tp_add(&A.scatspec[k], add);
+}
+
+/* one cell crossing of trace2d; the accumulator updates go to `d` */
+template <class R>
+TP_FN int f_cross(const FModel<R> &m, const TAcc &A, size_t off, FPkt<R> &p, FTrace &t, TLocal &L, FDep &d) {
+  (void)A;
+  (void)off;
   const int nlam = m.nlam;
-  const int l1 = p.ilam1;
+  const int c = p.i * m.nc + (p.j - 1);
+  /* Ni counts distinct packets per cell (lastphotnr, MCRadiation.f:943-946);
+   * re-entering one of its last two cells, the packet's own number is
+   * already there and the exchange is skipped */
+  const bool recent = (c == p.cprev1) || (c == p.cprev2);
+  if (!recent) {
+    p.cprev2 = p.cprev1;
+    p.cprev1 = c;
+  }
+  R kabs, kext;
+  if (m.uniform_mix) {
+    kabs = p.kabs;
+    kext = m.scattering ? p.kext : p.kabs;
+  } else {
+    const R *Ka = m.KabsTotR + (size_t)c * nlam, *Ke = m.KextTotR + (size_t)c * nlam;
+    kabs = Ka[p.ilam1] * p.wl1 + Ka[p.ilam1 + 1] * p.wl2;
+    kext = m.scattering ? Ke[p.ilam1] * p.wl1 + Ke[p.ilam1 + 1] * p.wl2 : kabs;
+  }
+  double v;
+  int inext, jnext;
+  const int geo = f_trace2edge<R>(m, p, &v, &inext, &jnext);
+  d.c = c;
+  d.ni = !recent;
+  d.ej = 0.0;
+  d.ej2 = 0.0;
+  if (geo) return FX_GEOFAIL;
+  L.cnt[TC_CROSS]++;
+  const double dAU = m.dens[c] * TP_AU;
+  const double tau1 = ((double)kext * v) * dAU;
+  if (t.tau + tau1 > t.tau0) {
+    v = (v * (t.tau0 - t.tau)) / tau1;
+    L.tautot += t.tau0 - t.tau;
+    p.x += p.vx * v;
+    p.y += p.vy * v;
+    p.z += p.vz * v;
+    p.onEdge = 0;
+    const double dj = (p.E * v) * TP_AU * (double)kabs;
+    d.ej = dj;
+    p.nEJv += dj;
+    /* the interaction's opacities at this point (Radiation.f:44-70) */
+    p.kabs_i = kabs;
+    p.ksca_i = kext - kabs;
+    return FX_INSIDE;
+  }
+  p.x += p.vx * v;
+  p.y += p.vy * v;
+  p.z += p.vz * v;
+  const double dj = (p.E * v) * TP_AU * (double)kabs;
+  p.nEJv += dj;
+  d.ej2 = p.nEJv * p.nEJv;
+  p.nEJv = 0.0;
+  d.ej = dj;
+  p.onEdge = 1;
+  t.tau += tau1;
+  L.tautot += tau1;
+  if (inext >= m.nr) return FX_ESCAPE;
+  if (inext < 0) return FX_STAR;
+  p.i = inext;
+  p.j = jnext;
+  if (++t.ntrace > m.nr * m.nt * 2) {
+    L.cnt[TC_ABANDON]++;
+    return FX_STAR;
+  }
+  return FX_CONT;
+}
+
+/* albedo test of an interaction (Radiation.f:74-76): FS_ABSORB or FS_SCATTER */
+template <class R>
+TP_FN int f_albedo(const FModel<R> &m, px_stream *r, FPkt<R> &p, TLocal &L) {
+  typedef FOps<R> O;
+  L.cnt[TC_INTERACT]++;
+  if (!m.scattering) return FS_ABSORB;
+  /* the non-uniform mixture's opacities at the interaction point are those
+   * of the crossing that ended inside the cell; a uniform mixture's are the
+   * packet's (kabs, kext - kabs).  Both give the reference's albedo. */
   R kabs, ksca;
   if (m.uniform_mix) {
     kabs = p.kabs;
     ksca = p.kext - p.kabs;
   } else {
-    const R *Ka = m.KabsTotR + (size_t)c * nlam, *Ke = m.KextTotR + (size_t)c * nlam;
-    kabs = Ka[l1] * p.wl1 + Ka[l1 + 1] * p.wl2;
-    ksca = (Ke[l1] * p.wl1 + Ke[l1 + 1] * p.wl2) - kabs;
+    kabs = p.kabs_i;
+    ksca = p.ksca_i;
   }
-  L.cnt[TC_INTERACT]++;
   const R albedo = ksca / (ksca + kabs);
-  if (!m.scattering || O::u(px_next(r)) > albedo) {
-    L.cnt[TC_ABSORB]++;
-    p.scatt = 0;
-    p.pol = 0;
-    p.q = p.u = p.v = (R)0;
-    const double *kp = m.KpCell + (m.uniform_mix ? (size_t)0 : (size_t)c * TP_TT);
-    const double dE = p.E;
-    const double Eold = tp_add(&A.Eabs[c], dE);
-    const double mass = m.mass[c];
-    int hint = A.kp_hint[c];
-    int ib0, ib1;
-    const double T0 = f_tinv(kp, Eold / mass, hint, &ib0);
-    const double T1 = f_tinv(kp, (Eold + dE) / mass, ib0, &ib1);
-    if (ib1 > hint) A.kp_hint[c] = ib1;
-    int iT0 = (int)T0, iT1 = (int)T1;
-    double e0 = T0 - (double)iT0, e1 = T1 - (double)iT1;
-    if (iT0 >= TP_TMAX - 1) iT0 = TP_TMAX - 2;
-    if (iT1 >= TP_TMAX - 1) iT1 = TP_TMAX - 1;
-    if (iT0 < 1) iT0 = 1;
-    if (iT1 < 2) iT1 = 2;
-    /* new direction first (emit), then the wavelength draw */
-    L.cnt[TC_EMIT]++;
-    {
-      R ux, uy, uz;
-      f_randomdirection<R>(r, &ux, &uy, &uz);
-      f_set_dir<R>(p, ux, uy, uz);
-    }
-    p.scatt = 0;
-    p.pol = 0;
-    f_set_s<R>(p);
-    const double xi = px_next(r);
-    const int n = nlam - 1;
-    if (m.uniform_mix) {
-      const double *D0 = m.Dcum + (size_t)iT0 * n;
-      if (iT0 == iT1) {
-        const double tot = D0[n - 1];
-        const double Lr = xi * tot;
-        int gk = (int)(xi * (double)F_NGUIDE);
-        if (gk > F_NGUIDE - 1) gk = F_NGUIDE - 1;
-        const int i = f_walk([&](int k) { return D0[k]; }, n, (int)m.emitG[(size_t)iT0 * F_NGUIDE + gk], Lr, true);
-        f_pick<R>(m, p, i, i < n ? D0[i] : 0.0, i > 0 ? D0[i - 1] : 0.0, Lr);
-      } else {
-        const double *C0 = m.Ccum + (size_t)iT0 * n, *C1 = m.Ccum + (size_t)iT1 * n;
-        const double *D1 = m.Dcum + (size_t)iT1 * n;
-        auto cum = [&](int i) { return (C1[i] + e1 * D1[i]) - (C0[i] + e0 * D0[i]); };
-        const double tot = cum(n - 1);
-        const double Lr = xi * tot;
-        int lo = 0, hi = n;
-        while (lo < hi) {
-          int mid = (lo + hi) >> 1;
-          if (cum(mid) >= Lr)
-            hi = mid;
-          else
-            lo = mid + 1;
-        }
-        f_pick<R>(m, p, lo, lo < n ? cum(lo) : 0.0, lo > 0 ? cum(lo - 1) : 0.0, Lr);
-      }
+  if (O::u(px_next(r)) > albedo) return FS_ABSORB;
+  p.ksca_i = ksca;
+  return FS_SCATTER;
+}
+
+/* absorption up to the wavelength draw: the cell's absorbed energy, the
+ * temperatures before and after, the new direction and the draw xi.  What
+ * the wavelength search needs is left in `a`. */
+struct FAbs {
+  int c, iT0, iT1;
+  double e0, e1, T1, xi;
+};
+
+template <class R>
+F_COLD void f_absorb_pre(const FModel<R> &m, const TAcc &A, size_t off, px_stream *r, FPkt<R> &p, TLocal &L,
+                         FAbs &a) {
+  const int c = p.i * m.nc + (p.j - 1);
+  L.cnt[TC_ABSORB]++;
+  if (A.Nabs) tp_addi(&A.Nabs[off + c], 1);
+  p.scatt = 0;
+  p.pol = 0;
+  p.q = p.u = p.v = (R)0;
+  const double *kp = m.KpCell + (m.uniform_mix ? (size_t)0 : (size_t)c * TP_TT);
+  const double dE = p.E;
+  const double Eold = tp_add(&A.Eabs[off + c], dE);
+  const double mass = m.mass[c];
+  int hint = A.kp_hint[off + c];
+  int ib0, ib1;
+  const double T0 = f_tinv(kp, Eold / mass, hint, &ib0);
+  const double T1 = f_tinv(kp, (Eold + dE) / mass, ib0, &ib1);
+  if (ib1 > hint) A.kp_hint[off + c] = ib1;
+  int iT0 = (int)T0, iT1 = (int)T1;
+  a.e0 = T0 - (double)iT0;
+  a.e1 = T1 - (double)iT1;
+  if (iT0 >= TP_TMAX - 1) iT0 = TP_TMAX - 2;
+  if (iT1 >= TP_TMAX - 1) iT1 = TP_TMAX - 1;
+  if (iT0 < 1) iT0 = 1;
+  if (iT1 < 2) iT1 = 2;
+  a.iT0 = iT0;
+  a.iT1 = iT1;
+  a.c = c;
+  a.T1 = T1;
+  /* new direction first (emit), then the wavelength draw */
+  L.cnt[TC_EMIT]++;
+  {
+    R ux, uy, uz;
+    f_randomdirection<R>(r, &ux, &uy, &uz);
+    f_set_dir<R>(p, ux, uy, uz);
+  }
+  p.scatt = 0;
+  p.pol = 0;
+  f_set_s<R>(p);
+  a.xi = px_next(r);
+}
+
+/* Re-emission spectrum of a uniform mixture as a cumulative over the nlam-1
+ * trapezoid intervals: C(iT)[i] = cumulative of BB(iT) K, D(iT)[i] =
+ * cumulative of (BB(iT+1) - BB(iT)) K, the (T0 -> T1) jump's cumulative is
+ * [C(iT1) + e1 D(iT1)] - [C(iT0) + e0 D(iT0)], the reference's interpolated
+ * Delta-B (Radiation.f:187-213) summed in the same order. */
+template <class R>
+struct FEmitU {
+  const double *C0, *D0, *C1, *D1;
+  double e0, e1;
+  bool same;
+  F_MFN double operator()(int i) const { return same ? D0[i] : (C1[i] + e1 * D1[i]) - (C0[i] + e0 * D0[i]); }
+};
+
+template <class R>
+TP_FN FEmitU<R> f_emit_u(const FModel<R> &m, const FAbs &a) {
+  const int n = m.nlam - 1;
+  FEmitU<R> f;
+  f.D0 = m.Dcum + (size_t)a.iT0 * n;
+  f.C0 = m.Ccum + (size_t)a.iT0 * n;
+  f.C1 = m.Ccum + (size_t)a.iT1 * n;
+  f.D1 = m.Dcum + (size_t)a.iT1 * n;
+  f.e0 = a.e0;
+  f.e1 = a.e1;
+  f.same = a.iT0 == a.iT1;
+  return f;
+}
+
+/* A non-uniform mixture's re-emission spectrum at wavelength l: the
+ * reference's spec(l) (Radiation.f:187-213) from the temperature-major
+ * Planck rows and the cell's KabsTot row. */
+template <class R>
+struct FEmitN {
+  const double *Ka, *P0, *P0p, *P1, *P1p;
+  double e0, e1;
+  bool same;
+  F_MFN double operator()(int l) const {
+    if (same) return (P0p[l] - P0[l]) * Ka[l];
+    return (((e1 * P1p[l] + (1.0 - e1) * P1[l]) - e0 * P0p[l]) - (1.0 - e0) * P0[l]) * Ka[l];
+  }
+};
+
+template <class R>
+TP_FN FEmitN<R> f_emit_n(const FModel<R> &m, const FAbs &a, double *Lr) {
+  const int nlam = m.nlam;
+  FEmitN<R> f;
+  f.Ka = m.KabsTot + (size_t)a.c * nlam;
+  f.P0 = m.BBT + (size_t)a.iT0 * nlam;
+  f.P0p = f.P0 + nlam;
+  f.P1 = m.BBT + (size_t)a.iT1 * nlam;
+  f.P1p = f.P1 + nlam;
+  f.e0 = a.e0;
+  f.e1 = a.e1;
+  f.same = a.iT0 == a.iT1;
+  const double *kp = m.KpCell + (size_t)a.c * TP_TT;
+  const int i0 = a.iT0, i1 = a.iT1;
+  const double e0 = a.e0, e1 = a.e1;
+  const double kpe = i0 == i1 ? kp[i0 + 1] - kp[i0]
+                              : ((e1 * kp[i1 + 1] + (1.0 - e1) * kp[i1]) - e0 * kp[i0 + 1]) - (1.0 - e0) * kp[i0];
+  *Lr = a.xi * kpe;
+  return f;
+}
+
+/* the wavelength search of one lane on its own */
+template <class R>
+F_COLD void f_absorb_search(const FModel<R> &m, FPkt<R> &p, const FAbs &a) {
+  const int n = m.nlam - 1;
+  if (m.uniform_mix) {
+    const FEmitU<R> f = f_emit_u<R>(m, a);
+    const double tot = f(n - 1);
+    const double Lr = a.xi * tot;
+    int i;
+    if (f.same) {
+      int gk = (int)(a.xi * (double)F_NGUIDE);
+      if (gk > F_NGUIDE - 1) gk = F_NGUIDE - 1;
+      i = f_walk([&](int k) { return f.D0[k]; }, n, (int)m.emitG[(size_t)a.iT0 * F_NGUIDE + gk], Lr, true);
     } else {
-      /* per-cell spectrum: sequential scan (Radiation.f:187-213), the
-       * additions in the reference's order; the Planck rows are read
-       * temperature-major and eight wavelengths at a time, so the loads of
-       * a block are issued together */
-      const double *Ka = m.KabsTot + (size_t)c * nlam;
-      const double *P0 = m.BBT + (size_t)iT0 * nlam, *P0p = P0 + nlam;
-      const double *P1 = m.BBT + (size_t)iT1 * nlam, *P1p = P1 + nlam;
-      auto spec = [&](int l) {
-        if (iT0 == iT1) return (P0p[l] - P0[l]) * Ka[l];
-        return (((e1 * P1p[l] + (1.0 - e1) * P1[l]) - e0 * P0p[l]) - (1.0 - e0) * P0[l]) * Ka[l];
-      };
-      double kpe = iT0 == iT1 ? kp[iT0 + 1] - kp[iT0]
-                              : ((e1 * kp[iT1 + 1] + (1.0 - e1) * kp[iT1]) - e0 * kp[iT0 + 1]) - (1.0 - e0) * kp[iT0];
-      const double Lr = xi * kpe;
-      double Lt = 0.0, Ltold = 0.0, s0 = spec(0);
-      int i = n;
-      for (int i0 = 0; i0 < n && i == n; i0 += 8) {
-        double sb[8], dn[8];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-          const int l = i0 + u;
-          sb[u] = l < n ? spec(l + 1) : 0.0;
-          dn[u] = l < n ? m.dnu_half[l] : 0.0;
-        }
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-          if (i0 + u >= n) break;
-          Lt = Lt + dn[u] * (s0 + sb[u]);
-          if (Lt >= Lr) {
-            i = i0 + u;
-            break;
-          }
-          Ltold = Lt;
-          s0 = sb[u];
-        }
+      int lo = 0, hi = n;
+      while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (f(mid) >= Lr)
+          hi = mid;
+        else
+          lo = mid + 1;
       }
-      f_pick<R>(m, p, i, Lt, Ltold, Lr);
+      i = lo;
     }
-    f_set_lambda<R>(m, p);
-    A.T[c] = T1;
+    f_pick<R>(m, p, i, i < n ? f(i) : 0.0, i > 0 ? f(i - 1) : 0.0, Lr);
   } else {
-    L.cnt[TC_SCATTER]++;
-    p.scatt = 1;
-    if (m.scat_how == 1) {
-      R ux, uy, uz;
-      f_randomdirection<R>(r, &ux, &uy, &uz);
-      f_set_dir<R>(p, ux, uy, uz);
-    } else {
-      R KscaR = O::u(px_next(r)) * ksca;
-      const double *w = m.comp_w + (size_t)c * m.ncomp;
-      int mat = -1, qlast = 0, llast = l1;
-      /* the reference's order (Radiation.f:273-290): per component the
-       * l1+1 term, then the l1 term; weights and opacities of four
-       * components are loaded together */
-      for (int q0 = 0; q0 < m.ncomp && mat < 0; q0 += 4) {
-        R w2b[4], w1b[4];
+    /* sequential scan (Radiation.f:187-213), the additions in the
+     * reference's order; eight wavelengths' loads are issued together */
+    double Lr;
+    const FEmitN<R> spec = f_emit_n<R>(m, a, &Lr);
+    double Lt = 0.0, Ltold = 0.0, s0 = spec(0);
+    int i = n;
+    for (int i0 = 0; i0 < n && i == n; i0 += 8) {
+      double sb[8], dn[8];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int q = q0 + u;
-          const R wq = q < m.ncomp ? (R)w[q] : (R)0;
-          w2b[u] = q < m.ncomp ? wq * p.wl2 * m.Ksca_c[q * nlam + l1 + 1] : (R)0;
-          w1b[u] = q < m.ncomp ? wq * p.wl1 * m.Ksca_c[q * nlam + l1] : (R)0;
-        }
+      for (int u = 0; u < 8; ++u) {
+        const int l = i0 + u;
+        sb[u] = l < n ? spec(l + 1) : 0.0;
+        dn[u] = l < n ? m.dnu_half[l] : 0.0;
+      }
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int q = q0 + u;
-          if (q >= m.ncomp) break;
-          KscaR -= w2b[u];
-          if (KscaR < (R)0) {
-            mat = q * nlam + l1 + 1;
-            break;
-          }
-          KscaR -= w1b[u];
-          if (KscaR < (R)0) {
-            mat = q * nlam + l1;
-            break;
-          }
-          if (w2b[u] > (R)0) { qlast = q; llast = l1 + 1; }
-          if (w1b[u] > (R)0) { qlast = q; llast = l1; }
+      for (int u = 0; u < 8; ++u) {
+        if (i0 + u >= n) break;
+        Lt = Lt + dn[u] * (s0 + sb[u]);
+        if (Lt >= Lr) {
+          i = i0 + u;
+          break;
         }
+        Ltold = Lt;
+        s0 = sb[u];
       }
-      if (mat < 0) {
-        L.cnt[TC_AVGMAT]++;
-        mat = qlast * nlam + llast;
-      }
-      f_scatangle<R>(m, r, p, mat);
     }
+    f_pick<R>(m, p, i, Lt, Ltold, Lr);
   }
 }
 
-/* ------------------------------------------------------------- random walk */
 template <class R>
-F_COLD int f_random_walk(const FModel<R> &m, const TAcc &A, px_stream *r, FPkt<R> &p, TLocal &L) {
+TP_FN void f_absorb_post(const FModel<R> &m, const TAcc &A, size_t off, FPkt<R> &p, const FAbs &a) {
+  f_set_lambda<R>(m, p);
+  A.T[off + a.c] = a.T1;
+}
+
+/* scattering up to the component pick (Radiation.f:259-290): isotropic
+ * scattering is complete here (returns -1 with the new direction set);
+ * otherwise returns 1 and leaves the draw KscaR for the pick */
+template <class R>
+TP_FN int f_scatter_pre(const FModel<R> &m, px_stream *r, FPkt<R> &p, TLocal &L, R *KscaR) {
+  typedef FOps<R> O;
+  L.cnt[TC_SCATTER]++;
+  p.scatt = 1;
+  if (m.scat_how == 1) {
+    R ux, uy, uz;
+    f_randomdirection<R>(r, &ux, &uy, &uz);
+    f_set_dir<R>(p, ux, uy, uz);
+    return -1;
+  }
+  *KscaR = O::u(px_next(r)) * p.ksca_i;
+  return 1;
+}
+
+/* the component and wavelength end whose scattering matrix is used: the
+ * reference's order (Radiation.f:273-290), per component the l1+1 term,
+ * then the l1 term; -1 - (fallback material) when the draw exceeds the sum
+ * (the averaged-matrix branch, :293-315) */
+template <class R>
+TP_FN int f_scatter_pick(const FModel<R> &m, const FPkt<R> &p, R KscaR) {
+  const int nlam = m.nlam, l1 = p.ilam1;
+  const int c = p.i * m.nc + (p.j - 1);
+  const double *w = m.comp_w + (size_t)c * m.ncomp;
+  int mat = -1, qlast = 0, llast = l1;
+  for (int q0 = 0; q0 < m.ncomp && mat < 0; q0 += 4) {
+    R w2b[4], w1b[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int q = q0 + u;
+      const R wq = q < m.ncomp ? (R)w[q] : (R)0;
+      w2b[u] = q < m.ncomp ? wq * p.wl2 * m.Ksca_c[q * nlam + l1 + 1] : (R)0;
+      w1b[u] = q < m.ncomp ? wq * p.wl1 * m.Ksca_c[q * nlam + l1] : (R)0;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int q = q0 + u;
+      if (q >= m.ncomp) break;
+      KscaR -= w2b[u];
+      if (KscaR < (R)0) {
+        mat = q * nlam + l1 + 1;
+        break;
+      }
+      KscaR -= w1b[u];
+      if (KscaR < (R)0) {
+        mat = q * nlam + l1;
+        break;
+      }
+      if (w2b[u] > (R)0) { qlast = q; llast = l1 + 1; }
+      if (w1b[u] > (R)0) { qlast = q; llast = l1; }
+    }
+  }
+  if (mat < 0) return -1 - (qlast * nlam + llast);
+  return mat;
+}
+
+/* the scattering matrix's use of the pick: the averaged-matrix counter and
+ * the new direction and Stokes vector (Radiation.f:381-495) */
+template <class R>
+TP_FN void f_scatter_post(const FModel<R> &m, px_stream *r, FPkt<R> &p, TLocal &L, int pick) {
+  if (pick < 0) {
+    L.cnt[TC_AVGMAT]++;
+    pick = -1 - pick;
+  }
+  f_scatangle<R>(m, r, p, pick);
+}
+
+/* the overflow roulette (MCRadiation.f:568-571) and the next tau (:573);
+ * returns 0 when the roulette ends the packet */
+template <class R>
+TP_FN int f_after_interact(const FModel<R> &m, px_stream *r, FPkt<R> &p, FTrace &t, TLocal &L) {
+  if (m.maxinteract > 0) {
+    if (px_next(r) < 1.0 / (double)m.maxinteract) {
+      L.cnt[TC_OVERFLOW]++;
+      return 0;
+    }
+    p.E = (p.E * (double)m.maxinteract) / (double)(m.maxinteract - 1);
+  }
+  t.tau0 = -log(px_next(r));
+  t.tau = 0.0;
+  t.ntrace = 0;
+  return 1;
+}
+
+/* ------------------------------------------------------------- random walk */
+/* one jump of the modified random walk (RandomWalk.f:15-147); returns 1
+ * when the packet jumped (then a new outward direction follows) */
+template <class R>
+F_COLD int f_random_walk(const FModel<R> &m, const TAcc &A, size_t off, px_stream *r, FPkt<R> &p, TLocal &L) {
   const int c = p.i * m.nc + (p.j - 1);
   /* distance to the nearest face (MinDist, RandomWalk.f:15-43) */
   double rho = p.x * p.x + p.y * p.y;
@@ -617,7 +955,7 @@ F_COLD int f_random_walk(const FModel<R> &m, const TAcc &A, px_stream *r, FPkt<R
   if (m.rw_dmin && dmin <= m.rw_dmin[c]) return 0;
   const int row = m.kd_index[c];
   if (row < 0) return 0;
-  int iT = (int)A.T[c];
+  int iT = (int)A.T[off + c];
   if (iT < 1) iT = 1;
   if (iT > TP_TMAX - 1) iT = TP_TMAX - 1;
   const double Kext = m.KDext[(size_t)row * TP_TT + iT];
@@ -635,196 +973,81 @@ F_COLD int f_random_walk(const FModel<R> &m, const TAcc &A, px_stream *r, FPkt<R
   p.z += dmin * p.vz;
   const double EJv = (p.E * v) * TP_AU;
   const double dEa = (EJv * Kabs) * m.dens[c];
-  const double Eold = tp_add(&A.Eabs[c], dEa);
-  tp_add(&A.EJv[c], EJv * Kabs);
+  const double Eold = tp_add(&A.Eabs[off + c], dEa);
+  tp_add(&A.EJv[off + c], EJv * Kabs);
   p.nEJv += EJv * Kabs;
   const double *kp = m.KpCell + (m.uniform_mix ? (size_t)0 : (size_t)c * TP_TT);
   int ib;
-  A.T[c] = f_tinv(kp, (Eold + dEa) / m.mass[c], A.kp_hint[c], &ib);
-  if (ib > A.kp_hint[c]) A.kp_hint[c] = ib;
+  A.T[off + c] = f_tinv(kp, (Eold + dEa) / m.mass[c], A.kp_hint[off + c], &ib);
+  if (ib > A.kp_hint[off + c]) A.kp_hint[off + c] = ib;
   L.tautot += v / dmin;
   L.cnt[TC_RWSTEP]++;
   return 1;
 }
 
-/* ------------------------------------------------------------- trace */
+/* the new direction after a jump: outward from the jump (RandomWalk.f) */
 template <class R>
-TP_FN int f_trace(const FModel<R> &m, const TAcc &A, px_stream *r, FPkt<R> &p, double tau0, TLocal &L) {
-  const int nlam = m.nlam;
-  double tau = 0.0;
-  int ntrace = 0;
-  if (m.rw && !p.onEdge && m.thick[p.i * m.nc + (p.j - 1)]) {
-    while (f_random_walk<R>(m, A, r, p, L)) {
-      R vx, vy, vz;
-      do {
-        f_randomdirection<R>(r, &vx, &vy, &vz);
-      } while ((R)p.vx * vx + (R)p.vy * vy + (R)p.vz * vz < (R)0);
-      f_set_dir<R>(p, vx, vy, vz);
-    }
-  }
-  for (;;) {
-    const int c = p.i * m.nc + (p.j - 1);
-    /* Ni counts distinct packets per cell (lastphotnr, MCRadiation.f:943-946);
-     * re-entering one of its last two cells, the packet's own number is
-     * already there */
-    const bool recent = (c == p.cprev1) || (c == p.cprev2);
-    const int prev = recent ? p.pid1 : tp_exch(&A.lastphot[c], p.pid1);
-    if (!recent) {
-      p.cprev2 = p.cprev1;
-      p.cprev1 = c;
-    }
-    R kabs, kext;
-    if (m.uniform_mix) {
-      kabs = p.kabs;
-      kext = m.scattering ? p.kext : p.kabs;
-    } else {
-      const R *Ka = m.KabsTotR + (size_t)c * nlam, *Ke = m.KextTotR + (size_t)c * nlam;
-      kabs = Ka[p.ilam1] * p.wl1 + Ka[p.ilam1 + 1] * p.wl2;
-      kext = m.scattering ? Ke[p.ilam1] * p.wl1 + Ke[p.ilam1 + 1] * p.wl2 : kabs;
-    }
-    double v;
-    int inext, jnext;
-    const int geo = f_trace2edge<R>(m, p, &v, &inext, &jnext);
-    if (prev != p.pid1) tp_addi(&A.Ni[c], 1);
-    if (geo) return -1;
-    L.cnt[TC_CROSS]++;
-    const double dAU = m.dens[c] * TP_AU;
-    const double tau1 = ((double)kext * v) * dAU;
-    if (tau + tau1 > tau0) {
-      v = (v * (tau0 - tau)) / tau1;
-      L.tautot += tau0 - tau;
-      p.x += p.vx * v;
-      p.y += p.vy * v;
-      p.z += p.vz * v;
-      p.onEdge = 0;
-      const double dj = (p.E * v) * TP_AU * (double)kabs;
-      tp_add(&A.EJv[c], dj);
-      p.nEJv += dj;
-      return 0;
-    }
-    p.x += p.vx * v;
-    p.y += p.vy * v;
-    p.z += p.vz * v;
-    const double dj = (p.E * v) * TP_AU * (double)kabs;
-    p.nEJv += dj;
-    tp_add(&A.EJv2[c], p.nEJv * p.nEJv);
-    p.nEJv = 0.0;
-    tp_add(&A.EJv[c], dj);
-    p.onEdge = 1;
-    tau += tau1;
-    L.tautot += tau1;
-    if (inext >= m.nr) return 1;
-    if (inext < 0) return 2;
-    p.i = inext;
-    p.j = jnext;
-    if (++ntrace > m.nr * m.nt * 2) {
-      L.cnt[TC_ABANDON]++;
-      return 2;
-    }
-  }
+TP_FN void f_rw_redirect(px_stream *r, FPkt<R> &p) {
+  R vx, vy, vz;
+  do {
+    f_randomdirection<R>(r, &vx, &vy, &vz);
+  } while ((R)p.vx * vx + (R)p.vy * vy + (R)p.vz * vz < (R)0);
+  f_set_dir<R>(p, vx, vy, vz);
 }
 
 /* ------------------------------------------------------------- one packet */
+/* All events of one packet back to back, accumulators updated directly:
+ * the host replay of the device code and the batched kernel. */
 template <class R>
-TP_FN void f_run_packet(const FModel<R> &m, const TAcc &A0, int64_t pid, TLocal &L) {
-  const TAcc A = tp_run_acc(A0, pid);
+TP_FN void f_run_packet(const FModel<R> &m, const TAcc &A, int64_t pid, TLocal &L) {
+  const size_t off = f_run_off(A, pid);
   px_stream rs;
   px_init(&rs, m.seed, (uint64_t)pid);
   px_stream *r = &rs;
   FPkt<R> p;
-  p.pid1 = (int)(pid + 1);
-  p.q = p.u = p.v = (R)0;
-  p.pol = 0;
-  p.scatt = 0;
-  p.cprev1 = p.cprev2 = -1;
+  f_packet_init<R>(p, pid);
+  FTrace t;
+  int st = FS_EMIT;
   for (;;) {
-    p.nEJv = 0.0;
-    (void)px_next(r); /* where_emit */
-    R x, y, z;
-    f_randomdirection<R>(r, &x, &y, &z);
-    p.x = m.R0 * (double)x;
-    p.y = m.R0 * (double)y;
-    p.z = m.R0 * (double)z;
-    L.cnt[TC_EMIT]++;
-    {
-      R ux, uy, uz;
-      f_randomdirection<R>(r, &ux, &uy, &uz);
-      f_set_dir<R>(p, ux, uy, uz);
-    }
-    p.scatt = 0;
-    p.pol = 0;
-    f_set_s<R>(p);
-    {
-      const double Lr = px_next(r) * m.Lstar;
-      const int n = m.nlam - 1;
-      int i = f_lower_bound(m.star_cdf, n, Lr);
-      f_pick<R>(m, p, i, i < n ? m.star_cdf[i] : 0.0, i > 0 ? m.star_cdf[i - 1] : 0.0, Lr);
-    }
-    f_set_lambda<R>(m, p);
-    p.E = m.Epkt;
-    {
-      R ux, uy, uz;
-      f_randomdirection<R>(r, &ux, &uy, &uz);
-      f_set_dir<R>(p, ux, uy, uz);
-    }
-    if (p.x * p.vx + p.y * p.vy + p.z * p.vz < 0.0) {
-      p.vx = -p.vx;
-      p.vy = -p.vy;
-      p.vz = -p.vz;
-    }
-    p.edgeNr = 1;
-    p.onEdge = 1;
-    const double ct = fabs(p.z) / m.R0;
-    p.i = 0;
-    p.j = m.nt - 1;
-    for (int j = 1; j <= m.nt - 1; ++j)
-      if (ct >= m.Theta[j]) {
-        p.j = j;
-        break;
-      }
-    if (m.scattering) {
-      p.pol = 0;
-      p.scatt = 0;
-      p.q = p.u = p.v = (R)0;
-      f_set_s<R>(p);
-    }
-    double tau = -log(px_next(r));
-    for (;;) {
-      const int st = f_trace<R>(m, A, r, p, tau, L);
-      if (st < 0) {
+    if (st == FS_EMIT) {
+      f_emit_star<R>(m, r, p, t, L);
+      st = FS_TRACE; /* on the star's surface: never inside a thick cell */
+    } else if (st == FS_RW) {
+      if (f_random_walk<R>(m, A, off, r, p, L))
+        f_rw_redirect<R>(r, p);
+      else
+        st = FS_TRACE;
+    } else if (st == FS_TRACE) {
+      FDep d;
+      const int o = f_cross<R>(m, A, off, p, t, L, d);
+      f_apply_dep(A, off, d, p.pid1);
+      if (o == FX_CONT) continue;
+      if (o == FX_INSIDE) {
+        st = f_albedo<R>(m, r, p, L);
+      } else if (o == FX_ESCAPE) {
+        f_escape<R>(m, A, p, L);
+        return;
+      } else if (o == FX_STAR) {
+        L.cnt[TC_HITSTAR]++;
+        st = FS_EMIT;
+      } else {
         L.cnt[TC_GEOFAIL]++;
         return;
       }
-      if (st == 2) {
-        L.cnt[TC_HITSTAR]++;
-        break;
+    } else {
+      if (st == FS_ABSORB) {
+        FAbs a;
+        f_absorb_pre<R>(m, A, off, r, p, L, a);
+        f_absorb_search<R>(m, p, a);
+        f_absorb_post<R>(m, A, off, p, a);
+      } else {
+        R KscaR;
+        if (f_scatter_pre<R>(m, r, p, L, &KscaR) > 0) f_scatter_post<R>(m, r, p, L, f_scatter_pick<R>(m, p, KscaR));
       }
-      if (st == 1) {
-        L.cnt[TC_ESCAPE]++;
-        const double av = fabs(p.vz);
-        int ia = (int)(av * (double)TP_NANG + 1.0);
-        if (ia > TP_NANG) ia = TP_NANG;
-        const int il = (p.wl1 > p.wl2) ? p.ilam1 : p.ilam1 + 1;
-        const size_t k = (size_t)il * (TP_NANG + 1) + ia;
-        const double wangle = 1.0 / ((double)ia / (double)TP_NANG - (double)(ia - 1) / (double)TP_NANG);
-        const double add = ((wangle * p.E) * m.wlam[il]) / m.nruns_d;
-        tp_add(&A.spec[k], add);
-        tp_addi(&A.ispec[k], 1);
-        if (p.scatt) tp_add(&A.scatspec[k], add);
-        return;
-      }
-      f_interact<R>(m, A, r, p, L);
-      if (m.maxinteract > 0) {
-        if (px_next(r) < 1.0 / (double)m.maxinteract) {
-          L.cnt[TC_OVERFLOW]++;
-          return;
-        }
-        p.E = (p.E * (double)m.maxinteract) / (double)(m.maxinteract - 1);
-      }
-      tau = -log(px_next(r));
+      if (!f_after_interact<R>(m, r, p, t, L)) return;
+      st = f_trace_state<R>(m, p);
     }
   }
 }
-
 
 #endif /* MCMAX_TRANSPORT_FAST_CUH */

@@ -1124,8 +1124,11 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
               Ksca=Ksca, F=F, BB=BB, Fstar=Fstar, Lstar=Lstar, Tstar=tstar, Rstar_cm=rstar_cm, scat_how=scat,
               bins=[g[0] for g in grain_info], w=w0, distance=v("distance", 100.0),
               gasdens=None if gasdens is None else gasdens.reshape(-1))
+    # the overflow roulette is on only when the deck sets maxinteract
+    # (overflow = .false. by default, Init.f:139,144,637-639); maxruntime -1
+    # is off (Init.f:355)
     run = dict(seed=abs(v("idum", -42, int)), randomwalk=v("randomwalk", False, bool), factRW=v("factrw", 10.0),
-               maxinteract=v("maxinteract", 1000000, int), nruns=v("nruns", 1, int),
+               maxinteract=v("maxinteract", 0, int), maxruntime=v("maxruntime", -1.0), nruns=v("nruns", 1, int),
                nphotdiffuse=v("nphotdiffuse", 25, int), dtdiffuse=v("dtdiffuse", 1.0),
                zones=[(z["rin"], z["rout"], z["sh"], z["rsh"], z["shpow"], z["denspow"], z["fix"]) for z in zones],
                Mstar=v("mstar", 2.5) * MSUN, maxiter=v("maxiter", 10, int), epsiter=v("epsiter", 3.0),

@@ -177,7 +177,7 @@ def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opac
     elif opacity not in ("dhs", "surrogate"):
         raise ValueError("opacity: 'dhs' or 'surrogate'")
     m, run = M.deck_model(ctx, deck, overrides, compute_parts=compute_parts)
-    rad = {k: run[k] for k in ("seed", "randomwalk", "factRW", "maxinteract", "nruns")}
+    rad = {k: run[k] for k in ("seed", "randomwalk", "factRW", "maxinteract", "maxruntime", "nruns")}
     diffused = structure = None
     if run.get("iterate", any(not z[6] for z in run["zones"])):
         # a zone without a fixed structure, or iter=.true.: structure

@@ -144,6 +144,7 @@ typedef struct {
    * 7 overflow kills, 8 cell crossings, 9 escapes */
   int64_t counters[16];
   double tautot;
+  int32_t *Nabs;                 /* ncell: absorption events (may be NULL) */
 } orc_result;
 
 int orc_mcradiation(const orc_model *m, const orc_run *run, orc_result *out);

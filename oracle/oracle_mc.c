@@ -400,6 +400,7 @@ static void interact(mc_t *s, rng_t *r, orc_phot *p) {
   s->out->counters[1]++;
   if (!s->scattering || rnd(r) > Albedo) {
     s->out->counters[2]++;
+    if (s->out->Nabs) s->out->Nabs[c] += 1;
     p->scatt = 0;
     p->pol = 0;
     p->Q = 0.0;
@@ -739,6 +740,7 @@ int orc_mcradiation(const orc_model *m, const orc_run *run, orc_result *out) {
   memset(out->EJv2, 0, sizeof(double) * ncell);
   memset(out->Eabs, 0, sizeof(double) * ncell);
   memset(out->Ni, 0, sizeof(int32_t) * ncell);
+  if (out->Nabs) memset(out->Nabs, 0, sizeof(int32_t) * ncell);
   memset(out->spec, 0, sizeof(double) * nlam * (ORC_NANGLE_SED + 1));
   memset(out->scatspec, 0, sizeof(double) * nlam * (ORC_NANGLE_SED + 1));
   memset(out->ispec, 0, sizeof(int32_t) * nlam * (ORC_NANGLE_SED + 1));

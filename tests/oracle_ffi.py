@@ -45,7 +45,8 @@ class OrcRun(C.Structure):
 
 class OrcResult(C.Structure):
     _fields_ = [("EJv", dp), ("EJv2", dp), ("Eabs", dp), ("T", dp), ("Ni", ip), ("spec", dp),
-                ("scatspec", dp), ("ispec", ip), ("counters", C.c_int64 * 16), ("tautot", C.c_double)]
+                ("scatspec", dp), ("ispec", ip), ("counters", C.c_int64 * 16), ("tautot", C.c_double),
+                ("Nabs", ip)]
 
 
 _lib = None
@@ -231,8 +232,9 @@ def mcradiation(model, nphot, seed=1, randomwalk=False, factRW=10.0, maxinteract
     nc = m.ncell
     ns = m.nlam * 31
     out = dict(EJv=np.zeros(nc), EJv2=np.zeros(nc), Eabs=np.zeros(nc), T=np.zeros(nc), Ni=np.zeros(nc, np.int32),
-               spec=np.zeros(ns), scatspec=np.zeros(ns), ispec=np.zeros(ns, np.int32))
+               spec=np.zeros(ns), scatspec=np.zeros(ns), ispec=np.zeros(ns, np.int32), Nabs=np.zeros(nc, np.int32))
     res = OrcResult(*[P(out[k]) for k in ("EJv", "EJv2", "Eabs", "T", "Ni", "spec", "scatspec", "ispec")])
+    res.Nabs = P(out["Nabs"])
     st = L.orc_mcradiation(C.byref(om), C.byref(run), C.byref(res))
     out["status"] = st
     out["counters"] = np.array(res.counters[:], np.int64)

@@ -153,3 +153,34 @@ def test_settled_mixture_fast_forms_match_reference_order(ctx):
         mg, sg = g.mean(0)[sel], g.std(0, ddof=1)[sel]
         z = np.abs(mr - mg) / (np.sqrt((sr ** 2 + sg ** 2) / 4) + 1e-3 * mr)
         assert np.mean(z < 3) > 0.95, (prec, np.sort(z)[-5:])
+
+
+@pytest.mark.parametrize("prec", ["exact", "fp64", "mixed"])
+def test_absorption_events_per_cell(ctx, prec):
+    """Nabs counts the absorption events of each cell: they add up to the
+    run's absorption counter, and only cells with matter absorb."""
+    m = models.small_disk()
+    ctx.set_model(m)
+    _, g = ctx.mcradiation(5000, seed=21, precision=prec, maxinteract=100000, nruns=2)
+    assert int(g["Nabs"].sum()) == int(g["counters"][2]) > 0
+    star_cells = np.arange(m.ncell) < (m.nt - 1)
+    assert g["Nabs"][star_cells].sum() == 0
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_maxruntime_shrinks_the_run(ctx, prec):
+    """maxruntime (MCRadiation.f:323-342): a run that would take longer
+    starts over with NphotTot (maxruntime / t) (0.5 i / Nphot) packets, and
+    the packets of the run that finished are all accounted for."""
+    m = models.small_disk()
+    ctx.set_model(m)
+    n0 = 4_000_000
+    _, full = ctx.mcradiation(n0, seed=22, precision=prec, maxinteract=100000)
+    limit = full["device_ms"] * 1e-3 / 20.0
+    n, g = ctx.mcradiation(n0, seed=22, precision=prec, maxinteract=100000, maxruntime=limit)
+    assert 10 <= n < n0 // 4, (n, limit)
+    c = g["counters"]
+    assert int(c[9]) + int(c[7]) + int(c[11]) == n
+    # an unlimited run is left alone
+    n2, _ = ctx.mcradiation(20000, seed=23, precision=prec, maxinteract=100000, maxruntime=1e6)
+    assert n2 == 20000

@@ -155,7 +155,7 @@ idum=-7
     zones = run.pop("zones")
     assert zones == [(0.5, 100.0, 0.0707, 1.0, 1.125, 1.0, False)]
     assert abs(run.pop("Mstar") / (2.5 * M.MSUN) - 1) < 1e-15
-    assert run == dict(seed=7, randomwalk=True, factRW=5.0, maxinteract=20000, nruns=1, nphotdiffuse=25,
+    assert run == dict(seed=7, randomwalk=True, factRW=5.0, maxinteract=20000, maxruntime=-1.0, nruns=1, nphotdiffuse=25,
                        dtdiffuse=1.0, maxiter=10, epsiter=3.0, incangle=45.0, outputfits=False, posangle=0.0,
                        iterate=True, thin_start=True, settling=None, vis_norm_fov=True)
     assert np.allclose(m.comp_w.sum(1), 1.0)

@@ -114,7 +114,7 @@ def test_command_line_runs_the_deck_and_writes_result_files(tmp_path):
     ctx = made[0]
     assert ctx.closed
     assert ctx.calls == [dict(nphot=20000, precision="fp64", seed=11, randomwalk=True, factRW=4.0,
-                              maxinteract=5000, nruns=2)]
+                              maxinteract=5000, maxruntime=-1.0, nruns=2)]
     assert ctx.diffuse_args == (7, 25, 1.0, 4.0) and r["diffused"] == (1, 5, 1, 0)
     # a deck with zones starts from three structure passes (a fixed zone's
     # profile rebuilt at the cell centres), as the reference's Init does
