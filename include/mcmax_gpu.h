@@ -230,7 +230,8 @@ typedef struct {
   /* 0 emissions (nemit), 1 interactions, 2 absorptions, 3 scatterings,
    * 4 random-walk steps, 5 star hits, 6 abandoned traces, 7 overflow
    * kills, 8 cell crossings, 9 escapes, 10 averaged-matrix scatterings,
-   * 11 geometry failures; FP64/MIXED forms with the warp scheduler:
+   * 11 geometry failures; FP64/MIXED forms with the warp scheduler, counted
+   * while all 32 lanes of a warp hold packets (the bulk of the run):
    * 12 scheduled warp phases, 13 lanes served by them, 14 warp crossing
    * steps, 15 lanes that crossed in them (13/12 and 15/14 are the mean
    * lanes per phase and per crossing step) */

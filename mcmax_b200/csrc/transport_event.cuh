@@ -188,7 +188,8 @@ __device__ __forceinline__ void fe_deposit(const TAcc &A, size_t off, const FDep
 #endif
 }
 
-/* phase statistics kept in the free counter slots 12..15 */
+/* phase statistics kept in the free counter slots 12..15, counted while all
+ * 32 lanes of the warp hold packets */
 enum { TC_PHASES = 12, TC_PHASE_LANES = 13, TC_XSTEPS = 14, TC_XLANES = 15 };
 
 template <class R>
@@ -260,7 +261,10 @@ __device__ void fe_event_loop(const FModel<R> &m, const TAcc &A, TLocal &L) {
     if (__popc(mS) > best) { kind = FS_SCATTER; best = __popc(mS); }
     if (__popc(mR) > best) { kind = FS_RW; best = __popc(mR); }
     if (__popc(mE) > best) { kind = FS_EMIT; best = __popc(mE); }
-    if (lane == 0) {
+    /* phase statistics of full warps only (every lane holds a packet): the
+     * lane efficiency of the bulk of the run, not of its tail */
+    const bool full = (mE | mR | mT | mA | mS) == FE_FULL;
+    if (lane == 0 && full) {
       L.cnt[TC_PHASES]++;
       L.cnt[TC_PHASE_LANES] += (unsigned)best;
     }
@@ -279,7 +283,7 @@ __device__ void fe_event_loop(const FModel<R> &m, const TAcc &A, TLocal &L) {
           }
         }
         fe_deposit(A, off, d, lane);
-        if (lane == 0) {
+        if (lane == 0 && full) {
           L.cnt[TC_XSTEPS]++;
           L.cnt[TC_XLANES] += (unsigned)__popc(mt);
         }
