@@ -167,6 +167,8 @@ void orc_kp_table(int nlam, const double *nu, const double *BB, int ncomp, const
 void orc_cell_tables(int ncell, int ncomp, int nlam, const double *comp_w, const double *Kabs_comp,
                      const double *Ksca_comp, const double *Kp_comp, double *KabsTot, double *KscaTot,
                      double *KpCell) {
+  /* cells are independent; each keeps the reference's summation order */
+#pragma omp parallel for schedule(static)
   for (int c = 0; c < ncell; ++c) {
     const double *w = comp_w + (size_t)c * ncomp;
     for (int l = 0; l < nlam; ++l) {
