@@ -196,6 +196,7 @@ template <class R>
 __device__ void fe_event_loop(const FModel<R> &m, const TAcc &A, TLocal &L) {
   const int lane = threadIdx.x & 31;
   FPkt<R> p;
+  p.pid1 = 0;
   px_stream rs;
   FTrace t;
   FAbs a;
