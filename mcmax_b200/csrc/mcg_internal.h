@@ -106,6 +106,9 @@ struct DevRun {
   /* absorption events per cell (nruns*ncell) and their sum over runs */
   int *Nabs = nullptr, *NabsTot = nullptr;
   unsigned long long *stop = nullptr; /* maxruntime record, 2 entries */
+  /* per-generation absorbed energies (Fenwick nodes), nruns x ngen x ncell */
+  double *Egen = nullptr;
+  size_t egen_bytes = 0;
   std::vector<void *> owned;
 };
 
@@ -144,6 +147,7 @@ struct RunPrep {
   TAcc ta;
   int nruns = 1;
   size_t nc = 0, ns = 0;
+  size_t egen_bytes = 0;
 };
 
 /* error helpers */

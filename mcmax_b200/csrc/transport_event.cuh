@@ -21,9 +21,13 @@
  * sum.  That is what shortens the tail of a run, where a few trapped
  * packets are alone in their warps.
  *
- * Per-cell deposits of a crossing step (EJv, EJv2) are combined over the
+ * Per-cell deposits of a crossing step (EJv, EJv2) can be combined over the
  * lanes that sit in the same cell (__match_any_sync on the cell) and written
- * with one atomic per cell.  The lastphotnr exchange of a crossing
+ * with one atomic per cell (FE_AGGREGATE=1).  Measured on the precision deck
+ * it does not pay: atomics on the cell accumulators are not contended enough,
+ * and the match and the group sums cost more than they save (the bulk of a
+ * 1e7-packet run is about 10 % faster with plain per-lane atomics), so it is
+ * off by default.  The lastphotnr exchange of a crossing
  * (MCRadiation.f:943-946) is issued at once and its answer read at the
  * packet's next crossing, so its round trip overlaps the next crossing's
  * arithmetic.
@@ -42,7 +46,7 @@
 #endif
 /* 1: combine same-cell deposits of a crossing step within the warp */
 #ifndef FE_AGGREGATE
-#define FE_AGGREGATE 1
+#define FE_AGGREGATE 0
 #endif
 
 /* first i in [0,n) with f(i) >= v (ge) or f(i) > v, n when none; f is
@@ -201,6 +205,7 @@ __device__ void fe_event_loop(const FModel<R> &m, const TAcc &A, TLocal &L) {
   FTrace t;
   FAbs a;
   size_t off = 0;
+  int gen = 0;
   int st = FS_NEW;
   int pend_c = -1, pend_prev = 0; /* lastphotnr exchange in flight */
   const int n1 = m.nlam - 1;
@@ -240,6 +245,7 @@ __device__ void fe_event_loop(const FModel<R> &m, const TAcc &A, TLocal &L) {
         } else {
           const int64_t pid = (int64_t)k + m.pid0;
           off = f_run_off(A, pid);
+          gen = f_generation(A, pid);
           px_init(&rs, m.seed, (uint64_t)pid);
           f_packet_init<R>(p, pid);
           st = FS_EMIT;
@@ -315,7 +321,7 @@ __device__ void fe_event_loop(const FModel<R> &m, const TAcc &A, TLocal &L) {
       }
     } else if (kind == FS_ABSORB) {
       const bool me = st == FS_ABSORB;
-      if (me) f_absorb_pre<R>(m, A, off, &rs, p, L, a);
+      if (me) f_absorb_pre<R>(m, A, off, gen, &rs, p, L, a);
       if (m.uniform_mix && __popc(mA) > FE_COOP_MAX) {
         if (me) f_absorb_search<R>(m, p, a);
       } else {
@@ -387,7 +393,7 @@ __device__ void fe_event_loop(const FModel<R> &m, const TAcc &A, TLocal &L) {
       }
     } else if (kind == FS_RW) {
       if (st == FS_RW) {
-        if (f_random_walk<R>(m, A, off, &rs, p, L))
+        if (f_random_walk<R>(m, A, off, gen, &rs, p, L))
           f_rw_redirect<R>(&rs, p);
         else
           st = FS_TRACE;

@@ -484,6 +484,8 @@ TP_FN void f_apply_dep(const TAcc &A, size_t off, const FDep &d, int pid1) {
 
 /* accumulator offset of the sub-run packet pid belongs to (nruns) */
 TP_FN size_t f_run_off(const TAcc &A, int64_t pid) { return (size_t)(pid / A.run_packets) * (size_t)A.ncell; }
+/* generation of packet pid (TAcc.ngen) */
+TP_FN int f_generation(const TAcc &A, int64_t pid) { return tp_generation(A, pid); }
 
 template <class R>
 TP_FN void f_packet_init(FPkt<R> &p, int64_t pid) {
@@ -679,8 +681,8 @@ struct FAbs {
 };
 
 template <class R>
-F_COLD void f_absorb_pre(const FModel<R> &m, const TAcc &A, size_t off, px_stream *r, FPkt<R> &p, TLocal &L,
-                         FAbs &a) {
+F_COLD void f_absorb_pre(const FModel<R> &m, const TAcc &A, size_t off, int gen, px_stream *r, FPkt<R> &p,
+                         TLocal &L, FAbs &a) {
   const int c = p.i * m.nc + (p.j - 1);
   L.cnt[TC_ABSORB]++;
   if (A.Nabs) tp_addi(&A.Nabs[off + c], 1);
@@ -689,7 +691,7 @@ F_COLD void f_absorb_pre(const FModel<R> &m, const TAcc &A, size_t off, px_strea
   p.q = p.u = p.v = (R)0;
   const double *kp = m.KpCell + (m.uniform_mix ? (size_t)0 : (size_t)c * TP_TT);
   const double dE = p.E;
-  const double Eold = tp_add(&A.Eabs[off + c], dE);
+  const double Eold = tp_eabs_add(A, off, gen, c, dE);
   const double mass = m.mass[c];
   int hint = A.kp_hint[off + c];
   int ib0, ib1;
@@ -935,7 +937,8 @@ TP_FN int f_after_interact(const FModel<R> &m, px_stream *r, FPkt<R> &p, FTrace 
 /* one jump of the modified random walk (RandomWalk.f:15-147); returns 1
  * when the packet jumped (then a new outward direction follows) */
 template <class R>
-F_COLD int f_random_walk(const FModel<R> &m, const TAcc &A, size_t off, px_stream *r, FPkt<R> &p, TLocal &L) {
+F_COLD int f_random_walk(const FModel<R> &m, const TAcc &A, size_t off, int gen, px_stream *r, FPkt<R> &p,
+                         TLocal &L) {
   const int c = p.i * m.nc + (p.j - 1);
   /* distance to the nearest face (MinDist, RandomWalk.f:15-43) */
   double rho = p.x * p.x + p.y * p.y;
@@ -973,7 +976,7 @@ F_COLD int f_random_walk(const FModel<R> &m, const TAcc &A, size_t off, px_strea
   p.z += dmin * p.vz;
   const double EJv = (p.E * v) * TP_AU;
   const double dEa = (EJv * Kabs) * m.dens[c];
-  const double Eold = tp_add(&A.Eabs[off + c], dEa);
+  const double Eold = tp_eabs_add(A, off, gen, c, dEa);
   tp_add(&A.EJv[off + c], EJv * Kabs);
   p.nEJv += EJv * Kabs;
   const double *kp = m.KpCell + (m.uniform_mix ? (size_t)0 : (size_t)c * TP_TT);
@@ -996,57 +999,78 @@ TP_FN void f_rw_redirect(px_stream *r, FPkt<R> &p) {
 }
 
 /* ------------------------------------------------------------- one packet */
-/* All events of one packet back to back, accumulators updated directly:
- * the host replay of the device code and the batched kernel. */
+/* One packet as a state machine: f_slot_start sets it up, f_slot_step
+ * advances it by one event (accumulators updated directly) and returns 1
+ * when the packet has ended. */
+template <class R>
+struct FSlot {
+  FPkt<R> p;
+  px_stream rs;
+  FTrace t;
+  size_t off;
+  int gen, st;
+};
+
+template <class R>
+TP_FN void f_slot_start(const FModel<R> &m, const TAcc &A, FSlot<R> &s, int64_t pid) {
+  s.off = f_run_off(A, pid);
+  s.gen = f_generation(A, pid);
+  px_init(&s.rs, m.seed, (uint64_t)pid);
+  f_packet_init<R>(s.p, pid);
+  s.st = FS_EMIT;
+}
+
+template <class R>
+TP_FN int f_slot_step(const FModel<R> &m, const TAcc &A, FSlot<R> &s, TLocal &L) {
+  FPkt<R> &p = s.p;
+  px_stream *r = &s.rs;
+  if (s.st == FS_EMIT) {
+    f_emit_star<R>(m, r, p, s.t, L);
+    s.st = FS_TRACE; /* on the star's surface: never inside a thick cell */
+  } else if (s.st == FS_RW) {
+    if (f_random_walk<R>(m, A, s.off, s.gen, r, p, L))
+      f_rw_redirect<R>(r, p);
+    else
+      s.st = FS_TRACE;
+  } else if (s.st == FS_TRACE) {
+    FDep d;
+    const int o = f_cross<R>(m, A, s.off, p, s.t, L, d);
+    f_apply_dep(A, s.off, d, p.pid1);
+    if (o == FX_INSIDE) {
+      s.st = f_albedo<R>(m, r, p, L);
+    } else if (o == FX_ESCAPE) {
+      f_escape<R>(m, A, p, L);
+      return 1;
+    } else if (o == FX_STAR) {
+      L.cnt[TC_HITSTAR]++;
+      s.st = FS_EMIT;
+    } else if (o == FX_GEOFAIL) {
+      L.cnt[TC_GEOFAIL]++;
+      return 1;
+    }
+  } else {
+    if (s.st == FS_ABSORB) {
+      FAbs a;
+      f_absorb_pre<R>(m, A, s.off, s.gen, r, p, L, a);
+      f_absorb_search<R>(m, p, a);
+      f_absorb_post<R>(m, A, s.off, p, a);
+    } else {
+      R KscaR;
+      if (f_scatter_pre<R>(m, r, p, L, &KscaR) > 0) f_scatter_post<R>(m, r, p, L, f_scatter_pick<R>(m, p, KscaR));
+    }
+    if (!f_after_interact<R>(m, r, p, s.t, L)) return 1;
+    s.st = f_trace_state<R>(m, p);
+  }
+  return 0;
+}
+
+/* All events of one packet back to back: the host replay of the device code
+ * and the batched kernel. */
 template <class R>
 TP_FN void f_run_packet(const FModel<R> &m, const TAcc &A, int64_t pid, TLocal &L) {
-  const size_t off = f_run_off(A, pid);
-  px_stream rs;
-  px_init(&rs, m.seed, (uint64_t)pid);
-  px_stream *r = &rs;
-  FPkt<R> p;
-  f_packet_init<R>(p, pid);
-  FTrace t;
-  int st = FS_EMIT;
-  for (;;) {
-    if (st == FS_EMIT) {
-      f_emit_star<R>(m, r, p, t, L);
-      st = FS_TRACE; /* on the star's surface: never inside a thick cell */
-    } else if (st == FS_RW) {
-      if (f_random_walk<R>(m, A, off, r, p, L))
-        f_rw_redirect<R>(r, p);
-      else
-        st = FS_TRACE;
-    } else if (st == FS_TRACE) {
-      FDep d;
-      const int o = f_cross<R>(m, A, off, p, t, L, d);
-      f_apply_dep(A, off, d, p.pid1);
-      if (o == FX_CONT) continue;
-      if (o == FX_INSIDE) {
-        st = f_albedo<R>(m, r, p, L);
-      } else if (o == FX_ESCAPE) {
-        f_escape<R>(m, A, p, L);
-        return;
-      } else if (o == FX_STAR) {
-        L.cnt[TC_HITSTAR]++;
-        st = FS_EMIT;
-      } else {
-        L.cnt[TC_GEOFAIL]++;
-        return;
-      }
-    } else {
-      if (st == FS_ABSORB) {
-        FAbs a;
-        f_absorb_pre<R>(m, A, off, r, p, L, a);
-        f_absorb_search<R>(m, p, a);
-        f_absorb_post<R>(m, A, off, p, a);
-      } else {
-        R KscaR;
-        if (f_scatter_pre<R>(m, r, p, L, &KscaR) > 0) f_scatter_post<R>(m, r, p, L, f_scatter_pick<R>(m, p, KscaR));
-      }
-      if (!f_after_interact<R>(m, r, p, t, L)) return;
-      st = f_trace_state<R>(m, p);
-    }
+  FSlot<R> s;
+  f_slot_start<R>(m, A, s, pid);
+  while (!f_slot_step<R>(m, A, s, L)) {
   }
 }
 

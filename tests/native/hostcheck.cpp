@@ -165,7 +165,8 @@ double hc_tinv(const double *kp, double E1, int lo) {
 
 template <class R>
 static int hc_fast_impl(const HcModel *h, double *EJv, double *EJv2, double *Eabs, double *T, int *Ni,
-                        double *spec, unsigned long long *counters, double *tautot, int64_t first, int64_t count) {
+                        double *spec, unsigned long long *counters, double *tautot, int64_t first, int64_t count,
+                        int inflight = 1, int ngen = 1, int *Nabs = nullptr) {
   const int nc = h->nt - 1, ncell = h->nr * nc, nlam = h->nlam, n = nlam - 1, ncomp = h->ncomp;
   std::vector<double> dens(ncell), mass(ncell), dnu(n), star_cdf(n), wlam(nlam);
   for (int c = 0; c < ncell; ++c) {
@@ -285,9 +286,45 @@ static int hc_fast_impl(const HcModel *h, double *EJv, double *EJv2, double *Eab
   Ac.kp_hint = kp_hint.data(); Ac.spec = spec; Ac.scatspec = scatspec.data(); Ac.ispec = ispec.data();
   Ac.counters = counters; Ac.tautot = tautot; Ac.next = &next; Ac.run_packets = h->nphot; Ac.ncell = ncell;
   Ac.done = &done; Ac.tmark = tmark;
+  Ac.Nabs = Nabs;
+  std::vector<double> egen;
+  if (ngen > 1) {
+    egen.assign((size_t)ngen * ncell, 0.0);
+    Ac.ngen = ngen;
+    Ac.gen_packets = (h->nphot + ngen - 1) / ngen;
+    Ac.Egen = egen.data();
+  }
   TLocal L;
   memset(&L, 0, sizeof L);
-  for (int64_t pid = first; pid < first + count; ++pid) f_run_packet<R>(m, Ac, pid, L);
+  if (inflight <= 1) {
+    for (int64_t pid = first; pid < first + count; ++pid) f_run_packet<R>(m, Ac, pid, L);
+  } else {
+    /* `inflight` packets at once, each advanced by one event in turn: the
+     * cell energies a packet sees include the deposits of packets started
+     * after it, as on the GPU */
+    std::vector<FSlot<R>> slots(inflight);
+    std::vector<char> live(inflight, 0);
+    int64_t next_pid = first;
+    const int64_t end = first + count;
+    int nlive = 0;
+    for (int k = 0; k < inflight && next_pid < end; ++k, ++nlive) {
+      f_slot_start<R>(m, Ac, slots[k], next_pid++);
+      live[k] = 1;
+    }
+    while (nlive > 0) {
+      for (int k = 0; k < inflight; ++k) {
+        if (!live[k]) continue;
+        if (f_slot_step<R>(m, Ac, slots[k], L)) {
+          if (next_pid < end) {
+            f_slot_start<R>(m, Ac, slots[k], next_pid++);
+          } else {
+            live[k] = 0;
+            --nlive;
+          }
+        }
+      }
+    }
+  }
   for (int k = 0; k < TC_N; ++k) counters[k] += (unsigned long long)L.cnt[k];
   *tautot += L.tautot;
   return 0;
@@ -297,6 +334,17 @@ extern "C" int hc_fast(const HcModel *h, int mixed, double *EJv, double *EJv2, d
                        double *spec, unsigned long long *counters, double *tautot, int64_t first, int64_t count) {
   if (mixed) return hc_fast_impl<float>(h, EJv, EJv2, Eabs, T, Ni, spec, counters, tautot, first, count);
   return hc_fast_impl<double>(h, EJv, EJv2, Eabs, T, Ni, spec, counters, tautot, first, count);
+}
+
+/* the GPU-ordered kernel with `inflight` packets interleaved event by event
+ * and `ngen` packet generations (the concurrency of the device launch,
+ * emulated in one host thread); Nabs per cell */
+extern "C" int hc_fast_interleaved(const HcModel *h, int mixed, double *EJv, double *EJv2, double *Eabs, double *T,
+                                   int *Ni, double *spec, unsigned long long *counters, double *tautot,
+                                   int inflight, int ngen, int *Nabs) {
+  if (mixed)
+    return hc_fast_impl<float>(h, EJv, EJv2, Eabs, T, Ni, spec, counters, tautot, 0, h->nphot, inflight, ngen, Nabs);
+  return hc_fast_impl<double>(h, EJv, EJv2, Eabs, T, Ni, spec, counters, tautot, 0, h->nphot, inflight, ngen, Nabs);
 }
 
 /* Diffuse on the host: the host logic of mcg_diffuse with a backend of
