@@ -202,8 +202,15 @@ typedef struct {
                              launch, each with its own accumulators, and are
                              averaged as the reference does */
   int precision;          /* mcg_precision */
-  int threads;            /* 0: persistent grid; n > 0: exactly n threads
-                             (1 reproduces the serial packet order) */
+  int threads;            /* 0: persistent grid of at most one thread per
+                             1333 packets of the run (at least 256), which
+                             keeps the results within the Monte Carlo noise
+                             of the reference's serial packet order (a
+                             packet's Bjorkman-Wood re-emissions see the
+                             cell temperatures of the packets in flight with
+                             it); n > 0: exactly n threads, rounded up to
+                             whole blocks (1 reproduces the serial packet
+                             order) */
   int block;              /* threads per block: 0 = default (256), else a
                              multiple of 32 up to 256 */
   double maxruntime;      /* keyword 'maxruntime' (Init.f:1094, default -1 =

@@ -106,9 +106,6 @@ struct DevRun {
   /* absorption events per cell (nruns*ncell) and their sum over runs */
   int *Nabs = nullptr, *NabsTot = nullptr;
   unsigned long long *stop = nullptr; /* maxruntime record, 2 entries */
-  /* per-generation absorbed energies (Fenwick nodes), nruns x ngen x ncell */
-  double *Egen = nullptr;
-  size_t egen_bytes = 0;
   std::vector<void *> owned;
 };
 
@@ -142,12 +139,28 @@ struct mcg_ctx {
 /* kernel arguments of one prepared run: the model tables and accumulators
  * as the transport kernels see them (transport_core.cuh) */
 #include "transport_core.cuh"
+/* Packets in flight of a run launched with threads = 0: at most one thread
+ * per MCG_PACKETS_PER_THREAD packets (and at least MCG_MIN_THREADS).  The
+ * Bjorkman-Wood re-emission of a packet uses the cell temperatures of the
+ * moment; in the reference's serial order a packet's whole life happens
+ * between two others, while in parallel a packet trapped in an optically
+ * thick cell sees the cell heated by the packets that run meanwhile.  The
+ * results depart from the serial order in proportion to the share of the
+ * run that is in flight at once; at one packet in flight per 1333 the
+ * per-cell temperatures agree with the serial CPU run within its Monte Carlo
+ * noise.  Large runs (1e8 packets) fill the GPU anyway. */
+#define MCG_PACKETS_PER_THREAD 1333
+#define MCG_MIN_THREADS 256
+inline long long mcg_default_threads(long long nphot) {
+  long long t = nphot / MCG_PACKETS_PER_THREAD;
+  return t < MCG_MIN_THREADS ? MCG_MIN_THREADS : t;
+}
+
 struct RunPrep {
   TModel tm;
   TAcc ta;
   int nruns = 1;
   size_t nc = 0, ns = 0;
-  size_t egen_bytes = 0;
 };
 
 /* error helpers */

@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -629,18 +630,6 @@ __global__ static void combine_runs_kernel(int nc, int nruns, const double *EJv,
   NabsTot[c] = na;
 }
 
-/* packet generations of a parallel run (TAcc.ngen): a packet's
- * Bjorkman-Wood temperatures come from the cell energy of its own and
- * earlier generations, as in the reference's serial order; 256 generations
- * keep what a packet can see of later packets under 0.4 % of the run.  The
- * one-thread serial launch needs none (the packet order is the reference's). */
-static int run_generations(const mcg_run *run, int64_t per_run) {
-  if (run->threads == 1) return 1;
-  int64_t g = 256;
-  if (g > per_run) g = per_run;
-  return g < 1 ? 1 : (int)g;
-}
-
 /* validation, run buffers and tables, zeroed accumulators and the kernel
  * arguments of one run of the current model (ctx->model / ctx->run) */
 mcg_status mcg_run_prepare(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot, RunPrep *rp, bool zero) {
@@ -669,24 +658,6 @@ mcg_status mcg_run_prepare(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot, Run
   rp->nruns = nruns;
   rp->nc = nc;
   rp->ns = ns;
-  const int ngen = run_generations(run, Nphot);
-  {
-    const size_t need = ngen > 1 ? sizeof(double) * nb * (size_t)ngen : 0;
-    if (need > R.egen_bytes) {
-      for (void *&q : R.owned)
-        if (q == (void *)R.Egen) {
-          cudaFree(q);
-          q = nullptr;
-        }
-      R.Egen = nullptr;
-      R.egen_bytes = 0;
-      cudaError_t e = cudaMalloc(&R.Egen, need);
-      if (e != cudaSuccess) return mcg_fail(ctx, MCG_ERR_NOMEM, "run buffers: %s", cudaGetErrorString(e));
-      R.owned.push_back(R.Egen);
-      R.egen_bytes = need;
-    }
-    rp->egen_bytes = need;
-  }
   if (zero) MCG_CUDA(ctx, mcg_run_zero(ctx, nb, ns));
 
   TModel &tm = rp->tm;
@@ -723,9 +694,6 @@ mcg_status mcg_run_prepare(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot, Run
   ta.tmark = R.tmark;
   ta.Nabs = R.Nabs;
   ta.stop = R.stop;
-  ta.ngen = ngen;
-  ta.gen_packets = (Nphot + ngen - 1) / ngen;
-  ta.Egen = ngen > 1 ? R.Egen : nullptr;
   {
     const unsigned long long tot = (unsigned long long)(Nphot * nruns);
     const double f[5] = {0.5, 0.9, 0.99, 0.999, 1.0};
@@ -752,7 +720,6 @@ cudaError_t mcg_run_zero(mcg_ctx *ctx, size_t nb, size_t ns) {
   if (e == cudaSuccess) e = cudaMemsetAsync(R.kp_hint, 0, nb * 4, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(R.Nabs, 0, nb * 4, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(R.stop, 0, 2 * 8, st);
-  if (e == cudaSuccess && R.Egen && R.egen_bytes) e = cudaMemsetAsync(R.Egen, 0, R.egen_bytes, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(R.spec, 0, ns * 8, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(R.scatspec, 0, ns * 8, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(R.ispec, 0, ns * 4, st);
@@ -842,6 +809,8 @@ static mcg_status mcg_mcradiation_once(mcg_ctx *ctx, const mcg_run *run, int64_t
       int per_sm = 0;
       MCG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, transport_fp64_kernel, block, 0));
       grid = ctx->sm_count * std::max(per_sm, 1);
+      const long long cap = (mcg_default_threads(tm.nphot) + block - 1) / block;
+      if (cap < grid) grid = (int)cap;
     }
     MCG_CUDA(ctx, cudaEventRecord(ctx->ev0, st));
     if (run->threads == 1)

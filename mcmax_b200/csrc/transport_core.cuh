@@ -103,19 +103,6 @@ struct TAcc {
   int *Nabs;                /* absorption events per cell (may be null) */
   unsigned long long *stop; /* maxruntime: [0] packets started when the run
                                stopped (0: running), [1] elapsed ns then */
-  /* Generations of packets (ngen > 1).  The serial reference processes
-   * packet k after packets 0..k-1 have ended, so the cell temperatures a
-   * packet's Bjorkman-Wood re-emissions use hold no energy of later packets.
-   * Run in parallel, a packet trapped in an optically thick cell lives while
-   * many later packets heat that cell, and re-emits from a hotter cell than
-   * it would in the serial order.  The packets of a sub-run are therefore
-   * numbered into ngen generations of gen_packets consecutive ids, and each
-   * cell's absorbed energy is also kept per generation (a Fenwick tree of
-   * ngen nodes per cell, Egen): a packet's temperatures come from the
-   * energy of its own and earlier generations only. */
-  int ngen;
-  int64_t gen_packets;
-  double *Egen;             /* nruns x ngen x ncell */
 };
 
 /* accumulators of the run that packet pid belongs to */
@@ -130,15 +117,7 @@ TP_FN TAcc tp_run_acc(const TAcc &A, int64_t pid) {
   R.lastphot += off;
   R.kp_hint += off;
   if (R.Nabs) R.Nabs += off;
-  if (R.Egen) R.Egen += off * (size_t)(R.ngen > 1 ? R.ngen : 1);
   return R;
-}
-
-/* generation of packet pid within its sub-run */
-TP_FN int tp_generation(const TAcc &A, int64_t pid) {
-  if (A.ngen <= 1) return 0;
-  const int g = (int)((pid % A.run_packets) / A.gen_packets);
-  return g < A.ngen ? g : A.ngen - 1;
 }
 
 TP_FN unsigned long long tp_globaltimer() {
@@ -206,32 +185,6 @@ TP_FN void tp_addi(int *p, int v) {
   *p += v;
 #endif
 }
-/* a value other threads update with atomics, read from L2 (not a stale L1
- * line) */
-TP_FN double tp_load_cg(const double *p) {
-#if defined(__CUDA_ARCH__)
-  return __ldcg(p);
-#else
-  return *p;
-#endif
-}
-
-/* Deposit dE into cell c (accumulators E already offset to the sub-run) for
- * a packet of generation g; returns the cell's absorbed energy before the
- * deposit as that packet's generation sees it (the plain Eabs with one
- * generation).  The plain Eabs total is kept up to date either way. */
-TP_FN double tp_eabs_add(const TAcc &A, size_t off, int g, int c, double dE) {
-  if (A.ngen <= 1 || !A.Egen) return tp_add(&A.Eabs[off + c], dE);
-  const size_t nc = (size_t)A.ncell;
-  double *E = A.Egen + off * (size_t)A.ngen;
-  const int k = g + 1;
-  double old = tp_add(&E[(size_t)(k - 1) * nc + c], dE);
-  for (int j = k - (k & -k); j > 0; j -= j & -j) old += tp_load_cg(&E[(size_t)(j - 1) * nc + c]);
-  for (int j = k + (k & -k); j <= A.ngen; j += j & -j) tp_add(&E[(size_t)(j - 1) * nc + c], dE);
-  tp_add(&A.Eabs[off + c], dE);
-  return old;
-}
-
 TP_FN int tp_exch(int *p, int v) {
 #if defined(__CUDA_ARCH__)
   return atomicExch(p, v);
@@ -251,7 +204,6 @@ struct TPkt {
   int ilam1, ilam2, i, j, edgeNr;
   int onEdge, scatt, pol;
   int pid1; /* packet number + 1 (lastphotnr) */
-  int gen;  /* generation of the packet (TAcc.ngen) */
 };
 
 struct TLocal {
@@ -681,7 +633,7 @@ TP_FN void tp_interact(const TModel &m, const TAcc &A, px_stream *r, TPkt &p, TL
     p.V = 0.0;
     const double *kp = m.KpCell + (m.uniform_mix ? (size_t)0 : (size_t)c * TP_TT);
     const double dE = (p.E * (KabsTot - 0.0)) / KabsTot;
-    const double Eold = tp_eabs_add(A, 0, p.gen, c, dE);
+    const double Eold = tp_add(&A.Eabs[c], dE);
     const double Enew = Eold + dE;
     const double mass = m.mass[c];
     int ib0, ib1;
@@ -893,7 +845,7 @@ TP_FN int tp_random_walk(const TModel &m, const TAcc &A, px_stream *r, TPkt &p, 
   p.z = p.z + dmin * p.vz;
   const double EJv = (p.E * v) * TP_AU;
   const double dEa = (EJv * Kabs) * m.dens[c];
-  const double Eold = tp_eabs_add(A, 0, p.gen, c, dEa);
+  const double Eold = tp_add(&A.Eabs[c], dEa);
   tp_add(&A.EJv[c], EJv * Kabs);
   p.nEJv = p.nEJv + EJv * Kabs;
   const double *kp = m.KpCell + (m.uniform_mix ? (size_t)0 : (size_t)c * TP_TT);
@@ -986,7 +938,6 @@ TP_FN void tp_run_packet(const TModel &m, const TAcc &A0, int64_t pid, TLocal &L
   px_stream *r = &rs;
   TPkt p;
   p.pid1 = (int)(pid + 1);
-  p.gen = tp_generation(A0, pid);
   p.Q = p.U = p.V = 0.0;
   p.pol = 0;
   p.scatt = 0;

@@ -205,7 +205,6 @@ __device__ void fe_event_loop(const FModel<R> &m, const TAcc &A, TLocal &L) {
   FTrace t;
   FAbs a;
   size_t off = 0;
-  int gen = 0;
   int st = FS_NEW;
   int pend_c = -1, pend_prev = 0; /* lastphotnr exchange in flight */
   const int n1 = m.nlam - 1;
@@ -245,7 +244,6 @@ __device__ void fe_event_loop(const FModel<R> &m, const TAcc &A, TLocal &L) {
         } else {
           const int64_t pid = (int64_t)k + m.pid0;
           off = f_run_off(A, pid);
-          gen = f_generation(A, pid);
           px_init(&rs, m.seed, (uint64_t)pid);
           f_packet_init<R>(p, pid);
           st = FS_EMIT;
@@ -321,7 +319,7 @@ __device__ void fe_event_loop(const FModel<R> &m, const TAcc &A, TLocal &L) {
       }
     } else if (kind == FS_ABSORB) {
       const bool me = st == FS_ABSORB;
-      if (me) f_absorb_pre<R>(m, A, off, gen, &rs, p, L, a);
+      if (me) f_absorb_pre<R>(m, A, off, &rs, p, L, a);
       if (m.uniform_mix && __popc(mA) > FE_COOP_MAX) {
         if (me) f_absorb_search<R>(m, p, a);
       } else {
@@ -393,7 +391,7 @@ __device__ void fe_event_loop(const FModel<R> &m, const TAcc &A, TLocal &L) {
       }
     } else if (kind == FS_RW) {
       if (st == FS_RW) {
-        if (f_random_walk<R>(m, A, off, gen, &rs, p, L))
+        if (f_random_walk<R>(m, A, off, &rs, p, L))
           f_rw_redirect<R>(&rs, p);
         else
           st = FS_TRACE;

@@ -327,6 +327,8 @@ mcg_status launch_fast(mcg_ctx *ctx, int pi, const TModel &tm, const TAcc &ta, i
     int per_sm = 0;
     MCG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, b, sp.bytes));
     grid = ctx->sm_count * std::max(per_sm, 1);
+    const long long cap = (mcg_default_threads(tm.nphot) + b - 1) / b;
+    if (cap < grid) grid = (int)cap;
   }
   MCG_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
   if (threads == 1)

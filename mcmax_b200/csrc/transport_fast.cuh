@@ -484,8 +484,6 @@ TP_FN void f_apply_dep(const TAcc &A, size_t off, const FDep &d, int pid1) {
 
 /* accumulator offset of the sub-run packet pid belongs to (nruns) */
 TP_FN size_t f_run_off(const TAcc &A, int64_t pid) { return (size_t)(pid / A.run_packets) * (size_t)A.ncell; }
-/* generation of packet pid (TAcc.ngen) */
-TP_FN int f_generation(const TAcc &A, int64_t pid) { return tp_generation(A, pid); }
 
 template <class R>
 TP_FN void f_packet_init(FPkt<R> &p, int64_t pid) {
@@ -681,8 +679,8 @@ struct FAbs {
 };
 
 template <class R>
-F_COLD void f_absorb_pre(const FModel<R> &m, const TAcc &A, size_t off, int gen, px_stream *r, FPkt<R> &p,
-                         TLocal &L, FAbs &a) {
+F_COLD void f_absorb_pre(const FModel<R> &m, const TAcc &A, size_t off, px_stream *r, FPkt<R> &p, TLocal &L,
+                         FAbs &a) {
   const int c = p.i * m.nc + (p.j - 1);
   L.cnt[TC_ABSORB]++;
   if (A.Nabs) tp_addi(&A.Nabs[off + c], 1);
@@ -691,7 +689,7 @@ F_COLD void f_absorb_pre(const FModel<R> &m, const TAcc &A, size_t off, int gen,
   p.q = p.u = p.v = (R)0;
   const double *kp = m.KpCell + (m.uniform_mix ? (size_t)0 : (size_t)c * TP_TT);
   const double dE = p.E;
-  const double Eold = tp_eabs_add(A, off, gen, c, dE);
+  const double Eold = tp_add(&A.Eabs[off + c], dE);
   const double mass = m.mass[c];
   int hint = A.kp_hint[off + c];
   int ib0, ib1;
@@ -937,8 +935,7 @@ TP_FN int f_after_interact(const FModel<R> &m, px_stream *r, FPkt<R> &p, FTrace 
 /* one jump of the modified random walk (RandomWalk.f:15-147); returns 1
  * when the packet jumped (then a new outward direction follows) */
 template <class R>
-F_COLD int f_random_walk(const FModel<R> &m, const TAcc &A, size_t off, int gen, px_stream *r, FPkt<R> &p,
-                         TLocal &L) {
+F_COLD int f_random_walk(const FModel<R> &m, const TAcc &A, size_t off, px_stream *r, FPkt<R> &p, TLocal &L) {
   const int c = p.i * m.nc + (p.j - 1);
   /* distance to the nearest face (MinDist, RandomWalk.f:15-43) */
   double rho = p.x * p.x + p.y * p.y;
@@ -976,7 +973,7 @@ F_COLD int f_random_walk(const FModel<R> &m, const TAcc &A, size_t off, int gen,
   p.z += dmin * p.vz;
   const double EJv = (p.E * v) * TP_AU;
   const double dEa = (EJv * Kabs) * m.dens[c];
-  const double Eold = tp_eabs_add(A, off, gen, c, dEa);
+  const double Eold = tp_add(&A.Eabs[off + c], dEa);
   tp_add(&A.EJv[off + c], EJv * Kabs);
   p.nEJv += EJv * Kabs;
   const double *kp = m.KpCell + (m.uniform_mix ? (size_t)0 : (size_t)c * TP_TT);
@@ -1008,13 +1005,12 @@ struct FSlot {
   px_stream rs;
   FTrace t;
   size_t off;
-  int gen, st;
+  int st;
 };
 
 template <class R>
 TP_FN void f_slot_start(const FModel<R> &m, const TAcc &A, FSlot<R> &s, int64_t pid) {
   s.off = f_run_off(A, pid);
-  s.gen = f_generation(A, pid);
   px_init(&s.rs, m.seed, (uint64_t)pid);
   f_packet_init<R>(s.p, pid);
   s.st = FS_EMIT;
@@ -1028,7 +1024,7 @@ TP_FN int f_slot_step(const FModel<R> &m, const TAcc &A, FSlot<R> &s, TLocal &L)
     f_emit_star<R>(m, r, p, s.t, L);
     s.st = FS_TRACE; /* on the star's surface: never inside a thick cell */
   } else if (s.st == FS_RW) {
-    if (f_random_walk<R>(m, A, s.off, s.gen, r, p, L))
+    if (f_random_walk<R>(m, A, s.off, r, p, L))
       f_rw_redirect<R>(r, p);
     else
       s.st = FS_TRACE;
@@ -1051,7 +1047,7 @@ TP_FN int f_slot_step(const FModel<R> &m, const TAcc &A, FSlot<R> &s, TLocal &L)
   } else {
     if (s.st == FS_ABSORB) {
       FAbs a;
-      f_absorb_pre<R>(m, A, s.off, s.gen, r, p, L, a);
+      f_absorb_pre<R>(m, A, s.off, r, p, L, a);
       f_absorb_search<R>(m, p, a);
       f_absorb_post<R>(m, A, s.off, p, a);
     } else {

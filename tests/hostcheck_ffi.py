@@ -58,12 +58,12 @@ def mie_sample(rad, lam, e1, e2):
 
 
 def mcradiation(model, tables, nphot, seed=1, randomwalk=False, factRW=10.0, maxinteract=0, fast=None, first=0,
-                count=None, inflight=1, ngen=1):
+                count=None, inflight=1):
     """Serial host replay of the device packet loop.  fast=None: the
     reference-order kernel; fast='fp64' / 'mixed': the GPU-ordered kernel
     (uniform mixtures), packets [first, first+count); with inflight > 1 that
     many packets advance one event at a time in turn (a GPU launch's
-    concurrency), with ngen packet generations."""
+    concurrency)."""
     L = load()
     m, t = model, tables
     keep = {}
@@ -89,10 +89,10 @@ def mcradiation(model, tables, nphot, seed=1, randomwalk=False, factRW=10.0, max
                spec=np.zeros(ns), scatspec=np.zeros(ns), ispec=np.zeros(ns, np.int32), Nabs=np.zeros(nc, np.int32))
     cnt = (C.c_ulonglong * 16)()
     tau = C.c_double(0.0)
-    if fast is not None and (inflight > 1 or ngen > 1):
+    if fast is not None and inflight > 1:
         L.hc_fast_interleaved(C.byref(h), int(fast == "mixed"),
                               *[P(out[k]) for k in ("EJv", "EJv2", "Eabs", "T", "Ni", "spec")], cnt, C.byref(tau),
-                              int(inflight), int(ngen), P(out["Nabs"]))
+                              int(inflight), P(out["Nabs"]))
     elif fast is None:
         L.hc_mcradiation(C.byref(h), *[P(out[k]) for k in ("EJv", "EJv2", "Eabs", "T", "Ni", "spec", "scatspec",
                                                            "ispec")], cnt, C.byref(tau))

@@ -166,7 +166,7 @@ double hc_tinv(const double *kp, double E1, int lo) {
 template <class R>
 static int hc_fast_impl(const HcModel *h, double *EJv, double *EJv2, double *Eabs, double *T, int *Ni,
                         double *spec, unsigned long long *counters, double *tautot, int64_t first, int64_t count,
-                        int inflight = 1, int ngen = 1, int *Nabs = nullptr) {
+                        int inflight = 1, int *Nabs = nullptr) {
   const int nc = h->nt - 1, ncell = h->nr * nc, nlam = h->nlam, n = nlam - 1, ncomp = h->ncomp;
   std::vector<double> dens(ncell), mass(ncell), dnu(n), star_cdf(n), wlam(nlam);
   for (int c = 0; c < ncell; ++c) {
@@ -287,13 +287,6 @@ static int hc_fast_impl(const HcModel *h, double *EJv, double *EJv2, double *Eab
   Ac.counters = counters; Ac.tautot = tautot; Ac.next = &next; Ac.run_packets = h->nphot; Ac.ncell = ncell;
   Ac.done = &done; Ac.tmark = tmark;
   Ac.Nabs = Nabs;
-  std::vector<double> egen;
-  if (ngen > 1) {
-    egen.assign((size_t)ngen * ncell, 0.0);
-    Ac.ngen = ngen;
-    Ac.gen_packets = (h->nphot + ngen - 1) / ngen;
-    Ac.Egen = egen.data();
-  }
   TLocal L;
   memset(&L, 0, sizeof L);
   if (inflight <= 1) {
@@ -337,14 +330,14 @@ extern "C" int hc_fast(const HcModel *h, int mixed, double *EJv, double *EJv2, d
 }
 
 /* the GPU-ordered kernel with `inflight` packets interleaved event by event
- * and `ngen` packet generations (the concurrency of the device launch,
- * emulated in one host thread); Nabs per cell */
+ * (the concurrency of a device launch, emulated in one host thread); Nabs
+ * per cell */
 extern "C" int hc_fast_interleaved(const HcModel *h, int mixed, double *EJv, double *EJv2, double *Eabs, double *T,
                                    int *Ni, double *spec, unsigned long long *counters, double *tautot,
-                                   int inflight, int ngen, int *Nabs) {
+                                   int inflight, int *Nabs) {
   if (mixed)
-    return hc_fast_impl<float>(h, EJv, EJv2, Eabs, T, Ni, spec, counters, tautot, 0, h->nphot, inflight, ngen, Nabs);
-  return hc_fast_impl<double>(h, EJv, EJv2, Eabs, T, Ni, spec, counters, tautot, 0, h->nphot, inflight, ngen, Nabs);
+    return hc_fast_impl<float>(h, EJv, EJv2, Eabs, T, Ni, spec, counters, tautot, 0, h->nphot, inflight, Nabs);
+  return hc_fast_impl<double>(h, EJv, EJv2, Eabs, T, Ni, spec, counters, tautot, 0, h->nphot, inflight, Nabs);
 }
 
 /* Diffuse on the host: the host logic of mcg_diffuse with a backend of
