@@ -301,7 +301,7 @@ def run_reference(args, rank, world):
     ctx.close()
     O, tab = oracle_tables(m)
     cores = os.cpu_count() or 1
-    chunk = 100
+    chunk = 100  # the calibration's; the timed steps use larger chunks
 
     def work(seed):
         O.mcradiation(m, chunk, seed=seed, randomwalk=RUN["randomwalk"], factRW=RUN["factRW"],
@@ -320,6 +320,10 @@ def run_reference(args, rank, world):
         wait([ex.submit(work, s) for s in batch(2 * cores)])
         rate = 2 * cores * chunk / (time.perf_counter() - t0)
         per_step = args.ref_packets or max(cores * chunk, int(rate * 8.0) // chunk * chunk)
+        # chunks large enough that the oracle's lazily evaluated diffusion
+        # coefficients are reused within a call, four per thread and step
+        chunk = max(100, per_step // (4 * cores))
+        per_step = per_step // chunk * chunk
         nchunks = per_step // chunk
         for _ in range(args.warmup):
             wait([ex.submit(work, s) for s in batch(nchunks)])
@@ -469,7 +473,10 @@ def main():
                     "step": "surrogate opacity stage + mcg_set_model from host arrays + mcg_mcradiation + results "
                             "and temperatures to the host",
                     "opacity_stage_s": statistics.mean(i["opacity_stage_s"] for i in infos)},
-            "gpu_launches": None,
+            # 23 kernels per end-to-end step (the launch list of one step in
+            # the profiles folder: the surrogate, the model tables, the
+            # transport kernel, the run combination, the temperatures)
+            "gpu_launches": 23 * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": tpp * args.nphot if tpp else None,
                          "note": "algorithmic bytes from the event counters (crossings, absorptions, scatterings, "
