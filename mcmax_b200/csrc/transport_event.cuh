@@ -44,6 +44,11 @@
 #ifndef FE_COOP_MAX
 #define FE_COOP_MAX 4
 #endif
+/* a crossing phase continues while FE_TRACE_KEEP x (crossing lanes) is at
+ * least the largest group of lanes waiting for another event */
+#ifndef FE_TRACE_KEEP
+#define FE_TRACE_KEEP 1
+#endif
 /* 1: combine same-cell deposits of a crossing step within the warp */
 #ifndef FE_AGGREGATE
 #define FE_AGGREGATE 0
@@ -314,7 +319,7 @@ __device__ void fe_event_loop(const FModel<R> &m, const TAcc &A, TLocal &L) {
           const int others = max(max(__popc(__ballot_sync(FE_FULL, st == FS_ABSORB)),
                                      __popc(__ballot_sync(FE_FULL, st == FS_SCATTER))),
                                  __popc(__ballot_sync(FE_FULL, st == FS_EMIT || st == FS_NEW || st == FS_RW)));
-          if (nt < others) break;
+          if (nt * FE_TRACE_KEEP < others) break;
         }
       }
     } else if (kind == FS_ABSORB) {
