@@ -8,12 +8,10 @@ flaring index uniform 1.0..1.3, surface-density exponent uniform 0.5..1.5,
 nr uniform 60..250, ntheta uniform 40..160, nlam 100 (0.1..3000 micron),
 packets log-uniform 1e6..1e7 (times --scale).  Dust: one synthetic .lnk,
 MRN 0.1-1 micron in 20 bins (DHS opacities computed once on the GPU), full
-Mueller scattering, maxinteract 1e5, mixed transport.  The random walk is
-off: its diffusion tables take one 10001-entry row per optically thick
-cell, which for the most massive disks of the sweep is gigabytes per
-model.  Prints
-one JSON line: packets/s of the batched launch (autotuned shape, CUDA
-graph) and of the per-model calls."""
+Mueller scattering, maxinteract 1e5, modified random walk (factRW 10; a
+uniform mixture's thick cells share one diffusion row), mixed transport.
+Prints one JSON line: packets/s of the batched launch (autotuned shape,
+CUDA graph) and of the per-model calls."""
 import argparse
 import json
 import math
@@ -63,7 +61,7 @@ def main():
     ids = [ctx.add_model(m) for m, _ in ms]
     t_build = time.perf_counter() - t0
     nphot = [max(1000, int(n * a.scale)) for _, n in ms]
-    run = dict(precision="mixed", randomwalk=False, maxinteract=100000)
+    run = dict(precision="mixed", randomwalk=True, factRW=10.0, maxinteract=100000)
     seeds = list(range(1000, 1000 + a.nmodels))
     # warm-up + autotune (1/50 of the packets per shape), then graph capture
     _, _, info0 = ctx.mcradiation_batch(ids, nphot, seeds, autotune=True, use_graph=True, fetch=False, **run)

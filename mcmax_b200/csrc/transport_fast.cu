@@ -355,11 +355,14 @@ mcg_status mcg_fast_run(mcg_ctx *ctx, int precision, const void *tmodel, const v
 /* ========================================================================
  * Many models in one launch (mcg_add_model, mcg_mcradiation_batch).
  *
- * Packets of all models are numbered consecutively (model k owns
- * [off[k], off[k+1])) and taken from one work counter, `chunk` at a time;
- * a thread finds a packet's model by bisection in the offsets (shared
- * memory) and runs it with that model's tables and accumulators, through
- * the same per-packet code as the single-model kernel.  A packet keeps its
+ * Every model has its own work counter; a thread works on one model at a
+ * time, taking its packets `chunk` at a time, with at most one thread per
+ * MCG_PACKETS_PER_THREAD packets of the model on it (the bound of the
+ * single-model launch, which keeps each model's Bjorkman-Wood temperatures
+ * in the regime of the reference's serial order), and runs them with that
+ * model's tables and accumulators through the same per-packet code as the
+ * single-model kernel.  With one thread, packets run in model order (model
+ * k owns [off[k], off[k+1]) of one counter).  A packet keeps its
  * own Philox stream (its model's seed, its number within the model), so a
  * model's packets are the same packets whether it runs alone or in a batch
  * (the two kernels are compiled separately, so FMA contraction may round a
@@ -370,7 +373,8 @@ namespace {
 template <class R>
 __global__ void __launch_bounds__(F_BLOCK, F_MINBLOCKS)
     transport_batch_kernel(const FModel<R> *__restrict__ models, const TAcc *__restrict__ accs,
-                           const long long *__restrict__ off, int nmodels, unsigned long long *next, int chunk) {
+                           const long long *__restrict__ off, int nmodels, unsigned long long *next, int chunk,
+                           unsigned long long *mnext, int *mactive, const int *__restrict__ mcap) {
   __shared__ long long soff[MCG_BATCH_MAX + 1];
   for (int i = threadIdx.x; i <= nmodels; i += blockDim.x) soff[i] = off[i];
   if (blockIdx.x == 0)
@@ -390,31 +394,72 @@ __global__ void __launch_bounds__(F_BLOCK, F_MINBLOCKS)
     if (L.tautot != 0.0) atomicAdd(A.tautot, L.tautot);
   };
   clear();
-  int cur = -1;
-  for (;;) {
-    const unsigned long long k0 = atomicAdd(next, (unsigned long long)chunk);
-    if (k0 >= (unsigned long long)total) break;
-    const long long k1 = (long long)k0 + chunk < total ? (long long)k0 + chunk : total;
-    for (long long k = (long long)k0; k < k1; ++k) {
-      int lo = 0, hi = nmodels;
-      while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (soff[mid] <= k)
-          lo = mid;
-        else
-          hi = mid;
+  if (gridDim.x == 1 && blockDim.x == 1) {
+    /* one thread: every packet in model order (the serial order of each
+     * model's single run) */
+    int cur = -1;
+    for (;;) {
+      const unsigned long long k0 = atomicAdd(next, (unsigned long long)chunk);
+      if (k0 >= (unsigned long long)total) break;
+      const long long k1 = (long long)k0 + chunk < total ? (long long)k0 + chunk : total;
+      for (long long k = (long long)k0; k < k1; ++k) {
+        int lo = 0, hi = nmodels;
+        while (hi - lo > 1) {
+          const int mid = (lo + hi) >> 1;
+          if (soff[mid] <= k)
+            lo = mid;
+          else
+            hi = mid;
+        }
+        if (lo != cur) {
+          if (cur >= 0) flush(accs[cur]);
+          clear();
+          cur = lo;
+        }
+        const FModel<R> &m = models[lo];
+        f_run_packet<R>(m, accs[lo], (int64_t)(k - soff[lo]) + m.pid0, L);
+        tp_packet_done(accs[lo]);
       }
-      if (lo != cur) {
-        if (cur >= 0) flush(accs[cur]);
-        clear();
-        cur = lo;
-      }
-      const FModel<R> &m = models[lo];
-      f_run_packet<R>(m, accs[lo], (int64_t)(k - soff[lo]) + m.pid0, L);
-      tp_packet_done(accs[lo]);
     }
+    if (cur >= 0) flush(accs[cur]);
+    return;
   }
-  if (cur >= 0) flush(accs[cur]);
+  /* Every model has its own work counter and at most mcap[m] threads on it
+   * at once (its packets in flight, as the single-model launch bounds them:
+   * see MCG_PACKETS_PER_THREAD).  A thread joins a model with packets left
+   * and room, takes its packets `chunk` at a time until none are left, and
+   * moves on; it ends when no model has both. */
+  const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int start = (int)(gt % nmodels);
+  for (;;) {
+    int found = -1;
+    for (int t = 0; t < nmodels && found < 0; ++t) {
+      const int mm = (start + t) % nmodels;
+      const long long nm = soff[mm + 1] - soff[mm];
+      if (*(volatile unsigned long long *)&mnext[mm] >= (unsigned long long)nm) continue;
+      if (atomicAdd(&mactive[mm], 1) < mcap[mm])
+        found = mm;
+      else
+        atomicSub(&mactive[mm], 1);
+    }
+    if (found < 0) break;
+    const FModel<R> &m = models[found];
+    const TAcc &A = accs[found];
+    const long long nm = soff[found + 1] - soff[found];
+    for (;;) {
+      const unsigned long long k0 = atomicAdd(&mnext[found], (unsigned long long)chunk);
+      if (k0 >= (unsigned long long)nm) break;
+      const long long k1 = (long long)k0 + chunk < nm ? (long long)k0 + chunk : nm;
+      for (long long k = (long long)k0; k < k1; ++k) {
+        f_run_packet<R>(m, A, (int64_t)k + m.pid0, L);
+        tp_packet_done(A);
+      }
+    }
+    flush(A);
+    clear();
+    atomicSub(&mactive[found], 1);
+    start = found + 1;
+  }
 }
 
 /* swap kept model `id` in as the context's current model (and back) */
@@ -460,7 +505,9 @@ mcg_status batch_run_t(mcg_ctx *ctx, int pi, int n, const int *ids, const mcg_ru
   const size_t b_fm = ((size_t)n * sizeof(FModel<R>) + 255) & ~(size_t)255;
   const size_t b_ta = ((size_t)n * sizeof(TAcc) + 255) & ~(size_t)255;
   const size_t b_off = ((size_t)(n + 1) * sizeof(long long) + 255) & ~(size_t)255;
-  const size_t need = b_fm + b_ta + b_off + 256;
+  /* per model: work counter, threads on it, their cap */
+  const size_t b_pm = (((size_t)n * (8 + 4 + 4)) + 255) & ~(size_t)255;
+  const size_t need = b_fm + b_ta + b_off + 256 + b_pm;
   if (ctx->batch_args.bytes < need) {
     if (ctx->batch_graph) {
       cudaGraphExecDestroy(ctx->batch_graph);
@@ -479,6 +526,14 @@ mcg_status batch_run_t(mcg_ctx *ctx, int pi, int n, const int *ids, const mcg_ru
   TAcc *d_ta = (TAcc *)(base + b_fm);
   long long *d_off = (long long *)(base + b_fm + b_ta);
   unsigned long long *d_next = (unsigned long long *)(base + b_fm + b_ta + b_off);
+  unsigned long long *d_mnext = (unsigned long long *)(base + b_fm + b_ta + b_off + 256);
+  int *d_mactive = (int *)(d_mnext + n);
+  int *d_mcap = d_mactive + n;
+  {
+    std::vector<int> cap(n);
+    for (int i = 0; i < n; ++i) cap[i] = (int)std::min<long long>(mcg_default_threads(rp[i].tm.nphot), 1LL << 30);
+    MCG_CUDA(ctx, cudaMemcpyAsync(d_mcap, cap.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
+  }
   MCG_CUDA(ctx, cudaMemcpyAsync(d_fm, fm.data(), (size_t)n * sizeof(FModel<R>), cudaMemcpyHostToDevice, st));
   MCG_CUDA(ctx, cudaMemcpyAsync(d_ta, ta.data(), (size_t)n * sizeof(TAcc), cudaMemcpyHostToDevice, st));
   MCG_CUDA(ctx, cudaMemcpyAsync(d_off, off.data(), (size_t)(n + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));
@@ -513,8 +568,10 @@ mcg_status batch_run_t(mcg_ctx *ctx, int pi, int n, const int *ids, const mcg_ru
       MCG_CUDA(ctx, cudaMemcpyAsync(d_fm, tf.data(), (size_t)n * sizeof(FModel<R>), cudaMemcpyHostToDevice, st));
       MCG_CUDA(ctx, cudaMemcpyAsync(d_off, toff.data(), (size_t)(n + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));
       MCG_CUDA(ctx, cudaMemsetAsync(d_next, 0, 8, st));
+      MCG_CUDA(ctx, cudaMemsetAsync(d_mnext, 0, (size_t)n * (8 + 4), st));
       MCG_CUDA(ctx, cudaEventRecord(ctx->ev0, st));
-      transport_batch_kernel<R><<<sms * c.bps, c.block, 0, st>>>(d_fm, d_ta, d_off, n, d_next, c.chunk);
+      transport_batch_kernel<R><<<sms * c.bps, c.block, 0, st>>>(d_fm, d_ta, d_off, n, d_next, c.chunk, d_mnext,
+                                                                  d_mactive, d_mcap);
       MCG_CUDA(ctx, cudaGetLastError());
       MCG_CUDA(ctx, cudaEventRecord(ctx->ev1, st));
       MCG_CUDA(ctx, cudaEventSynchronize(ctx->ev1));
@@ -549,11 +606,13 @@ mcg_status batch_run_t(mcg_ctx *ctx, int pi, int n, const int *ids, const mcg_ru
       MCG_CUDA(ctx, mcg_run_zero(ctx, (size_t)rp[i].nc * rp[i].nruns, rp[i].ns));
     }
     MCG_CUDA(ctx, cudaMemsetAsync(d_next, 0, 8, st));
+    MCG_CUDA(ctx, cudaMemsetAsync(d_mnext, 0, (size_t)n * (8 + 4), st));
     if (timed) MCG_CUDA(ctx, cudaEventRecord(ctx->ev0, st));
     if (serial)
-      transport_batch_kernel<R><<<1, 1, 0, st>>>(d_fm, d_ta, d_off, n, d_next, 1);
+      transport_batch_kernel<R><<<1, 1, 0, st>>>(d_fm, d_ta, d_off, n, d_next, 1, d_mnext, d_mactive, d_mcap);
     else
-      transport_batch_kernel<R><<<sms * sh.bps, sh.block, 0, st>>>(d_fm, d_ta, d_off, n, d_next, sh.chunk);
+      transport_batch_kernel<R><<<sms * sh.bps, sh.block, 0, st>>>(d_fm, d_ta, d_off, n, d_next, sh.chunk, d_mnext,
+                                                                  d_mactive, d_mcap);
     MCG_CUDA(ctx, cudaGetLastError());
     if (timed) MCG_CUDA(ctx, cudaEventRecord(ctx->ev1, st));
     for (int i = 0; i < n; ++i) {

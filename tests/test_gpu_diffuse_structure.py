@@ -1,8 +1,9 @@
 """mcg_diffuse and mcg_disk_structure on the GPU against the host replays
 of the same logic and per-element arithmetic (bit for bit: the library
 builds both units with --fmad=false, the replay with -ffp-contract=off, and
-the structure step takes exp and log from detmath.h), and mcg_diffuse
-against the oracle's dense DGESV form to rounding."""
+the structure step takes exp and log from detmath.h), mcg_disk_structure
+against the oracle's restatement of DiskStructure bit for bit, and
+mcg_diffuse against the oracle's dense DGESV form to rounding."""
 import numpy as np
 import pytest
 
@@ -36,7 +37,7 @@ def test_diffuse_matches_replay_and_oracle(ctx):
     assert np.max(np.abs(Tg / To - 1)) < 1e-12
 
 
-def test_disk_structure_matches_replay(ctx):
+def test_disk_structure_matches_replay_and_oracle(ctx):
     from mcmax_b200 import model as M
     m = models.small_disk(nrad=20, ntheta=14, nlam=16, mdust=1e-4, ngrains=2)
     nc = m.nt - 1
@@ -51,5 +52,7 @@ def test_disk_structure_matches_replay(ctx):
     st = dict(nr=m.nr, nt=m.nt, ng=m.ncomp, R=m.R, Theta=m.Theta, V=m.V, Mstar=2.5 * M.MSUN, zones=zones,
               grain_scale=gs)
     ref = H.disk_structure(st, Temp, dens, dens, dens, w.ravel(), w.ravel())
-    for a, b, name in zip(got, ref, ("dens", "dens0", "gasdens", "w", "w0")):
+    orc = O.disk_structure(st, Temp, dens, dens, dens, w.ravel(), w.ravel())
+    for a, b, c, name in zip(got, ref, orc, ("dens", "dens0", "gasdens", "w", "w0")):
         assert np.array_equal(np.ravel(a), np.ravel(b)), name
+        assert np.array_equal(np.ravel(a), np.ravel(c)), name

@@ -1,7 +1,8 @@
-"""mcg_trace_spectrum on the GPU against the host replay of the same host
-logic and per-ray arithmetic, bit for bit (the unit is built with
---fmad=false, the replay with -ffp-contract=off, and the ray set-up and
-attenuation use detmath.h)."""
+"""mcg_trace_spectrum and mcg_trace_image on the GPU against the host replay
+of the same host logic and per-ray arithmetic and against the oracle's own
+restatement of TraceMono/MakeImage, bit for bit (the unit is built with
+--fmad=false, the replay and the oracle with -ffp-contract=off, and the ray
+set-up and attenuation use detmath.h)."""
 import math
 
 import numpy as np
@@ -9,6 +10,7 @@ import pytest
 
 import hostcheck_ffi as H
 import models
+import oracle_ffi as O
 
 pytestmark = pytest.mark.gpu
 
@@ -25,6 +27,9 @@ def test_trace_spectrum_matches_replay(ctx, deg):
     fh, Rimg, _, bad = H.trace_spectrum(m, T, lam, math.radians(deg), nphi=30, nj0=2)
     assert info == (Rimg.size, bad) and bad == 0
     assert np.array_equal(fg, fh)
+    fo, nro, bo = O.trace_spectrum(m, T, lam, math.radians(deg), nphi=30, nj0=2)
+    assert (nro, bo) == info
+    assert np.array_equal(fg, fo)
 
 
 @pytest.mark.parametrize("deg,pa,linear", [(45.0, 20.0, 0), (80.0, 0.0, 1)])
@@ -44,6 +49,10 @@ def test_trace_image_matches_replay(ctx, deg, pa, linear):
     assert g["info"] == (nh, bh) and bh == 0
     assert g["flux"] == fh
     assert np.array_equal(g["image"], ih)
+    io, fo, no, bo = O.trace_image(m, T, 10.0, math.radians(deg), 64, 50, Rmax, pa=pa, seed=9, linear=linear,
+                                   nphi=30, nj0=2)
+    assert g["info"] == (no, bo) and g["flux"] == fo
+    assert np.array_equal(np.ravel(g["image"]), np.ravel(io))
     _, Rimg, rphi, _ = H.trace_spectrum(m, T, [10.0], math.radians(deg), nphi=30, nj0=2, lam_path=10.0)
     assert np.array_equal(g["R"], Rimg) and np.array_equal(g["rphi"], rphi)
 
