@@ -60,3 +60,31 @@ def test_batch_rejects_bad_arguments(ctx):
         ctx.mcradiation_batch([i, i], [10, 10], [1, 2])
     with pytest.raises(McgError):
         ctx.mcradiation_batch([i + 1000], [10], [1])
+
+
+def test_uneven_models_with_random_walk_match_their_single_runs(ctx):
+    """Four models of uneven grids and disk masses, the random walk on (a
+    uniform mixture's thick cells share one diffusion row), in one parallel
+    launch: each model's packets are accounted for, its energy is conserved,
+    and its absorbed energy and SED agree with its own single-model run."""
+    ms = [models.small_disk(nrad=12, ntheta=8, nlam=24, ngrains=2, ns=2, nf=3, mdust=1e-3),
+          models.small_disk(nrad=24, ntheta=14, nlam=24, ngrains=2, ns=2, nf=3, mdust=1e-2),
+          models.small_disk(nrad=16, ntheta=20, nlam=24, ngrains=2, ns=2, nf=3, mdust=1e-4),
+          models.small_disk(nrad=30, ntheta=10, nlam=24, ngrains=2, ns=2, nf=3, mdust=3e-3)]
+    ids = [ctx.add_model(m) for m in ms]
+    nphot = [40000, 60000, 30000, 50000]
+    run = dict(precision="mixed", randomwalk=True, factRW=10.0, maxinteract=100000)
+    _, outs, info = ctx.mcradiation_batch(ids, nphot, [31, 32, 33, 34], autotune=False, use_graph=False, **run)
+    assert info["device_ms"] > 0
+    rw_steps = 0
+    for m, n, o, s in zip(ms, nphot, outs, (41, 42, 43, 44)):
+        c = o["counters"]
+        assert int(c[9]) + int(c[7]) + int(c[11]) == n
+        assert int(c[11]) == 0
+        rw_steps += int(c[4])
+        assert abs(_energy_out(m, o) / m.Lstar - 1) < 0.03
+        ctx.set_model(m)
+        _, a = ctx.mcradiation(n, seed=s, **run)
+        assert abs(o["EJv"].sum() / a["EJv"].sum() - 1) < 0.05
+        assert abs(o["spec"].sum() / a["spec"].sum() - 1) < 0.03
+    assert rw_steps > 0
