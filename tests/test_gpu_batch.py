@@ -86,5 +86,13 @@ def test_uneven_models_with_random_walk_match_their_single_runs(ctx):
         ctx.set_model(m)
         _, a = ctx.mcradiation(n, seed=s, **run)
         assert abs(o["EJv"].sum() / a["EJv"].sum() - 1) < 0.05
-        assert abs(o["spec"].sum() / a["spec"].sum() - 1) < 0.03
+        # escaping energy in three inclination ranges (the raw SED total is
+        # weighted by 1/dnu and so dominated by the few far-infrared packets)
+        eo, ea = _energy_by_inclination(m, o), _energy_by_inclination(m, a)
+        assert np.all(np.abs(eo / ea - 1) < 0.05), (eo, ea)
     assert rw_steps > 0
+
+
+def _energy_by_inclination(m, out, groups=3):
+    e = _energy_out(m, {"spec": out["spec"]}, per_bin=True)
+    return e.sum(0).reshape(groups, -1).sum(1)
