@@ -323,10 +323,13 @@ mcg_status mcg_diffuse(mcg_ctx *ctx, int32_t nphotmin, double dtmax, double fact
  * temperatures Temp (the TempAverage of DiskStructure.f:25, >= 2.7 K), by the
  * reference's adaptive Cash-Karp integration (Subroutines.f:1933-2090),
  * renormalised to the species' mass in the ring; rings inside a zone with a
- * fixed structure keep the zone's analytic profile.  Then every cell's dust
- * and gas densities and abundances are rebuilt from the profiles.  All
- * grains have the 'DISK' scale-height type; no radiation pressure, gaps or
- * halo.  Cell arrays in the cell order above, w and w0 with ngrains values
+ * fixed structure keep the zone's analytic profile.  A grain whose
+ * scale-height type is not 'DISK' takes that type's closed-form profile
+ * along theta (DiskStructure.f:248-344; MCG_SH_* below, the keyword
+ * shtypeN of Init.f:920-926); MCG_SH_KEEP, the reference's unknown type,
+ * keeps the grain's current densities.  Then every cell's dust and gas
+ * densities and abundances are rebuilt from the profiles.  No radiation
+ * pressure, gaps or halo.  Cell arrays in the cell order above, w and w0 with ngrains values
  * per cell (C%w, C%w0), all in/out: dens (C%dens), dens0 (C%dens0, the
  * condensable total), gasdens (C%gasdens, in dust-density units). */
 typedef struct {
@@ -345,7 +348,22 @@ typedef struct {
   const mcg_zone *zones;
   const double *shscale;          /* nr scale-height factors per ring, or NULL (1) */
   const double *grain_scale;      /* ngrains*nr settling factors Grain(ii)%shscale(i), or NULL */
+  const int32_t *shtype;          /* ngrains scale-height types MCG_SH_*, or NULL (all MCG_SH_DISK) */
 } mcg_structure;
+
+/* scale-height types (Grain(ii)%shtype): HALO and SHELL read the grain's
+ * factor grain_scale directly, LOBE, JET, CYLI, CAVITY and WEDGE the
+ * column's scale (shscale times grain_scale) as degrees, AU or a slope */
+#define MCG_SH_DISK 0
+#define MCG_SH_ZODI 1
+#define MCG_SH_HALO 2
+#define MCG_SH_LOBE 3
+#define MCG_SH_JET 4
+#define MCG_SH_SHELL 5
+#define MCG_SH_CYLI 6
+#define MCG_SH_CAVITY 7
+#define MCG_SH_WEDGE 8
+#define MCG_SH_KEEP 9
 
 mcg_status mcg_disk_structure(mcg_ctx *ctx, const mcg_structure *s, const double *Temp, double *dens, double *dens0,
                               double *gasdens, double *w, double *w0);

@@ -50,7 +50,11 @@ class Structure(C.Structure):
     _fields_ = [("nr", C.c_int32), ("nt", C.c_int32), ("ngrains", C.c_int32), ("R", C.POINTER(C.c_double)),
                 ("Theta", C.POINTER(C.c_double)), ("V", C.POINTER(C.c_double)), ("Mstar", C.c_double),
                 ("nzones", C.c_int32), ("zones", C.POINTER(Zone)), ("shscale", C.POINTER(C.c_double)),
-                ("grain_scale", C.POINTER(C.c_double))]
+                ("grain_scale", C.POINTER(C.c_double)), ("shtype", C.POINTER(C.c_int32))]
+
+
+# scale-height types (MCG_SH_*), by the reference's keyword values
+SHTYPES = ("DISK", "ZODI", "HALO", "LOBE", "JET", "SHELL", "CYLI", "CAVITY", "WEDGE", "KEEP")
 
 
 class TraceOpts(C.Structure):

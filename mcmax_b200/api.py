@@ -273,10 +273,14 @@ class Context:
                     rphi=rphi[:n * int(nphi)].reshape(n, int(nphi)).copy(), info=(n, int(info[1])))
 
     def disk_structure(self, R, Theta, V, Mstar, zones, Temp, dens, dens0, gasdens, w, w0, shscale=None,
-                       grain_scale=None):
+                       grain_scale=None, shtype=None):
         """mcg_disk_structure: zones is a list of (rin, rout, sh, rsh, shpow,
         denspow, fix_struct); cell arrays in the library's cell order, w and
-        w0 (ncell, ngrains).  Returns the new (dens, dens0, gasdens, w, w0)."""
+        w0 (ncell, ngrains).  shtype: per grain a scale-height type, by name
+        ('DISK', 'ZODI', 'HALO', 'LOBE', 'JET', 'SHELL', 'CYLI', 'CAVITY',
+        'WEDGE'; any other name keeps the grain's densities, as the
+        reference does for an unknown type) or MCG_SH_* code; None: all
+        'DISK'.  Returns the new (dens, dens0, gasdens, w, w0)."""
         R, Theta, V, Temp = _f64(R), _f64(Theta), _f64(V), _f64(Temp)
         nr, nt = R.size - 1, Theta.size
         ncell = nr * (nt - 1)
@@ -289,8 +293,9 @@ class Context:
         for k, z in enumerate(zones):
             zs[k] = _ffi.Zone(*[float(x) for x in z[:6]], int(bool(z[6])))
         keep = [None if a is None else _f64(a) for a in (shscale, grain_scale)]
+        sht = None if shtype is None else shtype_codes(shtype, ng)
         st = _ffi.Structure(nr, nt, ng, _ffi.ptr(R), _ffi.ptr(Theta), _ffi.ptr(V), float(Mstar), len(zones), zs,
-                            _ffi.ptr(keep[0]), _ffi.ptr(keep[1]))
+                            _ffi.ptr(keep[0]), _ffi.ptr(keep[1]), _ffi.ptr(sht))
         self._check(self.lib.mcg_disk_structure(self.h, C.byref(st), _ffi.ptr(Temp), *[_ffi.ptr(a) for a in out]))
         out[3] = out[3].reshape(ncell, ng)
         out[4] = out[4].reshape(ncell, ng)
@@ -311,6 +316,22 @@ class Context:
         self._check(self.lib.mcg_diffuse(self.h, int(nphotmin), float(dtmax), float(factRW), _ffi.ptr(Ni),
                                          _ffi.ptr(dT), _ffi.ptr(T), _ffi.ptr(EJv), _ffi.ptr(counts)))
         return T, EJv, tuple(int(x) for x in counts)
+
+
+def shtype_codes(shtype, ngrains):
+    """int32 MCG_SH_* codes of a per-grain list of scale-height types (names
+    as the keyword shtypeN takes them, or codes); a name the reference does
+    not know keeps the grain's densities (MCG_SH_KEEP)"""
+    if len(shtype) != ngrains:
+        raise McgError(_ffi.MCG_ERR_ARG, "shtype needs %d entries" % ngrains)
+    out = np.zeros(ngrains, np.int32)
+    for k, v in enumerate(shtype):
+        if isinstance(v, str):
+            name = v.strip().upper()
+            out[k] = _ffi.SHTYPES.index(name) if name in _ffi.SHTYPES else _ffi.SHTYPES.index("KEEP")
+        else:
+            out[k] = int(v)
+    return out
 
 
 def bb_table(lam):

@@ -3,8 +3,10 @@
  * on the device.
  *
  *   ds_column_kernel  one thread per (ring, species) column: the hydrostatic
- *                     ODE march from the midplane up (odeint/rkqs/rkck), or
- *                     the fixed-zone profile, then the mass renormalisation
+ *                     ODE march from the midplane up (odeint/rkqs/rkck), the
+ *                     fixed-zone profile, or the closed-form profile of a
+ *                     grain's other scale-height type (formed on the host),
+ *                     then the mass renormalisation
  *   ds_cell_kernel    one thread per cell of rings 1..nR-1: densities and
  *                     abundances from the species' profiles
  *   ds_check_kernel   one thread per cell: CheckCells
@@ -23,7 +25,7 @@ namespace {
 struct DsDev {
   int nc, ncol, nr, ng;
   double Mstar;
-  const double *Temp, *V, *R_av, *z, *st, *ct, *cot, *theta_av;
+  const double *Temp, *V, *R_av, *z, *st, *ct, *cot, *theta_av, *prof;
   const DsColumn *cols;
   const int *ring;
   double *rho;
@@ -33,8 +35,9 @@ __global__ void ds_column_kernel(const __grid_constant__ DsDev d) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= d.ncol) return;
   const int i = d.ring[q], nc = d.nc;
-  ds_column(d.cols[q], nc, d.R_av[i], d.Mstar, d.Temp + (size_t)i * nc, d.V + (size_t)i * nc, d.z + (size_t)i * nc,
-            d.st, d.ct, d.cot, d.theta_av, d.rho + (size_t)q * nc);
+  const DsColumn col = d.cols[q];
+  ds_column(col, nc, d.R_av[i], d.Mstar, d.Temp + (size_t)i * nc, d.V + (size_t)i * nc, d.z + (size_t)i * nc,
+            d.st, d.ct, d.cot, d.theta_av, col.pre >= 0 ? d.prof + col.pre : nullptr, d.rho + (size_t)q * nc);
 }
 
 __global__ void ds_cell_kernel(int nr, int nc, int ng, const double *rho, double *dens, double *dens0,
@@ -91,7 +94,7 @@ struct DsDeviceBackend {
     return e == cudaSuccess ? true : fail(e, "disk structure: upload");
   }
   bool columns(const DsGrid &g, const DsTables &t, const double *, int ncol, const DsColumn *cols, const int *ring,
-               double *) {
+               const std::vector<double> &prof, double *) {
     const int nc = g.nt - 1;
     DsDev d;
     d.nc = nc;
@@ -114,6 +117,11 @@ struct DsDeviceBackend {
     d.cot = a;
     if (!up(&a, t.theta_av.data(), t.theta_av.size())) return false;
     d.theta_av = a;
+    d.prof = nullptr;
+    if (!prof.empty()) {
+      if (!up(&a, prof.data(), prof.size())) return false;
+      d.prof = a;
+    }
     DsColumn *dc;
     int *dr;
     if (!up(&dc, cols, (size_t)ncol)) return false;
@@ -148,6 +156,11 @@ mcg_status mcg_disk_structure_impl(mcg_ctx *ctx, const mcg_structure *s, const d
   if (s->nr < 2 || s->nt < 3 || s->ngrains < 1 || (s->nzones > 0 && !s->zones) || !(s->Mstar > 0.0))
     return mcg_fail(ctx, MCG_ERR_ARG, "disk_structure: nr >= 2, nt >= 3, ngrains >= 1, Mstar > 0 required");
   const int nc = s->nt - 1, ng = s->ngrains;
+  if (s->shtype)
+    for (int k = 0; k < ng; ++k)
+      if (s->shtype[k] < 0 || s->shtype[k] >= DS_SH_NTYPES)
+        return mcg_fail(ctx, MCG_ERR_ARG, "disk_structure: shtype[%d] = %d is not a scale-height type", k,
+                        (int)s->shtype[k]);
   const size_t ncell = (size_t)s->nr * nc;
   for (size_t c = 0; c < ncell; ++c)
     if (!(Temp[c] > 0.0)) return mcg_fail(ctx, MCG_ERR_ARG, "disk_structure: Temp[%zu] = %g is not positive", c, Temp[c]);
@@ -156,7 +169,8 @@ mcg_status mcg_disk_structure_impl(mcg_ctx *ctx, const mcg_structure *s, const d
     const mcg_zone &z = s->zones[k];
     zones[k] = DsZone{z.rin, z.rout, z.sh, z.rsh, z.shpow, z.denspow, z.fix_struct};
   }
-  DsGrid g{s->nr, s->nt, ng, s->R, s->Theta, s->V, s->Mstar, s->nzones, zones.data(), s->shscale, s->grain_scale};
+  DsGrid g{s->nr, s->nt, ng, s->R, s->Theta, s->V, s->Mstar, s->nzones, zones.data(), s->shscale, s->grain_scale,
+           (const int *)s->shtype};
   cudaStream_t st = ctx->stream;
   DsMem mem;
   DsDeviceBackend be;

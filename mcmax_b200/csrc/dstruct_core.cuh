@@ -9,9 +9,13 @@
  *
  * Built: 'DISK' scale-height species, gas included, zones with a fixed
  * structure (the analytic profile of DiskStructure.f:360-386, wedges too),
- * per-ring scale factors and per-grain settling factors as inputs.  Not
- * built: radiation pressure (beta = 0), the other shtype profiles, mpstr,
- * scset settling, gaps, halo, radial structure iterations.
+ * per-ring scale factors and per-grain settling factors as inputs, and the
+ * other scale-height types of DiskStructure.f:248-344 (ZODI, HALO, LOBE,
+ * JET, SHELL, CYLI, CAVITY, WEDGE, and an unknown type that keeps the
+ * grain's current densities).  Those closed-form profiles are formed on the
+ * host with the C library's functions (ds_shape_profile) and only
+ * renormalised on the device.  Not built: radiation pressure (beta = 0),
+ * mpstr, scset settling, gaps, halo, radial structure iterations.
  *
  * Shared by the library (dstruct.cu: one thread per column, one per cell)
  * and the host replay of the tests.  Every a*b+c is rounded twice (the unit
@@ -45,6 +49,21 @@
 #define DS_MU (0x1.2666660000000p+1 * 1.67262158e-24)   /* DiskStructure.f:475: 2.3 as a float */
 #define DS_G 6.67300e-8                                  /* DiskStructure.f:477 */
 #define DS_KB 1.3806503e-16                              /* Modules.f:11 */
+
+/* scale-height types of a grain (Grain(ii)%shtype, Init.f:920-926) */
+enum {
+  DS_SH_DISK = 0,   /* hydrostatic equilibrium */
+  DS_SH_ZODI = 1,   /* zodiacal cosine model */
+  DS_SH_HALO = 2,   /* constant, a wedge when the grain's factor is negative */
+  DS_SH_LOBE = 3,   /* Gaussian in theta, width scale degrees */
+  DS_SH_JET = 4,    /* Gaussian in theta, width growing with radius */
+  DS_SH_SHELL = 5,  /* 1 + factor sin^3 theta */
+  DS_SH_CYLI = 6,   /* cylinder of height scale AU */
+  DS_SH_CAVITY = 7, /* outside a paraboloidal cavity */
+  DS_SH_WEDGE = 8,  /* theta above (or below) scale degrees */
+  DS_SH_KEEP = 9,   /* an unknown type: the grain's densities as they are */
+  DS_SH_NTYPES = 10
+};
 
 /* one ODE segment: d ln(rho)/dz between z1 (cell j+1) and z2 (cell j), the
  * temperature linear in z between the two cell temperatures (derivs,
@@ -131,6 +150,7 @@ DS_HD double ds_odeint(const DsSeg &s, double ystart, double eps, double h1) {
  *   rho     out, nc values */
 struct DsColumn {
   int fix;          /* index of a fixed-structure zone containing the ring, or -1 */
+  long long pre;    /* offset of a closed-form log profile formed on the host, or -1 */
   double scale;     /* scale-height factor of the species in the ring */
   double M0;        /* the species' mass in the ring */
   double sh, rsh, shpow, denspow; /* the fixed zone's profile */
@@ -138,8 +158,10 @@ struct DsColumn {
 
 DS_HD void ds_column(const DsColumn &col, int nc, double R_av, double Mstar, const double *Trow, const double *Vrow,
                      const double *z, const double *st, const double *ct, const double *cot,
-                     const double *theta_av, double *rho) {
-  if (col.fix < 0) {
+                     const double *theta_av, const double *pre, double *rho) {
+  if (pre) {
+    for (int j = 0; j < nc; ++j) rho[j] = pre[j];
+  } else if (col.fix < 0) {
     rho[nc - 1] = 0.0;
     if (col.scale > 0.0) {
       DsSeg s;
@@ -279,11 +301,12 @@ struct DsGrid {
   const DsZone *zones;
   const double *shscale;    /* nr, or NULL (1) */
   const double *gscale;     /* ng*nr settling factor of each grain per ring, or NULL (1) */
+  const int *shtype;        /* ng scale-height types (DS_SH_*), or NULL (all DS_SH_DISK) */
 };
 
 /* per-ring and per-theta geometry, computed on the host */
 struct DsTables {
-  std::vector<double> R_av, z, st, ct, cot, theta_av; /* R_av[nr]; z[nr*nc]; the rest [nc] */
+  std::vector<double> R_av, z, st, ct, cot, theta_av, thet; /* R_av[nr]; z[nr*nc]; the rest [nc] */
 };
 
 static inline void ds_tables(const DsGrid &g, DsTables *t) {
@@ -294,6 +317,7 @@ static inline void ds_tables(const DsGrid &g, DsTables *t) {
   t->ct.assign(nc, 0.0);
   t->cot.assign(nc, 0.0);
   t->theta_av.assign(nc, 0.0);
+  t->thet.assign(nc, 0.0);
   for (int i = 0; i < nR; ++i) t->R_av[i] = DS_AU * pow(10.0, (log10(g.R[i]) + log10(g.R[i + 1])) / 2.0);
   for (int j = 1; j <= nc; ++j) {
     const double th = acos((g.Theta[j - 1] + g.Theta[j]) / 2.0);
@@ -301,6 +325,7 @@ static inline void ds_tables(const DsGrid &g, DsTables *t) {
     t->st[j - 1] = sin(th);
     t->ct[j - 1] = cos(th);
     t->cot[j - 1] = 1.0 / tan(th);
+    t->thet[j - 1] = acos(g.Theta[j - 1]); /* D%thet(j), the cell's polar edge */
   }
   for (int i = 0; i < nR; ++i)
     for (int j = 0; j < nc; ++j) t->z[(size_t)i * nc + j] = t->R_av[i] * t->ct[j];
@@ -336,6 +361,7 @@ static inline DsColumn ds_setup_column(const DsGrid &g, const DsTables &t, int i
       if (Rav > zn.rin * DS_AU && Rav < zn.rout * DS_AU && !zn.fix_struct) fix = -1;
     }
   col.fix = fix;
+  col.pre = -1;
   col.sh = col.rsh = col.shpow = col.denspow = 0.0;
   if (fix >= 0) {
     col.sh = g.zones[fix].sh;
@@ -346,8 +372,65 @@ static inline DsColumn ds_setup_column(const DsGrid &g, const DsTables &t, int i
   return col;
 }
 
-/* Backend: columns(g, t, Temp, ncol, cols, ring, rho[ncol*nc]) runs
- * ds_column per column, cells(g, rho, dens, dens0, gasdens, w, w0) runs
+/* the closed-form log-density profiles of the scale-height types other than
+ * DISK (DiskStructure.f:248-344) for grain k (1..ng) in ring i, formed on
+ * the host with the C library's functions, in the reference's operation
+ * order.  scale: the column's factor (ring times grain); gsh: the grain's own
+ * factor Grain(ii)%shscale(i), which HALO and SHELL read; dens, w: the cell
+ * arrays as they are (the unknown type keeps log(dens w)). */
+static inline void ds_shape_profile(const DsGrid &g, const DsTables &t, int i, int k, int type, double scale,
+                                    const double *dens, const double *w, double *rho) {
+  const int nc = g.nt - 1, ng = g.ng;
+  const double gsh = g.gscale ? g.gscale[(size_t)(k - 1) * g.nr + i] : 1.0;
+  const double *z = &t.z[(size_t)i * nc];
+  const double Rav = t.R_av[i], Rout = t.R_av[g.nr - 1];
+  for (int j = 0; j < nc; ++j) {
+    const double th = t.theta_av[j], deg = (180.0 * th) / DS_PI;
+    double r = 0.0;
+    switch (type) {
+      case DS_SH_ZODI: /* cosine model (Rittich 1986), DiskStructure.f:249-255 */
+        r = log(0.15 + (double)0.85f * pow(cos(DS_PI / 2.0 - th), 28.0));
+        break;
+      case DS_SH_HALO:
+        r = (gsh < 0.0 && DS_PI / 2.0 - th > -gsh) ? -60.0 : 0.0;
+        break;
+      case DS_SH_LOBE: {
+        const double q = deg / scale;
+        r = log10(exp(-(q * q)));
+        break;
+      }
+      case DS_SH_JET: {
+        const double q = ((t.thet[j] * 180.0) / DS_PI) / (scale * (Rav / Rout));
+        r = -(q * q);
+        break;
+      }
+      case DS_SH_SHELL:
+        r = log(1.0 + gsh * pow(sin(th), 3.0));
+        break;
+      case DS_SH_CYLI:
+        r = (j == nc - 1 || z[j] / DS_AU < scale) ? 0.0 : -60.0;
+        break;
+      case DS_SH_CAVITY: {
+        const double rc = (Rav * t.st[j]) / DS_AU;
+        r = (j == nc - 1) ? 0.0 : (j == 0) ? -60.0 : (z[j] / DS_AU < (rc * rc) * scale) ? 0.0 : -60.0;
+        break;
+      }
+      case DS_SH_WEDGE:
+        r = scale > 0.0 ? (deg > scale ? 0.0 : -60.0) : (deg < -scale ? 0.0 : -60.0);
+        break;
+      default: { /* DS_SH_KEEP */
+        const size_t c = (size_t)i * nc + j;
+        const double v = dens[c] * w[c * ng + (k - 1)];
+        r = v > 1e-60 ? log(v) : -60.0;
+      }
+    }
+    rho[j] = r;
+  }
+}
+
+/* Backend: columns(g, t, Temp, ncol, cols, ring, prof, rho[ncol*nc]) runs
+ * ds_column per column (prof: the host-formed profiles the columns' pre
+ * offsets point into), cells(g, rho, dens, dens0, gasdens, w, w0) runs
  * ds_cell per cell of rings 1..nR-1 and then ds_check_cell per cell of
  * rings 0..nR-1; each returns false on an execution error.  Cell arrays:
  * dens, dens0, gasdens (ncell), w, w0 (ncell*ng), all in/out. */
@@ -361,25 +444,34 @@ bool ds_disk_structure(const DsGrid &g, Backend &be, const double *Temp, double 
   const int ncol = (nR - 1) * ns;
   std::vector<DsColumn> cols(ncol);
   std::vector<int> ring(ncol);
+  std::vector<double> prof;
   for (int i = 1; i < nR; ++i)
     for (int k = 0; k < ns; ++k) {
       const int q = (i - 1) * ns + k;
       cols[q] = ds_setup_column(g, t, i, k, dens, dens0, gasdens, w, w0);
       ring[q] = i;
+      const int type = (k > 0 && g.shtype) ? g.shtype[k - 1] : DS_SH_DISK;
+      if (cols[q].fix < 0 && type != DS_SH_DISK) {
+        cols[q].pre = (long long)prof.size();
+        prof.resize(prof.size() + nc);
+        ds_shape_profile(g, t, i, k, type, cols[q].scale, dens, w, &prof[(size_t)cols[q].pre]);
+      }
     }
   std::vector<double> rho((size_t)ncol * nc);
-  if (!be.columns(g, t, Temp, ncol, cols.data(), ring.data(), rho.data())) return false;
+  if (!be.columns(g, t, Temp, ncol, cols.data(), ring.data(), prof, rho.data())) return false;
   return be.cells(g, rho.data(), dens, dens0, gasdens, w, w0);
 }
 
 /* serial loops of the two steps (host backend and replay) */
 static inline void ds_columns_host(const DsGrid &g, const DsTables &t, const double *Temp, int ncol,
-                                   const DsColumn *cols, const int *ring, double *rho) {
+                                   const DsColumn *cols, const int *ring, const std::vector<double> &prof,
+                                   double *rho) {
   const int nc = g.nt - 1;
   for (int q = 0; q < ncol; ++q) {
     const int i = ring[q];
     ds_column(cols[q], nc, t.R_av[i], g.Mstar, Temp + (size_t)i * nc, g.V + (size_t)i * nc, &t.z[(size_t)i * nc],
-              t.st.data(), t.ct.data(), t.cot.data(), t.theta_av.data(), rho + (size_t)q * nc);
+              t.st.data(), t.ct.data(), t.cot.data(), t.theta_av.data(),
+              cols[q].pre >= 0 ? &prof[(size_t)cols[q].pre] : nullptr, rho + (size_t)q * nc);
   }
 }
 

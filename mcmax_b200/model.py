@@ -1143,6 +1143,11 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
         raise ValueError("mpset and fixmpset: one settling prescription at a time")
     run["iterate"] = any(not z["fix"] for z in zones) or v("iter", False, bool) or (mpset and bool(zones))
     run["settling"] = None
+    run["fixed"] = None
+    if v("fixmpset", False, bool):
+        # FixedMPSettling again at the start of every structure pass
+        # (DiskStructure.f:108), from the state the pass starts from
+        run["fixed"] = dict(rho=rho_g, rv=rv, alpha=v("alphaturb", 1e-4), gas2dust=v("gas2dust", 100.0))
     if mpset:
         # MPSettling's inputs (Init.f:2906, 3070: the zones' alphaturb on their rings)
         R_av = AU * 10.0 ** ((np.log10(R[:-1]) + np.log10(R[1:])) / 2.0)

@@ -185,14 +185,14 @@ def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opac
         from . import structure as S
         structure = S.iterate(ctx, m, run["zones"], run["Mstar"], nphot, run=rad, maxiter=run["maxiter"],
                               epsiter=run["epsiter"], nphotdiffuse=run["nphotdiffuse"], dtdiffuse=run["dtdiffuse"],
-                              precision=precision, thin=True, settling=run.get("settling"))
+                              precision=precision, thin=True, settling=run.get("settling"), fixed=run.get("fixed"))
         T, n, res = structure["T"], structure["nphot"], structure["result"]
     else:
         if run.get("thin_start"):
             # a power-law density: its vertical structure at the optically
             # thin temperatures, then one pass (Init.f:3924-3960)
             from . import structure as S
-            S.thin_start(ctx, m, run["zones"], run["Mstar"], settling=run.get("settling"))
+            S.thin_start(ctx, m, run["zones"], run["Mstar"], settling=run.get("settling"), fixed=run.get("fixed"))
         ctx.set_model(m)
         n, res = ctx.mcradiation(int(nphot), precision=precision, **rad)
         T, dT, dE = ctx.finalize_t()

@@ -15,6 +15,8 @@ the final structure (Main.f:778-790).
     initial_state(model)                      dens0 = dens, w0 = w, gasdens = dens (Init.f:3904)
     planck_means(model)                       Kp(iT) and Kpabsstar of every grain (Init.f:3785-3798)
     thin_temperature(model)                   OpticallyThin's temperatures (Radiation.f:1253-1370)
+    mp_settling(...)                          MPSettling's per-grain scale factors (MPSettling.f:8-121)
+    fixed_settling(...)                       FixedMPSettling's factors (MPSettling.f:132-168)
     thin_start(ctx, model, zones, Mstar)      the structure the first pass starts from (Init.f:3924-3960)
     iterate(ctx, model, zones, Mstar, nphot)  the loop
 """
@@ -177,7 +179,51 @@ def mp_settling(model, state, T, Mstar, rho, rv, alpha, rscale=None, gas2dust=10
     return scale
 
 
-def thin_start(ctx, model, zones, Mstar, shscale=None, grain_scale=None, settling=None):
+def fixed_settling(model, state, rho, rv, alpha, rscale=None, gas2dust=100.0):
+    """Dust scale-height factors of FixedMPSettling (MPSettling.f:132-168),
+    which DiskStructure recomputes at the start of every structure pass
+    (DiskStructure.f:108): per ring i the gas surface density Sigma =
+    sum_j gasdens gas2dust V / (pi (R(i+1)^2 - R(i)^2) AU^2), per grain the
+    density-weighted mean of rho rv rscale over the ring's cells (rho rv
+    when the grain is absent), hH = (1/3)^(1/4) sqrt(alpha Sigma /
+    (sqrt(2 pi) <rho rv rscale>)) and the factor hH / sqrt(1 + hH^2).
+    alpha: a number or one value per ring (the midplane cell's alphaturb);
+    the sums over theta are numpy's.  Returns grain_scale (ngrains, nr) of
+    mcg_disk_structure (ring 0 unused, 1)."""
+    from .model import AU
+    nr, nc = model.nr, model.nt - 1
+    ng = model.ncomp
+    dens = np.asarray(state["dens"], float).reshape(nr, nc)
+    gas = np.asarray(state["gasdens"], float).reshape(nr, nc)
+    w = np.asarray(state["w"], float).reshape(nr, nc, ng)
+    V = np.asarray(model.V, float).reshape(nr, nc)
+    R = np.asarray(model.R, float)
+    rho = np.asarray(rho, float)
+    rv = np.asarray(rv, float)
+    rscale = np.ones(ng) if rscale is None else np.asarray(rscale, float)
+    alpha = np.broadcast_to(np.asarray(alpha, float), (nr,))
+    c1 = (1.0 / (1.0 + 2.0)) ** 0.25
+    scale = np.ones((ng, nr))
+    for i in range(1, nr):
+        sigma = (gas[i] * gas2dust * V[i]).sum() / (math.pi * (R[i + 1] ** 2 - R[i] ** 2) * AU ** 2)
+        dw = dens[i][:, None] * w[i]                                  # (nc, ng)
+        tot = dw.sum(0)
+        t = (dw * (rho * rv * rscale)[None, :]).sum(0)
+        t = np.where(tot > 1e-100, t / np.where(tot > 1e-100, tot, 1.0), rho * rv)
+        hH = c1 * np.sqrt(alpha[i] * sigma / (math.sqrt(2.0 * math.pi) * t))
+        scale[:, i] = hH / np.sqrt(1.0 + hH ** 2)
+    return scale
+
+
+def _grain_scale(model, state, T, Mstar, grain_scale, settling, fixed):
+    if fixed:
+        return fixed_settling(model, state, **fixed)
+    if settling:
+        return mp_settling(model, state, T, Mstar, **settling)
+    return grain_scale
+
+
+def thin_start(ctx, model, zones, Mstar, shscale=None, grain_scale=None, settling=None, fixed=None, shtype=None):
     """The vertical structure the first Monte Carlo pass starts from
     (Init.f:3924-3960): dens0 = gasdens = dens, the optically thin
     temperatures (BackWarming(1) changes nothing before the first pass:
@@ -185,17 +231,19 @@ def thin_start(ctx, model, zones, Mstar, shscale=None, grain_scale=None, settlin
     TempAverage copies them) and three DiskStructure passes on them.
     settling: the keyword arguments of mp_settling (rho, rv, alpha,
     rscale, gas2dust) when the grains settle (mpset); their factors are
-    then recomputed before every pass, at the thin temperatures.
+    then recomputed before every pass, at the thin temperatures.  fixed:
+    the keyword arguments of fixed_settling (fixmpset), recomputed before
+    every pass the same way.  shtype: per grain its scale-height type
+    (Context.disk_structure).
     Regridding in theta and dead zones are not built.  Updates the model's
     dens and comp_w; returns dict(state, Temp)."""
     state = initial_state(model)
     Tthin = thin_temperature(model)
     Temp = temp_average(None, Tthin, 1.0)
     for _ in range(3):
-        if settling:
-            grain_scale = mp_settling(model, state, Tthin, Mstar, **settling)
+        grain_scale = _grain_scale(model, state, Tthin, Mstar, grain_scale, settling, fixed)
         out = ctx.disk_structure(model.R, model.Theta, model.V, Mstar, zones, Temp, state["dens"], state["dens0"],
-                                 state["gasdens"], state["w"], state["w0"], shscale, grain_scale)
+                                 state["gasdens"], state["w"], state["w0"], shscale, grain_scale, shtype)
         state = dict(zip(("dens", "dens0", "gasdens", "w", "w0"), out))
     model.dens = state["dens"]
     model.comp_w = state["w"].reshape(model.ncell, -1)
@@ -204,7 +252,7 @@ def thin_start(ctx, model, zones, Mstar, shscale=None, grain_scale=None, settlin
 
 def iterate(ctx, model, zones, Mstar, nphot, run=None, maxiter=10, epsiter=3.0, f_weight=0.5, niter0=1000,
             nphotdiffuse=25, dtdiffuse=1.0, shscale=None, grain_scale=None, precision="mixed", log=None,
-            thin=False, settling=None):
+            thin=False, settling=None, fixed=None, shtype=None, on_pass=None):
     """Run the structure iterations on `model` (one opacity set per grain:
     comp_w holds the grains' abundances).  zones: (rin, rout, sh, rsh,
     shpow, denspow, fix_struct) per zone; Mstar in g; run: the keyword
@@ -212,14 +260,17 @@ def iterate(ctx, model, zones, Mstar, nphot, run=None, maxiter=10, epsiter=3.0, 
     structure (thin_start), as the reference does before its first pass;
     otherwise from the model's densities.  settling: mp_settling's keyword
     arguments when the grains settle (mpset): the factors are recomputed
-    from the current state and temperatures before every structure pass.
+    from the current state and temperatures before every structure pass;
+    fixed: fixed_settling's arguments (fixmpset), recomputed the same way.
+    shtype: per grain its scale-height type.  on_pass(n, result, T): called
+    after every packet run (n the run's packet count).
     The model's dens and comp_w are updated in place.  Returns dict(T, dT,
     Temp, state, history, nphot, result) with one history entry (niter,
     errT, packets) per structure pass and the last packet run's count and
     result."""
     run = dict(run or {})
     if thin:
-        state = thin_start(ctx, model, zones, Mstar, shscale, grain_scale, settling)["state"]
+        state = thin_start(ctx, model, zones, Mstar, shscale, grain_scale, settling, fixed, shtype)["state"]
     else:
         state = initial_state(model)
     Temp = None
@@ -235,6 +286,8 @@ def iterate(ctx, model, zones, Mstar, nphot, run=None, maxiter=10, epsiter=3.0, 
         T, dT, _ = ctx.finalize_t()
         if nphotdiffuse > 0 or dtdiffuse < 1.0:
             T, _, _ = ctx.diffuse(res["Ni"], dT, T, nphotdiffuse, dtdiffuse, run.get("factRW", 10.0))
+        if on_pass:
+            on_pass(n, res, T)
         if lastiter or maxiter <= 0:
             break
         niter += 1
@@ -245,10 +298,9 @@ def iterate(ctx, model, zones, Mstar, nphot, run=None, maxiter=10, epsiter=3.0, 
         else:
             fw = 1.0
         Temp = temp_average(Temp, T, fw)
-        if settling:
-            grain_scale = mp_settling(model, state, T, Mstar, **settling)
+        grain_scale = _grain_scale(model, state, T, Mstar, grain_scale, settling, fixed)
         out = ctx.disk_structure(model.R, model.Theta, model.V, Mstar, zones, Temp, state["dens"], state["dens0"],
-                                 state["gasdens"], state["w"], state["w0"], shscale, grain_scale)
+                                 state["gasdens"], state["w"], state["w0"], shscale, grain_scale, shtype)
         state = dict(zip(("dens", "dens0", "gasdens", "w", "w0"), out))
         errT = compare_cells(Tprev, dTprev, T, dT, model.nr, model.nt)
         history.append(dict(niter=niter, errT=errT, packets=n))

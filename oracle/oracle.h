@@ -172,8 +172,8 @@ int orc_diffuse(int nr, int nt, const double *R, const double *Theta, const doub
  * grain_scale (ng*nR) may be NULL.  Cell arrays in/out as mcg_disk_structure. */
 int orc_disk_structure(int nR, int nTheta, int ng, const double *R, const double *Theta, const double *V,
                        double Mstar, int nzones, const double *zones, const double *shscale,
-                       const double *grain_scale, const double *Temp, double *dens, double *dens0, double *gasdens,
-                       double *w, double *w0);
+                       const double *grain_scale, const int *shtype, const double *Temp, double *dens,
+                       double *dens0, double *gasdens, double *w, double *w0);
 
 /* Ray-traced spectrum without a scattering field (TracePath + TraceFlux,
  * TraceMono.f:2032-2297 and 8-497): Kabs_c, Ksca_c per component (ncomp*nlam),

@@ -12,8 +12,11 @@
  * values; then the cells of the ring.  exp and log, and the powers of the
  * step-size control and the fixed-zone profile, are the deterministic
  * functions of detmath.h (the reference calls libm; they differ in the last
- * bits).  'DISK' grains only, no radiation pressure, gaps, halo or radial
- * iterations.
+ * bits).  Grains of the other scale-height types take the closed-form
+ * profiles of DiskStructure.f:248-344 (ZODI, HALO, LOBE, JET, SHELL, CYLI,
+ * CAVITY, WEDGE, an unknown type keeping log(dens w)), formed with the C
+ * library's functions; D%thet(j) is taken as acos(Theta(j)).  No radiation
+ * pressure, gaps, halo or radial iterations.
  */
 #include <math.h>
 #include <stdint.h>
@@ -107,10 +110,72 @@ static double odeint(const seg_t *s, double ystart, double eps, double h1) {
   return y;
 }
 
+/* the closed-form profiles of DiskStructure.f:248-344 (types as
+ * MCG_SH_*: 1 ZODI, 2 HALO, 3 LOBE, 4 JET, 5 SHELL, 6 CYLI, 7 CAVITY,
+ * 8 WEDGE, 9 unknown), rho[1..nc] for grain ii of the ring; th, z 1-based
+ * (theta_av, R_av cos theta_av), Theta the cos-theta edges, dw/wr the
+ * ring's dens and abundance rows */
+static void shape_profile(int type, int nc, double scale, double gsh, double Rav, double Rout, const double *th,
+                          const double *Theta, const double *z, const double *dw, const double *wr, int ng, int ii,
+                          double *rho) {
+  const double pi = PI_D;
+  switch (type) {
+    case 1:
+      for (int j = 1; j <= nc; ++j) rho[j] = log(0.15 + (double)0.85f * pow(cos(pi / 2.0 - th[j]), 28.0));
+      break;
+    case 2:
+      for (int j = 1; j <= nc; ++j) {
+        rho[j] = 0.0;
+        if (gsh < 0.0 && pi / 2.0 - th[j] > -gsh) rho[j] = -60.0;
+      }
+      break;
+    case 3:
+      for (int j = 1; j <= nc; ++j) {
+        const double a = ((th[j] * 180.0) / pi) / scale;
+        rho[j] = log10(exp(-(a * a)));
+      }
+      break;
+    case 4:
+      for (int j = 1; j <= nc; ++j) {
+        const double a = ((acos(Theta[j - 1]) * 180.0) / pi) / (scale * (Rav / Rout));
+        rho[j] = -(a * a);
+      }
+      break;
+    case 5:
+      for (int j = 1; j <= nc; ++j) rho[j] = log(1.0 + gsh * pow(sin(th[j]), 3.0));
+      break;
+    case 6:
+      rho[nc] = 0.0;
+      for (int j = nc - 1; j >= 1; --j) rho[j] = (z[j] / AU_D < scale) ? 0.0 : -60.0;
+      break;
+    case 7:
+      rho[nc] = 0.0;
+      rho[1] = -60.0;
+      for (int j = nc - 1; j >= 2; --j) {
+        const double Rcyl = Rav * sin(th[j]);
+        rho[j] = (z[j] / AU_D < ((Rcyl / AU_D) * (Rcyl / AU_D)) * scale) ? 0.0 : -60.0;
+      }
+      break;
+    case 8:
+      for (int j = 1; j <= nc; ++j) {
+        if (scale > 0.0)
+          rho[j] = ((180.0 * th[j]) / pi > scale) ? 0.0 : -60.0;
+        else
+          rho[j] = ((180.0 * th[j]) / pi < -scale) ? 0.0 : -60.0;
+      }
+      break;
+    default:
+      for (int j = 1; j <= nc; ++j) {
+        const double v = dw[j - 1] * wr[(size_t)(j - 1) * ng + (ii - 1)];
+        rho[j] = v > 1e-60 ? log(v) : -60.0;
+      }
+  }
+}
+
 int orc_disk_structure(int nR, int nTheta, int ng, const double *R, const double *Theta, const double *V,
                        double Mstar, int nzones, const double *zones, const double *shscale,
-                       const double *grain_scale, const double *Temp, double *dens, double *dens0, double *gasdens,
-                       double *w, double *w0) {
+                       const double *grain_scale, const int *shtype, const double *Temp, double *dens,
+                       double *dens0, double *gasdens, double *w, double *w0) {
   const int nc = nTheta - 1;
 #define CI(i, j) ((size_t)(i) * nc + ((j) - 1))
   double *Rav = (double *)malloc(sizeof(double) * nR), *th = (double *)malloc(sizeof(double) * (nc + 1));
@@ -148,7 +213,12 @@ int orc_disk_structure(int nR, int nTheta, int ng, const double *R, const double
           const double *zn = zones + 7 * iz;
           if (Rav[i] > zn[0] * AU_D && Rav[i] < zn[1] * AU_D && zn[6] == 0.0) fix = -1;
         }
-      if (fix < 0) {
+      const int type = (ii != 0 && shtype) ? shtype[ii - 1] : 0;
+      if (fix < 0 && type != 0) {
+        const double gsh = grain_scale ? grain_scale[(size_t)(ii - 1) * nR + i] : 1.0;
+        shape_profile(type, nc, scale, gsh, Rav[i], Rav[nR - 1], th, Theta, z, dens + CI(i, 1), w + CI(i, 1) * ng,
+                      ng, ii, &RHO(0, ii));
+      } else if (fix < 0) {
         RHO(nc, ii) = 0.0;
         if (scale > 0.0) {
           for (int j = nc - 1; j >= 1; --j) {

@@ -141,15 +141,16 @@ def band_solve(nb, w, coef, rhs):
 
 def _structure_call(fn, st, Temp, dens, dens0, gasdens, w, w0):
     """st: dict(nr, nt, ng, R, Theta, V, Mstar, zones [(rin, rout, sh, rsh,
-    shpow, denspow, fix)], shscale, grain_scale).  Returns the updated
-    (dens, dens0, gasdens, w, w0)."""
+    shpow, denspow, fix)], shscale, grain_scale, shtype (ng codes)).
+    Returns the updated (dens, dens0, gasdens, w, w0)."""
     out = [np.array(a, dtype=np.float64) for a in (dens, dens0, gasdens, w, w0)]
     zones = np.ascontiguousarray(np.array(st.get("zones", []), dtype=np.float64).reshape(-1))
     arrs = [np.ascontiguousarray(st[k], float) for k in ("R", "Theta", "V")]
     sh = None if st.get("shscale") is None else np.ascontiguousarray(st["shscale"], float)
     gs = None if st.get("grain_scale") is None else np.ascontiguousarray(st["grain_scale"], float)
+    sht = None if st.get("shtype") is None else np.ascontiguousarray(st["shtype"], np.int32)
     rc = fn(int(st["nr"]), int(st["nt"]), int(st["ng"]), P(arrs[0]), P(arrs[1]), P(arrs[2]), C.c_double(st["Mstar"]),
-            len(st.get("zones", [])), P(zones) if zones.size else None, P(sh), P(gs),
+            len(st.get("zones", [])), P(zones) if zones.size else None, P(sh), P(gs), P(sht),
             P(np.ascontiguousarray(Temp, float)), *[P(a) for a in out])
     assert rc == 0
     return tuple(out)

@@ -396,11 +396,12 @@ extern "C" int hc_band_solve(int nb, int w, const double *coef, const double *rh
 
 /* DiskStructure on the host: the host logic of mcg_disk_structure with its
  * kernels replaced by serial loops over the same per-column and per-cell
- * functions.  zones as orc_disk_structure (7 values each). */
+ * functions.  zones as orc_disk_structure (7 values each); shtype: ng
+ * scale-height types or NULL. */
 struct HostStructBackend {
   bool columns(const DsGrid &g, const DsTables &t, const double *Temp, int ncol, const DsColumn *cols,
-               const int *ring, double *rho) {
-    ds_columns_host(g, t, Temp, ncol, cols, ring, rho);
+               const int *ring, const std::vector<double> &prof, double *rho) {
+    ds_columns_host(g, t, Temp, ncol, cols, ring, prof, rho);
     return true;
   }
   bool cells(const DsGrid &g, const double *rho, double *dens, double *dens0, double *gasdens, double *w,
@@ -412,14 +413,14 @@ struct HostStructBackend {
 
 extern "C" int hc_disk_structure(int nR, int nTheta, int ng, const double *R, const double *Theta, const double *V,
                                  double Mstar, int nzones, const double *zones, const double *shscale,
-                                 const double *grain_scale, const double *Temp, double *dens, double *dens0,
-                                 double *gasdens, double *w, double *w0) {
+                                 const double *grain_scale, const int *shtype, const double *Temp, double *dens,
+                                 double *dens0, double *gasdens, double *w, double *w0) {
   std::vector<DsZone> zs(nzones > 0 ? nzones : 0);
   for (int k = 0; k < nzones; ++k) {
     const double *z = zones + 7 * k;
     zs[k] = DsZone{z[0], z[1], z[2], z[3], z[4], z[5], z[6] != 0.0};
   }
-  DsGrid g{nR, nTheta, ng, R, Theta, V, Mstar, nzones, zs.data(), shscale, grain_scale};
+  DsGrid g{nR, nTheta, ng, R, Theta, V, Mstar, nzones, zs.data(), shscale, grain_scale, shtype};
   HostStructBackend be;
   return ds_disk_structure(g, be, Temp, dens, dens0, gasdens, w, w0) ? 0 : 1;
 }

@@ -13,6 +13,7 @@ import hostcheck_ffi as H
 import models
 import oracle_ffi as O
 from mcmax_b200 import model as M
+from mcmax_b200.api import shtype_codes
 
 MU, G, KB = float(np.float32(2.3)) * 1.67262158e-24, 6.67300e-8, 1.3806503e-16
 SH = 0.05 * math.sqrt(2.0)
@@ -143,6 +144,71 @@ def test_wedge_zone_and_ring_factors(disk):
     assert np.all(g[:-1][~open_] < 1e-20 * g[-1])
 
 
+SHAPES = ("DISK", "ZODI", "HALO", "LOBE", "JET", "SHELL", "CYLI", "CAVITY", "WEDGE", "KEEP")
+
+
+def _shape_case():
+    """one grain of every scale-height type, with the factors the closed
+    forms read: HALO a wedge (negative factor), LOBE 30 degrees, JET 20,
+    SHELL 2, CYLI 3 AU, CAVITY 0.3, WEDGE 60 degrees"""
+    m = models.small_disk(nrad=20, ntheta=14, nlam=16, mdust=1e-4, ngrains=len(SHAPES))
+    dens = np.maximum(m.dens, 1e-50)
+    w = m.comp_w.copy()
+    state = dict(dens=dens.copy(), dens0=dens.copy(), gasdens=dens.copy(), w=w.copy(), w0=w.copy())
+    gs = np.ones((m.ncomp, m.nr))
+    for k, f in ((2, -0.5), (3, 30.0), (4, 20.0), (5, 2.0), (6, 3.0), (7, 0.3), (8, 60.0)):
+        gs[k] = f
+    st = _st(m, [(0.5, 100.0, SH, 1.0, 1.125, 1.0, 0)], grain_scale=gs, shtype=np.arange(len(SHAPES), dtype=np.int32))
+    return m, state, st, gs
+
+
+def test_scale_height_types_match_oracle_and_closed_forms():
+    """DiskStructure.f:248-344: each grain's new profile along theta is its
+    type's closed form, renormalised to the grain's mass in the ring; the
+    host logic and the oracle agree bit for bit"""
+    m, s, st, gs = _shape_case()
+    T = _temp(m)
+    o = _run(O.disk_structure, st, T, s)
+    h = _run(H.disk_structure, st, T, s)
+    for k in o:
+        assert np.array_equal(o[k], h[k]), k
+    R_av, th, nc = _geometry(m)
+    thet = np.arccos(m.Theta[:-1])
+    V = m.V.reshape(m.nr, nc)
+    grain = (h["dens0"][:, None] * h["w0"]).reshape(m.nr, nc, m.ncomp)
+    old = (s["dens"][:, None] * s["w"]).reshape(m.nr, nc, m.ncomp)
+    deg = np.degrees(th)
+    for i in (5, 12, 19):
+        z = R_av[i] * np.cos(th) / M.AU
+        rc = R_av[i] * np.sin(th) / M.AU
+        expect = {
+            1: 0.15 + 0.85 * np.cos(np.pi / 2 - th) ** 28,
+            2: np.where(np.pi / 2 - th > 0.5, 0.0, 1.0),
+            3: np.exp(-(deg / 30.0) ** 2 / math.log(10.0)),
+            4: np.exp(-(np.degrees(thet) / (20.0 * R_av[i] / R_av[-1])) ** 2),
+            5: 1.0 + 2.0 * np.sin(th) ** 3,
+            6: np.where((z < 3.0) | (np.arange(nc) == nc - 1), 1.0, 0.0),
+            7: np.where(np.arange(nc) == nc - 1, 1.0,
+                        np.where((np.arange(nc) > 0) & (z < rc ** 2 * 0.3), 1.0, 0.0)),
+            8: np.where(deg > 60.0, 1.0, 0.0),
+            9: old[i, :, 9],
+        }
+        for k, e in expect.items():
+            e = e * (old[i, :, k] * V[i]).sum() / (e * V[i]).sum()
+            got = grain[i, :, k]
+            big = e > 1e-30 * e.max()
+            assert np.allclose(got[big], e[big], rtol=1e-9), (SHAPES[k], i)
+            assert np.all(got[~big] < 1e-20 * e.max()), (SHAPES[k], i)
+
+
+def test_scale_height_names_map_to_codes():
+    from mcmax_b200.api import McgError, shtype_codes
+    assert list(shtype_codes(["disk", "ZODI", "Halo", "lobe", "JET", "shell", "CYLI", "CAVITY", "WEDGE", "SPIRAL"],
+                             10)) == list(range(10))
+    with pytest.raises(McgError):
+        shtype_codes(["DISK"], 2)
+
+
 # ---------------------------------------------------------------- the iteration driver
 from mcmax_b200 import structure as S  # noqa: E402
 
@@ -169,6 +235,7 @@ class _FakeRun:
         self.temps = list(temps)
         self.calls = dict(mc=0, ds=0, diffuse=0)
         self.dens_seen = []
+        self.grain_scales = []
 
     def set_model(self, m):
         self.model = m
@@ -187,10 +254,12 @@ class _FakeRun:
         return T, None, (0, 0, 0, 0)
 
     def disk_structure(self, R, Theta, V, Mstar, zones, Temp, dens, dens0, gasdens, w, w0, shscale=None,
-                       grain_scale=None):
+                       grain_scale=None, shtype=None):
         self.calls["ds"] += 1
+        self.grain_scales.append(grain_scale)
         st = dict(nr=R.size - 1, nt=Theta.size, ng=np.asarray(w).shape[1], R=R, Theta=Theta, V=V, Mstar=Mstar,
-                  zones=zones, shscale=shscale, grain_scale=grain_scale)
+                  zones=zones, shscale=shscale, grain_scale=grain_scale,
+                  shtype=None if shtype is None else shtype_codes(shtype, np.asarray(w).shape[1]))
         out = H.disk_structure(st, Temp, dens, dens0, gasdens, np.ravel(w), np.ravel(w0))
         ncell = np.asarray(dens).size
         return out[0], out[1], out[2], out[3].reshape(ncell, -1), out[4].reshape(ncell, -1)
@@ -327,3 +396,38 @@ def test_settling_factors_reach_each_structure_pass():
     S.iterate(fake, m, zones, 2.5 * M.MSUN, 1000, thin=True, settling=settling)
     assert len(seen) == fake.calls["ds"] and all(g is not None and g.shape == (2, m.nr) for g in seen)
     assert all(np.all(g[1, 1:] < g[0, 1:]) for g in seen)
+
+
+def test_fixed_settling_factors_match_the_start_settling():
+    """FixedMPSettling's factors from the structure state equal those the
+    fixed-zone settling of the deck set-up applies (the same surface
+    density and grain stopping parameter); larger grains settle more"""
+    m = _driver_model()
+    st = S.initial_state(m)
+    nr, nc = m.nr, m.nt - 1
+    rho = np.array([3.0, 2.0])
+    rv = np.array([1e-5, 1e-2])
+    sc = S.fixed_settling(m, st, rho, rv, 1e-4)
+    assert sc.shape == (m.ncomp, nr) and np.all(sc[:, 0] == 1.0)
+    assert np.all(sc[1, 1:] < sc[0, 1:])
+    V = m.V.reshape(nr, nc)
+    d = st["dens"].reshape(nr, nc)
+    for i in (4, 11):
+        sigma = (d[i] * 100.0 * V[i]).sum() / (math.pi * (m.R[i + 1] ** 2 - m.R[i] ** 2) * M.AU ** 2)
+        for k in range(2):
+            hH = (1.0 / 3.0) ** 0.25 * math.sqrt(1e-4 * sigma / (math.sqrt(2 * math.pi) * rho[k] * rv[k]))
+            assert abs(sc[k, i] / (hH / math.sqrt(1 + hH * hH)) - 1) < 1e-12
+
+
+def test_fixed_settling_and_shapes_reach_each_structure_pass():
+    m = _driver_model()
+    T = _temp(m)
+    fake = _FakeRun([T])
+    zones = [(0.5, 100.0, SH, 1.0, 1.125, 1.0, 0)]
+    fixed = dict(rho=np.array([3.0, 3.0]), rv=np.array([1e-5, 1e-2]), alpha=1e-4)
+    passes = []
+    S.iterate(fake, m, zones, 2.5 * M.MSUN, 1000, thin=True, fixed=fixed, shtype=["DISK", "DISK"], maxiter=2,
+              epsiter=0.0, on_pass=lambda n, res, t: passes.append(n))
+    assert len(fake.grain_scales) == fake.calls["ds"] == 3 + 3
+    assert all(g is not None and np.all(g[1, 1:] < g[0, 1:]) for g in fake.grain_scales)
+    assert passes == [1000] * fake.calls["mc"] and fake.calls["mc"] == 4

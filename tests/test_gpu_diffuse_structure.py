@@ -56,3 +56,16 @@ def test_disk_structure_matches_replay_and_oracle(ctx):
     for a, b, c, name in zip(got, ref, orc, ("dens", "dens0", "gasdens", "w", "w0")):
         assert np.array_equal(np.ravel(a), np.ravel(b)), name
         assert np.array_equal(np.ravel(a), np.ravel(c)), name
+
+
+def test_scale_height_types_match_oracle(ctx):
+    """a grain of every scale-height type (DiskStructure.f:248-344): the
+    device against the oracle bit for bit"""
+    from test_dstruct import SHAPES, _shape_case, _temp
+    m, s, st, gs = _shape_case()
+    T = _temp(m)
+    got = ctx.disk_structure(m.R, m.Theta, m.V, st["Mstar"], st["zones"], T, s["dens"], s["dens0"], s["gasdens"],
+                             s["w"], s["w0"], grain_scale=gs, shtype=list(SHAPES))
+    orc = O.disk_structure(st, T, s["dens"], s["dens0"], s["gasdens"], s["w"].ravel(), s["w0"].ravel())
+    for a, c, name in zip(got, orc, ("dens", "dens0", "gasdens", "w", "w0")):
+        assert np.array_equal(np.ravel(a), np.ravel(c)), name

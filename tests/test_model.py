@@ -157,7 +157,7 @@ idum=-7
     assert abs(run.pop("Mstar") / (2.5 * M.MSUN) - 1) < 1e-15
     assert run == dict(seed=7, randomwalk=True, factRW=5.0, maxinteract=20000, maxruntime=-1.0, nruns=1, nphotdiffuse=25,
                        dtdiffuse=1.0, maxiter=10, epsiter=3.0, incangle=45.0, outputfits=False, posangle=0.0,
-                       iterate=True, thin_start=True, settling=None, vis_norm_fov=True)
+                       iterate=True, thin_start=True, settling=None, fixed=None, vis_norm_fov=True)
     assert np.allclose(m.comp_w.sum(1), 1.0)
     ref = M.disk_model(None, nrad=12, ntheta=8, nlam=20, lam2=3000.0, mdust=1e-5, sh=0.0707, ngrains=3,
                        opacities=(m.Kabs, m.Ksca, m.F))

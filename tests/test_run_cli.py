@@ -73,7 +73,7 @@ class FakeContext:
         return np.full(len(lam_obs), 1e20), (100, 0)
 
     def disk_structure(self, R, Theta, V, Mstar, zones, Temp, dens, dens0, gasdens, w, w0, shscale=None,
-                       grain_scale=None):
+                       grain_scale=None, shtype=None):
         self.structure_calls = getattr(self, "structure_calls", 0) + 1
         self.structure_zones = zones
         return (np.array(dens), np.array(dens0), np.array(gasdens), np.array(w), np.array(w0))
