@@ -799,11 +799,15 @@ def learned_disk_parts(lam, ngrains=50, amin=0.01, amax=1000.0, apow=3.5, ns=5, 
 def learned_disk_model(ctx, *, opacity="dhs", params=None, tstar=10000.0, rstar=2.5, rin=0.5, rout=100.0,
                        mdust=1e-3, sh=0.05 * math.sqrt(2.0), rsh=1.0, shpow=1.125, denspow=1.0, nrad=200,
                        ntheta=120, lam1=0.1, lam2=3000.0, nlam=200, ngrains=50, amin=0.01, amax=1000.0, apow=3.5,
-                       ns=5, nf=20, rho=3.0, alpha=1e-3, scat_how=2, compositions=LEARNED_COMPOSITIONS):
+                       ns=5, nf=20, rho=3.0, alpha=1e-3, scat_how=2, compositions=LEARNED_COMPOSITIONS,
+                       settle=True):
     """The learned-opacities deck: three compositions in ngrains log bins
     each, equal mass per composition and MRN within it, vertically settled
-    with alpha (FixedMPSettling), opacities from the DHS kernels
-    (opacity='dhs') or from the surrogate network (opacity='surrogate').
+    with alpha (FixedMPSettling; settle=False leaves the zone's unsettled
+    profile, for a structure loop that settles the grains itself),
+    opacities from the DHS kernels (opacity='dhs') or from the surrogate
+    network (opacity='surrogate').  The model carries each grain bin's
+    density (rho_grain, g/cm^3) and size (rv, cm) for the settling.
     Returns (model, opacity-stage seconds, bins served by the network)."""
     import time
     rstar_cm = rstar * RSUN
@@ -840,11 +844,14 @@ def learned_disk_model(ctx, *, opacity="dhs", params=None, tstar=10000.0, rstar=
     w = np.tile(w0, (nr, nc, 1))
     rho_grain = np.array([r["rho_av"] for r in res])
     rv = np.array([grain_rv(p["amin"], p["amax"], apow, ns) for p in parts])
-    dens2, w2 = fixed_mp_settling(R, Theta, ntheta, dens, V, w, rho_grain, rv, alpha, zone)
+    if settle:
+        dens2, w2 = fixed_mp_settling(R, Theta, ntheta, dens, V, w, rho_grain, rv, alpha, zone)
+    else:
+        dens2, w2 = dens, w
     m = Model(nr=nr, nt=Theta.size, R=R, Theta=Theta, SinTheta=SinTheta, thet=thet, dens=dens2.reshape(-1),
               V=V.reshape(-1), ncomp=ncomp, comp_w=w2.reshape(nr * nc, ncomp), nlam=nlam, lam=lam, nu=nu,
               Kabs=Kabs, Ksca=Ksca, F=F, BB=BB, Fstar=Fstar, Lstar=Lstar, Tstar=tstar, Rstar_cm=rstar_cm,
-              scat_how=scat_how, bins=bins, w=w0)
+              scat_how=scat_how, bins=bins, w=w0, rho_grain=rho_grain, rv=rv)
     return m, t_opac, served
 
 

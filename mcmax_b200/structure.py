@@ -263,7 +263,9 @@ def iterate(ctx, model, zones, Mstar, nphot, run=None, maxiter=10, epsiter=3.0, 
     from the current state and temperatures before every structure pass;
     fixed: fixed_settling's arguments (fixmpset), recomputed the same way.
     shtype: per grain its scale-height type.  on_pass(n, result, T): called
-    after every packet run (n the run's packet count).
+    after every packet run (n the run's packet count).  Each packet run
+    takes its own Philox key, run['seed'] plus the number of runs before
+    it, where the reference's one random stream runs on.
     The model's dens and comp_w are updated in place.  Returns dict(T, dT,
     Temp, state, history, nphot, result) with one history entry (niter,
     errT, packets) per structure pass and the last packet run's count and
@@ -282,7 +284,10 @@ def iterate(ctx, model, zones, Mstar, nphot, run=None, maxiter=10, epsiter=3.0, 
         model.dens = state["dens"]
         model.comp_w = state["w"].reshape(model.ncell, -1)
         ctx.set_model(model)
-        n, res = ctx.mcradiation(int(nphot), precision=precision, **run)
+        runk = dict(run)
+        if "seed" in runk:
+            runk["seed"] = int(runk["seed"]) + len(history)
+        n, res = ctx.mcradiation(int(nphot), precision=precision, **runk)
         T, dT, _ = ctx.finalize_t()
         if nphotdiffuse > 0 or dtdiffuse < 1.0:
             T, _, _ = ctx.diffuse(res["Ni"], dT, T, nphotdiffuse, dtdiffuse, run.get("factRW", 10.0))
