@@ -649,7 +649,6 @@ mcg_status mcg_run_prepare(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot, Run
   if ((s = ensure_run_buffers(ctx, nruns)) != MCG_OK) return s;
   if (run->randomwalk && (s = build_rw_tables(ctx, run->factRW)) != MCG_OK) return s;
   DevRun &R = ctx->run;
-  cudaStream_t st = ctx->stream;
   const int64_t Nphot = *nphot / nruns;
   if (Nphot < 1) return mcg_fail(ctx, MCG_ERR_ARG, "mcradiation: NphotTot/nruns must be >= 1");
   if (Nphot * nruns > (int64_t)2000000000)

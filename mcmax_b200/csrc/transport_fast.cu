@@ -100,11 +100,6 @@ __global__ void sum_cast_kernel(long long n, const double *a, const double *b, R
   if (t < n) c[t] = (R)(a[t] + b[t]);
 }
 
-__global__ void sum_kernel(long long n, const double *a, const double *b, double *c) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < n) c[t] = a[t] + b[t];
-}
-
 /* shared-memory layout of one block */
 struct SmemPlan {
   size_t off_R, off_Th, off_ST, off_cdf, off_c2, off_s2, off_ka, off_ke, off_ks, bytes;

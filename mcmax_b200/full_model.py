@@ -4,7 +4,7 @@ images, on one GPU.
 
     python -m mcmax_b200.full_model [--nphot 1e9] [--passes 5] [--nrad 300] [--ntheta 200] [--nlam 300]
                                     [--alpha 1e-4] [--angles 20,45,80] [--npix 512] [--nint 1000]
-                                    [--image-lam 10,100] [--check] [--out DIR]
+                                    [--image-lam 10,100] [--check] [--floor] [--out DIR]
 
 Deck: the learned-opacities disk (three compositions of 50 log size bins
 from 0.01 to 1000 micron each, MRN within a composition, porosity and
@@ -34,6 +34,9 @@ agreement: final per-cell temperatures of the cells with at least 1e3
 absorption events in the last packet run (within 1 %), the ray-traced
 spectra (within 2 % where the flux is above 1e-6 of its peak) and the
 images (total flux, and the pixels above 1e-3 of the peak within 5 %).
+--floor runs the mixed pipeline once more with another seed and reports
+the same statistics against the first run: the Monte Carlo noise floor of
+the comparison, structure feedback included.
 
 Prints one JSON line: the timings of every stage (device-synchronised
 wall clock per call), the packet rate of every packet run, the structure
@@ -186,6 +189,7 @@ def parse_args(argv=None):
     ap.add_argument("--image-lam", default="10,100", help="image wavelengths, micron")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--check", action="store_true", help="also the FP64 + DHS pipeline, and the agreement")
+    ap.add_argument("--floor", action="store_true", help="also the mixed pipeline with another seed (noise floor)")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     a.nphot = int(a.nphot)
@@ -216,6 +220,9 @@ def main(argv=None):
         res["agreement"] = agreement(ref, mixed)
         res["speedup_loop"] = res["mixed_surrogate"]["packets_per_s_loop"] / res["fp64_dhs"]["packets_per_s_loop"]
         res["speedup_total"] = ref["timings"]["total_s"] / mixed["timings"]["total_s"]
+    if a.floor:
+        again = pipeline(ctx, a, "mixed", "surrogate", a.seed + 2000, log)
+        res["noise_floor"] = agreement(mixed, again)
     ctx.close()
     print(json.dumps(res))
     return res
