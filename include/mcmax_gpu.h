@@ -372,9 +372,9 @@ mcg_status mcg_disk_structure(mcg_ctx *ctx, const mcg_structure *s, const double
  * Telescope.f:137-160 -- TracePath (TraceMono.f:2032) once, then TraceFlux
  * (TraceMono.f:8) per wavelength -- for the thermal emission of the dust
  * (thermal contact, cell temperatures T) and the star seen through the
- * disk, on the current model.  The scattering field of TraceMono's second
- * Monte Carlo is not included (flux as with no scattered light), and a
- * component's extinction is Kabs + Ksca as uploaded.  The image has nphi
+ * disk, on the current model, with the scattered light of TraceMono's
+ * second Monte Carlo when the options ask for it (below).  A component's
+ * extinction is Kabs + Ksca as uploaded.  The image has nphi
  * angles over half the plane and radii from the tau = 0.1 radius at
  * lam_path, the fixed radii Rfix, nr points per radial cell (nr < 0: one
  * point every -nr cells), 30 over the stellar disk and the outer edge.
@@ -390,10 +390,37 @@ typedef struct {
   double lam_path;    /* micron; 0.55 for a spectrum */
   int32_t tracestar;  /* 1: add the star behind the disk */
   double dimstar;     /* factor on the star (1) */
+  /* scattered light (TraceMono, TraceMono.f:583-914): with nphot_scatter or
+   * nphot_star > 0 every wavelength of a full-Mueller model (every grid
+   * wavelength around it, for isotropic scattering) gets a field from
+   * nphot_star packets of single-scattered starlight (MakeStarScatter) and
+   * nphot_scatter Monte Carlo packets of star and thermal light, and the
+   * rays add twice its scattered source; an observation's defaults are
+   * 1000 and 1000 (Telescope.f:606-607).  Both 0: no scattered light. */
+  int64_t nphot_scatter;
+  int64_t nphot_star;
+  uint64_t seed_scatter; /* Philox key of the first field of the call; each later field takes the next key */
+  int32_t nexits;        /* EmissionDistribution's exit rays per cell: 0 none, else >= 2 (observation default 5) */
 } mcg_trace_opts;
 
 mcg_status mcg_trace_spectrum(mcg_ctx *ctx, const mcg_trace_opts *opts, const double *T, int32_t nobs,
                               const double *lam_obs, double *flux, int32_t *info);
+
+/* One scattered-light field (one TraceMono call at lam0 for the inclination
+ * opts->angle, with opts' packet counts, key and nexits), for checking it:
+ * field[((i nsub + off(j) + irg - 1) 2 + side) 91 + b] with ring i, row j's
+ * sub-cell irg (off(j) = the sub-cells of the rows before j; a row of a
+ * full-Mueller model has int((thet(j+1) - thet(j)) 270 / pi) sub-cells, at
+ * least one, an isotropic model one), side 0 above the midplane, bin b = 0
+ * the accumulated E v AU (half of it on each side for isotropic scattering)
+ * and b = 1..90 the folded azimuth bins towards the observer
+ * (makescattfield, TraceMono.f:1416-1497).  cap: doubles field can hold;
+ * field may be NULL to ask for the size.  info: [0] nsub, [1] doubles of
+ * the field, [2] packets ended by a geometry failure, [3] packets ended by
+ * the interaction cap (1e6), [4] packets with no start after 1000 draws,
+ * [5] the mode (0 no field, 1 isotropic, 2 angular). */
+mcg_status mcg_scatter_field(mcg_ctx *ctx, const mcg_trace_opts *opts, const double *T, double lam0, double *field,
+                             int64_t cap, int64_t *info);
 
 /* Rectangular image at one wavelength: the 'IMAGE' observation of
  * Telescope.f:162-182 -- TracePath at lam0 (opts->lam_path = lam0 as the

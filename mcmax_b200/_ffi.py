@@ -60,7 +60,8 @@ SHTYPES = ("DISK", "ZODI", "HALO", "LOBE", "JET", "SHELL", "CYLI", "CAVITY", "WE
 class TraceOpts(C.Structure):
     _fields_ = [("angle", C.c_double), ("nphi", C.c_int32), ("nr", C.c_int32), ("nRfix", C.c_int32),
                 ("Rfix", C.POINTER(C.c_double)), ("lam_path", C.c_double), ("tracestar", C.c_int32),
-                ("dimstar", C.c_double)]
+                ("dimstar", C.c_double), ("nphot_scatter", C.c_int64), ("nphot_star", C.c_int64),
+                ("seed_scatter", C.c_uint64), ("nexits", C.c_int32)]
 
 
 class ImageOpts(C.Structure):
@@ -137,6 +138,8 @@ SIGNATURES = {
     "mcg_finalize_t": (C.c_int, [C.c_void_p, dp, dp, dp]),
     "mcg_trace_spectrum": (C.c_int, [C.c_void_p, C.POINTER(TraceOpts), dp, C.c_int32, dp, dp,
                                      C.POINTER(C.c_int32)]),
+    "mcg_scatter_field": (C.c_int, [C.c_void_p, C.POINTER(TraceOpts), dp, C.c_double, dp, C.c_int64,
+                                    C.POINTER(C.c_int64)]),
     "mcg_trace_image": (C.c_int, [C.c_void_p, C.POINTER(TraceOpts), dp, C.c_double, C.POINTER(ImageOpts), dp, dp,
                                   C.POINTER(C.c_int32)]),
     "mcg_disk_structure": (C.c_int, [C.c_void_p, C.POINTER(Structure), dp, dp, dp, dp, dp, dp]),

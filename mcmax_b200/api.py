@@ -214,26 +214,56 @@ class Context:
         self._check(self.lib.mcg_finalize_t(self.h, _ffi.ptr(T), _ffi.ptr(dT), _ffi.ptr(dE)))
         return T, dT, dE
 
+    @staticmethod
+    def _trace_opts(angle, nphi, nr, Rfix, lam_path, tracestar, dimstar, scatter):
+        sc = dict(nphot=0, nphot_star=0, seed=1, nexits=5)
+        sc.update(scatter or {})
+        return _ffi.TraceOpts(float(angle), int(nphi), int(nr), int(Rfix.size), _ffi.ptr(Rfix) if Rfix.size else None,
+                              float(lam_path), int(bool(tracestar)), float(dimstar), int(sc["nphot"]),
+                              int(sc["nphot_star"]), int(sc["seed"]) & (2 ** 64 - 1), int(sc["nexits"]))
+
     def trace_spectrum(self, T, lam_obs, angle, nphi=45, nr=2, Rfix=(), lam_path=0.55, tracestar=True,
-                       dimstar=1.0):
+                       dimstar=1.0, scatter=None):
         """mcg_trace_spectrum on the current model: the ray-traced flux at
         inclination `angle` [rad] for each wavelength of lam_obs, from the
-        cell temperatures T.  Returns (flux, info) with flux in the
-        reference's units (x 1e23 / distance^2 for Jy) and info = (image
-        radii, rays ended by a geometry failure)."""
+        cell temperatures T.  scatter: the scattered-light field's
+        settings, dict(nphot, nphot_star, seed, nexits) (an observation's
+        defaults are 1000, 1000, -, 5; None or both counts 0: no scattered
+        light).  Returns (flux, info) with flux in the reference's units
+        (x 1e23 / distance^2 for Jy) and info = (image radii, rays ended by
+        a geometry failure)."""
         T = _f64(T).reshape(-1)
         lam_obs = _f64(np.atleast_1d(lam_obs))
         Rfix = _f64(np.atleast_1d(np.asarray(Rfix, float)))
-        o = _ffi.TraceOpts(float(angle), int(nphi), int(nr), int(Rfix.size), _ffi.ptr(Rfix) if Rfix.size else None,
-                           float(lam_path), int(bool(tracestar)), float(dimstar))
+        o = self._trace_opts(angle, nphi, nr, Rfix, lam_path, tracestar, dimstar, scatter)
         flux = np.zeros(lam_obs.size)
         info = np.zeros(2, np.int32)
         self._check(self.lib.mcg_trace_spectrum(self.h, C.byref(o), _ffi.ptr(T), lam_obs.size, _ffi.ptr(lam_obs),
                                                 _ffi.ptr(flux), _ffi.ptr(info)))
         return flux, (int(info[0]), int(info[1]))
 
+    def scatter_field(self, T, lam0, angle, nphot=1000, nphot_star=1000, seed=1, nexits=5):
+        """mcg_scatter_field: one scattered-light field of the current model
+        at wavelength lam0 [micron] for inclination `angle` [rad].  Returns
+        (field (nr, nsub, 2, 91), info dict) or (None, info) when the model
+        gets no field (no scattering)."""
+        T = _f64(T).reshape(-1)
+        o = self._trace_opts(angle, 45, 2, np.zeros(0), 0.55, True, 1.0,
+                             dict(nphot=nphot, nphot_star=nphot_star, seed=seed, nexits=nexits))
+        info = np.zeros(6, np.int64)
+        ip = info.ctypes.data_as(C.POINTER(C.c_int64))
+        self._check(self.lib.mcg_scatter_field(self.h, C.byref(o), _ffi.ptr(T), float(lam0), None, 0, ip))
+        keys = ("nsub", "length", "geometry_failures", "interaction_cap", "no_start", "mode")
+        if int(info[5]) == 0:
+            return None, dict(zip(keys, (int(x) for x in info)))
+        field = np.zeros(int(info[1]))
+        self._check(self.lib.mcg_scatter_field(self.h, C.byref(o), _ffi.ptr(T), float(lam0), _ffi.ptr(field),
+                                               field.size, ip))
+        out = dict(zip(keys, (int(x) for x in info)))
+        return field.reshape(self.model.nr, out["nsub"], 2, 91), out
+
     def trace_image(self, T, lam0, angle, npixel=500, nint=1000, Rmax=None, pa=0.0, nphi=45, nr=2, Rfix=(),
-                    tracestar=True, dimstar=1.0, seed=42, linear=None, lam_path=None):
+                    tracestar=True, dimstar=1.0, seed=42, linear=None, lam_path=None, scatter=None):
         """mcg_trace_image on the current model: the rectangular image at
         wavelength lam0 [micron] and inclination `angle` [rad] (MakeImage).
         Rmax: half the field of view [AU], by default the grid's outer radius
@@ -259,8 +289,7 @@ class Context:
         Rimg = np.zeros(cap)
         rphi = np.zeros(cap * int(nphi))
         lam_path = float(lam0) if lam_path is None else float(lam_path)
-        o = _ffi.TraceOpts(float(angle), int(nphi), int(nr), nRfix, _ffi.ptr(Rfix) if nRfix else None, lam_path,
-                           int(bool(tracestar)), float(dimstar))
+        o = self._trace_opts(angle, nphi, nr, Rfix, lam_path, tracestar, dimstar, scatter)
         io = _ffi.ImageOpts(int(npixel), int(nint), float(Rmax), float(pa), int(seed) & (2 ** 64 - 1),
                             int(bool(linear)), int(cap), _ffi.ptr(Rimg), _ffi.ptr(rphi))
         flux = np.zeros(1)

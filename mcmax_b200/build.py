@@ -27,10 +27,11 @@ UNITS = {
     "diffuse.cu": ["--fmad=false"],
     "dstruct.cu": ["--fmad=false"],
     "raytrace.cu": ["--fmad=false"],
+    "scatfield.cu": ["--fmad=false"],
 }
 HEADERS = ["detmath.h", "cplx.h", "philox.h", "dhs_core.cuh", "transport_core.cuh", "transport_fast.cuh",
            "mcg_internal.h", "tc_sm100.cuh", "diffuse_core.cuh", "transport_event.cuh",
-           "dstruct_core.cuh", "rt_core.cuh"]
+           "dstruct_core.cuh", "rt_core.cuh", "scat_core.cuh", "scatfield.h"]
 
 
 def _nvcc():

@@ -124,6 +124,13 @@ mcg_status mcg_trace_spectrum(mcg_ctx *ctx, const mcg_trace_opts *opts, const do
   return mcg_trace_spectrum_impl(ctx, opts, T, nobs, lam_obs, flux, info);
 }
 
+mcg_status mcg_scatter_field(mcg_ctx *ctx, const mcg_trace_opts *opts, const double *T, double lam0, double *field,
+                             int64_t cap, int64_t *info) {
+  if (!ctx) return MCG_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  return mcg_scatter_field_impl(ctx, opts, T, lam0, field, cap, info);
+}
+
 mcg_status mcg_trace_image(mcg_ctx *ctx, const mcg_trace_opts *opts, const double *T, double lam0,
                            const mcg_image_opts *io, double *flux, double *im, int32_t *info) {
   if (!ctx) return MCG_ERR_ARG;

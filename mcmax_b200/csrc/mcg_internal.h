@@ -184,6 +184,8 @@ mcg_status mcg_trace_spectrum_impl(mcg_ctx *ctx, const mcg_trace_opts *o, const 
                                    const double *lam_obs, double *flux, int32_t *info);
 mcg_status mcg_trace_image_impl(mcg_ctx *ctx, const mcg_trace_opts *o, const double *T, double lam0,
                                 const mcg_image_opts *io, double *flux, double *im, int32_t *info);
+mcg_status mcg_scatter_field_impl(mcg_ctx *ctx, const mcg_trace_opts *o, const double *T, double lam0, double *field,
+                                  int64_t cap, int64_t *info);
 mcg_status mcg_disk_structure_impl(mcg_ctx *ctx, const mcg_structure *s, const double *Temp, double *dens,
                                    double *dens0, double *gasdens, double *w, double *w0);
 mcg_status mcg_diffuse_impl(mcg_ctx *ctx, int32_t nphotmin, double dtmax, double factRW, const int32_t *Ni,

@@ -6,7 +6,9 @@
  *   rt_cell_kernel  one thread per cell: extinction and source function at
  *                   a wavelength
  *   rt_ray_kernel   one thread per image ray (radius, angle): the path
- *                   through the cells and the formal solution
+ *                   through the cells and the formal solution, with the
+ *                   scattered light of the field of scatfield.cu when the
+ *                   options ask for one
  * The image grid, the tau = 0.1 radius and the flux sum are host logic
  * shared with the test replay.
  *
@@ -28,6 +30,7 @@
 
 #include "mcg_internal.h"
 #include "rt_core.cuh"
+#include "scatfield.h"
 
 namespace {
 
@@ -44,12 +47,13 @@ __global__ void rt_cell_kernel(int ncell, int ncomp, int nlam, const double *com
 __global__ void rt_ray_kernel(const __grid_constant__ TModel m, const double *dens, const double *kext,
                               const double *emis, int nr, int nphi, const double *Rimg, const double *phi,
                               double angle, double fstar, double dimstar, int tracestar, double *image,
-                              unsigned int *bad) {
+                              unsigned int *bad, const __grid_constant__ RtScat sc, int has_sc) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nr * nphi) return;
   const int i = t / nphi, k = t % nphi;
   int steps;
-  image[t] = rt_ray(m, dens, kext, emis, Rimg[i], phi[k], angle, fstar, dimstar, tracestar, RT_MAXSTEPS, &steps);
+  image[t] = rt_ray(m, dens, kext, emis, Rimg[i], phi[k], angle, fstar, dimstar, tracestar, RT_MAXSTEPS, &steps,
+                    has_sc ? &sc : nullptr);
   if (steps < 0) atomicAdd(bad, 1u);
 }
 
@@ -118,6 +122,9 @@ struct RtDeviceBackend {
   size_t nimage = 0;
   const double *lam = nullptr; /* host copy */
   int nlam = 0;
+  SfState *sf = nullptr;       /* the scattered-light fields, or null */
+  RtScat sc{};
+  int has_sc = 0;
   std::string err;
 
   bool fail(cudaError_t e, const char *what) {
@@ -136,6 +143,27 @@ struct RtDeviceBackend {
     if (e == cudaSuccess) e = cudaMemcpyAsync(emis_out, emis, sizeof(double) * m.ncell, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     return e == cudaSuccess ? true : fail(e, "trace: cell kernel");
+  }
+  bool field(double lam0) {
+    has_sc = 0;
+    if (!sf || !sf->mode) return true;
+    const double *f1, *f2;
+    double w1, w2;
+    if (!sf->prepare(lam0, T, &f1, &f2, &w1, &w2)) {
+      err = sf->err;
+      return false;
+    }
+    sc.mode = sf->mode;
+    sc.g = sf->g;
+    sc.thet = sf->thet;
+    sc.f1 = f1;
+    sc.f2 = f2;
+    sc.w1 = w1;
+    sc.w2 = w2;
+    sc.albedo = sf->albedo;
+    sc.V = ctx->model.V;
+    has_sc = 1;
+    return true;
   }
   bool rays(const std::vector<double> &R, const std::vector<double> &phi, double fstar, const RtOptions &o,
             double *image, int *bad) {
@@ -157,7 +185,8 @@ struct RtDeviceBackend {
     e = cudaMemsetAsync(dbad, 0, sizeof(unsigned int), st);
     if (e != cudaSuccess) return fail(e, "trace: memset");
     rt_ray_kernel<<<nblk((long long)n, 128), 128, 0, st>>>(tm, ctx->model.dens, kext, emis, nr, nphi, dRimg, dphi,
-                                                           o.angle, fstar, o.dimstar, o.tracestar, dimage, dbad);
+                                                           o.angle, fstar, o.dimstar, o.tracestar, dimage, dbad, sc,
+                                                           has_sc);
     unsigned int hb = 0;
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(image, dimage, sizeof(double) * n, cudaMemcpyDeviceToHost, st);
@@ -184,6 +213,10 @@ static mcg_status rt_trace(mcg_ctx *ctx, const char *who, const mcg_trace_opts *
   if (o->nphi < 1 || o->nr == 0 || o->nphi > 100000 || (o->nRfix > 0 && !o->Rfix) || o->nRfix < 0 ||
       !(o->lam_path > 0.0))
     return mcg_fail(ctx, MCG_ERR_ARG, "%s: nphi >= 1, nr != 0, lam_path > 0 required", who);
+  if (o->nphot_scatter < 0 || o->nphot_star < 0 || o->nphot_scatter > 2000000000LL || o->nphot_star > 2000000000LL ||
+      o->nexits < 0 || o->nexits == 1 || o->nexits > 10000)
+    return mcg_fail(ctx, MCG_ERR_ARG, "%s: 0 <= nphot_scatter, nphot_star <= 2e9 and nexits 0 or 2..10000 required",
+                    who);
   const int ncell = m.ncell;
   for (int c = 0; c < ncell; ++c)
     if (!(T[c] >= 0.0) || !(T[c] < 1e6)) return mcg_fail(ctx, MCG_ERR_ARG, "%s: T[%d] = %g", who, c, T[c]);
@@ -224,6 +257,12 @@ static mcg_status rt_trace(mcg_ctx *ctx, const char *who, const mcg_trace_opts *
   be.tm.R = m.R;
   be.tm.Theta = m.Theta;
   RtOptions ro{o->angle, o->nphi, o->nr, o->nRfix, o->Rfix, o->lam_path, o->tracestar, o->dimstar};
+  SfState sf;
+  if (o->nphot_scatter > 0 || o->nphot_star > 0) {
+    SfOpts so{(long long)o->nphot_scatter, (long long)o->nphot_star, o->seed_scatter, o->nexits};
+    if (!sf.init(ctx, o->angle, so, Theta.data())) return mcg_fail(ctx, MCG_ERR_CUDA, "%s: %s", who, sf.err.c_str());
+    be.sf = &sf;
+  }
   *bad = 0;
   if (!rt_spectrum(hm, be, ro, m.nlam, lam.data(), Fstar.data(), dens.data(), nobs, lam_obs, flux, Rimg, image_last,
                    bad))
@@ -316,5 +355,48 @@ mcg_status mcg_trace_image_impl(mcg_ctx *ctx, const mcg_trace_opts *o, const dou
   }
   MCG_CUDA(ctx, cudaMemcpyAsync(im, dim, sizeof(double) * npix2, cudaMemcpyDeviceToHost, st));
   MCG_CUDA(ctx, cudaStreamSynchronize(st));
+  return MCG_OK;
+}
+
+mcg_status mcg_scatter_field_impl(mcg_ctx *ctx, const mcg_trace_opts *o, const double *T, double lam0, double *field,
+                                  int64_t cap, int64_t *info) {
+  DevModel &m = ctx->model;
+  if (!m.valid) return mcg_fail(ctx, MCG_ERR_STATE, "scatter_field: no model set");
+  if (!o || !T || !info || cap < 0) return mcg_fail(ctx, MCG_ERR_ARG, "scatter_field: missing argument");
+  if (o->nphot_scatter < 0 || o->nphot_star < 0 || o->nphot_scatter > 2000000000LL || o->nphot_star > 2000000000LL ||
+      o->nexits < 0 || o->nexits == 1 || o->nexits > 10000 || !(lam0 > 0.0))
+    return mcg_fail(ctx, MCG_ERR_ARG, "scatter_field: packet counts 0..2e9, nexits 0 or 2..10000, lam0 > 0");
+  const int ncell = m.ncell;
+  for (int c = 0; c < ncell; ++c)
+    if (!(T[c] >= 0.0) || !(T[c] < 1e6)) return mcg_fail(ctx, MCG_ERR_ARG, "scatter_field: T[%d] = %g", c, T[c]);
+  cudaStream_t st = ctx->stream;
+  std::vector<double> Theta(m.nt);
+  MCG_CUDA(ctx, cudaMemcpyAsync(Theta.data(), m.Theta, sizeof(double) * m.nt, cudaMemcpyDeviceToHost, st));
+  MCG_CUDA(ctx, cudaStreamSynchronize(st));
+  SfState sf;
+  SfOpts so{(long long)o->nphot_scatter, (long long)o->nphot_star, o->seed_scatter, o->nexits};
+  if (!sf.init(ctx, o->angle, so, Theta.data())) return mcg_fail(ctx, MCG_ERR_CUDA, "scatter_field: %s", sf.err.c_str());
+  for (int k = 0; k < 6; ++k) info[k] = 0;
+  info[5] = sf.mode;
+  if (!sf.mode) return MCG_OK;
+  info[0] = sf.gh.nsub;
+  info[1] = (int64_t)sf.field_len;
+  if (!field) return MCG_OK;
+  if (cap < (int64_t)sf.field_len)
+    return mcg_fail(ctx, MCG_ERR_ARG, "scatter_field: cap %lld < %zu", (long long)cap, sf.field_len);
+  RtMem mem;
+  double *dT, *dF;
+  cudaError_t e = mem.alloc(&dT, (size_t)ncell);
+  if (e == cudaSuccess) e = mem.alloc(&dF, sf.field_len);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dT, T, sizeof(double) * ncell, cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return mcg_fail(ctx, MCG_ERR_CUDA, "scatter_field: %s", cudaGetErrorString(e));
+  if (!sf.compute(lam0, dT, dF)) return mcg_fail(ctx, MCG_ERR_CUDA, "%s", sf.err.c_str());
+  unsigned long long hs[3] = {0, 0, 0};
+  MCG_CUDA(ctx, cudaMemcpyAsync(field, dF, sizeof(double) * sf.field_len, cudaMemcpyDeviceToHost, st));
+  MCG_CUDA(ctx, cudaMemcpyAsync(hs, sf.stats, sizeof hs, cudaMemcpyDeviceToHost, st));
+  MCG_CUDA(ctx, cudaStreamSynchronize(st));
+  info[2] = (int64_t)hs[0];
+  info[3] = (int64_t)hs[1];
+  info[4] = (int64_t)hs[2];
   return MCG_OK;
 }

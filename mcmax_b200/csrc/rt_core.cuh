@@ -2,8 +2,8 @@
  * rt_core.cuh -- ray-traced flux of the disk at one inclination (the
  * 'SPECTRUM' observation of Telescope.f:137-160: TracePath once, then
  * TraceFlux per wavelength), for the thermal emission of the dust and the
- * attenuated star.  No scattering field: the scattered light of TraceMono's
- * second Monte Carlo is not part of it, as in a run with scattering off.
+ * attenuated star, and with a scattered-light field (scat_core.cuh) its
+ * scattered light.
  *
  *   image rays     TracePath (TraceMono.f:2032-2297): radial points from the
  *                  tau = 0.1 radius along the midplane (tau01R,
@@ -14,9 +14,13 @@
  *                  cell-edge geometry (tp_trace2edge; Trace2edgeRG with one
  *                  sub-cell per cell is the same code)
  *   formal solution TraceFlux (TraceMono.f:331-474): emission
- *                  B(T) Kabs/Kext (1 - albedo) per cell, the exp(-tau)
- *                  attenuation with its tau < 1e-6 branch, the star's
- *                  intensity behind the disk
+ *                  B(T) Kabs/Kext (1 - albedo) per cell plus twice the
+ *                  scattered source of the field when there is one
+ *                  (sf_segment_source; the path then also carries the
+ *                  sub-cell, the folded azimuth bins of its ends and the
+ *                  side of the midplane it ends on, and steps with
+ *                  Trace2edgeRG), the exp(-tau) attenuation with its
+ *                  tau < 1e-6 branch, the star's intensity behind the disk
  *   flux           the trapezoid over image radii and angles (TraceMono.f:
  *                  481-497)
  *
@@ -38,6 +42,7 @@
 #include <algorithm>
 #include <vector>
 
+#include "scat_core.cuh"
 #include "transport_core.cuh"
 
 #ifdef __CUDACC__
@@ -121,39 +126,71 @@ RT_HD void rt_ray_start(const TModel &m, double Rimg, double phi, double angle, 
   tp_rotate(&p->vx, &p->vy, &p->vz, 0.0, 1.0, 0.0, angle);
 }
 
+/* the scattered-light field a ray pass reads: mode 2 the angular field
+ * of the wavelength (f1), mode 1 the isotropic fields of the grid
+ * wavelengths around it, weighted w1, w2 (TraceMono.f:255-262); albedo
+ * and V per cell */
+struct RtScat {
+  int mode;
+  SfGeom g;
+  const double *thet, *f1, *f2, *albedo, *V;
+  double w1, w2;
+};
+
 /* the intensity of one image ray: its path through the cells and the
  * formal solution (trace2dpath, TraceMono.f:331-474).  dens, kext, emis
- * per cell; fstar the star's flux at the wavelength.  Returns the
- * intensity; *steps the segments traced (capped at maxsteps, *steps < 0
- * when the cap or a geometry failure ended the ray). */
+ * per cell; fstar the star's flux at the wavelength; sc the scattered-light
+ * field or null.  Returns the intensity; *steps the segments traced
+ * (capped at maxsteps, *steps < 0 when the cap or a geometry failure ended
+ * the ray). */
 RT_HD double rt_ray(const TModel &m, const double *dens, const double *kext, const double *emis, double Rimg,
-                    double phi, double angle, double fstar, double dimstar, int tracestar, int maxsteps, int *steps) {
+                    double phi, double angle, double fstar, double dimstar, int tracestar, int maxsteps, int *steps,
+                    const RtScat *sc = nullptr) {
   TPkt p;
   rt_ray_start(m, Rimg, phi, angle, &p);
   const int nc = m.nt - 1;
+  const bool ang = sc && sc->mode == 2;
+  int irg = 1;
+  if (ang) irg = sf_irg(sc->g, sc->thet, p.j, acos(fabs(p.z) / m.R[m.nr]));
   double I = 0.0, tau = 0.0, fact = 1.0;
   int hitstar = 0, n = 0;
   for (;;) {
     double v;
-    int inext, jnext;
-    if (tp_trace2edge(m, p, &v, &inext, &jnext) != 0 || ++n > maxsteps) {
+    int inext, jnext, irgn = irg;
+    const int fail = ang ? sf_trace2edge_rg(m, sc->g, p, irg, &v, &inext, &jnext, &irgn)
+                         : tp_trace2edge(m, p, &v, &inext, &jnext);
+    if (fail != 0 || ++n > maxsteps) {
       *steps = -n;
       return I;
     }
     p.onEdge = 1;
     const int ip = p.i, jp = p.j;
+    const double x1 = p.x, y1 = p.y;
     p.x = p.x + p.vx * v;
     p.y = p.y + p.vy * v;
     p.z = p.z + p.vz * v;
     if (ip != 0) {
       const size_t c = (size_t)ip * nc + (jp - 1);
       const double tau_e = ((v * dens[c]) * kext[c]) * RT_AU;
+      double src = emis[c];
+      if (sc) {
+        const int side = p.z > 0.0 ? 0 : 1;
+        double xs;
+        if (ang) {
+          xs = sf_segment_source(sc->g, sc->f1, ip, jp, irg, side, sf_jphi(x1, y1), sf_jphi(p.x, p.y),
+                                 sc->albedo[c], sc->V[c]);
+        } else {
+          const size_t b = (c * 2 + side) * SF_NB;
+          xs = ((sc->w1 * sc->f1[b] + sc->w2 * sc->f2[b]) / sc->V[c]) * sc->albedo[c];
+        }
+        src = 2.0 * xs + emis[c];
+      }
       if (tau_e < 1e-6) {
-        I = I + (emis[c] * tau_e) * fact;
+        I = I + (src * tau_e) * fact;
         fact = fact * (1.0 - tau_e);
       } else {
         const double ex = dm_exp(-tau_e);
-        I = I + (emis[c] * (1.0 - ex)) * fact;
+        I = I + (src * (1.0 - ex)) * fact;
         fact = fact * ex;
       }
       tau = tau + tau_e;
@@ -169,6 +206,7 @@ RT_HD double rt_ray(const TModel &m, const double *dens, const double *kext, con
     }
     p.i = inext;
     p.j = jnext;
+    irg = irgn;
   }
   if (hitstar && tracestar) I = I + ((fstar * fact) * dimstar) / (RT_PI * ((m.R[0] * RT_AU) * (m.R[0] * RT_AU)));
   *steps = n;
@@ -322,9 +360,10 @@ struct RtOptions {
 };
 
 /* Backend: cells(lam0, kext[ncell], emis[ncell]) -> per-cell arrays (also
- * kept on the backend's side for the rays); rays(R, phi, fstar, image
- * [nr*nphi], steps) -> the intensities.  Returns false on an execution
- * error. */
+ * kept on the backend's side for the rays); field(lam0) -> the scattered
+ * light field the next rays read (nothing to do without one); rays(R, phi,
+ * fstar, image[nr*nphi], steps) -> the intensities.  Returns false on an
+ * execution error. */
 template <class Backend>
 bool rt_spectrum(const TModel &m, Backend &be, const RtOptions &o, int nlam, const double *lam, const double *Fstar,
                  const double *dens, int nobs, const double *lam_obs, double *flux, std::vector<double> *Rimg,
@@ -349,6 +388,7 @@ bool rt_spectrum(const TModel &m, Backend &be, const RtOptions &o, int nlam, con
     rt_lam(nlam, lam, lam_obs[l], &l1, &l2, &w1, &w2);
     const double fstar = Fstar[l1] * w1 + Fstar[l2] * w2;
     if (!be.cells(lam_obs[l], kext.data(), emis.data())) return false;
+    if (!be.field(lam_obs[l])) return false;
     int bad = 0;
     if (!be.rays(*Rimg, phi, fstar, o, image.data(), &bad)) return false;
     *bad_rays += bad;

@@ -170,6 +170,15 @@ int orc_diffuse(int nr, int nt, const double *R, const double *Theta, const doub
  * CheckMinimumDensity and CheckCells.  zones: 7 values per zone (rin, rout
  * [AU], sh, rsh, shpow, denspow, fix_struct as 0/1); shscale (nR) and
  * grain_scale (ng*nR) may be NULL.  Cell arrays in/out as mcg_disk_structure. */
+/* one scattered-light field of the ray tracer (TraceMono, TraceMono.f:583-
+ * 914) at lam0 for inclination angle, nphot Monte Carlo and nstar starlight
+ * packets with Philox key `key`; SF laid out as mcg_scatter_field's;
+ * info: [0] nsub, [1] geometry failures, [2] interaction-cap kills, [3]
+ * packets with no start.  Kabs_c, Ksca_c: ncomp*nlam; T per cell. */
+int orc_scatter_field(const orc_model *m, const double *Kabs_c, const double *Ksca_c, const double *T, int scat_how,
+                      double angle, double lam0, int64_t nphot, int64_t nstar, uint64_t key, int nexits, double *SF,
+                      int64_t *info);
+
 int orc_disk_structure(int nR, int nTheta, int ng, const double *R, const double *Theta, const double *V,
                        double Mstar, int nzones, const double *zones, const double *shscale,
                        const double *grain_scale, const int *shtype, const double *Temp, double *dens,
@@ -179,6 +188,22 @@ int orc_disk_structure(int nR, int nTheta, int ng, const double *R, const double
  * TraceMono.f:2032-2297 and 8-497): Kabs_c, Ksca_c per component (ncomp*nlam),
  * T per cell; the model's dens is used as given.  info: [0] image radii,
  * [1] rays ended by a geometry failure. */
+/* the scattered-light field settings of the ray tracer (0 packets: none) */
+typedef struct {
+  int64_t nphot, nstar;
+  uint64_t seed;
+  int nexits;
+} orc_scat_opts;
+
+int orc_trace_spectrum_scat(const orc_model *m, const double *Kabs_c, const double *Ksca_c, const double *T,
+                            int scat_how, double angle, int nphi, int nj0, int nRfix, const double *Rfix,
+                            double lam_path, int tracestar, double dimstar, int nobs, const double *lam_obs,
+                            double *flux, int *info, const orc_scat_opts *so);
+int orc_trace_image_scat(const orc_model *m, const double *Kabs_c, const double *Ksca_c, const double *T,
+                         int scat_how, double angle, int nphi, int nj0, int nRfix, const double *Rfix, int tracestar,
+                         double dimstar, double lam0, int npix, int nint, double Rmax, double pa, uint64_t seed,
+                         int linear, double *flux, double *im, int *info, const orc_scat_opts *so);
+
 int orc_trace_spectrum(const orc_model *m, const double *Kabs_c, const double *Ksca_c, const double *T,
                        int scat_how, double angle, int nphi, int nj0, int nRfix, const double *Rfix,
                        double lam_path, int tracestar, double dimstar, int nobs, const double *lam_obs, double *flux,

@@ -903,7 +903,7 @@ void orc_init_random_walk(const orc_model *m, int scat_how, double factRW, uint8
 
 typedef struct {
   int n, cap, hitstar;
-  int *i, *j;
+  int *i, *j, *irg, *jphi1, *jphi2, *k; /* the last four with a scattered-light field */
   double *v;
 } orc_path;
 
@@ -912,13 +912,46 @@ static void path_push(orc_path *p, int i, int j, double v) {
     p->cap = p->cap ? 2 * p->cap : 64;
     p->i = (int *)realloc(p->i, sizeof(int) * p->cap);
     p->j = (int *)realloc(p->j, sizeof(int) * p->cap);
+    p->irg = (int *)realloc(p->irg, sizeof(int) * p->cap);
+    p->jphi1 = (int *)realloc(p->jphi1, sizeof(int) * p->cap);
+    p->jphi2 = (int *)realloc(p->jphi2, sizeof(int) * p->cap);
+    p->k = (int *)realloc(p->k, sizeof(int) * p->cap);
     p->v = (double *)realloc(p->v, sizeof(double) * p->cap);
   }
   p->i[p->n] = i;
   p->j[p->n] = j;
+  p->irg[p->n] = 1;
+  p->jphi1[p->n] = p->jphi2[p->n] = 1;
+  p->k[p->n] = 0;
   p->v[p->n] = v;
   p->n++;
 }
+
+/* the folded azimuth bin of a path point, trace2dpath TraceMono.f:2378-2382 */
+static int path_jphi(double x, double y) {
+  const double rho = sqrt(x * x + y * y); /* a point on the axis takes phi = 0 */
+  double c = rho > 0.0 ? x / rho : 1.0;
+  if (c > 1.0) c = 1.0;
+  if (c < -1.0) c = -1.0;
+  double phi = rho > 0.0 ? (180.0 * acos(c)) / PI_D : 0.0;
+  if (y < 0.0) phi = -phi;
+  int j = (int)(((double)(float)180 * phi) / 360.0);
+  j = j + 1;
+  if (j < 1) j = 1 - j;
+  if (j > 90) j = 181 - j;
+  return j;
+}
+
+/* the scattered-light part of the ray tracer, defined below */
+typedef struct {
+  int *nrg, *off, nsub;
+  double *thetrg, *thet;
+} sub_t;
+static void sub_build(const orc_model *m, int angular, sub_t *g);
+static void sub_free(sub_t *g);
+static int sub_irg(const sub_t *g, int j, double theta);
+static int trace2edge_rg(mc_t *s, const sub_t *g, orc_phot *p, int irg, double *v, int *inext, int *jnext,
+                         int *irgnext);
 
 static void rt_cells(const orc_model *m, const double *Kabs_c, const double *Ksca_c, const double *T, double lam0,
                      double *kext, double *emis) {
@@ -982,28 +1015,50 @@ static void sel_sort(double *x, int n) { /* sort, Subroutines.f:1907-1927 */
 static int trace_run(const orc_model *m, const double *Kabs_c, const double *Ksca_c, const double *T, int scat_how,
                      double angle, int nphi, int nj0, int nRfix, const double *Rfix, double lam_path, int tracestar,
                      double dimstar, int nobs, const double *lam_obs, double *flux, int *info, double **Ri_out,
-                     double **image_out);
+                     double **image_out, const orc_scat_opts *so);
 
 int orc_trace_spectrum(const orc_model *m, const double *Kabs_c, const double *Ksca_c, const double *T,
                        int scat_how, double angle, int nphi, int nj0, int nRfix, const double *Rfix,
                        double lam_path, int tracestar, double dimstar, int nobs, const double *lam_obs, double *flux,
                        int *info) {
   return trace_run(m, Kabs_c, Ksca_c, T, scat_how, angle, nphi, nj0, nRfix, Rfix, lam_path, tracestar, dimstar, nobs,
-                   lam_obs, flux, info, NULL, NULL);
+                   lam_obs, flux, info, NULL, NULL, NULL);
+}
+
+int orc_trace_spectrum_scat(const orc_model *m, const double *Kabs_c, const double *Ksca_c, const double *T,
+                            int scat_how, double angle, int nphi, int nj0, int nRfix, const double *Rfix,
+                            double lam_path, int tracestar, double dimstar, int nobs, const double *lam_obs,
+                            double *flux, int *info, const orc_scat_opts *so) {
+  return trace_run(m, Kabs_c, Ksca_c, T, scat_how, angle, nphi, nj0, nRfix, Rfix, lam_path, tracestar, dimstar, nobs,
+                   lam_obs, flux, info, NULL, NULL, so);
 }
 
 /* TracePath + TraceFlux (TraceMono.f:2032-2297, 8-497); when Ri_out and
  * image_out are given they receive (malloc'ed) the image radii and the last
- * wavelength's intensities, radius-major */
+ * wavelength's intensities, radius-major.  so (may be NULL): the
+ * scattered-light field's settings; with packets and a scattering model
+ * each wavelength gets its field (orc_scatter_field, keys seed, seed+1, ...
+ * in the order the fields are made; isotropic models one per grid
+ * wavelength, made when first needed) and the formal solution adds twice
+ * its source (TraceMono.f:356-395); a full-Mueller model's paths then step
+ * through the sub-cones with Trace2edgeRG. */
 static int trace_run(const orc_model *m, const double *Kabs_c, const double *Ksca_c, const double *T, int scat_how,
                      double angle, int nphi, int nj0, int nRfix, const double *Rfix, double lam_path, int tracestar,
                      double dimstar, int nobs, const double *lam_obs, double *flux, int *info, double **Ri_out,
-                     double **image_out) {
+                     double **image_out, const orc_scat_opts *so) {
   const int nR = m->nr, nTheta = m->nt, nc = nTheta - 1, ncell = nR * nc, nstar = 30;
   mc_t s;
   memset(&s, 0, sizeof s);
   s.m = m;
   s.nc = nc;
+  int smode = 0;
+  if (so && (so->nphot > 0 || so->nstar > 0) && (scat_how == 1 || scat_how == 2)) {
+    for (int q = 0; q < m->ncomp * m->nlam; ++q)
+      if (Ksca_c[q] > 0.0) smode = scat_how;
+  }
+  sub_t g;
+  memset(&g, 0, sizeof g);
+  if (smode) sub_build(m, smode == 2, &g);
   double *kext = (double *)malloc(sizeof(double) * ncell), *emis = (double *)malloc(sizeof(double) * ncell);
   /* tau01R, midplane direction */
   rt_cells(m, Kabs_c, Ksca_c, T, lam_path, kext, emis);
@@ -1121,6 +1176,7 @@ static int trace_run(const orc_model *m, const double *Kabs_c, const double *Ksc
       p.j = 1;
       for (int j = 1; j <= nc; ++j)
         if (ct < m->Theta[j - 1] && ct >= m->Theta[j]) p.j = j;
+      int irg = smode == 2 ? sub_irg(&g, p.j, acos(ct)) : 1;
       p.vx = 0.0;
       p.vy = 0.0;
       p.vz = -1.0;
@@ -1128,16 +1184,25 @@ static int trace_run(const orc_model *m, const double *Kabs_c, const double *Ksc
       orc_path *pa = &paths[(size_t)i * nphi + (k - 1)];
       for (int n = 0;; ++n) {
         double v;
-        int inext, jnext;
-        if (n >= (1 << 20) || trace2edge(&s, &p, &v, &inext, &jnext) != 0) {
+        int inext, jnext, irgn = irg;
+        const int f = smode == 2 ? trace2edge_rg(&s, &g, &p, irg, &v, &inext, &jnext, &irgn)
+                                 : trace2edge(&s, &p, &v, &inext, &jnext);
+        if (n >= (1 << 20) || f != 0) {
           bad++;
           break;
         }
         p.onEdge = 1;
         path_push(pa, p.i, p.j, v);
+        const int q = pa->n - 1;
+        pa->irg[q] = irg;
+        if (smode) pa->jphi1[q] = path_jphi(p.x, p.y);
         p.x = p.x + p.vx * v;
         p.y = p.y + p.vy * v;
         p.z = p.z + p.vz * v;
+        if (smode) {
+          pa->jphi2[q] = path_jphi(p.x, p.y);
+          pa->k[q] = p.z > 0.0 ? 0 : 1;
+        }
         if (inext >= nR) break;
         if (inext < 0) {
           pa->hitstar = 1;
@@ -1145,10 +1210,28 @@ static int trace_run(const orc_model *m, const double *Kabs_c, const double *Ksc
         }
         p.i = inext;
         p.j = jnext;
+        irg = irgn;
       }
     }
   /* TraceFlux per wavelength */
   double *image = (double *)calloc((size_t)nimg * nphi, sizeof(double));
+  size_t flen = smode ? (size_t)nR * g.nsub * 2 * 91 : 0;
+  double *SF = smode ? (double *)malloc(sizeof(double) * flen) : NULL, *alb = (double *)malloc(sizeof(double) * ncell);
+  double **iso = smode == 1 ? (double **)calloc((size_t)m->nlam, sizeof(double *)) : NULL;
+  double *fracirg = NULL;
+  uint64_t nfields = 0;
+  if (smode) {
+    fracirg = (double *)malloc(sizeof(double) * g.nsub);
+    for (int j = 1; j <= nc; ++j) {
+      const int kq = g.nrg[j - 1];
+      const double dth = (g.thet[j] - g.thet[j - 1]) / (double)(float)kq;
+      for (int q = 1; q <= kq; ++q)
+        fracirg[g.off[j - 1] + q - 1] = (cos(g.thet[j - 1] + (double)(float)(q - 1) * dth) -
+                                         cos(g.thet[j - 1] + (double)(float)q * dth)) /
+                                        (m->Theta[j - 1] - m->Theta[j]);
+    }
+  }
+  int64_t finfo[4];
   for (int l = 0; l < nobs; ++l) {
     const double lam0 = lam_obs[l];
     flux[l] = 0.0;
@@ -1169,6 +1252,34 @@ static int trace_run(const orc_model *m, const double *Kabs_c, const double *Ksc
       w2 = 1.0;
     }
     rt_cells(m, Kabs_c, Ksca_c, T, lam0, kext, emis);
+    const double *F1 = NULL, *F2 = NULL;
+    if (smode) {
+      for (int c = 0; c < ncell; ++c) { /* TraceFlux's albedo at lam0 */
+        const double *w = m->comp_w + (size_t)c * m->ncomp;
+        double Ke = 0.0, Ks = 0.0;
+        for (int q = 0; q < m->ncomp; ++q) {
+          const double *a = Kabs_c + (size_t)q * m->nlam, *sk = Ksca_c + (size_t)q * m->nlam;
+          Ke = Ke + (w1 * (a[l1] + sk[l1]) + w2 * (a[l2] + sk[l2])) * w[q];
+          Ks = Ks + (w1 * sk[l1] + w2 * sk[l2]) * w[q];
+        }
+        alb[c] = Ks / Ke;
+      }
+      if (smode == 2) {
+        orc_scatter_field(m, Kabs_c, Ksca_c, T, scat_how, angle, lam0, so->nphot, so->nstar, so->seed + nfields++,
+                          so->nexits, SF, finfo);
+        F1 = F2 = SF;
+      } else {
+        const int ls[2] = {l1, l2};
+        for (int q = 0; q < 2; ++q)
+          if (!iso[ls[q]]) {
+            iso[ls[q]] = (double *)malloc(sizeof(double) * flen);
+            orc_scatter_field(m, Kabs_c, Ksca_c, T, scat_how, angle, m->lam[ls[q]], so->nphot, so->nstar,
+                              so->seed + nfields++, so->nexits, iso[ls[q]], finfo);
+          }
+        F1 = iso[l1];
+        F2 = iso[l2];
+      }
+    }
     for (int i = 0; i < nimg; ++i)
       for (int k = 0; k < nphi; ++k) {
         const orc_path *pa = &paths[(size_t)i * nphi + k];
@@ -1179,12 +1290,34 @@ static int trace_run(const orc_model *m, const double *Kabs_c, const double *Ksc
           if (ip != 0) {
             const int c = ip * nc + (jp - 1);
             const double tau_e = ((pa->v[q] * m->dens[c]) * kext[c]) * AU_CM;
+            double src = emis[c];
+            if (smode) {
+              double xs = 0.0;
+              const int kp = pa->k[q];
+              if (smode == 2) {
+                const int irg = pa->irg[q], sub = g.off[jp - 1] + (irg - 1);
+                const size_t base = (((size_t)ip * g.nsub + sub) * 2 + kp) * 91;
+                const double ww = alb[c] / (m->V[c] * fracirg[sub]);
+                const int jj1 = pa->jphi1[q], jj2 = pa->jphi2[q], djj = jj1 <= jj2 ? 1 : -1;
+                int njj = 0;
+                for (int jj = jj1;; jj += djj) {
+                  xs = xs + ww * F1[base + jj];
+                  ++njj;
+                  if (jj == jj2) break;
+                }
+                xs = xs / (double)(float)njj;
+              } else {
+                const size_t b = ((size_t)c * 2 + kp) * 91;
+                xs = ((w1 * F1[b] + w2 * F2[b]) / m->V[c]) * alb[c];
+              }
+              src = 2.0 * xs + emis[c];
+            }
             if (tau_e < 1e-6) {
-              I = I + (emis[c] * tau_e) * fact;
+              I = I + (src * tau_e) * fact;
               fact = fact * (1.0 - tau_e);
             } else {
               const double ex = dm_exp(-tau_e);
-              I = I + (emis[c] * (1.0 - ex)) * fact;
+              I = I + (src * (1.0 - ex)) * fact;
               fact = fact * ex;
             }
             tau = tau + tau_e;
@@ -1213,8 +1346,20 @@ static int trace_run(const orc_model *m, const double *Kabs_c, const double *Ksc
   for (int q = 0; q < nimg * nphi; ++q) {
     free(paths[q].i);
     free(paths[q].j);
+    free(paths[q].irg);
+    free(paths[q].jphi1);
+    free(paths[q].jphi2);
+    free(paths[q].k);
     free(paths[q].v);
   }
+  free(SF);
+  free(alb);
+  free(fracirg);
+  if (iso) {
+    for (int l = 0; l < m->nlam; ++l) free(iso[l]);
+    free(iso);
+  }
+  if (smode) sub_free(&g);
   free(paths); free(phi); free(ta); free(kext); free(emis);
   if (Ri_out && image_out) {
     *Ri_out = Ri;
@@ -1239,9 +1384,17 @@ int orc_trace_image(const orc_model *m, const double *Kabs_c, const double *Ksca
                     double angle, int nphi, int nj0, int nRfix, const double *Rfix, int tracestar, double dimstar,
                     double lam0, int npix, int nint, double Rmax, double pa, uint64_t seed, int linear, double *flux,
                     double *im, int *info) {
+  return orc_trace_image_scat(m, Kabs_c, Ksca_c, T, scat_how, angle, nphi, nj0, nRfix, Rfix, tracestar, dimstar, lam0,
+                              npix, nint, Rmax, pa, seed, linear, flux, im, info, NULL);
+}
+
+int orc_trace_image_scat(const orc_model *m, const double *Kabs_c, const double *Ksca_c, const double *T,
+                         int scat_how, double angle, int nphi, int nj0, int nRfix, const double *Rfix, int tracestar,
+                         double dimstar, double lam0, int npix, int nint, double Rmax, double pa, uint64_t seed,
+                         int linear, double *flux, double *im, int *info, const orc_scat_opts *so) {
   double *Ri = NULL, *image = NULL;
   trace_run(m, Kabs_c, Ksca_c, T, scat_how, angle, nphi, nj0, nRfix, Rfix, lam0, tracestar, dimstar, 1, &lam0, flux,
-            info, &Ri, &image);
+            info, &Ri, &image, so);
   const int nimg = info[0];
   memset(im, 0, sizeof(double) * (size_t)npix * npix);
   const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
@@ -1299,5 +1452,651 @@ int orc_trace_image(const orc_model *m, const double *Kabs_c, const double *Ksca
     }
   free(Ri);
   free(image);
+  return 0;
+}
+
+/* ------------------------------------------------------------------------
+ * The scattered-light field of the ray tracer: TraceMono (TraceMono.f:583-
+ * 914) for one wavelength and inclination, single-threaded, packet after
+ * packet as the reference's loop runs: the cells' opacities and mixed
+ * Mueller matrices at lam0 (TraceMono.f:664-750), EmissionDistribution
+ * (:956-1121; thermal contact, exit depths over nexits directions with
+ * trace2exit :2659-2697), MakeStarScatter (:1585-1770), then the packets of
+ * emitposition (:1124-1290) through trace2dmono (:1291-1411) with
+ * makescattfield (:1416-1497) and the albedo roulette and scattering
+ * (:852-880).  Theta rows are split into sub-cones for a full-Mueller
+ * field (Telescope.f:93-110; thet taken as acos(Theta)) and traced with
+ * Trace2edgeRG (:2487-2657).
+ *
+ * Random numbers: starlight packet w draws the Philox stream (key, w),
+ * Monte Carlo packet w the stream (key, nstar + w), where the reference
+ * continues ran2.  Albedo**0.25 is taken as two square roots, exp, log, sin
+ * and cos are detmath's, acos is the C library's.  SF: nR*nsub*2*91, laid
+ * out as mcg_scatter_field documents.  info: [0] nsub, [1] geometry
+ * failures, [2] interaction-cap kills, [3] packets with no start. */
+
+#define SF_NPHI_O 180
+#define SF_NB_O 91
+
+static void sub_build(const orc_model *m, int angular, sub_t *g) {
+  const int nt = m->nt, nc = nt - 1;
+  g->thet = (double *)malloc(sizeof(double) * nt);
+  for (int j = 0; j < nt; ++j) g->thet[j] = acos(m->Theta[j]);
+  g->thet[0] = 0.0;
+  g->thet[nt - 1] = PI_D / 2.0;
+  g->nrg = (int *)malloc(sizeof(int) * nc);
+  g->off = (int *)malloc(sizeof(int) * nc);
+  int n = 0;
+  for (int j = 1; j <= nc; ++j) {
+    int k = 1;
+    if (angular) {
+      const int q = (int)((g->thet[j] - g->thet[j - 1]) * 270.0 / PI_D);
+      if (q > 1) k = q;
+    }
+    g->nrg[j - 1] = k;
+    g->off[j - 1] = n;
+    n += k;
+  }
+  g->nsub = n;
+  g->thetrg = (double *)malloc(sizeof(double) * (size_t)(n + nc));
+  for (int j = 1; j <= nc; ++j) {
+    const int k = g->nrg[j - 1];
+    double *tr = g->thetrg + g->off[j - 1] + (j - 1);
+    for (int q = 1; q <= k + 1; ++q) {
+      const double c = cos(g->thet[j - 1] + (double)(float)(q - 1) * ((g->thet[j] - g->thet[j - 1]) / (double)(float)k));
+      tr[q - 1] = c * c;
+    }
+    tr[0] = m->Theta[j - 1] * m->Theta[j - 1];
+    tr[k] = m->Theta[j] * m->Theta[j];
+  }
+}
+
+static void sub_free(sub_t *g) {
+  free(g->nrg); free(g->off); free(g->thetrg); free(g->thet);
+}
+
+static int sub_irg(const sub_t *g, int j, double theta) {
+  const int k = g->nrg[j - 1];
+  if (k <= 1 || !(theta == theta)) return 1;
+  int irg = (int)((double)(float)k * (theta - g->thet[j - 1]) / (g->thet[j] - g->thet[j - 1])) + 1;
+  if (irg > k) irg = k;
+  if (irg < 1) irg = 1;
+  return irg;
+}
+
+/* Trace2edgeRG, TraceMono.f:2487-2657 */
+static int trace2edge_rg(mc_t *s, const sub_t *g, orc_phot *p, int irg, double *v, int *inext, int *jnext,
+                         int *irgnext) {
+  const orc_model *m = s->m;
+  const int nt = m->nt, nrg = g->nrg[p->j - 1];
+  double r = (p->x * p->x + p->y * p->y) + p->z * p->z;
+  double R1 = m->R[p->i] * m->R[p->i], R2 = m->R[p->i + 1] * m->R[p->i + 1], T1, T2;
+  if (nrg <= 1) {
+    T1 = m->Theta[p->j - 1] * m->Theta[p->j - 1];
+    T2 = m->Theta[p->j] * m->Theta[p->j];
+  } else {
+    T1 = g->thetrg[g->off[p->j - 1] + (p->j - 1) + irg - 1];
+    T2 = g->thetrg[g->off[p->j - 1] + (p->j - 1) + irg];
+  }
+  double b = 2.0 * ((p->x * p->vx + p->y * p->vy) + p->z * p->vz);
+  int hitR1, hitR2, hitT1, hitT2;
+  double vR1, vR2, vT1, vT2;
+  if (!p->onEdge) {
+    hitR1 = hitR(R1, r, b, &vR1);
+    hitR2 = hitR(R2, r, b, &vR2);
+    hitT1 = hitT(p, T1, r, b, &vT1);
+    hitT2 = hitT(p, T2, r, b, &vT2);
+  } else if (p->edgeNr == 1) {
+    hitR1 = 0;
+    vR1 = 1e200;
+    hitR2 = hitR(R2, r, b, &vR2);
+    hitT1 = hitT(p, T1, r, b, &vT1);
+    hitT2 = hitT(p, T2, r, b, &vT2);
+  } else if (p->edgeNr == 2) {
+    hitR1 = hitR(R1, r, b, &vR1);
+    hitR2 = 1;
+    vR2 = -b;
+    hitT1 = hitT(p, T1, r, b, &vT1);
+    hitT2 = hitT(p, T2, r, b, &vT2);
+  } else if (p->edgeNr == 3) {
+    hitR1 = hitR(R1, r, b, &vR1);
+    hitR2 = hitR(R2, r, b, &vR2);
+    hitT1 = 0;
+    vT1 = 1e200;
+    if (p->j != nt - 1 || irg != nrg) {
+      hitT2 = hitT(p, T2, r, b, &vT2);
+    } else {
+      vT2 = -p->z / p->vz;
+      hitT2 = vT2 > 0.0;
+    }
+  } else {
+    hitR1 = hitR(R1, r, b, &vR1);
+    hitR2 = hitR(R2, r, b, &vR2);
+    if (p->j != 1 || irg != 1) {
+      hitT1 = hitT(p, T1, r, b, &vT1);
+    } else {
+      hitT1 = 0;
+      vT1 = 1e200;
+    }
+    if (p->j != nt - 1 || irg != nrg) {
+      hitT2 = hitTsame(p, T2, b, &vT2);
+    } else {
+      hitT2 = 0;
+      vT2 = 1e200;
+    }
+  }
+  if (!hitR1 && !hitR2 && !hitT1 && !hitT2) {
+    hitR1 = hitR(R1, r, b, &vR1);
+    hitR2 = hitR(R2, r, b, &vR2);
+    hitT1 = hitT(p, T1, r, b, &vT1);
+    hitT2 = hitT(p, T2, r, b, &vT2);
+    if (!hitR1 && !hitR2 && !hitT1 && !hitT2) return 1;
+  }
+  *v = 1e200;
+  *inext = p->i;
+  *jnext = p->j;
+  *irgnext = irg;
+  if (hitR1 && vR1 < *v) {
+    *v = vR1;
+    *inext = p->i - 1;
+    *jnext = p->j;
+    *irgnext = irg;
+    p->edgeNr = 2;
+  }
+  if (hitR2 && vR2 < *v) {
+    *v = vR2;
+    *inext = p->i + 1;
+    *jnext = p->j;
+    *irgnext = irg;
+    p->edgeNr = 1;
+  }
+  if (hitT1 && vT1 < *v) {
+    *v = vT1;
+    *inext = p->i;
+    if (nrg > 1) {
+      *irgnext = irg - 1;
+      *jnext = p->j;
+      if (*irgnext < 1) {
+        *jnext = p->j - 1;
+        *irgnext = *jnext > 0 ? g->nrg[*jnext - 1] : 1;
+      }
+    } else {
+      *jnext = p->j - 1;
+      if (*jnext > 0) *irgnext = g->nrg[*jnext - 1];
+    }
+    p->edgeNr = 4;
+  }
+  if (hitT2 && vT2 < *v) {
+    *v = vT2;
+    *inext = p->i;
+    if (nrg > 1) {
+      *irgnext = irg + 1;
+      *jnext = p->j;
+      if (*irgnext > nrg) {
+        *jnext = p->j + 1;
+        *irgnext = 1;
+        if (*jnext == nt) *irgnext = g->nrg[nt - 2];
+      }
+    } else {
+      *jnext = p->j + 1;
+      *irgnext = 1;
+    }
+    p->edgeNr = 3;
+  }
+  if (*jnext == nt) {
+    *jnext = nt - 1;
+    *irgnext = g->nrg[nt - 2];
+    p->edgeNr = 4;
+  }
+  if (*jnext == 0) {
+    *jnext = 1;
+    *irgnext = 1;
+    p->edgeNr = 3;
+  }
+  return 0;
+}
+
+typedef struct {
+  mc_t s;
+  sub_t g;
+  int mode, nc;
+  double *kabs, *kext, *alb, *F, *vis, *cum, *dirs, *SF;
+  long ncum;
+  double Etot, Estar;
+  int64_t nstar, nphot;
+  int64_t *info;
+} sf_run;
+
+static size_t sf_base_o(const sf_run *q, int i, int j, int irg, int side) {
+  return (((size_t)i * q->g.nsub + q->g.off[j - 1] + (irg - 1)) * 2 + side) * SF_NB_O;
+}
+
+/* the 180 observer directions' angle indices and rotated Q of a flight */
+static void sf_dirs_o(const sf_run *q, const orc_phot *p, int *ia, double *Qd) {
+  for (int k = 0; k < SF_NPHI_O; ++k) {
+    const double sx = q->dirs[3 * k], sy = q->dirs[3 * k + 1], sz = q->dirs[3 * k + 2];
+    double c = (p->vx * sx + p->vy * sy) + p->vz * sz;
+    if (c > 1.0) c = 1.0;
+    if (c < -1.0) c = -1.0;
+    int a = (int)((180.0 * acos(c)) / PI_D + 1.0);
+    if (a > 180) a = 180;
+    if (a < 1) a = 1;
+    ia[k] = a - 1;
+    Qd[k] = p->Q;
+    if (p->pol) {
+      double xn = p->vy * sz - p->vz * sy, yn = p->vz * sx - p->vx * sz, zn = p->vx * sy - p->vy * sx;
+      const double r = sqrt((xn * xn + yn * yn) + zn * zn);
+      if (r > 0.0) {
+        orc_phot t = *p;
+        rotate_stokes(&t, xn / r, yn / r, zn / r);
+        Qd[k] = t.Q;
+      }
+    }
+  }
+}
+
+/* the folded azimuth deposits of a segment, loop order i = 1..180 */
+static void sf_fold_o(sf_run *q, size_t base, const double *Fc, double x, double y, double E, double vAU,
+                      const int *ia, const double *Qd, int withQ) {
+  const double rho = sqrt(x * x + y * y);
+  double phi0 = rho > 0.0 ? (180.0 * acos(x / rho)) / PI_D : 0.0;
+  if (y < 0.0) phi0 = 360.0 - phi0;
+  const double phi = 180.0 / (double)(float)SF_NPHI_O;
+  int j = (int)(((double)(float)SF_NPHI_O * (phi + phi0)) / 360.0);
+  for (int i = 1; i <= SF_NPHI_O; ++i) {
+    if (j < 1) j = j + SF_NPHI_O;
+    if (j > SF_NPHI_O) j = j - SF_NPHI_O;
+    const int a = ia[j - 1];
+    const double sI = withQ ? Fc[a] * E + Fc[180 + a] * Qd[j - 1] : Fc[a] * E;
+    const int bin = i <= SF_NPHI_O / 2 ? i : SF_NPHI_O + 1 - i;
+    q->SF[base + bin] = q->SF[base + bin] + sI * vAU;
+    j = j + 1;
+  }
+}
+
+static int sf_star_start_o(sf_run *q, rng_t *r, orc_phot *p, int *irg, int byct) {
+  const orc_model *m = q->s.m;
+  const double R0 = m->R[0];
+  randomdirection(r, &p->x, &p->y, &p->z);
+  p->x = R0 * p->x;
+  p->y = R0 * p->y;
+  p->z = R0 * p->z;
+  randomdirection(r, &p->vx, &p->vy, &p->vz);
+  const double inp = (p->x * p->vx + p->y * p->vy) + p->z * p->vz;
+  if (inp < 0.0) {
+    p->vx = -p->vx;
+    p->vy = -p->vy;
+    p->vz = -p->vz;
+  }
+  p->edgeNr = 1;
+  p->onEdge = 1;
+  const double ct = fabs(p->z) / R0;
+  for (int j = 1; j <= q->nc; ++j)
+    if (ct < m->Theta[j - 1] && ct > m->Theta[j]) {
+      p->i = 0;
+      p->j = j;
+      *irg = sub_irg(&q->g, j, acos(byct ? ct : fabs(p->z) / sqrt((p->x * p->x + p->y * p->y) + p->z * p->z)));
+      return 1;
+    }
+  return 0;
+}
+
+static void sf_star_packet(sf_run *q, uint64_t key, int64_t w) {
+  const orc_model *m = q->s.m;
+  const int nc = q->nc;
+  rng_t r;
+  memset(&r, 0, sizeof r);
+  px_init(&r.px, key, (uint64_t)w);
+  orc_phot p;
+  memset(&p, 0, sizeof p);
+  int irg = 1, ia[SF_NPHI_O];
+  double Qd[SF_NPHI_O];
+  p.E = q->Estar / (double)(float)q->nstar;
+  if (!sf_star_start_o(q, &r, &p, &irg, 1)) {
+    const double ct = fabs(p.z) / m->R[0];
+    p.i = 0;
+    p.j = 1;
+    for (int j = 1; j <= nc; ++j)
+      if (ct <= m->Theta[j - 1] && ct >= m->Theta[j]) {
+        p.j = j;
+        break;
+      }
+    irg = sub_irg(&q->g, p.j, acos(ct));
+  }
+  if (q->mode == 2) sf_dirs_o(q, &p, ia, Qd);
+  for (int n = 0;; ++n) {
+    double v;
+    int inext, jnext, irgn;
+    if (n >= (1 << 20) || trace2edge_rg(&q->s, &q->g, &p, irg, &v, &inext, &jnext, &irgn) != 0) {
+      q->info[1]++;
+      return;
+    }
+    const size_t c = (size_t)p.i * nc + (p.j - 1);
+    const double tau = (m->dens[c] * q->kext[c]) * AU_CM;
+    const double w1 = (tau * v > 1e-5) ? (1.0 - dm_exp(-tau * v)) / tau : v;
+    if (q->mode == 1) {
+      const size_t b = sf_base_o(q, p.i, p.j, 1, 0);
+      q->SF[b] = q->SF[b] + ((p.E * w1) * AU_CM) / 2.0;
+      q->SF[b + SF_NB_O] = q->SF[b + SF_NB_O] + ((p.E * w1) * AU_CM) / 2.0;
+    } else {
+      const double x = p.x + (p.vx * v) / 2.0, y = p.y + (p.vy * v) / 2.0;
+      const size_t b = sf_base_o(q, p.i, p.j, irg < 1 ? 1 : irg, p.z > 0.0 ? 0 : 1);
+      q->SF[b] = q->SF[b] + (p.E * w1) * AU_CM;
+      sf_fold_o(q, b, q->F + c * 1082, x, y, p.E, (v * AU_CM) / 2.0, ia, Qd, 0);
+    }
+    p.E = p.E * dm_exp(-tau * v);
+    p.x = p.x + p.vx * v;
+    p.y = p.y + p.vy * v;
+    p.z = p.z + p.vz * v;
+    p.onEdge = 1;
+    if (inext >= m->nr || inext < 0) return;
+    p.i = inext;
+    p.j = jnext;
+    irg = irgn;
+  }
+}
+
+static int sf_emit_o(sf_run *q, rng_t *r, orc_phot *p, int *irg) {
+  const orc_model *m = q->s.m;
+  const int nc = q->nc;
+  for (int tries = 0; tries < 1000; ++tries) {
+    p->pol = 0;
+    double Er = q->Etot * rnd(r);
+    if (Er < q->Estar) {
+      p->E = q->Etot;
+      p->scatt = 0;
+      if (sf_star_start_o(q, r, p, irg, 0)) return 1;
+      continue;
+    }
+    p->scatt = 1;
+    Er = Er - q->Estar;
+    long k = 0; /* the cell scan of TraceMono.f:1253-1256 */
+    while (k < q->ncum && !(Er < q->cum[k])) ++k;
+    if (k >= q->ncum) continue;
+    const int i = 1 + (int)(k / nc), j = 1 + (int)(k % nc);
+    double Rad = rnd(r);
+    Rad = sqrt(m->R[i] * m->R[i] * Rad + m->R[i + 1] * m->R[i + 1] * (1.0 - Rad));
+    double Th = rnd(r);
+    Th = m->Theta[j - 1] * Th + m->Theta[j] * (1.0 - Th);
+    p->z = Rad * Th;
+    if (rnd(r) < 0.5) p->z = -p->z;
+    const double phi = (rnd(r) * PI_D) * 2.0;
+    p->x = (Rad * sqrt(1.0 - Th * Th)) * dm_sin(phi);
+    p->y = (Rad * sqrt(1.0 - Th * Th)) * dm_cos(phi);
+    randomdirection(r, &p->vx, &p->vy, &p->vz);
+    p->i = i;
+    p->j = j;
+    *irg = sub_irg(&q->g, j, acos(fabs(p->z) / sqrt((p->x * p->x + p->y * p->y) + p->z * p->z)));
+    p->onEdge = 0;
+    p->edgeNr = 0;
+    p->E = q->Etot / q->vis[(size_t)i * nc + (j - 1)];
+    return 1;
+  }
+  return 0;
+}
+
+static void sf_mc_packet(sf_run *q, uint64_t key, int64_t w) {
+  const orc_model *m = q->s.m;
+  const int nc = q->nc;
+  rng_t r;
+  memset(&r, 0, sizeof r);
+  px_init(&r.px, key, (uint64_t)(q->nstar + w));
+  orc_phot p;
+  memset(&p, 0, sizeof p);
+  int irg = 1, ia[SF_NPHI_O];
+  double Qd[SF_NPHI_O];
+  if (!sf_emit_o(q, &r, &p, &irg)) {
+    q->info[3]++;
+    return;
+  }
+  p.E = p.E / (double)(float)q->nphot;
+  if (q->mode == 2) {
+    p.pol = 0;
+    p.Q = p.U = p.V = 0.0;
+    double x = 1.0, y = 0.0, z = 0.0;
+    if (p.vz != 1.0) {
+      x = -p.vy;
+      y = p.vx;
+    }
+    const double rr = sqrt((x * x + y * y) + z * z);
+    p.Sx = x / rr;
+    p.Sy = y / rr;
+    p.Sz = z / rr;
+  }
+  const int maxv = (m->nr + m->nt + 360) * 2;
+  for (int nint = 0;; ++nint) {
+    const double tau0 = -dm_log(rnd(&r));
+    if (q->mode == 2 && p.scatt) sf_dirs_o(q, &p, ia, Qd);
+    double tau = 0.0;
+    int escape = 0, interact = 0;
+    for (int nv = 1;; ++nv) {
+      double v;
+      int inext, jnext, irgn;
+      if (nv > maxv) {
+        escape = 1;
+        break;
+      }
+      if (trace2edge_rg(&q->s, &q->g, &p, irg, &v, &inext, &jnext, &irgn) != 0) {
+        q->info[1]++;
+        escape = 1;
+        break;
+      }
+      const size_t c = (size_t)p.i * nc + (p.j - 1);
+      const double tau1 = ((v * m->dens[c]) * q->kext[c]) * AU_CM;
+      if (tau + tau1 > tau0) {
+        v = (v * (tau0 - tau)) / tau1;
+        interact = 1;
+      }
+      if (p.scatt) {
+        if (q->mode == 1) {
+          const size_t b = sf_base_o(q, p.i, p.j, 1, 0);
+          q->SF[b] = q->SF[b] + ((p.E * v) * AU_CM) / 2.0;
+          q->SF[b + SF_NB_O] = q->SF[b + SF_NB_O] + ((p.E * v) * AU_CM) / 2.0;
+        } else {
+          const double x = p.x + (p.vx * v) / 2.0, y = p.y + (p.vy * v) / 2.0;
+          const size_t b = sf_base_o(q, p.i, p.j, irg < 1 ? 1 : irg, p.z > 0.0 ? 0 : 1);
+          q->SF[b] = q->SF[b] + (p.E * v) * AU_CM;
+          sf_fold_o(q, b, q->F + c * 1082, x, y, p.E, (v * AU_CM) / 2.0, ia, Qd, 1);
+        }
+      }
+      p.x = p.x + p.vx * v;
+      p.y = p.y + p.vy * v;
+      p.z = p.z + p.vz * v;
+      if (interact) {
+        p.onEdge = 0;
+        break;
+      }
+      p.onEdge = 1;
+      tau = tau + tau1;
+      if (inext >= m->nr || inext < 0) {
+        escape = 1;
+        break;
+      }
+      p.i = inext;
+      p.j = jnext;
+      irg = irgn;
+    }
+    if (escape) return;
+    const size_t c = (size_t)p.i * nc + (p.j - 1);
+    const double alb = q->alb[c];
+    const double fstop = sqrt(sqrt(alb));
+    if (!(fstop > 0.0)) return;
+    const double fact = alb / fstop;
+    p.E = p.E * fact;
+    p.Q = p.Q * fact;
+    p.U = p.U * fact;
+    p.V = p.V * fact;
+    if (rnd(&r) > fstop) return;
+    if (nint >= 1000000) {
+      q->info[2]++;
+      return;
+    }
+    p.scatt = 1;
+    if (q->mode == 1)
+      randomdirection(&r, &p.vx, &p.vy, &p.vz);
+    else
+      scatangle(&q->s, &r, &p, q->F + c * 1082, q->F + c * 1082 + 1080);
+  }
+}
+
+int orc_scatter_field(const orc_model *m, const double *Kabs_c, const double *Ksca_c, const double *T, int scat_how,
+                      double angle, double lam0, int64_t nphot, int64_t nstar, uint64_t key, int nexits, double *SF,
+                      int64_t *info) {
+  const int nR = m->nr, nt = m->nt, nc = nt - 1, ncell = nR * nc, nlam = m->nlam, TT = ORC_TMAX + 1;
+  sf_run q;
+  memset(&q, 0, sizeof q);
+  q.s.m = m;
+  q.s.nc = nc;
+  q.s.scat_how = scat_how;
+  q.nc = nc;
+  q.mode = scat_how == 2 ? 2 : 1;
+  q.nstar = nstar;
+  q.nphot = nphot;
+  q.info = info;
+  q.SF = SF;
+  for (int k = 0; k < 4; ++k) info[k] = 0;
+  sub_build(m, q.mode == 2, &q.g);
+  info[0] = q.g.nsub;
+  /* the wavelength bracket of TraceMono.f:617-643 */
+  int l1 = 0, l2 = 1;
+  double w1 = 1.0, w2 = 0.0;
+  for (int i = 0; i < nlam - 1; ++i)
+    if (lam0 >= m->lam[i] && lam0 <= m->lam[i + 1]) {
+      l1 = i;
+      l2 = i + 1;
+      w1 = (m->lam[i + 1] - lam0) / (m->lam[i + 1] - m->lam[i]);
+      w2 = (lam0 - m->lam[i]) / (m->lam[i + 1] - m->lam[i]);
+    }
+  if (lam0 >= m->lam[nlam - 1]) {
+    l1 = nlam - 2;
+    l2 = nlam - 1;
+    w1 = 0.0;
+    w2 = 1.0;
+  }
+  q.kabs = (double *)malloc(sizeof(double) * ncell);
+  q.kext = (double *)malloc(sizeof(double) * ncell);
+  q.alb = (double *)malloc(sizeof(double) * ncell);
+  q.vis = (double *)malloc(sizeof(double) * ncell);
+  double *emis = (double *)calloc((size_t)ncell, sizeof(double)), *ksca = (double *)malloc(sizeof(double) * ncell);
+  if (q.mode == 2) q.F = (double *)malloc(sizeof(double) * (size_t)ncell * 1082);
+  for (int c = 0; c < ncell; ++c) {
+    const double *w = m->comp_w + (size_t)c * m->ncomp;
+    double Ka = 0.0, Ke = 0.0, Ks = 0.0;
+    for (int k = 0; k < m->ncomp; ++k) {
+      const double *a = Kabs_c + (size_t)k * nlam, *s = Ksca_c + (size_t)k * nlam;
+      Ka = Ka + (w1 * a[l1] + w2 * a[l2]) * w[k];
+      Ke = Ke + (w1 * (a[l1] + s[l1]) + w2 * (a[l2] + s[l2])) * w[k];
+      Ks = Ks + (w1 * s[l1] + w2 * s[l2]) * w[k];
+    }
+    q.kabs[c] = Ka;
+    q.kext[c] = Ke;
+    ksca[c] = Ks;
+    q.alb[c] = Ks / Ke;
+    if (q.mode == 2)
+      for (int e = 0; e < 1082; ++e) {
+        double f;
+        if (Ks == 0.0) {
+          f = e < 180 ? 1.0 : 0.0;
+        } else {
+          f = 0.0;
+          for (int k = 0; k < m->ncomp; ++k) {
+            const double *ks = Ksca_c + (size_t)k * nlam;
+            double f1, f2;
+            if (e < 1080) {
+              f1 = m->F_comp[((size_t)k * nlam + l1) * 1080 + e];
+              f2 = m->F_comp[((size_t)k * nlam + l2) * 1080 + e];
+            } else {
+              f1 = m->IF_comp[((size_t)k * nlam + l1) * 2 + (e - 1080)];
+              f2 = m->IF_comp[((size_t)k * nlam + l2) * 2 + (e - 1080)];
+            }
+            f = f + ((f1 * ks[l1]) * w1 + (f2 * ks[l2]) * w2) * w[k];
+          }
+          f = f / Ks;
+        }
+        q.F[(size_t)c * 1082 + e] = f;
+      }
+  }
+  /* EmissionDistribution: the thermal weight, the exit depth and the running sum */
+  q.ncum = (long)(nR - 1) * nc;
+  q.cum = (double *)malloc(sizeof(double) * (q.ncum > 0 ? q.ncum : 1));
+  double Et = 0.0;
+  for (int i = 1; i <= nR - 1; ++i)
+    for (int j = 1; j <= nc; ++j) {
+      const int c = i * nc + (j - 1);
+      double e = 0.0;
+      if (T[c] != 0.0) {
+        int iT = (int)(T[c] / 1.0);
+        const double wT1 = (double)(iT + 1) - T[c] / 1.0, wT2 = T[c] / 1.0 - (double)iT;
+        if (iT < 1) iT = 1;
+        if (iT > ORC_TMAX - 1) iT = ORC_TMAX - 1;
+        const double *w = m->comp_w + (size_t)c * m->ncomp;
+        const double *B1 = m->BB + (size_t)l1 * TT, *B2 = m->BB + (size_t)l2 * TT;
+        for (int k = 0; k < m->ncomp; ++k) {
+          const double *a = Kabs_c + (size_t)k * nlam;
+          e = e + ((w1 * (wT1 * B1[iT] + wT2 * B1[iT + 1])) * a[l1] + (w2 * (wT1 * B2[iT] + wT2 * B2[iT + 1])) * a[l2]) *
+                      w[k];
+        }
+      }
+      e = (e * m->dens[c]) * m->V[c];
+      double taumin = 0.0;
+      for (int k = 1; k <= nexits; ++k) {
+        orc_phot p;
+        memset(&p, 0, sizeof p);
+        double Rad = 0.5;
+        Rad = sqrt(m->R[i] * m->R[i] * Rad + m->R[i + 1] * m->R[i + 1] * (1.0 - Rad));
+        double Th = 0.5;
+        Th = m->Theta[j - 1] * Th + m->Theta[j] * (1.0 - Th);
+        p.z = Rad * Th;
+        double phi = 1e-4;
+        p.x = Rad * sqrt(1.0 - Th * Th) * dm_sin(phi);
+        p.y = Rad * sqrt(1.0 - Th * Th) * dm_cos(phi);
+        phi = (PI_D * (double)(float)(k - 1)) / (double)(float)(nexits - 1);
+        p.vy = dm_cos(phi);
+        p.vz = dm_sin(phi);
+        p.i = i;
+        p.j = j;
+        p.onEdge = 0;
+        double tau = 0.0;
+        for (int n = 0; n < 1000000; ++n) {
+          double v;
+          int inext, jnext;
+          if (trace2edge(&q.s, &p, &v, &inext, &jnext) != 0) break;
+          p.onEdge = 1;
+          p.x = p.x + p.vx * v;
+          p.y = p.y + p.vy * v;
+          p.z = p.z + p.vz * v;
+          const int cc = p.i * nc + (p.j - 1);
+          tau = tau + ((v * m->dens[cc]) * AU_CM) * q.kabs[cc];
+          if (inext >= nR || inext <= 0) break;
+          p.i = inext;
+          p.j = jnext;
+        }
+        if (tau < taumin || k == 1) taumin = tau;
+      }
+      q.vis[c] = nexits > 0 ? dm_exp(-taumin) : 1.0;
+      emis[c] = e * q.vis[c];
+      Et = Et + emis[c];
+      q.cum[(size_t)(i - 1) * nc + (j - 1)] = Et;
+    }
+  q.Estar = m->Fstar[l1] * w1 + m->Fstar[l2] * w2;
+  q.Etot = Et + q.Estar;
+  q.dirs = (double *)calloc(3 * SF_NPHI_O, sizeof(double));
+  if (q.mode == 2)
+    for (int i = 1; i <= SF_NPHI_O; ++i) { /* TracePath, TraceMono.f:2058-2075 */
+      const double phi = (PI_D * ((double)(float)i - 0.5)) / ((double)(float)SF_NPHI_O / 2.0);
+      double x = 0.0, y = 0.0, z = 1.0;
+      rotate(&x, &y, &z, 0.0, 1.0, 0.0, angle);
+      rotate(&x, &y, &z, 0.0, 0.0, 1.0, phi);
+      const double r = sqrt((x * x + y * y) + z * z);
+      q.dirs[3 * (i - 1)] = x / r;
+      q.dirs[3 * (i - 1) + 1] = y / r;
+      q.dirs[3 * (i - 1) + 2] = z / r;
+    }
+  memset(SF, 0, sizeof(double) * (size_t)nR * q.g.nsub * 2 * SF_NB_O);
+  for (int64_t w = 0; w < nstar; ++w) sf_star_packet(&q, key, w);
+  if (q.Etot > 0.0)
+    for (int64_t w = 0; w < nphot; ++w) sf_mc_packet(&q, key, w);
+  free(q.kabs); free(q.kext); free(q.alb); free(q.vis); free(emis); free(ksca); free(q.F); free(q.cum); free(q.dirs);
+  sub_free(&q.g);
   return 0;
 }

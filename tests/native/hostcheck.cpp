@@ -446,6 +446,7 @@ struct HostRtBackend {
     std::copy(emis.begin(), emis.end(), em);
     return true;
   }
+  bool field(double) { return true; } /* the host replay has no scattered-light field */
   bool rays(const std::vector<double> &R, const std::vector<double> &phi, double fstar, const RtOptions &o,
             double *image, int *bad) {
     const int nr = (int)R.size(), nphi = (int)phi.size();

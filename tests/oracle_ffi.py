@@ -268,44 +268,111 @@ def disk_structure(st, Temp, dens, dens0, gasdens, w, w0):
     return H._structure_call(load().orc_disk_structure, st, Temp, dens, dens0, gasdens, w, w0)
 
 
-def trace_spectrum(model, T, lam_obs, angle, nphi=45, nj0=2, Rfix=(), lam_path=0.55, tracestar=1, dimstar=1.0,
-                   dens=None):
-    """orc_trace_spectrum; returns (flux, image radii count, bad rays)"""
-    L = load()
-    m = model
+class OrcScatOpts(C.Structure):
+    _fields_ = [("nphot", C.c_int64), ("nstar", C.c_int64), ("seed", C.c_uint64), ("nexits", C.c_int)]
+
+
+def _trace_model(m, T, dens, scatter):
+    """the orc_model of the ray tracer (with the Mueller tables when a
+    scattered-light field is asked for) and the arrays it points into"""
     dens = np.maximum(np.asarray(m.dens, float), 1e-50) if dens is None else np.asarray(dens, float)
     keep = [np.ascontiguousarray(a, float) for a in (m.R, m.Theta, m.SinTheta, dens, m.V, m.lam, m.nu, m.BB, m.Fstar,
                                                      m.comp_w, m.Kabs, m.Ksca, T)]
-    om = OrcModel(m.nr, m.nt, P(keep[0]), P(keep[1]), P(keep[2]), P(keep[3]), P(keep[4]), None, m.nlam, P(keep[5]),
-                  P(keep[6]), None, None, None, 0, P(keep[7]), P(keep[8]), float(m.Lstar), m.ncomp, P(keep[9]), None,
-                  None, None, None, None, None, None, None, None, None, None)
+    if scatter:
+        t = transport_tables(m)
+        more = [np.ascontiguousarray(a, float) for a in (m.F, t["IF"], t["sinthet"], t["cos2phi"], t["sin2phi"])]
+        keep += more
+        om = OrcModel(m.nr, m.nt, P(keep[0]), P(keep[1]), P(keep[2]), P(keep[3]), P(keep[4]), None, m.nlam,
+                      P(keep[5]), P(keep[6]), None, None, None, 0, P(keep[7]), P(keep[8]), float(m.Lstar), m.ncomp,
+                      P(keep[9]), P(keep[11]), P(more[0]), P(more[1]), P(more[2]), P(more[3]), P(more[4]), None, None,
+                      None, None, None)
+        so = OrcScatOpts(int(scatter.get("nphot", 0)), int(scatter.get("nphot_star", 0)),
+                         int(scatter.get("seed", 1)) & (2 ** 64 - 1), int(scatter.get("nexits", 5)))
+    else:
+        om = OrcModel(m.nr, m.nt, P(keep[0]), P(keep[1]), P(keep[2]), P(keep[3]), P(keep[4]), None, m.nlam,
+                      P(keep[5]), P(keep[6]), None, None, None, 0, P(keep[7]), P(keep[8]), float(m.Lstar), m.ncomp,
+                      P(keep[9]), None, None, None, None, None, None, None, None, None, None, None)
+        so = None
+    return om, so, keep
+
+
+def trace_spectrum(model, T, lam_obs, angle, nphi=45, nj0=2, Rfix=(), lam_path=0.55, tracestar=1, dimstar=1.0,
+                   dens=None, scatter=None):
+    """orc_trace_spectrum (orc_trace_spectrum_scat with a scattered-light
+    field: scatter = dict(nphot, nphot_star, seed, nexits)); returns (flux,
+    image radii count, bad rays)"""
+    L = load()
+    m = model
+    om, so, keep = _trace_model(m, T, dens, scatter)
     lam_obs = np.ascontiguousarray(lam_obs, float)
     Rfix = np.ascontiguousarray(Rfix, float)
     flux = np.zeros(lam_obs.size)
     info = np.zeros(2, np.int32)
-    L.orc_trace_spectrum(C.byref(om), P(keep[10]), P(keep[11]), P(keep[12]), int(m.scat_how), C.c_double(angle),
-                         int(nphi), int(nj0), int(Rfix.size), P(Rfix) if Rfix.size else None, C.c_double(lam_path),
-                         int(tracestar), C.c_double(dimstar), int(lam_obs.size), P(lam_obs), P(flux), P(info))
+    args = [C.byref(om), P(keep[10]), P(keep[11]), P(keep[12]), int(m.scat_how), C.c_double(angle),
+            int(nphi), int(nj0), int(Rfix.size), P(Rfix) if Rfix.size else None, C.c_double(lam_path),
+            int(tracestar), C.c_double(dimstar), int(lam_obs.size), P(lam_obs), P(flux), P(info)]
+    if so is None:
+        L.orc_trace_spectrum(*args)
+    else:
+        L.orc_trace_spectrum_scat(*args, C.byref(so))
     return flux, int(info[0]), int(info[1])
 
 
 def trace_image(model, T, lam0, angle, npix, nint, Rmax, pa=0.0, seed=42, linear=0, nphi=45, nj0=2, Rfix=(),
-                tracestar=1, dimstar=1.0, dens=None):
-    """orc_trace_image; returns (image (npix, npix), flux, image radii, bad rays)"""
+                tracestar=1, dimstar=1.0, dens=None, scatter=None):
+    """orc_trace_image (orc_trace_image_scat with a scattered-light field);
+    returns (image (npix, npix), flux, image radii, bad rays)"""
     L = load()
     m = model
-    dens = np.maximum(np.asarray(m.dens, float), 1e-50) if dens is None else np.asarray(dens, float)
-    keep = [np.ascontiguousarray(a, float) for a in (m.R, m.Theta, m.SinTheta, dens, m.V, m.lam, m.nu, m.BB, m.Fstar,
-                                                     m.comp_w, m.Kabs, m.Ksca, T)]
-    om = OrcModel(m.nr, m.nt, P(keep[0]), P(keep[1]), P(keep[2]), P(keep[3]), P(keep[4]), None, m.nlam, P(keep[5]),
-                  P(keep[6]), None, None, None, 0, P(keep[7]), P(keep[8]), float(m.Lstar), m.ncomp, P(keep[9]), None,
-                  None, None, None, None, None, None, None, None, None, None)
+    om, so, keep = _trace_model(m, T, dens, scatter)
     Rfix = np.ascontiguousarray(Rfix, float)
     flux = np.zeros(1)
     im = np.zeros(npix * npix)
     info = np.zeros(2, np.int32)
-    L.orc_trace_image(C.byref(om), P(keep[10]), P(keep[11]), P(keep[12]), int(m.scat_how), C.c_double(angle),
-                      int(nphi), int(nj0), int(Rfix.size), P(Rfix) if Rfix.size else None, int(tracestar),
-                      C.c_double(dimstar), C.c_double(lam0), int(npix), int(nint), C.c_double(Rmax), C.c_double(pa),
-                      C.c_uint64(seed), int(linear), P(flux), P(im), P(info))
+    args = [C.byref(om), P(keep[10]), P(keep[11]), P(keep[12]), int(m.scat_how), C.c_double(angle),
+            int(nphi), int(nj0), int(Rfix.size), P(Rfix) if Rfix.size else None, int(tracestar),
+            C.c_double(dimstar), C.c_double(lam0), int(npix), int(nint), C.c_double(Rmax), C.c_double(pa),
+            C.c_uint64(seed), int(linear), P(flux), P(im), P(info)]
+    if so is None:
+        L.orc_trace_image(*args)
+    else:
+        L.orc_trace_image_scat(*args, C.byref(so))
     return im.reshape(npix, npix), float(flux[0]), int(info[0]), int(info[1])
+
+
+def scatter_field(model, T, lam0, angle, nphot=1000, nphot_star=1000, seed=1, nexits=5, tables=None):
+    """orc_scatter_field: the ray tracer's scattered-light field at lam0
+    [micron] for inclination angle [rad]; returns (field (nr, nsub, 2, 91),
+    info [nsub, geometry failures, interaction-cap kills, no start])"""
+    L = load()
+    m = model
+    t = tables or transport_tables(model)
+    keep = {}
+
+    def A(name, a, dt=np.float64):
+        keep[name] = np.ascontiguousarray(a, dt)
+        return P(keep[name])
+
+    om = OrcModel(m.nr, m.nt, A("R", m.R), A("Theta", m.Theta), A("SinTheta", m.SinTheta),
+                  A("dens", np.maximum(np.asarray(m.dens, float), 1e-50)), A("V", m.V), None, m.nlam,
+                  A("lam", m.lam), A("nu", m.nu), A("KabsTot", t["KabsTot"]), A("KscaTot", t["KscaTot"]),
+                  A("KpCell", t["KpCell"]), int(t["kp_uniform"]), A("BB", m.BB), A("Fstar", m.Fstar), float(m.Lstar),
+                  m.ncomp, A("comp_w", m.comp_w), A("Ksca", m.Ksca), A("F", m.F), A("IF", t["IF"]),
+                  A("sinthet", t["sinthet"]), A("cos2phi", t["cos2phi"]), A("sin2phi", t["sin2phi"]), None, None,
+                  A("g", t["g"]), A("rw_y", t["rw_y"]), A("rw_phi", t["rw_phi"]))
+    nc = m.nt - 1
+    th = np.arccos(np.asarray(m.Theta, float))
+    th[0], th[-1] = 0.0, np.pi / 2
+    if int(m.scat_how) == 2:
+        nrg = [max(1, int((th[j] - th[j - 1]) * 270.0 / np.pi)) for j in range(1, nc + 1)]
+    else:
+        nrg = [1] * nc
+    nsub = int(sum(nrg))
+    SF = np.zeros(m.nr * nsub * 2 * 91)
+    info = np.zeros(4, np.int64)
+    st = L.orc_scatter_field(C.byref(om), A("Kabs_c", m.Kabs), A("Ksca_c", m.Ksca), A("T", T), int(m.scat_how),
+                             C.c_double(angle), C.c_double(lam0), C.c_int64(int(nphot)), C.c_int64(int(nphot_star)),
+                             C.c_uint64(int(seed) & (2 ** 64 - 1)), int(nexits), P(SF),
+                             info.ctypes.data_as(C.POINTER(C.c_int64)))
+    assert st == 0 and int(info[0]) == nsub
+    return SF.reshape(m.nr, nsub, 2, 91), info
