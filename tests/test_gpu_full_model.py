@@ -24,7 +24,7 @@ def test_full_model_pipeline_small(tmp_path):
     ag, fl = res["agreement"], res["noise_floor"]
     print("agreement", ag)
     print("floor", fl)
-    assert ag["cells_nabs_ge_1e3"] > 50
+    assert ag["cells_nabs_ge_1e3"] > 20
     # the FP64 + DHS pipeline differs from the mixed one by little more
     # than a second seed of the mixed one does
     assert ag["T_median_rel"] < 2.0 * fl["T_median_rel"] + 0.01
