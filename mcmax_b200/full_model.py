@@ -4,7 +4,8 @@ images, on one GPU.
 
     python -m mcmax_b200.full_model [--nphot 1e9] [--passes 5] [--nrad 300] [--ntheta 200] [--nlam 300]
                                     [--alpha 1e-4] [--angles 20,45,80] [--npix 512] [--nint 1000]
-                                    [--image-lam 10,100] [--check] [--floor] [--out DIR]
+                                    [--image-lam 1,10,100] [--scatter-nphot 1000] [--scatter-nstar 1000]
+                                    [--check] [--floor] [--out DIR]
 
 Deck: the learned-opacities disk (three compositions of 50 log size bins
 from 0.01 to 1000 micron each, MRN within a composition, porosity and
@@ -25,8 +26,10 @@ temperatures and Diffuse.  Then for every inclination the ray-traced
 spectrum (the 'SPECTRUM' observation: 45 angles, 2 points per radial
 cell, at the model's wavelengths) and an --npix square image at each
 --image-lam (the 'IMAGE' observation, field of view the grid's diameter).
-The ray tracer has no scattered-light source, so images are taken in the
-thermal infrared.
+Both carry the scattered light of TraceMono's field: per wavelength
+--scatter-nstar packets of single-scattered starlight and --scatter-nphot
+Monte Carlo packets, five exit rays per cell (an observation's defaults,
+Telescope.f:606-619).
 
 --check runs the same pipeline again in the FP64 form with the DHS
 opacities (the FP64 GPU oracle of the mixed form) and reports the
@@ -63,6 +66,10 @@ def _surrogate_params():
     from . import surrogate as SU
     params, _ = SU.load(os.path.join(os.path.dirname(__file__), "data", "surrogate_nf20.npz"))
     return params
+
+
+def _scatter(a, seed):
+    return dict(nphot=a.scatter_nphot, nphot_star=a.scatter_nstar, seed=seed, nexits=5)
 
 
 def pipeline(ctx, a, precision, opacity, seed, log=None):
@@ -111,12 +118,13 @@ def pipeline(ctx, a, precision, opacity, seed, log=None):
     spectra, images = {}, {}
     t2 = time.perf_counter()
     for ang in a.angle_list:
-        spectra[ang], _ = ctx.trace_spectrum(T, m.lam, math.radians(ang), nphi=45, nr=2)
+        spectra[ang], _ = ctx.trace_spectrum(T, m.lam, math.radians(ang), nphi=45, nr=2, scatter=_scatter(a, seed))
     t["spectra_s"] = time.perf_counter() - t2
     t3 = time.perf_counter()
     for ang in a.angle_list:
         for lam in a.lam_list:
-            images[(ang, lam)] = ctx.trace_image(T, lam, math.radians(ang), npixel=a.npix, nint=a.nint)["image"]
+            images[(ang, lam)] = ctx.trace_image(T, lam, math.radians(ang), npixel=a.npix, nint=a.nint,
+                                                 scatter=_scatter(a, seed))["image"]
     t["images_s"] = time.perf_counter() - t3
     t["total_s"] = time.perf_counter() - t0
     return dict(model=m, T=T, Nabs=np.asarray(out["result"]["Nabs"]), history=out["history"], passes=passes,
@@ -186,7 +194,9 @@ def parse_args(argv=None):
     ap.add_argument("--angles", default="20,45,80")
     ap.add_argument("--npix", type=int, default=512)
     ap.add_argument("--nint", type=int, default=1000)
-    ap.add_argument("--image-lam", default="10,100", help="image wavelengths, micron")
+    ap.add_argument("--image-lam", default="1,10,100", help="image wavelengths, micron")
+    ap.add_argument("--scatter-nphot", type=int, default=1000, help="scattered-light Monte Carlo packets per field")
+    ap.add_argument("--scatter-nstar", type=int, default=1000, help="single-scattered starlight packets per field")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--check", action="store_true", help="also the FP64 + DHS pipeline, and the agreement")
     ap.add_argument("--floor", action="store_true", help="also the mixed pipeline with another seed (noise floor)")
@@ -209,7 +219,8 @@ def main(argv=None):
            "config": {"nrad": a.nrad, "ntheta": a.ntheta, "nlam": a.nlam, "ngrains": 150, "mdust": a.mdust,
                       "alpha": a.alpha, "packets_per_run": a.nphot, "structure_passes": a.passes,
                       "packet_runs": a.passes + 1, "angles_deg": a.angle_list, "image_lam_um": a.lam_list,
-                      "npix": a.npix, "nint": a.nint}}
+                      "npix": a.npix, "nint": a.nint, "scatter_nphot": a.scatter_nphot,
+                      "scatter_nstar": a.scatter_nstar}}
     mixed = pipeline(ctx, a, "mixed", "surrogate", a.seed, log)
     res["mixed_surrogate"] = _summary(mixed)
     if a.out:

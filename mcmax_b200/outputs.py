@@ -249,17 +249,19 @@ def read_observations(path, lam, incangle=45.0, rout=None):
     dicts with kind, inc [deg], lam1, lam2, nlam, lamfile, nphi, nrad, flag,
     npix, nint, fov (list, AU or arcsec), scaletype, the VISIBILITY
     baselines b [m] and theta [deg] (default one of 100 m at 0), d (the
-    telescope diameter, m) (and the other keywords
-    as given, lower-case).  Defaults: inc from the deck's incangle, lam1/lam2
-    the model's range, nphi 45, nrad 2, npix 500, nint 1000, fov twice the
-    grid's outer radius `rout`, scaletype 1.  An IMAGE observation's lam1 is
+    telescope diameter, m), the scattered-light packets nphot and nphotstar
+    and the exit rays nexits (and the other keywords as given, lower-case).
+    Defaults: inc from the deck's incangle, lam1/lam2 the model's range,
+    nphi 45, nrad 2, npix 500, nint 1000, fov twice the grid's outer radius
+    `rout`, scaletype 1, nphot 1000, nphotstar 1000, nexits 5
+    (Telescope.f:602-619).  An IMAGE observation's lam1 is
     the default-level `lam`, else the middle of the wavelength range
     (Telescope.f:591,710-712); a `lam` among an observation's own keywords
     sets its lam1."""
     lam = np.asarray(lam, float)
     default = dict(inc=float(incangle), lam1=float(lam[0]), lam2=float(lam[-1]), nlam=-1, lamfile="", nphi=45,
                    nrad=2, flag="", npix=500, nint=1000, fov=[] if rout is None else [2.0 * float(rout)],
-                   scaletype=1, b=[100.0], theta=[0.0], d=-1.0)
+                   scaletype=1, b=[100.0], theta=[0.0], d=-1.0, nphot=1000, nphotstar=1000, nexits=5)
     deflam = (float(lam[0]) + float(lam[-1])) / 2.0
     obs, cur = [], default
     base = os.path.dirname(os.path.abspath(path))
@@ -281,7 +283,7 @@ def read_observations(path, lam, incangle=45.0, rout=None):
                     cur["lam1"] = deflam
                 obs.append(cur)
                 continue
-            if key in ("nphi", "nrad", "nlam", "npix", "nint", "scaletype"):
+            if key in ("nphi", "nrad", "nlam", "npix", "nint", "scaletype", "nphot", "nphotstar", "nexits"):
                 cur[key] = int(num(val))
             elif cur is not default and cur["kind"] == "BASEVIS" and key[:3] == "lam" and key[3:].isdigit():
                 # lamN: the wavelengths of a BASEVIS observation (Telescope.f:1129-1133)

@@ -45,6 +45,14 @@ def fixed_radii(zones, rin, rout):
     return sorted(out)
 
 
+def scatter_opts(ob, seed):
+    """the scattered-light settings of an observation (Telescope.f:606-619,
+    943-973): its nphot Monte Carlo and nphotstar starlight packets per
+    field and nexits exit rays, the field keys from the run's seed"""
+    return dict(nphot=int(ob.get("nphot", 1000)), nphot_star=int(ob.get("nphotstar", 1000)), seed=int(seed),
+                nexits=int(ob.get("nexits", 5)))
+
+
 def observe_image(ctx, m, T, ob, outdir, rfix=(), seed=42, posangle=0.0):
     """An IMAGE observation (Telescope.f:162-182) without convolution,
     noise or opening: the rays traced at the observation's wavelength
@@ -66,7 +74,8 @@ def observe_image(ctx, m, T, ob, outdir, rfix=(), seed=42, posangle=0.0):
         else:
             rscale, zscale = 1.0, 1.0
         r = ctx.trace_image(T, lam0, angle, npixel=ob["npix"], nint=ob["nint"], Rmax=fov / 2.0, pa=posangle,
-                            nphi=ob["nphi"], nr=ob["nrad"], Rfix=rfix, seed=seed + n)
+                            nphi=ob["nphi"], nr=ob["nrad"], Rfix=rfix, seed=seed + n,
+                            scatter=scatter_opts(ob, seed + n))
         if n == 0:
             files.append(outputs.write_rimage(os.path.join(outdir, outputs.rimage_name(angle, lam0, ob["flag"])),
                                               r["R"], r["rphi"], rscale, zscale, dcm, fov, ob["npix"],
@@ -101,7 +110,8 @@ def observe_ifu(ctx, m, T, ob, outdir, rfix=(), seed=42, posangle=0.0):
             else:
                 rscale, zscale = 1.0, 1.0
             r = ctx.trace_image(T, lam0, angle, npixel=ob["npix"], nint=ob["nint"], Rmax=fov / 2.0, pa=posangle,
-                                nphi=ob["nphi"], nr=ob["nrad"], Rfix=rfix, seed=seed + n, lam_path=0.55)
+                                nphi=ob["nphi"], nr=ob["nrad"], Rfix=rfix, seed=seed + n, lam_path=0.55,
+                                scatter=scatter_opts(ob, seed + n))
             n += 1
             im = r["image"] * 1e23 * zscale / dcm ** 2
             files.append(outputs.write_image_fits(
@@ -124,7 +134,7 @@ def observe_visibility(ctx, m, T, ob, outdir, rfix=(), seed=42, posangle=0.0, vi
     spec, V, ph = [], [], []
     for n, lam0 in enumerate(lam_obs):
         r = ctx.trace_image(T, lam0, angle, npixel=1, nint=1, nphi=ob["nphi"], nr=ob["nrad"], Rfix=rfix,
-                            seed=seed + n, lam_path=0.55)
+                            seed=seed + n, lam_path=0.55, scatter=scatter_opts(ob, seed + n))
         spec.append(1e23 * r["flux"] / dcm ** 2)
         vp = [outputs.visibility(r["R"], r["rphi"], bk, math.pi * tk / 180.0, lam0, dcm, ob["d"], posangle,
                                  vis_norm_fov) for bk, tk in zip(b, th)]
@@ -151,7 +161,7 @@ def observe_basevis(ctx, m, T, ob, outdir, rfix=(), seed=42, posangle=0.0, vis_n
     for j, lam0 in enumerate(lams):
         if j == 0 or lam0 != lams[j - 1]:
             r = ctx.trace_image(T, lam0, angle, npixel=1, nint=1, nphi=ob["nphi"], nr=ob["nrad"], Rfix=rfix,
-                                seed=seed + j, lam_path=ob["lam1"])
+                                seed=seed + j, lam_path=ob["lam1"], scatter=scatter_opts(ob, seed + j))
         vp = [outputs.visibility(r["R"], r["rphi"], bk, math.pi * th[j] / 180.0, lam0, dcm, ob["d"], posangle,
                                  vis_norm_fov) for bk in base]
         V.append([x[0] for x in vp])
@@ -216,7 +226,8 @@ def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opac
     rfix = fixed_radii(run["zones"], m.R[1], m.R[-1])
     for ob in todo:
         lam_obs = outputs.spectrum_wavelengths(m.lam, ob["lam1"], ob["lam2"], ob["nlam"], ob["lamfile"] or None)
-        flux, _ = ctx.trace_spectrum(T, lam_obs, math.radians(ob["inc"]), nphi=ob["nphi"], nr=ob["nrad"], Rfix=rfix)
+        flux, _ = ctx.trace_spectrum(T, lam_obs, math.radians(ob["inc"]), nphi=ob["nphi"], nr=ob["nrad"], Rfix=rfix,
+                                     scatter=scatter_opts(ob, run["seed"]))
         files.append(outputs.write_spectrum(outdir, ob["inc"], lam_obs, flux, m.lam, m.Fstar, m.distance,
                                             flag=ob["flag"], polarised=int(m.scat_how) == 2))
     for ob in images:

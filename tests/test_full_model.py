@@ -9,7 +9,8 @@ from mcmax_b200.model import Model
 def test_defaults_are_the_full_model():
     a = F.parse_args([])
     assert (a.nrad, a.ntheta, a.nlam, a.nphot, a.passes, a.alpha, a.npix) == (300, 200, 300, 10 ** 9, 5, 1e-4, 512)
-    assert a.angle_list == [20.0, 45.0, 80.0] and a.lam_list == [10.0, 100.0]
+    assert a.angle_list == [20.0, 45.0, 80.0] and a.lam_list == [1.0, 10.0, 100.0]
+    assert (a.scatter_nphot, a.scatter_nstar) == (1000, 1000)
 
 
 def test_agreement_statistics():

@@ -68,8 +68,9 @@ class FakeContext:
         T = np.linspace(20.0, 900.0, self.model.ncell)
         return T, 0 * T, 0 * T
 
-    def trace_spectrum(self, T, lam_obs, angle, nphi=45, nr=2, Rfix=()):
+    def trace_spectrum(self, T, lam_obs, angle, nphi=45, nr=2, Rfix=(), scatter=None):
         self.trace_args = (angle, nphi, nr, tuple(Rfix))
+        self.scatter_args = scatter
         return np.full(len(lam_obs), 1e20), (100, 0)
 
     def disk_structure(self, R, Theta, V, Mstar, zones, Temp, dens, dens0, gasdens, w, w0, shscale=None,
@@ -79,9 +80,9 @@ class FakeContext:
         return (np.array(dens), np.array(dens0), np.array(gasdens), np.array(w), np.array(w0))
 
     def trace_image(self, T, lam0, angle, npixel=500, nint=1000, Rmax=None, pa=0.0, nphi=45, nr=2, Rfix=(),
-                    seed=42, lam_path=None):
+                    seed=42, lam_path=None, scatter=None):
         self.image_args = dict(lam0=lam0, angle=angle, npixel=npixel, nint=nint, Rmax=Rmax, pa=pa, nphi=nphi, nr=nr,
-                               seed=seed, lam_path=lam_path)
+                               seed=seed, lam_path=lam_path, scatter=scatter)
         self.image_calls = getattr(self, "image_calls", []) + [self.image_args]
         R = np.linspace(0.0, 50.0, 11)
         return dict(image=np.full((npixel, npixel), 2.0), flux=1.0, R=R, rphi=np.ones((R.size, nphi)),
@@ -134,8 +135,9 @@ def test_command_line_runs_the_deck_and_writes_result_files(tmp_path):
 
 def test_observation_files_drive_spectra(tmp_path):
     deck = _write_inputs(tmp_path)
-    (tmp_path / "Spectrum.out").write_text("nphi=30\nnrad=1\n*****\ntype='SPECTRUM'\ninc=60\nflag='_a'\n"
-                                           "type='IMAGE'\nlam=0.6\nnpix=16\nnint=3\n"
+    (tmp_path / "Spectrum.out").write_text("nphi=30\nnrad=1\nnphot=300\n*****\ntype='SPECTRUM'\ninc=60\n"
+                                           "flag='_a'\n"
+                                           "type='IMAGE'\nlam=0.6\nnpix=16\nnint=3\nnphotstar=70\nnexits=0\n"
                                            "type='SPECTRUM'\nlam1=1\nlam2=100\nnlam=5\n"
                                            "type='LINE'\n")
     made = []
@@ -161,6 +163,9 @@ def test_observation_files_drive_spectra(tmp_path):
     rows = np.loadtxt(str(tmp_path / "o" / "spectrum45.0.dat"))
     assert rows.shape[0] == 5 and np.allclose(rows[[0, -1], 0], [1.0, 100.0])
     assert made[0].trace_args[1:3] == (30, 1)
+    # the observations' scattered-light packets (Telescope.f:943-973)
+    assert made[0].scatter_args == dict(nphot=300, nphot_star=1000, seed=11, nexits=5)
+    assert a["scatter"] == dict(nphot=300, nphot_star=70, seed=11, nexits=0)
 
 
 def test_command_line_arguments():
