@@ -220,7 +220,8 @@ def post_mc_steps(ctx, model, res):
     with a device synchronisation): the temperatures (mcg_finalize_t),
     Diffuse (mcg_diffuse), one vertical-structure pass on the zone taken as
     not fixed (mcg_disk_structure), the ray-traced spectrum at 45 degrees on
-    the grid's wavelengths (mcg_trace_spectrum) and a 500 x 500 image with
+    the grid's wavelengths (mcg_trace_spectrum), without and with scattered
+    light, and a 500 x 500 image with
     1000 points per image cell at the middle of the wavelength range
     (mcg_trace_image).  Not part of the headline metric."""
     import numpy as np
@@ -247,6 +248,14 @@ def post_mc_steps(ctx, model, res):
     (flux, info), t = timed(lambda: ctx.trace_spectrum(Td, lam_obs, math.radians(45.0)))
     out["trace_spectrum"] = {"s": t, "wavelengths": int(lam_obs.size), "image_radii": info[0],
                              "rays_per_s": info[0] * 45 * lam_obs.size / t, "bad_rays": info[1]}
+    # the same spectrum with scattered light at an observation's defaults:
+    # per wavelength one TraceMono field of 1000 starlight and 1000 Monte
+    # Carlo packets, five exit rays per cell
+    sc = dict(nphot=1000, nphot_star=1000, seed=7, nexits=5)
+    (fsc, info), t = timed(lambda: ctx.trace_spectrum(Td, lam_obs, math.radians(45.0), scatter=sc))
+    ok = flux > 0
+    out["trace_spectrum_scattered"] = {"s": t, "fields": int(lam_obs.size), "packets_per_field": 2000,
+                                       "median_scattered_share": float(np.median(1.0 - flux[ok] / fsc[ok]))}
     lam0 = (model.lam[0] + model.lam[-1]) / 2.0
     img, t = timed(lambda: ctx.trace_image(Td, lam0, math.radians(45.0), npixel=500, nint=1000))
     pts = (img["info"][0] - 1) * 45 * 1000

@@ -461,16 +461,16 @@ mcg_status mcg_trace_image(mcg_ctx *ctx, const mcg_trace_opts *opts, const doubl
  * Opacity-surrogate network.  No counterpart in the reference: it stands in
  * for ComputePart's coated-sphere inner loop (ComputePart.f:318-447) inside
  * a training box (see mcg_compute_part_surrogate).  6 normalised inputs ->
- * 4 x 256 SiLU -> 32 outputs; the 256-wide layers run as BF16 tcgen05 MMAs
+ * 4 x 256 SiLU -> 64 outputs; the 256-wide layers run as BF16 tcgen05 MMAs
  * with FP32 accumulation, forward and backward.
  *
  * Parameters are one flat FP32 vector of MCG_MLP_NPARAMS values:
  *   W0[256][6], b0[256], W1..W3[3][256][256] (out, in), b1..b3[3][256],
- *   W4[32][256], b4[32].
+ *   W4[64][256], b4[64].
  * -------------------------------------------------------------------- */
 #define MCG_MLP_NIN 6
-#define MCG_MLP_NOUT 32
-#define MCG_MLP_NPARAMS 207392
+#define MCG_MLP_NOUT 64
+#define MCG_MLP_NPARAMS 215616
 #define MCG_MLP_MAX_EPOCH_LOG 256
 
 typedef struct {
@@ -490,14 +490,14 @@ typedef struct {
 /* Load / read the parameters; loading also resets the optimizer state. */
 mcg_status mcg_mlp_set_params(mcg_ctx *ctx, const float *params, int64_t nparams);
 mcg_status mcg_mlp_get_params(mcg_ctx *ctx, float *params, int64_t nparams);
-/* y[n][32] = network(x[n][6]), host arrays. */
+/* y[n][64] = network(x[n][6]), host arrays. */
 mcg_status mcg_mlp_forward(mcg_ctx *ctx, int64_t n, const float *x, float *y);
 /* Loss sum_o w[o] (y - t)^2 averaged over the n rows, and its gradient with
  * respect to every parameter (flat layout above), for one batch. */
 mcg_status mcg_mlp_gradient(mcg_ctx *ctx, int64_t n, const float *x, const float *t, const float *w,
                             float *grad, double *loss);
-/* Adam training on a data set of n rows (x[n][6], targets t[n][32], output
- * weights w[32]), starting from the loaded parameters. */
+/* Adam training on a data set of n rows (x[n][6], targets t[n][64], output
+ * weights w[64]), starting from the loaded parameters. */
 mcg_status mcg_mlp_train(mcg_ctx *ctx, int64_t n, const float *x, const float *t, const float *w,
                          const mcg_mlp_train_opts *opts, mcg_mlp_train_report *report);
 /* Device time of one forward pass over n device-resident rows and of one
@@ -518,13 +518,14 @@ mcg_status mcg_mlp_gemm_check(mcg_ctx *ctx, int N, const uint16_t *A, const uint
  *   log10 k in [-3.5, log10 2], porosity in [0, 0.6], fmax in [0, 0.8].
  * Outputs (per single grain size, physical units, see mcg_surrogate_targets):
  *   [0] log10 kappa_abs, [1] log10 kappa_sca, [2..13] moments chi_1..chi_12
- *   of F11, [14..26] moments beta_0..beta_12 of F12, [27..31] unused.
+ *   of F11, [14..26] moments beta_0..beta_12 of F12, [27..39] gamma_0..
+ *   gamma_12 of F33, [40..52] delta_0..delta_12 of F34, [53..63] unused.
  * -------------------------------------------------------------------- */
 
 /* Training targets: one ComputePart evaluation (same kernels and loop order
  * as mcg_compute_part) per sample in6[n][6] = (a [micron], lambda [micron],
  * n, k, porosity, fmax) for a single grain size, material density rho and
- * nf DHS filling fractions; out[n][32] as above. */
+ * nf DHS filling fractions; out[n][64] as above. */
 mcg_status mcg_surrogate_targets(mcg_ctx *ctx, int64_t n, const double *in6, double rho, int nf, float *out);
 
 /* ComputePart for nparts grain bins with the loaded network in place of the
@@ -535,7 +536,8 @@ mcg_status mcg_surrogate_targets(mcg_ctx *ctx, int64_t n, const double *in6, dou
  * bin p.  Opacities are mass-weighted over the bin's sizes and scaled by
  * rho_train / rho (kappa ~ 1 / material density); the Mueller matrix is
  * rebuilt on the 180 bins from the scattering-weighted moments (F22 = F11,
- * F33 = F44 = sqrt(F11^2 - F12^2), F34 = 0) and normalised as ComputePart
+ * F44 = F33 as for spheres; F33 and F34 scaled back where a prediction
+ * breaks F12^2 + F33^2 + F34^2 <= F11^2) and normalised as ComputePart
  * normalises F11 (ComputePart.f:407-415). */
 mcg_status mcg_compute_part_surrogate(mcg_ctx *ctx, int nparts, const mcg_part_in *in, mcg_part_out *out,
                                       double rho_train, int nf_train, int *used);

@@ -103,7 +103,7 @@ class Result(C.Structure):
     ]
 
 
-MLP_NIN, MLP_NOUT, MLP_NPARAMS, MLP_MAX_EPOCH_LOG = 6, 32, 207392, 256
+MLP_NIN, MLP_NOUT, MLP_NPARAMS, MLP_MAX_EPOCH_LOG = 6, 64, 215616, 256
 fp = C.POINTER(C.c_float)
 
 

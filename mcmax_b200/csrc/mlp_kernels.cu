@@ -2,16 +2,17 @@
  * mlp_kernels.cu -- the opacity-surrogate network on sm_100a tensor cores.
  *
  * Network: 6 normalised inputs (log10 a, log10 lambda, n, log10 k,
- * porosity, fmax) -> 4 hidden layers of 256 SiLU units -> 32 outputs
+ * porosity, fmax) -> 4 hidden layers of 256 SiLU units -> 64 outputs
  * (standardised log10 kappa_abs, log10 kappa_sca and Legendre moments of
- * F11 and F12; see surrogate.cu).  No counterpart in the reference: it
+ * F11, F12, F33 and F34; the targets are described at moments_kernel in
+ * part_kernels.cu).  No counterpart in the reference: it
  * replaces calls of ComputePart's DHS inner loop (ComputePart.f:318-447)
  * inside its training box.
  *
  * Kernels (one CTA = one warpgroup of 128 threads, one tile = 128 samples):
  *   mlp_fwd_kernel     forward pass.  Layer 0 (6 -> 256) on CUDA cores;
  *                      layers 1-3 (256 -> 256) and the output layer
- *                      (256 -> 32) as tcgen05 BF16 MMAs with FP32
+ *                      (256 -> 64) as tcgen05 BF16 MMAs with FP32
  *                      accumulators in tensor memory; bias + SiLU epilogue
  *                      from tensor memory back into the shared A operand.
  *                      Optionally keeps pre-activations (FP32) and
@@ -38,17 +39,17 @@
 
 namespace mlp {
 
-constexpr int IN = 6, H = 256, OUT = 32, TILE = 128, NT = 128;
+constexpr int IN = 6, H = 256, OUT = 64, TILE = 128, NT = 128;
 constexpr uint32_t A_BYTES = TILE * H * 2;   /* 64 KB activation tile */
 constexpr uint32_t B_BYTES = H * H * 2;      /* 128 KB weight tile */
 
 struct Params {
   const float *W0, *b0;          /* 256 x 6, 256 */
   const float *b123;             /* 3 x 256 */
-  const float *b4;               /* 32 */
+  const float *b4;               /* OUT */
   const __nv_bfloat16 *Wc;       /* 3 x canonical (out rows, in cols) */
   const __nv_bfloat16 *Wtc;      /* 3 x canonical (in rows, out cols) */
-  const __nv_bfloat16 *W4c;      /* canonical 32 rows x 256 */
+  const __nv_bfloat16 *W4c;      /* canonical OUT rows x 256 */
 };
 
 __device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
@@ -209,13 +210,13 @@ __global__ void __launch_bounds__(NTF, 1)
       tc_fence_before();
     }
     if (!ok) break;
-    /* output layer: N = 32, read by the first two warpgroups */
+    /* output layer: N = OUT = 64, 16 columns per warpgroup */
     ok = wait_w();
     if (!ok) break;
     ok = run_gemm(tc, mbar, a0, b0, OUT, H);
     if (!ok) break;
     if (tile + (int)gridDim.x < ntiles) issue_w(P.Wc, B_BYTES);
-    if (t < 2 * TILE) {
+    if (t < (OUT / 16) * TILE) {
       const int c = (t >> 7) * 16;
       float v[16];
       tc_ld16(lane_base + (uint32_t)c, v);
@@ -475,7 +476,7 @@ __global__ void mlp_adam_kernel(float *__restrict__ p, const float *__restrict__
 }
 
 /* BF16 K-major copies of the tensor-core weights from the FP32 masters:
- * Wc[l] (out rows, in cols), Wtc[l] (in rows, out cols), W4c (32 x 256) */
+ * Wc[l] (out rows, in cols), Wtc[l] (in rows, out cols), W4c (OUT x 256) */
 __global__ void mlp_pack_kernel(const float *__restrict__ W123, const float *__restrict__ W4,
                                 __nv_bfloat16 *__restrict__ Wc, __nv_bfloat16 *__restrict__ Wtc,
                                 __nv_bfloat16 *__restrict__ W4c) {
@@ -1025,7 +1026,8 @@ extern "C" mcg_status mcg_compute_part_surrogate(mcg_ctx *ctx, int nparts, const
       const SurrogatePart &s = sp[p];
       const double scale = rho_train / s.rho; /* kappa ~ 1 / material density */
       for (int l = 0; l < s.nlam; ++l) {
-        double ka = 0.0, ks = 0.0, wsum = 0.0, chi[SURR_NMOM + 1] = {0}, beta[SURR_NMOM + 1] = {0};
+        double ka = 0.0, ks = 0.0, wsum = 0.0, chi[SURR_NMOM + 1] = {0}, beta[SURR_NMOM + 1] = {0},
+               gam[SURR_NMOM + 1] = {0}, del[SURR_NMOM + 1] = {0};
         for (int k = 0; k < s.ns; ++k) {
           const float *y = Y.data() + (size_t)(s.row0 + (int64_t)k * s.nlam + l) * OUT;
           const double kak = pow(10.0, (double)y[0]) * scale, ksk = pow(10.0, (double)y[1]) * scale;
@@ -1035,25 +1037,35 @@ extern "C" mcg_status mcg_compute_part_surrogate(mcg_ctx *ctx, int nparts, const
           wsum += w;
           chi[0] += w;
           for (int m = 1; m <= SURR_NMOM; ++m) chi[m] += w * (double)y[1 + m];
-          for (int m = 0; m <= SURR_NMOM; ++m) beta[m] += w * (double)y[14 + m];
+          for (int m = 0; m <= SURR_NMOM; ++m) {
+            beta[m] += w * (double)y[14 + m];
+            gam[m] += w * (double)y[27 + m];
+            del[m] += w * (double)y[40 + m];
+          }
         }
         for (int m = 0; m <= SURR_NMOM; ++m) {
           chi[m] /= wsum;
           beta[m] /= wsum;
+          gam[m] /= wsum;
+          del[m] /= wsum;
         }
         out[p].kabs[l] = ka;
         out[p].ksca[l] = ks;
         out[p].kext[l] = ka + ks;
         /* phase matrix on the 180 bins from the moments */
-        double f11[NA], f12[NA], norm = 0.0;
+        double f11[NA], f12[NA], f33[NA], f34[NA], norm = 0.0;
         for (int j = 0; j < NA; ++j) {
-          double a = 0.0, b = 0.0;
+          double a = 0.0, b = 0.0, g = 0.0, d = 0.0;
           for (int m = 0; m <= SURR_NMOM; ++m) {
             a += (2.0 * m + 1.0) * chi[m] * P[m][j];
             b += (2.0 * m + 1.0) * beta[m] * P[m][j];
+            g += (2.0 * m + 1.0) * gam[m] * P[m][j];
+            d += (2.0 * m + 1.0) * del[m] * P[m][j];
           }
           f11[j] = a > 0.0 ? a : 0.0;
           f12[j] = b;
+          f33[j] = g;
+          f34[j] = d;
           norm += f11[j] * sinw[j];
         }
         const double c = norm > 0.0 ? tot2 / norm : 1.0;
@@ -1063,12 +1075,21 @@ extern "C" mcg_status mcg_compute_part_surrogate(mcg_ctx *ctx, int nparts, const
           double b = f12[j] * c;
           if (b > a) b = a;
           if (b < -a) b = -a;
+          /* spheres: F22 = F11, F44 = F33, and F12^2 + F33^2 + F34^2 <= F11^2
+           * for any mixture of them; a prediction outside is scaled back */
+          double g = f33[j] * c, d = f34[j] * c;
+          const double room = a * a - b * b, gd = g * g + d * d;
+          if (gd > room) {
+            const double f = gd > 0.0 ? sqrt(room / gd) : 0.0;
+            g *= f;
+            d *= f;
+          }
           F[0 * NA + j] = a;
           F[1 * NA + j] = b;
           F[2 * NA + j] = a;
-          F[3 * NA + j] = sqrt(a * a - b * b);
-          F[4 * NA + j] = 0.0;
-          F[5 * NA + j] = F[3 * NA + j];
+          F[3 * NA + j] = g;
+          F[4 * NA + j] = d;
+          F[5 * NA + j] = g;
         }
       }
       out[p].rho_av = (1.0 - s.por) * s.rho;

@@ -1020,36 +1020,48 @@ mcg_status mcg_part_static_impl(mcg_ctx *ctx, const mcg_part_in *in, mcg_part_ou
  * moments_kernel reduces each row's Mueller elements to the targets:
  *   [0] log10 kappa_abs, [1] log10 kappa_sca (cm^2/g),
  *   [2 + l - 1] chi_l, l = 1..12  moments of F11: sum_j F11_j P_l(mu_j) w_j
- *   [14 + l]    beta_l, l = 0..12 moments of F12, both / sum_j F11_j w_j,
- *   mu_j = cos((j + 1/2) deg), w_j = sin((j + 1/2) deg); [27..31] = 0.
+ *   [14 + l]    beta_l, l = 0..12 moments of F12,
+ *   [27 + l]    gamma_l, l = 0..12 moments of F33,
+ *   [40 + l]    delta_l, l = 0..12 moments of F34, all / sum_j F11_j w_j,
+ *   mu_j = cos((j + 1/2) deg), w_j = sin((j + 1/2) deg); [53..63] = 0.
+ * (F22 = F11 and F44 = F33 for the spheres of DHS and Mie.)
  * ---------------------------------------------------------------------- */
 namespace {
 
 constexpr int SURR_L = 12;
+constexpr int SURR_OUT = 64; /* targets per sample */
 
 __global__ void __launch_bounds__(128) moments_kernel(int nrows, const double *kabs, const double *ksca,
                                                       const double *Fout, float *out) {
   const int lane = threadIdx.x & 31;
   const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (row >= nrows) return;
-  double s11[SURR_L + 1], s12[SURR_L + 1];
+  double s11[SURR_L + 1], s12[SURR_L + 1], s33[SURR_L + 1], s34[SURR_L + 1];
 #pragma unroll
-  for (int l = 0; l <= SURR_L; ++l) s11[l] = s12[l] = 0.0;
+  for (int l = 0; l <= SURR_L; ++l) s11[l] = s12[l] = s33[l] = s34[l] = 0.0;
   for (int j = lane; j < NA; j += WARP) {
     const double th = DHS_PI * ((double)j + 0.5) / (double)NA;
     const double mu = cos(th), w = sin(th);
     const double f11 = Fout[((size_t)row * 6 + 0) * NA + j] * w;
     const double f12 = Fout[((size_t)row * 6 + 1) * NA + j] * w;
+    const double f33 = Fout[((size_t)row * 6 + 3) * NA + j] * w;
+    const double f34 = Fout[((size_t)row * 6 + 4) * NA + j] * w;
     double p0 = 1.0, p1 = mu;
     s11[0] += f11;
     s12[0] += f12;
+    s33[0] += f33;
+    s34[0] += f34;
     s11[1] += f11 * p1;
     s12[1] += f12 * p1;
+    s33[1] += f33 * p1;
+    s34[1] += f34 * p1;
 #pragma unroll
     for (int l = 1; l < SURR_L; ++l) {
       const double p2 = ((2.0 * l + 1.0) * mu * p1 - (double)l * p0) / (double)(l + 1);
       s11[l + 1] += f11 * p2;
       s12[l + 1] += f12 * p2;
+      s33[l + 1] += f33 * p2;
+      s34[l + 1] += f34 * p2;
       p0 = p1;
       p1 = p2;
     }
@@ -1059,15 +1071,19 @@ __global__ void __launch_bounds__(128) moments_kernel(int nrows, const double *k
     for (int s = 16; s > 0; s >>= 1) {
       s11[l] += __shfl_down_sync(0xffffffffu, s11[l], s);
       s12[l] += __shfl_down_sync(0xffffffffu, s12[l], s);
+      s33[l] += __shfl_down_sync(0xffffffffu, s33[l], s);
+      s34[l] += __shfl_down_sync(0xffffffffu, s34[l], s);
     }
   if (lane == 0) {
-    float *o = out + (size_t)row * 32;
+    float *o = out + (size_t)row * SURR_OUT;
     o[0] = (float)log10(fmax(kabs[row], 1e-30));
     o[1] = (float)log10(fmax(ksca[row], 1e-30));
     const double inv = s11[0] > 0.0 ? 1.0 / s11[0] : 0.0;
     for (int l = 1; l <= SURR_L; ++l) o[1 + l] = (float)(s11[l] * inv);
     for (int l = 0; l <= SURR_L; ++l) o[14 + l] = (float)(s12[l] * inv);
-    for (int k = 27; k < 32; ++k) o[k] = 0.0f;
+    for (int l = 0; l <= SURR_L; ++l) o[27 + l] = (float)(s33[l] * inv);
+    for (int l = 0; l <= SURR_L; ++l) o[40 + l] = (float)(s34[l] * inv);
+    for (int k = 53; k < SURR_OUT; ++k) o[k] = 0.0f;
   }
 }
 
@@ -1214,7 +1230,7 @@ mcg_status mcg_surrogate_targets_impl(mcg_ctx *ctx, int64_t n, const double *in6
     double *d_Fout = ALLOC(double, (size_t)m * 6 * NA, "F out");
     double *d_rhoav = ALLOC(double, m, "rho_av");
     double *d_pflat = ALLOC(double, pflat.size(), "part tables");
-    float *d_out = ALLOC(float, (size_t)m * 32, "targets");
+    float *d_out = ALLOC(float, (size_t)m * SURR_OUT, "targets");
 #undef ALLOC
     for (int r = 0; r < m; ++r) {
       double *b = d_pflat + poff[r];
@@ -1286,7 +1302,7 @@ mcg_status mcg_surrogate_targets_impl(mcg_ctx *ctx, int64_t n, const double *in6
     accum_kernel<<<(m + 3) / 4, 128, 0, st>>>(ad);
     moments_kernel<<<(m + 3) / 4, 128, 0, st>>>(m, d_kabs, d_ksca, d_Fout, d_out);
     ce = cudaGetLastError();
-    tout.resize((size_t)m * 32);
+    tout.resize((size_t)m * SURR_OUT);
     std::vector<int8_t> mok(nslot);
     cudaMemcpyAsync(tout.data(), d_out, tout.size() * sizeof(float), cudaMemcpyDeviceToHost, st);
     cudaMemcpyAsync(mok.data(), d_mok, nslot, cudaMemcpyDeviceToHost, st);
@@ -1299,7 +1315,8 @@ mcg_status mcg_surrogate_targets_impl(mcg_ctx *ctx, int64_t n, const double *in6
       if (mneed[q] && !mok[q])
         return mcg_fail(ctx, MCG_ERR_LIMIT, "surrogate_targets: homogeneous-sphere fallback did not fit");
     for (int r = 0; r < m; ++r)
-      memcpy(out + 32 * order[(size_t)(c0 + r)], tout.data() + (size_t)r * 32, 32 * sizeof(float));
+      memcpy(out + (size_t)SURR_OUT * order[(size_t)(c0 + r)], tout.data() + (size_t)r * SURR_OUT,
+             SURR_OUT * sizeof(float));
   }
   return MCG_OK;
 }

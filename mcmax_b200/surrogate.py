@@ -1,4 +1,4 @@
-"""Opacity surrogate: a 6 -> 4x256 -> 32 network standing in for the
+"""Opacity surrogate: a 6 -> 4x256 -> 64 network standing in for the
 coated-sphere (DHS) sums of ComputePart (ComputePart.f:318-447) inside its
 training box, with the DHS kernels as the fallback outside it.  No
 counterpart in the reference.
@@ -18,18 +18,20 @@ import numpy as np
 
 from . import _ffi
 
-NIN, NOUT, H = 6, 32, 256
+NIN, NOUT, H = 6, 64, 256
 NMOM = 12
 # training box: log10 a [micron], log10 lambda [micron], n, log10 k, porosity, fmax
 BOX_LO = np.array([-2.0, -1.0, 1.5, -3.5, 0.0, 0.0])
 BOX_HI = np.array([3.0, np.log10(3000.0), 3.5, np.log10(2.0), 0.6, 0.8])
 RHO_TRAIN = 3.0
 NF_TRAIN = 20
-# loss weight per output: the two opacities, the F11 moments, the F12 moments
+# loss weight per output: the two opacities, the F11 moments, the F12
+# moments, the F33 and F34 moments (polarisation only)
 OUT_WEIGHT = np.zeros(NOUT, np.float32)
 OUT_WEIGHT[0:2] = 16.0
 OUT_WEIGHT[2:14] = 1.0
 OUT_WEIGHT[14:27] = 0.5
+OUT_WEIGHT[27:53] = 0.25
 
 
 def sobol_samples(n, seed=0):

@@ -5,7 +5,10 @@
 Samples: a scrambled Sobol sequence over the training box (see surrogate.py);
 targets: ComputePart on the GPU for each sample (one grain size, nf = 20,
 material density 3 g/cm^3); training: the tensor-core forward/backward
-kernels with Adam.  Prints the held-out error of the network."""
+kernels with Adam.  Prints the held-out error of the network and its error
+on the learned-opacities deck's 150 grain bins (200 wavelengths) against the
+DHS kernels: kappa_abs and kappa_sca in dex, and the polarisation elements
+F33 and F34 as the median of |F_net - F_DHS| / F11_DHS over the angles."""
 import argparse
 import json
 import time
@@ -40,6 +43,18 @@ def main():
                 test_median_dex_kabs=float(np.median(err[:, 0])), test_p95_dex_kabs=float(np.percentile(err[:, 0], 95)),
                 test_median_dex_ksca=float(np.median(err[:, 1])), test_p95_dex_ksca=float(np.percentile(err[:, 1], 95)),
                 test_median_g=float(np.median(err[:, 2])))
+    from . import model as M
+    lam, _ = M.wavelength_grid(0.1, 3000.0, 200)
+    parts, _ = M.learned_disk_parts(lam)
+    got, used = S.compute_part_surrogate(ctx, parts, params)
+    ref = ctx.compute_part_batch(parts)
+    lk = np.concatenate([np.log10(g["kabs"] / r["kabs"]) for g, r in zip(got, ref)])
+    ls = np.concatenate([np.log10(g["ksca"] / r["ksca"]) for g, r in zip(got, ref)])
+    f33 = np.concatenate([(np.abs(g["F"][:, 3] - r["F"][:, 3]) / r["F"][:, 0]).ravel() for g, r in zip(got, ref)])
+    f34 = np.concatenate([(np.abs(g["F"][:, 4] - r["F"][:, 4]) / r["F"][:, 0]).ravel() for g, r in zip(got, ref)])
+    info.update(bins_served=int(np.sum(used)), bins_median_dex_kabs=float(np.median(np.abs(lk))),
+                bins_median_dex_ksca=float(np.median(np.abs(ls))), bins_median_f33_rel=float(np.median(f33)),
+                bins_median_f34_rel=float(np.median(f34)), kappa_weight=float(S.OUT_WEIGHT[0]))
     S.save(a.out, params, info)
     print(json.dumps({k: (v.tolist() if isinstance(v, np.ndarray) else v) for k, v in info.items()}))
 

@@ -5,7 +5,7 @@ back-propagated dZ), FP32 elsewhere.  `emulate=False` gives the plain
 float64 network for finite-difference checks of the formulas."""
 import numpy as np
 
-IN, H, OUT = 6, 256, 32
+IN, H, OUT = 6, 256, 64
 NP = H * IN + H + 3 * H * H + 3 * H + OUT * H + OUT
 
 

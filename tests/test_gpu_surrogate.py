@@ -19,10 +19,12 @@ def _moments(F, nmom=S.NMOM):
     P = [np.ones(180), mu]
     for l in range(1, nmom):
         P.append(((2 * l + 1) * mu * P[l] - l * P[l - 1]) / (l + 1))
-    f11, f12 = F[0] * w, F[1] * w
+    f11, f12, f33, f34 = F[0] * w, F[1] * w, F[3] * w, F[4] * w
     s0 = f11.sum()
-    return np.array([(f11 * P[l]).sum() / s0 for l in range(1, nmom + 1)]), \
-        np.array([(f12 * P[l]).sum() / s0 for l in range(0, nmom + 1)])
+    return (np.array([(f11 * P[l]).sum() / s0 for l in range(1, nmom + 1)]),
+            np.array([(f12 * P[l]).sum() / s0 for l in range(0, nmom + 1)]),
+            np.array([(f33 * P[l]).sum() / s0 for l in range(0, nmom + 1)]),
+            np.array([(f34 * P[l]).sum() / s0 for l in range(0, nmom + 1)]))
 
 
 def test_targets_are_compute_part_of_one_size(ctx):
@@ -36,10 +38,12 @@ def test_targets_are_compute_part_of_one_size(ctx):
                                          nf=20)])[0]
         assert abs(t[0] - np.log10(r["kabs"][0])) < 1e-5
         assert abs(t[1] - np.log10(r["ksca"][0])) < 1e-5
-        chi, beta = _moments(r["F"][0])
+        chi, beta, gamma, delta = _moments(r["F"][0])
         assert np.allclose(t[2:14], chi, atol=2e-6)
         assert np.allclose(t[14:27], beta, atol=2e-6)
-        assert np.all(t[27:] == 0)
+        assert np.allclose(t[27:40], gamma, atol=2e-6)
+        assert np.allclose(t[40:53], delta, atol=2e-6)
+        assert np.all(t[53:] == 0)
 
 
 def _config_bins(nlam=60):
@@ -87,6 +91,12 @@ def test_surrogate_trains_and_serves_bins(ctx):
     for g in got:
         F = g["F"]
         assert np.all(F[:, 0] >= 0) and np.all(np.abs(F[:, 1]) <= F[:, 0] + 1e-12)
+        # spheres: F22 = F11, F44 = F33 and F12^2 + F33^2 + F34^2 <= F11^2
+        assert np.array_equal(F[:, 2], F[:, 0]) and np.array_equal(F[:, 5], F[:, 3])
+        assert np.all(F[:, 1] ** 2 + F[:, 3] ** 2 + F[:, 4] ** 2 <= F[:, 0] ** 2 * (1 + 1e-9) + 1e-300)
+    # the polarisation elements follow the DHS kernels': F34 is not zero
+    f34 = np.concatenate([g["F"][:, 4].ravel() for g in got])
+    assert np.abs(f34).max() > 0
 
 
 def test_surrogate_falls_back_outside_the_box(ctx):
