@@ -86,7 +86,7 @@ def fold_output_scaling(params, mean, std):
     return p
 
 
-def train(ctx, samples, T, epochs=300, batch=8192, lr=2e-3, lr_min=2e-5, seed=1):
+def train(ctx, samples, T, epochs=300, batch=8192, lr=2e-3, lr_min=2e-5, seed=1, weights=None):
     """Train on (samples, targets); returns (params, info).  Targets are
     standardised per output for training and the scaling is folded into
     the output layer, so the returned network outputs physical targets."""
@@ -102,7 +102,8 @@ def train(ctx, samples, T, epochs=300, batch=8192, lr=2e-3, lr_min=2e-5, seed=1)
     Ts = ((T - mean) / std).astype(np.float32)
     ctx.mlp_set_params(init_params(seed))
     t0 = time.perf_counter()
-    rep = ctx.mlp_train(X, Ts, OUT_WEIGHT, epochs=epochs, batch=batch, lr=lr, lr_min=lr_min, seed=seed)
+    w = OUT_WEIGHT if weights is None else np.asarray(weights, np.float32)
+    rep = ctx.mlp_train(X, Ts, w, epochs=epochs, batch=batch, lr=lr, lr_min=lr_min, seed=seed)
     wall = time.perf_counter() - t0
     p = fold_output_scaling(ctx.mlp_get_params(), mean, std)
     ctx.mlp_set_params(p)

@@ -27,6 +27,8 @@ def main():
     ap.add_argument("--batch", type=int, default=8192)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--pol-weight", type=float, default=float(S.OUT_WEIGHT[27]),
+                    help="loss weight of the F33 and F34 moments")
     ap.add_argument("--out", default="surrogate.npz")
     a = ap.parse_args()
     ctx = api.Context(0)
@@ -34,7 +36,10 @@ def main():
     X = S.sobol_samples(a.samples, seed=a.seed)
     T = S.targets(ctx, X)
     t_targets = time.perf_counter() - t0
-    params, info = S.train(ctx, X, T, epochs=a.epochs, batch=a.batch, lr=a.lr, lr_min=a.lr * 1e-2, seed=a.seed)
+    w = S.OUT_WEIGHT.copy()
+    w[27:53] = a.pol_weight
+    params, info = S.train(ctx, X, T, epochs=a.epochs, batch=a.batch, lr=a.lr, lr_min=a.lr * 1e-2, seed=a.seed,
+                           weights=w)
     Xt = S.sobol_samples(a.test, seed=a.seed + 1000)
     Tt = S.targets(ctx, Xt)
     Y = ctx.mlp_forward(S.normalize(Xt))
@@ -54,7 +59,7 @@ def main():
     f34 = np.concatenate([(np.abs(g["F"][:, 4] - r["F"][:, 4]) / r["F"][:, 0]).ravel() for g, r in zip(got, ref)])
     info.update(bins_served=int(np.sum(used)), bins_median_dex_kabs=float(np.median(np.abs(lk))),
                 bins_median_dex_ksca=float(np.median(np.abs(ls))), bins_median_f33_rel=float(np.median(f33)),
-                bins_median_f34_rel=float(np.median(f34)), kappa_weight=float(S.OUT_WEIGHT[0]))
+                bins_median_f34_rel=float(np.median(f34)), kappa_weight=float(w[0]), pol_weight=float(a.pol_weight))
     S.save(a.out, params, info)
     print(json.dumps({k: (v.tolist() if isinstance(v, np.ndarray) else v) for k, v in info.items()}))
 
