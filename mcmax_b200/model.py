@@ -1115,6 +1115,11 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
     else:
         Fstar = np.array([math.pi * rstar_cm ** 2 * api.planck(tstar, x) for x in lam])
         Lstar = integrate(nu, Fstar)
+    if v("av", 0.0) != 0.0 or v("adjustav", False, bool):
+        # the interstellar extinction of the observed fluxes (Reddening.f,
+        # Telescope.f:85-92, 233-234) is not built: refuse rather than write
+        # unreddened fluxes
+        raise ValueError("av / adjustav: interstellar reddening is not built")
     nr, nt = R.size - 1, Theta.size
     w0 = np.array(weights)
     w = np.tile(w0, (nr, nt - 1, 1))

@@ -242,7 +242,7 @@ def spectrum_wavelengths(lam, lam1, lam2, nlam=-1, lamfile=None):
     return 10.0 ** (math.log10(lam1) + math.log10(lam2 / lam1) * np.arange(n) / (n - 1))
 
 
-def read_observations(path, lam, incangle=45.0, rout=None):
+def read_observations(path, lam, incangle=45.0, rout=None, vis_norm_fov=True):
     """The observations of an MCMax observation file (Telescope.f:583-1100):
     keywords before the first type= line set the defaults, each type= line
     starts an observation whose own keywords follow.  Returns a list of
@@ -254,14 +254,17 @@ def read_observations(path, lam, incangle=45.0, rout=None):
     Defaults: inc from the deck's incangle, lam1/lam2 the model's range,
     nphi 45, nrad 2, npix 500, nint 1000, fov twice the grid's outer radius
     `rout`, scaletype 1, nphot 1000, nphotstar 1000, nexits 5
-    (Telescope.f:602-619).  An IMAGE observation's lam1 is
+    (Telescope.f:602-619), and vis_norm_fov from the input deck's
+    (Telescope.f:657), which the file can set for all observations or one
+    (Telescope.f:1023, 1176).  An IMAGE observation's lam1 is
     the default-level `lam`, else the middle of the wavelength range
     (Telescope.f:591,710-712); a `lam` among an observation's own keywords
     sets its lam1."""
     lam = np.asarray(lam, float)
     default = dict(inc=float(incangle), lam1=float(lam[0]), lam2=float(lam[-1]), nlam=-1, lamfile="", nphi=45,
                    nrad=2, flag="", npix=500, nint=1000, fov=[] if rout is None else [2.0 * float(rout)],
-                   scaletype=1, b=[100.0], theta=[0.0], d=-1.0, nphot=1000, nphotstar=1000, nexits=5)
+                   scaletype=1, b=[100.0], theta=[0.0], d=-1.0, nphot=1000, nphotstar=1000, nexits=5,
+                   vis_norm_fov=bool(vis_norm_fov))
     deflam = (float(lam[0]) + float(lam[-1])) / 2.0
     obs, cur = [], default
     base = os.path.dirname(os.path.abspath(path))
@@ -308,6 +311,8 @@ def read_observations(path, lam, incangle=45.0, rout=None):
                 cur["b" if key[:4] == "base" else "theta"][i - 1] = num(val)
             elif key == "d":
                 cur["d"] = num(val)
+            elif key == "vis_norm_fov":
+                cur[key] = val.strip().strip(".").lower() in ("true", "t")
             elif key[:3] == "fov":
                 i = int(key[3:]) if len(key) > 3 else 1
                 while len(cur["fov"]) < i:

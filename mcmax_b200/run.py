@@ -220,7 +220,8 @@ def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opac
                  flag="") for a in spectra]
     skipped, images = [], []
     for path in observations:
-        for ob in outputs.read_observations(path, m.lam, run.get("incangle", 45.0), rout=m.R[-1]):
+        for ob in outputs.read_observations(path, m.lam, run.get("incangle", 45.0), rout=m.R[-1],
+                                            vis_norm_fov=run.get("vis_norm_fov", True)):
             {"SPECTRUM": todo, "IMAGE": images, "IFU": images, "VISIBILITY": images,
              "BASEVIS": images}.get(ob["kind"], skipped).append(ob)
     rfix = fixed_radii(run["zones"], m.R[1], m.R[-1])
@@ -234,12 +235,12 @@ def run_deck(ctx, deck, nphot, outdir=".", overrides=(), precision="mixed", opac
         if ob["kind"] == "BASEVIS":
             files.append(observe_basevis(ctx, m, T, ob, outdir, rfix, seed=run["seed"],
                                          posangle=run.get("posangle", 0.0),
-                                         vis_norm_fov=run.get("vis_norm_fov", True)))
+                                         vis_norm_fov=ob.get("vis_norm_fov", True)))
             continue
         if ob["kind"] == "VISIBILITY":
             files.append(observe_visibility(ctx, m, T, ob, outdir, rfix, seed=run["seed"],
                                             posangle=run.get("posangle", 0.0),
-                                            vis_norm_fov=run.get("vis_norm_fov", True)))
+                                            vis_norm_fov=ob.get("vis_norm_fov", True)))
             continue
         observe = observe_ifu if ob["kind"] == "IFU" else observe_image
         files += observe(ctx, m, T, ob, outdir, rfix, seed=run["seed"], posangle=run.get("posangle", 0.0))

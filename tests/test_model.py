@@ -158,6 +158,9 @@ idum=-7
     assert run == dict(seed=7, randomwalk=True, factRW=5.0, maxinteract=20000, maxruntime=-1.0, nruns=1, nphotdiffuse=25,
                        dtdiffuse=1.0, maxiter=10, epsiter=3.0, incangle=45.0, outputfits=False, posangle=0.0,
                        iterate=True, thin_start=True, settling=None, fixed=None, vis_norm_fov=True)
+    # interstellar reddening of the observed fluxes is not built: the deck is refused
+    with pytest.raises(ValueError, match="reddening"):
+        M.deck_model(None, str(deck), overrides=["av=1.5"], compute_parts=oracle_parts)
     assert np.allclose(m.comp_w.sum(1), 1.0)
     ref = M.disk_model(None, nrad=12, ntheta=8, nlam=20, lam2=3000.0, mdust=1e-5, sh=0.0707, ngrains=3,
                        opacities=(m.Kabs, m.Ksca, m.F))

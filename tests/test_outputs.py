@@ -150,3 +150,17 @@ def test_visibility_of_a_uniform_disk():
     # a telescope taper (diameter d) only lowers the long-baseline response
     V1, _ = OUT.visibility(R, rphi, 60.0, 0.3, 2.0, d, diam=8.0)
     assert 0.0 <= V1 <= 1.0 + 1e-12
+
+
+def test_observation_vis_norm_fov(tmp_path):
+    """vis_norm_fov: the input deck's value unless the observation file sets
+    it for all observations or for one (Telescope.f:657, 1023, 1176)"""
+    p = tmp_path / "obs.out"
+    p.write_text("nphi=30\nvis_norm_fov=.false.\n*****\ntype='VISIBILITY'\n"
+                 "type='VISIBILITY'\nvis_norm_fov=.true.\n")
+    lam = np.geomspace(0.1, 1000.0, 20)
+    obs = OUT.read_observations(str(p), lam, rout=100.0)
+    assert [o["vis_norm_fov"] for o in obs] == [False, True]
+    p.write_text("*****\ntype='VISIBILITY'\n")
+    assert OUT.read_observations(str(p), lam, vis_norm_fov=False)[0]["vis_norm_fov"] is False
+    assert OUT.read_observations(str(p), lam)[0]["vis_norm_fov"] is True
