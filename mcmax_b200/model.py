@@ -1172,11 +1172,12 @@ def deck_model(ctx, deck, overrides=(), compute_parts=None):
             raise ValueError("mpset: an opacNN grain has no size or density to settle")
         run["settling"] = dict(rho=rho_g, rv=rv, alpha=alpha,
                                rscale=np.array([r.get("rscale", 1.0) for r in res]), gas2dust=v("gas2dust", 100.0))
-    # the reference runs the start whenever the deck has zones (nzones /= 0):
-    # its structure pass rebuilds a fixed zone's profile at the cell
-    # centres.  With fixmpset the settled zone above is that rebuild already.
+    # the reference runs the start whenever the deck has zones (nzones /= 0)
+    # or settles with fixmpset (Init.f:3923-3927): its structure passes
+    # rebuild a fixed zone's profile at the cell centres, with
+    # FixedMPSettling's factors recomputed before each (run["fixed"])
     run["thin_start"] = (run["iterate"] or denstype in THIN_START_DENSITIES or mpset
-                         or (bool(zones) and not v("fixmpset", False, bool)))
+                         or v("fixmpset", False, bool) or bool(zones))
     return m, run
 
 

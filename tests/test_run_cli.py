@@ -77,6 +77,7 @@ class FakeContext:
                        grain_scale=None, shtype=None):
         self.structure_calls = getattr(self, "structure_calls", 0) + 1
         self.structure_zones = zones
+        self.grain_scales = getattr(self, "grain_scales", []) + [grain_scale]
         return (np.array(dens), np.array(dens0), np.array(gasdens), np.array(w), np.array(w0))
 
     def trace_image(self, T, lam0, angle, npixel=500, nint=1000, Rmax=None, pa=0.0, nphi=45, nr=2, Rfix=(),
@@ -274,3 +275,19 @@ def test_image_in_arcsec(tmp_path):
     d = 100.0 * outputs.PARSEC
     zscale = 1e3 * (10 / 0.4) ** 2
     assert np.allclose(im, 2.0 * 1e23 * zscale / d ** 2, rtol=1e-12)
+
+
+def test_fixed_settling_deck_starts_with_settled_structure_passes(tmp_path):
+    """fixmpset: the optically thin start runs (Init.f:3923-3927) and every
+    structure pass gets FixedMPSettling's factors (DiskStructure.f:108)"""
+    deck = _write_inputs(tmp_path)
+    made = []
+
+    def factory(device):
+        made.append(FakeContext(device))
+        return made[-1]
+
+    R.main([deck, "1e3", "-o", str(tmp_path / "o"), "-s", "fixmpset=.true.", "-s", "alphaturb=1d-3"], context=factory)
+    ctx = made[0]
+    assert ctx.structure_calls == 3
+    assert all(g is not None and g.shape[0] == 2 and np.all((g[:, 1:] > 0) & (g[:, 1:] <= 1)) for g in ctx.grain_scales)
