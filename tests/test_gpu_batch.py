@@ -87,10 +87,17 @@ def test_uneven_models_with_random_walk_match_their_single_runs(ctx):
         _, a = ctx.mcradiation(n, seed=s, **run)
         assert abs(o["EJv"].sum() / a["EJv"].sum() - 1) < 0.05
         # escaping energy in three inclination ranges (the raw SED total is
-        # weighted by 1/dnu and so dominated by the few far-infrared packets)
+        # weighted by 1/dnu and so dominated by the few far-infrared
+        # packets), within 4 sigma of the packets' Poisson noise in the range
         eo, ea = _energy_by_inclination(m, o), _energy_by_inclination(m, a)
-        assert np.all(np.abs(eo / ea - 1) < 0.05), (eo, ea)
+        no, na = _packets_by_inclination(o), _packets_by_inclination(a)
+        tol = 4.0 * np.sqrt(1.0 / np.maximum(no, 1) + 1.0 / np.maximum(na, 1)) + 0.01
+        assert np.all(np.abs(eo / ea - 1) < tol), (eo, ea, no, na)
     assert rw_steps > 0
+
+
+def _packets_by_inclination(out, groups=3):
+    return np.asarray(out["ispec"], float).reshape(-1, 31)[:, 1:].sum(0).reshape(groups, -1).sum(1)
 
 
 def _energy_by_inclination(m, out, groups=3):
