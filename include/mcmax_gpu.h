@@ -225,6 +225,12 @@ typedef struct {
                              MCRadiation.f:323-342 does; *nphot_inout returns
                              the count that ran.  Time is measured on the
                              device from the kernel's start. */
+  int32_t t4_single;      /* 1: the temperature interpolations of increaseT
+                             and determineT form real(i)**4 in single
+                             precision as the reference does (Radiation.f:
+                             551, 584, 698), here and in the next
+                             mcg_finalize_t; 0 (default): exact FP64, which
+                             differs by under 1e-7 relative */
 } mcg_run;
 
 typedef struct {

@@ -90,7 +90,7 @@ class Run(C.Structure):
     _fields_ = [
         ("seed", C.c_uint64), ("randomwalk", C.c_int), ("factRW", C.c_double),
         ("maxinteract", C.c_int64), ("nruns", C.c_int), ("precision", C.c_int),
-        ("threads", C.c_int), ("block", C.c_int), ("maxruntime", C.c_double),
+        ("threads", C.c_int), ("block", C.c_int), ("maxruntime", C.c_double), ("t4_single", C.c_int32),
     ]
 
 

@@ -116,13 +116,15 @@ class Context:
         self.model = m
 
     def mcradiation(self, nphot, seed=1, randomwalk=False, factRW=10.0, maxinteract=0, nruns=1,
-                    precision="exact", threads=0, block=0, fetch=True, maxruntime=-1.0):
+                    precision="exact", threads=0, block=0, fetch=True, maxruntime=-1.0, t4_single=False):
         """Run the packet loop; returns (nphot_out, result dict).  nphot_out
-        is smaller than nphot when maxruntime (seconds, > 0) cut the run."""
+        is smaller than nphot when maxruntime (seconds, > 0) cut the run.
+        t4_single: the temperature interpolations in the reference's single
+        precision (mcg_run.t4_single)."""
         m = self.model
         prec = {"fp64": _ffi.PREC_FP64, "mixed": _ffi.PREC_MIXED, "exact": _ffi.PREC_EXACT}[precision]
         run = _ffi.Run(int(seed), int(bool(randomwalk)), float(factRW), int(maxinteract), int(nruns), prec,
-                       int(threads), int(block), float(maxruntime))
+                       int(threads), int(block), float(maxruntime), int(bool(t4_single)))
         out = {}
         res = _ffi.Result()
         if fetch:

@@ -87,6 +87,7 @@ struct DevModel {
 /* Accumulators of a run on the device. */
 struct DevRun {
   int ncell = 0, nlam = 0, nruns = 0;
+  int t4single = 0;         /* the last run's temperature-interpolation precision, for mcg_finalize_t */
   /* per-run blocks (nruns*ncell) below; the combined results of the last
    * call are EJvTot/EJv2Tot (run averages), NiTot (sum), and the last run's
    * Eabs/T block */

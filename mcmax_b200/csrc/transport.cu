@@ -191,7 +191,8 @@ namespace {
 
 __global__ void finalize_kernel(int nr, int nc, const double *V, const double *EJv, const double *EJv2,
                                 const int *Ni, const double *Tbw, const double *KpCell, int uniform,
-                                double Tstar_cell, double *Tout, double *dTout, double *dEJvout) {
+                                double Tstar_cell, int t4single, double *Tout, double *dTout,
+                                double *dEJvout) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nr * nc) return;
   const int i = c / nc;
@@ -204,7 +205,7 @@ __global__ void finalize_kernel(int nr, int nc, const double *V, const double *E
   const double *kp = KpCell + (uniform ? (size_t)0 : (size_t)c * TP_TT);
   const double e = EJv[c] / V[c];
   const double e2 = EJv2[c] / (V[c] * V[c]);
-  double T = tp_determine_t(kp, e, Tbw[c]);
+  double T = tp_determine_t(kp, e, Tbw[c], t4single);
   if (T < 1.0) T = 1.0;
   double dEJv, dT;
   if (Ni[c] > 1) {
@@ -681,6 +682,8 @@ mcg_status mcg_run_prepare(mcg_ctx *ctx, const mcg_run *run, int64_t *nphot, Run
   tm.kd_index = m.kd_index; tm.thick = m.thick;
   tm.R0 = m.R0;
   tm.maxruntime = run->maxruntime;
+  tm.t4single = run->t4_single ? 1 : 0;
+  ctx->run.t4single = tm.t4single;
   TAcc &ta = rp->ta;
   memset(&ta, 0, sizeof ta);
   ta.EJv = R.EJv; ta.EJv2 = R.EJv2; ta.Eabs = R.Eabs; ta.T = R.T; ta.Ni = R.Ni; ta.lastphot = R.lastphot;
@@ -862,7 +865,7 @@ mcg_status mcg_finalize_impl(mcg_ctx *ctx, double *T, double *dT, double *dEJv) 
   if (Tsc < 1.0) Tsc = 1.0;
   finalize_kernel<<<nblk(nc, 256), 256, 0, ctx->stream>>>(m.nr, m.nc, m.V, R.EJvTot, R.EJv2Tot, R.NiTot,
                                                           R.T + (size_t)(R.nruns - 1) * nc, m.KpCell,
-                                                          m.uniform_mix, Tsc, d, d + nc, d + 2 * nc);
+                                                          m.uniform_mix, Tsc, R.t4single, d, d + nc, d + 2 * nc);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess && T) e = cudaMemcpyAsync(T, d, sizeof(double) * nc, cudaMemcpyDeviceToHost, ctx->stream);
   if (e == cudaSuccess && dT) e = cudaMemcpyAsync(dT, d + nc, sizeof(double) * nc, cudaMemcpyDeviceToHost, ctx->stream);

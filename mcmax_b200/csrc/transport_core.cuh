@@ -80,6 +80,7 @@ struct TModel {
   const int *kd_index;
   const unsigned char *thick;
   double maxruntime; /* seconds; > 0: the run-time limit of MCRadiation.f:323-342 */
+  int t4single;      /* 1: the temperature interpolation's i^4 in single precision, as the reference */
 };
 
 /* accumulators */
@@ -466,8 +467,27 @@ TP_FN double tp_t4(int i) {
 }
 TP_FN double tp_qroot(double x) { return sqrt(sqrt(x)); }
 
+/* the reference's real(i)**4 (Radiation.f:551, 584, 698): single precision,
+ * the integer power expanded as (x x)(x x) */
+TP_FN float tp_t4f(int i) {
+  const float x = (float)i;
+  const float x2 = x * x;
+  return x2 * x2;
+}
+
+/* i^4 + (j^4 - i^4) num / den, the T^4 interpolation of increaseT and
+ * determineT, with the powers in double or (single) as the reference forms
+ * them: its difference is a single-precision subtraction widened to double */
+TP_FN double tp_t4_interp(int i, int j, double num, double den, int single) {
+  if (single) {
+    const float a = tp_t4f(i), d = tp_t4f(j) - tp_t4f(i);
+    return (double)a + ((double)d * num) / den;
+  }
+  return tp_t4(i) + ((tp_t4(j) - tp_t4(i)) * num) / den;
+}
+
 /* determineT, Radiation.f:629-702, on the cell's Planck-mean table kp */
-TP_NOINLINE double tp_determine_t(const double *kp, double E1, double Tcur) {
+TP_NOINLINE double tp_determine_t(const double *kp, double E1, double Tcur, int single = 0) {
   int iTmin = 1, iTmax = TP_TMAX;
   int iT = (int)(Tcur / 1.0);
   if (iT < 1) iT = 1;
@@ -503,7 +523,7 @@ TP_NOINLINE double tp_determine_t(const double *kp, double E1, double Tcur) {
     iT0 = iT;
   }
   if (iTmin == iTmax) return (double)iTmin;
-  return tp_qroot(tp_t4(iTmin) + ((tp_t4(iTmax) - tp_t4(iTmin)) * (E1 - Emin)) / (Emax - Emin));
+  return tp_qroot(tp_t4_interp(iTmin, iTmax, E1 - Emin, Emax - Emin, single));
 }
 
 /* Temperature of a cell with absorbed energy per mass E1: the value the
@@ -512,9 +532,9 @@ TP_NOINLINE double tp_determine_t(const double *kp, double E1, double Tcur) {
  * kp[i+1] >= E1 brackets E1 when kp[i] <= E1.  `lo` is a known lower bound
  * of that i (0 when unknown); *ibr returns the bracket (0 when the
  * determineT fallback was taken). */
-TP_FN double tp_tinv(const double *kp, double E1, int lo, int *ibr) {
+TP_FN double tp_tinv(const double *kp, double E1, int lo, int *ibr, int single = 0) {
   *ibr = 0;
-  if (!(E1 >= kp[1]) || !(E1 <= kp[TP_TMAX])) return tp_determine_t(kp, E1, 0.0);
+  if (!(E1 >= kp[1]) || !(E1 <= kp[TP_TMAX])) return tp_determine_t(kp, E1, 0.0, single);
   /* galloping search from lo for the first p in [2, TMAX] with kp[p] >= E1;
    * a hint is used only when kp[lo] < E1 (then lo is below the answer) */
   if (lo < 1 || lo >= TP_TMAX || !(kp[lo] < E1)) lo = 1;
@@ -538,7 +558,7 @@ TP_FN double tp_tinv(const double *kp, double E1, int lo, int *ibr) {
   int i = l - 1;
   *ibr = i;
   double kp0 = kp[i], kp1 = kp[i + 1];
-  return tp_qroot(tp_t4(i) + ((tp_t4(i + 1) - tp_t4(i)) * (E1 - kp0)) / (kp1 - kp0));
+  return tp_qroot(tp_t4_interp(i, i + 1, E1 - kp0, kp1 - kp0, single));
 }
 
 /* ------------------------------------------------------------- scattering */
@@ -637,8 +657,8 @@ TP_FN void tp_interact(const TModel &m, const TAcc &A, px_stream *r, TPkt &p, TL
     const double Enew = Eold + dE;
     const double mass = m.mass[c];
     int ib0, ib1;
-    const double T0 = tp_tinv(kp, Eold / mass, 0, &ib0);
-    const double T1 = tp_tinv(kp, Enew / mass, ib0, &ib1);
+    const double T0 = tp_tinv(kp, Eold / mass, 0, &ib0, m.t4single);
+    const double T1 = tp_tinv(kp, Enew / mass, ib0, &ib1, m.t4single);
     int iT0 = (int)(T0 / 1.0), iT1 = (int)(T1 / 1.0);
     double epsT0 = T0 - (double)iT0 * 1.0, epsT1 = T1 - (double)iT1 * 1.0;
     if (iT0 >= TP_TMAX - 1) iT0 = TP_TMAX - 2;
@@ -850,7 +870,7 @@ TP_FN int tp_random_walk(const TModel &m, const TAcc &A, px_stream *r, TPkt &p, 
   p.nEJv = p.nEJv + EJv * Kabs;
   const double *kp = m.KpCell + (m.uniform_mix ? (size_t)0 : (size_t)c * TP_TT);
   int ib;
-  A.T[c] = tp_tinv(kp, (Eold + dEa) / m.mass[c], 0, &ib);
+  A.T[c] = tp_tinv(kp, (Eold + dEa) / m.mass[c], 0, &ib, m.t4single);
   L.tautot += v / dmin;
   L.cnt[TC_RWSTEP]++;
   return 1;

@@ -296,6 +296,7 @@ void fill_fmodel(mcg_ctx *ctx, int pi, const TModel &tm, FModel<R> &g) {
   g.KDext = m.KDext; g.KDabs = m.KDabs; g.rw_logy = m.rw_logy; g.rw_phi = m.rw_phi;
   g.kd_index = m.kd_index; g.thick = m.thick; g.rw_dmin = m.rw_dmin;
   g.maxruntime = tm.maxruntime;
+  g.t4single = tm.t4single;
 }
 
 template <class R>

@@ -67,6 +67,7 @@ struct FModel {
   const unsigned char *thick;
   const double *rw_dmin;        /* factRW x the cell's shortest mean free path */
   double maxruntime;            /* seconds; > 0: MCRadiation.f:323-342 */
+  int t4single;                 /* 1: single-precision i^4 in the temperature inversion */
 };
 
 #define F_NGUIDE 32
@@ -434,8 +435,8 @@ TP_FN void f_scatangle(const FModel<R> &m, px_stream *r, FPkt<R> &p, int mat) {
 
 /* ------------------------------------------------------------- temperature */
 /* gallop from `lo` (a valid lower bound of the bracket) */
-TP_FN double f_tinv(const double *kp, double E1, int lo, int *ibr) {
-  return tp_tinv(kp, E1, lo, ibr);
+TP_FN double f_tinv(const double *kp, double E1, int lo, int *ibr, int single) {
+  return tp_tinv(kp, E1, lo, ibr, single);
 }
 
 /* ------------------------------------------------------------- event steps
@@ -693,8 +694,8 @@ F_COLD void f_absorb_pre(const FModel<R> &m, const TAcc &A, size_t off, px_strea
   const double mass = m.mass[c];
   int hint = A.kp_hint[off + c];
   int ib0, ib1;
-  const double T0 = f_tinv(kp, Eold / mass, hint, &ib0);
-  const double T1 = f_tinv(kp, (Eold + dE) / mass, ib0, &ib1);
+  const double T0 = f_tinv(kp, Eold / mass, hint, &ib0, m.t4single);
+  const double T1 = f_tinv(kp, (Eold + dE) / mass, ib0, &ib1, m.t4single);
   if (ib1 > hint) A.kp_hint[off + c] = ib1;
   int iT0 = (int)T0, iT1 = (int)T1;
   a.e0 = T0 - (double)iT0;
@@ -978,7 +979,7 @@ F_COLD int f_random_walk(const FModel<R> &m, const TAcc &A, size_t off, px_strea
   p.nEJv += EJv * Kabs;
   const double *kp = m.KpCell + (m.uniform_mix ? (size_t)0 : (size_t)c * TP_TT);
   int ib;
-  A.T[off + c] = f_tinv(kp, (Eold + dEa) / m.mass[c], A.kp_hint[off + c], &ib);
+  A.T[off + c] = f_tinv(kp, (Eold + dEa) / m.mass[c], A.kp_hint[off + c], &ib, m.t4single);
   if (ib > A.kp_hint[off + c]) A.kp_hint[off + c] = ib;
   L.tautot += v / dmin;
   L.cnt[TC_RWSTEP]++;

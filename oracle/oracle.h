@@ -152,6 +152,9 @@ int orc_mcradiation(const orc_model *m, const orc_run *run, orc_result *out);
 /* temperature from absorbed energy per mass, Radiation.f:629-702 (used for
  * the post-MC step Main.f:498-549) */
 double orc_determine_t(const double *kp, double E1, double Tcur);
+/* 1: orc_determine_t and orc_increase_t (and the packet loop through them)
+ * form real(i)**4 in single precision as the reference does; 0: FP64 */
+void orc_set_t4_single(int on);
 /* Bjorkman-Wood upward scan, Radiation.f:537-562 */
 double orc_increase_t(const double *kp, double E1, double Tcur);
 

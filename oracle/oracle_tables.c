@@ -48,6 +48,26 @@ static double t4(int i) {
   return d2 * d2;
 }
 
+/* 1: the interpolations below form real(i)**4 in single precision as the
+ * reference does (Radiation.f:551, 584, 698), (x x)(x x) with x = real(i),
+ * their difference a single-precision subtraction widened to double */
+static int t4_single = 0;
+void orc_set_t4_single(int on) { t4_single = on != 0; }
+
+static float t4f(int i) {
+  const float x = (float)i;
+  const float x2 = x * x;
+  return x2 * x2;
+}
+
+static double t4_interp(int i, int j, double num, double den) {
+  if (t4_single) {
+    const float a = t4f(i), d = t4f(j) - t4f(i);
+    return (double)a + ((double)d * num) / den;
+  }
+  return t4(i) + ((t4(j) - t4(i)) * num) / den;
+}
+
 /* (x)^(1/4) as sqrt(sqrt(x)): within 1 ulp of pow(x, 0.25), deterministic on
  * host and device */
 static double qroot(double x) { return sqrt(sqrt(x)); }
@@ -101,7 +121,7 @@ double orc_determine_t(const double *kp, double E1, double Tcur) {
     iT0 = iT;
   }
   if (iTmin == iTmax) return (double)iTmin;
-  return qroot(t4(iTmin) + ((t4(iTmax) - t4(iTmin)) * (E1 - Emin)) / (Emax - Emin));
+  return qroot(t4_interp(iTmin, iTmax, E1 - Emin, Emax - Emin));
 }
 
 double orc_increase_t(const double *kp, double E1, double Tcur) {
@@ -112,7 +132,7 @@ double orc_increase_t(const double *kp, double E1, double Tcur) {
   for (int i = j; i <= ORC_TMAX - 1; ++i) {
     double kp1 = kp[i + 1];
     if (kp0 <= E1 && kp1 >= E1)
-      return qroot(t4(i) + ((t4(i + 1) - t4(i)) * (E1 - kp0)) / (kp1 - kp0));
+      return qroot(t4_interp(i, i + 1, E1 - kp0, kp1 - kp0));
     kp0 = kp1;
   }
   return orc_determine_t(kp, E1, Tcur);

@@ -187,3 +187,29 @@ def test_maxruntime_shrinks_the_run(ctx, prec):
     # an unlimited run is left alone
     n2, _ = ctx.mcradiation(20000, seed=23, precision=prec, maxinteract=100000, maxruntime=1e6)
     assert n2 == 20000
+
+
+def test_single_precision_t4_replays_the_oracle(ctx):
+    """mcg_run.t4_single: the reference's single-precision real(i)**4 in
+    increaseT and determineT (Radiation.f:551, 584, 698); the serial replay
+    and the post-run temperatures equal the oracle's with the same switch,
+    bit for bit, and differ from the FP64 form by under 1e-6"""
+    import oracle_ffi as OF
+    m = models.small_disk(mdust=1e-4)
+    ctx.set_model(m)
+    L = OF.load()
+    L.orc_set_t4_single(1)
+    try:
+        o = O.mcradiation(m, 150, seed=9)
+    finally:
+        L.orc_set_t4_single(0)
+    _, g = ctx.mcradiation(150, seed=9, threads=1, precision="exact", t4_single=True)
+    assert list(o["counters"][:12]) == list(g["counters"][:12])
+    for k in KEYS:
+        assert np.array_equal(o[k], g[k]), k
+    Ts, _, _ = ctx.finalize_t()
+    _, g64 = ctx.mcradiation(150, seed=9, threads=1, precision="exact")
+    T64, _, _ = ctx.finalize_t()
+    ok = (T64 > 1.0) & (Ts > 1.0)
+    rel = np.abs(Ts[ok] / T64[ok] - 1)
+    assert rel.max() < 1e-6 and np.any(Ts[ok] != T64[ok])

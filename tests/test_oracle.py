@@ -129,3 +129,28 @@ def test_ran1_sequence_properties():
     xs = np.array([L.orc_ran1(C.byref(idum), iv, C.byref(iy)) for _ in range(20000)])
     assert np.all((xs > 0) & (xs < 1))
     assert abs(xs.mean() - 0.5) < 0.01 and abs(xs.var() - 1 / 12) < 0.003
+
+
+def test_single_precision_t4_interpolation():
+    """orc_set_t4_single: determineT and increaseT interpolate T^4 between the
+    bracketing steps with the reference's single-precision real(i)**4"""
+    import oracle_ffi as OF
+    L = OF.load()
+    iT = np.arange(0, 10001, dtype=float)
+    kp = np.ascontiguousarray(1e-3 * iT ** 4 + 1e-6 * iT)
+    P = OF.P
+    E1 = 0.37 * kp[1234] + 0.63 * kp[1235]
+    t64 = L.orc_determine_t(P(kp), E1, 100.0)
+    L.orc_set_t4_single(1)
+    try:
+        t32 = L.orc_determine_t(P(kp), E1, 100.0)
+        u32 = L.orc_increase_t(P(kp), E1, 1000.0)
+    finally:
+        L.orc_set_t4_single(0)
+    a = np.float32(1234.0) ** 2
+    a = a * a
+    b = np.float32(1235.0) ** 2
+    b = b * b
+    expect = (float(a) + (float(np.float32(b - a)) * (E1 - kp[1234])) / (kp[1235] - kp[1234])) ** 0.25
+    assert abs(t32 / expect - 1) < 1e-15 and t32 == u32
+    assert t32 != t64 and abs(t32 / t64 - 1) < 1e-7
