@@ -156,23 +156,9 @@ TP_FN void f_randomdirection(px_stream *r, R *x, R *y, R *z) {
   *z *= rr;
 }
 
-/* FE_DIR32 = 1 (a build option for measuring it, off in the library): the
- * mixed form keeps the FP32 direction as rotated, |v| = 1 to FP32 rounding
- * only, where the default renormalises it in FP64 for the intersection
- * quadratics that assume |v| = 1 */
-#ifndef FE_DIR32
-#define FE_DIR32 0
-#endif
-
 template <class R>
 TP_FN void f_set_dir(FPkt<R> &p, R x, R y, R z) {
   const double dx = (double)x, dy = (double)y, dz = (double)z;
-  if (FE_DIR32 && sizeof(R) == 4) {
-    p.vx = dx;
-    p.vy = dy;
-    p.vz = dz;
-    return;
-  }
   const double inv = 1.0 / sqrt(dx * dx + dy * dy + dz * dz);
   p.vx = dx * inv;
   p.vy = dy * inv;
