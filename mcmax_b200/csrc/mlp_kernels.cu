@@ -9,14 +9,17 @@
  * replaces calls of ComputePart's DHS inner loop (ComputePart.f:318-447)
  * inside its training box.
  *
- * Kernels (one CTA = one warpgroup of 128 threads, one tile = 128 samples):
- *   mlp_fwd_kernel     forward pass.  Layer 0 (6 -> 256) on CUDA cores;
- *                      layers 1-3 (256 -> 256) and the output layer
- *                      (256 -> 64) as tcgen05 BF16 MMAs with FP32
- *                      accumulators in tensor memory; bias + SiLU epilogue
- *                      from tensor memory back into the shared A operand.
- *                      Optionally keeps pre-activations (FP32) and
- *                      activations (BF16) for the backward pass.
+ * Kernels (one tile = 128 samples):
+ *   mlp_fwd_kernel     forward pass, two tiles in flight per CTA with warps
+ *                      split into epilogue, MMA-issue and weight-copy roles.
+ *                      Layer 0 (6 -> 256) on CUDA cores; layers 1-3
+ *                      (256 -> 256) and the output layer (256 -> 64) as
+ *                      tcgen05 BF16 MMAs with FP32 accumulators in tensor
+ *                      memory; bias + SiLU epilogue from tensor memory back
+ *                      into the shared A operand.  Optionally keeps
+ *                      pre-activations (FP32) and activations (BF16) for
+ *                      the backward pass.
+ *   (the backward kernels use one warpgroup of 128 threads per CTA)
  *   mlp_dx_kernel      dZ_{l-1} = (dZ_l W_l) * SiLU'(Z_{l-1}), tcgen05 with
  *                      the transposed weights.
  *   mlp_dw_kernel      dW_l += dZ_l^T H_{l-1} over the batch, tcgen05 with
@@ -47,12 +50,11 @@ struct Params {
   const float *W0, *b0;          /* 256 x 6, 256 */
   const float *b123;             /* 3 x 256 */
   const float *b4;               /* OUT */
-  const __nv_bfloat16 *Wc;       /* 3 x canonical (out rows, in cols) */
-  const __nv_bfloat16 *Wtc;      /* 3 x canonical (in rows, out cols) */
-  const __nv_bfloat16 *W4c;      /* canonical OUT rows x 256 */
+  const __nv_bfloat16 *Wc;       /* 3 x 4 chunks of 64 inputs, (out rows, in cols) */
+  const __nv_bfloat16 *Wtc;      /* 3 x K-major (in rows, out cols) */
+  const __nv_bfloat16 *W4c;      /* 4 chunks of 64 inputs, OUT rows */
 };
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
 __device__ __forceinline__ float dsilu(float z) {
   const float s = 1.0f / (1.0f + __expf(-z));
   return s * (1.0f + z * (1.0f - s));
@@ -104,136 +106,284 @@ __device__ __forceinline__ int run_gemm(Tc &tc, uint64_t *mbar, uint32_t a0, uin
 }
 
 /* ------------------------------------------------------------------ forward */
-/* Four warpgroups per CTA: the four warps that share a TMEM lane quarter
- * (rows 32q..32q+31) split the 256 columns of every layer into quarters, so
- * the CUDA-core work (input layer, bias + SiLU epilogues) has 16 warps per
- * SM to hide its latency.  Weights reach shared memory by bulk copy: the
- * copy of the next layer's weights starts as soon as the current MMA has
- * finished reading them and runs while the epilogue works. */
-constexpr int NTF = 512;
+/* SiLU z * sigmoid(z) with one special-function operation: u = 2^(-|z| log2 e)
+ * by ex2.approx, then r = 1 / (1 + u) for 1 + u in (1, 2] by Newton-Raphson
+ * from the linear minimax estimate 24/17 - 8/17 (1 + u), whose relative error
+ * is at most 1/17; two steps bring it below 2e-5, far under the BF16 rounding
+ * of the result.  sigmoid(z) = r for z >= 0 and u r for z < 0. */
+__device__ __forceinline__ float silu_fast(float z) {
+  float u;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(u) : "f"(-1.4426950408889634f * fabsf(z)));
+  const float d = 1.0f + u;
+  float r = fmaf(-0.47058823529411764f, d, 1.4117647058823529f);
+  r = fmaf(r, fmaf(-d, r, 1.0f), r);
+  r = fmaf(r, fmaf(-d, r, 1.0f), r);
+  return z * (z >= 0.0f ? r : u * r);
+}
 
-__global__ void __launch_bounds__(NTF, 1)
+/* Forward pass with two 128-row tiles (slots X = 0, Y = 1) in flight per CTA
+ * and warps split by role:
+ *   warps 0-15  epilogue: the input layer on CUDA cores, the bias + SiLU of
+ *               each hidden layer from tensor memory into the slot's shared A
+ *               operand, the output layer's bias into y.  The four warps of a
+ *               TMEM lane quarter split the columns in four.
+ *   warp 16     issues the MMAs (one lane);
+ *   warp 17     streams the weights by bulk copy (one lane) through a ring of
+ *               three 32 KB slots.
+ * Weights are stored in chunks of 64 input columns (mlp_pack_kernel).  Each
+ * chunk serves the same layer of both tiles: a layer's MMAs alternate X chunk
+ * c, Y chunk c, so the weights cross L2 once per 256 rows.  While the tensor
+ * cores run a layer of one tile, the epilogue warps work on the other.
+ * Barriers: full / empty per weight slot (copy landed / MMAs done reading it);
+ * ready per tile slot (all 512 epilogue threads have written the A operand
+ * and read the accumulator); done per tile slot (MMA commit: the accumulator
+ * holds the layer).  Tensor memory: X accumulates in columns 0-255, Y in
+ * 256-511.  Every wait is bounded and gives up once another role has; the
+ * MMA and copy warps then wait (bounded) for their operations in flight
+ * before the CTA frees tensor memory. */
+constexpr int FW_EPI = 512, FW_NT = FW_EPI + 64, FW_SLOTS = 3, FW_KC = 64;
+constexpr uint32_t FW_CHUNK = H * FW_KC * 2;    /* 32 KB: 256 output rows x 64 inputs */
+constexpr uint32_t FW_CHUNK4 = OUT * FW_KC * 2; /* 8 KB: the output layer's chunk */
+constexpr uint32_t FW_OFF_W = 2 * A_BYTES;      /* A_X | A_Y | weight slots | barriers */
+constexpr uint32_t FW_OFF_BAR = FW_OFF_W + FW_SLOTS * FW_CHUNK;
+constexpr uint32_t FW_NBAR = 2 * FW_SLOTS + 5;  /* full, empty, ready x2, done x2, drain */
+
+/* the input layer of one tile into its A operand: this thread's row, its
+ * quarter of the 256 units */
+__device__ __forceinline__ void fw_input_layer(const Params &P, const float *__restrict__ x, int n, int tile,
+                                               int row, int c0, unsigned char *A, float *__restrict__ zs,
+                                               __nv_bfloat16 *__restrict__ hs) {
+  static_assert(IN == 6, "the vector loads below read six inputs per row");
+  const int g = tile * TILE + row;
+  const bool live = g < n;
+  float xi[IN];
+  {
+    float2 a = make_float2(0.0f, 0.0f), b = a, c = a;
+    if (live) {
+      const float2 *xp = reinterpret_cast<const float2 *>(x + (size_t)g * IN); /* 8-byte aligned rows */
+      a = __ldg(xp);
+      b = __ldg(xp + 1);
+      c = __ldg(xp + 2);
+    }
+    xi[0] = a.x, xi[1] = a.y, xi[2] = b.x, xi[3] = b.y, xi[4] = c.x, xi[5] = c.y;
+  }
+  for (int j0 = c0; j0 < c0 + H / 4; j0 += 8) {
+    /* the 8 units' weights (48 floats) and biases, 16-byte aligned */
+    float w[8 * IN], bj[8];
+    const float4 *wp = reinterpret_cast<const float4 *>(P.W0 + j0 * IN);
+#pragma unroll
+    for (int k = 0; k < 2 * IN; ++k) {
+      const float4 q = __ldg(wp + k);
+      w[4 * k] = q.x, w[4 * k + 1] = q.y, w[4 * k + 2] = q.z, w[4 * k + 3] = q.w;
+    }
+    const float4 *bp = reinterpret_cast<const float4 *>(P.b0 + j0);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const float4 q = __ldg(bp + k);
+      bj[4 * k] = q.x, bj[4 * k + 1] = q.y, bj[4 * k + 2] = q.z, bj[4 * k + 3] = q.w;
+    }
+    float v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      float z = bj[u];
+#pragma unroll
+      for (int i = 0; i < IN; ++i) z = fmaf(w[u * IN + i], xi[i], z);
+      if (zs && live) zs[((size_t)g * 4 + 0) * H + j0 + u] = z;
+      v[u] = silu_fast(z);
+    }
+    store_row8(A, row, j0, v);
+    if (hs && live)
+      *reinterpret_cast<uint4 *>(hs + ((size_t)g * 4 + 0) * H + j0) =
+          *reinterpret_cast<const uint4 *>(A + tc_kmaj_off(row, j0, H));
+  }
+}
+
+/* bias + SiLU of hidden layer l + 1 (the result of tensor-core product l,
+ * l = 0..2) from the accumulator into the A operand */
+__device__ __forceinline__ void fw_hidden(const Params &P, uint32_t acc, int l, int g, bool live, int row, int c0,
+                                          unsigned char *A, float *__restrict__ zs, __nv_bfloat16 *__restrict__ hs) {
+  for (int cc = c0; cc < c0 + H / 4; cc += 32) {
+    float v[32];
+    tc_ld32(acc + (uint32_t)cc, v);
+    const float4 *bias = reinterpret_cast<const float4 *>(P.b123 + l * H + cc); /* 16-byte aligned */
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const float4 q = __ldg(bias + k);
+      v[4 * k] += q.x, v[4 * k + 1] += q.y, v[4 * k + 2] += q.z, v[4 * k + 3] += q.w;
+    }
+#pragma unroll
+    for (int u = 0; u < 32; ++u) {
+      const float z = v[u];
+      if (zs && live) zs[((size_t)g * 4 + l + 1) * H + cc + u] = z;
+      v[u] = silu_fast(z);
+    }
+#pragma unroll
+    for (int k = 0; k < 32; k += 8) {
+      store_row8(A, row, cc + k, v + k);
+      if (hs && live)
+        *reinterpret_cast<uint4 *>(hs + ((size_t)g * 4 + l + 1) * H + cc + k) =
+            *reinterpret_cast<const uint4 *>(A + tc_kmaj_off(row, cc + k, H));
+    }
+  }
+}
+
+__global__ void __launch_bounds__(FW_NT, 1)
     mlp_fwd_kernel(Params P, const float *__restrict__ x, int n, float *__restrict__ y, float *__restrict__ zs,
                    __nv_bfloat16 *__restrict__ hs, int *err) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  unsigned char *A = smem;
-  unsigned char *B = smem + A_BYTES;
-  float *sW0 = reinterpret_cast<float *>(B + B_BYTES);
-  float *sb = sW0 + H * IN;                 /* b0 | b1 | b2 | b3 | b4 */
-  uint64_t *mbar = reinterpret_cast<uint64_t *>(sb + 4 * H + OUT);
-  uint64_t *mbar_w = mbar + 1;
-  uint32_t *slot = reinterpret_cast<uint32_t *>(mbar + 2);
-  const int t = threadIdx.x, warp = t >> 5;
-  const int row = t & (TILE - 1);   /* = 32 * (warp % 4) + lane: this thread's TMEM lane */
-  const int c0 = (t >> 7) * (H / 4); /* this thread's quarter of the columns */
-  for (int i = t; i < H * IN; i += NTF) sW0[i] = P.W0[i];
-  for (int i = t; i < H; i += NTF) sb[i] = P.b0[i];
-  for (int i = t; i < 3 * H; i += NTF) sb[H + i] = P.b123[i];
-  for (int i = t; i < OUT; i += NTF) sb[4 * H + i] = P.b4[i];
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + FW_OFF_BAR);
+  uint64_t *full = bar, *empty = bar + FW_SLOTS, *ready = bar + 2 * FW_SLOTS, *done = ready + 2, *drain = done + 2;
+  uint32_t *slot = reinterpret_cast<uint32_t *>(bar + FW_NBAR);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(slot + 1);
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   if (t == 0) {
-    tc_mbar_init(mbar, 1);
-    tc_mbar_init(mbar_w, 1);
+    for (int i = 0; i < FW_SLOTS; ++i) {
+      tc_mbar_init(full + i, 1);
+      tc_mbar_init(empty + i, 1);
+    }
+    for (int s = 0; s < 2; ++s) {
+      tc_mbar_init(ready + s, FW_EPI);
+      tc_mbar_init(done + s, 1);
+    }
+    tc_mbar_init(drain, 1);
+    *abort_flag = 0;
   }
-  if (warp == 0) tc_alloc(slot, 256);
+  if (warp == 0) tc_alloc(slot, 512);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  Tc tc{*slot, 0u};
-  uint32_t wphase = 0u;
-  int w_in_flight = 0;
-  const uint32_t lane_base = tc.tmem + ((uint32_t)((warp & 3) * 32) << 16);
-  const uint32_t a0 = tc_smem_addr(A), b0 = tc_smem_addr(B);
-  const int ntiles = (n + TILE - 1) / TILE;
+  const uint32_t tmem = *slot;
+  /* tiles per step: two (X, Y) while there are more tiles than CTAs, else
+   * one (X); step p holds tiles per * p + s */
+  const int ntiles = (n + TILE - 1) / TILE, per = ntiles <= (int)gridDim.x ? 1 : 2;
+  const int nsteps = (ntiles + per - 1) / per, stride = (int)gridDim.x;
   int ok = 1;
-  auto issue_w = [&](const __nv_bfloat16 *src, uint32_t bytes) {
-    if (t == 0) tc_bulk_load(B, src, bytes, mbar_w);
-    w_in_flight = 1;
-  };
-  auto wait_w = [&]() {
-    const int w = tc_mbar_wait(mbar_w, wphase);
-    wphase ^= 1u;
-    w_in_flight = 0;
-    return __syncthreads_and(w);
-  };
-  if ((int)blockIdx.x < ntiles) issue_w(P.Wc, B_BYTES);
-  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-    const int g = tile * TILE + row;
-    const bool live = g < n;
-    /* layer 0 on CUDA cores: this thread's row, its quarter of the units */
-    float xi[IN];
-#pragma unroll
-    for (int i = 0; i < IN; ++i) xi[i] = live ? x[(size_t)g * IN + i] : 0.0f;
-    for (int j0 = c0; j0 < c0 + H / 4; j0 += 8) {
-      float v[8];
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        float z = sb[j0 + u];
-#pragma unroll
-        for (int i = 0; i < IN; ++i) z = fmaf(sW0[(j0 + u) * IN + i], xi[i], z);
-        if (zs && live) zs[((size_t)g * 4 + 0) * H + j0 + u] = z;
-        v[u] = silu(z);
-      }
-      store_row8(A, row, j0, v);
-      if (hs && live) {
-        uint4 q = *reinterpret_cast<uint4 *>(A + tc_kmaj_off(row, j0, H));
-        *reinterpret_cast<uint4 *>(hs + ((size_t)g * 4 + 0) * H + j0) = q;
+  if (warp < FW_EPI / 32) {
+    /* epilogue warps: thread = TMEM lane (row) x quarter of the columns */
+    const int row = t & (TILE - 1), c0 = (t >> 7) * (H / 4);
+    const uint32_t lanes = (uint32_t)((warp & 3) * 32) << 16;
+    uint32_t dphase = 0u; /* bit s: parity of slot s's next done phase */
+    int p = blockIdx.x;
+    if (p < nsteps) {
+      for (int s = 0; s < per; ++s) {
+        fw_input_layer(P, x, n, per * p + s, row, c0, smem + s * A_BYTES, zs, hs);
+        tc_fence_async_smem();
+        tc_mbar_arrive(ready + s);
       }
     }
-    /* layers 1..3 on the tensor cores */
-    for (int l = 0; l < 3 && ok; ++l) {
-      ok = wait_w();
-      if (!ok) break;
-      ok = run_gemm(tc, mbar, a0, b0, H, H);
-      if (!ok) break;
-      if (l < 2)
-        issue_w(P.Wc + (size_t)(l + 1) * H * H, B_BYTES);
-      else
-        issue_w(P.W4c, OUT * H * 2);
-      for (int c = c0; c < c0 + H / 4; c += 16) {
-        float v[16];
-        tc_ld16(lane_base + (uint32_t)c, v);
+    for (; p < nsteps && ok; p += stride) {
+      for (int L = 0; L < 4 && ok; ++L) {
+        for (int s = 0; s < per; ++s) {
+          ok = __all_sync(0xffffffffu, tc_mbar_wait_or_abort(done + s, (dphase >> s) & 1u, abort_flag));
+          dphase ^= 1u << s;
+          if (!ok) break;
+          tc_fence_after();
+          const uint32_t acc = tmem + lanes + 256u * (uint32_t)s;
+          unsigned char *A = smem + s * A_BYTES;
+          const int g = (per * p + s) * TILE + row;
+          const bool live = g < n;
+          if (L < 3) {
+            fw_hidden(P, acc, L, g, live, row, c0, A, zs, hs);
+          } else {
+            /* output layer: 64 columns, 16 per column quarter */
+            const int c = (t >> 7) * 16;
+            float v[16];
+            tc_ld16(acc + (uint32_t)c, v);
+            if (live) {
+              const float4 *bias = reinterpret_cast<const float4 *>(P.b4 + c);
+              float4 *yo = reinterpret_cast<float4 *>(y + (size_t)g * OUT + c);
 #pragma unroll
-        for (int u = 0; u < 16; ++u) {
-          const float z = v[u] + sb[H * (l + 1) + c + u];
-          if (zs && live) zs[((size_t)g * 4 + l + 1) * H + c + u] = z;
-          v[u] = silu(z);
-        }
-        store_row8(A, row, c, v);
-        store_row8(A, row, c + 8, v + 8);
-        if (hs && live) {
-          *reinterpret_cast<uint4 *>(hs + ((size_t)g * 4 + l + 1) * H + c) =
-              *reinterpret_cast<uint4 *>(A + tc_kmaj_off(row, c, H));
-          *reinterpret_cast<uint4 *>(hs + ((size_t)g * 4 + l + 1) * H + c + 8) =
-              *reinterpret_cast<uint4 *>(A + tc_kmaj_off(row, c + 8, H));
+              for (int k = 0; k < 4; ++k) {
+                const float4 q = __ldg(bias + k);
+                yo[k] = make_float4(v[4 * k] + q.x, v[4 * k + 1] + q.y, v[4 * k + 2] + q.z, v[4 * k + 3] + q.w);
+              }
+            }
+            if (p + stride >= nsteps) continue; /* no further product on this slot */
+            /* the slot's A operand is free: the next step's input layer */
+            fw_input_layer(P, x, n, per * (p + stride) + s, row, c0, A, zs, hs);
+          }
+          tc_fence_async_smem();
+          tc_fence_before();
+          tc_mbar_arrive(ready + s);
         }
       }
-      tc_fence_before();
     }
-    if (!ok) break;
-    /* output layer: N = OUT = 64, 16 columns per warpgroup */
-    ok = wait_w();
-    if (!ok) break;
-    ok = run_gemm(tc, mbar, a0, b0, OUT, H);
-    if (!ok) break;
-    if (tile + (int)gridDim.x < ntiles) issue_w(P.Wc, B_BYTES);
-    if (t < (OUT / 16) * TILE) {
-      const int c = (t >> 7) * 16;
-      float v[16];
-      tc_ld16(lane_base + (uint32_t)c, v);
-      if (live) {
+  } else if (warp == FW_EPI / 32) {
+    /* MMA warp: per step, layers L = 0..3 (three hidden products and the
+     * output), per layer four weight chunks, each for X then Y */
+    uint32_t rphase = 0u; /* bit s: parity of slot s's next ready phase */
+    int q = 0;
+    for (int p = blockIdx.x; p < nsteps && ok; p += stride) {
+      for (int L = 0; L < 4 && ok; ++L) {
+        const uint32_t idesc = tc_idesc_bf16(TILE, L < 3 ? H : OUT);
+        for (int c = 0; c < 4 && ok; ++c, ++q) {
+          const int ws = q % FW_SLOTS;
+          ok = __all_sync(0xffffffffu,
+                          tc_mbar_wait_or_abort(full + ws, (uint32_t)(q / FW_SLOTS) & 1u, abort_flag));
+          if (!ok) break;
+          const uint32_t b = tc_smem_addr(smem + FW_OFF_W + ws * FW_CHUNK);
+          for (int s = 0; s < per; ++s) {
+            if (c == 0) {
+              ok = __all_sync(0xffffffffu, tc_mbar_wait_or_abort(ready + s, (rphase >> s) & 1u, abort_flag));
+              rphase ^= 1u << s;
+              if (!ok) break;
+            }
+            tc_fence_after();
+            if (lane == 0) {
+              const uint32_t a = tc_smem_addr(smem + s * A_BYTES);
 #pragma unroll
-        for (int u = 0; u < 16; ++u) y[(size_t)g * OUT + c + u] = v[u] + sb[4 * H + c + u];
+              for (int j = 0; j < FW_KC / 16; ++j) {
+                const uint64_t ad = tc_desc(a + 256u * (uint32_t)(4 * c + j), 128u, (uint32_t)H * 16u);
+                const uint64_t bd = tc_desc(b + 256u * (uint32_t)j, 128u, (uint32_t)FW_KC * 16u);
+                tc_mma(tmem + 256u * (uint32_t)s, ad, bd, idesc, (c > 0 || j > 0) ? 1u : 0u);
+              }
+              if (c == 3) tc_commit(done + s);
+            }
+            __syncwarp();
+          }
+          if (!ok) break;
+          if (lane == 0) tc_commit(empty + ws);
+          __syncwarp();
+        }
       }
     }
-    tc_fence_before();
+    /* every MMA issued here completes before tensor memory is freed */
+    if (lane == 0) tc_commit(drain);
+    __syncwarp();
+    (void)tc_mbar_wait(drain, 0u);
+  } else {
+    /* weight stream: 16 chunks per step, chunk q = (layer (q / 4) % 4,
+     * columns 64 (q % 4) ..), slot q % 3 */
+    const int mine = (int)blockIdx.x < nsteps ? (nsteps - 1 - (int)blockIdx.x) / stride + 1 : 0;
+    int issued = 0; /* chunk q goes to slot q % 3 as its (q / 3)-th fill */
+    for (int q = 0; q < 16 * mine && ok; ++q) {
+      const int ws = q % FW_SLOTS, u = q / FW_SLOTS;
+      if (u > 0) {
+        ok = __all_sync(0xffffffffu, tc_mbar_wait_or_abort(empty + ws, (uint32_t)(u - 1) & 1u, abort_flag));
+        if (!ok) break;
+      }
+      const int L = (q >> 2) & 3, c = q & 3;
+      const unsigned char *src = L < 3 ? reinterpret_cast<const unsigned char *>(P.Wc) + (size_t)(L * 4 + c) * FW_CHUNK
+                                       : reinterpret_cast<const unsigned char *>(P.W4c) + (size_t)c * FW_CHUNK4;
+      if (lane == 0) tc_bulk_load(smem + FW_OFF_W + ws * FW_CHUNK, src, L < 3 ? FW_CHUNK : FW_CHUNK4, full + ws);
+      __syncwarp();
+      issued = q + 1;
+    }
+    /* every copy issued here lands before the CTA leaves: the last fill of
+     * each slot */
+    for (int ws = 0; ws < FW_SLOTS && ws < issued; ++ws) {
+      const int last = ws + FW_SLOTS * ((issued - 1 - ws) / FW_SLOTS);
+      (void)tc_mbar_wait(full + ws, (uint32_t)(last / FW_SLOTS) & 1u);
+    }
   }
-  if (!ok && t == 0) atomicExch(err, 1);
-  /* nothing may still write shared or tensor memory when the CTA leaves */
-  if (w_in_flight) (void)tc_mbar_wait(mbar_w, wphase);
-  if (!ok) (void)tc_mbar_wait(mbar, tc.phase ^ 1u);
+  if (!ok) {
+    *abort_flag = 1;
+    if (lane == 0) atomicExch(err, 1);
+  }
+  tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  if (warp == 0) tc_dealloc(tc.tmem, 256);
+  if (warp == 0) tc_dealloc(tmem, 512);
 }
 
 /* ---------------------------------------------------------------- backward */
@@ -476,7 +626,10 @@ __global__ void mlp_adam_kernel(float *__restrict__ p, const float *__restrict__
 }
 
 /* BF16 K-major copies of the tensor-core weights from the FP32 masters:
- * Wc[l] (out rows, in cols), Wtc[l] (in rows, out cols), W4c (OUT x 256) */
+ * Wc[l] (out rows, in cols) and W4c (OUT x 256) for the forward pass, in
+ * chunks of 64 input columns, each chunk a K-major tile of its own (chunk
+ * (l, c) at (4 l + c) x 32 KB); Wtc[l] (in rows, out cols), one 256-column
+ * K-major tile per layer, for the backward pass */
 __global__ void mlp_pack_kernel(const float *__restrict__ W123, const float *__restrict__ W4,
                                 __nv_bfloat16 *__restrict__ Wc, __nv_bfloat16 *__restrict__ Wtc,
                                 __nv_bfloat16 *__restrict__ W4c) {
@@ -484,14 +637,14 @@ __global__ void mlp_pack_kernel(const float *__restrict__ W123, const float *__r
   if (i < 3 * H * H) {
     const int l = i / (H * H), r = (i / H) % H, c = i % H; /* W[l][r = out][c = in] */
     const __nv_bfloat16 v = __float2bfloat16_rn(W123[i]);
-    unsigned char *wc = reinterpret_cast<unsigned char *>(Wc + (size_t)l * H * H);
+    unsigned char *wc = reinterpret_cast<unsigned char *>(Wc) + (size_t)(l * 4 + c / FW_KC) * FW_CHUNK;
     unsigned char *wt = reinterpret_cast<unsigned char *>(Wtc + (size_t)l * H * H);
-    *reinterpret_cast<__nv_bfloat16 *>(wc + tc_kmaj_off(r, c, H)) = v;
+    *reinterpret_cast<__nv_bfloat16 *>(wc + tc_kmaj_off(r, c % FW_KC, FW_KC)) = v;
     *reinterpret_cast<__nv_bfloat16 *>(wt + tc_kmaj_off(c, r, H)) = v;
   } else if (i < 3 * H * H + OUT * H) {
     const int j = i - 3 * H * H, r = j / H, c = j % H;
-    unsigned char *w4 = reinterpret_cast<unsigned char *>(W4c);
-    *reinterpret_cast<__nv_bfloat16 *>(w4 + tc_kmaj_off(r, c, H)) = __float2bfloat16_rn(W4[j]);
+    unsigned char *w4 = reinterpret_cast<unsigned char *>(W4c) + (size_t)(c / FW_KC) * FW_CHUNK4;
+    *reinterpret_cast<__nv_bfloat16 *>(w4 + tc_kmaj_off(r, c % FW_KC, FW_KC)) = __float2bfloat16_rn(W4[j]);
   }
 }
 
@@ -559,7 +712,7 @@ constexpr int64_t OFF_W0 = 0, OFF_B0 = OFF_W0 + H * IN, OFF_W123 = OFF_B0 + H, O
                   OFF_W4 = OFF_B123 + 3 * H, OFF_B4 = OFF_W4 + OUT * H, NPARAMS = OFF_B4 + OUT;
 static_assert(NPARAMS == MCG_MLP_NPARAMS, "parameter count");
 
-constexpr size_t SMEM_FWD = A_BYTES + B_BYTES + (H * IN + 4 * H + OUT) * 4 + 24;
+constexpr size_t SMEM_FWD = FW_OFF_BAR + FW_NBAR * 8 + 8;
 constexpr size_t SMEM_DX = A_BYTES + B_BYTES + 16;
 constexpr size_t SMEM_DW = 4 * 128 * 128 * 2 + 16;
 constexpr size_t SMEM_CHECK = A_BYTES + B_BYTES + 16;
@@ -667,12 +820,21 @@ int grid_tiles(mcg_ctx *ctx, int64_t n) {
   return std::max(1, std::min(tiles, ctx->sm_count > 0 ? ctx->sm_count : 148));
 }
 
+/* the forward kernel: one tile per CTA while the tiles fit on the SMs, else
+ * pairs of tiles (the kernel takes two per step when tiles > CTAs) */
+int grid_fwd(mcg_ctx *ctx, int64_t n) {
+  const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;
+  const int tiles = (int)((n + TILE - 1) / TILE);
+  if (tiles <= sms) return std::max(1, tiles);
+  return std::min((tiles + 1) / 2, sms);
+}
+
 /* forward of rows already in s.xb; zs/hs kept when `keep` */
 void mlp_fwd_launch(mcg_ctx *ctx, int64_t n, bool keep) {
   MlpState &s = *ctx->mlp;
-  mlp_fwd_kernel<<<grid_tiles(ctx, n), NTF, SMEM_FWD, ctx->stream>>>(mlp_params(s), s.xb, (int)n, s.yb,
-                                                                     keep ? s.zs : nullptr,
-                                                                     keep ? s.hs : nullptr, s.err);
+  mlp_fwd_kernel<<<grid_fwd(ctx, n), FW_NT, SMEM_FWD, ctx->stream>>>(mlp_params(s), s.xb, (int)n, s.yb,
+                                                                       keep ? s.zs : nullptr,
+                                                                       keep ? s.hs : nullptr, s.err);
 }
 
 /* loss and gradient of the batch in s.xb / s.tb into s.G (zeroed here) */

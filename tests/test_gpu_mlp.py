@@ -20,10 +20,13 @@ def test_tensor_core_product_layout(ctx, N):
     assert np.max(np.abs(d - ref)) < 1e-4 * np.max(np.abs(ref)), np.max(np.abs(d - ref))
 
 
-def test_forward_matches_reference(ctx):
+# 1000 rows: one tile per CTA; 40063 rows: 313 tiles, two per CTA step,
+# the last step with a second tile past the end
+@pytest.mark.parametrize("n", [1000, 40063])
+def test_forward_matches_reference(ctx, n):
     rng = np.random.default_rng(1)
     p = R.init(seed=2)
-    x = rng.uniform(-1, 1, (1000, R.IN)).astype(np.float32)
+    x = rng.uniform(-1, 1, (n, R.IN)).astype(np.float32)
     ctx.mlp_set_params(p)
     y = ctx.mlp_forward(x)
     ref, _, _ = R.forward(p, x)
@@ -34,11 +37,12 @@ def test_forward_matches_reference(ctx):
     assert np.mean(np.abs(y - ref)) < 1e-3 * scale
 
 
-def test_gradient_matches_reference(ctx):
+@pytest.mark.parametrize("n", [2000, 40063])
+def test_gradient_matches_reference(ctx, n):
     rng = np.random.default_rng(7)
     p = R.init(seed=4)
-    x = rng.uniform(-1, 1, (2000, R.IN)).astype(np.float32)
-    t = rng.normal(0, 1, (2000, R.OUT)).astype(np.float32)
+    x = rng.uniform(-1, 1, (n, R.IN)).astype(np.float32)
+    t = rng.normal(0, 1, (n, R.OUT)).astype(np.float32)
     w = rng.uniform(0.5, 1.5, R.OUT).astype(np.float32)
     ctx.mlp_set_params(p)
     g, loss = ctx.mlp_gradient(x, t, w)
