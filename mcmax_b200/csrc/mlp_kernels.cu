@@ -149,7 +149,8 @@ constexpr uint32_t FW_OFF_BAR = FW_OFF_W + FW_SLOTS * FW_CHUNK;
 constexpr uint32_t FW_NBAR = 2 * FW_SLOTS + 5;  /* full, empty, ready x2, done x2, drain */
 
 /* the input layer of one tile into its A operand: this thread's row, its
- * quarter of the 256 units */
+ * quarter of the 256 units; KEEP also writes zs and hs */
+template <bool KEEP>
 __device__ __forceinline__ void fw_input_layer(const Params &P, const float *__restrict__ x, int n, int tile,
                                                int row, int c0, unsigned char *A, float *__restrict__ zs,
                                                __nv_bfloat16 *__restrict__ hs) {
@@ -188,11 +189,11 @@ __device__ __forceinline__ void fw_input_layer(const Params &P, const float *__r
       float z = bj[u];
 #pragma unroll
       for (int i = 0; i < IN; ++i) z = fmaf(w[u * IN + i], xi[i], z);
-      if (zs && live) zs[((size_t)g * 4 + 0) * H + j0 + u] = z;
+      if (KEEP && live) zs[((size_t)g * 4 + 0) * H + j0 + u] = z;
       v[u] = silu_fast(z);
     }
     store_row8(A, row, j0, v);
-    if (hs && live)
+    if (KEEP && live)
       *reinterpret_cast<uint4 *>(hs + ((size_t)g * 4 + 0) * H + j0) =
           *reinterpret_cast<const uint4 *>(A + tc_kmaj_off(row, j0, H));
   }
@@ -200,6 +201,7 @@ __device__ __forceinline__ void fw_input_layer(const Params &P, const float *__r
 
 /* bias + SiLU of hidden layer l + 1 (the result of tensor-core product l,
  * l = 0..2) from the accumulator into the A operand */
+template <bool KEEP>
 __device__ __forceinline__ void fw_hidden(const Params &P, uint32_t acc, int l, int g, bool live, int row, int c0,
                                           unsigned char *A, float *__restrict__ zs, __nv_bfloat16 *__restrict__ hs) {
   for (int cc = c0; cc < c0 + H / 4; cc += 32) {
@@ -214,19 +216,21 @@ __device__ __forceinline__ void fw_hidden(const Params &P, uint32_t acc, int l, 
 #pragma unroll
     for (int u = 0; u < 32; ++u) {
       const float z = v[u];
-      if (zs && live) zs[((size_t)g * 4 + l + 1) * H + cc + u] = z;
+      if (KEEP && live) zs[((size_t)g * 4 + l + 1) * H + cc + u] = z;
       v[u] = silu_fast(z);
     }
 #pragma unroll
     for (int k = 0; k < 32; k += 8) {
       store_row8(A, row, cc + k, v + k);
-      if (hs && live)
+      if (KEEP && live)
         *reinterpret_cast<uint4 *>(hs + ((size_t)g * 4 + l + 1) * H + cc + k) =
             *reinterpret_cast<const uint4 *>(A + tc_kmaj_off(row, cc + k, H));
     }
   }
 }
 
+/* KEEP: also write the pre-activations zs and activations hs (training) */
+template <bool KEEP>
 __global__ void __launch_bounds__(FW_NT, 1)
     mlp_fwd_kernel(Params P, const float *__restrict__ x, int n, float *__restrict__ y, float *__restrict__ zs,
                    __nv_bfloat16 *__restrict__ hs, int *err) {
@@ -266,7 +270,7 @@ __global__ void __launch_bounds__(FW_NT, 1)
     int p = blockIdx.x;
     if (p < nsteps) {
       for (int s = 0; s < per; ++s) {
-        fw_input_layer(P, x, n, per * p + s, row, c0, smem + s * A_BYTES, zs, hs);
+        fw_input_layer<KEEP>(P, x, n, per * p + s, row, c0, smem + s * A_BYTES, zs, hs);
         tc_fence_async_smem();
         tc_mbar_arrive(ready + s);
       }
@@ -283,7 +287,7 @@ __global__ void __launch_bounds__(FW_NT, 1)
           const int g = (per * p + s) * TILE + row;
           const bool live = g < n;
           if (L < 3) {
-            fw_hidden(P, acc, L, g, live, row, c0, A, zs, hs);
+            fw_hidden<KEEP>(P, acc, L, g, live, row, c0, A, zs, hs);
           } else {
             /* output layer: 64 columns, 16 per column quarter */
             const int c = (t >> 7) * 16;
@@ -300,7 +304,7 @@ __global__ void __launch_bounds__(FW_NT, 1)
             }
             if (p + stride >= nsteps) continue; /* no further product on this slot */
             /* the slot's A operand is free: the next step's input layer */
-            fw_input_layer(P, x, n, per * (p + stride) + s, row, c0, A, zs, hs);
+            fw_input_layer<KEEP>(P, x, n, per * (p + stride) + s, row, c0, A, zs, hs);
           }
           tc_fence_async_smem();
           tc_fence_before();
@@ -760,7 +764,10 @@ mcg_status mlp_init(mcg_ctx *ctx) {
   if (e == cudaSuccess) e = dalloc(*s, &s->loss, 1);
   if (e == cudaSuccess) e = dalloc(*s, &s->wout, OUT);
   if (e != cudaSuccess) return mcg_fail(ctx, MCG_ERR_NOMEM, "mlp: cudaMalloc failed: %s", cudaGetErrorString(e));
-  MCG_CUDA(ctx, cudaFuncSetAttribute(mlp_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_FWD));
+  MCG_CUDA(ctx, cudaFuncSetAttribute(mlp_fwd_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)SMEM_FWD));
+  MCG_CUDA(ctx, cudaFuncSetAttribute(mlp_fwd_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)SMEM_FWD));
   MCG_CUDA(ctx, cudaFuncSetAttribute(mlp_dx_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_DX));
   MCG_CUDA(ctx, cudaFuncSetAttribute(mlp_dw_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_DW));
   MCG_CUDA(ctx, cudaFuncSetAttribute(mlp_gemm_check_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -832,9 +839,12 @@ int grid_fwd(mcg_ctx *ctx, int64_t n) {
 /* forward of rows already in s.xb; zs/hs kept when `keep` */
 void mlp_fwd_launch(mcg_ctx *ctx, int64_t n, bool keep) {
   MlpState &s = *ctx->mlp;
-  mlp_fwd_kernel<<<grid_fwd(ctx, n), FW_NT, SMEM_FWD, ctx->stream>>>(mlp_params(s), s.xb, (int)n, s.yb,
-                                                                       keep ? s.zs : nullptr,
-                                                                       keep ? s.hs : nullptr, s.err);
+  if (keep)
+    mlp_fwd_kernel<true><<<grid_fwd(ctx, n), FW_NT, SMEM_FWD, ctx->stream>>>(mlp_params(s), s.xb, (int)n, s.yb,
+                                                                             s.zs, s.hs, s.err);
+  else
+    mlp_fwd_kernel<false><<<grid_fwd(ctx, n), FW_NT, SMEM_FWD, ctx->stream>>>(mlp_params(s), s.xb, (int)n, s.yb,
+                                                                              nullptr, nullptr, s.err);
 }
 
 /* loss and gradient of the batch in s.xb / s.tb into s.G (zeroed here) */
