@@ -800,13 +800,15 @@ def learned_disk_model(ctx, *, opacity="dhs", params=None, tstar=10000.0, rstar=
                        mdust=1e-3, sh=0.05 * math.sqrt(2.0), rsh=1.0, shpow=1.125, denspow=1.0, nrad=200,
                        ntheta=120, lam1=0.1, lam2=3000.0, nlam=200, ngrains=50, amin=0.01, amax=1000.0, apow=3.5,
                        ns=5, nf=20, rho=3.0, alpha=1e-3, scat_how=2, compositions=LEARNED_COMPOSITIONS,
-                       settle=True):
+                       settle=True, correct_stride=10):
     """The learned-opacities deck: three compositions in ngrains log bins
     each, equal mass per composition and MRN within it, vertically settled
     with alpha (FixedMPSettling; settle=False leaves the zone's unsettled
     profile, for a structure loop that settles the grains itself),
-    opacities from the DHS kernels (opacity='dhs') or from the surrogate
-    network (opacity='surrogate').  The model carries each grain bin's
+    opacities from the DHS kernels (opacity='dhs'), from the surrogate
+    network (opacity='surrogate'), or from the network corrected by the DHS
+    kernels at every correct_stride-th wavelength (opacity='corrected',
+    surrogate.compute_part_corrected).  The model carries each grain bin's
     density (rho_grain, g/cm^3) and size (rv, cm) for the settling.
     Returns (model, opacity-stage seconds, bins served by the network)."""
     import time
@@ -827,8 +829,12 @@ def learned_disk_model(ctx, *, opacity="dhs", params=None, tstar=10000.0, rstar=
         from . import surrogate as S
         res, used = S.compute_part_surrogate(ctx, parts, params)
         served = int(used.sum())
+    elif opacity == "corrected":
+        from . import surrogate as S
+        res, used, _ = S.compute_part_corrected(ctx, parts, params, stride=correct_stride)
+        served = int(used.sum())
     else:
-        raise ValueError("opacity must be 'dhs' or 'surrogate'")
+        raise ValueError("opacity must be 'dhs', 'surrogate' or 'corrected'")
     t_opac = time.perf_counter() - t0
     Kabs = np.array([r["kabs"] for r in res])
     Ksca = np.array([r["ksca"] for r in res])

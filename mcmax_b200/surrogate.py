@@ -157,3 +157,58 @@ def compute_part_surrogate(ctx, parts, params=None, rho_train=RHO_TRAIN, nf_trai
         o.update(rho_av=outs[k].rho_av, mscale=outs[k].mscale, rscale=outs[k].rscale, n_dhs=outs[k].n_dhs,
                  n_mie=outs[k].n_mie, n_dhs_fail=outs[k].n_dhs_fail)
     return res, used
+
+
+def correction_wavelengths(nlam, stride):
+    """indices of the wavelengths ComputePart evaluates for the correction:
+    every stride-th and the last"""
+    return np.unique(np.r_[np.arange(0, nlam, max(1, int(stride))), nlam - 1])
+
+
+def correct_with_exact(res, used, parts, exact, idx):
+    """Scale the network's kappa_abs and kappa_sca of every bin it served by
+    the ratio ComputePart / network at the wavelengths idx, the log10 ratio
+    interpolated linearly in log10 lambda between them (constant beyond the
+    ends); kappa_ext becomes their sum.  `exact` holds ComputePart's results
+    at parts' wavelengths idx, one per served bin in order.  The Mueller
+    matrix stays the network's.  A key whose values are not all positive
+    keeps the network's values."""
+    served = [k for k in range(len(parts)) if used[k]]
+    if len(exact) != len(served):
+        raise ValueError("one exact result per bin served by the network")
+    for k, e in zip(served, exact):
+        o = res[k]
+        ll = np.log10(np.asarray(parts[k]["lam"], np.float64))
+        for key in ("kabs", "ksca"):
+            net = np.asarray(o[key], np.float64)
+            ex = np.asarray(e[key], np.float64)
+            if np.all(net[idx] > 0) and np.all(ex > 0):
+                o[key] = net * 10.0 ** np.interp(ll, ll[idx], np.log10(ex) - np.log10(net[idx]))
+        o["kext"] = np.asarray(o["kabs"]) + np.asarray(o["ksca"])
+    return res
+
+
+def compute_part_corrected(ctx, parts, params=None, stride=10, rho_train=RHO_TRAIN, nf_train=NF_TRAIN):
+    """compute_part_surrogate, then ComputePart itself (the DHS kernels) at
+    every stride-th wavelength of the bins the network served, which
+    corrects the network's kappa_abs and kappa_sca (correct_with_exact).
+    Every bin's wavelengths are evaluated independently by ComputePart, so
+    the subset gives the same values as the full grid there.  Returns
+    (results, used, wavelengths evaluated per served bin)."""
+    res, used = compute_part_surrogate(ctx, parts, params, rho_train, nf_train)
+    served = [k for k in range(len(parts)) if used[k]]
+    if not served:
+        return res, used, 0
+    idx = correction_wavelengths(np.asarray(parts[served[0]]["lam"]).size, stride)
+    sub = []
+    for k in served:
+        p = parts[k]
+        if np.asarray(p["lam"]).size != np.asarray(parts[served[0]]["lam"]).size:
+            raise ValueError("the bins served by the network must share one wavelength count")
+        q = dict(p)
+        q["lam"] = np.asarray(p["lam"], np.float64)[idx]
+        q["e1"] = np.atleast_2d(p["e1"])[:, idx]
+        q["e2"] = np.atleast_2d(p["e2"])[:, idx]
+        sub.append(q)
+    exact = ctx.compute_part_batch(sub)
+    return correct_with_exact(res, used, parts, exact, idx), used, int(idx.size)
