@@ -540,11 +540,15 @@ mcg_status mcg_surrogate_targets(mcg_ctx *ctx, int64_t n, const double *in6, dou
  * inside the training box; the others go through mcg_compute_part_batch
  * (the DHS/Mie kernels).  used[p] (may be NULL) = 1 when the network served
  * bin p.  Opacities are mass-weighted over the bin's sizes and scaled by
- * rho_train / rho (kappa ~ 1 / material density); the Mueller matrix is
- * rebuilt on the 180 bins from the scattering-weighted moments (F22 = F11,
- * F44 = F33 as for spheres; F33 and F34 scaled back where a prediction
- * breaks F12^2 + F33^2 + F34^2 <= F11^2) and normalised as ComputePart
- * normalises F11 (ComputePart.f:407-415). */
+ * rho_train / rho (kappa ~ 1 / material density).  The Mueller matrix is
+ * rebuilt on the 180 bins from the scattering-weighted moments in the
+ * delta-M form (Wiscombe 1977): a forward fraction f = chi_12^2 / chi_11
+ * (at most chi_12 and 0.99) goes into the first bin of F11 and F33, and the
+ * rest comes from the series of (chi_l - f) / (1 - f), which keeps the
+ * asymmetry parameter of forward-peaked grains.  F22 = F11 and F44 = F33 as
+ * for spheres; F33 and F34 are scaled back where a prediction breaks
+ * F12^2 + F33^2 + F34^2 <= F11^2.  F11 is normalised as ComputePart
+ * normalises it (ComputePart.f:407-415). */
 mcg_status mcg_compute_part_surrogate(mcg_ctx *ctx, int nparts, const mcg_part_in *in, mcg_part_out *out,
                                       double rho_train, int nf_train, int *used);
 

@@ -31,7 +31,7 @@ UNITS = {
 }
 HEADERS = ["detmath.h", "cplx.h", "philox.h", "dhs_core.cuh", "transport_core.cuh", "transport_fast.cuh",
            "mcg_internal.h", "tc_sm100.cuh", "diffuse_core.cuh", "transport_event.cuh",
-           "dstruct_core.cuh", "rt_core.cuh", "scat_core.cuh", "scatfield.h"]
+           "dstruct_core.cuh", "rt_core.cuh", "scat_core.cuh", "scatfield.h", "surrogate_phase.h"]
 
 
 def _nvcc():

@@ -707,6 +707,7 @@ __global__ void __launch_bounds__(NT, 1)
 #include <vector>
 
 #include "mcg_internal.h"
+#include "surrogate_phase.h"
 
 namespace {
 
@@ -1093,6 +1094,7 @@ namespace {
 
 constexpr int SURR_NMOM = 12; /* Legendre moments per Mueller element */
 constexpr int NA = 180;       /* scattering-angle bins (ComputePart.f:41) */
+static_assert(SURR_NMOM == SURR_PH_L && NA == SURR_PH_NA, "surrogate_phase.h works on the same moments and bins");
 
 /* training box of the network inputs: log10 a [micron], log10 lambda
  * [micron], n, log10 k, porosity, fmax */
@@ -1182,16 +1184,7 @@ extern "C" mcg_status mcg_compute_part_surrogate(mcg_ctx *ctx, int nparts, const
   if (rows > 0) {
     std::vector<float> Y((size_t)rows * OUT);
     if ((st = mcg_mlp_forward(ctx, rows, X.data(), Y.data())) != MCG_OK) return st;
-    double P[SURR_NMOM + 1][NA], sinw[NA], tot2 = 0.0;
-    for (int j = 0; j < NA; ++j) {
-      const double th = 3.14159265358979323846 * ((double)j + 0.5) / (double)NA;
-      const double mu = cos(th);
-      sinw[j] = sin(th);
-      tot2 += sinw[j];
-      P[0][j] = 1.0;
-      P[1][j] = mu;
-      for (int l = 1; l < SURR_NMOM; ++l) P[l + 1][j] = ((2.0 * l + 1.0) * mu * P[l][j] - (double)l * P[l - 1][j]) / (l + 1);
-    }
+    static const SurrLegendre legendre; /* Legendre table of the 180 angle bins */
     for (int p = 0; p < nparts; ++p) {
       if (used && !used[p]) continue;
       if (!used && std::find(fallback.begin(), fallback.end(), p) != fallback.end()) continue;
@@ -1224,45 +1217,8 @@ extern "C" mcg_status mcg_compute_part_surrogate(mcg_ctx *ctx, int nparts, const
         out[p].kabs[l] = ka;
         out[p].ksca[l] = ks;
         out[p].kext[l] = ka + ks;
-        /* phase matrix on the 180 bins from the moments */
-        double f11[NA], f12[NA], f33[NA], f34[NA], norm = 0.0;
-        for (int j = 0; j < NA; ++j) {
-          double a = 0.0, b = 0.0, g = 0.0, d = 0.0;
-          for (int m = 0; m <= SURR_NMOM; ++m) {
-            a += (2.0 * m + 1.0) * chi[m] * P[m][j];
-            b += (2.0 * m + 1.0) * beta[m] * P[m][j];
-            g += (2.0 * m + 1.0) * gam[m] * P[m][j];
-            d += (2.0 * m + 1.0) * del[m] * P[m][j];
-          }
-          f11[j] = a > 0.0 ? a : 0.0;
-          f12[j] = b;
-          f33[j] = g;
-          f34[j] = d;
-          norm += f11[j] * sinw[j];
-        }
-        const double c = norm > 0.0 ? tot2 / norm : 1.0;
-        double *F = out[p].F + (size_t)l * 6 * NA;
-        for (int j = 0; j < NA; ++j) {
-          const double a = f11[j] * c;
-          double b = f12[j] * c;
-          if (b > a) b = a;
-          if (b < -a) b = -a;
-          /* spheres: F22 = F11, F44 = F33, and F12^2 + F33^2 + F34^2 <= F11^2
-           * for any mixture of them; a prediction outside is scaled back */
-          double g = f33[j] * c, d = f34[j] * c;
-          const double room = a * a - b * b, gd = g * g + d * d;
-          if (gd > room) {
-            const double f = gd > 0.0 ? sqrt(room / gd) : 0.0;
-            g *= f;
-            d *= f;
-          }
-          F[0 * NA + j] = a;
-          F[1 * NA + j] = b;
-          F[2 * NA + j] = a;
-          F[3 * NA + j] = g;
-          F[4 * NA + j] = d;
-          F[5 * NA + j] = g;
-        }
+        /* phase matrix on the 180 bins from the moments, delta-M form */
+        surr_phase_matrix(legendre, chi, beta, gam, del, 1, out[p].F + (size_t)l * 6 * NA);
       }
       out[p].rho_av = (1.0 - s.por) * s.rho;
       out[p].mscale = 1.0;

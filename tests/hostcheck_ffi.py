@@ -13,7 +13,7 @@ SRC = os.path.join(HERE, "native", "hostcheck.cpp")
 LIB = os.path.join(HERE, "native", "libhostcheck.so")
 DEPS = [SRC] + [os.path.join(HERE, "..", "mcmax_b200", "csrc", f) for f in
                 ("dhs_core.cuh", "transport_core.cuh", "transport_fast.cuh", "diffuse_core.cuh", "dstruct_core.cuh",
-                 "rt_core.cuh", "detmath.h", "cplx.h", "philox.h")]
+                 "rt_core.cuh", "surrogate_phase.h", "detmath.h", "cplx.h", "philox.h")]
 
 
 class HcModel(C.Structure):
@@ -205,3 +205,12 @@ def trace_image(model, T, lam0, angle, npix, nint, Rmax, pa=0.0, seed=42, linear
                           C.c_double(Rmax), C.c_double(pa), C.c_ulonglong(seed), int(linear), P(flux), P(im), P(info))
     assert rc == 0
     return im.reshape(npix, npix), float(flux[0]), int(info[0]), int(info[1])
+
+
+def surr_phase(chi, beta, gam, delta, deltam=1):
+    """surrogate_phase.h: the Mueller matrix (6, 180) from Legendre moments"""
+    L = load()
+    a = [np.ascontiguousarray(x, float) for x in (chi, beta, gam, delta)]
+    F = np.zeros(6 * 180)
+    L.hc_surr_phase(P(a[0]), P(a[1]), P(a[2]), P(a[3]), int(deltam), P(F))
+    return F.reshape(6, 180)

@@ -12,6 +12,7 @@
 #include "../../mcmax_b200/csrc/diffuse_core.cuh"
 #include "../../mcmax_b200/csrc/dstruct_core.cuh"
 #include "../../mcmax_b200/csrc/rt_core.cuh"
+#include "../../mcmax_b200/csrc/surrogate_phase.h"
 
 extern "C" {
 
@@ -526,4 +527,11 @@ extern "C" int hc_trace_image(int nr, int nt, const double *R, const double *The
       if (key[m] < (uint32_t)npix * (uint32_t)npix) im[key[m]] = im[key[m]] + v;
   }
   return 0;
+}
+
+/* the surrogate's Mueller matrix F[6][180] from moments [0..12] */
+extern "C" void hc_surr_phase(const double *chi, const double *beta, const double *gam, const double *del, int deltam,
+                              double *F) {
+  static const SurrLegendre legendre;
+  surr_phase_matrix(legendre, chi, beta, gam, del, deltam, F);
 }
