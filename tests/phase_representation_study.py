@@ -11,7 +11,14 @@ events, and the inclination-summed SED where both sides have > 2500 packets.
 The exact matrix on seed 2 gives the Monte Carlo floor.  Six runs in
 parallel on the host cores; 1e7 packets take about 7 minutes.
 
-    python tests/phase_representation_study.py [NPHOT]"""
+With `network`, the runs use the trained surrogate's own predictions instead:
+the network (tests/mlp_ref.py, BF16 emulated) on each bin's sizes and
+wavelengths, aggregated over the sizes as mcg_compute_part_surrogate does,
+with its matrices rebuilt by delta-M or the plain series, and the two mixed
+cases (network opacities with exact matrices, exact opacities with the
+network's delta-M matrices).
+
+    python tests/phase_representation_study.py [NPHOT] [network]"""
 import json
 import math
 import multiprocessing as mp
@@ -41,6 +48,43 @@ def rebuild(F, dm):
     s0 = np.sum(F[0] * w)
     mom = [np.array([np.sum(F[e] * w * P[l]) / s0 for l in range(L + 1)]) for e in (0, 1, 3, 4)]
     return H.surr_phase(*mom, deltam=int(dm))
+
+
+def network_optics(parts, deltam):
+    """(Kabs, Ksca, F) of the trained surrogate for every bin, as
+    mcg_compute_part_surrogate forms them; None for a bin outside the
+    training box"""
+    import hostcheck_ffi as H
+    import mlp_ref as R
+    from mcmax_b200 import surrogate as S
+    params, _ = S.load(os.path.join(os.path.dirname(HERE), "mcmax_b200", "data", "surrogate_nf20.npz"))
+    out = []
+    for p in parts:
+        lam, n, k = np.asarray(p["lam"], float), np.atleast_2d(p["e1"])[0], np.atleast_2d(p["e2"])[0]
+        ns, por = int(p["ns"]), (p["porosity"] if p["blend"] else 0.0)
+        lo, hi = math.log10(p["amin"]), math.log10(p["amax"])
+        r = 10.0 ** (lo + (hi - lo) * np.arange(ns) / (ns - 1)) if ns > 1 else np.array([10.0 ** ((lo + hi) / 2)])
+        mw = r ** (-p["apow"] + 1.0) * r ** 3 if ns > 1 else np.ones(1)
+        mw = mw / mw.sum()
+        v = np.array([[math.log10(rk), math.log10(lam[l]), n[l], math.log10(k[l]), por, p["fmax"]]
+                      for rk in r for l in range(lam.size)])
+        if np.any(v < S.BOX_LO) or np.any(v > S.BOX_HI):
+            out.append(None)
+            continue
+        x = (2.0 * (v - S.BOX_LO) / (S.BOX_HI - S.BOX_LO) - 1.0).astype(np.float32)
+        y = R.forward(params, x)[0].astype(np.float64).reshape(ns, lam.size, -1)
+        scale = S.RHO_TRAIN / float(np.atleast_1d(p["rho"])[0])
+        ksk = 10.0 ** y[:, :, 1] * scale
+        kabs = np.sum(mw[:, None] * 10.0 ** y[:, :, 0] * scale, 0)
+        ksca = np.sum(mw[:, None] * ksk, 0)
+        wgt = mw[:, None] * ksk
+        F = np.zeros((lam.size, 6, NA))
+        for l in range(lam.size):
+            m = lambda i0, n0: np.sum(wgt[:, l, None] * y[:, l, i0:i0 + n0], 0) / wgt[:, l].sum()
+            chi = np.r_[1.0, m(2, L)]
+            F[l] = H.surr_phase(chi, m(14, L + 1), m(27, L + 1), m(40, L + 1), deltam=int(deltam))
+        out.append((kabs, ksca, F))
+    return out
 
 
 def build(nrad=60, ntheta=40, nlam=100, ngrains=10):
@@ -74,6 +118,7 @@ def build(nrad=60, ntheta=40, nlam=100, ngrains=10):
               V=V.reshape(-1), ncomp=len(parts), comp_w=w2.reshape(nr * nc, len(parts)), nlam=nlam, lam=lam, nu=nu,
               Kabs=Kabs, Ksca=Ksca, F=F, BB=BB, Fstar=Fstar, Lstar=Lstar, Tstar=10000.0, Rstar_cm=rstar_cm,
               scat_how=2, bins=bins, w=w0, rho_grain=rho_grain, rv=rv)
+    kw["_parts"] = parts
     return kw
 
 
@@ -83,12 +128,24 @@ def run(args):
     import oracle_ffi as O
     from mcmax_b200 import model as M
     kw = dict(kw)
-    if variant != "exact":
+    parts = kw.pop("_parts")
+    if variant in ("clipped", "deltam"):
         F = kw["F"].copy()
         for c in range(F.shape[0]):
             for l in range(F.shape[1]):
                 F[c, l] = rebuild(F[c, l], variant == "deltam")
         kw["F"] = F
+    elif variant != "exact":
+        net = network_optics(parts, variant != "net_plain")
+        Kabs, Ksca, F = kw["Kabs"].copy(), kw["Ksca"].copy(), kw["F"].copy()
+        for c, o in enumerate(net):
+            if o is None:
+                continue
+            if variant in ("net_deltam", "net_plain", "netk_exactF"):
+                Kabs[c], Ksca[c] = o[0], o[1]
+            if variant in ("net_deltam", "net_plain", "exactk_netF"):
+                F[c] = o[2]
+        kw.update(Kabs=Kabs, Ksca=Ksca, F=F)
     m = M.Model(**kw)
     t0 = time.time()
     o = O.mcradiation(m, nphot, seed=seed, randomwalk=True, factRW=10.0, maxinteract=100000)
@@ -102,9 +159,13 @@ if __name__ == "__main__":
     t0 = time.time()
     kw = build()
     print("built in %.0f s" % (time.time() - t0), flush=True)
-    jobs = [(kw, "exact", 1, nphot), (kw, "exact", 2, nphot), (kw, "clipped", 1, nphot), (kw, "deltam", 1, nphot),
-            (kw, "clipped", 3, nphot), (kw, "deltam", 3, nphot)]
-    with mp.get_context("spawn").Pool(6) as pool:
+    if "network" in sys.argv[2:]:
+        variants = [("exact", 2), ("net_deltam", 1), ("net_deltam", 3), ("net_plain", 1), ("netk_exactF", 1),
+                    ("exactk_netF", 1)]
+    else:
+        variants = [("exact", 2), ("clipped", 1), ("deltam", 1), ("clipped", 3), ("deltam", 3)]
+    jobs = [(kw, "exact", 1, nphot)] + [(kw, v, sd, nphot) for v, sd in variants]
+    with mp.get_context("spawn").Pool(min(len(jobs), os.cpu_count() or 1)) as pool:
         outs = pool.map(run, jobs)
     _, _, _, ej_ref, nabs_ref, spec_ref, ispec_ref, nt = outs[0]
     # cells outside the star cell with >= 1e3 absorption events in the reference run
