@@ -133,7 +133,8 @@ __device__ __forceinline__ float silu_fast(float z) {
  * Weights are stored in chunks of 64 input columns (mlp_pack_kernel).  Each
  * chunk serves the same layer of both tiles: a layer's MMAs alternate X chunk
  * c, Y chunk c, so the weights cross L2 once per 256 rows.  While the tensor
- * cores run a layer of one tile, the epilogue warps work on the other.
+ * cores run a layer of one tile, the epilogue warps work on the other.  When
+ * there are no more tiles than CTAs, each CTA takes one tile (slot X only).
  * Barriers: full / empty per weight slot (copy landed / MMAs done reading it);
  * ready per tile slot (all 512 epilogue threads have written the A operand
  * and read the accumulator); done per tile slot (MMA commit: the accumulator
