@@ -112,3 +112,34 @@ def test_delta_fraction_bounds():
     Fd = H.surr_phase(chi, np.zeros(L + 1), chi, np.zeros(L + 1), deltam=1)
     Fp = H.surr_phase(chi, np.zeros(L + 1), chi, np.zeros(L + 1), deltam=0)
     assert np.array_equal(Fd, Fp)
+
+
+def test_oracle_transport_with_delta_m_matrices_conserves_energy():
+    """A delta-M matrix puts a large value in the first angle bin; the
+    transport's angle tables take it like any other row: every run ends,
+    and the escaping energy is the star's (the model's matrices replaced by
+    their delta-M rebuilds from 12 moments)."""
+    import models
+    from mcmax_b200 import model as M
+    m = models.small_disk(nrad=20, ntheta=12, nlam=24, mdust=1e-4, amin=1.0, amax=30.0)
+    F = m.F.copy()
+    fmax = 0.0
+    for c in range(F.shape[0]):
+        for l in range(F.shape[1]):
+            mom = moments(m.F[c, l])
+            chi = mom[0]
+            if chi[L - 1] > 0 and chi[L] > 0:
+                fmax = max(fmax, min(chi[L] ** 2 / chi[L - 1], chi[L]))
+            F[c, l] = H.surr_phase(*mom, deltam=1)
+            check_sphere_constraints(F[c, l])
+    assert fmax > 0.3  # rows with a strong forward delta are in the model
+    out = O.mcradiation(M.Model(**{**m.__dict__, "F": F}), 20000, seed=5)
+    assert out["status"] == 0
+    nu = m.nu
+    dn = np.empty_like(nu)
+    dn[0], dn[-1], dn[1:-1] = nu[1] / 2, (nu[-1] - nu[-2]) / 2, (nu[2:] - nu[:-2]) / 2
+    cos = np.arange(31) / 30.0
+    wang = 1.0 / (cos[1:] - cos[:-1])
+    e = out["spec"][:, 1:] / ((-1e23 / dn)[:, None] * wang[None, :])
+    assert abs(e.sum() / m.Lstar - 1) < 0.02
+    assert np.all(np.isfinite(out["EJv"])) and np.all(out["EJv"] >= 0)
